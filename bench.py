@@ -1,0 +1,492 @@
+#!/usr/bin/env python
+"""Benchmark of the SCBA hot path: the operator-level batch of the
+(E, k) Green's-function solves.
+
+Workload (one "step"): N_E x N_k = 4096 x 32 blocks of size N_b = 24 --
+the batched retarded Dyson solve G^R = (E - h - Sigma^R)^-1, the Keldysh
+product G^< = G^R Sigma^< G^A, and the zero-padded length-8192 FFT Hilbert
+transform of Gamma over all N_k N_b^2 columns, in complex128 (FP64).  The
+metric is (E, k) Green solves per second.  Inputs are seeded synthetic fields
+with the stated distributions (h Hermitian block-tridiagonal, Sigma^R
+negative-definite anti-Hermitian part ~1 meV, Sigma^< = i PSD ~0.5 meV);
+each field is 1.2 GB, far larger than L2.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+With N > 1 (torchrun, one process per GPU) every rank runs an independent
+replica of the batch (the path does not shard) and `value` is the total over
+ranks divided by the slowest rank's time.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import math
+import os
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "qclnegf.jl_b200"))
+
+NE, NK, NB = 4096, 32, 24
+E0_EV = 0.1
+# Roofline accounting of the dominant kernel (Dyson + Keldysh, G^R and G^<):
+# FP64 flop per block = 8 N^3 (LU + inverse) + 16 N^3 (one triple product);
+# bytes per block = read Sigma^R, Sigma^< + write G^R, G^< = 4 * 16 N^2.
+FLOP_PER_BLOCK = 24 * NB ** 3
+BYTES_PER_BLOCK = 4 * 16 * NB * NB
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-extras", action="store_true", help="skip the variant and SCBA side measurements")
+    return ap.parse_args()
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+# ---------------------------------------------------------------------------
+# clocks sampled during the timed region
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    def __init__(self, index=0):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        mhz, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            p = [x.strip() for x in ln.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                mhz.append(float(p[1]))
+                mx = float(p[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, p[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        if not mhz:
+            return None
+        mhz.sort()
+        return {"sm_mhz": mhz[len(mhz) // 2], "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(mhz)}
+
+
+# ---------------------------------------------------------------------------
+# inputs
+# ---------------------------------------------------------------------------
+def grids():
+    import numpy as np
+    from qclb200.problem import energy_grid
+
+    eps, wE = energy_grid(-0.05 / E0_EV, 0.35 / E0_EV, NE)
+    return eps, wE
+
+
+def device_inputs(torch, dev, N, seed, cdt):
+    """Sigma^R, Sigma^<, Gamma as E-fastest (Julia-layout) device fields."""
+    import numpy as np
+    from qclb200.problem import operator_batch_hamiltonian
+
+    h, wk, _ = operator_batch_hamiltonian(N, NK, seed=seed)
+    g = torch.Generator(device=dev)
+    g.manual_seed(seed)
+
+    def psd(scale):
+        out = torch.empty((N, N, NK, NE), dtype=cdt, device=dev)
+        chunk = 4  # momenta per chunk keeps the temporaries small
+        for m0 in range(0, NK, chunk):
+            X = torch.randn((chunk * NE, N, N), dtype=torch.complex128, device=dev, generator=g)
+            P = (X @ X.mH) * (scale / N)
+            # batch index (m, e) -> element (e, m, a, b) at [b, a, m, e]
+            out[:, :, m0:m0 + chunk, :] = P.reshape(chunk, NE, N, N).permute(3, 2, 0, 1).to(cdt)
+            del X, P
+        return out
+
+    PR = psd(0.01)  # ~1 meV broadening (solver units E0 = 0.1 eV)
+    SR = (-1j) * PR
+    SL = 1j * psd(0.005)
+    Gam = (2.0 * PR).contiguous()  # i (SR - SR^H) = 2 P
+    hf = torch.from_numpy(np.asfortranarray(h).ravel(order="F").copy()).to(dev)
+    return hf, SR.contiguous(), SL.contiguous(), Gam
+
+
+def cpu_inputs(N, m_count, seed):
+    """The same distributions on the host, for m_count momenta."""
+    import numpy as np
+    from qclb200.problem import operator_batch_hamiltonian
+
+    h, wk, _ = operator_batch_hamiltonian(N, NK, seed=seed)
+    h = np.asfortranarray(h[:m_count])
+    rng = np.random.default_rng(seed)
+
+    def psd(scale):
+        X = rng.standard_normal((NE, m_count, N, N)) + 1j * rng.standard_normal((NE, m_count, N, N))
+        return np.asfortranarray(np.einsum("emab,emcb->emac", X, np.conj(X)) * (scale / N))
+
+    PR = psd(0.01)
+    return h, np.asfortranarray(-1j * PR), np.asfortranarray(1j * psd(0.005)), np.asfortranarray(2 * PR)
+
+
+# ---------------------------------------------------------------------------
+# CPU path (the reference algorithm on the host cores: the oracle port)
+# ---------------------------------------------------------------------------
+def cpu_step(orc, eps, wE, h, SR, SL, Gam):
+    orc.dyson_keldysh(eps, h, SR, SL)
+    orc.fft_hilbert(Gam, eps, wE)
+
+
+def cpu_rate(m_count=4, reps=1, warm=0):
+    """Green solves/s of the CPU port on m_count momenta (all energies)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as orc
+
+    eps, wE = grids()
+    h, SR, SL, Gam = cpu_inputs(NB, m_count, seed=11)
+    for _ in range(warm):
+        cpu_step(orc, eps, wE, h, SR, SL, Gam)
+    t = []
+    for _ in range(reps):
+        t0 = time.perf_counter()
+        cpu_step(orc, eps, wE, h, SR, SL, Gam)
+        t.append(time.perf_counter() - t0)
+    t.sort()
+    sec = t[len(t) // 2]
+    return NE * m_count / sec, sec
+
+
+def cores():
+    try:
+        return len(os.sched_getaffinity(0))
+    except Exception:
+        return os.cpu_count() or 1
+
+
+# ---------------------------------------------------------------------------
+# distributed plumbing
+# ---------------------------------------------------------------------------
+def dist_init(args):
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    if ws > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+        dist.init_process_group("nccl" if args.impl == "ours" else "gloo", timeout=datetime.timedelta(seconds=120))
+        return dist, dist.get_rank(), ws
+    return None, 0, 1
+
+
+def run_reference(args):
+    dist, rank, ws = dist_init(args)
+    if rank != 0:
+        if dist:
+            dist.destroy_process_group()
+        return
+    m_count = 4  # a bounded sample of 4 of the 32 momenta (all 4096 energies) per step
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as orc
+
+    eps, wE = grids()
+    h, SR, SL, Gam = cpu_inputs(NB, m_count, seed=11)
+    for _ in range(args.warmup):
+        cpu_step(orc, eps, wE, h, SR, SL, Gam)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        cpu_step(orc, eps, wE, h, SR, SL, Gam)
+    sec = (time.perf_counter() - t0) / args.steps
+    rate = NE * m_count / sec
+    full_ms = NE * NK / rate * 1e3
+    sample = f"{m_count} of {NK} momenta x {NE} energies per step (Dyson+Keldysh and the Hilbert columns of those momenta)"
+    line = {
+        "impl": "reference", "metric": "(E,k) Green solves/s", "value": rate, "unit": "solves/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": full_ms,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64 (complex128)",
+        "data": "synthetic", "config": {"workload": f"operator batch N_E x N_k = {NE} x {NK}, N_b = {NB}, "
+                                                    "Dyson + Keldysh G^< + FFT Hilbert (L = 8192)"},
+        "cpu_baseline": {"value": rate, "unit": "solves/s", "cores": cores(), "kind": "port", "sample": sample},
+        "e2e": {"value": rate, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    if dist:
+        dist.destroy_process_group()
+
+
+# ---------------------------------------------------------------------------
+# GPU arm
+# ---------------------------------------------------------------------------
+def run_gpu(args):
+    import numpy as np
+    import torch
+
+    from qclb200 import _lib
+
+    dist, rank, ws = dist_init(args)
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    L = _lib.lib()
+    P = ctypes.c_void_p
+    prec = _lib.QCL_C128
+    cdt = torch.complex128
+    eps, wE = grids()
+    de = float(eps[1] - eps[0])
+    eps_d = torch.tensor(eps, dtype=torch.float64, device=dev)
+    wE_d = torch.tensor(wE, dtype=torch.float64, device=dev)
+    hf, SR, SL, Gam = device_inputs(torch, dev, NB, seed=7 + rank, cdt=cdt)
+    GR = torch.empty_like(SR)
+    GL = torch.empty_like(SR)
+    Lam = torch.empty_like(Gam)
+    status = torch.zeros(2, dtype=torch.int32, device=dev)
+    stream = torch.cuda.current_stream(dev)
+    sp = P(stream.cuda_stream)
+    ncols = NK * NB * NB
+    launches = [0]
+
+    def dyson():
+        st = L.qcl_dev_dyson_keldysh(sp, prec, NE, NK, NB, P(eps_d.data_ptr()), 0.0, P(hf.data_ptr()),
+                                     P(SR.data_ptr()), P(SL.data_ptr()), None, P(GR.data_ptr()), P(GL.data_ptr()),
+                                     None, None, None, None, P(status.data_ptr()))
+        _lib.check(st)
+        launches[0] += 1
+
+    def hilbert():
+        _lib.check(L.qcl_dev_fft_hilbert_transform(sp, prec, NE, ncols, de, P(wE_d.data_ptr()), P(Gam.data_ptr()),
+                                                   P(Lam.data_ptr()), None))
+        launches[0] += 1
+
+    for _ in range(max(args.warmup, 3)):
+        dyson()
+        hilbert()
+    torch.cuda.synchronize()
+    if int(status[0]) != 0:
+        raise RuntimeError(f"device status {status.tolist()}")
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    launches[0] = 0
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    t0 = torch.cuda.Event(enable_timing=True)
+    t1 = torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        t0.record(stream)
+        for i in range(args.steps):
+            ev[i][0].record(stream)
+            dyson()
+            ev[i][1].record(stream)
+            hilbert()
+        t1.record(stream)
+        torch.cuda.synchronize()
+    total_ms = t0.elapsed_time(t1)
+    dyson_ms = sum(a.elapsed_time(b) for a, b in ev) / args.steps
+    step_ms = total_ms / args.steps
+    if dist:
+        tt = torch.tensor([step_ms], device=dev)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        step_ms = float(tt.item())
+    value = ws * NE * NK / (step_ms / 1e3)
+    gpu_launches = launches[0]
+
+    # ---- end to end through the host-buffer C ABI (pinned host arrays) ------------
+    e2e = None
+    if rank == 0 or True:
+        hSR = SR.cpu().pin_memory()
+        hSL = SL.cpu().pin_memory()
+        hGam = Gam.cpu().pin_memory()
+        hGR = torch.empty_like(hSR).pin_memory()
+        hGL = torch.empty_like(hSR).pin_memory()
+        hLam = torch.empty_like(hGam).pin_memory()
+        h_host = hf.cpu().numpy()
+        eps_c = np.ascontiguousarray(eps)
+        wE_c = np.ascontiguousarray(wE)
+
+        def e2e_step():
+            _lib.check(L.qcl_dyson_keldysh(prec, NE, NK, NB, P(eps_c.ctypes.data), 0.0, P(h_host.ctypes.data),
+                                           P(hSR.data_ptr()), P(hSL.data_ptr()), None, P(hGR.data_ptr()),
+                                           P(hGL.data_ptr()), None, None, None, None))
+            _lib.check(L.qcl_fft_hilbert_transform(prec, NE, ncols, P(eps_c.ctypes.data), P(wE_c.ctypes.data),
+                                                   P(hGam.data_ptr()), P(hLam.data_ptr()), None))
+
+        e2e_step()
+        torch.cuda.synchronize()
+        k = max(2, min(args.steps, 5))
+        if dist:
+            dist.barrier()
+        t = time.perf_counter()
+        for _ in range(k):
+            e2e_step()
+        torch.cuda.synchronize()
+        e2e_ms = (time.perf_counter() - t) / k * 1e3
+        if dist:
+            tt = torch.tensor([e2e_ms], device=dev)
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+            e2e_ms = float(tt.item())
+        fb = NE * NK * NB * NB * 16
+        e2e = {"value": ws * NE * NK / (e2e_ms / 1e3), "unit": "solves/s", "h2d_bytes_per_step": 3 * fb,
+               "d2h_bytes_per_step": 3 * fb, "ms_per_step": e2e_ms,
+               "path": "qcl_dyson_keldysh + qcl_fft_hilbert_transform with pinned host buffers"}
+        # parity of this very run: GPU G^< equals the device-resident result
+        diff = float((hGL.to(dev) - GL).abs().max().item())
+        e2e["max_abs_diff_vs_device_run"] = diff
+        del hSR, hSL, hGam, hGR, hGL, hLam
+
+    peak, peak_kind = measured_peaks()
+    achieved_gbs = BYTES_PER_BLOCK * NE * NK / (dyson_ms / 1e3) / 1e9
+    achieved_tflops = FLOP_PER_BLOCK * NE * NK / (dyson_ms / 1e3) / 1e12
+    fp64_nominal = 148 * 64 * 2 * 1.965e9 / 1e12
+    line = {
+        "metric": "(E,k) Green solves/s", "value": value, "unit": "solves/s", "n_gpus": ws, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64 (complex128)", "data": "synthetic (seeded)",
+        "config": {"workload": f"operator batch N_E x N_k = {NE} x {NK}, N_b = {NB}: Dyson G^R + Keldysh G^< + "
+                               f"FFT Hilbert of Gamma (L = 8192, {ncols} columns)",
+                   "l2": "inputs larger than L2 (each field 1.2 GB)", "parallelism": f"replicas x{ws}"},
+        "roofline": {"bound": "hbm", "achieved": achieved_gbs, "peak": peak, "unit": "GB/s",
+                     "frac": achieved_gbs / peak, "traffic": None, "kernel": "dyson_keldysh_kernel",
+                     "kernel_ms": dyson_ms, "peak_kind": peak_kind,
+                     "fp64_tflops": achieved_tflops, "fp64_nominal_tflops": fp64_nominal,
+                     "fp64_frac_of_nominal": achieved_tflops / fp64_nominal},
+        "gpu_launches": gpu_launches,
+        "e2e": e2e,
+    }
+    # ---- CPU baseline on the host cores (rank 0, N = 1) ------------------------------
+    if ws == 1:
+        try:
+            rate, sec = cpu_rate(m_count=4)
+            line["cpu_baseline"] = {"value": rate, "unit": "solves/s", "cores": cores(), "kind": "port",
+                                    "sample": f"4 of {NK} momenta x {NE} energies ({sec:.1f} s)"}
+        except Exception as ex:  # noqa: BLE001
+            line["cpu_baseline"] = {"value": None, "error": str(ex)}
+    line["clocks"] = clk.summary()
+    if rank == 0:
+        if not args.no_extras and ws == 1:
+            try:
+                line["extras"] = extras(torch, dev, L, _lib)
+            except Exception as ex:  # noqa: BLE001
+                line["extras"] = {"error": repr(ex)}
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def extras(torch, dev, L, _lib):
+    """Side measurements: complex64 / mixed Dyson, N_b = 48, and SCBA
+    iterations/s of the tutorial-scale problem (FP64 vs mixed, J error)."""
+    import numpy as np
+
+    P = ctypes.c_void_p
+    out = {}
+    eps, wE = grids()
+    eps_d = torch.tensor(eps, dtype=torch.float64, device=dev)
+    s = torch.cuda.current_stream(dev)
+    sp = P(s.cuda_stream)
+    for N, prec, name in ((24, _lib.QCL_C64, "c64_N24"), (24, _lib.QCL_MIXED, "mixed_N24"),
+                          (48, _lib.QCL_C128, "c128_N48"), (48, _lib.QCL_MIXED, "mixed_N48")):
+        cdt = torch.complex128 if prec == _lib.QCL_C128 else torch.complex64
+        hf, SR, SL, _ = device_inputs(torch, dev, N, seed=3, cdt=cdt)
+        GR = torch.empty_like(SR)
+        GL = torch.empty_like(SR)
+        st = torch.zeros(2, dtype=torch.int32, device=dev)
+
+        def call():
+            _lib.check(L.qcl_dev_dyson_keldysh(sp, prec, NE, NK, N, P(eps_d.data_ptr()), 0.0, P(hf.data_ptr()),
+                                               P(SR.data_ptr()), P(SL.data_ptr()), None, P(GR.data_ptr()),
+                                               P(GL.data_ptr()), None, None, None, None, P(st.data_ptr())))
+
+        for _ in range(3):
+            call()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(s)
+        for _ in range(5):
+            call()
+        b.record(s)
+        torch.cuda.synchronize()
+        ms = a.elapsed_time(b) / 5
+        out[name] = {"dyson_keldysh_ms": ms, "solves_per_s": NE * NK / (ms / 1e3)}
+        del SR, SL, GR, GL
+        torch.cuda.empty_cache()
+    # SCBA iterations/s at tutorial scale
+    from qclb200.problem import tutorial_problem
+    from qclb200.scba import ProductionSCBA
+
+    pr = tutorial_problem()
+    res = {}
+    Jref = None
+    for precision in ("c128", "mixed"):
+        solver = ProductionSCBA(pr, precision=precision, use_graph=True)
+        solver.seed()
+        rows = [solver.step() for _ in range(3)]
+        torch.cuda.synchronize()
+        t = time.perf_counter()
+        n = 27
+        for _ in range(n):
+            rows.append(solver.step())
+        sec = (time.perf_counter() - t) / n
+        J = [r["J"] for r in rows]
+        res[precision] = {"iter_per_s": 1.0 / sec, "ms_per_iter": sec * 1e3, "J_final": J[-1],
+                          "r_Sigma_final": rows[-1]["r_Sigma"]}
+        if precision == "c128":
+            Jref = J
+        else:
+            res[precision]["J_rel_err_vs_fp64"] = max(abs(a - b) / abs(a) for a, b in zip(Jref, J))
+        solver.close()
+    out["scba_tutorial_N12_30iter"] = res
+    return out
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_gpu(args)
+
+
+if __name__ == "__main__":
+    main()

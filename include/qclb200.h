@@ -1,0 +1,254 @@
+/*
+ * qclb200 -- C ABI of the B200 (sm_100a) SCBA hot path for QCLNEGF.jl.
+ *
+ * Every entry point returns an int status (QCL_OK on success); the message of
+ * the last failure on the calling thread is available from qcl_last_error().
+ * The Julia shim maps the codes to the reference's exceptions exactly as the
+ * reference maps LAPACK's `info` (numerics/optimized/production_operators.jl:
+ * 39-61): QCL_SINGULAR -> SingularException, QCL_DOMAIN -> DomainError,
+ * QCL_DIM -> DimensionMismatch, QCL_ARG -> ArgumentError, QCL_NONFINITE ->
+ * the :nonfinite_metrics status (numerics/optimized/production_solver.jl:
+ * 624-656).
+ *
+ * Array convention (all entry points): the reference's Julia layout.  A field
+ * is a column-major (N_E, N_k, N_b, N_b) array of complex numbers stored as
+ * interleaved (re, im) pairs, energy fastest: element (e, m, a, b) (0-based)
+ * is at e + N_E*(m + N_k*(a + N_b*b)).  h is (N_k, N_b, N_b) complex128.
+ * Matrices are column-major.  `precision` selects the storage/arithmetic:
+ *   QCL_C128  complex128 fields, FP64 arithmetic (the reference's precision);
+ *   QCL_C64   complex64 fields, FP32 arithmetic;
+ *   QCL_MIXED complex64 fields, FP64 Dyson inversion, FP32 products,
+ *             FP64 reductions.
+ * Host-buffer entry points (qcl_<name>) take host pointers, copy in, compute
+ * and copy out; device entry points (qcl_dev_<name>) take device pointers and
+ * a cudaStream_t (NULL = legacy default stream) and are asynchronous.
+ */
+#ifndef QCLB200_H
+#define QCLB200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define QCL_OK 0
+#define QCL_SINGULAR 1
+#define QCL_DOMAIN 2
+#define QCL_DIM 3
+#define QCL_ARG 4
+#define QCL_NONFINITE 5
+#define QCL_TIMEOUT 6
+#define QCL_CUDA 7
+#define QCL_NOMEM 8
+#define QCL_UNSUPPORTED 9
+
+#define QCL_KERNEL_MOMENTUM_INDEPENDENT 0
+#define QCL_KERNEL_DENSE 1
+#define QCL_KERNEL_IFR 2
+
+#define QCL_C128 0
+#define QCL_C64 1
+#define QCL_MIXED 2
+
+/* Library version (major*10000 + minor*100 + patch). */
+int qcl_version(void);
+/* Message of the last failing call on this thread ("" if none). */
+const char* qcl_last_error(void);
+/* Largest supported basis size N_b. */
+int qcl_max_basis(void);
+
+/* ------------------------------------------------------------------------ */
+/* Operator level                                                           */
+/* ------------------------------------------------------------------------ */
+
+/* Batched retarded Dyson solve and raw Keldysh products.
+ * Replaces retarded_green (numerics/reference/greens.jl:18-42) /
+ * _retarded_green_production (numerics/optimized/production_operators.jl:
+ * 1337-1385) fused with keldysh_green (greens.jl:67-75) and the sandwiches of
+ * _current_green_production (numerics/optimized/production_state.jl:23-48).
+ * GR = inv(D/s)/s, D = (eps+i eta)I - h - sigR, s = max row sum |D|;
+ * GL = GR sigL GR^H; GG = GR sigG GR^H.  sigL/sigG/GR/GL/GG/scale/traceL/
+ * traceG may be NULL (the matching product or output is skipped).  scale is
+ * (N_E, N_k) float64; traceL/traceG are (N_E, N_k) complex128 raw block
+ * traces (unweighted).  A singular block returns QCL_SINGULAR. */
+int qcl_dyson_keldysh(int precision, int NE, int Nk, int Nb, const double* eps, double eta, const void* h,
+                      const void* sigR, const void* sigL, const void* sigG, void* GR, void* GL, void* GG,
+                      double* scale, void* traceL, void* traceG);
+int qcl_dev_dyson_keldysh(void* stream, int precision, int NE, int Nk, int Nb, const double* eps, double eta,
+                          const void* h, const void* sigR, const void* sigL, const void* sigG, void* GR, void* GL,
+                          void* GG, double* scale, void* traceL, void* traceG, int* status);
+
+/* Weighted trace sum  sum_{e,m} wE_e wk_m tr_em  in FP64 with a fixed
+ * reduction order; out = (re, im).  Replaces the sum of
+ * _number_functional_production (production_operators.jl:1417-1445). */
+int qcl_dev_weighted_trace(void* stream, int NE, int Nk, const void* trace, const double* wE, const double* wk,
+                           double* out);
+
+/* Paired number normalisation, in place on device fields:
+ * GL <- a GL - c GG,  GG <- (1-c) GG - (1-a) GL  with (a, c, lambda) from
+ * _paired_number_coefficients (numerics/reference/greens.jl:155-185) applied
+ * as in production_state.jl:62-70.  coeffs = device double[3] (a, c, lambda)
+ * produced by qcl_dev_paired_coefficients. */
+int qcl_dev_paired_coefficients(void* stream, const double* trL, const double* trG, int gs, double target,
+                                double* coeffs, int* status);
+int qcl_dev_normalize_pair(void* stream, int precision, size_t n, void* GL, void* GG, const double* coeffs);
+
+/* Zero-padded linear-convolution Hilbert transform of the columns of an
+ * (N_E, ncols) complex array: Lam_e = sum_{e'!=e} wE_e' Gam_e' /
+ * (2 pi (eps_e - eps_e')) on a uniform grid, through FFTs of length
+ * L = nextpow2(2 N_E - 1).  Replaces fft_hilbert_transform /
+ * production_fft_hilbert_transform (production_operators.jl:793-809,
+ * numerics/optimized/fft_parallel.jl:266-291).  If roundoff != NULL the
+ * transform is repeated at length 2L and ||Lam_2L - Lam_L||/(||Lam_L||+1e-14)
+ * is returned there (fft_parallel.jl:279-290). */
+int qcl_fft_hilbert_transform(int precision, int NE, size_t ncols, const double* eps, const double* wE,
+                              const void* Gam, void* Lam, double* roundoff);
+
+/* Device variant (asynchronous on `stream`): de is the uniform energy
+ * spacing, wE a device array.  If roundoff_sums != NULL it receives (device,
+ * 2 doubles) sum |Lam_2L - Lam_L|^2 and sum |Lam_L|^2. */
+int qcl_dev_fft_hilbert_transform(void* stream, int precision, int NE, size_t ncols, double de, const double* wE,
+                                  const void* Gam, void* Lam, double* roundoff_sums);
+
+/* Retarded self-energy from the Keldysh components: Gam = i (SG - SL),
+ * SR = H[Gam] - i Gam/2 (retarded_self_energy_fft / _retarded_self_energy_
+ * fft_production, production_operators.jl:811-884).  Gam may be NULL. */
+int qcl_retarded_self_energy(int precision, int NE, size_t ncols, const double* eps, const double* wE,
+                             const void* SL, const void* SG, void* SR, void* Gam, double* roundoff);
+
+/* Non-periodic two-point energy shift X(eps + delta) of the columns of an
+ * (N_E, ncols) array, zero outside the window.  Replaces build_shift_plan +
+ * apply_energy_shift! (numerics/optimized/production_cache.jl:258-325). */
+int qcl_apply_energy_shift(int precision, int NE, size_t ncols, const double* eps, double delta, const void* X,
+                           void* Y);
+
+/* One factorised scattering-kernel operator (the AbstractProductionKernel
+ * subtypes of numerics/optimized/production_contracts.jl:262-323, built by
+ * production_cache.jl:387-448).  Arrays are complex128, column-major:
+ *   QCL_KERNEL_MOMENTUM_INDEPENDENT  block  (N^2, N^2), rows (a,b), cols (c,d)
+ *   QCL_KERNEL_DENSE                 matrix (Nk N^2)^2, rows (m,a,b), cols (m',c,d)
+ *   QCL_KERNEL_IFR                   left (N^2, J), right (J, N^2), radial (Nk, Nk)
+ * q is the kernel scale q^K; is_LO selects the phonon-shifted contraction in
+ * the SCBA loop. */
+typedef struct qcl_mechanism {
+  int kind;
+  int is_LO;
+  int J;
+  double q;
+  const void* block;
+  const void* matrix;
+  const void* left;
+  const void* right;
+  const void* radial;
+} qcl_mechanism;
+
+/* S = beta S + alpha q K[wk G]: production_static_contraction /
+ * _production_static_contraction! (production_operators.jl:402-722). */
+int qcl_static_contraction(int precision, const qcl_mechanism* op, int NE, int Nk, int Nb, const double* wk,
+                           double alpha, double beta, const void* G, void* S);
+
+/* Shifted sandwich S(e) = T G(eps_e + delta) T^H for one field:
+ * _embedding_component_production (production_operators.jl:886-922). */
+int qcl_embedding_component(int precision, int NE, int Nk, int Nb, const double* eps, double delta, const void* T,
+                            const void* G, void* S);
+
+/* Fixed-point residual suite, out = (r_D, r_A, r_K, r_PSD, r_caus):
+ * production_residual_suite (numerics/optimized/residuals.jl:537-770).
+ * SR/SL/SG are the current totals, SLc the candidate total lesser. */
+int qcl_residual_suite(int precision, int NE, int Nk, int Nb, const double* eps, const void* h, const void* GR,
+                       const void* GL, const void* GG, const void* SR, const void* SL, const void* SG,
+                       const void* SLc, double* out);
+
+/* Eigenvalues (unsorted) of `count` Hermitian n x n matrices stored back to
+ * back (column-major complex128; the Hermitian part is used), n <= 48.
+ * Replaces the per-block LAPACK zheev calls of the residual suite
+ * (_production_hermitian_eigvals!, numerics/optimized/residuals.jl:311-353). */
+int qcl_hermitian_eigvals(int n, size_t count, const void* H, double* vals);
+
+/* out = ||new - old||_F / (||new||_F + 1e-14) for one component
+ * (production_selfenergy_residual, residuals.jl:802-865). */
+int qcl_selfenergy_residual(int precision, size_t n, const void* old_, const void* new_, double* out);
+
+/* Boundary flux and populations: out[0] = Jbar (solver units,
+ * _production_boundary_flux_bar, production_iteration.jl:174-201),
+ * out[1] = imaginary part of the complex flux (diagnostic), out[2 + a] =
+ * population p_a (_production_state_populations, :204-215).  SG/SL are the
+ * plus-embedding family components. */
+int qcl_current_populations(int precision, int NE, int Nk, int Nb, const double* wE, const double* wk, int gs,
+                            double target, const void* SG, const void* SL, const void* GL, const void* GG,
+                            double* out);
+
+/* ------------------------------------------------------------------------ */
+/* SCBA level: one device-resident production cache + state per context    */
+/* ------------------------------------------------------------------------ */
+
+/* The inputs solve_scba_production consumes at fixed Hartree potential
+ * (numerics/optimized/production_solver.jl:21-846), in solver units
+ * (domain/scaling.jl:10-110).  eps is uniform (FFT Hilbert); Tminus =
+ * Tplus^H (numerics/reference/basis.jl:56-57). */
+typedef struct qcl_scba_problem {
+  int NE, Nk, Nb;
+  const double* eps;
+  const double* wE;
+  const double* wk;
+  const void* h;      /* (Nk, Nb, Nb) complex128 */
+  const void* Tplus;  /* (Nb, Nb) complex128 */
+  const void* Tminus; /* (Nb, Nb) complex128 */
+  double Ep;          /* period energy drop F L_p */
+  double hw_LO;       /* LO phonon energy */
+  double N_LO;        /* thermal LO occupation */
+  int gs;             /* spin degeneracy */
+  double target;      /* sheet doping N_D in solver units */
+  double eta_seed;    /* seed broadening */
+  double kBT;         /* lattice temperature in solver units */
+  double alpha;       /* linear mixing factor in (0, 1] */
+  double J0;          /* current unit in A/m^2 */
+  int precision;      /* QCL_C128 / QCL_C64 / QCL_MIXED */
+  int verify_roundoff;/* repeat each Hilbert transform at 2L */
+  int nmech;          /* number of mechanisms, in _SCATTERING_MECHANISM_ORDER */
+} qcl_scba_problem;
+
+/* One SCBAIteration row (domain/types.jl:908).  status: QCL_OK or
+ * QCL_NONFINITE (the :nonfinite_metrics exit). */
+typedef struct qcl_scba_row {
+  int nu;
+  int status;
+  double r_D, r_A, r_K, r_Sigma, r_lambda, lambda, r_PSD, r_caus, r_roundoff;
+  double r_J, r_pop, J, Jbar, number, holes, occupied_fraction, empty_fraction;
+} qcl_scba_row;
+
+typedef struct qcl_scba qcl_scba;
+
+/* Allocates the device state and uploads grids, h, T+-, shift plans and
+ * kernel operators (build_production_cache, production_cache.jl:759-840). */
+int qcl_scba_create(const qcl_scba_problem* problem, const qcl_mechanism* mechanisms, qcl_scba** out);
+void qcl_scba_destroy(qcl_scba* ctx);
+/* Equilibrium seed + initial candidates (_seed_green_production,
+ * numerics/optimized/seed.jl:151-197); mu receives the seed chemical
+ * potential. */
+int qcl_scba_seed(qcl_scba* ctx, double* mu);
+/* One SCBA iteration (production_solver.jl:435-844).  The linear mixing of
+ * the iteration is committed when the next step starts, so a caller that
+ * stops after reading `row` keeps the unmixed state, as the reference does on
+ * a terminal decision. */
+int qcl_scba_step(qcl_scba* ctx, qcl_scba_row* row);
+/* Up to max_iter steps, stopping early once r_Sigma <= tol_sigma or on a
+ * non-finite row; history receives n_done rows. */
+int qcl_scba_run(qcl_scba* ctx, int max_iter, double tol_sigma, qcl_scba_row* history, int* n_done);
+/* Populations p_a of the last step (N_b doubles). */
+int qcl_scba_populations(qcl_scba* ctx, double* out);
+/* Checkpoint / warm start.  which: 0, 1, 2 = GR, G<, G> of the last step;
+ * 3 + 3 f + c = family f (0..nmech-1 mechanisms, nmech plus, nmech+1 minus),
+ * component c (0 R, 1 <, 2 >) of the current state. */
+int qcl_scba_download(qcl_scba* ctx, int which, void* host);
+int qcl_scba_upload(qcl_scba* ctx, int which, const void* host);
+/* Replay each iteration as one captured CUDA graph (default off). */
+int qcl_scba_use_graph(qcl_scba* ctx, int enable);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* QCLB200_H */

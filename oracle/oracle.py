@@ -1,0 +1,539 @@
+"""Python driver of the CPU FP64 oracle (test infrastructure only).
+
+Binds ``oracle/_build/liborc.so`` (built from ``qcl_oracle.c`` by
+``oracle/Makefile``) with ctypes and composes the reference's SCBA inner
+loop from its operators, following ``numerics/reference/scba.jl:142-354``
+(educational loop) with the production operator choices of
+``numerics/optimized/production_solver.jl:435-844`` (sparse shift plans,
+FFT Hilbert with roundoff verification, factorised kernel operators, paired
+number normalisation, linear mixing).
+
+Only tests, the smoke check and the benchmark's CPU-baseline leg import this
+module.  Arrays follow the Julia layout: numpy Fortran order, fields of
+shape (N_E, N_k, N_b, N_b).
+"""
+from __future__ import annotations
+
+import ctypes
+import math
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB = None
+
+REALNESS_LIMIT = 1.0e-10  # _NUMBER_FUNCTIONAL_REALNESS_LIMIT (domain/numerical_invariants.jl:5)
+FERMI_SATURATION = 40.0  # _FERMI_EXPONENT_SATURATION (domain/numerical_invariants.jl:10)
+
+
+class OracleError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"{msg} (status {code})")
+        self.code = code
+
+
+def build():
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+
+
+def lib():
+    """The loaded library.  Each wrapper calls lib() before building its
+    argument list; that is where the previous call's temporaries are dropped."""
+    del _ALIVE[:]
+    global _LIB
+    if _LIB is None:
+        path = os.path.join(_HERE, "_build", "liborc.so")
+        if not os.path.exists(path):
+            build()
+        _LIB = ctypes.CDLL(path)
+        _declare(_LIB)
+    return _LIB
+
+
+P = ctypes.c_void_p
+I = ctypes.c_int
+D = ctypes.c_double
+Z = ctypes.c_size_t
+L = ctypes.c_long
+
+
+def _declare(l):
+    sig = {
+        "orc_inverse": (I, [I, P, P, P]),
+        "orc_hermitian_eigvals": (None, [I, P, P]),
+        "orc_retarded_green": (I, [I, I, I, P, D, P, P, P, P, P, P, P]),
+        "orc_keldysh_green": (None, [I, I, I, P, P, P]),
+        "orc_greater_green": (None, [I, I, I, P, P, P]),
+        "orc_spectral_function": (None, [I, I, I, P, P]),
+        "orc_number_functional": (I, [I, I, I, P, P, P, I, D, P]),
+        "orc_paired_coefficients": (I, [D, D, D, P, P, P]),
+        "orc_normalize_pair": (None, [Z, P, P, D, D]),
+        "orc_shift_plan": (I, [I, P, D, P, P, P, P]),
+        "orc_apply_shift": (None, [I, Z, P, P, P, P, P, P]),
+        "orc_shift_matrix": (None, [I, P, D, P]),
+        "orc_contraction_literal": (None, [I, I, I, P, P, P, D, P]),
+        "orc_contraction_momentum_independent": (None, [I, I, I, P, P, P, D, D, P]),
+        "orc_contraction_dense": (None, [I, I, I, P, P, P, D, D, P]),
+        "orc_contraction_ifr": (None, [I, I, I, I, P, P, P, P, P, D, D, P]),
+        "orc_direct_hilbert": (None, [I, Z, P, P, P, P, I]),
+        "orc_fft_hilbert": (I, [I, Z, P, P, P, P, I]),
+        "orc_fft_hilbert_roundoff": (I, [I, Z, P, P, P, P, P]),
+        "orc_retarded_self_energy": (I, [I, Z, P, P, P, P, P, P, I, P]),
+        "orc_embedding_component": (None, [I, I, I, P, P, P, P, P, P, P]),
+        "orc_current": (D, [I, I, I, P, P, P, I, P, P, P, P]),
+        "orc_populations": (None, [I, I, I, P, P, I, D, P, P]),
+        "orc_mix": (None, [Z, P, P, D]),
+        "orc_relative_change": (D, [Z, P, P]),
+        "orc_residual_suite": (None, [I, I, I, P, P, P, P, P, P, P, P, P, P]),
+        "orc_dyson_keldysh": (I, [I, I, I, P, P, P, P, P, P, P, P, P]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(l, name)
+        fn.restype = res
+        fn.argtypes = args
+
+
+_ALIVE = []
+
+
+def _p(a):
+    """Pointer to a numpy array's data.  The array is kept referenced until the
+    next call that starts (`_begin`), so temporaries made by layout
+    conversions inside an argument list outlive the C call they feed."""
+    if a is None:
+        return None
+    _ALIVE.append(a)
+    return ctypes.c_void_p(a.ctypes.data)
+
+
+def _field(x, shape=None):
+    a = np.asarray(x, dtype=np.complex128)
+    a = np.asfortranarray(a)
+    if shape is not None and a.shape != tuple(shape):
+        raise ValueError(f"shape {a.shape} != {shape}")
+    return a
+
+
+def _real(x):
+    return np.ascontiguousarray(np.asarray(x, dtype=np.float64))
+
+
+# --------------------------------------------------------------------------
+# Operators
+# --------------------------------------------------------------------------
+
+def inverse(A):
+    A = _field(A).copy(order="F")
+    n = A.shape[0]
+    work = np.zeros((n, n), dtype=np.complex128, order="F")
+    piv = np.zeros(n, dtype=np.int32)
+    st = lib().orc_inverse(n, _p(A), _p(work), _p(piv))
+    if st:
+        raise OracleError(st, f"singular pivot {st}")
+    return A
+
+
+def eigvalsh(H):
+    H = _field(H).copy(order="F")
+    n = H.shape[0]
+    vals = np.zeros(n)
+    lib().orc_hermitian_eigvals(n, _p(H), _p(vals))
+    return vals
+
+
+def retarded_green(eps, h, sigR=None, eta=0.0):
+    """retarded_green (numerics/reference/greens.jl:18-42).  Returns
+    (GR, kappa2, scale, kappa1)."""
+    eps = _real(eps)
+    h = _field(h)
+    Nk, Nb = h.shape[0], h.shape[1]
+    NE = eps.shape[0]
+    sigR = None if sigR is None else _field(sigR, (NE, Nk, Nb, Nb))
+    GR = np.zeros((NE, Nk, Nb, Nb), dtype=np.complex128, order="F")
+    k1 = np.zeros((NE, Nk), order="F")
+    k2 = np.zeros((NE, Nk), order="F")
+    sc = np.zeros((NE, Nk), order="F")
+    bad = ctypes.c_long(-1)
+    st = lib().orc_retarded_green(NE, Nk, Nb, _p(eps), eta, _p(h), _p(sigR), _p(GR), _p(k1), _p(k2),
+                                  _p(sc), ctypes.byref(bad))
+    if st:
+        raise OracleError(st, f"singular Dyson block {bad.value}")
+    return GR, k2, sc, k1
+
+
+def keldysh_green(GR, sig):
+    GR = _field(GR)
+    sig = _field(sig, GR.shape)
+    out = np.zeros_like(GR, order="F")
+    NE, Nk, Nb, _ = GR.shape
+    lib().orc_keldysh_green(NE, Nk, Nb, _p(GR), _p(sig), _p(out))
+    return out
+
+
+def greater_green(GR, GL):
+    GR, GL = _field(GR), _field(GL)
+    out = np.zeros_like(GR, order="F")
+    NE, Nk, Nb, _ = GR.shape
+    lib().orc_greater_green(NE, Nk, Nb, _p(GR), _p(GL), _p(out))
+    return out
+
+
+def spectral_function(GR):
+    GR = _field(GR)
+    out = np.zeros_like(GR, order="F")
+    NE, Nk, Nb, _ = GR.shape
+    lib().orc_spectral_function(NE, Nk, Nb, _p(GR), _p(out))
+    return out
+
+
+def number_functional(GL, wE, wk, gs):
+    GL = _field(GL)
+    NE, Nk, Nb, _ = GL.shape
+    out = ctypes.c_double()
+    st = lib().orc_number_functional(NE, Nk, Nb, _p(GL), _p(_real(wE)), _p(_real(wk)), gs, REALNESS_LIMIT,
+                                     ctypes.byref(out))
+    if st:
+        raise OracleError(st, "number functional is not real")
+    return out.value
+
+
+def paired_coefficients(number, holes, target):
+    a, c, lam = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
+    st = lib().orc_paired_coefficients(number, holes, target, ctypes.byref(a), ctypes.byref(c),
+                                       ctypes.byref(lam))
+    if st:
+        raise OracleError(st, "paired number coefficients rejected")
+    return a.value, c.value, lam.value
+
+
+def normalize_pair(GL, GG, a, c):
+    lib().orc_normalize_pair(GL.size, _p(GL), _p(GG), a, c)
+
+
+class ShiftPlan:
+    """EnergyShiftPlan (numerics/optimized/production_contracts.jl:13-19),
+    0-based."""
+
+    def __init__(self, eps, delta):
+        eps = _real(eps)
+        NE = eps.shape[0]
+        self.NE = NE
+        self.delta = float(delta)
+        self.left = np.zeros(NE, dtype=np.int32)
+        self.right = np.zeros(NE, dtype=np.int32)
+        self.theta = np.zeros(NE)
+        self.valid = np.zeros(NE, dtype=np.uint8)
+        st = lib().orc_shift_plan(NE, _p(eps), float(delta), _p(self.left), _p(self.right), _p(self.theta),
+                                  _p(self.valid))
+        if st:
+            raise OracleError(st, "invalid shift plan")
+
+    def apply(self, X):
+        X = _field(X)
+        Y = np.zeros_like(X, order="F")
+        lib().orc_apply_shift(self.NE, X.size // self.NE, _p(self.left), _p(self.right), _p(self.theta),
+                              _p(self.valid), _p(X), _p(Y))
+        return Y
+
+
+def shift_matrix(eps, delta):
+    eps = _real(eps)
+    W = np.zeros((eps.shape[0], eps.shape[0]), order="F")
+    lib().orc_shift_matrix(eps.shape[0], _p(eps), float(delta), _p(W))
+    return W
+
+
+def contraction_literal(K, G, wk, q=1.0):
+    G = _field(G)
+    K = _field(K)
+    NE, Nk, Nb, _ = G.shape
+    S = np.zeros_like(G, order="F")
+    lib().orc_contraction_literal(NE, Nk, Nb, _p(K), _p(G), _p(_real(wk)), float(q), _p(S))
+    return S
+
+
+def contraction(mech, G, wk, alpha=1.0, beta=0.0, S=None):
+    """production_static_contraction for one factorised operator
+    (production_operators.jl:402-658): S = beta S + alpha q K[wk G]."""
+    G = _field(G)
+    NE, Nk, Nb, _ = G.shape
+    if S is None:
+        S = np.zeros_like(G, order="F")
+    wk = _real(wk)
+    aq = float(alpha * mech.q)
+    if mech.kind == "momentum_independent":
+        lib().orc_contraction_momentum_independent(NE, Nk, Nb, _p(_field(mech.block)), _p(G), _p(wk), aq,
+                                                   float(beta), _p(S))
+    elif mech.kind == "dense":
+        lib().orc_contraction_dense(NE, Nk, Nb, _p(_field(mech.matrix)), _p(G), _p(wk), aq, float(beta), _p(S))
+    elif mech.kind == "ifr":
+        J = mech.left.shape[1]
+        lib().orc_contraction_ifr(NE, Nk, Nb, J, _p(_field(mech.left)), _p(_field(mech.right)),
+                                  _p(_field(mech.radial)), _p(G), _p(wk), aq, float(beta), _p(S))
+    else:
+        raise ValueError(mech.kind)
+    return S
+
+
+def direct_hilbert(Gam, eps, wE, reverse=False):
+    Gam = _field(Gam)
+    NE = Gam.shape[0]
+    out = np.zeros_like(Gam, order="F")
+    lib().orc_direct_hilbert(NE, Gam.size // NE, _p(_real(eps)), _p(_real(wE)), _p(Gam), _p(out), int(reverse))
+    return out
+
+
+def fft_hilbert(Gam, eps, wE, L=0, return_roundoff=False):
+    Gam = _field(Gam)
+    NE = Gam.shape[0]
+    out = np.zeros_like(Gam, order="F")
+    if return_roundoff:
+        r = ctypes.c_double()
+        st = lib().orc_fft_hilbert_roundoff(NE, Gam.size // NE, _p(_real(eps)), _p(_real(wE)), _p(Gam), _p(out),
+                                            ctypes.byref(r))
+        if st:
+            raise OracleError(st, "fft hilbert")
+        return out, r.value
+    st = lib().orc_fft_hilbert(NE, Gam.size // NE, _p(_real(eps)), _p(_real(wE)), _p(Gam), _p(out), int(L))
+    if st:
+        raise OracleError(st, "fft hilbert")
+    return out
+
+
+def retarded_self_energy(SL, SG, eps, wE, method="fft", return_roundoff=False):
+    SL, SG = _field(SL), _field(SG)
+    NE = SL.shape[0]
+    SR = np.zeros_like(SL, order="F")
+    Gam = np.zeros_like(SL, order="F")
+    r = ctypes.c_double()
+    st = lib().orc_retarded_self_energy(NE, SL.size // NE, _p(_real(eps)), _p(_real(wE)), _p(SL), _p(SG), _p(SR),
+                                        _p(Gam), 0 if method == "fft" else 1,
+                                        ctypes.byref(r) if return_roundoff else None)
+    if st:
+        raise OracleError(st, "retarded self-energy")
+    return (SR, Gam, r.value) if return_roundoff else (SR, Gam)
+
+
+def embedding_component(T, G, plan: ShiftPlan):
+    G = _field(G)
+    NE, Nk, Nb, _ = G.shape
+    S = np.zeros_like(G, order="F")
+    lib().orc_embedding_component(NE, Nk, Nb, _p(_field(T)), _p(G), _p(plan.left), _p(plan.right),
+                                  _p(plan.theta), _p(plan.valid), _p(S))
+    return S
+
+
+def current(problem, SG, SL, GL, GG):
+    NE, Nk, Nb = problem.NE, problem.Nk, problem.Nb
+    return lib().orc_current(NE, Nk, Nb, _p(_real(problem.eps)), _p(_real(problem.wE)), _p(_real(problem.wk)),
+                             problem.gs, _p(_field(SG)), _p(_field(SL)), _p(_field(GL)), _p(_field(GG)))
+
+
+def populations(problem, GL):
+    pop = np.zeros(problem.Nb)
+    lib().orc_populations(problem.NE, problem.Nk, problem.Nb, _p(_real(problem.wE)), _p(_real(problem.wk)),
+                          problem.gs, problem.target, _p(_field(GL)), _p(pop))
+    return pop
+
+
+def relative_change(old, new):
+    return lib().orc_relative_change(old.size, _p(_field(old)), _p(_field(new)))
+
+
+def residual_suite(eps, h, GR, GL, GG, total, candidate_SL):
+    NE, Nk, Nb, _ = GR.shape
+    out = np.zeros(5)
+    SR, SL, SG = total
+    lib().orc_residual_suite(NE, Nk, Nb, _p(_real(eps)), _p(_field(h)), _p(_field(GR)), _p(_field(GL)),
+                             _p(_field(GG)), _p(_field(SR)), _p(_field(SL)), _p(_field(SG)),
+                             _p(_field(candidate_SL)), _p(out))
+    return dict(rD=out[0], rA=out[1], rK=out[2], rPSD=out[3], rcaus=out[4])
+
+
+def dyson_keldysh(eps, h, SR, SL, SG=None):
+    eps = _real(eps)
+    SR = _field(SR)
+    NE, Nk, Nb, _ = SR.shape
+    GR = np.zeros_like(SR, order="F")
+    GL = np.zeros_like(SR, order="F")
+    GG = np.zeros_like(SR, order="F") if SG is not None else None
+    sc = np.zeros((NE, Nk), order="F")
+    st = lib().orc_dyson_keldysh(NE, Nk, Nb, _p(eps), _p(_field(h)), _p(SR), _p(_field(SL)),
+                                 _p(None if SG is None else _field(SG)), _p(GR), _p(GL), _p(GG), _p(sc))
+    if st:
+        raise OracleError(st, "singular Dyson block")
+    return GR, GL, GG, sc
+
+
+# --------------------------------------------------------------------------
+# SCBA composition
+# --------------------------------------------------------------------------
+
+def fermi(energy, mu, kBT):
+    x = (energy - mu) / kBT
+    with np.errstate(over="ignore"):
+        f = 1.0 / (np.exp(x) + 1.0)
+    f = np.where(x > FERMI_SATURATION, 0.0, f)
+    f = np.where(x < -FERMI_SATURATION, 1.0, f)
+    return f
+
+
+def bisection(fn, lo, hi):
+    """Bisection to adjacent floating-point numbers (the role of Roots.jl
+    `find_zero(f, (lo, hi), Bisection())`, seed.jl:182)."""
+    flo = fn(lo)
+    if flo == 0:
+        return lo
+    for _ in range(2000):
+        mid = 0.5 * (lo + hi)
+        if mid == lo or mid == hi:
+            break
+        fm = fn(mid)
+        if fm == 0:
+            return mid
+        if (fm < 0) == (flo < 0):
+            lo, flo = mid, fm
+        else:
+            hi = mid
+    return lo if abs(fn(lo)) <= abs(fn(hi)) else hi
+
+
+def seed_green(problem):
+    """_seed_green_production (numerics/optimized/seed.jl:151-197)."""
+    GR, k2, scale, _ = retarded_green(problem.eps, problem.h, None, eta=problem.eta_seed)
+    NE, Nk, Nb = problem.NE, problem.Nk, problem.Nb
+    # q_e = g_s/(2 pi) wE_e sum_m wk_m tr A_em  (seed.jl:28-66)
+    trA = np.zeros((NE, Nk))
+    for a in range(Nb):
+        z = GR[:, :, a, a]
+        trA += np.real(1j * (z - np.conj(z)))
+    q = problem.gs / (2 * math.pi) * problem.wE * (trA @ problem.wk)
+
+    def number_at(mu):
+        return float(np.sum(q * fermi(problem.eps, mu, problem.kBT))) - problem.target
+
+    lo = problem.eps[0] - 50 * problem.kBT
+    hi = problem.eps[-1] + 50 * problem.kBT
+    if number_at(lo) * number_at(hi) > 0:
+        raise OracleError(4, "seed chemical-potential root is not bracketed")
+    mu = bisection(number_at, lo, hi)
+    f = fermi(problem.eps, mu, problem.kBT)
+    diff = GR - np.conj(np.transpose(GR, (0, 1, 3, 2)))
+    GL = np.asfortranarray(-f[:, None, None, None] * diff)
+    GG = greater_green(GR, GL)
+    return dict(GR=GR, GL=GL, GG=GG, scale=scale), mu
+
+
+def scattering_candidate(problem, green, plans, verify=True):
+    """_scattering_candidate_production (production_operators.jl:1258-1335)
+    with the thermal-LO branch of _production_lo_contraction (:1045-1163)."""
+    out = {}
+    roundoff = 0.0
+    wk = problem.wk
+    for mech in problem.mechanisms:
+        if mech.name == "LO":
+            N = problem.N_LO
+            SL = contraction(mech, plans["+LO"].apply(green["GL"]), wk, alpha=N + 1)
+            contraction(mech, plans["-LO"].apply(green["GL"]), wk, alpha=N, beta=1.0, S=SL)
+            SG = contraction(mech, plans["-LO"].apply(green["GG"]), wk, alpha=N + 1)
+            contraction(mech, plans["+LO"].apply(green["GG"]), wk, alpha=N, beta=1.0, S=SG)
+        else:
+            SL = contraction(mech, green["GL"], wk)
+            SG = contraction(mech, green["GG"], wk)
+        if verify:
+            SR, _, r = retarded_self_energy(SL, SG, problem.eps, problem.wE, return_roundoff=True)
+            roundoff = max(roundoff, r)
+        else:
+            SR, _ = retarded_self_energy(SL, SG, problem.eps, problem.wE)
+        out[mech.name] = (SR, SL, SG)
+    return out, roundoff
+
+
+def embedding_candidate(problem, green, plans):
+    """_embedding_self_energy_production (production_operators.jl:924-941)."""
+    plus = tuple(embedding_component(problem.Tplus, green[k], plans["+Ep"]) for k in ("GR", "GL", "GG"))
+    minus = tuple(embedding_component(problem.Tminus, green[k], plans["-Ep"]) for k in ("GR", "GL", "GG"))
+    return plus, minus
+
+
+def total_family(problem, scattering, plus, minus):
+    """_total_family_production (production_operators.jl:1447-1473)."""
+    tot = []
+    for c in range(3):
+        x = plus[c] + minus[c]
+        for mech in problem.mechanisms:
+            x = x + scattering[mech.name][c]
+        tot.append(np.asfortranarray(x))
+    return tuple(tot)
+
+
+def current_green(problem, total):
+    """_current_green_production (numerics/optimized/production_state.jl)."""
+    GR, GL, GG, scale = dyson_keldysh(problem.eps, problem.h, total[0], total[1], total[2])
+    number = number_functional(GL, problem.wE, problem.wk, problem.gs)
+    lam = number / problem.target
+    if not (math.isfinite(lam) and lam > 0):
+        raise OracleError(2, "kinetic eigenvalue must be positive")
+    holes = -number_functional(GG, problem.wE, problem.wk, problem.gs)
+    a, c, lam = paired_coefficients(number, holes, problem.target)
+    normalize_pair(GL, GG, a, c)
+    return dict(GR=GR, GL=GL, GG=GG, scale=scale, number=number, holes=holes, a=a, c=c), lam
+
+
+def make_plans(problem):
+    return {
+        "+Ep": ShiftPlan(problem.eps, +problem.Ep),
+        "-Ep": ShiftPlan(problem.eps, -problem.Ep),
+        "+LO": ShiftPlan(problem.eps, +problem.hw_LO),
+        "-LO": ShiftPlan(problem.eps, -problem.hw_LO),
+    }
+
+
+def scba(problem, iterations, verify=True, state=None, keep_state=False):
+    """Run `iterations` SCBA steps (solve_scba, scba.jl:142-354, with the
+    production operators).  Returns (history, state)."""
+    plans = make_plans(problem)
+    if state is None:
+        green, mu = seed_green(problem)
+        scattering, _ = scattering_candidate(problem, green, plans, verify=False)
+        plus, minus = embedding_candidate(problem, green, plans)
+    else:
+        scattering, plus, minus = state["scattering"], state["plus"], state["minus"]
+    history = []
+    Jprev = None
+    pprev = None
+    for nu in range(1, iterations + 1):
+        total = total_family(problem, scattering, plus, minus)
+        green, lam = current_green(problem, total)
+        cand_sc, rround = scattering_candidate(problem, green, plans, verify=verify)
+        cplus, cminus = embedding_candidate(problem, green, plans)
+        cand_total = total_family(problem, cand_sc, cplus, cminus)
+        res = residual_suite(problem.eps, problem.h, green["GR"], green["GL"], green["GG"], total, cand_total[1])
+        rS = 0.0
+        for old, new in [(plus, cplus), (minus, cminus)] + [
+                (scattering[m.name], cand_sc[m.name]) for m in problem.mechanisms]:
+            for c in range(3):
+                rS = max(rS, relative_change(old[c], new[c]))
+        emb_old = tuple(plus[c] + minus[c] for c in range(3))
+        emb_new = tuple(cplus[c] + cminus[c] for c in range(3))
+        for c in range(3):
+            rS = max(rS, relative_change(emb_old[c], emb_new[c]))
+        Jbar = current(problem, plus[2], plus[1], green["GL"], green["GG"])
+        J = Jbar * problem.J0
+        pops = populations(problem, green["GL"])
+        rJ = math.inf if Jprev is None else abs(J - Jprev) / max(abs(J), abs(Jprev), 1e-12)
+        rp = math.inf if pprev is None else float(np.linalg.norm(pops - pprev) / (np.linalg.norm(pops) + 1e-14))
+        row = dict(nu=nu, lam=lam, rlam=abs(lam - 1), rSigma=rS, rround=rround, J=J, Jbar=Jbar,
+                   populations=pops, rJ=rJ, rpop=rp, number=green["number"], holes=green["holes"], **res)
+        history.append(row)
+        a = problem.alpha
+        for m in problem.mechanisms:
+            scattering[m.name] = tuple(np.asfortranarray((1 - a) * scattering[m.name][c] + a * cand_sc[m.name][c])
+                                       for c in range(3))
+        plus = tuple(np.asfortranarray((1 - a) * plus[c] + a * cplus[c]) for c in range(3))
+        minus = tuple(np.asfortranarray((1 - a) * minus[c] + a * cminus[c]) for c in range(3))
+        Jprev, pprev = J, pops
+    out_state = dict(scattering=scattering, plus=plus, minus=minus, green=green) if keep_state else None
+    return history, out_state

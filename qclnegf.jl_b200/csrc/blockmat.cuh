@@ -1,0 +1,171 @@
+// Block-matrix building blocks shared by the per-(E,k) kernels: swizzled
+// shared-memory N x N tiles, team barriers and reductions, team-tiled complex
+// matmuls, and coalesced copies between E-fastest fields and the tiles.
+#pragma once
+#include "kernels.cuh"
+
+namespace qcl {
+
+template <int NP> __device__ __forceinline__ int sw(int r, int c) { return r * NP + (c ^ (r & 7)); }
+
+// Static tiling per padded block size NP.
+template <int NP> struct Tile;
+template <> struct Tile<8> { static constexpr int CPR = 4, TT = 32, TR = 1, TC = 2; };
+template <> struct Tile<16> { static constexpr int CPR = 2, TT = 32, TR = 2, TC = 4; };
+template <> struct Tile<24> { static constexpr int CPR = 1, TT = 32, TR = 3, TC = 6; };
+template <> struct Tile<32> { static constexpr int CPR = 2, TT = 64, TR = 4, TC = 4; };
+template <> struct Tile<48> { static constexpr int CPR = 2, TT = 96, TR = 4, TC = 6; };
+
+// Team barrier: a warp sync for one-warp teams, a named barrier otherwise.
+template <int TT> __device__ __forceinline__ void team_sync(int team) {
+  if (TT == 32) {
+    __syncwarp();
+  } else {
+    asm volatile("bar.sync %0, %1;" ::"r"(team + 1), "n"(TT) : "memory");
+  }
+}
+
+// Team-wide sum of a double (fixed tree order -> deterministic).
+template <int TT>
+__device__ __forceinline__ double team_sum(double v, int tt, double* scratch /* TT/32 */, int team) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  if (TT == 32) return v;
+  team_sync<TT>(team);
+  if ((tt & 31) == 0) scratch[tt >> 5] = v;
+  team_sync<TT>(team);
+  double s = 0;
+#pragma unroll
+  for (int w = 0; w < TT / 32; ++w) s += scratch[w];
+  return s;
+}
+
+template <int TT>
+__device__ __forceinline__ double team_max(double v, int tt, double* scratch, int team) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+  if (TT == 32) return v;
+  team_sync<TT>(team);
+  if ((tt & 31) == 0) scratch[tt >> 5] = v;
+  team_sync<TT>(team);
+  double s = scratch[0];
+#pragma unroll
+  for (int w = 1; w < TT / 32; ++w) s = fmax(s, scratch[w]);
+  return s;
+}
+
+// Per-team shared scratch besides the three matrices.
+template <typename RL, int NP, int TT> struct TeamScratch {
+  Cx<RL> rowbuf[2][NP];
+  int pivrow[NP];
+  double red[TT / 32 > 0 ? TT / 32 : 1];
+  // multi-warp argmax exchange
+  unsigned long long wkey[TT / 32 > 0 ? TT / 32 : 1];
+};
+
+// Warp argmax of (mag, row), ties broken towards the smaller row index.
+__device__ __forceinline__ void warp_argmax(double& mag, int& row) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    double om = __shfl_xor_sync(0xffffffffu, mag, o);
+    int orow = __shfl_xor_sync(0xffffffffu, row, o);
+    if (om > mag || (om == mag && orow < row)) {
+      mag = om;
+      row = orow;
+    }
+  }
+}
+
+// C = A * B (adjB = false) or C = A * B^H (adjB = true); NxN active part of
+// NP x NP swizzled shared matrices.  RM is the arithmetic precision.
+template <typename RS, typename RM, int NP>
+__device__ __forceinline__ void team_matmul(const Cx<RS>* A, const Cx<RS>* B, Cx<RS>* C, int N, int tt,
+                                            bool adjB) {
+  constexpr int TR = Tile<NP>::TR, TC = Tile<NP>::TC, RG = NP / TR;
+  const int rg = tt % RG, cg = tt / RG;
+  Cx<RM> acc[TR][TC];
+#pragma unroll
+  for (int t = 0; t < TR; ++t)
+#pragma unroll
+    for (int u = 0; u < TC; ++u) acc[t][u] = cx<RM>(0, 0);
+  for (int l = 0; l < N; ++l) {
+    Cx<RM> a[TR], b[TC];
+#pragma unroll
+    for (int t = 0; t < TR; ++t) a[t] = cvt<RM>(A[sw<NP>(rg * TR + t, l)]);
+#pragma unroll
+    for (int u = 0; u < TC; ++u) {
+      const int j = cg * TC + u;
+      b[u] = adjB ? conj(cvt<RM>(B[sw<NP>(j, l)])) : cvt<RM>(B[sw<NP>(l, j)]);
+    }
+#pragma unroll
+    for (int t = 0; t < TR; ++t)
+#pragma unroll
+      for (int u = 0; u < TC; ++u) cfma(acc[t][u], a[t], b[u]);
+  }
+#pragma unroll
+  for (int t = 0; t < TR; ++t)
+#pragma unroll
+    for (int u = 0; u < TC; ++u) C[sw<NP>(rg * TR + t, cg * TC + u)] = cvt<RS>(acc[t][u]);
+}
+
+// Cooperative, coalesced copy of BPC consecutive-energy blocks between a
+// global field (E fastest) and the per-block shared matrices.
+template <typename RG_, typename RS, int NP, int BPC>
+__device__ __forceinline__ void load_blocks(const Cx<RG_>* __restrict__ X, Cx<RS>* bufs, size_t stride_buf,
+                                            int e0, int m, int NE, int Nk, int N) {
+  const int total = BPC * N * N;
+  for (int i = threadIdx.x; i < total; i += blockDim.x) {
+    const int eloc = i % BPC, el = i / BPC;
+    const int a = el % N, b = el / N;
+    const int e = e0 + eloc;
+    Cx<RS> v = cx<RS>(0, 0);
+    if (e < NE) v = cvt<RS>(X[(size_t)e + (size_t)NE * ((size_t)m + (size_t)Nk * ((size_t)a + (size_t)N * b))]);
+    bufs[eloc * stride_buf + sw<NP>(a, b)] = v;
+  }
+}
+
+// Asynchronous variant (cp.async, zero fill past N_E): issues every copy of the
+// tile without waiting, so the whole tile is in flight at once; the caller
+// commits, waits and synchronises.  Storage and shared precision must match.
+template <typename R> __device__ __forceinline__ void cp_async_elem(Cx<R>* smem, const Cx<R>* gmem, bool valid) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  const int n = valid ? (int)sizeof(Cx<R>) : 0;
+  if (sizeof(Cx<R>) == 16)
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(s), "l"(gmem), "r"(n) : "memory");
+  else
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(s), "l"(gmem), "r"(n) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
+
+template <typename R, int NP, int BPC>
+__device__ __forceinline__ void load_blocks_async(const Cx<R>* __restrict__ X, Cx<R>* bufs, size_t stride_buf, int e0,
+                                                  int m, int NE, int Nk, int N) {
+  const int total = BPC * N * N;
+  for (int i = threadIdx.x; i < total; i += blockDim.x) {
+    const int eloc = i % BPC, el = i / BPC;
+    const int a = el % N, b = el / N;
+    const int e = e0 + eloc;
+    const bool ok = e < NE;
+    const Cx<R>* src = X + (ok ? (size_t)e + (size_t)NE * ((size_t)m + (size_t)Nk * ((size_t)a + (size_t)N * b)) : 0);
+    cp_async_elem<R>(bufs + eloc * stride_buf + sw<NP>(a, b), src, ok);
+  }
+  cp_async_commit();
+}
+
+template <typename RG_, typename RS, int NP, int BPC>
+__device__ __forceinline__ void store_blocks(Cx<RG_>* __restrict__ X, const Cx<RS>* bufs, size_t stride_buf,
+                                             int e0, int m, int NE, int Nk, int N) {
+  const int total = BPC * N * N;
+  for (int i = threadIdx.x; i < total; i += blockDim.x) {
+    const int eloc = i % BPC, el = i / BPC;
+    const int a = el % N, b = el / N;
+    const int e = e0 + eloc;
+    if (e < NE)
+      X[(size_t)e + (size_t)NE * ((size_t)m + (size_t)Nk * ((size_t)a + (size_t)N * b))] =
+          cvt<RG_>(bufs[eloc * stride_buf + sw<NP>(a, b)]);
+  }
+}
+
+
+}  // namespace qcl

@@ -1,0 +1,607 @@
+// C-ABI entry points (declared in include/qclb200.h).
+#include <stdarg.h>
+#include <string.h>
+
+#include <algorithm>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "kernels.cuh"
+
+namespace qcl {
+
+static thread_local char g_last_error[512] = "";
+
+void set_last_error(const char* fmt, ...) {
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(g_last_error, sizeof(g_last_error), fmt, ap);
+  va_end(ap);
+}
+
+int cuda_status(cudaError_t e, const char* where) {
+  set_last_error("CUDA error %s (%s) at %s", cudaGetErrorName(e), cudaGetErrorString(e), where);
+  if (e == cudaErrorMemoryAllocation) return QCL_NOMEM;
+  return QCL_CUDA;
+}
+
+// ---------------------------------------------------------------------------
+// Small RAII device buffer for the host-buffer entry points.
+// ---------------------------------------------------------------------------
+struct DevBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+  ~DevBuf() {
+    if (p) cudaFree(p);
+  }
+  int alloc(size_t n) {
+    bytes = n;
+    if (n == 0) return QCL_OK;
+    cudaError_t e = cudaMalloc(&p, n);
+    if (e != cudaSuccess) return cuda_status(e, "cudaMalloc");
+    return QCL_OK;
+  }
+  int upload(const void* host, size_t n) {
+    int s = alloc(n);
+    if (s) return s;
+    if (host && n) {
+      cudaError_t e = cudaMemcpy(p, host, n, cudaMemcpyHostToDevice);
+      if (e != cudaSuccess) return cuda_status(e, "cudaMemcpy H2D");
+    }
+    return QCL_OK;
+  }
+  int download(void* host) const {
+    if (host && bytes) {
+      cudaError_t e = cudaMemcpy(host, p, bytes, cudaMemcpyDeviceToHost);
+      if (e != cudaSuccess) return cuda_status(e, "cudaMemcpy D2H");
+    }
+    return QCL_OK;
+  }
+};
+
+static size_t cbytes(int precision) { return precision == QCL_C128 ? 16 : 8; }
+
+static int check_precision(int precision) {
+  if (precision != QCL_C128 && precision != QCL_C64 && precision != QCL_MIXED) {
+    set_last_error("unknown precision %d", precision);
+    return QCL_ARG;
+  }
+  return QCL_OK;
+}
+
+static int read_status(const int* dstatus, const char* what) {
+  int h[2] = {0, 0};
+  cudaError_t e = cudaMemcpy(h, dstatus, sizeof(h), cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) return cuda_status(e, what);
+  if (h[0] == QCL_SINGULAR) {
+    set_last_error("%s: singular block (linear block index %d)", what, h[1]);
+    return QCL_SINGULAR;
+  }
+  if (h[0] != 0) {
+    set_last_error("%s: device status %d at %d", what, h[0], h[1]);
+    return h[0];
+  }
+  return QCL_OK;
+}
+
+// Device workspace of the host-buffer entry points: grows to the largest
+// problem seen and is reused across calls, so a call allocates nothing once
+// warm.  Calls are serialised by a mutex (one workspace per process).
+struct Grow {
+  void* p = nullptr;
+  size_t cap = 0;
+  int ensure(size_t n) {
+    if (n <= cap && p) return QCL_OK;
+    if (p) cudaFree(p);
+    p = nullptr;
+    cap = 0;
+    cudaError_t e = cudaMalloc(&p, n > 0 ? n : 16);
+    if (e != cudaSuccess) return cuda_status(e, "cudaMalloc (workspace)");
+    cap = n;
+    return QCL_OK;
+  }
+};
+
+struct Pipeline {
+  cudaStream_t st[3] = {nullptr, nullptr, nullptr};
+  Grow eps, h, in[3], out[3], scale, trL, trG, status, wE, sum, gam;
+  int init() {
+    for (auto& s : st)
+      if (!s) {
+        cudaError_t e = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
+        if (e != cudaSuccess) return cuda_status(e, "cudaStreamCreate");
+      }
+    return QCL_OK;
+  }
+};
+static std::mutex g_pipe_mutex;
+static Pipeline& pipeline() {
+  static Pipeline p;
+  return p;
+}
+
+static HilbertTables& shared_hilbert_tables() {
+  static HilbertTables t;
+  return t;
+}
+static std::mutex g_hilbert_mutex;
+
+struct ScbaCtx;
+int scba_create(const qcl_scba_problem* p, const qcl_mechanism* mechs, ScbaCtx** out);
+void scba_destroy(ScbaCtx* c);
+int scba_seed(ScbaCtx* c, double* mu_out);
+int scba_step(ScbaCtx* c, qcl_scba_row* row);
+int scba_populations(ScbaCtx* c, double* out);
+int scba_download(ScbaCtx* c, int which, void* host);
+int scba_upload(ScbaCtx* c, int which, const void* host);
+int scba_set_graph(ScbaCtx* c, int enable);
+
+static int shift_plan_dev(int NE, const double* eps, double delta, DevBuf& l, DevBuf& r, DevBuf& th, DevBuf& v,
+                          ShiftPlanDev* out) {
+  std::vector<int> hl(NE), hr(NE);
+  std::vector<double> ht(NE);
+  std::vector<unsigned char> hv(NE);
+  int s = build_shift_plan_host(NE, eps, delta, hl.data(), hr.data(), ht.data(), hv.data());
+  if (s) return s;
+  if ((s = l.upload(hl.data(), NE * sizeof(int)))) return s;
+  if ((s = r.upload(hr.data(), NE * sizeof(int)))) return s;
+  if ((s = th.upload(ht.data(), NE * sizeof(double)))) return s;
+  if ((s = v.upload(hv.data(), NE))) return s;
+  out->left = (const int*)l.p;
+  out->right = (const int*)r.p;
+  out->theta = (const double*)th.p;
+  out->valid = (const unsigned char*)v.p;
+  return QCL_OK;
+}
+
+int launch_convert(int precision, size_t n, const void* in_c128, void* out, cudaStream_t st);
+
+// upload a complex128 host array converted to the field precision
+static int upload_converted(int precision, const void* host, size_t n, DevBuf& dst) {
+  DevBuf tmp;
+  int s;
+  if ((s = tmp.upload(host, n * 16))) return s;
+  if ((s = dst.alloc(n * cbytes(precision)))) return s;
+  return launch_convert(precision, n, tmp.p, dst.p, 0);
+}
+
+}  // namespace qcl
+
+using namespace qcl;
+
+extern "C" {
+
+int qcl_version(void) { return 100; }
+const char* qcl_last_error(void) { return g_last_error; }
+int qcl_max_basis(void) { return 48; }
+
+int qcl_dev_dyson_keldysh(void* stream, int precision, int NE, int Nk, int Nb, const double* eps, double eta,
+                          const void* h, const void* sigR, const void* sigL, const void* sigG, void* GR, void* GL,
+                          void* GG, double* scale, void* traceL, void* traceG, int* status) {
+  if (int s = check_precision(precision)) return s;
+  return launch_dyson_keldysh(precision, NE, Nk, Nb, eps, eta, h, sigR, sigL, sigG, GR, GL, GG, scale, traceL,
+                              traceG, status, (cudaStream_t)stream);
+}
+
+int qcl_dyson_keldysh(int precision, int NE, int Nk, int Nb, const double* eps, double eta, const void* h,
+                      const void* sigR, const void* sigL, const void* sigG, void* GR, void* GL, void* GG,
+                      double* scale, void* traceL, void* traceG) {
+  if (int s = check_precision(precision)) return s;
+  if (NE <= 0 || Nk <= 0 || Nb <= 0) {
+    set_last_error("non-positive dimension (%d,%d,%d)", NE, Nk, Nb);
+    return QCL_DIM;
+  }
+  if (!eps || !h || !sigR) {
+    set_last_error("eps, h and sigR are required");
+    return QCL_ARG;
+  }
+  if (padded_size(Nb) == 0) {
+    set_last_error("basis size N_b=%d exceeds the supported maximum 48", Nb);
+    return QCL_UNSUPPORTED;
+  }
+  std::lock_guard<std::mutex> lock(g_pipe_mutex);
+  Pipeline& P = pipeline();
+  int s;
+  if ((s = P.init())) return s;
+  const size_t es = cbytes(precision);
+  const size_t nf = field_elems(NE, Nk, Nb) * es;
+  const size_t nb = (size_t)NE * Nk;
+  const void* hin[3] = {sigR, sigL, sigG};
+  void* hout[3] = {GR, sigL ? GL : nullptr, sigG ? GG : nullptr};
+  if ((s = P.eps.ensure(NE * sizeof(double)))) return s;
+  if ((s = P.h.ensure((size_t)Nk * Nb * Nb * 16))) return s;
+  for (int i = 0; i < 3; ++i) {
+    if (hin[i] && (s = P.in[i].ensure(nf))) return s;
+    if (hout[i] && (s = P.out[i].ensure(nf))) return s;
+  }
+  if (scale && (s = P.scale.ensure(nb * sizeof(double)))) return s;
+  if (traceL && sigL && (s = P.trL.ensure(nb * 16))) return s;
+  if (traceG && sigG && (s = P.trG.ensure(nb * 16))) return s;
+  if ((s = P.status.ensure(2 * sizeof(int)))) return s;
+  QCL_CUDA_CHECK(cudaMemcpy(P.eps.p, eps, NE * sizeof(double), cudaMemcpyHostToDevice));
+  QCL_CUDA_CHECK(cudaMemcpy(P.h.p, h, (size_t)Nk * Nb * Nb * 16, cudaMemcpyHostToDevice));
+  QCL_CUDA_CHECK(cudaMemset(P.status.p, 0, 2 * sizeof(int)));
+  // momentum slabs of ~64 MiB per field, round-robin over three streams so
+  // that the upload of one slab, the kernel of the previous one and the
+  // download of the one before overlap
+  const size_t slab_bytes = (size_t)NE * Nb * Nb * es;
+  int ms = (int)std::max<size_t>(1, (64u << 20) / std::max<size_t>(slab_bytes, 1));
+  ms = std::min(ms, Nk);
+  const size_t pitch = (size_t)NE * Nk * es;
+  int k = 0;
+  for (int m0 = 0; m0 < Nk; m0 += ms, ++k) {
+    const int cnt = std::min(ms, Nk - m0);
+    cudaStream_t st = P.st[k % 3];
+    const size_t off = (size_t)NE * m0 * es, width = (size_t)NE * cnt * es;
+    for (int i = 0; i < 3; ++i)
+      if (hin[i])
+        QCL_CUDA_CHECK(cudaMemcpy2DAsync((char*)P.in[i].p + off, pitch, (const char*)hin[i] + off, pitch, width,
+                                         (size_t)Nb * Nb, cudaMemcpyHostToDevice, st));
+    s = launch_dyson_keldysh(precision, NE, Nk, Nb, (const double*)P.eps.p, eta, P.h.p, P.in[0].p,
+                             sigL ? P.in[1].p : nullptr, sigG ? P.in[2].p : nullptr, GR ? P.out[0].p : nullptr,
+                             hout[1] ? P.out[1].p : nullptr, hout[2] ? P.out[2].p : nullptr,
+                             scale ? (double*)P.scale.p : nullptr, (traceL && sigL) ? P.trL.p : nullptr,
+                             (traceG && sigG) ? P.trG.p : nullptr, (int*)P.status.p, st, m0, cnt);
+    if (s) return s;
+    for (int i = 0; i < 3; ++i)
+      if (hout[i])
+        QCL_CUDA_CHECK(cudaMemcpy2DAsync((char*)hout[i] + off, pitch, (const char*)P.out[i].p + off, pitch, width,
+                                         (size_t)Nb * Nb, cudaMemcpyDeviceToHost, st));
+    const size_t boff = (size_t)NE * m0, bcnt = (size_t)NE * cnt;
+    if (scale)
+      QCL_CUDA_CHECK(cudaMemcpyAsync(scale + boff, (double*)P.scale.p + boff, bcnt * sizeof(double),
+                                     cudaMemcpyDeviceToHost, st));
+    if (traceL && sigL)
+      QCL_CUDA_CHECK(cudaMemcpyAsync((char*)traceL + boff * 16, (char*)P.trL.p + boff * 16, bcnt * 16,
+                                     cudaMemcpyDeviceToHost, st));
+    if (traceG && sigG)
+      QCL_CUDA_CHECK(cudaMemcpyAsync((char*)traceG + boff * 16, (char*)P.trG.p + boff * 16, bcnt * 16,
+                                     cudaMemcpyDeviceToHost, st));
+  }
+  for (int i = 0; i < 3; ++i) QCL_CUDA_CHECK(cudaStreamSynchronize(P.st[i]));
+  return read_status((int*)P.status.p, "dyson_keldysh");
+}
+
+int qcl_dev_weighted_trace(void* stream, int NE, int Nk, const void* trace, const double* wE, const double* wk,
+                           double* out) {
+  static double* partial = nullptr;
+  if (!partial) QCL_CUDA_CHECK(cudaMalloc(&partial, 296 * 2 * sizeof(double)));
+  return launch_weighted_trace(NE, Nk, trace, wE, wk, partial, out, (cudaStream_t)stream);
+}
+
+int qcl_dev_paired_coefficients(void* stream, const double* trL, const double* trG, int gs, double target,
+                                double* coeffs, int* status) {
+  return launch_paired_coefficients(trL, trG, gs, target, coeffs, status, (cudaStream_t)stream);
+}
+
+int qcl_dev_normalize_pair(void* stream, int precision, size_t n, void* GL, void* GG, const double* coeffs) {
+  if (int s = check_precision(precision)) return s;
+  return launch_normalize_pair(precision, n, GL, GG, coeffs, (cudaStream_t)stream);
+}
+
+static int hilbert_host(int precision, int NE, size_t ncols, const double* eps, const double* wE, const void* Gam,
+                        const void* SL, const void* SG, void* out_lam, void* out_SR, void* out_gam,
+                        double* roundoff) {
+  if (int s = check_precision(precision)) return s;
+  if (!eps || !wE) {
+    set_last_error("eps and wE are required");
+    return QCL_ARG;
+  }
+  double de;
+  if (int s = check_uniform_grid(NE, eps, &de)) return s;
+  std::lock_guard<std::mutex> lock(g_pipe_mutex);
+  std::lock_guard<std::mutex> lock2(g_hilbert_mutex);
+  HilbertTables& t = shared_hilbert_tables();
+  Pipeline& P = pipeline();
+  int s;
+  if ((s = P.init())) return s;
+  if ((s = prepare_hilbert_tables(t, NE, de, precision))) return s;
+  const int sp = precision == QCL_MIXED ? QCL_C64 : precision;
+  const size_t es = cbytes(sp);
+  const size_t nf = (size_t)NE * ncols * es;
+  const bool verify = roundoff != nullptr;
+  if ((s = P.wE.ensure(NE * sizeof(double)))) return s;
+  if (Gam && (s = P.in[0].ensure(nf))) return s;
+  if (SL && (s = P.in[1].ensure(nf))) return s;
+  if (SG && (s = P.in[2].ensure(nf))) return s;
+  if ((s = P.out[0].ensure(nf))) return s;
+  if (out_gam && (s = P.gam.ensure(nf))) return s;
+  if (verify && (s = ensure_partial(t, (long long)ncols))) return s;
+  if ((s = P.sum.ensure(2 * sizeof(double)))) return s;
+  QCL_CUDA_CHECK(cudaMemcpy(P.wE.p, wE, NE * sizeof(double), cudaMemcpyHostToDevice));
+  // column slabs of ~64 MiB, three streams
+  size_t cs = std::max<size_t>(1, (64u << 20) / ((size_t)NE * es));
+  cs = std::min(cs, ncols);
+  int k = 0;
+  for (size_t c0 = 0; c0 < ncols; c0 += cs, ++k) {
+    const size_t cnt = std::min(cs, ncols - c0);
+    cudaStream_t st = P.st[k % 3];
+    const size_t off = c0 * NE * es, bytes = cnt * NE * es;
+    if (Gam) QCL_CUDA_CHECK(cudaMemcpyAsync((char*)P.in[0].p + off, (const char*)Gam + off, bytes, cudaMemcpyHostToDevice, st));
+    if (SL) QCL_CUDA_CHECK(cudaMemcpyAsync((char*)P.in[1].p + off, (const char*)SL + off, bytes, cudaMemcpyHostToDevice, st));
+    if (SG) QCL_CUDA_CHECK(cudaMemcpyAsync((char*)P.in[2].p + off, (const char*)SG + off, bytes, cudaMemcpyHostToDevice, st));
+    s = launch_hilbert(t, sp, (long long)cnt, (const double*)P.wE.p, Gam ? (char*)P.in[0].p + off : nullptr,
+                       SL ? (char*)P.in[1].p + off : nullptr, SG ? (char*)P.in[2].p + off : nullptr,
+                       out_lam ? (char*)P.out[0].p + off : nullptr, out_SR ? (char*)P.out[0].p + off : nullptr,
+                       out_gam ? (char*)P.gam.p + off : nullptr, verify, st, (long long)c0);
+    if (s) return s;
+    QCL_CUDA_CHECK(cudaMemcpyAsync((char*)(out_lam ? out_lam : out_SR) + off, (char*)P.out[0].p + off, bytes,
+                                   cudaMemcpyDeviceToHost, st));
+    if (out_gam) QCL_CUDA_CHECK(cudaMemcpyAsync((char*)out_gam + off, (char*)P.gam.p + off, bytes, cudaMemcpyDeviceToHost, st));
+  }
+  for (int i = 0; i < 3; ++i) QCL_CUDA_CHECK(cudaStreamSynchronize(P.st[i]));
+  if (verify) {
+    if ((s = launch_combine(t.partial, (int)ncols, 2, (double*)P.sum.p, 0))) return s;
+    double h2[2];
+    QCL_CUDA_CHECK(cudaMemcpy(h2, P.sum.p, sizeof(h2), cudaMemcpyDeviceToHost));
+    *roundoff = isfinite(h2[0]) && isfinite(h2[1]) ? sqrt(h2[0]) / (sqrt(h2[1]) + 1e-14) : INFINITY;
+  }
+  return QCL_OK;
+}
+
+int qcl_dev_fft_hilbert_transform(void* stream, int precision, int NE, size_t ncols, double de, const double* wE,
+                                  const void* Gam, void* Lam, double* roundoff_sums) {
+  if (int s = check_precision(precision)) return s;
+  if (NE < 2 || !(de > 0)) {
+    set_last_error("fft_hilbert: need N_E >= 2 and a positive spacing");
+    return QCL_ARG;
+  }
+  std::lock_guard<std::mutex> lock(g_hilbert_mutex);
+  HilbertTables& t = shared_hilbert_tables();
+  int s;
+  if ((s = prepare_hilbert_tables(t, NE, de, precision))) return s;
+  const int sp = precision == QCL_MIXED ? QCL_C64 : precision;
+  const bool verify = roundoff_sums != nullptr;
+  if ((s = launch_hilbert(t, sp, (long long)ncols, wE, Gam, nullptr, nullptr, Lam, nullptr, nullptr, verify,
+                          (cudaStream_t)stream)))
+    return s;
+  if (verify) return launch_combine(t.partial, (int)ncols, 2, roundoff_sums, (cudaStream_t)stream);
+  return QCL_OK;
+}
+
+int qcl_fft_hilbert_transform(int precision, int NE, size_t ncols, const double* eps, const double* wE,
+                              const void* Gam, void* Lam, double* roundoff) {
+  if (!Gam || !Lam) {
+    set_last_error("Gam and Lam are required");
+    return QCL_ARG;
+  }
+  return hilbert_host(precision, NE, ncols, eps, wE, Gam, nullptr, nullptr, Lam, nullptr, nullptr, roundoff);
+}
+
+int qcl_apply_energy_shift(int precision, int NE, size_t ncols, const double* eps, double delta, const void* X,
+                           void* Y) {
+  if (int s = check_precision(precision)) return s;
+  if (!eps || !X || !Y) {
+    set_last_error("eps, X and Y are required");
+    return QCL_ARG;
+  }
+  if (X == Y) {
+    set_last_error("in-place aliasing is not supported");  // production_cache.jl:308-309
+    return QCL_ARG;
+  }
+  const int sp = precision == QCL_MIXED ? QCL_C64 : precision;
+  DevBuf l, r, th, v, dX, dY;
+  ShiftPlanDev plan;
+  int s;
+  if ((s = shift_plan_dev(NE, eps, delta, l, r, th, v, &plan))) return s;
+  const size_t nb = (size_t)NE * ncols * cbytes(sp);
+  if ((s = dX.upload(X, nb))) return s;
+  if ((s = dY.alloc(nb))) return s;
+  if ((s = launch_shift(sp, NE, (long long)ncols, plan, dX.p, dY.p, 0))) return s;
+  QCL_CUDA_CHECK(cudaDeviceSynchronize());
+  return dY.download(Y);
+}
+
+int qcl_static_contraction(int precision, const qcl_mechanism* op, int NE, int Nk, int Nb, const double* wk,
+                           double alpha, double beta, const void* G, void* S) {
+  if (int s = check_precision(precision)) return s;
+  if (!op || !wk || !G || !S) {
+    set_last_error("operator, wk, G and S are required");
+    return QCL_ARG;
+  }
+  const int sp = precision == QCL_MIXED ? QCL_C64 : precision;
+  const size_t N2 = (size_t)Nb * Nb;
+  DevBuf blk, mat, le, ri, ra, dwk, dG, dS, work;
+  KernelOpDev k;
+  k.kind = op->kind;
+  k.J = op->J;
+  int s;
+  if (op->kind == QCL_KERNEL_MOMENTUM_INDEPENDENT) {
+    if ((s = upload_converted(sp, op->block, N2 * N2, blk))) return s;
+    k.block = blk.p;
+  } else if (op->kind == QCL_KERNEL_DENSE) {
+    const size_t nc = (size_t)Nk * N2;
+    if ((s = upload_converted(sp, op->matrix, nc * nc, mat))) return s;
+    k.matrix = mat.p;
+  } else if (op->kind == QCL_KERNEL_IFR) {
+    if (op->J < 1) {
+      set_last_error("IFR operator needs J >= 1");
+      return QCL_ARG;
+    }
+    if ((s = upload_converted(sp, op->left, N2 * op->J, le))) return s;
+    if ((s = upload_converted(sp, op->right, N2 * op->J, ri))) return s;
+    if ((s = upload_converted(sp, op->radial, (size_t)Nk * Nk, ra))) return s;
+    k.left = le.p;
+    k.right = ri.p;
+    k.radial = ra.p;
+  } else {
+    set_last_error("unknown kernel kind %d", op->kind);
+    return QCL_ARG;
+  }
+  const size_t nb = field_elems(NE, Nk, Nb) * cbytes(sp);
+  if ((s = dwk.upload(wk, Nk * sizeof(double)))) return s;
+  if ((s = dG.upload(G, nb))) return s;
+  if ((s = dS.upload(beta != 0.0 ? S : nullptr, nb))) return s;
+  if ((s = work.alloc(contraction_work_elems(k, NE, Nk, Nb) * cbytes(sp)))) return s;
+  if ((s = launch_contraction(sp, k, NE, Nk, Nb, (const double*)dwk.p, dG.p, dS.p, alpha * op->q, beta, work.p, 0)))
+    return s;
+  QCL_CUDA_CHECK(cudaDeviceSynchronize());
+  return dS.download(S);
+}
+
+int qcl_embedding_component(int precision, int NE, int Nk, int Nb, const double* eps, double delta, const void* T,
+                            const void* G, void* S) {
+  if (int s = check_precision(precision)) return s;
+  if (!eps || !T || !G || !S) {
+    set_last_error("eps, T, G and S are required");
+    return QCL_ARG;
+  }
+  if (padded_size(Nb) == 0) {
+    set_last_error("basis size N_b=%d exceeds the supported maximum 48", Nb);
+    return QCL_UNSUPPORTED;
+  }
+  const int sp = precision == QCL_MIXED ? QCL_C64 : precision;
+  DevBuf l, r, th, v, dT, dG, dS;
+  ShiftPlanDev plan;
+  int s;
+  if ((s = shift_plan_dev(NE, eps, delta, l, r, th, v, &plan))) return s;
+  const size_t nb = field_elems(NE, Nk, Nb) * cbytes(sp);
+  if ((s = dT.upload(T, (size_t)Nb * Nb * 16))) return s;
+  if ((s = dG.upload(G, nb))) return s;
+  if ((s = dS.alloc(nb))) return s;
+  SandwichJob job;
+  job.X[0] = dG.p;
+  job.S[0] = dS.p;
+  job.T = dT.p;
+  job.plan = plan;
+  if ((s = launch_sandwich(sp, NE, Nk, Nb, &job, 1, 0))) return s;
+  QCL_CUDA_CHECK(cudaDeviceSynchronize());
+  return dS.download(S);
+}
+
+int qcl_residual_suite(int precision, int NE, int Nk, int Nb, const double* eps, const void* h, const void* GR,
+                       const void* GL, const void* GG, const void* SR, const void* SL, const void* SG,
+                       const void* SLc, double* out) {
+  if (int s = check_precision(precision)) return s;
+  if (!eps || !h || !GR || !GL || !GG || !SR || !SL || !SG || !SLc || !out) {
+    set_last_error("all residual-suite arrays are required");
+    return QCL_ARG;
+  }
+  if (padded_size(Nb) == 0) {
+    set_last_error("basis size N_b=%d exceeds the supported maximum 48", Nb);
+    return QCL_UNSUPPORTED;
+  }
+  const int sp = precision == QCL_MIXED ? QCL_C64 : precision;
+  const size_t nb = field_elems(NE, Nk, Nb) * cbytes(sp);
+  DevBuf de, dh, d[7], work, o;
+  const void* host[7] = {GR, GL, GG, SR, SL, SG, SLc};
+  int s;
+  if ((s = de.upload(eps, NE * sizeof(double)))) return s;
+  if ((s = dh.upload(h, (size_t)Nk * Nb * Nb * 16))) return s;
+  for (int i = 0; i < 7; ++i)
+    if ((s = d[i].upload(host[i], nb))) return s;
+  if ((s = work.alloc(residual_work_doubles(NE, Nk) * sizeof(double)))) return s;
+  if ((s = o.alloc(5 * sizeof(double)))) return s;
+  if ((s = launch_residual_suite(sp, NE, Nk, Nb, (const double*)de.p, dh.p, d[0].p, d[1].p, d[2].p, d[3].p, d[4].p,
+                                 d[5].p, d[6].p, (double*)work.p, (double*)o.p, 0)))
+    return s;
+  QCL_CUDA_CHECK(cudaDeviceSynchronize());
+  return o.download(out);
+}
+
+int qcl_hermitian_eigvals(int n, size_t count, const void* H, double* vals) {
+  if (n < 1 || !H || !vals) {
+    set_last_error("hermitian_eigvals: n >= 1 and arrays are required");
+    return QCL_ARG;
+  }
+  DevBuf dH, dv;
+  int s;
+  if ((s = dH.upload(H, (size_t)n * n * count * 16))) return s;
+  if ((s = dv.alloc((size_t)n * count * sizeof(double)))) return s;
+  if ((s = launch_eigvals(n, (long long)count, dH.p, (double*)dv.p, 0))) return s;
+  QCL_CUDA_CHECK(cudaDeviceSynchronize());
+  return dv.download(vals);
+}
+
+int qcl_selfenergy_residual(int precision, size_t n, const void* old_, const void* new_, double* out) {
+  if (int s = check_precision(precision)) return s;
+  const int sp = precision == QCL_MIXED ? QCL_C64 : precision;
+  DevBuf a, b, part, o;
+  int s;
+  if ((s = a.upload(old_, n * cbytes(sp)))) return s;
+  if ((s = b.upload(new_, n * cbytes(sp)))) return s;
+  if ((s = part.alloc(kReduceCtas * 2 * sizeof(double)))) return s;
+  if ((s = o.alloc(2 * sizeof(double)))) return s;
+  if ((s = launch_residual_mix(sp, n, a.p, b.p, 0.0, (double*)part.p, (double*)o.p, 0))) return s;
+  QCL_CUDA_CHECK(cudaDeviceSynchronize());
+  double h2[2];
+  if ((s = o.download(h2))) return s;
+  *out = (isfinite(h2[0]) && isfinite(h2[1])) ? sqrt(h2[0]) / (sqrt(h2[1]) + 1e-14) : INFINITY;
+  return QCL_OK;
+}
+
+int qcl_current_populations(int precision, int NE, int Nk, int Nb, const double* wE, const double* wk, int gs,
+                            double target, const void* SG, const void* SL, const void* GL, const void* GG,
+                            double* out) {
+  if (int s = check_precision(precision)) return s;
+  const int sp = precision == QCL_MIXED ? QCL_C64 : precision;
+  const size_t nb = field_elems(NE, Nk, Nb) * cbytes(sp);
+  DevBuf dwE, dwk, a, b, c, d, part, o;
+  int s;
+  if ((s = dwE.upload(wE, NE * sizeof(double)))) return s;
+  if ((s = dwk.upload(wk, Nk * sizeof(double)))) return s;
+  if ((s = a.upload(SG, nb))) return s;
+  if ((s = b.upload(SL, nb))) return s;
+  if ((s = c.upload(GL, nb))) return s;
+  if ((s = d.upload(GG, nb))) return s;
+  if ((s = part.alloc(observables_partial_doubles(Nb) * sizeof(double)))) return s;
+  if ((s = o.alloc((2 + Nb) * sizeof(double)))) return s;
+  if ((s = launch_observables(sp, NE, Nk, Nb, (const double*)dwE.p, (const double*)dwk.p, a.p, b.p, c.p, d.p, gs,
+                              target, (double*)part.p, (double*)o.p, 0)))
+    return s;
+  QCL_CUDA_CHECK(cudaDeviceSynchronize());
+  return o.download(out);
+}
+
+int qcl_scba_create(const qcl_scba_problem* problem, const qcl_mechanism* mechanisms, qcl_scba** out) {
+  if (!out) {
+    set_last_error("out is required");
+    return QCL_ARG;
+  }
+  ScbaCtx* c = nullptr;
+  int s = scba_create(problem, mechanisms, &c);
+  *out = (qcl_scba*)c;
+  return s;
+}
+void qcl_scba_destroy(qcl_scba* ctx) { scba_destroy((ScbaCtx*)ctx); }
+int qcl_scba_seed(qcl_scba* ctx, double* mu) { return ctx ? scba_seed((ScbaCtx*)ctx, mu) : QCL_ARG; }
+int qcl_scba_step(qcl_scba* ctx, qcl_scba_row* row) {
+  if (!ctx || !row) {
+    set_last_error("ctx and row are required");
+    return QCL_ARG;
+  }
+  return scba_step((ScbaCtx*)ctx, row);
+}
+int qcl_scba_run(qcl_scba* ctx, int max_iter, double tol_sigma, qcl_scba_row* history, int* n_done) {
+  if (!ctx || !history || max_iter < 0) {
+    set_last_error("ctx and history are required");
+    return QCL_ARG;
+  }
+  int n = 0, s = QCL_OK;
+  for (; n < max_iter; ++n) {
+    s = scba_step((ScbaCtx*)ctx, &history[n]);
+    if (s) break;
+    if (history[n].status != QCL_OK || history[n].r_Sigma <= tol_sigma) {
+      ++n;
+      break;
+    }
+  }
+  if (n_done) *n_done = n;
+  return s;
+}
+int qcl_scba_populations(qcl_scba* ctx, double* out) { return scba_populations((ScbaCtx*)ctx, out); }
+int qcl_scba_download(qcl_scba* ctx, int which, void* host) { return scba_download((ScbaCtx*)ctx, which, host); }
+int qcl_scba_upload(qcl_scba* ctx, int which, const void* host) { return scba_upload((ScbaCtx*)ctx, which, host); }
+int qcl_scba_use_graph(qcl_scba* ctx, int enable) { return scba_set_graph((ScbaCtx*)ctx, enable); }
+
+int qcl_retarded_self_energy(int precision, int NE, size_t ncols, const double* eps, const double* wE,
+                             const void* SL, const void* SG, void* SR, void* Gam, double* roundoff) {
+  if (!SL || !SG || !SR) {
+    set_last_error("SL, SG and SR are required");
+    return QCL_ARG;
+  }
+  return hilbert_host(precision, NE, ncols, eps, wE, nullptr, SL, SG, nullptr, SR, Gam, roundoff);
+}
+
+}  // extern "C"

@@ -1,0 +1,293 @@
+// Energy shifts and the static self-energy contractions.
+//
+// Shift: apply_energy_shift! (numerics/optimized/production_cache.jl:300-325)
+//   Y[e] = valid[e] ? ((l == r || th == 0) ? X[l] : (1-th) X[l] + th X[r]) : 0
+// Contractions (production_static_contraction, production_operators.jl:
+// 402-658), S = beta S + alpha q K[wk G]:
+//   momentum independent: X[e,(c,d)] = sum_m' wk G[e,m',c,d]; Y = B X;
+//                         S[e,m,(a,b)] broadcast over m;
+//   dense:                S[e,(m,a,b)] = sum_(m',c,d) M wk[m'] G[e,(m',c,d)];
+//   separable IFR:        S = left * (radial * (wk .* (right * G))).
+// Every stage is one call of a tiled complex GEMM whose operand and output
+// index maps are strided views of the E-fastest fields: the energy axis is the
+// GEMM's M dimension, so all A loads and C stores are coalesced along E.
+#include "kernels.cuh"
+
+namespace qcl {
+
+// ---------------------------------------------------------------------------
+template <typename R>
+__global__ void shift_kernel(int NE, long long ncols, const int* __restrict__ left, const int* __restrict__ right,
+                             const double* __restrict__ theta, const unsigned char* __restrict__ valid,
+                             const Cx<R>* __restrict__ X, Cx<R>* __restrict__ Y) {
+  const long long n = (long long)NE * ncols;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const int e = (int)(i % NE);
+    const long long base = i - e;
+    Cx<R> v = cx<R>(0, 0);
+    if (valid[e]) {
+      const int l = left[e], r = right[e];
+      const double th = theta[e];
+      if (l == r || th == 0.0) {
+        v = X[base + l];
+      } else {
+        const Cx<R> a = X[base + l], b = X[base + r];
+        v = cx<R>((R)((1 - th) * a.x + th * b.x), (R)((1 - th) * a.y + th * b.y));
+      }
+    }
+    Y[i] = v;
+  }
+}
+
+static unsigned grid_cap(long long n, int threads) {
+  long long g = (n + threads - 1) / threads;
+  const long long cap = 148 * 16;
+  return (unsigned)(g < cap ? (g > 0 ? g : 1) : cap);
+}
+
+int launch_shift(int precision, int NE, long long ncols, const ShiftPlanDev& plan, const void* X, void* Y,
+                 cudaStream_t st) {
+  const long long n = (long long)NE * ncols;
+  if (precision == QCL_C128)
+    shift_kernel<double><<<grid_cap(n, 256), 256, 0, st>>>(NE, ncols, plan.left, plan.right, plan.theta, plan.valid,
+                                                          (const Cx<double>*)X, (Cx<double>*)Y);
+  else
+    shift_kernel<float><<<grid_cap(n, 256), 256, 0, st>>>(NE, ncols, plan.left, plan.right, plan.theta, plan.valid,
+                                                         (const Cx<float>*)X, (Cx<float>*)Y);
+  QCL_LAUNCH_CHECK("shift_kernel");
+  return QCL_OK;
+}
+
+// build_shift_plan (production_cache.jl:258-290), 0-based, on the host.
+int build_shift_plan_host(int NE, const double* eps, double delta, int* left, int* right, double* theta,
+                          unsigned char* valid) {
+  if (NE < 2 || !isfinite(delta)) {
+    set_last_error("shift plan: at least two nodes and a finite displacement are required");
+    return QCL_ARG;
+  }
+  for (int e = 1; e < NE; ++e)
+    if (!(eps[e] > eps[e - 1]) || !isfinite(eps[e])) {
+      set_last_error("energy nodes must be finite and strictly increasing");
+      return QCL_ARG;
+    }
+  int j = 0;
+  for (int e = 0; e < NE; ++e) {
+    const double target = eps[e] + delta;
+    left[e] = right[e] = 0;
+    theta[e] = 0.0;
+    valid[e] = 0;
+    if (target < eps[0] || target > eps[NE - 1]) continue;
+    if (target == eps[NE - 1]) {
+      left[e] = right[e] = NE - 1;
+      valid[e] = 1;
+      continue;
+    }
+    while (j < NE - 2 && eps[j + 1] <= target) ++j;
+    left[e] = j;
+    right[e] = j + 1;
+    theta[e] = (target - eps[j]) / (eps[j + 1] - eps[j]);
+    valid[e] = 1;
+  }
+  return QCL_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Momentum reduction: X[e + NE q] = sum_m' wk[m'] G[e + NE (m' + Nk q)]
+// ---------------------------------------------------------------------------
+template <typename R>
+__global__ void momentum_sum_kernel(int NE, int Nk, int NQ, const double* __restrict__ wk,
+                                    const Cx<R>* __restrict__ G, Cx<R>* __restrict__ X) {
+  const long long n = (long long)NE * NQ;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const int e = (int)(i % NE);
+    const long long q = i / NE;
+    double sx = 0, sy = 0;
+    for (int mp = 0; mp < Nk; ++mp) {
+      const Cx<R> g = G[(size_t)e + (size_t)NE * ((size_t)mp + (size_t)Nk * q)];
+      sx += wk[mp] * (double)g.x;
+      sy += wk[mp] * (double)g.y;
+    }
+    X[i] = cx<R>((R)sx, (R)sy);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Tiled complex GEMM over strided views:
+//   C[e, j] (bcast copies) = alpha * sum_k A[e,k] w(k,b) B[j,k] + beta * C
+//   A[e,k] = A[e + lda k + a_b b],  B[j,k] = B[j ldb_j + k ldb_k + b_b b],
+//   C[e,j] = C[e + ldc j + c_b b + bcast_stride r], r < bcast.
+// ---------------------------------------------------------------------------
+template <typename R> struct GemmArgs {
+  int M, Nout, K, batch;
+  const Cx<R>* A;
+  long long lda, a_b;
+  const double* wk;  // optional weight wk[k % wk_mod]
+  int wk_mod;
+  const double* wb;  // optional weight wb[b]
+  const Cx<R>* B;
+  long long ldb_j, ldb_k, b_b;
+  Cx<R>* C;
+  long long ldc, c_b;
+  int bcast;
+  long long bcast_stride;
+  double alpha, beta;
+};
+
+constexpr int GE = 64, GJ = 32, GK = 16, GT = 256;
+
+template <typename R> __global__ void __launch_bounds__(GT) gemm_kernel(GemmArgs<R> p) {
+  __shared__ Cx<R> As[GK][GE];
+  __shared__ Cx<R> Bs[GK][GJ];
+  const int b = blockIdx.z;
+  const int e0 = blockIdx.x * GE, j0 = blockIdx.y * GJ;
+  const int te = threadIdx.x % 16, tj = threadIdx.x / 16;
+  const double wbb = p.wb ? p.wb[b] : 1.0;
+  Cx<R> acc[4][2];
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int u = 0; u < 2; ++u) acc[i][u] = cx<R>(0, 0);
+  for (int k0 = 0; k0 < p.K; k0 += GK) {
+    for (int idx = threadIdx.x; idx < GE * GK; idx += GT) {
+      const int el = idx % GE, kl = idx / GE;
+      const int e = e0 + el, k = k0 + kl;
+      Cx<R> v = cx<R>(0, 0);
+      if (e < p.M && k < p.K) {
+        v = p.A[(size_t)e + (size_t)p.lda * k + (size_t)p.a_b * b];
+        double w = wbb;
+        if (p.wk) w *= p.wk[k % p.wk_mod];
+        if (w != 1.0) v = cx<R>((R)(w * v.x), (R)(w * v.y));
+      }
+      As[kl][el] = v;
+    }
+    for (int idx = threadIdx.x; idx < GJ * GK; idx += GT) {
+      const int jl = idx % GJ, kl = idx / GJ;
+      const int j = j0 + jl, k = k0 + kl;
+      Bs[kl][jl] = (j < p.Nout && k < p.K) ? p.B[(size_t)p.ldb_j * j + (size_t)p.ldb_k * k + (size_t)p.b_b * b]
+                                           : cx<R>(0, 0);
+    }
+    __syncthreads();
+#pragma unroll
+    for (int kl = 0; kl < GK; ++kl) {
+      Cx<R> a[4], bb[2];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) a[i] = As[kl][te + 16 * i];
+#pragma unroll
+      for (int u = 0; u < 2; ++u) bb[u] = Bs[kl][tj + 16 * u];
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int u = 0; u < 2; ++u) cfma(acc[i][u], a[i], bb[u]);
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const int e = e0 + te + 16 * i;
+    if (e >= p.M) continue;
+#pragma unroll
+    for (int u = 0; u < 2; ++u) {
+      const int j = j0 + tj + 16 * u;
+      if (j >= p.Nout) continue;
+      const double vx = p.alpha * (double)acc[i][u].x, vy = p.alpha * (double)acc[i][u].y;
+      for (int r = 0; r < p.bcast; ++r) {
+        const size_t idx = (size_t)e + (size_t)p.ldc * j + (size_t)p.c_b * b + (size_t)p.bcast_stride * r;
+        if (p.beta == 0.0) {
+          p.C[idx] = cx<R>((R)vx, (R)vy);
+        } else {
+          const Cx<R> o = p.C[idx];
+          p.C[idx] = cx<R>((R)(p.beta * o.x + vx), (R)(p.beta * o.y + vy));
+        }
+      }
+    }
+  }
+}
+
+template <typename R> static int launch_gemm(const GemmArgs<R>& a, cudaStream_t st) {
+  if (a.M <= 0 || a.Nout <= 0 || a.batch <= 0) return QCL_OK;
+  dim3 grid((a.M + GE - 1) / GE, (a.Nout + GJ - 1) / GJ, a.batch);
+  gemm_kernel<R><<<grid, GT, 0, st>>>(a);
+  QCL_LAUNCH_CHECK("gemm_kernel");
+  return QCL_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Contraction dispatch
+// ---------------------------------------------------------------------------
+template <typename R>
+static int contraction_t(const KernelOpDev& op, int NE, int Nk, int N, const double* wk, const void* Gv, void* Sv,
+                         double alpha_q, double beta, void* work, cudaStream_t st) {
+  const Cx<R>* G = (const Cx<R>*)Gv;
+  Cx<R>* S = (Cx<R>*)Sv;
+  const int N2 = N * N;
+  const long long NEl = NE;
+  if (op.kind == QCL_KERNEL_MOMENTUM_INDEPENDENT) {
+    Cx<R>* X = (Cx<R>*)work;  // NE * N2
+    const long long n = NEl * N2;
+    momentum_sum_kernel<R><<<grid_cap(n, 256), 256, 0, st>>>(NE, Nk, N2, wk, G, X);
+    QCL_LAUNCH_CHECK("momentum_sum_kernel");
+    GemmArgs<R> g{};
+    g.M = NE; g.Nout = N2; g.K = N2; g.batch = 1;
+    g.A = X; g.lda = NEl; g.a_b = 0;
+    g.B = (const Cx<R>*)op.block; g.ldb_j = 1; g.ldb_k = N2; g.b_b = 0;
+    g.C = S; g.ldc = NEl * Nk; g.c_b = 0; g.bcast = Nk; g.bcast_stride = NEl;
+    g.alpha = alpha_q; g.beta = beta;
+    return launch_gemm<R>(g, st);
+  }
+  if (op.kind == QCL_KERNEL_DENSE) {
+    const int Nc = Nk * N2;
+    GemmArgs<R> g{};
+    g.M = NE; g.Nout = Nc; g.K = Nc; g.batch = 1;
+    g.A = G; g.lda = NEl; g.wk = wk; g.wk_mod = Nk;
+    g.B = (const Cx<R>*)op.matrix; g.ldb_j = 1; g.ldb_k = Nc;
+    g.C = S; g.ldc = NEl; g.bcast = 1;
+    g.alpha = alpha_q; g.beta = beta;
+    return launch_gemm<R>(g, st);
+  }
+  if (op.kind == QCL_KERNEL_IFR) {
+    const int J = op.J;
+    Cx<R>* T = (Cx<R>*)work;                  // T[e + NE (j + J m')]
+    Cx<R>* F = T + (size_t)NE * J * Nk;       // F[e + NE (j + J m)]
+    int s;
+    GemmArgs<R> g{};
+    // stage 1, batch m': T = wk[m'] right * G_m'
+    g.M = NE; g.Nout = J; g.K = N2; g.batch = Nk;
+    g.A = G; g.lda = NEl * Nk; g.a_b = NEl; g.wb = wk;
+    g.B = (const Cx<R>*)op.right; g.ldb_j = 1; g.ldb_k = J; g.b_b = 0;
+    g.C = T; g.ldc = NEl; g.c_b = NEl * J; g.bcast = 1;
+    g.alpha = 1.0; g.beta = 0.0;
+    if ((s = launch_gemm<R>(g, st))) return s;
+    // stage 2, batch j: F[., j, m] = sum_m' radial[m, m'] T[., j, m']
+    GemmArgs<R> h{};
+    h.M = NE; h.Nout = Nk; h.K = Nk; h.batch = J;
+    h.A = T; h.lda = NEl * J; h.a_b = NEl;
+    h.B = (const Cx<R>*)op.radial; h.ldb_j = 1; h.ldb_k = Nk; h.b_b = 0;
+    h.C = F; h.ldc = NEl * J; h.c_b = NEl; h.bcast = 1;
+    h.alpha = 1.0; h.beta = 0.0;
+    if ((s = launch_gemm<R>(h, st))) return s;
+    // stage 3, batch m: S[., m, p] = alpha q sum_j left[p, j] F[., j, m] + beta S
+    GemmArgs<R> f{};
+    f.M = NE; f.Nout = N2; f.K = J; f.batch = Nk;
+    f.A = F; f.lda = NEl; f.a_b = NEl * J;
+    f.B = (const Cx<R>*)op.left; f.ldb_j = 1; f.ldb_k = N2; f.b_b = 0;
+    f.C = S; f.ldc = NEl * Nk; f.c_b = NEl; f.bcast = 1;
+    f.alpha = alpha_q; f.beta = beta;
+    return launch_gemm<R>(f, st);
+  }
+  set_last_error("unknown kernel operator kind %d", op.kind);
+  return QCL_ARG;
+}
+
+size_t contraction_work_elems(const KernelOpDev& op, int NE, int Nk, int N) {
+  if (op.kind == QCL_KERNEL_MOMENTUM_INDEPENDENT) return (size_t)NE * N * N;
+  if (op.kind == QCL_KERNEL_IFR) return 2 * (size_t)NE * op.J * Nk;
+  return 0;
+}
+
+int launch_contraction(int precision, const KernelOpDev& op, int NE, int Nk, int N, const double* wk, const void* G,
+                       void* S, double alpha_q, double beta, void* work, cudaStream_t st) {
+  if (precision == QCL_C128) return contraction_t<double>(op, NE, Nk, N, wk, G, S, alpha_q, beta, work, st);
+  return contraction_t<float>(op, NE, Nk, N, wk, G, S, alpha_q, beta, work, st);
+}
+
+}  // namespace qcl

@@ -1,0 +1,504 @@
+// Zero-padded linear-convolution Hilbert transform, fused with the retarded
+// self-energy assembly.
+//
+// Reference: _fft_hilbert_with_length / fft_hilbert_transform
+// (numerics/optimized/production_operators.jl:735-809) and
+// ProductionFFTHilbertPlan (numerics/optimized/fft_parallel.jl:27-291):
+//   kernel[lag + NE - 1] = 1 / (2 pi lag de), 0 < |lag| < NE, zero elsewhere
+//   buffer = wE .* Gam padded to L = nextpow2(2 NE - 1)
+//   Lam_e = IFFT(FFT(buffer) .* FFT(kernel))[e + NE - 1]
+// and _retarded_self_energy_fft_production (:842-884):
+//   Gam = i (S> - S<),  SR = Lam - i Gam / 2.
+//
+// B200 mapping: one CTA per column (m, a, b).  The whole padded column lives
+// in shared memory (L <= 8192 complex128 = 136 KiB padded), the two FFTs are
+// radix-16 Stockham passes with the butterflies in registers, the kernel
+// spectrum is read from L2, and the inputs are read once and the outputs
+// written once (E is the contiguous axis, so every load/store is coalesced).
+//
+// Roundoff verification (fft_parallel.jl:279-290 runs a second transform at
+// length 2L).  Because the input is zero beyond N_E <= L/2 + 1 and only
+// outputs below L are used, the length-2L convolution splits exactly into the
+// length-L convolution (even frequencies; its kernel spectrum folds to the
+// length-L one) plus one twisted length-L convolution (odd frequencies):
+//   y_2L[n] = (y_L[n] + W_2L^{-n} IFFT_L(FFT_L(x W_2L^n) .* K2L_odd)[n]) / 2.
+// So verification costs two extra length-L FFTs instead of two length-2L
+// ones, and the same per-column partial sums of |y_2L - y_L|^2 and |y_L|^2.
+#include <math.h>
+
+#include <vector>
+
+#include "kernels.cuh"
+
+namespace qcl {
+
+__device__ __forceinline__ int fpad(int p) { return p + (p >> 4); }
+
+// W_16^t = exp(-2 pi i t / 16); multiply z by W_16^t (t compile-time).
+template <typename R, int t> __device__ __forceinline__ Cx<R> w16mul(Cx<R> z) {
+  constexpr int u = t & 15;
+  if (u == 0) return z;
+  if (u == 4) return cx<R>(z.y, -z.x);
+  if (u == 8) return cx<R>(-z.x, -z.y);
+  if (u == 12) return cx<R>(-z.y, z.x);
+  const R c1 = (R)0.92387953251128674, s1 = (R)0.38268343236508978, c2 = (R)0.70710678118654752;
+  R c, s;  // W = c - i s
+  switch (u) {
+    case 1: c = c1; s = s1; break;
+    case 2: c = c2; s = c2; break;
+    case 3: c = s1; s = c1; break;
+    case 5: c = -s1; s = c1; break;
+    case 6: c = -c2; s = c2; break;
+    case 7: c = -c1; s = s1; break;
+    case 9: c = -c1; s = -s1; break;
+    case 10: c = -c2; s = -c2; break;
+    case 11: c = -s1; s = -c1; break;
+    case 13: c = s1; s = -c1; break;
+    case 14: c = c2; s = -c2; break;
+    default: c = c1; s = -s1; break;  // 15
+  }
+  return cx<R>(z.x * c + z.y * s, z.y * c - z.x * s);
+}
+
+template <int P> __host__ __device__ constexpr int bitrev(int i) {
+  int r = 0;
+  for (int b = 1; b < P; b <<= 1) {
+    r <<= 1;
+    if (i & b) r |= 1;
+  }
+  return r;
+}
+
+// In-register forward DFT of size P in {2,4,8,16} (radix-2 DIF); output is
+// left in bit-reversed order: X[i] = v[bitrev<P>(i)].
+template <typename R, int P, int H> struct DifStage {
+  __device__ __forceinline__ static void run(Cx<R> (&v)[P]) {
+#pragma unroll
+    for (int start = 0; start < P; start += 2 * H) {
+#pragma unroll
+      for (int k = 0; k < H; ++k) {
+        Cx<R> a = v[start + k], b = v[start + k + H];
+        v[start + k] = a + b;
+        Cx<R> d = a - b;
+        // W_{2H}^k = W_16^{k * 8 / H}
+        switch ((k * 8 / H) & 15) {
+          case 0: v[start + k + H] = d; break;
+          case 1: v[start + k + H] = w16mul<R, 1>(d); break;
+          case 2: v[start + k + H] = w16mul<R, 2>(d); break;
+          case 3: v[start + k + H] = w16mul<R, 3>(d); break;
+          case 4: v[start + k + H] = w16mul<R, 4>(d); break;
+          case 5: v[start + k + H] = w16mul<R, 5>(d); break;
+          case 6: v[start + k + H] = w16mul<R, 6>(d); break;
+          default: v[start + k + H] = w16mul<R, 7>(d); break;
+        }
+      }
+    }
+    DifStage<R, P, H / 2>::run(v);
+  }
+};
+template <typename R, int P> struct DifStage<R, P, 0> {
+  __device__ __forceinline__ static void run(Cx<R> (&)[P]) {}
+};
+
+template <int L> struct FftPlan {
+  static constexpr int T = (L / 16 >= 32) ? L / 16 : 32;
+};
+
+// One mixed-radix Stockham pass (natural-order output after all passes).
+template <typename R, int L, int RADIX, int NS>
+__device__ __forceinline__ void stockham_pass(Cx<R>* buf, const Cx<R>* __restrict__ tw) {
+  constexpr int T = FftPlan<L>::T;
+  constexpr int NB = L / RADIX;
+  constexpr int Q = (NB + T - 1) / T;
+  Cx<R> v[Q][RADIX];
+#pragma unroll
+  for (int q = 0; q < Q; ++q) {
+    const int j = threadIdx.x + q * T;
+    if (j < NB) {
+#pragma unroll
+      for (int r = 0; r < RADIX; ++r) v[q][r] = buf[fpad(j + r * NB)];
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int q = 0; q < Q; ++q) {
+    const int j = threadIdx.x + q * T;
+    if (j < NB) {
+      const int k = j % NS;
+      if (NS > 1) {
+#pragma unroll
+        for (int r = 1; r < RADIX; ++r) {
+          const Cx<R> w = tw[(r * k) * (L / (NS * RADIX))];
+          v[q][r] = v[q][r] * w;
+        }
+      }
+      DifStage<R, RADIX, RADIX / 2>::run(v[q]);
+      const int idxD = (j / NS) * NS * RADIX + k;
+#pragma unroll
+      for (int r = 0; r < RADIX; ++r) buf[fpad(idxD + r * NS)] = v[q][bitrev<RADIX>(r)];
+    }
+  }
+  __syncthreads();
+}
+
+// Forward FFT of length L in shared memory (padded indexing), natural order.
+template <typename R, int L> __device__ __forceinline__ void fft_smem(Cx<R>* buf, const Cx<R>* tw) {
+  static_assert(L >= 64 && L <= 16384, "unsupported FFT length");
+  stockham_pass<R, L, 16, 1>(buf, tw);
+  if constexpr (L == 64) {
+    stockham_pass<R, L, 4, 16>(buf, tw);
+  } else if constexpr (L == 128) {
+    stockham_pass<R, L, 8, 16>(buf, tw);
+  } else {
+    stockham_pass<R, L, 16, 16>(buf, tw);
+    if constexpr (L == 512) stockham_pass<R, L, 2, 256>(buf, tw);
+    if constexpr (L == 1024) stockham_pass<R, L, 4, 256>(buf, tw);
+    if constexpr (L == 2048) stockham_pass<R, L, 8, 256>(buf, tw);
+    if constexpr (L >= 4096) stockham_pass<R, L, 16, 256>(buf, tw);
+    if constexpr (L == 8192) stockham_pass<R, L, 2, 4096>(buf, tw);
+    if constexpr (L == 16384) stockham_pass<R, L, 4, 4096>(buf, tw);
+  }
+}
+
+template <typename R> struct HilbertArgs {
+  int NE;
+  long long ncols;
+  const double* wE;
+  const Cx<R>* Gam;   // input Gam (if SL == null)
+  const Cx<R>* SL;    // fused input: Gam = i (SG - SL)
+  const Cx<R>* SG;
+  Cx<R>* Lam;         // output Lam (if SR == null)
+  Cx<R>* SR;          // fused output: SR = Lam - i Gam / 2
+  Cx<R>* GamOut;      // optional copy of Gam
+  const Cx<R>* khat;  // FFT_L(kernel), L entries
+  const Cx<R>* kodd;  // FFT_2L(kernel)[2k+1], L entries (verification)
+  const Cx<R>* tw;    // W_L^t, t < L
+  const Cx<R>* twist; // W_2L^n, n < L
+  double* partial;    // per column (|y2L - yL|^2, |yL|^2), or null
+  double scale_out;   // 1 / L
+};
+
+template <typename R>
+__device__ __forceinline__ Cx<R> gamma_at(const HilbertArgs<R>& p, size_t idx) {
+  if (p.SL) {
+    Cx<R> d = p.SG[idx] - p.SL[idx];
+    return cx<R>(-d.y, d.x);  // i * d
+  }
+  return p.Gam[idx];
+}
+
+template <typename R, int L>
+__global__ void __launch_bounds__(FftPlan<L>::T) hilbert_kernel(HilbertArgs<R> p) {
+  constexpr int T = FftPlan<L>::T;
+  constexpr int PER = (L / 2 + T - 1) / T;  // outputs per thread (NE <= L/2 + 1)
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  Cx<R>* buf = reinterpret_cast<Cx<R>*>(smem_raw);
+  const long long col = blockIdx.x + (long long)blockIdx.y * gridDim.x;
+  if (col >= p.ncols) return;
+  const int NE = p.NE;
+  const size_t base = (size_t)col * NE;
+  const bool verify = p.partial != nullptr;
+
+  // x = wE .* Gam, zero padded
+  for (int e = threadIdx.x; e < L; e += T) {
+    Cx<R> x = cx<R>(0, 0);
+    if (e < NE) {
+      Cx<R> g = gamma_at(p, base + e);
+      if (p.GamOut) p.GamOut[base + e] = g;
+      x = (R)p.wE[e] * g;
+    }
+    buf[fpad(e)] = x;
+  }
+  __syncthreads();
+  fft_smem<R, L>(buf, p.tw);
+  for (int t = threadIdx.x; t < L; t += T) buf[fpad(t)] = conj(buf[fpad(t)] * p.khat[t]);
+  __syncthreads();
+  fft_smem<R, L>(buf, p.tw);
+  Cx<R> lam[PER];
+  const R sc = (R)p.scale_out;
+#pragma unroll
+  for (int q = 0; q < PER; ++q) {
+    const int e = threadIdx.x + q * T;
+    if (e < NE) {
+      Cx<R> y = conj(buf[fpad(e + NE - 1)]);
+      lam[q] = sc * y;
+      if (!verify) {
+        if (p.SR) {
+          Cx<R> g = gamma_at(p, base + e);
+          p.SR[base + e] = cx<R>(lam[q].x + (R)0.5 * g.y, lam[q].y - (R)0.5 * g.x);
+        } else {
+          p.Lam[base + e] = lam[q];
+        }
+      }
+    }
+  }
+  if (!verify) return;
+  // ---- odd-frequency half of the length-2L transform -------------------------
+  __syncthreads();
+  for (int e = threadIdx.x; e < L; e += T) {
+    Cx<R> x = cx<R>(0, 0);
+    if (e < NE) x = (R)p.wE[e] * (gamma_at(p, base + e) * p.twist[e]);
+    buf[fpad(e)] = x;
+  }
+  __syncthreads();
+  fft_smem<R, L>(buf, p.tw);
+  for (int t = threadIdx.x; t < L; t += T) buf[fpad(t)] = conj(buf[fpad(t)] * p.kodd[t]);
+  __syncthreads();
+  fft_smem<R, L>(buf, p.tw);
+  double dsum = 0, lsum = 0;
+#pragma unroll
+  for (int q = 0; q < PER; ++q) {
+    const int e = threadIdx.x + q * T;
+    if (e < NE) {
+      const int n = e + NE - 1;
+      Cx<R> yo = sc * (conj(buf[fpad(n)]) * conj(p.twist[n]));
+      // y_2L - y_L = (y_L + yo)/2 - y_L = (yo - y_L)/2
+      Cx<R> d = (R)0.5 * (yo - lam[q]);
+      dsum += (double)d.x * d.x + (double)d.y * d.y;
+      lsum += (double)lam[q].x * lam[q].x + (double)lam[q].y * lam[q].y;
+      if (p.SR) {
+        Cx<R> g = gamma_at(p, base + e);
+        p.SR[base + e] = cx<R>(lam[q].x + (R)0.5 * g.y, lam[q].y - (R)0.5 * g.x);
+      } else {
+        p.Lam[base + e] = lam[q];
+      }
+    }
+  }
+  // deterministic block reduction
+  __shared__ double red[2][T / 32];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    dsum += __shfl_xor_sync(0xffffffffu, dsum, o);
+    lsum += __shfl_xor_sync(0xffffffffu, lsum, o);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    red[0][threadIdx.x >> 5] = dsum;
+    red[1][threadIdx.x >> 5] = lsum;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double a = 0, b = 0;
+    for (int w = 0; w < T / 32; ++w) {
+      a += red[0][w];
+      b += red[1][w];
+    }
+    p.partial[2 * col] = a;
+    p.partial[2 * col + 1] = b;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Host side: per-(N_E, spacing) tables.
+// ---------------------------------------------------------------------------
+static void host_fft(std::vector<double>& re, std::vector<double>& im) {
+  const size_t n = re.size();
+  for (size_t i = 1, j = 0; i < n; ++i) {
+    size_t bit = n >> 1;
+    for (; j & bit; bit >>= 1) j ^= bit;
+    j ^= bit;
+    if (i < j) {
+      std::swap(re[i], re[j]);
+      std::swap(im[i], im[j]);
+    }
+  }
+  for (size_t len = 2; len <= n; len <<= 1) {
+    for (size_t k = 0; k < len / 2; ++k) {
+      const double ang = -2.0 * M_PI * (double)k / (double)len;
+      const double wr = cos(ang), wi = sin(ang);
+      for (size_t i = 0; i < n; i += len) {
+        const size_t a = i + k, b = i + k + len / 2;
+        const double xr = re[b] * wr - im[b] * wi, xi = re[b] * wi + im[b] * wr;
+        re[b] = re[a] - xr;
+        im[b] = im[a] - xi;
+        re[a] += xr;
+        im[a] += xi;
+      }
+    }
+  }
+}
+
+int next_pow2(int n) {
+  int L = 1;
+  while (L < n) L <<= 1;
+  return L;
+}
+
+void free_hilbert_tables(HilbertTables& t) {
+  cudaFree(t.khat);
+  cudaFree(t.kodd);
+  cudaFree(t.tw);
+  cudaFree(t.twist);
+  cudaFree(t.partial);
+  t = HilbertTables();
+}
+
+template <typename R> static int upload_cx(void** dst, const std::vector<double>& re, const std::vector<double>& im) {
+  std::vector<Cx<R>> h(re.size());
+  for (size_t i = 0; i < re.size(); ++i) h[i] = cx<R>((R)re[i], (R)im[i]);
+  QCL_CUDA_CHECK(cudaMalloc(dst, h.size() * sizeof(Cx<R>)));
+  QCL_CUDA_CHECK(cudaMemcpy(*dst, h.data(), h.size() * sizeof(Cx<R>), cudaMemcpyHostToDevice));
+  return QCL_OK;
+}
+
+int check_uniform_grid(int NE, const double* eps_host, double* de_out) {
+  if (NE < 2) {
+    set_last_error("at least two energy nodes are required");
+    return QCL_ARG;
+  }
+  const double de = eps_host[1] - eps_host[0];
+  if (!(de > 0)) {
+    set_last_error("energy grid must be strictly increasing");
+    return QCL_ARG;
+  }
+  double dev = 0, mx = fmax(fabs(de), 1.0);
+  for (int e = 0; e < NE; ++e) mx = fmax(mx, fabs(eps_host[e]));
+  for (int e = 1; e < NE; ++e) dev = fmax(dev, fabs((eps_host[e] - eps_host[e - 1]) - de));
+  if (!(dev <= 256 * 2.220446049250313e-16 * mx)) {
+    set_last_error("FFT Hilbert transform requires a uniform energy grid");
+    return QCL_ARG;
+  }
+  *de_out = de;
+  return QCL_OK;
+}
+
+// Builds (or reuses) the tables for (NE, de, precision).
+int prepare_hilbert_tables(HilbertTables& t, int NE, double de, int precision) {
+  const int L = next_pow2(2 * NE - 1);
+  const int storage = precision == QCL_C128 ? QCL_C128 : QCL_C64;
+  if (t.NE == NE && t.de == de && t.precision == storage && t.khat) return QCL_OK;
+  free_hilbert_tables(t);
+  const int maxL = storage == QCL_C128 ? 8192 : 16384;
+  if (L < 64 || L > maxL) {
+    set_last_error("FFT Hilbert length %d outside the supported range [64, %d]", L, maxL);
+    return QCL_UNSUPPORTED;
+  }
+  // kernel spectra at L and 2L
+  std::vector<double> kr(L, 0.0), ki(L, 0.0), kr2(2 * L, 0.0), ki2(2 * L, 0.0);
+  for (int lag = -(NE - 1); lag <= NE - 1; ++lag) {
+    if (lag == 0) continue;
+    const double v = 1.0 / (2.0 * M_PI * lag * de);
+    kr[lag + NE - 1] = v;
+    kr2[lag + NE - 1] = v;
+  }
+  host_fft(kr, ki);
+  host_fft(kr2, ki2);
+  std::vector<double> kor(L), koi(L), twr(L), twi(L), tsr(L), tsi(L);
+  for (int k = 0; k < L; ++k) {
+    kor[k] = kr2[2 * k + 1];
+    koi[k] = ki2[2 * k + 1];
+    twr[k] = cos(2.0 * M_PI * k / L);
+    twi[k] = -sin(2.0 * M_PI * k / L);
+    tsr[k] = cos(M_PI * k / L);
+    tsi[k] = -sin(M_PI * k / L);
+  }
+  int st;
+  if (storage == QCL_C128) {
+    if ((st = upload_cx<double>(&t.khat, kr, ki))) return st;
+    if ((st = upload_cx<double>(&t.kodd, kor, koi))) return st;
+    if ((st = upload_cx<double>(&t.tw, twr, twi))) return st;
+    if ((st = upload_cx<double>(&t.twist, tsr, tsi))) return st;
+  } else {
+    if ((st = upload_cx<float>(&t.khat, kr, ki))) return st;
+    if ((st = upload_cx<float>(&t.kodd, kor, koi))) return st;
+    if ((st = upload_cx<float>(&t.tw, twr, twi))) return st;
+    if ((st = upload_cx<float>(&t.twist, tsr, tsi))) return st;
+  }
+  t.NE = NE;
+  t.L = L;
+  t.de = de;
+  t.precision = storage;
+  return QCL_OK;
+}
+
+int ensure_partial(HilbertTables& t, long long ncols) {
+  if (t.partial_cols >= ncols) return QCL_OK;
+  cudaFree(t.partial);
+  t.partial = nullptr;
+  QCL_CUDA_CHECK(cudaMalloc(&t.partial, (size_t)ncols * 2 * sizeof(double)));
+  t.partial_cols = ncols;
+  return QCL_OK;
+}
+
+template <typename R, int L> static int launch_hilbert_L(const HilbertArgs<R>& a, cudaStream_t st) {
+  constexpr int T = FftPlan<L>::T;
+  constexpr size_t smem = (size_t)(L + L / 16) * sizeof(Cx<R>);
+  static bool configured = false;
+  if (!configured) {
+    QCL_CUDA_CHECK(cudaFuncSetAttribute(hilbert_kernel<R, L>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)smem));
+    configured = true;
+  }
+  const long long nc = a.ncols;
+  dim3 grid((unsigned)(nc < 65535 ? nc : 65535), (unsigned)((nc + 65534) / 65535));
+  hilbert_kernel<R, L><<<grid, T, smem, st>>>(a);
+  QCL_LAUNCH_CHECK("hilbert_kernel");
+  return QCL_OK;
+}
+
+template <typename R> static int launch_hilbert_t(const HilbertArgs<R>& a, int L, cudaStream_t st) {
+  switch (L) {
+    case 64: return launch_hilbert_L<R, 64>(a, st);
+    case 128: return launch_hilbert_L<R, 128>(a, st);
+    case 256: return launch_hilbert_L<R, 256>(a, st);
+    case 512: return launch_hilbert_L<R, 512>(a, st);
+    case 1024: return launch_hilbert_L<R, 1024>(a, st);
+    case 2048: return launch_hilbert_L<R, 2048>(a, st);
+    case 4096: return launch_hilbert_L<R, 4096>(a, st);
+    case 8192: return launch_hilbert_L<R, 8192>(a, st);
+    case 16384:
+      if constexpr (sizeof(R) == 4) return launch_hilbert_L<R, 16384>(a, st);
+      [[fallthrough]];
+    default:
+      set_last_error("unsupported FFT length %d", L);
+      return QCL_UNSUPPORTED;
+  }
+}
+
+// Launch on device arrays.  Exactly one of (Gam) or (SL, SG) is the input and
+// one of (Lam) or (SR) the output.  If verify, per-column partial sums land in
+// t.partial (2 doubles per column).
+int launch_hilbert(HilbertTables& t, int precision, long long ncols, const double* wE, const void* Gam,
+                   const void* SL, const void* SG, void* Lam, void* SR, void* GamOut, bool verify,
+                   cudaStream_t st, long long partial_offset) {
+  if (verify) {
+    int s = ensure_partial(t, ncols + partial_offset);
+    if (s) return s;
+  }
+  if (ncols <= 0) return QCL_OK;
+  if (precision == QCL_C128) {
+    HilbertArgs<double> a{t.NE,
+                          ncols,
+                          wE,
+                          (const Cx<double>*)Gam,
+                          (const Cx<double>*)SL,
+                          (const Cx<double>*)SG,
+                          (Cx<double>*)Lam,
+                          (Cx<double>*)SR,
+                          (Cx<double>*)GamOut,
+                          (const Cx<double>*)t.khat,
+                          (const Cx<double>*)t.kodd,
+                          (const Cx<double>*)t.tw,
+                          (const Cx<double>*)t.twist,
+                          verify ? t.partial + 2 * partial_offset : nullptr,
+                          1.0 / t.L};
+    return launch_hilbert_t<double>(a, t.L, st);
+  }
+  HilbertArgs<float> a{t.NE,
+                       ncols,
+                       wE,
+                       (const Cx<float>*)Gam,
+                       (const Cx<float>*)SL,
+                       (const Cx<float>*)SG,
+                       (Cx<float>*)Lam,
+                       (Cx<float>*)SR,
+                       (Cx<float>*)GamOut,
+                       (const Cx<float>*)t.khat,
+                       (const Cx<float>*)t.kodd,
+                       (const Cx<float>*)t.tw,
+                       (const Cx<float>*)t.twist,
+                       verify ? t.partial + 2 * partial_offset : nullptr,
+                       1.0 / t.L};
+  return launch_hilbert_t<float>(a, t.L, st);
+}
+
+}  // namespace qcl

@@ -1,0 +1,99 @@
+// Internal launch interfaces shared by the translation units.
+#pragma once
+#include "common.cuh"
+
+namespace qcl {
+
+int padded_size(int N);
+int next_pow2(int n);
+
+int launch_dyson_keldysh(int precision, int NE, int Nk, int N, const double* eps, double eta, const void* h,
+                         const void* sigR, const void* sigL, const void* sigG, void* GR, void* GL, void* GG,
+                         double* scale, void* traceL, void* traceG, int* status, cudaStream_t st, int m0 = 0,
+                         int mcount = -1);
+
+int launch_weighted_trace(int NE, int Nk, const void* tr, const double* wE, const double* wk, double* partial,
+                          double* out, cudaStream_t st);
+int launch_paired_coefficients(const double* trL, const double* trG, int gs, double target, double* coeffs,
+                               int* status, cudaStream_t st, double realness_limit = 1e-10);
+int launch_normalize_pair(int precision, size_t n, void* GL, void* GG, const double* coeffs, cudaStream_t st);
+int launch_sum_fields(int precision, size_t n, const void* const* src, int count, void* out, cudaStream_t st);
+int launch_residual_mix(int precision, size_t n, const void* old, void* new_, double alpha, double* partial,
+                        double* out2, cudaStream_t st);
+int launch_combine(const double* partial, int count, int K, double* out, cudaStream_t st);
+int launch_axpby(int precision, size_t n, double a, const void* x, double b, const void* y, void* out,
+                 cudaStream_t st);
+constexpr int kReduceCtas = 296;
+
+// Device view of an EnergyShiftPlan (0-based left/right).
+struct ShiftPlanDev {
+  const int* left = nullptr;
+  const int* right = nullptr;
+  const double* theta = nullptr;
+  const unsigned char* valid = nullptr;
+};
+int build_shift_plan_host(int NE, const double* eps, double delta, int* left, int* right, double* theta,
+                          unsigned char* valid);
+int launch_shift(int precision, int NE, long long ncols, const ShiftPlanDev& plan, const void* X, void* Y,
+                 cudaStream_t st);
+
+// Device view of a factorised kernel operator (arrays in the field precision).
+struct KernelOpDev {
+  int kind = 0;
+  int J = 0;
+  const void* block = nullptr;   // (N^2, N^2): rows (a,b), cols (c,d)
+  const void* matrix = nullptr;  // (Nk N^2)^2: rows (m,a,b), cols (m',c,d)
+  const void* left = nullptr;    // (N^2, J)
+  const void* right = nullptr;   // (J, N^2)
+  const void* radial = nullptr;  // (Nk, Nk)
+};
+size_t contraction_work_elems(const KernelOpDev& op, int NE, int Nk, int N);
+int launch_contraction(int precision, const KernelOpDev& op, int NE, int Nk, int N, const double* wk, const void* G,
+                       void* S, double alpha_q, double beta, void* work, cudaStream_t st);
+
+// Shifted sandwiches  S_c(e,m) = T X_c(shift(e), m) T^H  for up to 3
+// components and 2 signs (embedding self-energies).
+struct SandwichJob {
+  const void* X[3] = {nullptr, nullptr, nullptr};
+  void* S[3] = {nullptr, nullptr, nullptr};
+  const void* T = nullptr;  // complex128 N x N (column-major)
+  ShiftPlanDev plan;
+};
+int launch_sandwich(int precision, int NE, int Nk, int N, const SandwichJob* jobs, int njobs, cudaStream_t st);
+
+struct HilbertTables {
+  int NE = 0, L = 0, precision = -1;
+  double de = 0;
+  void* khat = nullptr;
+  void* kodd = nullptr;
+  void* tw = nullptr;
+  void* twist = nullptr;
+  double* partial = nullptr;
+  long long partial_cols = 0;
+};
+void free_hilbert_tables(HilbertTables& t);
+int check_uniform_grid(int NE, const double* eps_host, double* de_out);
+int prepare_hilbert_tables(HilbertTables& t, int NE, double de, int precision);
+int ensure_partial(HilbertTables& t, long long ncols);
+int launch_hilbert(HilbertTables& t, int precision, long long ncols, const double* wE, const void* Gam,
+                   const void* SL, const void* SG, void* Lam, void* SR, void* GamOut, bool verify,
+                   cudaStream_t st, long long partial_offset = 0);
+
+int launch_residual_suite(int precision, int NE, int Nk, int N, const double* eps, const void* h, const void* GR,
+                          const void* GL, const void* GG, const void* SR, const void* SL, const void* SG,
+                          const void* SLc, double* work, double* out5, cudaStream_t st);
+size_t residual_work_doubles(int NE, int Nk);
+int launch_eigvals(int n, long long count, const void* A, double* vals, cudaStream_t st);
+size_t observables_partial_doubles(int N);
+int launch_observables(int precision, int NE, int Nk, int N, const double* wE, const double* wk, const void* SG,
+                       const void* SL, const void* GL, const void* GG, int gs, double target, double* partial,
+                       double* out, cudaStream_t st);
+int launch_seed_weights(int precision, int NE, int Nk, int N, const void* GR, const double* wE, const double* wk,
+                        int gs, double* q, cudaStream_t st);
+int launch_seed_green(int precision, int NE, int Nk, int N, const void* GR, const double* f, void* GL, void* GG,
+                      cudaStream_t st);
+int launch_residual_pair(int precision, size_t n, const void* o1, const void* o2, const void* n1, const void* n2,
+                         double* partial, double* out2, cudaStream_t st);
+int launch_convert(int precision, size_t n, const void* in_c128, void* out, cudaStream_t st);
+
+}  // namespace qcl

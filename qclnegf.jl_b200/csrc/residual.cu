@@ -1,0 +1,524 @@
+// Fixed-point residual suite, FP64.
+//
+// Reference: production_residual_suite (numerics/optimized/residuals.jl:
+// 537-770) with the definitions of numerics/reference/validation.jl:33-103:
+//   r_D   = max_em ||D G - I||_F / (||D||_F ||G||_F + sqrt(N))
+//   r_A   = sqrt(sum ||A - G Gam G^H||^2) / (sqrt(sum ||A||^2) + 1e-14)
+//   r_K   = sqrt(sum ||G< - G S^<_cand G^H||^2) / (sqrt(sum ||G<||^2) + 1e-14)
+//   r_PSD = max over {A, -iG<, iG>, Gam, -i G S< G^H, i G S> G^H} of
+//           max(0, -lmin - 64 n eps max(|l|max, 1)) / |l|max
+//           (psd_error_budget, numerics/reference/positivity_diagnostics.jl:
+//           15-40, witness ratio :60-90)
+//   r_caus = max_em max(0, lmax(Im_H SR)) / (||SR||_2 + 1e-14)
+// with D = eps I - h - SR_total, Gam = i(S>_total - S<_total), A = i(G - G^H).
+//
+// B200 mapping: one team per (E,k) block as in the Dyson kernel; the Hermitian
+// eigenvalues (LAPACK zheev in the reference, residuals.jl:311-353) come from a
+// team-parallel complex Jacobi iteration (round-robin pairing, all rotations
+// of a round applied at once), the spectral norm of SR (zgesvd, :355-409) from
+// the same solver on SR SR^H, needed only when lmax(Im SR) > 0.  Per-block
+// partial results go to global memory and are reduced in a fixed order.
+#include "blockmat.cuh"
+
+namespace qcl {
+
+template <typename RS> struct ResidualArgs {
+  int NE, Nk, N;
+  const double* eps;
+  const Cx<double>* h;
+  const Cx<RS>* GR;
+  const Cx<RS>* GL;
+  const Cx<RS>* GG;
+  const Cx<RS>* SR;   // totals
+  const Cx<RS>* SL;
+  const Cx<RS>* SG;
+  const Cx<RS>* SLc;  // candidate total lesser
+  double* block_out;  // 7 doubles per block
+};
+
+struct JacobiRot {
+  double c, s, pr, pi;  // rotation cosine/sine and the phase e^{i phi}
+  int p, q;
+};
+
+template <int NP> struct ResScratch {
+  JacobiRot rot[NP / 2];
+  double red[8];
+  double vals[NP];
+};
+
+// Team sum of two doubles (fixed order).
+template <int TT>
+__device__ __forceinline__ void team_sum2(double& a, double& b, int tt, double* scratch, int team) {
+  a = team_sum<TT>(a, tt, scratch, team);
+  b = team_sum<TT>(b, tt, scratch + 2, team);
+}
+
+// Eigenvalues of the Hermitian NxN matrix H (swizzled NP x NP shared tile);
+// H is destroyed, S.vals[0..N-1] receives the eigenvalues (unsorted).
+template <int NP, int TT>
+__device__ void team_eigvals(Cx<double>* H, int N, int tt, ResScratch<NP>& S, int team) {
+  const int n2 = N + (N & 1);
+  for (int sweep = 0; sweep < 40; ++sweep) {
+    double off = 0, dia = 0;
+    for (int idx = tt; idx < N * N; idx += TT) {
+      const int i = idx % N, j = idx / N;
+      const Cx<double> v = H[sw<NP>(i, j)];
+      const double m2 = v.x * v.x + v.y * v.y;
+      if (i == j) dia += m2; else off += m2;
+    }
+    off = team_sum<TT>(off, tt, S.red, team);
+    dia = team_sum<TT>(dia, tt, S.red + 2, team);
+    if (!(off > 1e-32 * dia) || !isfinite(off)) break;
+    for (int r = 0; r < n2 - 1; ++r) {
+      if (tt < n2 / 2) {
+        const int i = tt;
+        const int a = (r + i) % (n2 - 1);
+        const int b = (i == 0) ? n2 - 1 : (r - i + n2 - 1) % (n2 - 1);
+        JacobiRot rt;
+        rt.p = a < b ? a : b;
+        rt.q = a < b ? b : a;
+        rt.c = 1;
+        rt.s = 0;
+        rt.pr = 1;
+        rt.pi = 0;
+        if (rt.q < N) {
+          const Cx<double> apq = H[sw<NP>(rt.p, rt.q)];
+          const double mag = sqrt(apq.x * apq.x + apq.y * apq.y);
+          if (mag > 0 && isfinite(mag)) {
+            const double app = H[sw<NP>(rt.p, rt.p)].x, aqq = H[sw<NP>(rt.q, rt.q)].x;
+            const double theta = (aqq - app) / (2 * mag);
+            double t;
+            if (fabs(theta) > 1e150) t = 0.5 / theta;
+            else t = (theta >= 0 ? 1.0 : -1.0) / (fabs(theta) + sqrt(theta * theta + 1.0));
+            rt.c = 1.0 / sqrt(t * t + 1.0);
+            rt.s = t * rt.c;
+            rt.pr = apq.x / mag;
+            rt.pi = apq.y / mag;
+          }
+        } else {
+          rt.q = rt.p;  // phantom partner: identity
+        }
+        S.rot[i] = rt;
+      }
+      team_sync<TT>(team);
+      // columns: H <- H J
+      for (int idx = tt; idx < N * (n2 / 2); idx += TT) {
+        const int k = idx % N;
+        const JacobiRot rt = S.rot[idx / N];
+        if (rt.p == rt.q || rt.s == 0) continue;
+        const Cx<double> hp = H[sw<NP>(k, rt.p)], hq = H[sw<NP>(k, rt.q)];
+        const Cx<double> eq = cx<double>(rt.pr, -rt.pi) * hq;  // e^{-i phi} H[k][q]
+        H[sw<NP>(k, rt.p)] = cx<double>(rt.c * hp.x - rt.s * eq.x, rt.c * hp.y - rt.s * eq.y);
+        H[sw<NP>(k, rt.q)] = cx<double>(rt.s * hp.x + rt.c * eq.x, rt.s * hp.y + rt.c * eq.y);
+      }
+      team_sync<TT>(team);
+      // rows: H <- J^H H
+      for (int idx = tt; idx < N * (n2 / 2); idx += TT) {
+        const int k = idx % N;
+        const JacobiRot rt = S.rot[idx / N];
+        if (rt.p == rt.q || rt.s == 0) continue;
+        const Cx<double> xp = H[sw<NP>(rt.p, k)], xq = H[sw<NP>(rt.q, k)];
+        const Cx<double> eq = cx<double>(rt.pr, rt.pi) * xq;  // e^{i phi} H[q][k]
+        H[sw<NP>(rt.p, k)] = cx<double>(rt.c * xp.x - rt.s * eq.x, rt.c * xp.y - rt.s * eq.y);
+        H[sw<NP>(rt.q, k)] = cx<double>(rt.s * xp.x + rt.c * eq.x, rt.s * xp.y + rt.c * eq.y);
+      }
+      team_sync<TT>(team);
+    }
+  }
+  for (int i = tt; i < N; i += TT) S.vals[i] = H[sw<NP>(i, i)].x;
+  team_sync<TT>(team);
+}
+
+// Writes the Hermitian part of f*X into H; returns false if X has non-finite
+// entries (team-uniform).
+template <int NP, int TT>
+__device__ bool hermitian_part(const Cx<double>* X, Cx<double> f, Cx<double>* H, int N, int tt, ResScratch<NP>& S,
+                               int team) {
+  double bad = 0;
+  for (int idx = tt; idx < N * N; idx += TT) {
+    const int i = idx % N, j = idx / N;
+    const Cx<double> v = f * X[sw<NP>(i, j)], w = f * X[sw<NP>(j, i)];
+    if (!isfinite(v.x) || !isfinite(v.y) || !isfinite(w.x) || !isfinite(w.y)) bad = 1;
+    H[sw<NP>(i, j)] = cx<double>(0.5 * (v.x + w.x), 0.5 * (v.y - w.y));
+  }
+  bad = team_max<TT>(bad, tt, S.red, team);
+  return bad == 0;
+}
+
+// Positivity ratio of the (already Hermitian) H.
+template <int NP, int TT>
+__device__ double psd_ratio(Cx<double>* H, int N, int tt, ResScratch<NP>& S, int team) {
+  team_eigvals<NP, TT>(H, N, tt, S, team);
+  double lmin = INFINITY, bn = 0;
+  bool finite = true;
+  for (int i = 0; i < N; ++i) {
+    const double v = S.vals[i];
+    finite = finite && isfinite(v);
+    lmin = fmin(lmin, v);
+    bn = fmax(bn, fabs(v));
+  }
+  if (!finite) return INFINITY;
+  const double budget = 64.0 * N * 2.220446049250313e-16 * fmax(bn, 1.0);
+  const double absolute = fmax(0.0, -lmin);
+  return fmax(0.0, absolute - budget) / fmax(bn, 2.2250738585072014e-308);
+}
+
+template <typename RS, int NP, int BPC>
+__device__ __forceinline__ void load_tile(const Cx<RS>* X, Cx<double>* bufs, int e0, int m, int NE, int Nk, int N) {
+  load_blocks<RS, double, NP, BPC>(X, bufs, (size_t)NP * NP, e0, m, NE, Nk, N);
+}
+
+template <typename RS, int NP, int BPC>
+__global__ void __launch_bounds__(BPC* Tile<NP>::TT) residual_kernel(ResidualArgs<RS> p) {
+  constexpr int TT = Tile<NP>::TT;
+  constexpr size_t MSZ = (size_t)NP * NP;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  Cx<double>* bG = reinterpret_cast<Cx<double>*>(smem_raw);
+  Cx<double>* bX = bG + BPC * MSZ;
+  Cx<double>* bW = bX + BPC * MSZ;
+  Cx<double>* bH = bW + BPC * MSZ;
+  Cx<double>* bY = bH + BPC * MSZ;
+  ResScratch<NP>* scr = reinterpret_cast<ResScratch<NP>*>(bY + BPC * MSZ);
+  const int N = p.N, NE = p.NE, Nk = p.Nk;
+  const int m = blockIdx.y, e0 = blockIdx.x * BPC;
+  const int team = threadIdx.x / TT, tt = threadIdx.x % TT;
+  const int e = e0 + team;
+  const bool live = e < NE;
+  Cx<double>* G = bG + team * MSZ;
+  Cx<double>* X = bX + team * MSZ;
+  Cx<double>* W = bW + team * MSZ;
+  Cx<double>* H = bH + team * MSZ;
+  Cx<double>* Y = bY + team * MSZ;
+  ResScratch<NP>& S = scr[team];
+  const Cx<double> one = cx<double>(1, 0), mi = cx<double>(0, -1), pi = cx<double>(0, 1);
+
+  load_tile<RS, NP, BPC>(p.GR, bG, e0, m, NE, Nk, N);
+  load_tile<RS, NP, BPC>(p.SR, bX, e0, m, NE, Nk, N);
+  __syncthreads();
+  const double eps_e = live ? p.eps[e] : 0.0;
+
+  // ---- causality: lmax(Im_H SR) --------------------------------------------
+  double caus_num = 0;
+  {
+    double bad = 0;
+    for (int idx = tt; idx < N * N; idx += TT) {
+      const int i = idx % N, j = idx / N;
+      const Cx<double> a = X[sw<NP>(i, j)], b = X[sw<NP>(j, i)];
+      if (!isfinite(a.x) || !isfinite(a.y)) bad = 1;
+      // (a - conj(b)) / (2i)
+      const double dx = a.x - b.x, dy = a.y + b.y;
+      H[sw<NP>(i, j)] = cx<double>(0.5 * dy, -0.5 * dx);
+    }
+    bad = team_max<TT>(bad, tt, S.red, team);
+    if (bad != 0) {
+      caus_num = INFINITY;
+    } else {
+      team_eigvals<NP, TT>(H, N, tt, S, team);
+      double lmax = -INFINITY;
+      for (int i = 0; i < N; ++i) lmax = fmax(lmax, S.vals[i]);
+      caus_num = fmax(0.0, lmax);
+    }
+  }
+  double caus = 0;
+  if (caus_num > 0 && isfinite(caus_num)) {  // team-uniform
+    // ||SR||_2^2 = lmax(SR SR^H)
+    team_matmul<double, double, NP>(X, X, H, N, tt, true);
+    team_sync<TT>(team);
+    team_eigvals<NP, TT>(H, N, tt, S, team);
+    double lmax = 0;
+    for (int i = 0; i < N; ++i) lmax = fmax(lmax, S.vals[i]);
+    caus = caus_num / (sqrt(fmax(lmax, 0.0)) + 1e-14);
+  } else if (!isfinite(caus_num)) {
+    caus = INFINITY;
+  }
+
+  // ---- r_D -------------------------------------------------------------------
+  double nD = 0, nG = 0;
+  for (int idx = tt; idx < N * N; idx += TT) {
+    const int i = idx % N, j = idx / N;
+    const Cx<double> hv = p.h[(size_t)m + (size_t)Nk * ((size_t)i + (size_t)N * j)];
+    Cx<double> d = X[sw<NP>(i, j)];
+    d = cx<double>(-hv.x - d.x, -hv.y - d.y);
+    if (i == j) d.x += eps_e;
+    X[sw<NP>(i, j)] = d;
+    nD += d.x * d.x + d.y * d.y;
+    const Cx<double> g = G[sw<NP>(i, j)];
+    nG += g.x * g.x + g.y * g.y;
+  }
+  team_sum2<TT>(nD, nG, tt, S.red, team);
+  team_sync<TT>(team);
+  team_matmul<double, double, NP>(X, G, W, N, tt, false);
+  team_sync<TT>(team);
+  double nR = 0;
+  for (int idx = tt; idx < N * N; idx += TT) {
+    const int i = idx % N, j = idx / N;
+    Cx<double> v = W[sw<NP>(i, j)];
+    if (i == j) v.x -= 1;
+    nR += v.x * v.x + v.y * v.y;
+  }
+  nR = team_sum<TT>(nR, tt, S.red, team);
+  double rD = sqrt(nR) / (sqrt(nD) * sqrt(nG) + sqrt((double)N));
+  if (!isfinite(rD)) rD = INFINITY;
+
+  // ---- spectral function A and its positivity ---------------------------------
+  double psd = 0;
+  for (int idx = tt; idx < N * N; idx += TT) {
+    const int i = idx % N, j = idx / N;
+    const Cx<double> g = G[sw<NP>(i, j)], gt = G[sw<NP>(j, i)];
+    // A = i (G - G^H)
+    Y[sw<NP>(i, j)] = pi * cx<double>(g.x - gt.x, g.y + gt.y);
+  }
+  team_sync<TT>(team);
+  if (hermitian_part<NP, TT>(Y, one, H, N, tt, S, team)) psd = fmax(psd, psd_ratio<NP, TT>(H, N, tt, S, team));
+  else psd = INFINITY;
+
+  // ---- Gamma = i (S> - S<), its positivity, r_A ---------------------------------
+  __syncthreads();
+  load_tile<RS, NP, BPC>(p.SG, bX, e0, m, NE, Nk, N);
+  load_tile<RS, NP, BPC>(p.SL, bW, e0, m, NE, Nk, N);
+  __syncthreads();
+  for (int idx = tt; idx < N * N; idx += TT) {
+    const int i = idx % N, j = idx / N;
+    const Cx<double> g = X[sw<NP>(i, j)], l = W[sw<NP>(i, j)];
+    X[sw<NP>(i, j)] = pi * cx<double>(g.x - l.x, g.y - l.y);
+  }
+  team_sync<TT>(team);
+  if (hermitian_part<NP, TT>(X, one, H, N, tt, S, team)) psd = fmax(psd, psd_ratio<NP, TT>(H, N, tt, S, team));
+  else psd = INFINITY;
+  team_matmul<double, double, NP>(G, X, W, N, tt, false);  // W = G Gam
+  team_sync<TT>(team);
+  team_matmul<double, double, NP>(W, G, H, N, tt, true);   // H = G Gam G^H
+  team_sync<TT>(team);
+  double aNum = 0, aDen = 0;
+  for (int idx = tt; idx < N * N; idx += TT) {
+    const int i = idx % N, j = idx / N;
+    const Cx<double> a = Y[sw<NP>(i, j)], q = H[sw<NP>(i, j)];
+    aNum += (a.x - q.x) * (a.x - q.x) + (a.y - q.y) * (a.y - q.y);
+    aDen += a.x * a.x + a.y * a.y;
+  }
+  team_sum2<TT>(aNum, aDen, tt, S.red, team);
+
+  // ---- raw Keldysh products -i G S< G^H, i G S> G^H ------------------------------
+  for (int which = 0; which < 2; ++which) {
+    __syncthreads();
+    load_tile<RS, NP, BPC>(which == 0 ? p.SL : p.SG, bX, e0, m, NE, Nk, N);
+    __syncthreads();
+    team_matmul<double, double, NP>(G, X, W, N, tt, false);
+    team_sync<TT>(team);
+    team_matmul<double, double, NP>(W, G, Y, N, tt, true);
+    team_sync<TT>(team);
+    if (hermitian_part<NP, TT>(Y, which == 0 ? mi : pi, H, N, tt, S, team))
+      psd = fmax(psd, psd_ratio<NP, TT>(H, N, tt, S, team));
+    else
+      psd = INFINITY;
+  }
+
+  // ---- G< : positivity and r_K against the candidate lesser self-energy ----------
+  __syncthreads();
+  load_tile<RS, NP, BPC>(p.GL, bX, e0, m, NE, Nk, N);
+  load_tile<RS, NP, BPC>(p.SLc, bY, e0, m, NE, Nk, N);
+  __syncthreads();
+  if (hermitian_part<NP, TT>(X, mi, H, N, tt, S, team)) psd = fmax(psd, psd_ratio<NP, TT>(H, N, tt, S, team));
+  else psd = INFINITY;
+  team_matmul<double, double, NP>(G, Y, W, N, tt, false);
+  team_sync<TT>(team);
+  team_matmul<double, double, NP>(W, G, H, N, tt, true);
+  team_sync<TT>(team);
+  double kNum = 0, kDen = 0;
+  for (int idx = tt; idx < N * N; idx += TT) {
+    const int i = idx % N, j = idx / N;
+    const Cx<double> a = X[sw<NP>(i, j)], q = H[sw<NP>(i, j)];
+    kNum += (a.x - q.x) * (a.x - q.x) + (a.y - q.y) * (a.y - q.y);
+    kDen += a.x * a.x + a.y * a.y;
+  }
+  team_sum2<TT>(kNum, kDen, tt, S.red, team);
+
+  // ---- G> positivity ---------------------------------------------------------------
+  __syncthreads();
+  load_tile<RS, NP, BPC>(p.GG, bX, e0, m, NE, Nk, N);
+  __syncthreads();
+  if (hermitian_part<NP, TT>(X, pi, H, N, tt, S, team)) psd = fmax(psd, psd_ratio<NP, TT>(H, N, tt, S, team));
+  else psd = INFINITY;
+
+  if (tt == 0 && live) {
+    double* o = p.block_out + 7 * ((size_t)e + (size_t)NE * m);
+    o[0] = rD;
+    o[1] = isfinite(aNum) ? aNum : INFINITY;
+    o[2] = isfinite(aDen) ? aDen : INFINITY;
+    o[3] = isfinite(kNum) ? kNum : INFINITY;
+    o[4] = isfinite(kDen) ? kDen : INFINITY;
+    o[5] = psd;
+    o[6] = caus;
+  }
+}
+
+// Fixed-order reduction of the per-block outputs:
+// out = (r_D, r_A, r_K, r_PSD, r_caus).
+__global__ void residual_reduce_kernel(long long blocks, const double* __restrict__ bo, double* partial) {
+  double mx[3] = {0, 0, 0}, sm[4] = {0, 0, 0, 0};
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < blocks;
+       i += (long long)gridDim.x * blockDim.x) {
+    const double* o = bo + 7 * i;
+    mx[0] = fmax(mx[0], o[0]) + (isnan(o[0]) ? INFINITY : 0.0);
+    sm[0] += o[1];
+    sm[1] += o[2];
+    sm[2] += o[3];
+    sm[3] += o[4];
+    mx[1] = fmax(mx[1], o[5]) + (isnan(o[5]) ? INFINITY : 0.0);
+    mx[2] = fmax(mx[2], o[6]) + (isnan(o[6]) ? INFINITY : 0.0);
+  }
+  __shared__ double red[7][8];
+  double v[7] = {mx[0], sm[0], sm[1], sm[2], sm[3], mx[1], mx[2]};
+#pragma unroll
+  for (int k = 0; k < 7; ++k)
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      const double q = __shfl_xor_sync(0xffffffffu, v[k], o);
+      v[k] = (k == 0 || k >= 5) ? fmax(v[k], q) : v[k] + q;
+    }
+  if ((threadIdx.x & 31) == 0)
+    for (int k = 0; k < 7; ++k) red[k][threadIdx.x >> 5] = v[k];
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int k = 0; k < 7; ++k) {
+      double s = red[k][0];
+      for (int w = 1; w < 8; ++w) s = (k == 0 || k >= 5) ? fmax(s, red[k][w]) : s + red[k][w];
+      partial[7 * blockIdx.x + k] = s;
+    }
+  }
+}
+
+__global__ void residual_final_kernel(int ncta, const double* partial, double* out) {
+  if (threadIdx.x != 0) return;
+  double v[7] = {0, 0, 0, 0, 0, 0, 0};
+  for (int c = 0; c < ncta; ++c)
+    for (int k = 0; k < 7; ++k) {
+      const double q = partial[7 * c + k];
+      v[k] = (k == 0 || k >= 5) ? fmax(v[k], q) : v[k] + q;
+    }
+  out[0] = v[0];
+  out[1] = (isfinite(v[1]) && isfinite(v[2])) ? sqrt(v[1]) / (sqrt(v[2]) + 1e-14) : INFINITY;
+  out[2] = (isfinite(v[3]) && isfinite(v[4])) ? sqrt(v[3]) / (sqrt(v[4]) + 1e-14) : INFINITY;
+  out[3] = v[5];
+  out[4] = v[6];
+}
+
+template <typename RS, int NP, int BPC> static int launch_residual_t(const ResidualArgs<RS>& a, cudaStream_t st) {
+  constexpr int TT = Tile<NP>::TT;
+  constexpr size_t smem = 5 * (size_t)BPC * NP * NP * sizeof(Cx<double>) + BPC * sizeof(ResScratch<NP>);
+  static bool configured = false;
+  if (!configured) {
+    QCL_CUDA_CHECK(cudaFuncSetAttribute(residual_kernel<RS, NP, BPC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)smem));
+    configured = true;
+  }
+  dim3 grid((a.NE + BPC - 1) / BPC, a.Nk);
+  residual_kernel<RS, NP, BPC><<<grid, BPC * TT, smem, st>>>(a);
+  QCL_LAUNCH_CHECK("residual_kernel");
+  return QCL_OK;
+}
+
+template <typename RS> static int launch_residual_p(const ResidualArgs<RS>& a, cudaStream_t st) {
+  switch (padded_size(a.N)) {
+    case 8: return launch_residual_t<RS, 8, 8>(a, st);
+    case 16: return launch_residual_t<RS, 16, 4>(a, st);
+    case 24: return launch_residual_t<RS, 24, 2>(a, st);
+    case 32: return launch_residual_t<RS, 32, 1>(a, st);
+    case 48: return launch_residual_t<RS, 48, 1>(a, st);
+    default:
+      set_last_error("basis size N_b=%d exceeds the supported maximum 48", a.N);
+      return QCL_UNSUPPORTED;
+  }
+}
+
+// Batched Hermitian eigenvalues: matrices (n x n, column-major, complex128)
+// stored back to back; one team per matrix.
+template <int NP, int BPC>
+__global__ void __launch_bounds__(BPC* Tile<NP>::TT) eigvals_kernel(int n, long long count,
+                                                                    const Cx<double>* __restrict__ A, double* vals) {
+  constexpr int TT = Tile<NP>::TT;
+  constexpr size_t MSZ = (size_t)NP * NP;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  Cx<double>* bH = reinterpret_cast<Cx<double>*>(smem_raw);
+  ResScratch<NP>* scr = reinterpret_cast<ResScratch<NP>*>(bH + BPC * MSZ);
+  const int team = threadIdx.x / TT, tt = threadIdx.x % TT;
+  const long long mat = (long long)blockIdx.x * BPC + team;
+  const bool live = mat < count;
+  Cx<double>* H = bH + team * MSZ;
+  for (int idx = tt; idx < n * n; idx += TT) {
+    const int i = idx % n, j = idx / n;
+    H[sw<NP>(i, j)] = live ? A[(size_t)mat * n * n + idx] : cx<double>(i == j ? 1.0 : 0.0, 0.0);
+  }
+  team_sync<TT>(team);
+  // Hermitian part (as zheev reads one triangle of a Hermitian input)
+  for (int idx = tt; idx < n * n; idx += TT) {
+    const int i = idx % n, j = idx / n;
+    if (i > j) {
+      const Cx<double> a = H[sw<NP>(i, j)], b = H[sw<NP>(j, i)];
+      const Cx<double> m = cx<double>(0.5 * (a.x + b.x), 0.5 * (a.y - b.y));
+      H[sw<NP>(i, j)] = m;
+      H[sw<NP>(j, i)] = conj(m);
+    } else if (i == j) {
+      H[sw<NP>(i, i)] = cx<double>(H[sw<NP>(i, i)].x, 0.0);
+    }
+  }
+  team_sync<TT>(team);
+  team_eigvals<NP, TT>(H, n, tt, scr[team], team);
+  if (live)
+    for (int i = tt; i < n; i += TT) vals[(size_t)mat * n + i] = scr[team].vals[i];
+}
+
+int launch_eigvals(int n, long long count, const void* A, double* vals, cudaStream_t st) {
+  const int NP = padded_size(n);
+  if (NP == 0) {
+    set_last_error("matrix size %d exceeds the supported maximum 48", n);
+    return QCL_UNSUPPORTED;
+  }
+#define EIGV(NPV, BPCV)                                                                                       \
+  do {                                                                                                         \
+    constexpr size_t smem = (size_t)BPCV * NPV * NPV * sizeof(Cx<double>) + BPCV * sizeof(ResScratch<NPV>);  \
+    cudaFuncSetAttribute(eigvals_kernel<NPV, BPCV>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem); \
+    eigvals_kernel<NPV, BPCV><<<(unsigned)((count + BPCV - 1) / BPCV), BPCV * Tile<NPV>::TT, smem, st>>>(    \
+        n, count, (const Cx<double>*)A, vals);                                                                \
+  } while (0)
+  switch (NP) {
+    case 8: EIGV(8, 8); break;
+    case 16: EIGV(16, 4); break;
+    case 24: EIGV(24, 4); break;
+    case 32: EIGV(32, 2); break;
+    default: EIGV(48, 1); break;
+  }
+#undef EIGV
+  QCL_LAUNCH_CHECK("eigvals_kernel");
+  return QCL_OK;
+}
+
+constexpr int RES_CTAS = 148;
+
+size_t residual_work_doubles(int NE, int Nk) { return 7 * (size_t)NE * Nk + 7 * RES_CTAS; }
+
+int launch_residual_suite(int precision, int NE, int Nk, int N, const double* eps, const void* h, const void* GR,
+                          const void* GL, const void* GG, const void* SR, const void* SL, const void* SG,
+                          const void* SLc, double* work, double* out5, cudaStream_t st) {
+  int s;
+  if (precision == QCL_C128) {
+    ResidualArgs<double> a{NE, Nk, N, eps, (const Cx<double>*)h, (const Cx<double>*)GR, (const Cx<double>*)GL,
+                           (const Cx<double>*)GG, (const Cx<double>*)SR, (const Cx<double>*)SL,
+                           (const Cx<double>*)SG, (const Cx<double>*)SLc, work};
+    s = launch_residual_p<double>(a, st);
+  } else {
+    ResidualArgs<float> a{NE, Nk, N, eps, (const Cx<double>*)h, (const Cx<float>*)GR, (const Cx<float>*)GL,
+                          (const Cx<float>*)GG, (const Cx<float>*)SR, (const Cx<float>*)SL, (const Cx<float>*)SG,
+                          (const Cx<float>*)SLc, work};
+    s = launch_residual_p<float>(a, st);
+  }
+  if (s) return s;
+  double* partial = work + 7 * (size_t)NE * Nk;
+  residual_reduce_kernel<<<RES_CTAS, 256, 0, st>>>((long long)NE * Nk, work, partial);
+  residual_final_kernel<<<1, 32, 0, st>>>(RES_CTAS, partial, out5);
+  QCL_LAUNCH_CHECK("residual_reduce");
+  return QCL_OK;
+}
+
+}  // namespace qcl

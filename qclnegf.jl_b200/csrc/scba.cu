@@ -1,0 +1,691 @@
+// Device-resident SCBA inner loop (the production cache + state + iteration).
+//
+// Reference: solve_scba_production (numerics/optimized/production_solver.jl:
+// 21-846; loop body :435-844) and the educational solve_scba
+// (numerics/reference/scba.jl:142-354).  One iteration nu:
+//   1. total = plus + minus + sum_mech                (_total_family_production)
+//   2. GR, G<, G> = Dyson + Keldysh(total); paired number normalisation
+//                                                       (_current_green_production)
+//   3. candidate scattering families (contractions, LO shifts, FFT Hilbert
+//      with roundoff verification)                      (_scattering_candidate_production)
+//   4. candidate embedding families (shifted sandwiches)
+//   5. residual suite and r_Sigma                       (_production_fixed_point_measurement)
+//   6. J, populations                                   (_production_observable_measurement)
+//   7. mixing (linear), committed only if the caller continues
+// Every field stays in HBM; each iteration reads back one small block of
+// scalars (residuals, J, populations, lambda) to the host, which applies the
+// reference's termination policy.  The whole launch sequence of an
+// iteration can be captured once into a CUDA graph and replayed.
+#include <math.h>
+#include <string.h>
+
+#include <algorithm>
+#include <vector>
+
+#include "kernels.cuh"
+
+namespace qcl {
+
+struct DevShift {
+  int* left = nullptr;
+  int* right = nullptr;
+  double* theta = nullptr;
+  unsigned char* valid = nullptr;
+  ShiftPlanDev view() const { return ShiftPlanDev{left, right, theta, valid}; }
+};
+
+struct Mech {
+  int kind = 0, is_LO = 0, J = 0;
+  double q = 0;
+  void* block = nullptr;
+  void* matrix = nullptr;
+  void* left = nullptr;
+  void* right = nullptr;
+  void* radial = nullptr;
+  KernelOpDev view() const {
+    KernelOpDev k;
+    k.kind = kind;
+    k.J = J;
+    k.block = block;
+    k.matrix = matrix;
+    k.left = left;
+    k.right = right;
+    k.radial = radial;
+    return k;
+  }
+};
+
+// Device scalar block layout (doubles), downloaded once per iteration.
+enum {
+  SC_TRL = 0,      // 2: sum wE wk tr G<  (raw)
+  SC_TRG = 2,      // 2: sum wE wk tr G>
+  SC_COEF = 4,     // 5: a, c, lambda, N, H
+  SC_RES = 9,      // 5: rD, rA, rK, rPSD, rcaus
+  SC_EMB = 14,     // 6: embedding-total residual (num, den) x 3 components
+  SC_OBS = 20,     // 2 + N: Jbar, Im, populations
+  SC_FAM = 20 + 2 + 48,  // (M + 2) families x 3 components x (num, den)
+  SC_ROUND = SC_FAM + 7 * 3 * 2,  // M x (num, den) Hilbert roundoff
+  SC_TOTAL = SC_ROUND + 5 * 2
+};
+
+struct ScbaCtx {
+  int NE, Nk, N, M, precision, gs, verify;
+  double Ep, hw_LO, N_LO, target, eta_seed, kBT, alpha, J0;
+  size_t nfield, fbytes;
+  cudaStream_t st = nullptr;
+  // grids and operators
+  double *eps = nullptr, *wE = nullptr, *wk = nullptr;
+  void *h = nullptr, *Tp = nullptr, *Tm = nullptr;
+  std::vector<double> eps_h, wE_h;
+  DevShift shift[4];  // +Ep, -Ep, +LO, -LO
+  std::vector<Mech> mech;
+  // fields: family f (0..M-1 mechanisms, M plus, M+1 minus), component c (R,<,>)
+  std::vector<void*> state, cand;  // (M+2)*3 each
+  void *GR = nullptr, *GL = nullptr, *GG = nullptr;
+  void *tot[3] = {nullptr, nullptr, nullptr};
+  void* candSL = nullptr;
+  void* tmp = nullptr;
+  void* cwork = nullptr;
+  // reductions
+  Cx<double>*trL = nullptr, *trG = nullptr;
+  double* rpartial = nullptr;
+  double* reswork = nullptr;
+  double* obspartial = nullptr;
+  double* scal = nullptr;
+  double* scal_h = nullptr;  // pinned
+  int* status = nullptr;
+  HilbertTables hil;
+  // graph of one iteration (two parities: state/cand swap)
+  cudaGraphExec_t graph[2] = {nullptr, nullptr};
+  bool use_graph = false;
+  int parity = 0;
+  bool pending_commit = false;
+  int nu = 0;
+  double Jprev = NAN;
+  std::vector<double> pprev, pops;
+  bool seeded = false;
+};
+
+static void* field_of(const std::vector<void*>& v, int f, int c) { return v[3 * f + c]; }
+
+static int dalloc(void** p, size_t bytes) {
+  cudaError_t e = cudaMalloc(p, bytes > 0 ? bytes : 16);
+  if (e != cudaSuccess) return cuda_status(e, "cudaMalloc (SCBA context)");
+  return QCL_OK;
+}
+template <typename T> static int dupload(T** p, const void* host, size_t bytes) {
+  int s = dalloc((void**)p, bytes);
+  if (s) return s;
+  QCL_CUDA_CHECK(cudaMemcpy(*p, host, bytes, cudaMemcpyHostToDevice));
+  return QCL_OK;
+}
+
+static int upload_op(ScbaCtx* c, void** dst, const void* host_c128, size_t n) {
+  void* tmp = nullptr;
+  int s = dupload(&tmp, host_c128, n * 16);
+  if (s) return s;
+  if ((s = dalloc(dst, n * (c->precision == QCL_C128 ? 16 : 8)))) {
+    cudaFree(tmp);
+    return s;
+  }
+  s = launch_convert(c->precision, n, tmp, *dst, c->st);
+  cudaStreamSynchronize(c->st);
+  cudaFree(tmp);
+  return s;
+}
+
+static int build_plan(ScbaCtx* c, DevShift& d, double delta) {
+  std::vector<int> l(c->NE), r(c->NE);
+  std::vector<double> th(c->NE);
+  std::vector<unsigned char> v(c->NE);
+  int s = build_shift_plan_host(c->NE, c->eps_h.data(), delta, l.data(), r.data(), th.data(), v.data());
+  if (s) return s;
+  if ((s = dupload(&d.left, l.data(), c->NE * sizeof(int)))) return s;
+  if ((s = dupload(&d.right, r.data(), c->NE * sizeof(int)))) return s;
+  if ((s = dupload(&d.theta, th.data(), c->NE * sizeof(double)))) return s;
+  return dupload(&d.valid, v.data(), c->NE);
+}
+
+void scba_destroy(ScbaCtx* c) {
+  if (!c) return;
+  if (c->st) cudaStreamSynchronize(c->st);
+  for (int g = 0; g < 2; ++g)
+    if (c->graph[g]) cudaGraphExecDestroy(c->graph[g]);
+  cudaFree(c->eps);
+  cudaFree(c->wE);
+  cudaFree(c->wk);
+  cudaFree(c->h);
+  cudaFree(c->Tp);
+  cudaFree(c->Tm);
+  for (auto& d : c->shift) {
+    cudaFree(d.left);
+    cudaFree(d.right);
+    cudaFree(d.theta);
+    cudaFree(d.valid);
+  }
+  for (auto& m : c->mech) {
+    cudaFree(m.block);
+    cudaFree(m.matrix);
+    cudaFree(m.left);
+    cudaFree(m.right);
+    cudaFree(m.radial);
+  }
+  for (void* p : c->state) cudaFree(p);
+  for (void* p : c->cand) cudaFree(p);
+  cudaFree(c->GR);
+  cudaFree(c->GL);
+  cudaFree(c->GG);
+  for (auto p : c->tot) cudaFree(p);
+  cudaFree(c->candSL);
+  cudaFree(c->tmp);
+  cudaFree(c->cwork);
+  cudaFree(c->trL);
+  cudaFree(c->trG);
+  cudaFree(c->rpartial);
+  cudaFree(c->reswork);
+  cudaFree(c->obspartial);
+  cudaFree(c->scal);
+  cudaFreeHost(c->scal_h);
+  cudaFree(c->status);
+  free_hilbert_tables(c->hil);
+  if (c->st) cudaStreamDestroy(c->st);
+  delete c;
+}
+
+int scba_create(const qcl_scba_problem* p, const qcl_mechanism* mechs, ScbaCtx** out) {
+  *out = nullptr;
+  if (!p || p->NE < 2 || p->Nk < 1 || p->Nb < 1) {
+    set_last_error("scba_create: invalid dimensions");
+    return QCL_DIM;
+  }
+  if (padded_size(p->Nb) == 0) {
+    set_last_error("basis size N_b=%d exceeds the supported maximum 48", p->Nb);
+    return QCL_UNSUPPORTED;
+  }
+  if (p->nmech < 0 || p->nmech > 5) {
+    set_last_error("scba_create: 0..5 scattering mechanisms supported, got %d", p->nmech);
+    return QCL_ARG;
+  }
+  if (!(p->alpha > 0 && p->alpha <= 1)) {
+    set_last_error("mixing factor must lie in (0,1]");
+    return QCL_ARG;
+  }
+  if (p->precision != QCL_C128 && p->precision != QCL_C64 && p->precision != QCL_MIXED) {
+    set_last_error("unknown precision %d", p->precision);
+    return QCL_ARG;
+  }
+  ScbaCtx* c = new ScbaCtx();
+  c->NE = p->NE;
+  c->Nk = p->Nk;
+  c->N = p->Nb;
+  c->M = p->nmech;
+  c->precision = p->precision;
+  c->gs = p->gs;
+  c->verify = p->verify_roundoff;
+  c->Ep = p->Ep;
+  c->hw_LO = p->hw_LO;
+  c->N_LO = p->N_LO;
+  c->target = p->target;
+  c->eta_seed = p->eta_seed;
+  c->kBT = p->kBT;
+  c->alpha = p->alpha;
+  c->J0 = p->J0;
+  c->nfield = field_elems(c->NE, c->Nk, c->N);
+  c->fbytes = c->nfield * (c->precision == QCL_C128 ? 16 : 8);
+  c->eps_h.assign(p->eps, p->eps + p->NE);
+  c->wE_h.assign(p->wE, p->wE + p->NE);
+  int s;
+#define TRY(x)            \
+  do {                    \
+    if ((s = (x))) {      \
+      scba_destroy(c);    \
+      return s;           \
+    }                     \
+  } while (0)
+  double de;
+  TRY(check_uniform_grid(c->NE, p->eps, &de));
+  {
+    cudaError_t e = cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking);
+    if (e != cudaSuccess) TRY(cuda_status(e, "cudaStreamCreate"));
+  }
+  TRY(dupload(&c->eps, p->eps, c->NE * sizeof(double)));
+  TRY(dupload(&c->wE, p->wE, c->NE * sizeof(double)));
+  TRY(dupload(&c->wk, p->wk, c->Nk * sizeof(double)));
+  TRY(dupload(&c->h, p->h, (size_t)c->Nk * c->N * c->N * 16));
+  TRY(dupload(&c->Tp, p->Tplus, (size_t)c->N * c->N * 16));
+  TRY(dupload(&c->Tm, p->Tminus, (size_t)c->N * c->N * 16));
+  TRY(build_plan(c, c->shift[0], +c->Ep));
+  TRY(build_plan(c, c->shift[1], -c->Ep));
+  TRY(build_plan(c, c->shift[2], +c->hw_LO));
+  TRY(build_plan(c, c->shift[3], -c->hw_LO));
+  size_t cwork = 0;
+  const int N2 = c->N * c->N;
+  for (int i = 0; i < c->M; ++i) {
+    const qcl_mechanism& q = mechs[i];
+    Mech m;
+    m.kind = q.kind;
+    m.is_LO = q.is_LO;
+    m.q = q.q;
+    m.J = q.J;
+    c->mech.push_back(m);
+    Mech& d = c->mech.back();
+    if (q.kind == QCL_KERNEL_MOMENTUM_INDEPENDENT) {
+      TRY(upload_op(c, &d.block, q.block, (size_t)N2 * N2));
+    } else if (q.kind == QCL_KERNEL_DENSE) {
+      const size_t nc = (size_t)c->Nk * N2;
+      TRY(upload_op(c, &d.matrix, q.matrix, nc * nc));
+    } else if (q.kind == QCL_KERNEL_IFR) {
+      if (q.J < 1) TRY((set_last_error("IFR operator needs J >= 1"), QCL_ARG));
+      TRY(upload_op(c, &d.left, q.left, (size_t)N2 * q.J));
+      TRY(upload_op(c, &d.right, q.right, (size_t)q.J * N2));
+      TRY(upload_op(c, &d.radial, q.radial, (size_t)c->Nk * c->Nk));
+    } else {
+      TRY((set_last_error("unknown kernel kind %d", q.kind), QCL_ARG));
+    }
+    cwork = std::max(cwork, contraction_work_elems(d.view(), c->NE, c->Nk, c->N));
+  }
+  const int F = c->M + 2;
+  c->state.assign(3 * F, nullptr);
+  c->cand.assign(3 * F, nullptr);
+  for (int i = 0; i < 3 * F; ++i) {
+    TRY(dalloc(&c->state[i], c->fbytes));
+    TRY(dalloc(&c->cand[i], c->fbytes));
+  }
+  TRY(dalloc(&c->GR, c->fbytes));
+  TRY(dalloc(&c->GL, c->fbytes));
+  TRY(dalloc(&c->GG, c->fbytes));
+  for (auto& t : c->tot) TRY(dalloc(&t, c->fbytes));
+  TRY(dalloc(&c->candSL, c->fbytes));
+  TRY(dalloc(&c->tmp, c->fbytes));
+  TRY(dalloc(&c->cwork, cwork * (c->precision == QCL_C128 ? 16 : 8)));
+  TRY(dalloc((void**)&c->trL, (size_t)c->NE * c->Nk * 16));
+  TRY(dalloc((void**)&c->trG, (size_t)c->NE * c->Nk * 16));
+  TRY(dalloc((void**)&c->rpartial, kReduceCtas * 2 * sizeof(double)));
+  TRY(dalloc((void**)&c->reswork, residual_work_doubles(c->NE, c->Nk) * sizeof(double)));
+  TRY(dalloc((void**)&c->obspartial, observables_partial_doubles(c->N) * sizeof(double)));
+  TRY(dalloc((void**)&c->scal, SC_TOTAL * sizeof(double)));
+  {
+    cudaError_t e = cudaMallocHost((void**)&c->scal_h, SC_TOTAL * sizeof(double));
+    if (e != cudaSuccess) TRY(cuda_status(e, "cudaMallocHost"));
+  }
+  TRY(dalloc((void**)&c->status, 2 * sizeof(int)));
+  QCL_CUDA_CHECK(cudaMemsetAsync(c->status, 0, 2 * sizeof(int), c->st));
+  QCL_CUDA_CHECK(cudaMemsetAsync(c->scal, 0, SC_TOTAL * sizeof(double), c->st));
+  TRY(prepare_hilbert_tables(c->hil, c->NE, de, c->precision));
+  TRY(ensure_partial(c->hil, (long long)c->Nk * N2));
+#undef TRY
+  QCL_CUDA_CHECK(cudaStreamSynchronize(c->st));
+  c->pops.assign(c->N, 0.0);
+  *out = c;
+  return QCL_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Candidate maps (stream-ordered launches; no host synchronisation)
+// ---------------------------------------------------------------------------
+static int scattering_candidates(ScbaCtx* c, const void* GL, const void* GG, std::vector<void*>& dst, bool verify) {
+  int s;
+  const int p = c->precision;
+  // contractions run at storage precision (mixed: FP32 with FP64 k-sums)
+  const int cp = p == QCL_MIXED ? QCL_C64 : p;
+  const long long ncols = (long long)c->Nk * c->N * c->N;
+  for (int i = 0; i < c->M; ++i) {
+    const Mech& m = c->mech[i];
+    const KernelOpDev op = m.view();
+    void* SL = field_of(dst, i, 1);
+    void* SG = field_of(dst, i, 2);
+    if (m.is_LO) {
+      // _production_lo_contraction, thermal branch (production_operators.jl:1045-1163)
+      const double n = c->N_LO;
+      if ((s = launch_shift(cp, c->NE, ncols, c->shift[2].view(), GL, c->tmp, c->st))) return s;
+      if ((s = launch_contraction(cp, op, c->NE, c->Nk, c->N, c->wk, c->tmp, SL, (n + 1) * m.q, 0.0, c->cwork, c->st)))
+        return s;
+      if ((s = launch_shift(cp, c->NE, ncols, c->shift[3].view(), GL, c->tmp, c->st))) return s;
+      if ((s = launch_contraction(cp, op, c->NE, c->Nk, c->N, c->wk, c->tmp, SL, n * m.q, 1.0, c->cwork, c->st)))
+        return s;
+      if ((s = launch_shift(cp, c->NE, ncols, c->shift[3].view(), GG, c->tmp, c->st))) return s;
+      if ((s = launch_contraction(cp, op, c->NE, c->Nk, c->N, c->wk, c->tmp, SG, (n + 1) * m.q, 0.0, c->cwork, c->st)))
+        return s;
+      if ((s = launch_shift(cp, c->NE, ncols, c->shift[2].view(), GG, c->tmp, c->st))) return s;
+      if ((s = launch_contraction(cp, op, c->NE, c->Nk, c->N, c->wk, c->tmp, SG, n * m.q, 1.0, c->cwork, c->st)))
+        return s;
+    } else {
+      if ((s = launch_contraction(cp, op, c->NE, c->Nk, c->N, c->wk, GL, SL, m.q, 0.0, c->cwork, c->st))) return s;
+      if ((s = launch_contraction(cp, op, c->NE, c->Nk, c->N, c->wk, GG, SG, m.q, 0.0, c->cwork, c->st))) return s;
+    }
+    if ((s = launch_hilbert(c->hil, cp, ncols, c->wE, nullptr, SL, SG, nullptr, field_of(dst, i, 0), nullptr, verify,
+                            c->st)))
+      return s;
+    if (verify && (s = launch_combine(c->hil.partial, (int)ncols, 2, c->scal + SC_ROUND + 2 * i, c->st))) return s;
+  }
+  return QCL_OK;
+}
+
+static int embedding_candidates(ScbaCtx* c, std::vector<void*>& dst) {
+  const int cp = c->precision == QCL_MIXED ? QCL_C64 : c->precision;
+  SandwichJob jobs[2];
+  for (int sgn = 0; sgn < 2; ++sgn) {
+    jobs[sgn].X[0] = c->GR;
+    jobs[sgn].X[1] = c->GL;
+    jobs[sgn].X[2] = c->GG;
+    for (int k = 0; k < 3; ++k) jobs[sgn].S[k] = field_of(dst, c->M + sgn, k);
+    jobs[sgn].T = sgn == 0 ? c->Tp : c->Tm;
+    jobs[sgn].plan = c->shift[sgn].view();
+  }
+  return launch_sandwich(cp, c->NE, c->Nk, c->N, jobs, 2, c->st);
+}
+
+static int totals(ScbaCtx* c, const std::vector<void*>& fam, void* const* out, int comps_mask) {
+  const int F = c->M + 2;
+  for (int k = 0; k < 3; ++k) {
+    if (!(comps_mask & (1 << k))) continue;
+    const void* src[8];
+    for (int f = 0; f < F; ++f) src[f] = field_of(fam, f, k);
+    int s = launch_sum_fields(c->precision == QCL_MIXED ? QCL_C64 : c->precision, c->nfield, src, F, out[k], c->st);
+    if (s) return s;
+  }
+  return QCL_OK;
+}
+
+// The current Green state from the state families (_current_green_production).
+static int current_green(ScbaCtx* c, const std::vector<void*>& fam) {
+  int s;
+  if ((s = totals(c, fam, c->tot, 7))) return s;
+  if ((s = launch_dyson_keldysh(c->precision, c->NE, c->Nk, c->N, c->eps, 0.0, c->h, c->tot[0], c->tot[1], c->tot[2],
+                                c->GR, c->GL, c->GG, nullptr, c->trL, c->trG, c->status, c->st)))
+    return s;
+  if ((s = launch_weighted_trace(c->NE, c->Nk, c->trL, c->wE, c->wk, c->rpartial, c->scal + SC_TRL, c->st))) return s;
+  if ((s = launch_weighted_trace(c->NE, c->Nk, c->trG, c->wE, c->wk, c->rpartial, c->scal + SC_TRG, c->st))) return s;
+  if ((s = launch_paired_coefficients(c->scal + SC_TRL, c->scal + SC_TRG, c->gs, c->target, c->scal + SC_COEF,
+                                      c->status, c->st, c->precision == QCL_C128 ? 1e-10 : 1e-5)))
+    return s;
+  const int sp = c->precision == QCL_MIXED ? QCL_C64 : c->precision;
+  return launch_normalize_pair(sp, c->nfield, c->GL, c->GG, c->scal + SC_COEF, c->st);
+}
+
+// Everything of one iteration after the state is fixed; writes candidates into
+// `cand`, mixed values into `cand` as well (speculatively) and all scalars.
+static int iteration_body(ScbaCtx* c, std::vector<void*>& state, std::vector<void*>& cand) {
+  int s;
+  const int sp = c->precision == QCL_MIXED ? QCL_C64 : c->precision;
+  if ((s = current_green(c, state))) return s;
+  if ((s = scattering_candidates(c, c->GL, c->GG, cand, c->verify != 0))) return s;
+  if ((s = embedding_candidates(c, cand))) return s;
+  // candidate total lesser for r_K
+  {
+    const void* src[8];
+    const int F = c->M + 2;
+    for (int f = 0; f < F; ++f) src[f] = field_of(cand, f, 1);
+    if ((s = launch_sum_fields(sp, c->nfield, src, F, c->candSL, c->st))) return s;
+  }
+  if ((s = launch_residual_suite(c->precision, c->NE, c->Nk, c->N, c->eps, c->h, c->GR, c->GL, c->GG, c->tot[0],
+                                 c->tot[1], c->tot[2], c->candSL, c->reswork, c->scal + SC_RES, c->st)))
+    return s;
+  // embedding-total residual (before the plus/minus candidates are mixed over)
+  for (int k = 0; k < 3; ++k)
+    if ((s = launch_residual_pair(sp, c->nfield, field_of(state, c->M, k), field_of(state, c->M + 1, k),
+                                  field_of(cand, c->M, k), field_of(cand, c->M + 1, k), c->rpartial,
+                                  c->scal + SC_EMB + 2 * k, c->st)))
+      return s;
+  // J from the (unmixed) plus family and the state's G
+  if ((s = launch_observables(sp, c->NE, c->Nk, c->N, c->wE, c->wk, field_of(state, c->M, 2), field_of(state, c->M, 1),
+                              c->GL, c->GG, c->gs, c->target, c->obspartial, c->scal + SC_OBS, c->st)))
+    return s;
+  // per-family residual + speculative linear mixing into the candidate buffers
+  const int F = c->M + 2;
+  for (int f = 0; f < F; ++f)
+    for (int k = 0; k < 3; ++k)
+      if ((s = launch_residual_mix(sp, c->nfield, field_of(state, f, k), field_of(cand, f, k), c->alpha, c->rpartial,
+                                   c->scal + SC_FAM + 2 * (3 * f + k), c->st)))
+        return s;
+  QCL_CUDA_CHECK(cudaMemcpyAsync(c->scal_h, c->scal, SC_TOTAL * sizeof(double), cudaMemcpyDeviceToHost, c->st));
+  return QCL_OK;
+}
+
+static double fermi(double e, double mu, double kBT) {
+  const double x = (e - mu) / kBT;
+  if (x > 40.0) return 0.0;   // _FERMI_EXPONENT_SATURATION
+  if (x < -40.0) return 1.0;
+  return 1.0 / (exp(x) + 1.0);
+}
+
+int scba_seed(ScbaCtx* c, double* mu_out) {
+  int s;
+  const int sp = c->precision == QCL_MIXED ? QCL_C64 : c->precision;
+  // Dyson with eta_seed and Sigma = 0 (cand fields used as scratch zeros)
+  QCL_CUDA_CHECK(cudaMemsetAsync(c->tot[0], 0, c->fbytes, c->st));
+  if ((s = launch_dyson_keldysh(c->precision, c->NE, c->Nk, c->N, c->eps, c->eta_seed, c->h, c->tot[0], nullptr,
+                                nullptr, c->GR, nullptr, nullptr, nullptr, nullptr, nullptr, c->status, c->st)))
+    return s;
+  double* q_d = c->reswork;  // scratch
+  if ((s = launch_seed_weights(sp, c->NE, c->Nk, c->N, c->GR, c->wE, c->wk, c->gs, q_d, c->st))) return s;
+  std::vector<double> q(c->NE), f(c->NE);
+  QCL_CUDA_CHECK(cudaMemcpyAsync(q.data(), q_d, c->NE * sizeof(double), cudaMemcpyDeviceToHost, c->st));
+  QCL_CUDA_CHECK(cudaStreamSynchronize(c->st));
+  int hst[2];
+  QCL_CUDA_CHECK(cudaMemcpy(hst, c->status, sizeof(hst), cudaMemcpyDeviceToHost));
+  if (hst[0]) {
+    set_last_error("seed Dyson solve failed (status %d at block %d)", hst[0], hst[1]);
+    return hst[0];
+  }
+  for (int e = 0; e < c->NE; ++e)
+    if (!isfinite(q[e])) {
+      set_last_error("seed spectral number weights must be finite");
+      return QCL_DOMAIN;
+    }
+  auto number_at = [&](double mu) {
+    double v = 0;
+    for (int e = 0; e < c->NE; ++e) v += q[e] * fermi(c->eps_h[e], mu, c->kBT);
+    return v - c->target;
+  };
+  double lo = c->eps_h.front() - 50 * c->kBT, hi = c->eps_h.back() + 50 * c->kBT;
+  double flo = number_at(lo), fhi = number_at(hi);
+  if (!(flo * fhi <= 0)) {
+    set_last_error("seed chemical-potential root is not bracketed");
+    return QCL_ARG;
+  }
+  // bisection to adjacent doubles (the role of Roots.jl Bisection, seed.jl:182)
+  double mu;
+  if (flo == 0) mu = lo;
+  else if (fhi == 0) mu = hi;
+  else {
+    for (int it = 0; it < 2000; ++it) {
+      const double mid = 0.5 * (lo + hi);
+      if (mid == lo || mid == hi) break;
+      const double fm = number_at(mid);
+      if (fm == 0) {
+        lo = hi = mid;
+        break;
+      }
+      if ((fm < 0) == (flo < 0)) {
+        lo = mid;
+        flo = fm;
+      } else {
+        hi = mid;
+      }
+    }
+    mu = fabs(number_at(lo)) <= fabs(number_at(hi)) ? lo : hi;
+  }
+  for (int e = 0; e < c->NE; ++e) f[e] = fermi(c->eps_h[e], mu, c->kBT);
+  double* f_d = c->reswork + c->NE;
+  QCL_CUDA_CHECK(cudaMemcpyAsync(f_d, f.data(), c->NE * sizeof(double), cudaMemcpyHostToDevice, c->st));
+  if ((s = launch_seed_green(sp, c->NE, c->Nk, c->N, c->GR, f_d, c->GL, c->GG, c->st))) return s;
+  // initial candidates (no roundoff verification), straight into the state
+  if ((s = scattering_candidates(c, c->GL, c->GG, c->state, false))) return s;
+  if ((s = embedding_candidates(c, c->state))) return s;
+  QCL_CUDA_CHECK(cudaStreamSynchronize(c->st));
+  QCL_CUDA_CHECK(cudaMemcpy(hst, c->status, sizeof(hst), cudaMemcpyDeviceToHost));
+  if (hst[0]) {
+    set_last_error("seed candidate failed (status %d)", hst[0]);
+    return hst[0];
+  }
+  if (mu_out) *mu_out = mu;
+  c->seeded = true;
+  c->nu = 0;
+  c->pending_commit = false;
+  c->Jprev = NAN;
+  c->pprev.clear();
+  return QCL_OK;
+}
+
+static int run_body(ScbaCtx* c) {
+  std::vector<void*>& st = c->parity == 0 ? c->state : c->cand;
+  std::vector<void*>& cd = c->parity == 0 ? c->cand : c->state;
+  // graphs are captured once every kernel has been launched (and configured) eagerly
+  if (!c->use_graph || c->nu < 1) return iteration_body(c, st, cd);
+  if (!c->graph[c->parity]) {
+    cudaGraph_t g;
+    QCL_CUDA_CHECK(cudaStreamBeginCapture(c->st, cudaStreamCaptureModeThreadLocal));
+    int s = iteration_body(c, st, cd);
+    cudaError_t e = cudaStreamEndCapture(c->st, &g);
+    if (s) {
+      if (e == cudaSuccess) cudaGraphDestroy(g);
+      return s;
+    }
+    if (e != cudaSuccess) return cuda_status(e, "cudaStreamEndCapture");
+    e = cudaGraphInstantiate(&c->graph[c->parity], g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) return cuda_status(e, "cudaGraphInstantiate");
+  }
+  QCL_CUDA_CHECK(cudaGraphLaunch(c->graph[c->parity], c->st));
+  return QCL_OK;
+}
+
+// One SCBA iteration.  Commits the previous iteration's mixing first.
+int scba_step(ScbaCtx* c, qcl_scba_row* row) {
+  if (!c->seeded) {
+    set_last_error("scba_step before scba_seed");
+    return QCL_ARG;
+  }
+  if (c->pending_commit) {
+    c->parity ^= 1;
+    c->pending_commit = false;
+  }
+  int s = run_body(c);
+  if (s) return s;
+  QCL_CUDA_CHECK(cudaStreamSynchronize(c->st));
+  int hst[2];
+  QCL_CUDA_CHECK(cudaMemcpy(hst, c->status, sizeof(hst), cudaMemcpyDeviceToHost));
+  const double* h = c->scal_h;
+  c->nu += 1;
+  memset(row, 0, sizeof(*row));
+  row->nu = c->nu;
+  row->lambda = h[SC_COEF + 2];
+  row->r_lambda = fabs(row->lambda - 1.0);
+  row->number = h[SC_COEF + 3];
+  row->holes = h[SC_COEF + 4];
+  row->occupied_fraction = h[SC_COEF + 0];
+  row->empty_fraction = h[SC_COEF + 1];
+  row->r_D = h[SC_RES + 0];
+  row->r_A = h[SC_RES + 1];
+  row->r_K = h[SC_RES + 2];
+  row->r_PSD = h[SC_RES + 3];
+  row->r_caus = h[SC_RES + 4];
+  double rS = 0;
+  auto rel = [](double num, double den) {
+    return (isfinite(num) && isfinite(den)) ? sqrt(num) / (sqrt(den) + 1e-14) : INFINITY;
+  };
+  for (int k = 0; k < 3; ++k) rS = fmax(rS, rel(h[SC_EMB + 2 * k], h[SC_EMB + 2 * k + 1]));
+  for (int f = 0; f < c->M + 2; ++f)
+    for (int k = 0; k < 3; ++k) {
+      const double v = rel(h[SC_FAM + 2 * (3 * f + k)], h[SC_FAM + 2 * (3 * f + k) + 1]);
+      rS = isfinite(v) ? fmax(rS, v) : INFINITY;
+    }
+  row->r_Sigma = rS;
+  double rr = 0;
+  if (c->verify)
+    for (int i = 0; i < c->M; ++i) rr = fmax(rr, rel(h[SC_ROUND + 2 * i], h[SC_ROUND + 2 * i + 1]));
+  row->r_roundoff = rr;
+  row->Jbar = h[SC_OBS + 0];
+  row->J = row->Jbar * c->J0;
+  for (int a = 0; a < c->N; ++a) c->pops[a] = h[SC_OBS + 2 + a];
+  row->r_J = isnan(c->Jprev) ? INFINITY : fabs(row->J - c->Jprev) / fmax(fmax(fabs(row->J), fabs(c->Jprev)), 1e-12);
+  if (c->pprev.empty()) {
+    row->r_pop = INFINITY;
+  } else {
+    double dn = 0, nn = 0;
+    for (int a = 0; a < c->N; ++a) {
+      dn += (c->pops[a] - c->pprev[a]) * (c->pops[a] - c->pprev[a]);
+      nn += c->pops[a] * c->pops[a];
+    }
+    row->r_pop = sqrt(dn) / (sqrt(nn) + 1e-14);
+  }
+  row->status = hst[0];
+  c->Jprev = row->J;
+  c->pprev = c->pops;
+  c->pending_commit = true;
+  if (hst[0] == QCL_SINGULAR) {
+    // a Dyson failure carries no partial state (production_solver.jl:447-469)
+    c->pending_commit = false;
+    set_last_error("singular Dyson block (linear block index %d)", hst[1]);
+    return QCL_SINGULAR;
+  }
+  if (hst[0] == QCL_DOMAIN) {
+    c->pending_commit = false;
+    set_last_error("paired number normalisation rejected the raw occupation");
+    return QCL_DOMAIN;
+  }
+  const double m[] = {row->r_D, row->r_A, row->r_K, row->r_Sigma, row->r_lambda, row->r_PSD, row->r_caus,
+                      row->r_roundoff, row->J, row->lambda};
+  for (double v : m)
+    if (!isfinite(v)) {
+      row->status = QCL_NONFINITE;
+      c->pending_commit = false;
+      return QCL_OK;  // reported as a row status (:nonfinite_metrics), not an error
+    }
+  return QCL_OK;
+}
+
+int scba_populations(ScbaCtx* c, double* out) {
+  for (int a = 0; a < c->N; ++a) out[a] = c->pops[a];
+  return QCL_OK;
+}
+
+// Copies a state field to host memory (checkpoint).  which: 0..2 = GR, G<, G>
+// of the last iteration; 3 + 3 f + k = family f component k of the current
+// (unmixed) state, f in [0, M) mechanisms, M plus, M + 1 minus.
+int scba_download(ScbaCtx* c, int which, void* host) {
+  const void* src = nullptr;
+  if (which == 0) src = c->GR;
+  else if (which == 1) src = c->GL;
+  else if (which == 2) src = c->GG;
+  else {
+    const int idx = which - 3;
+    if (idx < 0 || idx >= 3 * (c->M + 2)) {
+      set_last_error("download: field index %d out of range", which);
+      return QCL_ARG;
+    }
+    std::vector<void*>& st = c->parity == 0 ? c->state : c->cand;
+    src = st[idx];
+  }
+  QCL_CUDA_CHECK(cudaStreamSynchronize(c->st));
+  QCL_CUDA_CHECK(cudaMemcpy(host, src, c->fbytes, cudaMemcpyDeviceToHost));
+  return QCL_OK;
+}
+
+// Replaces a state family component (warm start / resume, production_solver.jl:216-429).
+int scba_upload(ScbaCtx* c, int which, const void* host) {
+  const int idx = which - 3;
+  if (idx < 0 || idx >= 3 * (c->M + 2)) {
+    set_last_error("upload: field index %d out of range", which);
+    return QCL_ARG;
+  }
+  if (c->pending_commit) {
+    c->parity ^= 1;
+    c->pending_commit = false;
+  }
+  std::vector<void*>& st = c->parity == 0 ? c->state : c->cand;
+  QCL_CUDA_CHECK(cudaStreamSynchronize(c->st));
+  QCL_CUDA_CHECK(cudaMemcpy(st[idx], host, c->fbytes, cudaMemcpyHostToDevice));
+  c->seeded = true;
+  return QCL_OK;
+}
+
+int scba_set_graph(ScbaCtx* c, int enable) {
+  c->use_graph = enable != 0;
+  return QCL_OK;
+}
+
+cudaStream_t scba_stream(ScbaCtx* c) { return c->st; }
+
+}  // namespace qcl

@@ -1,0 +1,328 @@
+"""Host-side SCBA problem description and seeded synthetic structures.
+
+The reference assembles an ``NEGFProblem`` from a layer stack (grids, basis,
+projected Hamiltonian, kernels; ``numerics/reference/{grids,basis,kernels}.jl``
+and ``numerics/optimized/kernels.jl:790-836``).  Those builders are one-time
+host set-up and stay outside the accelerated path; here a problem is the
+finished set of inputs the SCBA fixed-point map consumes:
+
+* grids ``eps, wE`` (``grids.jl:20-27``: uniform energies, trapezoid weights)
+  and ``wk`` (``grids.jl:29-37``: annulus weights ``(b_{m+1}^2-b_m^2)/(4 pi)``);
+* the projected Hamiltonians ``h[m, a, b]`` (``basis.jl:288-331``);
+* the neighbour couplings ``T+`` and ``T- = T+^H`` (``basis.jl:56-57``);
+* the kernel operators per mechanism (the factorised forms built by
+  ``production_cache.jl:387-448``);
+* the scalars ``g_s``, the target sheet density ``N_D`` (solver units),
+  ``E^p = F L_p`` and ``hbar omega_LO`` (``scaling.jl:95-110``).
+
+All arrays use the reference's Julia layout: numpy arrays in Fortran order
+with shape ``(N_E, N_k, N_b, N_b)`` for fields, ``(N_k, N_b, N_b)`` for ``h``.
+
+The structures below are synthetic and seeded: they have the shapes, sizes
+and value ranges of the workloads they stand for, not the reference's
+converged physics of a particular device.
+"""
+from __future__ import annotations
+
+import dataclasses
+import math
+from typing import List, Optional
+
+import numpy as np
+
+# Solver units (scaling.jl:10-24): E0 = 0.1 eV, L0 = 10 nm, m_ref = 0.067 m0.
+E0_EV = 0.1
+L0_NM = 10.0
+HBAR2_OVER_2M0_EV_NM2 = 0.0380998212  # hbar^2 / (2 m0) in eV nm^2
+KB_EV = 8.617333262e-5
+E_CHARGE = 1.602176634e-19
+HBAR_EV_S = 6.582119569e-16
+# J0 = e E0 / (hbar L0^2) in A/m^2 (scaling.jl:22)
+J0_A_M2 = E_CHARGE * E0_EV / (HBAR_EV_S * (L0_NM * 1e-9) ** 2)
+
+MECHANISM_ORDER = ("LO", "acoustic", "impurity", "IFR", "alloy")
+
+
+def fortran_zeros(shape, dtype=np.complex128):
+    return np.zeros(shape, dtype=dtype, order="F")
+
+
+@dataclasses.dataclass
+class Mechanism:
+    """One enabled scattering mechanism in its factorised operator form.
+
+    kind:
+      * ``"momentum_independent"`` -- ``block`` is ``K[1,1,:,:,:,:]`` in
+        ``(a,c,d,b)`` order (``production_cache.jl:394-398``);
+      * ``"dense"`` -- ``matrix`` has rows ``(m,a,b)`` and columns
+        ``(m',c,d)`` (``production_cache.jl:400-405``);
+      * ``"ifr"`` -- ``left (Nb^2,J)``, ``right (J,Nb^2)``, ``radial (Nk,Nk)``
+        (``production_cache.jl:414-448``).
+    ``q`` is the kernel scale ``q^K`` (``kernels.jl:388-405``).
+    """
+
+    name: str
+    kind: str
+    q: float
+    block: Optional[np.ndarray] = None
+    matrix: Optional[np.ndarray] = None
+    left: Optional[np.ndarray] = None
+    right: Optional[np.ndarray] = None
+    radial: Optional[np.ndarray] = None
+
+    def literal_kernel(self, Nk: int, Nb: int) -> np.ndarray:
+        """The six-index tensor K[m,m',a,c,d,b] this operator represents."""
+        K = np.zeros((Nk, Nk, Nb, Nb, Nb, Nb), dtype=np.complex128, order="F")
+        if self.kind == "momentum_independent":
+            for m in range(Nk):
+                for mp in range(Nk):
+                    K[m, mp] = self.block
+        elif self.kind == "dense":
+            # rows (m,a,b), cols (m',c,d), first index fastest
+            M = self.matrix.reshape((Nk, Nb, Nb, Nk, Nb, Nb), order="F")
+            # M[m,a,b,m',c,d] -> K[m,m',a,c,d,b]
+            K[...] = np.transpose(M, (0, 3, 1, 4, 5, 2))
+        elif self.kind == "ifr":
+            J = self.left.shape[1]
+            L = self.left.reshape((Nb, Nb, J), order="F")  # [a,b,j]
+            R = self.right.reshape((J, Nb, Nb), order="F")  # [j,c,d]
+            blk = np.einsum("abj,jcd->acdb", L, R)
+            for m in range(Nk):
+                for mp in range(Nk):
+                    K[m, mp] = self.radial[m, mp] * blk
+        else:
+            raise ValueError(self.kind)
+        return K
+
+
+@dataclasses.dataclass
+class SCBAProblem:
+    NE: int
+    Nk: int
+    Nb: int
+    eps: np.ndarray
+    wE: np.ndarray
+    wk: np.ndarray
+    h: np.ndarray  # (Nk, Nb, Nb) F-order complex
+    Tplus: np.ndarray  # (Nb, Nb)
+    Tminus: np.ndarray
+    Ep: float
+    hw_LO: float
+    N_LO: float
+    gs: int
+    target: float
+    kBT: float
+    eta_seed: float
+    alpha: float
+    mechanisms: List[Mechanism]
+    J0: float = J0_A_M2
+    name: str = "problem"
+
+    @property
+    def shape(self):
+        return (self.NE, self.Nk, self.Nb, self.Nb)
+
+    def field_bytes(self, itemsize=16):
+        return self.NE * self.Nk * self.Nb * self.Nb * itemsize
+
+
+def energy_grid(emin: float, emax: float, NE: int):
+    """Uniform grid and trapezoid weights (grids.jl:20-27)."""
+    eps = np.linspace(emin, emax, NE)
+    de = (emax - emin) / (NE - 1)
+    wE = np.full(NE, de)
+    wE[[0, -1]] /= 2
+    return eps, wE
+
+
+def momentum_grid(kmax: float, Nk: int):
+    """Uniform radial grid and annulus weights (grids.jl:29-37)."""
+    kappa = np.linspace(0.0, kmax, Nk)
+    bnd = np.zeros(Nk + 1)
+    for m in range(1, Nk):
+        bnd[m] = 0.5 * (kappa[m - 1] + kappa[m])
+    bnd[-1] = kmax
+    wk = (bnd[1:] ** 2 - bnd[:-1] ** 2) / (4 * math.pi)
+    return kappa, wk
+
+
+def _kinetic_coefficient(mass_ratio=0.067):
+    """hbar^2/(2 m*) in solver units (E0 L0^2)."""
+    return HBAR2_OVER_2M0_EV_NM2 / mass_ratio / (E0_EV * L0_NM ** 2)
+
+
+def _supercell(rng, periods, states, level_ev, Ep, coupling_ev, mass_spread=0.03):
+    """Onsite block h0 (solver units) of a `periods` x `states` supercell,
+    the neighbour coupling T+ and a weak mass-mixing matrix."""
+    Nb = periods * states
+    h0 = np.zeros((Nb, Nb), dtype=np.complex128)
+    for p in range(periods):
+        for s in range(states):
+            h0[p * states + s, p * states + s] = level_ev[s] / E0_EV - p * Ep
+    c = coupling_ev / E0_EV
+    for p in range(periods - 1):
+        blk = c * (rng.standard_normal((states, states)) + 1j * rng.standard_normal((states, states))) / math.sqrt(2)
+        h0[p * states:(p + 1) * states, (p + 1) * states:(p + 2) * states] = blk
+        h0[(p + 1) * states:(p + 2) * states, p * states:(p + 1) * states] = blk.conj().T
+    intra = 0.2 * c * (rng.standard_normal((Nb, Nb)) + 1j * rng.standard_normal((Nb, Nb)))
+    intra = np.triu(intra, 1)
+    h0 += intra + intra.conj().T
+    Tplus = np.zeros((Nb, Nb), dtype=np.complex128)
+    blk = c * (rng.standard_normal((states, states)) + 1j * rng.standard_normal((states, states))) / math.sqrt(2)
+    Tplus[(periods - 1) * states:, :states] = blk
+    mix = mass_spread * rng.standard_normal((Nb, Nb))
+    mix = 0.5 * (mix + mix.T)
+    return h0, Tplus, mix
+
+
+def _localized_states(rng, Nb, Nz=96, length=3.0):
+    """Real, normalised, localised synthetic basis functions chi[g, a] on a
+    cell-centred grid (the role of basis.chi, basis.jl:15-110)."""
+    dx = length / Nz
+    x = (np.arange(Nz) + 0.5) * dx
+    centres = np.linspace(0.1 * length, 0.9 * length, Nb) + 0.02 * rng.standard_normal(Nb)
+    widths = 0.12 * length / max(Nb / 4, 1) * (1 + 0.2 * rng.random(Nb))
+    chi = np.exp(-0.5 * ((x[:, None] - centres[None, :]) / widths[None, :]) ** 2)
+    chi *= 1 + 0.3 * np.sin(3 * x[:, None] / length * math.pi * (1 + np.arange(Nb)[None, :] % 3))
+    chi /= np.sqrt((chi ** 2).sum(axis=0) * dx)[None, :]
+    return x, np.full(Nz, dx), chi
+
+
+def acoustic_block(chi, wx, prefactor):
+    """Deformation-potential kernel block K[a,c,d,b] = P sum_g w chi_a chi_c
+    chi_d chi_b (acoustic_kernel, numerics/reference/kernels.jl:246-283, real
+    basis functions) in (a,c,d,b) order."""
+    K = prefactor * np.einsum("g,ga,gc,gd,gb->acdb", wx, chi, chi, chi, chi)
+    return np.asfortranarray(K.astype(np.complex128))
+
+
+def tutorial_problem(seed: int = 1, NE: int = 400, Nk: int = 16, alpha: float = 0.3) -> SCBAProblem:
+    """Plain-FP64 tutorial-scale SCBA structure: 3 periods x 4 states
+    (N_b = 12), N_E = 400 energies over 0.3 eV, N_k = 16 in-plane momenta on
+    0-60 meV kinetic energy, acoustic phonons only, T = 50 K, 50 mV/period,
+    linear mixing 0.3."""
+    rng = np.random.default_rng(seed)
+    periods, states = 3, 4
+    Nb = periods * states
+    Ep = 0.050 / E0_EV
+    eps, wE = energy_grid(-0.13 / E0_EV, 0.17 / E0_EV, NE)
+    Cbar = _kinetic_coefficient()
+    kmax = math.sqrt(0.060 / E0_EV / Cbar)
+    kappa, wk = momentum_grid(kmax, Nk)
+    h0, Tplus, mix = _supercell(rng, periods, states, [0.010, 0.045, 0.085, 0.120], Ep, 0.004)
+    h = np.zeros((Nk, Nb, Nb), dtype=np.complex128, order="F")
+    for m in range(Nk):
+        h[m] = h0 + Cbar * kappa[m] ** 2 * (np.eye(Nb) + mix)
+    x, wx, chi = _localized_states(rng, Nb)
+    # Xi^2 kB T / (rho v_s^2) / (L0 K0) with Xi = 7 eV, T = 50 K, GaAs rho, v_s
+    # (acoustic_kernel prefactor, kernels.jl:262-266; presets.jl:76-78).
+    Xi = 7.0 * E_CHARGE
+    kBT_J = 1.380649e-23 * 50.0
+    pref = Xi ** 2 * kBT_J / (5317.0 * 5220.0 ** 2) / (L0_NM * 1e-9)
+    K0 = (E0_EV * E_CHARGE) ** 2 * (L0_NM * 1e-9) ** 2
+    K = acoustic_block(chi, wx, pref / K0)
+    q = float(np.max(np.abs(K)))
+    mech = Mechanism("acoustic", "momentum_independent", q, block=np.asfortranarray(K / q))
+    # 4.5e14 m^-2 sheet doping (presets.jl:62) in solver units (x L0^2)
+    target = 4.5e14 * (L0_NM * 1e-9) ** 2
+    kBT = KB_EV * 50.0 / E0_EV
+    hw_LO = 0.0367 / E0_EV
+    return SCBAProblem(
+        NE=NE, Nk=Nk, Nb=Nb, eps=eps, wE=wE, wk=wk, h=h, Tplus=np.asfortranarray(Tplus),
+        Tminus=np.asfortranarray(Tplus.conj().T), Ep=Ep, hw_LO=hw_LO,
+        N_LO=1.0 / math.expm1(0.0367 / (KB_EV * 50.0)), gs=2, target=target, kBT=kBT,
+        eta_seed=0.0005 / E0_EV, alpha=alpha, mechanisms=[mech], name="tutorial_N12",
+    )
+
+
+def small_problem(seed=3, NE=33, Nk=3, Nb=4, mechanisms=("acoustic",), alpha=0.3,
+                  strength=0.05) -> SCBAProblem:
+    """A tiny structure for exhaustive oracle/GPU comparisons of every
+    mechanism kind (LO with its shifts, dense impurity, separable IFR,
+    momentum-independent acoustic and alloy)."""
+    rng = np.random.default_rng(seed)
+    states = Nb if Nb < 4 else Nb // 2
+    periods = max(Nb // states, 1)
+    Ep = 0.3
+    eps, wE = energy_grid(-1.0, 2.0, NE)
+    kappa, wk = momentum_grid(2.0, Nk)
+    Cbar = 0.06
+    h0 = np.diag(np.linspace(-0.3, 1.2, Nb)).astype(np.complex128)
+    cpl = 0.05 * (rng.standard_normal((Nb, Nb)) + 1j * rng.standard_normal((Nb, Nb)))
+    cpl = np.triu(cpl, 1)
+    h0 += cpl + cpl.conj().T
+    h = np.zeros((Nk, Nb, Nb), dtype=np.complex128, order="F")
+    for m in range(Nk):
+        h[m] = h0 + Cbar * kappa[m] ** 2 * np.eye(Nb)
+    Tplus = 0.05 * (rng.standard_normal((Nb, Nb)) + 1j * rng.standard_normal((Nb, Nb)))
+    x, wx, chi = _localized_states(rng, Nb, Nz=48, length=2.0)
+    mechs = []
+    for name in MECHANISM_ORDER:
+        if name not in mechanisms:
+            continue
+        if name in ("acoustic", "alloy"):
+            K = acoustic_block(chi, wx, 1.0)
+            q = float(np.max(np.abs(K)))
+            mechs.append(Mechanism(name, "momentum_independent", strength * (1.3 if name == "alloy" else 1.0),
+                                   block=np.asfortranarray(K / q)))
+        elif name in ("LO", "impurity"):
+            # sum_h R_h(m,m') F_h (x) F_h^* -- the LO/impurity covariance form
+            # (kernels.jl:321-356) with synthetic form factors.
+            Nq = 5
+            F = rng.standard_normal((Nq, Nb, Nb)) + 1j * rng.standard_normal((Nq, Nb, Nb))
+            F = 0.5 * (F + np.conj(np.transpose(F, (0, 2, 1))))
+            R = np.empty((Nq, Nk, Nk))
+            for hq in range(Nq):
+                R[hq] = 1.0 / (1.0 + (kappa[:, None] - kappa[None, :]) ** 2 + hq)
+            K = np.einsum("hmn,hac,hbd->mnacdb", R, F, np.conj(F))
+            q = float(np.max(np.abs(K)))
+            K = K / q
+            # rows (m,a,b), cols (m',c,d)
+            M = np.transpose(K, (0, 2, 5, 1, 3, 4)).reshape((Nk * Nb * Nb, Nk * Nb * Nb), order="F")
+            mechs.append(Mechanism(name, "dense", strength * (0.8 if name == "LO" else 0.5),
+                                   matrix=np.asfortranarray(M.astype(np.complex128))))
+        elif name == "IFR":
+            J = 3
+            v = rng.standard_normal((Nb, J)) + 0.3j * rng.standard_normal((Nb, J))
+            left = np.zeros((Nb * Nb, J), dtype=np.complex128)
+            right = np.zeros((J, Nb * Nb), dtype=np.complex128)
+            for j in range(J):
+                for b in range(Nb):
+                    for a in range(Nb):
+                        val = v[a, j] * np.conj(v[b, j])
+                        left[a + Nb * b, j] = val
+                        right[j, a + Nb * b] = np.conj(val)
+            radial = np.exp(-0.5 * (kappa[:, None] - kappa[None, :]) ** 2).astype(np.complex128)
+            mech = Mechanism(name, "ifr", 1.0, left=np.asfortranarray(left), right=np.asfortranarray(right),
+                             radial=np.asfortranarray(radial))
+            K = mech.literal_kernel(Nk, Nb)
+            q = float(np.max(np.abs(K)))
+            mech.left = np.asfortranarray(left / q)
+            mech.q = strength * 0.6
+            mechs.append(mech)
+    return SCBAProblem(
+        NE=NE, Nk=Nk, Nb=Nb, eps=eps, wE=wE, wk=wk, h=h, Tplus=np.asfortranarray(Tplus),
+        Tminus=np.asfortranarray(Tplus.conj().T), Ep=Ep, hw_LO=0.367, N_LO=0.25, gs=2,
+        target=0.05, kBT=0.2, eta_seed=0.02, alpha=alpha, mechanisms=mechs, name="small",
+    )
+
+
+def operator_batch_hamiltonian(N: int, Nk: int, seed: int = 7):
+    """Hermitian block-tridiagonal h per k (blocks of 8 states, diagonal
+    subband energies U(0, 250 meV), inter-period couplings N(0, 2 meV)) plus
+    a parabolic in-plane dispersion; solver units."""
+    rng = np.random.default_rng(seed)
+    blocks = N // 8
+    h0 = np.zeros((N, N), dtype=np.complex128)
+    h0[np.arange(N), np.arange(N)] = rng.uniform(0.0, 0.250, N) / E0_EV
+    for p in range(blocks - 1):
+        blk = (rng.standard_normal((8, 8)) + 1j * rng.standard_normal((8, 8))) * (0.002 / E0_EV) / math.sqrt(2)
+        h0[p * 8:(p + 1) * 8, (p + 1) * 8:(p + 2) * 8] = blk
+        h0[(p + 1) * 8:(p + 2) * 8, p * 8:(p + 1) * 8] = blk.conj().T
+    Cbar = _kinetic_coefficient()
+    kappa, wk = momentum_grid(math.sqrt(0.060 / E0_EV / Cbar), Nk)
+    h = np.zeros((Nk, N, N), dtype=np.complex128, order="F")
+    for m in range(Nk):
+        h[m] = h0 + Cbar * kappa[m] ** 2 * np.eye(N)
+    eps, wE = energy_grid(-0.05 / E0_EV, 0.35 / E0_EV, 4096)
+    return h, wk, kappa

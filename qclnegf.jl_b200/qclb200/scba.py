@@ -1,0 +1,133 @@
+"""The SCBA inner loop at fixed Hartree potential on the GPU.
+
+Mirror of ``solve_scba_production`` (numerics/optimized/production_solver.jl:
+21-846) over the C ABI ``qcl_scba_*``: the production cache and all fields
+live in device memory; each iteration returns one ``SCBAIteration``-like row
+(domain/types.jl:908).  The termination policy stays on the host, as in the
+reference (``scba_iteration_decision``, domain/research_policy.jl:166); the
+default used here stops when r_Sigma falls below a tolerance.
+"""
+from __future__ import annotations
+
+import ctypes
+import math
+
+import numpy as np
+
+from . import _lib
+from ._lib import check, lib
+from .operators import _CDT, _prec, mechanism_struct
+
+
+class _Problem(ctypes.Structure):
+    _fields_ = [("NE", ctypes.c_int), ("Nk", ctypes.c_int), ("Nb", ctypes.c_int),
+                ("eps", ctypes.c_void_p), ("wE", ctypes.c_void_p), ("wk", ctypes.c_void_p),
+                ("h", ctypes.c_void_p), ("Tplus", ctypes.c_void_p), ("Tminus", ctypes.c_void_p),
+                ("Ep", ctypes.c_double), ("hw_LO", ctypes.c_double), ("N_LO", ctypes.c_double),
+                ("gs", ctypes.c_int), ("target", ctypes.c_double), ("eta_seed", ctypes.c_double),
+                ("kBT", ctypes.c_double), ("alpha", ctypes.c_double), ("J0", ctypes.c_double),
+                ("precision", ctypes.c_int), ("verify_roundoff", ctypes.c_int), ("nmech", ctypes.c_int)]
+
+
+class Row(ctypes.Structure):
+    _fields_ = [("nu", ctypes.c_int), ("status", ctypes.c_int)] + [
+        (n, ctypes.c_double) for n in ("r_D", "r_A", "r_K", "r_Sigma", "r_lambda", "lambda_", "r_PSD", "r_caus",
+                                       "r_roundoff", "r_J", "r_pop", "J", "Jbar", "number", "holes",
+                                       "occupied_fraction", "empty_fraction")]
+
+    def as_dict(self):
+        d = {n: getattr(self, n) for n, _ in self._fields_}
+        d["lam"] = d.pop("lambda_")
+        return d
+
+
+def _c(a, dtype=np.complex128):
+    return np.asfortranarray(np.asarray(a, dtype=dtype))
+
+
+class ProductionSCBA:
+    """A device-resident SCBA solve for one problem (one context = one
+    ``ProductionCache`` + state; calls on one context must be serialised,
+    like the reference's plans, fft_parallel.jl:16-17)."""
+
+    def __init__(self, problem, precision="c128", verify_roundoff=True, use_graph=False):
+        self.problem = problem
+        self.precision = _prec(precision)
+        pr = problem
+        self._keep = [np.ascontiguousarray(pr.eps, dtype=np.float64), np.ascontiguousarray(pr.wE, dtype=np.float64),
+                      np.ascontiguousarray(pr.wk, dtype=np.float64), _c(pr.h), _c(pr.Tplus), _c(pr.Tminus)]
+        ptr = [ctypes.c_void_p(a.ctypes.data) for a in self._keep]
+        self._p = _Problem(pr.NE, pr.Nk, pr.Nb, *ptr, float(pr.Ep), float(pr.hw_LO), float(pr.N_LO), int(pr.gs),
+                           float(pr.target), float(pr.eta_seed), float(pr.kBT), float(pr.alpha), float(pr.J0),
+                           self.precision, 1 if verify_roundoff else 0, len(pr.mechanisms))
+        self._mechs = [mechanism_struct(m) for m in pr.mechanisms]
+        arr = (type(self._mechs[0]) * max(len(self._mechs), 1))(*self._mechs) if self._mechs else None
+        self._marr = arr
+        h = ctypes.c_void_p()
+        check(lib().qcl_scba_create(ctypes.byref(self._p), arr, ctypes.byref(h)))
+        self._h = h
+        if use_graph:
+            check(lib().qcl_scba_use_graph(self._h, 1))
+        self.mu = None
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().qcl_scba_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def seed(self):
+        mu = ctypes.c_double()
+        check(lib().qcl_scba_seed(self._h, ctypes.byref(mu)))
+        self.mu = mu.value
+        return self.mu
+
+    def step(self):
+        r = Row()
+        check(lib().qcl_scba_step(self._h, ctypes.byref(r)))
+        d = r.as_dict()
+        d["populations"] = self.populations()
+        return d
+
+    def run(self, iterations, tol_sigma=-1.0):
+        rows = []
+        for _ in range(iterations):
+            d = self.step()
+            rows.append(d)
+            if d["status"] != 0 or d["r_Sigma"] <= tol_sigma:
+                break
+        return rows
+
+    def populations(self):
+        out = np.zeros(self.problem.Nb)
+        check(lib().qcl_scba_populations(self._h, ctypes.c_void_p(out.ctypes.data)))
+        return out
+
+    def download(self, which):
+        out = np.zeros(self.problem.shape, dtype=_CDT[self.precision], order="F")
+        check(lib().qcl_scba_download(self._h, int(which), ctypes.c_void_p(out.ctypes.data)))
+        return out
+
+    def upload(self, which, array):
+        a = _c(array, _CDT[self.precision])
+        check(lib().qcl_scba_upload(self._h, int(which), ctypes.c_void_p(a.ctypes.data)))
+
+    def green(self):
+        return dict(GR=self.download(0), GL=self.download(1), GG=self.download(2))
+
+    def family(self, f):
+        """(SigmaR, Sigma<, Sigma>) of family f: 0..M-1 mechanisms, M plus, M+1 minus."""
+        return tuple(self.download(3 + 3 * f + c) for c in range(3))
+
+
+def solve_scba_production(problem, iterations, *, precision="c128", verify_roundoff=True, tol_sigma=-1.0,
+                          use_graph=False):
+    """Seed + up to `iterations` SCBA steps; returns (history, solver)."""
+    s = ProductionSCBA(problem, precision=precision, verify_roundoff=verify_roundoff, use_graph=use_graph)
+    s.seed()
+    return s.run(iterations, tol_sigma), s

@@ -1,0 +1,272 @@
+"""GPU parity of the operator-level C ABI against the FP64 oracle.
+
+Tolerances: complex128 paths must agree with the oracle within the
+reference's own operator-equivalence tolerances (relative, Julia isapprox
+sense: 1e-12 for Dyson/Keldysh products -- the reference pins its inverse at
+5e-13 against `inv`; 2e-13 for the Hilbert transform).  complex64 / mixed
+paths are checked at 2e-5 (Dyson, FP32 products) and 1e-5 (FFT in FP32).
+"""
+import math
+
+import numpy as np
+import pytest
+
+from helpers import approx_err, dyson_inputs
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("N", [1, 3, 8, 12, 16, 20, 24, 32, 40, 48])
+def test_dyson_keldysh_c128_matches_oracle(gpu_ops, orc, N):
+    NE, Nk = 37, 3
+    eps, h, SR, SL, SG = dyson_inputs(100 + N, NE, Nk, N)
+    GR, GL, GG, scale, trL, trG = gpu_ops.dyson_keldysh(eps, h, SR, SL, SG, precision="c128", return_traces=True)
+    oGR, _, oscale, _ = orc.retarded_green(eps, h, SR)
+    oGL = orc.keldysh_green(oGR, SL)
+    oGG = orc.keldysh_green(oGR, SG)
+    assert approx_err(GR, oGR) < 1e-12
+    assert approx_err(GL, oGL) < 1e-12
+    assert approx_err(GG, oGG) < 1e-12
+    np.testing.assert_allclose(scale, oscale, rtol=1e-14)
+    otr = np.trace(oGL, axis1=2, axis2=3)
+    assert approx_err(trL, otr) < 1e-12
+    assert approx_err(trG, np.trace(oGG, axis1=2, axis2=3)) < 1e-12
+
+
+@pytest.mark.parametrize("precision", ["c64", "mixed"])
+@pytest.mark.parametrize("N", [4, 12, 24, 48])
+def test_dyson_keldysh_reduced_precision(gpu_ops, orc, precision, N):
+    NE, Nk = 33, 2
+    eps, h, SR, SL, SG = dyson_inputs(200 + N, NE, Nk, N)
+    GR, GL, GG, _ = gpu_ops.dyson_keldysh(eps, h, SR, SL, SG, precision=precision)
+    oGR = orc.retarded_green(eps, h, SR)[0]
+    tol = 2e-5 if precision == "mixed" else 5e-5
+    assert GR.dtype == np.complex64
+    assert approx_err(GR, oGR) < tol
+    assert approx_err(GL, orc.keldysh_green(oGR, SL)) < tol
+    assert approx_err(GG, orc.keldysh_green(oGR, SG)) < tol
+
+
+def test_dyson_scalar_lorentzian_on_gpu(gpu_ops):
+    # test/physics/scalar_dyson_and_spectral_identity.jl:4-21 through the C ABI
+    eps = np.linspace(-1.0, 1.0, 2001)
+    Estar, Gam = 0.17, 0.08
+    h = np.full((1, 1, 1), Estar, dtype=complex)
+    SR = np.full((len(eps), 1, 1, 1), -0.5j * Gam, order="F")
+    GR = gpu_ops.retarded_green(eps, h, SR)
+    A = (1j * (GR - np.conj(GR)))[:, 0, 0, 0].real
+    exact = Gam / ((eps - Estar) ** 2 + (Gam / 2) ** 2)
+    assert np.linalg.norm(A - exact) <= 2e-13 * np.linalg.norm(exact)
+
+
+def test_dyson_singular_block_raises(gpu_ops):
+    from qclb200 import SingularException
+
+    eps = np.linspace(0, 1, 5)
+    h = np.zeros((1, 3, 3), dtype=complex)
+    SR = np.zeros((5, 1, 3, 3), dtype=complex, order="F")
+    SR[:, 0] = np.diag([0.0, 0.0, 0.0])
+    # eps[0] = 0 with h = 0 and SR = 0 gives D = 0: scale 0 -> SingularException(0)
+    with pytest.raises(SingularException):
+        gpu_ops.retarded_green(eps, h, SR)
+    # a rank-deficient (but non-zero) block
+    SR2 = np.zeros((5, 1, 3, 3), dtype=complex, order="F")
+    for e in range(5):
+        SR2[e, 0] = eps[e] * np.eye(3) - np.ones((3, 3))
+    with pytest.raises(SingularException):
+        gpu_ops.retarded_green(eps, h, SR2)
+
+
+@pytest.mark.parametrize("NE", [37, 64, 400, 1000, 2048, 4096])
+def test_fft_hilbert_c128_matches_direct_pv(gpu_ops, orc, NE):
+    rng = np.random.default_rng(NE)
+    ncols = 6
+    eps = np.linspace(-1.3, 0.9, NE)
+    w = np.full(NE, eps[1] - eps[0])
+    w[[0, -1]] /= 2
+    G = np.asfortranarray(rng.standard_normal((NE, ncols)) + 1j * rng.standard_normal((NE, ncols)))
+    Lam, r = gpu_ops.fft_hilbert_transform(G, eps, w, return_roundoff=True)
+    direct = orc.direct_hilbert(G, eps, w)
+    assert approx_err(Lam, direct) < 2e-13
+    assert approx_err(Lam, orc.fft_hilbert(G, eps, w)) < 2e-13
+    assert math.isfinite(r) and r < 1e-12
+    # roundoff agrees in magnitude with the oracle's 2L rerun
+    _, ro = orc.fft_hilbert(G, eps, w, return_roundoff=True)
+    assert r < 100 * ro + 1e-15
+
+
+@pytest.mark.parametrize("NE", [400, 4096])
+def test_fft_hilbert_c64(gpu_ops, orc, NE):
+    rng = np.random.default_rng(7)
+    eps = np.linspace(-1.3, 0.9, NE)
+    w = np.full(NE, eps[1] - eps[0])
+    w[[0, -1]] /= 2
+    G = np.asfortranarray(rng.standard_normal((NE, 4)) + 1j * rng.standard_normal((NE, 4)))
+    Lam, r = gpu_ops.fft_hilbert_transform(G, eps, w, precision="c64", return_roundoff=True)
+    assert Lam.dtype == np.complex64
+    assert approx_err(Lam, orc.direct_hilbert(G, eps, w)) < 1e-5
+    assert r < 1e-5
+
+
+def test_retarded_self_energy_fft_matches_oracle(gpu_ops, orc):
+    rng = np.random.default_rng(0xFF71)
+    NE, Nk, Nb = 37, 2, 2
+    eps = np.linspace(-1.3, 0.9, NE)
+    w = np.full(NE, eps[1] - eps[0])
+    w[[0, -1]] /= 2
+    SL = np.asfortranarray(rng.standard_normal((NE, Nk, Nb, Nb)) + 1j * rng.standard_normal((NE, Nk, Nb, Nb)))
+    SG = np.asfortranarray(rng.standard_normal((NE, Nk, Nb, Nb)) + 1j * rng.standard_normal((NE, Nk, Nb, Nb)))
+    SR, Gam, r = gpu_ops.retarded_self_energy_fft(SL, SG, eps, w, return_roundoff=True)
+    oSR, oGam = orc.retarded_self_energy(SL, SG, eps, w, method="direct")
+    assert np.array_equal(Gam, oGam)
+    assert approx_err(SR, oSR) < 2e-13
+    assert r < 1e-12
+
+
+# ---------------------------------------------------------------------------
+# shifts, contractions, embedding, residuals, observables
+# ---------------------------------------------------------------------------
+
+def _rand_field(rng, shape):
+    return np.asfortranarray(rng.standard_normal(shape) + 1j * rng.standard_normal(shape))
+
+
+@pytest.mark.parametrize("delta", [0.367, -0.367, 0.3, 0.0, 3.5, 0.075])
+def test_energy_shift_matches_oracle(gpu_ops, orc, delta):
+    rng = np.random.default_rng(11)
+    eps = np.linspace(-1.0, 2.0, 41)
+    X = _rand_field(rng, (41, 3, 2, 2))
+    Y = gpu_ops.apply_energy_shift(X, eps, delta)
+    assert approx_err(Y, orc.ShiftPlan(eps, delta).apply(X)) < 5e-15
+
+
+def test_energy_shift_rejects_aliasing(gpu_ops):
+    import ctypes
+    from qclb200 import _lib
+
+    X = np.zeros((8, 1), dtype=complex, order="F")
+    eps = np.linspace(0, 1, 8)
+    p = ctypes.c_void_p(X.ctypes.data)
+    st = _lib.lib().qcl_apply_energy_shift(0, 8, 1, ctypes.c_void_p(eps.ctypes.data), 0.1, p, p)
+    assert st == _lib.QCL_ARG
+
+
+@pytest.mark.parametrize("kind", ["momentum_independent", "dense", "ifr"])
+@pytest.mark.parametrize("beta", [0.0, 1.0])
+def test_static_contraction_matches_literal_oracle(gpu_ops, orc, kind, beta):
+    from qclb200.problem import small_problem
+
+    names = {"momentum_independent": ("acoustic",), "dense": ("impurity",), "ifr": ("IFR",)}[kind]
+    pr = small_problem(NE=37, Nk=4, Nb=4, mechanisms=names)
+    mech = pr.mechanisms[0]
+    rng = np.random.default_rng(3)
+    G = _rand_field(rng, pr.shape)
+    S0 = _rand_field(rng, pr.shape)
+    got = gpu_ops.production_static_contraction(mech, G, pr.wk, alpha=1.7, beta=beta, S=S0)
+    lit = orc.contraction_literal(mech.literal_kernel(pr.Nk, pr.Nb), G, pr.wk, 1.7 * mech.q) + beta * S0
+    assert approx_err(got, lit) < 1e-13
+    got32 = gpu_ops.production_static_contraction(mech, G, pr.wk, alpha=1.7, beta=beta, S=S0, precision="c64")
+    assert approx_err(got32, lit) < 1e-5
+
+
+@pytest.mark.parametrize("Nb", [3, 12, 24])
+def test_embedding_component_matches_oracle(gpu_ops, orc, Nb):
+    rng = np.random.default_rng(Nb)
+    NE, Nk = 45, 3
+    eps = np.linspace(-1.0, 2.0, NE)
+    T = rng.standard_normal((Nb, Nb)) + 1j * rng.standard_normal((Nb, Nb))
+    G = _rand_field(rng, (NE, Nk, Nb, Nb))
+    for delta in (0.5, -0.5, 0.0):
+        got = gpu_ops.embedding_component(T, G, eps, delta)
+        ref = orc.embedding_component(T, G, orc.ShiftPlan(eps, delta))
+        assert approx_err(got, ref) < 1e-13
+
+
+def _consistent_state(orc, seed, NE, Nk, Nb):
+    from helpers import dyson_inputs
+
+    eps, h, SR, SL, SG = dyson_inputs(seed, NE, Nk, Nb)
+    GR = orc.retarded_green(eps, h, SR)[0]
+    GL = orc.keldysh_green(GR, SL)
+    GG = orc.keldysh_green(GR, SG)
+    return eps, h, GR, GL, GG, (SR, SL, SG)
+
+
+@pytest.mark.parametrize("Nb", [4, 12, 24])
+def test_residual_suite_matches_oracle(gpu_ops, orc, Nb):
+    NE, Nk = 29, 2
+    eps, h, GR, GL, GG, tot = _consistent_state(orc, 50 + Nb, NE, Nk, Nb)
+    rng = np.random.default_rng(5)
+    cand = np.asfortranarray(tot[1] * (1 + 0.01 * rng.standard_normal(tot[1].shape)))
+    ref = orc.residual_suite(eps, h, GR, GL, GG, tot, cand)
+    got = gpu_ops.production_residual_suite(eps, h, GR, GL, GG, tot, cand)
+    for k in ("rA", "rK"):
+        assert abs(got[k] - ref[k]) <= 1e-10 * max(ref[k], 1e-14) + 1e-15, (k, got[k], ref[k])
+    assert abs(got["rD"] - ref["rD"]) <= 1e-14
+    assert got["rPSD"] == pytest.approx(ref["rPSD"], abs=1e-13)
+    assert got["rcaus"] == pytest.approx(ref["rcaus"], abs=1e-13)
+
+
+def test_residual_suite_detects_indefinite_and_acausal_blocks(gpu_ops, orc):
+    NE, Nk, Nb = 17, 2, 5
+    eps, h, GR, GL, GG, tot = _consistent_state(orc, 77, NE, Nk, Nb)
+    SR, SL, SG = (np.array(t, order="F") for t in tot)
+    SR[3, 1] += 0.3j * np.eye(Nb)        # Im SigmaR > 0 in one block: acausal
+    GL2 = np.array(GL, order="F")
+    GL2[5, 0, 0, 0] += 2.0j              # -i G< gains a negative eigenvalue
+    ref = orc.residual_suite(eps, h, GR, GL2, GG, (SR, SL, SG), SL)
+    got = gpu_ops.production_residual_suite(eps, h, GR, GL2, GG, (SR, SL, SG), SL)
+    assert ref["rPSD"] > 1e-3 and ref["rcaus"] > 1e-3
+    assert got["rPSD"] == pytest.approx(ref["rPSD"], rel=1e-10)
+    assert got["rcaus"] == pytest.approx(ref["rcaus"], rel=1e-10)
+
+
+def test_selfenergy_residual(gpu_ops, orc):
+    rng = np.random.default_rng(8)
+    a = _rand_field(rng, (33, 2, 3, 3))
+    b = a + 0.01 * _rand_field(rng, a.shape)
+    assert gpu_ops.production_selfenergy_residual(a, b) == pytest.approx(orc.relative_change(a, b), rel=1e-13)
+    bad = np.array(b, order="F")
+    bad[0, 0, 0, 0] = np.nan
+    assert gpu_ops.production_selfenergy_residual(a, bad) == math.inf
+
+
+def test_current_and_populations_match_oracle(gpu_ops, orc):
+    from qclb200.problem import small_problem
+
+    pr = small_problem(NE=41, Nk=3, Nb=4)
+    rng = np.random.default_rng(21)
+    SG, SL, GL, GG = (_rand_field(rng, pr.shape) for _ in range(4))
+    Jbar, pops = gpu_ops.current_and_populations(pr, SG, SL, GL, GG)
+    assert Jbar == pytest.approx(orc.current(pr, SG, SL, GL, GG), rel=1e-12, abs=1e-14)
+    np.testing.assert_allclose(pops, orc.populations(pr, GL), rtol=1e-12, atol=1e-14)
+
+
+def test_zero_bias_equilibrium_current_on_gpu(gpu_ops, orc):
+    # analytic_equilibrium_..._anchors.jl:71-138 through the device reductions
+    from qclb200.problem import small_problem
+
+    pr = small_problem(NE=61, Nk=3, Nb=4)
+    gamma = 0.02
+    f = 1 / (np.exp(pr.eps / pr.kBT) + 1)
+    SR = np.zeros(pr.shape, dtype=complex, order="F")
+    SL = np.zeros(pr.shape, dtype=complex, order="F")
+    SG = np.zeros(pr.shape, dtype=complex, order="F")
+    for a in range(pr.Nb):
+        SR[:, :, a, a] = -0.5j * gamma
+        SL[:, :, a, a] = (1j * f * gamma)[:, None]
+        SG[:, :, a, a] = (-1j * (1 - f) * gamma)[:, None]
+    GR, GL, _, _ = gpu_ops.dyson_keldysh(pr.eps, pr.h, SR, SL)
+    GG = GR - np.conj(np.transpose(GR, (0, 1, 3, 2))) + GL
+    Jbar, _ = gpu_ops.current_and_populations(pr, SG, SL, GL, GG)
+    assert abs(Jbar) < 2e-13
+
+
+@pytest.mark.parametrize("n", [1, 2, 3, 4, 5, 8, 12, 16, 17, 24, 32, 33, 48])
+def test_batched_hermitian_eigvals_match_numpy(gpu_ops, n):
+    rng = np.random.default_rng(n)
+    X = rng.standard_normal((20, n, n)) + 1j * rng.standard_normal((20, n, n))
+    H = X + np.conj(np.transpose(X, (0, 2, 1)))
+    got = gpu_ops.hermitian_eigvals(H)
+    ref = np.linalg.eigvalsh(H)
+    assert np.max(np.abs(got - ref)) <= 1e-12 * np.max(np.abs(ref))

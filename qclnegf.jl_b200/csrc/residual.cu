@@ -56,20 +56,18 @@ __device__ __forceinline__ void team_sum2(double& a, double& b, int tt, double* 
 
 // Eigenvalues of the Hermitian NxN matrix H (swizzled NP x NP shared tile);
 // H is destroyed, S.vals[0..N-1] receives the eigenvalues (unsorted).
+// Round-robin parallel Jacobi: in each of the n2-1 rounds of a sweep the
+// rotations of n2/2 disjoint index pairs are computed from the same matrix
+// and applied together (all column updates, then all row updates).  The
+// rotated pair is set to exactly zero and its diagonal to exactly real, so
+// rounding cannot leave a non-Hermitian remainder; a pair whose coupling is
+// negligible against its diagonal (1e-18 relative) is skipped, and a sweep
+// that rotates nothing ends the iteration.
 template <int NP, int TT>
 __device__ void team_eigvals(Cx<double>* H, int N, int tt, ResScratch<NP>& S, int team) {
   const int n2 = N + (N & 1);
   for (int sweep = 0; sweep < 40; ++sweep) {
-    double off = 0, dia = 0;
-    for (int idx = tt; idx < N * N; idx += TT) {
-      const int i = idx % N, j = idx / N;
-      const Cx<double> v = H[sw<NP>(i, j)];
-      const double m2 = v.x * v.x + v.y * v.y;
-      if (i == j) dia += m2; else off += m2;
-    }
-    off = team_sum<TT>(off, tt, S.red, team);
-    dia = team_sum<TT>(dia, tt, S.red + 2, team);
-    if (!(off > 1e-32 * dia) || !isfinite(off)) break;
+    double rotated = 0;
     for (int r = 0; r < n2 - 1; ++r) {
       if (tt < n2 / 2) {
         const int i = tt;
@@ -84,9 +82,9 @@ __device__ void team_eigvals(Cx<double>* H, int N, int tt, ResScratch<NP>& S, in
         rt.pi = 0;
         if (rt.q < N) {
           const Cx<double> apq = H[sw<NP>(rt.p, rt.q)];
-          const double mag = sqrt(apq.x * apq.x + apq.y * apq.y);
-          if (mag > 0 && isfinite(mag)) {
-            const double app = H[sw<NP>(rt.p, rt.p)].x, aqq = H[sw<NP>(rt.q, rt.q)].x;
+          const double mag = hypot(apq.x, apq.y);
+          const double app = H[sw<NP>(rt.p, rt.p)].x, aqq = H[sw<NP>(rt.q, rt.q)].x;
+          if (mag > 1e-18 * (fabs(app) + fabs(aqq)) && isfinite(mag)) {
             const double theta = (aqq - app) / (2 * mag);
             double t;
             if (fabs(theta) > 1e150) t = 0.5 / theta;
@@ -95,6 +93,7 @@ __device__ void team_eigvals(Cx<double>* H, int N, int tt, ResScratch<NP>& S, in
             rt.s = t * rt.c;
             rt.pr = apq.x / mag;
             rt.pi = apq.y / mag;
+            rotated = 1;
           }
         } else {
           rt.q = rt.p;  // phantom partner: identity
@@ -113,18 +112,29 @@ __device__ void team_eigvals(Cx<double>* H, int N, int tt, ResScratch<NP>& S, in
         H[sw<NP>(k, rt.q)] = cx<double>(rt.s * hp.x + rt.c * eq.x, rt.s * hp.y + rt.c * eq.y);
       }
       team_sync<TT>(team);
-      // rows: H <- J^H H
+      // rows: H <- J^H H; the rotated pair becomes exactly diagonal
       for (int idx = tt; idx < N * (n2 / 2); idx += TT) {
         const int k = idx % N;
         const JacobiRot rt = S.rot[idx / N];
         if (rt.p == rt.q || rt.s == 0) continue;
         const Cx<double> xp = H[sw<NP>(rt.p, k)], xq = H[sw<NP>(rt.q, k)];
         const Cx<double> eq = cx<double>(rt.pr, rt.pi) * xq;  // e^{i phi} H[q][k]
-        H[sw<NP>(rt.p, k)] = cx<double>(rt.c * xp.x - rt.s * eq.x, rt.c * xp.y - rt.s * eq.y);
-        H[sw<NP>(rt.q, k)] = cx<double>(rt.s * xp.x + rt.c * eq.x, rt.s * xp.y + rt.c * eq.y);
+        Cx<double> np_ = cx<double>(rt.c * xp.x - rt.s * eq.x, rt.c * xp.y - rt.s * eq.y);
+        Cx<double> nq_ = cx<double>(rt.s * xp.x + rt.c * eq.x, rt.s * xp.y + rt.c * eq.y);
+        if (k == rt.p) {
+          np_.y = 0;             // H[p][p] real
+          nq_ = cx<double>(0, 0);  // H[q][p] = 0
+        } else if (k == rt.q) {
+          np_ = cx<double>(0, 0);  // H[p][q] = 0
+          nq_.y = 0;             // H[q][q] real
+        }
+        H[sw<NP>(rt.p, k)] = np_;
+        H[sw<NP>(rt.q, k)] = nq_;
       }
       team_sync<TT>(team);
     }
+    rotated = team_max<TT>(rotated, tt, S.red, team);
+    if (rotated == 0) break;
   }
   for (int i = tt; i < N; i += TT) S.vals[i] = H[sw<NP>(i, i)].x;
   team_sync<TT>(team);

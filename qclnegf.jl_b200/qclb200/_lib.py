@@ -120,6 +120,7 @@ def _declare(l):
         "qcl_dev_paired_coefficients": (I, [P, P, P, I, D, P, P]),
         "qcl_dev_normalize_pair": (I, [P, I, Z, P, P, P]),
         "qcl_fft_hilbert_transform": (I, [I, I, Z, P, P, P, P, P]),
+        "qcl_dev_fft_hilbert_transform": (I, [P, I, I, Z, D, P, P, P, P]),
         "qcl_retarded_self_energy": (I, [I, I, Z, P, P, P, P, P, P, P]),
         "qcl_apply_energy_shift": (I, [I, I, Z, P, D, P, P]),
         "qcl_static_contraction": (I, [I, P, I, I, I, P, D, D, P, P]),

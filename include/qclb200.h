@@ -167,6 +167,20 @@ int qcl_residual_suite(int precision, int NE, int Nk, int Nb, const double* eps,
  * (_production_hermitian_eigvals!, numerics/optimized/residuals.jl:311-353). */
 int qcl_hermitian_eigvals(int n, size_t count, const void* H, double* vals);
 
+/* Allocation-free residual suite on device arrays (no counterpart in the
+ * reference).  For callers that cannot call cudaMalloc -- a host whose
+ * device memory belongs to its own pool allocator, a fixed up-front device
+ * budget, or a loop that must not risk the synchronisation of an allocation.
+ * Same result as qcl_residual_suite (out: 5 doubles in device memory, written
+ * asynchronously on `stream`); the per-block scratch is a fixed device array
+ * of the library (about 14.7 MB per GPU, held until exit), so N_E * N_k must
+ * not exceed 262144 (QCL_UNSUPPORTED otherwise).  Calls share that array:
+ * calls that overlap on the GPU race.  The first call on a device looks up
+ * the array's address on that device; make it before any stream capture. */
+int qcl_dev_residual_suite_noalloc(void* stream, int precision, int NE, int Nk, int Nb, const double* eps,
+                                   const void* h, const void* GR, const void* GL, const void* GG, const void* SR,
+                                   const void* SL, const void* SG, const void* SLc, double* out);
+
 /* out = ||new - old||_F / (||new||_F + 1e-14) for one component
  * (production_selfenergy_residual, residuals.jl:802-865). */
 int qcl_selfenergy_residual(int precision, size_t n, const void* old_, const void* new_, double* out);

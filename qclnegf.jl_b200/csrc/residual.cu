@@ -18,6 +18,8 @@
 // of a round applied at once), the spectral norm of SR (zgesvd, :355-409) from
 // the same solver on SR SR^H, needed only when lmax(Im SR) > 0.  Per-block
 // partial results go to global memory and are reduced in a fixed order.
+#include <mutex>
+
 #include "blockmat.cuh"
 
 namespace qcl {
@@ -508,6 +510,41 @@ constexpr int RES_CTAS = 148;
 
 size_t residual_work_doubles(int NE, int Nk) { return 7 * (size_t)NE * Nk + 7 * RES_CTAS; }
 
+// ---------------------------------------------------------------------------
+// Allocation-free variant.  Some callers cannot call cudaMalloc: a Julia
+// session whose device memory is owned by its own pool allocator, a host
+// application that reserves a fixed device budget up front, or a solver loop
+// that must not pay the device synchronisation an allocation can imply.  For
+// them the residual suite's scratch (7 doubles per (E,k) block plus 7 per
+// reduction CTA) lives in this file-scope device array instead.  Every GPU
+// that loads the library holds it (about 14.7 MB) until the process exits.
+// ---------------------------------------------------------------------------
+constexpr long long kNoAllocMaxBlocks = 1ll << 18;  // N_E * N_k <= 262144
+static __device__ __align__(256) double g_residual_scratch[7 * kNoAllocMaxBlocks + 7 * 148];
+
+static std::mutex g_noalloc_mutex;
+static double* g_noalloc_ptr[64] = {nullptr};
+
+// Device address of the scratch array on the current device, resolved once
+// per device (host code cannot use the symbol itself as an address).
+static int noalloc_scratch(double** out) {
+  int dev = 0;
+  QCL_CUDA_CHECK(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 64) {
+    set_last_error("device ordinal %d out of range", dev);
+    return QCL_ARG;
+  }
+  std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+  if (!g_noalloc_ptr[dev]) {
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_residual_scratch);
+    if (e != cudaSuccess) return cuda_status(e, "cudaGetSymbolAddress(g_residual_scratch)");
+    g_noalloc_ptr[dev] = (double*)p;
+  }
+  *out = g_noalloc_ptr[dev];
+  return QCL_OK;
+}
+
 int launch_residual_suite(int precision, int NE, int Nk, int N, const double* eps, const void* h, const void* GR,
                           const void* GL, const void* GG, const void* SR, const void* SL, const void* SG,
                           const void* SLc, double* work, double* out5, cudaStream_t st) {
@@ -532,3 +569,40 @@ int launch_residual_suite(int precision, int NE, int Nk, int N, const double* ep
 }
 
 }  // namespace qcl
+
+using namespace qcl;
+
+// The scratch is fully rewritten by every call before it is read (each live
+// block writes its 7 values, the reduction writes all its partials), so
+// nothing needs clearing between calls.  Calls share the array: two calls that
+// overlap on the GPU (different streams, or concurrent host threads) race on
+// it.  The first call on a device resolves the array's address on that
+// device; make that first call before any stream capture.
+extern "C" int qcl_dev_residual_suite_noalloc(void* stream, int precision, int NE, int Nk, int Nb, const double* eps,
+                                              const void* h, const void* GR, const void* GL, const void* GG,
+                                              const void* SR, const void* SL, const void* SG, const void* SLc,
+                                              double* out) {
+  if (precision != QCL_C128 && precision != QCL_C64 && precision != QCL_MIXED) {
+    set_last_error("unknown precision %d", precision);
+    return QCL_ARG;
+  }
+  if (NE <= 0 || Nk <= 0 || Nb <= 0) {
+    set_last_error("residual_suite_noalloc: non-positive dimension (%d,%d,%d)", NE, Nk, Nb);
+    return QCL_DIM;
+  }
+  if ((long long)NE * Nk > kNoAllocMaxBlocks) {
+    set_last_error("residual_suite_noalloc: N_E*N_k = %lld exceeds the fixed scratch capacity of %lld blocks",
+                   (long long)NE * Nk, kNoAllocMaxBlocks);
+    return QCL_UNSUPPORTED;
+  }
+  if (!eps || !h || !GR || !GL || !GG || !SR || !SL || !SG || !SLc || !out) {
+    set_last_error("residual_suite_noalloc: all arrays are required");
+    return QCL_ARG;
+  }
+  double* scratch = nullptr;
+  int s = noalloc_scratch(&scratch);
+  if (s) return s;
+  const int sp = precision == QCL_MIXED ? QCL_C64 : precision;
+  return launch_residual_suite(sp, NE, Nk, Nb, eps, h, GR, GL, GG, SR, SL, SG, SLc, scratch, out,
+                               (cudaStream_t)stream);
+}

@@ -128,6 +128,7 @@ def _declare(l):
         "qcl_residual_suite": (I, [I, I, I, I, P, P, P, P, P, P, P, P, P, P]),
         "qcl_selfenergy_residual": (I, [I, Z, P, P, P]),
         "qcl_hermitian_eigvals": (I, [I, Z, P, P]),
+        "qcl_dev_residual_suite_noalloc": (I, [P, I, I, I, I, P, P, P, P, P, P, P, P, P, P]),
         "qcl_current_populations": (I, [I, I, I, I, P, P, I, D, P, P, P, P, P]),
         "qcl_scba_create": (I, [P, P, P]),
         "qcl_scba_destroy": (None, [P]),

@@ -26,6 +26,7 @@
 // ones, and the same per-column partial sums of |y_2L - y_L|^2 and |y_L|^2.
 #include <math.h>
 
+#include <algorithm>
 #include <vector>
 
 #include "kernels.cuh"
@@ -126,11 +127,18 @@ __device__ __forceinline__ void stockham_pass(Cx<R>* buf, const Cx<R>* __restric
     if (j < NB) {
       const int k = j % NS;
       if (NS > 1) {
+        // One table load per butterfly: w_r = w_1^r by binary powering
+        // (products of at most four factors, so the twiddle error stays a
+        // few ulps), instead of RADIX - 1 dependent global loads.
+        Cx<R> w[RADIX];
+        w[1] = tw[k * (L / (NS * RADIX))];
 #pragma unroll
-        for (int r = 1; r < RADIX; ++r) {
-          const Cx<R> w = tw[(r * k) * (L / (NS * RADIX))];
-          v[q][r] = v[q][r] * w;
+        for (int r = 2; r < RADIX; ++r) {
+          const int hi = (r & (r - 1)) ? (r & (r - 1)) : r / 2;  // r = hi + lo, hi >= lo
+          w[r] = w[hi] * w[r - hi];
         }
+#pragma unroll
+        for (int r = 1; r < RADIX; ++r) v[q][r] = v[q][r] * w[r];
       }
       DifStage<R, RADIX, RADIX / 2>::run(v[q]);
       const int idxD = (j / NS) * NS * RADIX + k;

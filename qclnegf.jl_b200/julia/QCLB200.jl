@@ -1,0 +1,166 @@
+"""
+    QCLB200
+
+Julia binding of libqclb200.so, the B200 (sm_100a) implementation of the SCBA
+hot path of QCLNEGF.jl.  Every function keeps the argument meaning and the
+array layout of the QCLNEGF.jl function it replaces (fields are
+`Array{ComplexF64,4}` of size `(N_E, N_k, N_b, N_b)`, energy fastest), calls
+the library through `ccall` in the same way QCLNEGF.jl already calls LAPACK
+(`numerics/optimized/production_operators.jl:20-61`), and maps the library
+status to the same exceptions.
+
+Set `ENV["QCLB200_LIB"]` to the path of `libqclb200.so` before loading.
+"""
+module QCLB200
+
+using LinearAlgebra
+
+const libqcl = get(ENV, "QCLB200_LIB", joinpath(@__DIR__, "..", "lib", "libqclb200.so"))
+
+const QCL_C128 = Cint(0)
+const QCL_C64 = Cint(1)
+const QCL_MIXED = Cint(2)
+
+function check(status::Cint)
+    status == 0 && return nothing
+    msg = unsafe_string(ccall((:qcl_last_error, libqcl), Cstring, ()))
+    status == 1 && throw(SingularException(0))
+    status == 2 && throw(DomainError(msg))
+    status == 3 && throw(DimensionMismatch(msg))
+    status == 4 && throw(ArgumentError(msg))
+    error("qclb200 status $status: $msg")
+end
+
+"""Fused `_retarded_green_production` + the raw sandwiches of
+`_current_green_production`: returns `(Gᴿ, Gˡ, Gᵍ, scale)`."""
+function dyson_keldysh(ε::Vector{Float64}, h::Array{ComplexF64,3}, Σᴿ::Array{ComplexF64,4},
+                       Σˡ::Array{ComplexF64,4}, Σᵍ::Array{ComplexF64,4}; η::Real = 0.0)
+    NE, Nk, Nb, _ = size(Σᴿ)
+    size(h) == (Nk, Nb, Nb) || throw(DimensionMismatch("h has wrong shape"))
+    Gᴿ = similar(Σᴿ); Gˡ = similar(Σᴿ); Gᵍ = similar(Σᴿ)
+    scale = zeros(Float64, NE, Nk)
+    check(ccall((:qcl_dyson_keldysh, libqcl), Cint,
+                (Cint, Cint, Cint, Cint, Ptr{Float64}, Float64, Ptr{ComplexF64}, Ptr{ComplexF64},
+                 Ptr{ComplexF64}, Ptr{ComplexF64}, Ptr{ComplexF64}, Ptr{ComplexF64}, Ptr{ComplexF64},
+                 Ptr{Float64}, Ptr{ComplexF64}, Ptr{ComplexF64}),
+                QCL_C128, NE, Nk, Nb, ε, Float64(η), h, Σᴿ, Σˡ, Σᵍ, Gᴿ, Gˡ, Gᵍ, scale, C_NULL, C_NULL))
+    return Gᴿ, Gˡ, Gᵍ, scale
+end
+
+"""`production_fft_hilbert_transform(Γ, ε, wᴱ, plan; return_roundoff)`."""
+function fft_hilbert_transform(Γ::Array{ComplexF64,4}, ε::Vector{Float64}, wᴱ::Vector{Float64};
+                               return_roundoff::Bool = false)
+    NE = size(Γ, 1)
+    Λ = similar(Γ)
+    r = Ref{Float64}(0.0)
+    check(ccall((:qcl_fft_hilbert_transform, libqcl), Cint,
+                (Cint, Cint, Csize_t, Ptr{Float64}, Ptr{Float64}, Ptr{ComplexF64}, Ptr{ComplexF64}, Ptr{Float64}),
+                QCL_C128, NE, length(Γ) ÷ NE, ε, wᴱ, Γ, Λ, return_roundoff ? r : C_NULL))
+    return return_roundoff ? (Λ, r[]) : Λ
+end
+
+"""`apply_energy_shift!(destination, build_shift_plan(ε, δ), X)`."""
+function apply_energy_shift!(dst::Array{ComplexF64,4}, ε::Vector{Float64}, δ::Real, X::Array{ComplexF64,4})
+    Base.mightalias(dst, X) && throw(ArgumentError("in-place aliasing is not supported"))
+    NE = size(X, 1)
+    check(ccall((:qcl_apply_energy_shift, libqcl), Cint,
+                (Cint, Cint, Csize_t, Ptr{Float64}, Float64, Ptr{ComplexF64}, Ptr{ComplexF64}),
+                QCL_C128, NE, length(X) ÷ NE, ε, Float64(δ), X, dst))
+    return dst
+end
+
+struct Mechanism
+    kind::Cint
+    is_LO::Cint
+    J::Cint
+    q::Float64
+    block::Ptr{ComplexF64}
+    matrix::Ptr{ComplexF64}
+    left::Ptr{ComplexF64}
+    right::Ptr{ComplexF64}
+    radial::Ptr{ComplexF64}
+end
+
+"""`production_static_contraction(op, G, wᵏ, qᴷ)` for the factorised
+operators: `:momentum_independent` (block), `:dense` (matrix), `:ifr`
+(left, right, radial).  Arrays must stay rooted during the call."""
+function production_static_contraction(kind::Symbol, arrays::NamedTuple, G::Array{ComplexF64,4},
+                                       wᵏ::Vector{Float64}, qᴷ::Real; α::Real = 1, β::Real = 0,
+                                       Σ::Array{ComplexF64,4} = zeros(ComplexF64, size(G)))
+    NE, Nk, Nb, _ = size(G)
+    k = kind === :momentum_independent ? 0 : kind === :dense ? 1 : kind === :ifr ? 2 :
+        throw(ArgumentError("unknown kernel kind $kind"))
+    GC.@preserve arrays begin
+        p(name) = haskey(arrays, name) ? pointer(getfield(arrays, name)) : Ptr{ComplexF64}(C_NULL)
+        J = haskey(arrays, :left) ? size(arrays.left, 2) : 0
+        op = Ref(Mechanism(k, 0, J, Float64(qᴷ), p(:block), p(:matrix), p(:left), p(:right), p(:radial)))
+        check(ccall((:qcl_static_contraction, libqcl), Cint,
+                    (Cint, Ref{Mechanism}, Cint, Cint, Cint, Ptr{Float64}, Float64, Float64,
+                     Ptr{ComplexF64}, Ptr{ComplexF64}),
+                    QCL_C128, op, NE, Nk, Nb, wᵏ, Float64(α), Float64(β), G, Σ))
+    end
+    return Σ
+end
+
+"""`production_residual_suite(ε, h, green, total, candidate)` →
+`(r_D, r_A, r_K, r_PSD, r_caus)`."""
+function production_residual_suite(ε, h, Gᴿ, Gˡ, Gᵍ, Σᴿ, Σˡ, Σᵍ, candidate_Σˡ)
+    NE, Nk, Nb, _ = size(Gᴿ)
+    out = zeros(Float64, 5)
+    check(ccall((:qcl_residual_suite, libqcl), Cint,
+                (Cint, Cint, Cint, Cint, Ptr{Float64}, Ptr{ComplexF64}, Ptr{ComplexF64}, Ptr{ComplexF64},
+                 Ptr{ComplexF64}, Ptr{ComplexF64}, Ptr{ComplexF64}, Ptr{ComplexF64}, Ptr{ComplexF64},
+                 Ptr{Float64}),
+                QCL_C128, NE, Nk, Nb, ε, h, Gᴿ, Gˡ, Gᵍ, Σᴿ, Σˡ, Σᵍ, candidate_Σˡ, out))
+    return (r_D = out[1], r_A = out[2], r_K = out[3], r_PSD = out[4], r_caus = out[5])
+end
+
+# ---------------------------------------------------------------------------
+# SCBA level (solve_scba_production inner loop on the device)
+# ---------------------------------------------------------------------------
+struct Problem
+    NE::Cint; Nk::Cint; Nb::Cint
+    eps::Ptr{Float64}; wE::Ptr{Float64}; wk::Ptr{Float64}
+    h::Ptr{ComplexF64}; Tplus::Ptr{ComplexF64}; Tminus::Ptr{ComplexF64}
+    Ep::Float64; hw_LO::Float64; N_LO::Float64
+    gs::Cint; target::Float64; eta_seed::Float64; kBT::Float64; alpha::Float64; J0::Float64
+    precision::Cint; verify_roundoff::Cint; nmech::Cint
+end
+
+struct Row
+    nu::Cint; status::Cint
+    r_D::Float64; r_A::Float64; r_K::Float64; r_Sigma::Float64; r_lambda::Float64; lambda::Float64
+    r_PSD::Float64; r_caus::Float64; r_roundoff::Float64; r_J::Float64; r_pop::Float64
+    J::Float64; Jbar::Float64; number::Float64; holes::Float64
+    occupied_fraction::Float64; empty_fraction::Float64
+end
+
+mutable struct Solver
+    handle::Ptr{Cvoid}
+    keep::Vector{Any}
+end
+
+function create(problem::Problem, mechanisms::Vector{Mechanism}, keep::Vector{Any})
+    h = Ref{Ptr{Cvoid}}(C_NULL)
+    check(ccall((:qcl_scba_create, libqcl), Cint, (Ref{Problem}, Ptr{Mechanism}, Ref{Ptr{Cvoid}}),
+                problem, mechanisms, h))
+    s = Solver(h[], keep)
+    finalizer(x -> ccall((:qcl_scba_destroy, libqcl), Cvoid, (Ptr{Cvoid},), x.handle), s)
+    return s
+end
+
+seed!(s::Solver) = (μ = Ref(0.0); check(ccall((:qcl_scba_seed, libqcl), Cint, (Ptr{Cvoid}, Ref{Float64}), s.handle, μ)); μ[])
+
+function step!(s::Solver)
+    r = Ref{Row}()
+    check(ccall((:qcl_scba_step, libqcl), Cint, (Ptr{Cvoid}, Ref{Row}), s.handle, r))
+    return r[]
+end
+
+function download(s::Solver, which::Integer, shape::NTuple{4,Int})
+    out = Array{ComplexF64,4}(undef, shape)
+    check(ccall((:qcl_scba_download, libqcl), Cint, (Ptr{Cvoid}, Cint, Ptr{ComplexF64}), s.handle, which, out))
+    return out
+end
+
+end # module

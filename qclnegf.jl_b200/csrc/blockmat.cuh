@@ -76,18 +76,24 @@ __device__ __forceinline__ void warp_argmax(double& mag, int& row) {
   }
 }
 
-// C = A * B (adjB = false) or C = A * B^H (adjB = true); NxN active part of
-// NP x NP swizzled shared matrices.  RM is the arithmetic precision.
+// Register tile of a team matmul: thread tt owns rows rg*TR + t and columns
+// cg*TC + u of the NP x NP product.
+template <typename RM, int NP> struct MatTile {
+  static constexpr int TR = Tile<NP>::TR, TC = Tile<NP>::TC, RG = NP / TR;
+  Cx<RM> v[TR][TC];
+};
+
+// acc = A * B (adjB = false) or A * B^H (adjB = true) over the N x N active
+// part of NP x NP swizzled shared matrices; RM is the arithmetic precision.
 template <typename RS, typename RM, int NP>
-__device__ __forceinline__ void team_matmul(const Cx<RS>* A, const Cx<RS>* B, Cx<RS>* C, int N, int tt,
-                                            bool adjB) {
+__device__ __forceinline__ void team_matmul_regs(const Cx<RS>* A, const Cx<RS>* B, MatTile<RM, NP>& acc, int N,
+                                                 int tt, bool adjB) {
   constexpr int TR = Tile<NP>::TR, TC = Tile<NP>::TC, RG = NP / TR;
   const int rg = tt % RG, cg = tt / RG;
-  Cx<RM> acc[TR][TC];
 #pragma unroll
   for (int t = 0; t < TR; ++t)
 #pragma unroll
-    for (int u = 0; u < TC; ++u) acc[t][u] = cx<RM>(0, 0);
+    for (int u = 0; u < TC; ++u) acc.v[t][u] = cx<RM>(0, 0);
   for (int l = 0; l < N; ++l) {
     Cx<RM> a[TR], b[TC];
 #pragma unroll
@@ -100,12 +106,27 @@ __device__ __forceinline__ void team_matmul(const Cx<RS>* A, const Cx<RS>* B, Cx
 #pragma unroll
     for (int t = 0; t < TR; ++t)
 #pragma unroll
-      for (int u = 0; u < TC; ++u) cfma(acc[t][u], a[t], b[u]);
+      for (int u = 0; u < TC; ++u) cfma(acc.v[t][u], a[t], b[u]);
   }
+}
+
+template <typename RS, typename RM, int NP>
+__device__ __forceinline__ void team_store_regs(Cx<RS>* C, const MatTile<RM, NP>& acc, int tt) {
+  constexpr int TR = Tile<NP>::TR, TC = Tile<NP>::TC, RG = NP / TR;
+  const int rg = tt % RG, cg = tt / RG;
 #pragma unroll
   for (int t = 0; t < TR; ++t)
 #pragma unroll
-    for (int u = 0; u < TC; ++u) C[sw<NP>(rg * TR + t, cg * TC + u)] = cvt<RS>(acc[t][u]);
+    for (int u = 0; u < TC; ++u) C[sw<NP>(rg * TR + t, cg * TC + u)] = cvt<RS>(acc.v[t][u]);
+}
+
+// C = A * B (adjB = false) or C = A * B^H (adjB = true); C distinct from A, B.
+template <typename RS, typename RM, int NP>
+__device__ __forceinline__ void team_matmul(const Cx<RS>* A, const Cx<RS>* B, Cx<RS>* C, int N, int tt,
+                                            bool adjB) {
+  MatTile<RM, NP> acc;
+  team_matmul_regs<RS, RM, NP>(A, B, acc, N, tt, adjB);
+  team_store_regs<RS, RM, NP>(C, acc, tt);
 }
 
 // Cooperative, coalesced copy of BPC consecutive-energy blocks between a
@@ -113,13 +134,15 @@ __device__ __forceinline__ void team_matmul(const Cx<RS>* A, const Cx<RS>* B, Cx
 template <typename RG_, typename RS, int NP, int BPC>
 __device__ __forceinline__ void load_blocks(const Cx<RG_>* __restrict__ X, Cx<RS>* bufs, size_t stride_buf,
                                             int e0, int m, int NE, int Nk, int N) {
-  const int total = BPC * N * N;
+  const int total = BPC * NP * N;  // rows padded to NP: compile-time index split
+  const size_t base = (size_t)e0 + (size_t)NE * m, cstride = (size_t)NE * Nk;
   for (int i = threadIdx.x; i < total; i += blockDim.x) {
     const int eloc = i % BPC, el = i / BPC;
-    const int a = el % N, b = el / N;
+    const int a = el % NP, b = el / NP;
+    if (a >= N) continue;
     const int e = e0 + eloc;
     Cx<RS> v = cx<RS>(0, 0);
-    if (e < NE) v = cvt<RS>(X[(size_t)e + (size_t)NE * ((size_t)m + (size_t)Nk * ((size_t)a + (size_t)N * b))]);
+    if (e < NE) v = cvt<RS>(X[base + eloc + cstride * ((size_t)a + (size_t)N * b)]);
     bufs[eloc * stride_buf + sw<NP>(a, b)] = v;
   }
 }
@@ -141,13 +164,14 @@ __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wai
 template <typename R, int NP, int BPC>
 __device__ __forceinline__ void load_blocks_async(const Cx<R>* __restrict__ X, Cx<R>* bufs, size_t stride_buf, int e0,
                                                   int m, int NE, int Nk, int N) {
-  const int total = BPC * N * N;
+  const int total = BPC * NP * N;
+  const size_t base = (size_t)e0 + (size_t)NE * m, cstride = (size_t)NE * Nk;
   for (int i = threadIdx.x; i < total; i += blockDim.x) {
     const int eloc = i % BPC, el = i / BPC;
-    const int a = el % N, b = el / N;
-    const int e = e0 + eloc;
-    const bool ok = e < NE;
-    const Cx<R>* src = X + (ok ? (size_t)e + (size_t)NE * ((size_t)m + (size_t)Nk * ((size_t)a + (size_t)N * b)) : 0);
+    const int a = el % NP, b = el / NP;
+    if (a >= N) continue;
+    const bool ok = e0 + eloc < NE;
+    const Cx<R>* src = X + (ok ? base + eloc + cstride * ((size_t)a + (size_t)N * b) : 0);
     cp_async_elem<R>(bufs + eloc * stride_buf + sw<NP>(a, b), src, ok);
   }
   cp_async_commit();
@@ -156,14 +180,13 @@ __device__ __forceinline__ void load_blocks_async(const Cx<R>* __restrict__ X, C
 template <typename RG_, typename RS, int NP, int BPC>
 __device__ __forceinline__ void store_blocks(Cx<RG_>* __restrict__ X, const Cx<RS>* bufs, size_t stride_buf,
                                              int e0, int m, int NE, int Nk, int N) {
-  const int total = BPC * N * N;
+  const int total = BPC * NP * N;
+  const size_t base = (size_t)e0 + (size_t)NE * m, cstride = (size_t)NE * Nk;
   for (int i = threadIdx.x; i < total; i += blockDim.x) {
     const int eloc = i % BPC, el = i / BPC;
-    const int a = el % N, b = el / N;
-    const int e = e0 + eloc;
-    if (e < NE)
-      X[(size_t)e + (size_t)NE * ((size_t)m + (size_t)Nk * ((size_t)a + (size_t)N * b))] =
-          cvt<RG_>(bufs[eloc * stride_buf + sw<NP>(a, b)]);
+    const int a = el % NP, b = el / NP;
+    if (a >= N || e0 + eloc >= NE) continue;
+    X[base + eloc + cstride * ((size_t)a + (size_t)N * b)] = cvt<RG_>(bufs[eloc * stride_buf + sw<NP>(a, b)]);
   }
 }
 

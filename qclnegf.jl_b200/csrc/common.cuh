@@ -85,6 +85,33 @@ template <typename R> __device__ __forceinline__ Cx<R> crecip_scaled(Cx<R> z) {
   return cx<R>(ldexp(xs * r, -ex), ldexp(-ys * r, -ex));
 }
 
+// 1 / z for the pivots of the elimination.  Both parts are multiplied by the
+// power of two 2^(bias - e) built from the exponent field e of max(|re|, |im|)
+// (exact), so that d = |z|^2 lies in [1, 8); 1 / d is refined by Newton-Raphson
+// (r <- r + r (1 - d r)) from a single-precision seed, two steps for double
+// (relative error ~2^-92 before the final rounding).  Valid for finite
+// non-zero z; the caller flags zero pivots and never uses their reciprocal.
+__device__ __forceinline__ Cx<double> crecip_pivot(Cx<double> z) {
+  const double mx = fmax(fabs(z.x), fabs(z.y));
+  const int e = min((__double2hiint(mx) >> 20) & 0x7ff, 2045);
+  const double sc = __hiloint2double((2046 - e) << 20, 0);
+  const double xs = z.x * sc, ys = z.y * sc;
+  const double d = fma(xs, xs, ys * ys);
+  double r = (double)__frcp_rn((float)d);
+  r = fma(r, fma(-d, r, 1.0), r);
+  r = fma(r, fma(-d, r, 1.0), r);
+  return cx<double>((xs * r) * sc, (-ys * r) * sc);
+}
+__device__ __forceinline__ Cx<float> crecip_pivot(Cx<float> z) {
+  const float mx = fmaxf(fabsf(z.x), fabsf(z.y));
+  const int e = min((__float_as_int(mx) >> 23) & 0xff, 253);
+  const float sc = __int_as_float((254 - e) << 23);
+  const float xs = z.x * sc, ys = z.y * sc;
+  const float d = fmaf(xs, xs, ys * ys);
+  float r = __frcp_rn(d);
+  return cx<float>((xs * r) * sc, (-ys * r) * sc);
+}
+
 template <typename R> struct Real;
 template <> struct Real<double> { static constexpr int dtype = QCL_C128; };
 template <> struct Real<float> { static constexpr int dtype = QCL_C64; };

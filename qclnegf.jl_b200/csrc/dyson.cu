@@ -40,32 +40,83 @@ template <typename RS> struct DysonArgs {
   int mcount;
 };
 
-// Argmax key: the pivot magnitude's IEEE bits with the low 8 bits replaced
-// by (255 - row).  Unsigned order = magnitude order with ties to the smaller
-// row (the perturbation is below 2^-44 relative, far below the gap between
-// distinct pivot candidates that matters for stability).
-__device__ __forceinline__ unsigned long long pivot_key(double mag, int row) {
-  return (((unsigned long long)__double_as_longlong(mag)) & ~0xffull) | (unsigned long long)(255 - row);
+// Argmax key of a pivot candidate: the high 32 bits of its magnitude (IEEE
+// order = unsigned order for non-negative values) with the low 6 bits replaced
+// by (63 - row), so that one unsigned warp max (redux.sync) finds the largest
+// candidate, ties and near-ties (below 2^-14 relative, for double; 2^-17 for
+// float) going to the smaller row.  Any candidate within that margin of the
+// maximum is as good a partial pivot.  Key 0 = no candidate.
+__device__ __forceinline__ unsigned pivot_key(double mag, int row) {
+  return ((unsigned)__double2hiint(mag) & ~63u) | (unsigned)(63 - row);
 }
-__device__ __forceinline__ unsigned long long warp_max_key(unsigned long long k) {
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) {
-    const unsigned long long q = __shfl_xor_sync(0xffffffffu, k, o);
-    k = q > k ? q : k;
-  }
-  return k;
+__device__ __forceinline__ unsigned pivot_key(float mag, int row) {
+  return (__float_as_uint(mag) & ~63u) | (unsigned)(63 - row);
+}
+__device__ __forceinline__ bool pivot_key_zero(unsigned key) { return (key >> 6) == 0u; }
+
+// Shared-memory store under a predicate, without a branch.
+__device__ __forceinline__ void st_shared_if(Cx<double>* ptr, Cx<double> v, bool pred) {
+  const unsigned a = (unsigned)__cvta_generic_to_shared(ptr);
+  asm volatile(
+      "{\n .reg .pred q;\n setp.ne.u32 q, %3, 0;\n @q st.shared.v2.f64 [%0], {%1, %2};\n}" ::"r"(a),
+      "d"(v.x), "d"(v.y), "r"((unsigned)pred)
+      : "memory");
+}
+__device__ __forceinline__ void st_shared_if(Cx<float>* ptr, Cx<float> v, bool pred) {
+  const unsigned a = (unsigned)__cvta_generic_to_shared(ptr);
+  asm volatile(
+      "{\n .reg .pred q;\n setp.ne.u32 q, %3, 0;\n @q st.shared.v2.f32 [%0], {%1, %2};\n}" ::"r"(a),
+      "f"(v.x), "f"(v.y), "r"((unsigned)pred)
+      : "memory");
+}
+
+// Per-team scratch of the Dyson kernel (the pivot-row exchange buffer lives in
+// the team's G^R tile, which is unused until the elimination ends).
+template <int TT> struct DysonScratch {
+  int pivrow[48];
+  double red[TT / 32];
+  unsigned wkey[2 * (TT / 32)];
+};
+
+// Steps of the elimination unrolled per group (static register indices); the
+// row chunk is rotated by the group width between groups.  Wider groups save
+// the rotation moves, narrower ones keep the loop in the instruction cache.
+#ifndef QCL_GJ_GROUP
+#define QCL_GJ_GROUP 4
+#endif
+template <int NP> struct GjUnroll {
+  static constexpr int COLS = NP / Tile<NP>::CPR;
+  static constexpr int U = COLS % QCL_GJ_GROUP == 0 ? QCL_GJ_GROUP : COLS;
+};
+
+template <typename RS, typename RL, int NP, int TT, int BPC> constexpr size_t dyson_smem() {
+  static_assert(2 * (NP + 1) * sizeof(Cx<RL>) <= NP * NP * sizeof(Cx<RS>), "pivot rows fit the G tile");
+  return 2 * (size_t)BPC * NP * NP * sizeof(Cx<RS>) + BPC * sizeof(DysonScratch<TT>);
+}
+
+// CTAs per SM that the shared memory allows (228 KB per SM, 1 KB reserved per
+// CTA), as the register budget's occupancy target -- but never below 128
+// registers per thread, where the elimination rows would spill.
+template <typename RS, typename RL, int NP, int BPC> constexpr int dyson_min_ctas() {
+  constexpr size_t per = dyson_smem<RS, RL, NP, Tile<NP>::TT, BPC>() + 1024;
+  constexpr int by_smem = (int)((228 * 1024) / per);
+  constexpr int by_regs = 65536 / (BPC * Tile<NP>::TT * 128);
+  constexpr int n = by_smem < by_regs ? by_smem : by_regs;
+  return n < 1 ? 1 : n;
 }
 
 // RS: storage precision, RL: inversion precision, RM: product precision.
 template <typename RS, typename RL, typename RM, int NP, int BPC>
-__global__ void __launch_bounds__(BPC* Tile<NP>::TT) dyson_keldysh_kernel(DysonArgs<RS> p) {
+__global__ void __launch_bounds__(BPC* Tile<NP>::TT, (dyson_min_ctas<RS, RL, NP, BPC>()))
+    dyson_keldysh_kernel(DysonArgs<RS> p) {
   constexpr int CPR = Tile<NP>::CPR, TT = Tile<NP>::TT, COLS = NP / CPR;
+  constexpr int U = GjUnroll<NP>::U, GROUPS = COLS / U;
+  static_assert(COLS % U == 0, "group width must divide the row chunk");
   constexpr size_t MSZ = (size_t)NP * NP;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  Cx<RS>* bufA = reinterpret_cast<Cx<RS>*>(smem_raw);  // BPC matrices: staged Sigma / products
-  Cx<RS>* bufG = bufA + BPC * MSZ;                    // BPC matrices: G^R
-  Cx<RS>* bufT = bufG + BPC * MSZ;                    // BPC matrices: G^R Sigma
-  TeamScratch<RL, NP, TT>* scr = reinterpret_cast<TeamScratch<RL, NP, TT>*>(bufT + BPC * MSZ);
+  Cx<RS>* bufX = reinterpret_cast<Cx<RS>*>(smem_raw);  // BPC tiles: Sigma^R, then Sigma^<,> and products
+  Cx<RS>* bufG = bufX + BPC * MSZ;                    // BPC tiles: pivot rows, then G^R
+  DysonScratch<TT>* scr = reinterpret_cast<DysonScratch<TT>*>(bufG + BPC * MSZ);
 
   const int N = p.N, NE = p.NE, Nk = p.Nk;
   const int m = p.m0 + blockIdx.y;
@@ -74,15 +125,15 @@ __global__ void __launch_bounds__(BPC* Tile<NP>::TT) dyson_keldysh_kernel(DysonA
   const int tt = threadIdx.x % TT;
   const int e = e0 + team;
   const bool live = e < NE;
-  Cx<RS>* A = bufA + team * MSZ;
+  Cx<RS>* X = bufX + team * MSZ;
   Cx<RS>* G = bufG + team * MSZ;
-  Cx<RS>* T = bufT + team * MSZ;
-  TeamScratch<RL, NP, TT>& S = scr[team];
+  Cx<RL>* rowbuf = reinterpret_cast<Cx<RL>*>(G);  // 2 x (NP + 1): row chunks + pivot reciprocal
+  DysonScratch<TT>& S = scr[team];
   const Cx<RS>* first_sig = p.sigL ? p.sigL : p.sigG;
   const bool first_is_L = p.sigL != nullptr;
 
   // ---- stage SigmaR (all copies in flight at once) ---------------------------
-  load_blocks_async<RS, NP, BPC>(p.sigR, bufA, MSZ, e0, m, NE, Nk, N);
+  load_blocks_async<RS, NP, BPC>(p.sigR, bufX, MSZ, e0, m, NE, Nk, N);
   cp_async_wait_all();
   __syncthreads();
 
@@ -98,7 +149,7 @@ __global__ void __launch_bounds__(BPC* Tile<NP>::TT) dyson_keldysh_kernel(DysonA
     Cx<RL> d = cx<RL>(0, 0);
     if (has_row && row < N && col < N) {
       const Cx<double> hv = p.h[(size_t)m + (size_t)Nk * ((size_t)row + (size_t)N * col)];
-      const Cx<RS> sv = A[sw<NP>(row, col)];
+      const Cx<RS> sv = X[sw<NP>(row, col)];
       double re = -hv.x - (double)sv.x, im = -hv.y - (double)sv.y;
       if (row == col) {
         re += eps_e;
@@ -109,9 +160,9 @@ __global__ void __launch_bounds__(BPC* Tile<NP>::TT) dyson_keldysh_kernel(DysonA
     }
     w[j] = d;
   }
-  __syncthreads();  // every team has read its SigmaR tile: bufA is free
+  __syncthreads();  // every team has read its SigmaR tile: bufX is free
   // prefetch the first Keldysh input while the inversion runs
-  if (first_sig && (first_is_L ? p.GL : p.GG)) load_blocks_async<RS, NP, BPC>(first_sig, bufA, MSZ, e0, m, NE, Nk, N);
+  if (first_sig && (first_is_L ? p.GL : p.GG)) load_blocks_async<RS, NP, BPC>(first_sig, bufX, MSZ, e0, m, NE, Nk, N);
 
 #pragma unroll
   for (int o = 1; o < CPR; o <<= 1) rowsum += __shfl_xor_sync(0xffffffffu, rowsum, o);
@@ -125,85 +176,93 @@ __global__ void __launch_bounds__(BPC* Tile<NP>::TT) dyson_keldysh_kernel(DysonA
     if (has_row && row >= N && col == row) w[j] = cx<RL>(1, 0);  // identity padding
   }
 
-  // ---- register-resident Gauss-Jordan with implicit row pivoting -------------
+  // ---- register-resident Gauss-Jordan, implicit pivoting, deferred scaling ----
+  // Step k picks the pivot row p among the unused rows (largest |Re|+|Im| in
+  // column k), every other row i does  w_i[k] = 0;  w_i -= (w_i[k] / w_p[k]) w_p
+  // with w_p[k] replaced by 1, and row p is left unscaled (its column-k entry
+  // becomes 1).  A row that was pivot at step k is then 1 / w_p[k] times the
+  // row of the standard in-place inverse, and it stays that multiple under the
+  // later (linear) updates, so the division by the pivot is applied once per
+  // row at the end instead of to the whole pivot row at every step.
   bool used = !has_row;
   bool singular = !scale_ok;
   int mystep = row;
+  Cx<RL> myrc = cx<RL>(1, 0);
   const int lane = threadIdx.x & 31;
   const int srclane = lane - chunk;  // first lane of this row's chunk group
-  if (tt < NP && tt >= N) S.pivrow[tt] = tt;  // padded steps are identities
-  // The step loop stays rolled (small code, no instruction-cache misses); the
-  // pivot column is picked out of the register row with predicated selects.
 #pragma unroll 1
-  for (int k = 0; k < N; ++k) {
-    const int kc = k / COLS, kj = k - kc * COLS;
-    Cx<RL> wk = w[0];
+  for (int kc = 0; kc < CPR; ++kc) {
+#pragma unroll 1
+    for (int grp = 0; grp < GROUPS; ++grp) {
 #pragma unroll
-    for (int j = 1; j < COLS; ++j)
-      if (j == kj) wk = w[j];
-    const bool cand = !used && chunk == kc;
-    // speculative reciprocal of every candidate (off the argmax critical path)
-    Cx<RL> rc = cx<RL>(0, 0);
-    unsigned long long key = 0ull;
-    if (cand) {
-      key = pivot_key((double)cabs1(wk), row);
-      rc = crecip_scaled(wk);
-    }
-    key = warp_max_key(key);
-    if (TT > 32) {
-      if (lane == 0) S.wkey[tt >> 5] = key;
-      team_sync<TT>(team);
+      for (int u = 0; u < U; ++u) {
+        // Steps k >= N (padding) pick the identity rows and change nothing.
+        const int k = kc * COLS + grp * U + u;
+        const Cx<RL> wk = w[u];  // column k in the lanes of chunk kc (rotated chunk)
+        const bool cand = !used && chunk == kc;
+        const Cx<RL> rc = crecip_pivot(wk);  // speculative, off the argmax path
+        unsigned key = cand ? pivot_key(cabs1(wk), row) : 0u;
+        key = __reduce_max_sync(0xffffffffu, key);
+        if (TT > 32) {
+          if (lane == 0) S.wkey[(k & 1) * (TT / 32) + (tt >> 5)] = key;
+          team_sync<TT>(team);
 #pragma unroll
-      for (int q = 0; q < TT / 32; ++q) {
-        const unsigned long long o = S.wkey[q];
-        key = o > key ? o : key;
+          for (int q = 0; q < TT / 32; ++q) key = max(key, S.wkey[(k & 1) * (TT / 32) + q]);
+        }
+        const int best = 63 - (int)(key & 63u);
+        const bool zero = pivot_key_zero(key);
+        singular |= zero;
+        if (tt == 0) S.pivrow[k] = best;
+        Cx<RL> f = wk;
+        if (CPR > 1) {
+          f.x = __shfl_sync(0xffffffffu, wk.x, srclane + kc);
+          f.y = __shfl_sync(0xffffffffu, wk.y, srclane + kc);
+        }
+        const bool is_pivot = row == best;
+        if (chunk == kc) w[u] = is_pivot ? cx<RL>(1, 0) : cx<RL>(0, 0);
+        Cx<RL>* rb = rowbuf + (k & 1) * (NP + 1);
+#pragma unroll
+        for (int j = 0; j < COLS; ++j) st_shared_if(rb + chunk * COLS + j, w[j], is_pivot);
+        Cx<RL> rp;
+        if (TT == 32) {
+          const int plane = (best * CPR + kc) & 31;
+          rp.x = __shfl_sync(0xffffffffu, rc.x, plane);
+          rp.y = __shfl_sync(0xffffffffu, rc.y, plane);
+          team_sync<TT>(team);
+        } else {
+          st_shared_if(rb + NP, rc, is_pivot && chunk == kc);
+          team_sync<TT>(team);
+          rp = rb[NP];
+        }
+        if (zero) rp = cx<RL>(0, 0);
+        used |= is_pivot;
+        mystep = is_pivot ? k : mystep;
+        myrc = is_pivot ? rp : myrc;
+        const Cx<RL> fp = is_pivot ? cx<RL>(0, 0) : f * rp;
+#pragma unroll
+        for (int j = 0; j < COLS; ++j) cfms(w[j], fp, rb[chunk * COLS + j]);
       }
-    }
-    const int best = 255 - (int)(key & 0xffull);
-    const bool zero = (key >> 8) == 0ull;
-    if (zero) singular = true;
-    if (tt == 0) S.pivrow[k] = best;
-    // multiplier of this row and (for the pivot row) its reciprocal
-    Cx<RL> f = wk;
-    if (CPR > 1) {
-      f.x = __shfl_sync(0xffffffffu, wk.x, srclane + kc);
-      f.y = __shfl_sync(0xffffffffu, wk.y, srclane + kc);
-      rc.x = __shfl_sync(0xffffffffu, rc.x, srclane + kc);
-      rc.y = __shfl_sync(0xffffffffu, rc.y, srclane + kc);
-    }
-    Cx<RL>* rb = S.rowbuf[k & 1];
-    const bool is_pivot = has_row && row == best;
-    const Cx<RL> colk = is_pivot ? cx<RL>(1, 0) : cx<RL>(0, 0);
-    if (chunk == kc) {
+      if (GROUPS > 1) {  // rotate the chunk so that the next group is at w[0..U)
+        Cx<RL> t[U];
 #pragma unroll
-      for (int j = 0; j < COLS; ++j)
-        if (j == kj) w[j] = colk;
-    }
-    if (is_pivot) {
-      const Cx<RL> inv = zero ? cx<RL>(0, 0) : rc;
+        for (int j = 0; j < U; ++j) t[j] = w[j];
 #pragma unroll
-      for (int j = 0; j < COLS; ++j) {
-        w[j] = w[j] * inv;
-        rb[chunk * COLS + j] = w[j];
+        for (int j = 0; j < COLS - U; ++j) w[j] = w[j + U];
+#pragma unroll
+        for (int j = 0; j < U; ++j) w[COLS - U + j] = t[j];
       }
-      used = true;
-      mystep = k;
-    }
-    team_sync<TT>(team);
-    if (has_row && !is_pivot) {
-#pragma unroll
-      for (int j = 0; j < COLS; ++j) cfms(w[j], f, rb[chunk * COLS + j]);
     }
   }
   team_sync<TT>(team);
   if (singular && live && tt == 0) record_status(p.status, QCL_SINGULAR, (long long)e + (long long)NE * m);
-  // inverse(D/s)[step][pivrow[k']] = w[k'];  GR = that / s
+  // inverse(D/s)[step][pivrow[k']] = w[k'] / pivot(step);  GR = that / s
   if (has_row) {
+    const Cx<RL> rs = inv_s * myrc;
 #pragma unroll
     for (int j = 0; j < COLS; ++j) {
       const int kp = chunk * COLS + j;
       const int col = S.pivrow[kp];
-      Cx<RL> g = inv_s * w[j];
+      Cx<RL> g = rs * w[j];
       if (mystep >= N || col >= N) g = cx<RL>(0, 0);
       G[sw<NP>(mystep, col)] = cvt<RS>(g);
     }
@@ -212,7 +271,7 @@ __global__ void __launch_bounds__(BPC* Tile<NP>::TT) dyson_keldysh_kernel(DysonA
   __syncthreads();
   if (p.GR) store_blocks<RS, RS, NP, BPC>(p.GR, bufG, MSZ, e0, m, NE, Nk, N);
 
-  // ---- Keldysh products ------------------------------------------------------
+  // ---- Keldysh products: X = G (X G^H), product tiles in registers ----------
   bool prefetched = first_sig && (first_is_L ? p.GL : p.GG);
   for (int which = 0; which < 2; ++which) {
     const Cx<RS>* sig = which == 0 ? p.sigL : p.sigG;
@@ -220,20 +279,25 @@ __global__ void __launch_bounds__(BPC* Tile<NP>::TT) dyson_keldysh_kernel(DysonA
     Cx<double>* tr = which == 0 ? p.traceL : p.traceG;
     if (sig == nullptr || out == nullptr) continue;  // uniform
     if (!prefetched) {
-      __syncthreads();  // previous store out of bufA is complete
-      load_blocks_async<RS, NP, BPC>(sig, bufA, MSZ, e0, m, NE, Nk, N);
+      __syncthreads();  // previous store out of bufX is complete
+      load_blocks_async<RS, NP, BPC>(sig, bufX, MSZ, e0, m, NE, Nk, N);
     }
     prefetched = false;
     cp_async_wait_all();
     __syncthreads();
-    team_matmul<RS, RM, NP>(G, A, T, N, tt, false);
+    MatTile<RM, NP> acc;
+    team_matmul_regs<RS, RM, NP>(G, X, acc, N, tt, false);  // T = G Sigma
     team_sync<TT>(team);
-    team_matmul<RS, RM, NP>(T, G, A, N, tt, true);
+    team_store_regs<RS, RM, NP>(X, acc, tt);
+    team_sync<TT>(team);
+    team_matmul_regs<RS, RM, NP>(X, G, acc, N, tt, true);  // T G^H
+    team_sync<TT>(team);
+    team_store_regs<RS, RM, NP>(X, acc, tt);
     team_sync<TT>(team);
     if (tr) {
       double re = 0, im = 0;
       if (tt < N) {
-        const Cx<RS> d = A[sw<NP>(tt, tt)];
+        const Cx<RS> d = X[sw<NP>(tt, tt)];
         re = d.x;
         im = d.y;
       }
@@ -242,12 +306,8 @@ __global__ void __launch_bounds__(BPC* Tile<NP>::TT) dyson_keldysh_kernel(DysonA
       if (tt == 0 && live) tr[(size_t)e + (size_t)NE * m] = cx<double>(re, im);
     }
     __syncthreads();
-    store_blocks<RS, RS, NP, BPC>(out, bufA, MSZ, e0, m, NE, Nk, N);
+    store_blocks<RS, RS, NP, BPC>(out, bufX, MSZ, e0, m, NE, Nk, N);
   }
-}
-
-template <typename RS, typename RL, int NP, int TT, int BPC> constexpr size_t dyson_smem() {
-  return 3 * (size_t)BPC * NP * NP * sizeof(Cx<RS>) + BPC * sizeof(TeamScratch<RL, NP, TT>);
 }
 
 template <typename RS, typename RL, typename RM, int NP, int BPC>

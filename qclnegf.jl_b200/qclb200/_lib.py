@@ -13,7 +13,7 @@ import re
 _HERE = os.path.dirname(os.path.abspath(__file__))
 PKG_ROOT = os.path.dirname(_HERE)
 REPO_ROOT = os.path.dirname(PKG_ROOT)
-LIB_PATH = os.path.join(PKG_ROOT, "lib", "libqclb200.so")
+LIB_PATH = os.environ.get("QCLB200_LIB") or os.path.join(PKG_ROOT, "lib", "libqclb200.so")
 HEADER_PATH = os.path.join(REPO_ROOT, "include", "qclb200.h")
 
 QCL_OK = 0

@@ -24,6 +24,7 @@
 //   y_2L[n] = (y_L[n] + W_2L^{-n} IFFT_L(FFT_L(x W_2L^n) .* K2L_odd)[n]) / 2.
 // So verification costs two extra length-L FFTs instead of two length-2L
 // ones, and the same per-column partial sums of |y_2L - y_L|^2 and |y_L|^2.
+
 #include <math.h>
 
 #include <algorithm>
@@ -34,6 +35,16 @@
 namespace qcl {
 
 __device__ __forceinline__ int fpad(int p) { return p + (p >> 4); }
+
+// Read-only (non-coherent cache) loads of the constant tables.
+__device__ __forceinline__ Cx<double> ldg_cx(const Cx<double>* p) {
+  const double2 v = __ldg(reinterpret_cast<const double2*>(p));
+  return cx<double>(v.x, v.y);
+}
+__device__ __forceinline__ Cx<float> ldg_cx(const Cx<float>* p) {
+  const float2 v = __ldg(reinterpret_cast<const float2*>(p));
+  return cx<float>(v.x, v.y);
+}
 
 // W_16^t = exp(-2 pi i t / 16); multiply z by W_16^t (t compile-time).
 template <typename R, int t> __device__ __forceinline__ Cx<R> w16mul(Cx<R> z) {
@@ -105,33 +116,91 @@ template <int L> struct FftPlan {
   static constexpr int T = (L / 16 >= 32) ? L / 16 : 32;
 };
 
+// Pass adaptors: a pass reads its inputs through In(i) and writes its outputs
+// through Out(t, v), so that the first pass can read the field from global
+// memory and the last pass can multiply by the kernel spectrum or write the
+// result straight to global memory, without extra shared-memory sweeps.
+template <typename R> struct SmemIn {
+  static constexpr bool kShared = true;
+  const Cx<R>* buf;
+  __device__ __forceinline__ Cx<R> operator()(int i) const { return buf[fpad(i)]; }
+};
+template <typename R> struct SmemOut {
+  Cx<R>* buf;
+  __device__ __forceinline__ void operator()(int t, Cx<R> v) const { buf[fpad(t)] = v; }
+};
+// conj(v * K[t]) into shared memory: the spectrum product, conjugated so that
+// the next forward transform computes the inverse one (IFFT(X) = conj(FFT(conj X)) / L).
+template <typename R> struct SpectrumOut {
+  Cx<R>* buf;
+  const Cx<R>* __restrict__ K;
+  __device__ __forceinline__ void operator()(int t, Cx<R> v) const { buf[fpad(t)] = conj(v * ldg_cx(K + t)); }
+};
+
+// v * W_{2H}^k for compile-time k (H a power of two, 2H <= 16).
+template <typename R, int H, int k> __device__ __forceinline__ Cx<R> w2h_mul(Cx<R> d) {
+  switch ((k * 8 / H) & 15) {
+    case 0: return d;
+    case 1: return w16mul<R, 1>(d);
+    case 2: return w16mul<R, 2>(d);
+    case 3: return w16mul<R, 3>(d);
+    case 4: return w16mul<R, 4>(d);
+    case 5: return w16mul<R, 5>(d);
+    case 6: return w16mul<R, 6>(d);
+    default: return w16mul<R, 7>(d);
+  }
+}
+template <typename R, int H, int K> struct ZeroHiStage {
+  // first DIF stage when v[H..2H) are zero: v[k] stays, v[k + H] = v[k] W_{2H}^k
+  __device__ __forceinline__ static void run(Cx<R>* v) {
+    v[K - 1 + H] = w2h_mul<R, H, K - 1>(v[K - 1]);
+    ZeroHiStage<R, H, K - 1>::run(v);
+  }
+};
+template <typename R, int H> struct ZeroHiStage<R, H, 0> {
+  __device__ __forceinline__ static void run(Cx<R>*) {}
+};
+
 // One mixed-radix Stockham pass (natural-order output after all passes).
-template <typename R, int L, int RADIX, int NS>
-__device__ __forceinline__ void stockham_pass(Cx<R>* buf, const Cx<R>* __restrict__ tw) {
+// ZHI: the inputs of slots r >= RADIX/2 are known to be zero (the padding).
+template <typename R, int L, int RADIX, int NS, bool ZHI, typename In, typename Out>
+__device__ __forceinline__ void stockham_pass(const In& in, const Out& out, const Cx<R>* __restrict__ tw) {
+  const int tid = threadIdx.x;
   constexpr int T = FftPlan<L>::T;
   constexpr int NB = L / RADIX;
   constexpr int Q = (NB + T - 1) / T;
+  constexpr int RIN = ZHI ? RADIX / 2 : RADIX;
+  static_assert(!ZHI || NS == 1, "pruned inputs only in the first pass");
+  // One twiddle-table load per butterfly, issued first (read-only path) so
+  // that its latency overlaps the shared-memory reads and the barrier.
+  Cx<R> w1[Q];
+  if (NS > 1) {
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+      const int j = tid + q * T;
+      w1[q] = ldg_cx(tw + (j < NB ? (j % NS) * (L / (NS * RADIX)) : 0));
+    }
+  }
   Cx<R> v[Q][RADIX];
 #pragma unroll
   for (int q = 0; q < Q; ++q) {
-    const int j = threadIdx.x + q * T;
+    const int j = tid + q * T;
     if (j < NB) {
 #pragma unroll
-      for (int r = 0; r < RADIX; ++r) v[q][r] = buf[fpad(j + r * NB)];
+      for (int r = 0; r < RIN; ++r) v[q][r] = in(j + r * NB);
     }
   }
-  __syncthreads();
+  if (In::kShared) __syncthreads();  // in place: every read before any write
 #pragma unroll
   for (int q = 0; q < Q; ++q) {
-    const int j = threadIdx.x + q * T;
+    const int j = tid + q * T;
     if (j < NB) {
       const int k = j % NS;
       if (NS > 1) {
-        // One table load per butterfly: w_r = w_1^r by binary powering
-        // (products of at most four factors, so the twiddle error stays a
-        // few ulps), instead of RADIX - 1 dependent global loads.
+        // w_r = w_1^r by binary powering (products of at most four factors, so
+        // the twiddle error stays a few ulps) instead of RADIX - 1 table loads.
         Cx<R> w[RADIX];
-        w[1] = tw[k * (L / (NS * RADIX))];
+        w[1] = w1[q];
 #pragma unroll
         for (int r = 2; r < RADIX; ++r) {
           const int hi = (r & (r - 1)) ? (r & (r - 1)) : r / 2;  // r = hi + lo, hi >= lo
@@ -140,31 +209,51 @@ __device__ __forceinline__ void stockham_pass(Cx<R>* buf, const Cx<R>* __restric
 #pragma unroll
         for (int r = 1; r < RADIX; ++r) v[q][r] = v[q][r] * w[r];
       }
-      DifStage<R, RADIX, RADIX / 2>::run(v[q]);
+      if (ZHI) {
+        ZeroHiStage<R, RADIX / 2, RADIX / 2>::run(v[q]);
+        DifStage<R, RADIX, RADIX / 4>::run(v[q]);
+      } else {
+        DifStage<R, RADIX, RADIX / 2>::run(v[q]);
+      }
       const int idxD = (j / NS) * NS * RADIX + k;
 #pragma unroll
-      for (int r = 0; r < RADIX; ++r) buf[fpad(idxD + r * NS)] = v[q][bitrev<RADIX>(r)];
+      for (int r = 0; r < RADIX; ++r) out(idxD + r * NS, v[q][bitrev<RADIX>(r)]);
     }
   }
   __syncthreads();
 }
 
-// Forward FFT of length L in shared memory (padded indexing), natural order.
-template <typename R, int L> __device__ __forceinline__ void fft_smem(Cx<R>* buf, const Cx<R>* tw) {
+// Forward FFT of length L: first pass reads through `in`, last pass writes
+// through `out`, the passes between work in place on `buf` (padded indexing).
+// ZHI: the input is zero on [L/2, L) (the zero padding of the convolution).
+template <typename R, int L, bool ZHI, typename In, typename Out>
+__device__ __forceinline__ void fft_run(const In& in, const Out& out, Cx<R>* buf, const Cx<R>* tw) {
   static_assert(L >= 64 && L <= 16384, "unsupported FFT length");
-  stockham_pass<R, L, 16, 1>(buf, tw);
+  const SmemIn<R> si{buf};
+  const SmemOut<R> so{buf};
   if constexpr (L == 64) {
-    stockham_pass<R, L, 4, 16>(buf, tw);
+    stockham_pass<R, L, 16, 1, ZHI>(in, so, tw);
+    stockham_pass<R, L, 4, 16, false>(si, out, tw);
   } else if constexpr (L == 128) {
-    stockham_pass<R, L, 8, 16>(buf, tw);
+    stockham_pass<R, L, 16, 1, ZHI>(in, so, tw);
+    stockham_pass<R, L, 8, 16, false>(si, out, tw);
+  } else if constexpr (L == 256) {
+    stockham_pass<R, L, 16, 1, ZHI>(in, so, tw);
+    stockham_pass<R, L, 16, 16, false>(si, out, tw);
+  } else if constexpr (L <= 2048) {
+    // small radix first: with the zero half pruned it is a plain copy
+    stockham_pass<R, L, L / 256, 1, ZHI>(in, so, tw);
+    stockham_pass<R, L, 16, L / 256, false>(si, so, tw);
+    stockham_pass<R, L, 16, L / 16, false>(si, out, tw);
+  } else if constexpr (L == 4096) {
+    stockham_pass<R, L, 16, 1, ZHI>(in, so, tw);
+    stockham_pass<R, L, 16, 16, false>(si, so, tw);
+    stockham_pass<R, L, 16, 256, false>(si, out, tw);
   } else {
-    stockham_pass<R, L, 16, 16>(buf, tw);
-    if constexpr (L == 512) stockham_pass<R, L, 2, 256>(buf, tw);
-    if constexpr (L == 1024) stockham_pass<R, L, 4, 256>(buf, tw);
-    if constexpr (L == 2048) stockham_pass<R, L, 8, 256>(buf, tw);
-    if constexpr (L >= 4096) stockham_pass<R, L, 16, 256>(buf, tw);
-    if constexpr (L == 8192) stockham_pass<R, L, 2, 4096>(buf, tw);
-    if constexpr (L == 16384) stockham_pass<R, L, 4, 4096>(buf, tw);
+    stockham_pass<R, L, L / 4096, 1, ZHI>(in, so, tw);
+    stockham_pass<R, L, 16, L / 4096, false>(si, so, tw);
+    stockham_pass<R, L, 16, L / 256, false>(si, so, tw);
+    stockham_pass<R, L, 16, L / 16, false>(si, out, tw);
   }
 }
 
@@ -195,7 +284,44 @@ __device__ __forceinline__ Cx<R> gamma_at(const HilbertArgs<R>& p, size_t idx) {
   return p.Gam[idx];
 }
 
-template <typename R, int L>
+// x_e = wE_e Gam_e (times the twist W_2L^e for the odd-frequency half), zero
+// for e >= N_E; optionally copies Gam out.
+template <typename R> struct FieldIn {
+  static constexpr bool kShared = false;
+  const HilbertArgs<R>* p;
+  size_t base;
+  bool twist;
+  __device__ __forceinline__ Cx<R> operator()(int e) const {
+    if (e >= p->NE) return cx<R>(0, 0);
+    Cx<R> g = gamma_at(*p, base + e);
+    if (twist) {
+      g = g * ldg_cx(p->twist + e);
+    } else if (p->GamOut) {
+      p->GamOut[base + e] = g;
+    }
+    return (R)__ldg(p->wE + e) * g;
+  }
+};
+// Lam_e = conj(y[e + NE - 1]) / L straight to global memory (or the fused
+// SR_e = Lam_e - i Gam_e / 2); outputs outside [NE - 1, 2 NE - 2] are dropped.
+template <typename R> struct ResultOut {
+  const HilbertArgs<R>* p;
+  size_t base;
+  __device__ __forceinline__ void operator()(int t, Cx<R> v) const {
+    const int e = t - (p->NE - 1);
+    if (e < 0 || e >= p->NE) return;
+    const R sc = (R)p->scale_out;
+    const Cx<R> lam = cx<R>(sc * v.x, -sc * v.y);
+    if (p->SR) {
+      const Cx<R> g = gamma_at(*p, base + e);
+      p->SR[base + e] = cx<R>(lam.x + (R)0.5 * g.y, lam.y - (R)0.5 * g.x);
+    } else {
+      p->Lam[base + e] = lam;
+    }
+  }
+};
+
+template <typename R, int L, bool VERIFY>
 __global__ void __launch_bounds__(FftPlan<L>::T) hilbert_kernel(HilbertArgs<R> p) {
   constexpr int T = FftPlan<L>::T;
   constexpr int PER = (L / 2 + T - 1) / T;  // outputs per thread (NE <= L/2 + 1)
@@ -205,54 +331,28 @@ __global__ void __launch_bounds__(FftPlan<L>::T) hilbert_kernel(HilbertArgs<R> p
   if (col >= p.ncols) return;
   const int NE = p.NE;
   const size_t base = (size_t)col * NE;
-  const bool verify = p.partial != nullptr;
+  const SmemIn<R> si{buf};
+  const SmemOut<R> so{buf};
 
-  // x = wE .* Gam, zero padded
-  for (int e = threadIdx.x; e < L; e += T) {
-    Cx<R> x = cx<R>(0, 0);
-    if (e < NE) {
-      Cx<R> g = gamma_at(p, base + e);
-      if (p.GamOut) p.GamOut[base + e] = g;
-      x = (R)p.wE[e] * g;
-    }
-    buf[fpad(e)] = x;
+  // forward transform of the padded column, times the kernel spectrum
+  fft_run<R, L, true>(FieldIn<R>{&p, base, false}, SpectrumOut<R>{buf, p.khat}, buf, p.tw);
+  if constexpr (!VERIFY) {
+    // inverse transform, results written from registers
+    fft_run<R, L, false>(si, ResultOut<R>{&p, base}, buf, p.tw);
+    return;
   }
-  __syncthreads();
-  fft_smem<R, L>(buf, p.tw);
-  for (int t = threadIdx.x; t < L; t += T) buf[fpad(t)] = conj(buf[fpad(t)] * p.khat[t]);
-  __syncthreads();
-  fft_smem<R, L>(buf, p.tw);
+  fft_run<R, L, false>(si, so, buf, p.tw);
   Cx<R> lam[PER];
   const R sc = (R)p.scale_out;
 #pragma unroll
   for (int q = 0; q < PER; ++q) {
     const int e = threadIdx.x + q * T;
-    if (e < NE) {
-      Cx<R> y = conj(buf[fpad(e + NE - 1)]);
-      lam[q] = sc * y;
-      if (!verify) {
-        if (p.SR) {
-          Cx<R> g = gamma_at(p, base + e);
-          p.SR[base + e] = cx<R>(lam[q].x + (R)0.5 * g.y, lam[q].y - (R)0.5 * g.x);
-        } else {
-          p.Lam[base + e] = lam[q];
-        }
-      }
-    }
+    if (e < NE) lam[q] = sc * conj(buf[fpad(e + NE - 1)]);
   }
-  if (!verify) return;
+  __syncthreads();
   // ---- odd-frequency half of the length-2L transform -------------------------
-  __syncthreads();
-  for (int e = threadIdx.x; e < L; e += T) {
-    Cx<R> x = cx<R>(0, 0);
-    if (e < NE) x = (R)p.wE[e] * (gamma_at(p, base + e) * p.twist[e]);
-    buf[fpad(e)] = x;
-  }
-  __syncthreads();
-  fft_smem<R, L>(buf, p.tw);
-  for (int t = threadIdx.x; t < L; t += T) buf[fpad(t)] = conj(buf[fpad(t)] * p.kodd[t]);
-  __syncthreads();
-  fft_smem<R, L>(buf, p.tw);
+  fft_run<R, L, true>(FieldIn<R>{&p, base, true}, SpectrumOut<R>{buf, p.kodd}, buf, p.tw);
+  fft_run<R, L, false>(si, so, buf, p.tw);
   double dsum = 0, lsum = 0;
 #pragma unroll
   for (int q = 0; q < PER; ++q) {
@@ -427,20 +527,23 @@ int ensure_partial(HilbertTables& t, long long ncols) {
   return QCL_OK;
 }
 
-template <typename R, int L> static int launch_hilbert_L(const HilbertArgs<R>& a, cudaStream_t st) {
+template <typename R, int L, bool VERIFY> static int launch_hilbert_LV(const HilbertArgs<R>& a, cudaStream_t st) {
   constexpr int T = FftPlan<L>::T;
   constexpr size_t smem = (size_t)(L + L / 16) * sizeof(Cx<R>);
   static bool configured = false;
   if (!configured) {
-    QCL_CUDA_CHECK(cudaFuncSetAttribute(hilbert_kernel<R, L>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    QCL_CUDA_CHECK(cudaFuncSetAttribute(hilbert_kernel<R, L, VERIFY>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                         (int)smem));
     configured = true;
   }
   const long long nc = a.ncols;
   dim3 grid((unsigned)(nc < 65535 ? nc : 65535), (unsigned)((nc + 65534) / 65535));
-  hilbert_kernel<R, L><<<grid, T, smem, st>>>(a);
+  hilbert_kernel<R, L, VERIFY><<<grid, T, smem, st>>>(a);
   QCL_LAUNCH_CHECK("hilbert_kernel");
   return QCL_OK;
+}
+template <typename R, int L> static int launch_hilbert_L(const HilbertArgs<R>& a, cudaStream_t st) {
+  return a.partial ? launch_hilbert_LV<R, L, true>(a, st) : launch_hilbert_LV<R, L, false>(a, st);
 }
 
 template <typename R> static int launch_hilbert_t(const HilbertArgs<R>& a, int L, cudaStream_t st) {

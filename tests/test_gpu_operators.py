@@ -93,6 +93,11 @@ def test_fft_hilbert_c128_matches_direct_pv(gpu_ops, orc, NE):
     # roundoff agrees in magnitude with the oracle's 2L rerun
     _, ro = orc.fft_hilbert(G, eps, w, return_roundoff=True)
     assert r < 100 * ro + 1e-15
+    # the transform without the roundoff rerun (its own kernel instance) gives
+    # the same values
+    Lam2 = gpu_ops.fft_hilbert_transform(G, eps, w)
+    assert approx_err(Lam2, direct) < 2e-13
+    assert np.max(np.abs(Lam2 - Lam)) <= 1e-13 * max(np.max(np.abs(Lam)), 1.0)
 
 
 @pytest.mark.parametrize("NE", [400, 4096])
@@ -104,13 +109,16 @@ def test_fft_hilbert_c64(gpu_ops, orc, NE):
     G = np.asfortranarray(rng.standard_normal((NE, 4)) + 1j * rng.standard_normal((NE, 4)))
     Lam, r = gpu_ops.fft_hilbert_transform(G, eps, w, precision="c64", return_roundoff=True)
     assert Lam.dtype == np.complex64
-    assert approx_err(Lam, orc.direct_hilbert(G, eps, w)) < 1e-5
+    direct = orc.direct_hilbert(G, eps, w)
+    assert approx_err(Lam, direct) < 1e-5
     assert r < 1e-5
+    assert approx_err(gpu_ops.fft_hilbert_transform(G, eps, w, precision="c64"), direct) < 1e-5
 
 
-def test_retarded_self_energy_fft_matches_oracle(gpu_ops, orc):
+@pytest.mark.parametrize("NE", [37, 2500])
+def test_retarded_self_energy_fft_matches_oracle(gpu_ops, orc, NE):
     rng = np.random.default_rng(0xFF71)
-    NE, Nk, Nb = 37, 2, 2
+    Nk, Nb = 2, 2
     eps = np.linspace(-1.3, 0.9, NE)
     w = np.full(NE, eps[1] - eps[0])
     w[[0, -1]] /= 2
@@ -121,6 +129,9 @@ def test_retarded_self_energy_fft_matches_oracle(gpu_ops, orc):
     assert np.array_equal(Gam, oGam)
     assert approx_err(SR, oSR) < 2e-13
     assert r < 1e-12
+    SR2, Gam2 = gpu_ops.retarded_self_energy_fft(SL, SG, eps, w)
+    assert np.array_equal(Gam2, oGam)
+    assert approx_err(SR2, oSR) < 2e-13
 
 
 # ---------------------------------------------------------------------------

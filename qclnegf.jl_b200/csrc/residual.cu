@@ -12,12 +12,16 @@
 //   r_caus = max_em max(0, lmax(Im_H SR)) / (||SR||_2 + 1e-14)
 // with D = eps I - h - SR_total, Gam = i(S>_total - S<_total), A = i(G - G^H).
 //
-// B200 mapping: one team per (E,k) block as in the Dyson kernel; the Hermitian
-// eigenvalues (LAPACK zheev in the reference, residuals.jl:311-353) come from a
-// team-parallel complex Jacobi iteration (round-robin pairing, all rotations
-// of a round applied at once), the spectral norm of SR (zgesvd, :355-409) from
-// the same solver on SR SR^H, needed only when lmax(Im SR) > 0.  Per-block
-// partial results go to global memory and are reduced in a fixed order.
+// B200 mapping: one team per (E,k) block as in the Dyson kernel.  Only the
+// extreme Hermitian eigenvalues enter the suite (LAPACK zheev in the
+// reference, residuals.jl:311-353): each matrix is reduced to real
+// tridiagonal form by team-parallel Householder steps, and Sturm counts on the
+// tridiagonal settle the positive (causal) case with one count; lmin / lmax
+// are found by multisection only for indefinite blocks.  The spectral norm of
+// SR (zgesvd, :355-409) is lmax(SR SR^H), needed only when lmax(Im SR) > 0.
+// The full spectrum (qcl_hermitian_eigvals) uses a team-parallel complex
+// Jacobi iteration.  Per-block partial results go to global memory and are
+// reduced in a fixed order.
 #include <mutex>
 
 #include "blockmat.cuh"
@@ -47,6 +51,8 @@ template <int NP> struct ResScratch {
   JacobiRot rot[NP / 2];
   double red[8];
   double vals[NP];
+  double d[NP], e2[NP];  // tridiagonal form
+  Cx<double> u[NP], w[NP];
 };
 
 // Team sum of two doubles (fixed order).
@@ -158,22 +164,148 @@ __device__ bool hermitian_part(const Cx<double>* X, Cx<double> f, Cx<double>* H,
   return bad == 0;
 }
 
-// Positivity ratio of the (already Hermitian) H.
+// ---- extreme eigenvalues through a tridiagonal form ---------------------------
+// Householder reduction of the Hermitian N x N tile H (destroyed) to a real
+// symmetric tridiagonal matrix with the same eigenvalues: S.d[0..N) its
+// diagonal, S.e2[0..N-1) its squared off-diagonal.  Step k applies the
+// Hermitian unitary reflector P = I - c u u^H that maps column k below the
+// diagonal onto its first entry, as the rank-2 update of the trailing block
+//   A <- P A P = A - u w^H - w u^H,  p = c A u,  w = p - (c/2)(u^H p) u
+// (Golub & Van Loan, Matrix Computations, sec. 8.3.1).  One team thread per
+// row of the trailing block; backward stable like LAPACK's zhetrd.
+template <int NP, int TT>
+__device__ void team_tridiagonalize(Cx<double>* H, int N, int tt, ResScratch<NP>& S, int team) {
+  for (int k = 0; k + 2 < N; ++k) {
+    const int m = N - k - 1;  // entries below the diagonal in column k
+    const Cx<double> xi = tt < m ? H[sw<NP>(k + 1 + tt, k)] : cx<double>(0, 0);
+    const double a2 = team_sum<TT>(xi.x * xi.x + xi.y * xi.y, tt, S.red, team);
+    const Cx<double> x0 = H[sw<NP>(k + 1, k)];
+    if (tt == 0) {
+      S.d[k] = H[sw<NP>(k, k)].x;
+      S.e2[k] = a2;
+    }
+    if (!(a2 > 0)) {  // team-uniform: column already reduced
+      team_sync<TT>(team);
+      continue;
+    }
+    const double alpha = sqrt(a2), ax0 = hypot(x0.x, x0.y);
+    const Cx<double> ph = ax0 > 0 ? cx<double>(x0.x / ax0, x0.y / ax0) : cx<double>(1, 0);
+    const double c = 1.0 / (alpha * (alpha + ax0));
+    const Cx<double> ui = tt == 0 ? cx<double>(x0.x + alpha * ph.x, x0.y + alpha * ph.y) : xi;
+    if (tt < m) S.u[tt] = ui;
+    team_sync<TT>(team);
+    Cx<double> pv = cx<double>(0, 0);
+    if (tt < m) {
+      for (int j = 0; j < m; ++j) cfma(pv, H[sw<NP>(k + 1 + tt, k + 1 + j)], S.u[j]);
+      pv = c * pv;
+    }
+    const double kk = 0.5 * c * team_sum<TT>(tt < m ? ui.x * pv.x + ui.y * pv.y : 0.0, tt, S.red, team);
+    if (tt < m) S.w[tt] = cx<double>(pv.x - kk * ui.x, pv.y - kk * ui.y);
+    team_sync<TT>(team);
+    for (int idx = tt; idx < m * m; idx += TT) {
+      const int i = idx % m, j = idx / m;
+      Cx<double>& a = H[sw<NP>(k + 1 + i, k + 1 + j)];
+      const Cx<double> t = S.u[i] * conj(S.w[j]) + S.w[i] * conj(S.u[j]);
+      a = cx<double>(a.x - t.x, a.y - t.y);
+    }
+    team_sync<TT>(team);
+  }
+  if (tt == 0) {
+    if (N >= 2) {
+      const Cx<double> t = H[sw<NP>(N - 1, N - 2)];
+      S.d[N - 2] = H[sw<NP>(N - 2, N - 2)].x;
+      S.e2[N - 2] = t.x * t.x + t.y * t.y;
+    }
+    S.d[N - 1] = H[sw<NP>(N - 1, N - 1)].x;
+  }
+  team_sync<TT>(team);
+}
+
+// Number of eigenvalues of the tridiagonal (d, e2) below sigma (Sturm
+// sequence / LDL^T inertia, pivots clamped away from zero as in LAPACK dstebz).
+__device__ __forceinline__ int sturm_count(const double* d, const double* e2, int N, double sigma, double pivmin) {
+  double q = d[0] - sigma;
+  if (fabs(q) < pivmin) q = -pivmin;
+  int c = q < 0;
+  for (int i = 1; i < N; ++i) {
+    q = (d[i] - sigma) - e2[i - 1] / q;
+    if (fabs(q) < pivmin) q = -pivmin;
+    c += q < 0;
+  }
+  return c;
+}
+
+__device__ __forceinline__ double tri_pivmin(const double* e2, int N) {
+  double emax = 0;
+  for (int i = 0; i + 1 < N; ++i) emax = fmax(emax, e2[i]);
+  return 2.2250738585072014e-308 * fmax(1.0, emax);
+}
+
+// kth smallest eigenvalue (kth = 1..N) of the tridiagonal by multisection of
+// the Gershgorin interval: each warp evaluates the same 32 shifts per round
+// (every lane of the team ends with the same interval, no exchange needed),
+// until the interval is a few ulps wide.
+__device__ double tri_eig(const double* d, const double* e2, int N, int kth) {
+  constexpr double eps = 2.220446049250313e-16;
+  double lo = INFINITY, hi = -INFINITY;
+  for (int i = 0; i < N; ++i) {
+    const double r = (i > 0 ? sqrt(e2[i - 1]) : 0.0) + (i + 1 < N ? sqrt(e2[i]) : 0.0);
+    lo = fmin(lo, d[i] - r);
+    hi = fmax(hi, d[i] + r);
+  }
+  const double pivmin = tri_pivmin(e2, N);
+  const double tnorm = fmax(fabs(lo), fabs(hi));
+  lo -= 2 * eps * tnorm * N + 2 * pivmin;
+  hi += 2 * eps * tnorm * N + 2 * pivmin;
+  const int lane = threadIdx.x & 31;
+  for (int round = 0; round < 64; ++round) {
+    if (hi - lo <= 2 * eps * fmax(fabs(lo), fabs(hi)) + pivmin) break;
+    const double width = hi - lo;
+    const double sig = lo + width * (double)(lane + 1) / 33.0;
+    const unsigned mask = __ballot_sync(0xffffffffu, sturm_count(d, e2, N, sig, pivmin) >= kth);
+    const int f = mask ? __ffs(mask) - 1 : 32;  // first shift with kth eigenvalues below it
+    const double nlo = f > 0 ? lo + width * (double)f / 33.0 : lo;
+    const double nhi = f < 32 ? lo + width * (double)(f + 1) / 33.0 : hi;
+    lo = nlo;
+    hi = nhi;
+  }
+  return 0.5 * (lo + hi);
+}
+
+// Positivity ratio of the (already Hermitian) H:
+//   max(0, -lmin - 64 n eps max(|l|max, 1)) / |l|max.
+// One Sturm count decides the common case: the diagonal of the tridiagonal
+// form bounds |l|max from below, so no eigenvalue below -64 n eps
+// max(max|d|, 1) means the ratio is exactly 0; otherwise lmin and lmax are
+// found by multisection.
 template <int NP, int TT>
 __device__ double psd_ratio(Cx<double>* H, int N, int tt, ResScratch<NP>& S, int team) {
-  team_eigvals<NP, TT>(H, N, tt, S, team);
-  double lmin = INFINITY, bn = 0;
+  constexpr double eps = 2.220446049250313e-16;
+  team_tridiagonalize<NP, TT>(H, N, tt, S, team);
+  double dmax = 0;
   bool finite = true;
   for (int i = 0; i < N; ++i) {
-    const double v = S.vals[i];
-    finite = finite && isfinite(v);
-    lmin = fmin(lmin, v);
-    bn = fmax(bn, fabs(v));
+    finite = finite && isfinite(S.d[i]) && (i + 1 == N || isfinite(S.e2[i]));
+    dmax = fmax(dmax, fabs(S.d[i]));
   }
   if (!finite) return INFINITY;
-  const double budget = 64.0 * N * 2.220446049250313e-16 * fmax(bn, 1.0);
-  const double absolute = fmax(0.0, -lmin);
-  return fmax(0.0, absolute - budget) / fmax(bn, 2.2250738585072014e-308);
+  const double pivmin = tri_pivmin(S.e2, N);
+  if (sturm_count(S.d, S.e2, N, -64.0 * N * eps * fmax(dmax, 1.0), pivmin) == 0) return 0.0;
+  const double lmin = tri_eig(S.d, S.e2, N, 1), lmax = tri_eig(S.d, S.e2, N, N);
+  const double bn = fmax(fabs(lmin), fabs(lmax));
+  const double budget = 64.0 * N * eps * fmax(bn, 1.0);
+  return fmax(0.0, fmax(0.0, -lmin) - budget) / fmax(bn, 2.2250738585072014e-308);
+}
+
+// Largest eigenvalue of the Hermitian H (destroyed); if `only_if_positive`,
+// returns 0 without the multisection when no eigenvalue is >= 0.
+template <int NP, int TT>
+__device__ double team_lmax(Cx<double>* H, int N, int tt, ResScratch<NP>& S, int team, bool only_if_positive) {
+  team_tridiagonalize<NP, TT>(H, N, tt, S, team);
+  for (int i = 0; i < N; ++i)
+    if (!isfinite(S.d[i]) || (i + 1 < N && !isfinite(S.e2[i]))) return INFINITY;
+  if (only_if_positive && sturm_count(S.d, S.e2, N, 0.0, tri_pivmin(S.e2, N)) == N) return 0.0;
+  return tri_eig(S.d, S.e2, N, N);
 }
 
 template <typename RS, int NP, int BPC>
@@ -226,10 +358,8 @@ __global__ void __launch_bounds__(BPC* Tile<NP>::TT) residual_kernel(ResidualArg
     if (bad != 0) {
       caus_num = INFINITY;
     } else {
-      team_eigvals<NP, TT>(H, N, tt, S, team);
-      double lmax = -INFINITY;
-      for (int i = 0; i < N; ++i) lmax = fmax(lmax, S.vals[i]);
-      caus_num = fmax(0.0, lmax);
+      // lmax(Im_H SR) <= 0 (the causal case) is settled by one Sturm count
+      caus_num = fmax(0.0, team_lmax<NP, TT>(H, N, tt, S, team, true));
     }
   }
   double caus = 0;
@@ -237,9 +367,7 @@ __global__ void __launch_bounds__(BPC* Tile<NP>::TT) residual_kernel(ResidualArg
     // ||SR||_2^2 = lmax(SR SR^H)
     team_matmul<double, double, NP>(X, X, H, N, tt, true);
     team_sync<TT>(team);
-    team_eigvals<NP, TT>(H, N, tt, S, team);
-    double lmax = 0;
-    for (int i = 0; i < N; ++i) lmax = fmax(lmax, S.vals[i]);
+    const double lmax = team_lmax<NP, TT>(H, N, tt, S, team, false);
     caus = caus_num / (sqrt(fmax(lmax, 0.0)) + 1e-14);
   } else if (!isfinite(caus_num)) {
     caus = INFINITY;

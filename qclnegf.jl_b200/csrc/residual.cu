@@ -161,6 +161,7 @@ __device__ bool hermitian_part(const Cx<double>* X, Cx<double> f, Cx<double>* H,
     H[sw<NP>(i, j)] = cx<double>(0.5 * (v.x + w.x), 0.5 * (v.y - w.y));
   }
   bad = team_max<TT>(bad, tt, S.red, team);
+  team_sync<TT>(team);  // H complete for every thread of the team
   return bad == 0;
 }
 
@@ -272,23 +273,51 @@ __device__ double tri_eig(const double* d, const double* e2, int N, int kth) {
   return 0.5 * (lo + hi);
 }
 
-// Positivity ratio of the (already Hermitian) H:
-//   max(0, -lmin - 64 n eps max(|l|max, 1)) / |l|max.
-// One Sturm count decides the common case: the diagonal of the tridiagonal
-// form bounds |l|max from below, so no eigenvalue below -64 n eps
-// max(max|d|, 1) means the ratio is exactly 0; otherwise lmin and lmax are
-// found by multisection.
+// True if H + shift I is numerically positive definite: LDL^T without pivoting
+// (trailing lower triangle updated in place) meets only positive pivots.  H is
+// destroyed.  A success certifies lmin(H) > -shift up to the factorization's
+// backward error O(n eps ||H||) -- the same order as the error of the
+// eigenvalues themselves.
 template <int NP, int TT>
-__device__ double psd_ratio(Cx<double>* H, int N, int tt, ResScratch<NP>& S, int team) {
-  constexpr double eps = 2.220446049250313e-16;
-  team_tridiagonalize<NP, TT>(H, N, tt, S, team);
-  double dmax = 0;
-  bool finite = true;
-  for (int i = 0; i < N; ++i) {
-    finite = finite && isfinite(S.d[i]) && (i + 1 == N || isfinite(S.e2[i]));
-    dmax = fmax(dmax, fabs(S.d[i]));
+__device__ bool team_posdef(Cx<double>* H, int N, double shift, int tt, int team) {
+  for (int k = 0; k < N; ++k) {
+    const double dk = H[sw<NP>(k, k)].x + shift;
+    if (!(dk > 0)) return false;  // team-uniform: every thread read the same pivot
+    const double inv = 1.0 / dk;
+    const int m = N - k - 1;
+    for (int idx = tt; idx < m * m; idx += TT) {
+      const int i = k + 1 + idx % m, j = k + 1 + idx / m;
+      if (i < j) continue;
+      const Cx<double> a = H[sw<NP>(i, k)], b = H[sw<NP>(j, k)];
+      Cx<double>& h = H[sw<NP>(i, j)];
+      const Cx<double> t = a * conj(b);
+      h = cx<double>(h.x - inv * t.x, h.y - inv * t.y);
+    }
+    team_sync<TT>(team);
   }
-  if (!finite) return INFINITY;
+  return true;
+}
+
+// Positivity ratio of the Hermitian part of f X (written to H, destroyed):
+//   max(0, -lmin - 64 n eps max(|l|max, 1)) / |l|max,
+// INFINITY if f X has non-finite entries.  The diagonal bounds |l|max from
+// below, so when H + 64 n eps max(max|H_ii|, 1) I is positive definite (one
+// LDL^T, the common case) the ratio is 0; otherwise H is rebuilt, reduced to
+// tridiagonal form and lmin, lmax are found by multisection.
+template <int NP, int TT>
+__device__ double psd_of(const Cx<double>* X, Cx<double> f, Cx<double>* H, int N, int tt, ResScratch<NP>& S,
+                         int team) {
+  constexpr double eps = 2.220446049250313e-16;
+  if (!hermitian_part<NP, TT>(X, f, H, N, tt, S, team)) return INFINITY;
+  double dmax = 0;
+  for (int i = 0; i < N; ++i) dmax = fmax(dmax, fabs(H[sw<NP>(i, i)].x));
+  team_sync<TT>(team);
+  if (team_posdef<NP, TT>(H, N, 64.0 * N * eps * fmax(dmax, 1.0), tt, team)) return 0.0;
+  team_sync<TT>(team);
+  hermitian_part<NP, TT>(X, f, H, N, tt, S, team);
+  team_tridiagonalize<NP, TT>(H, N, tt, S, team);
+  for (int i = 0; i < N; ++i)
+    if (!isfinite(S.d[i]) || (i + 1 < N && !isfinite(S.e2[i]))) return INFINITY;
   const double pivmin = tri_pivmin(S.e2, N);
   if (sturm_count(S.d, S.e2, N, -64.0 * N * eps * fmax(dmax, 1.0), pivmin) == 0) return 0.0;
   const double lmin = tri_eig(S.d, S.e2, N, 1), lmax = tri_eig(S.d, S.e2, N, N);
@@ -358,8 +387,15 @@ __global__ void __launch_bounds__(BPC* Tile<NP>::TT) residual_kernel(ResidualArg
     if (bad != 0) {
       caus_num = INFINITY;
     } else {
-      // lmax(Im_H SR) <= 0 (the causal case) is settled by one Sturm count
-      caus_num = fmax(0.0, team_lmax<NP, TT>(H, N, tt, S, team, true));
+      // the causal case, -Im_H SR positive definite, is settled by one LDL^T
+      for (int idx = tt; idx < N * N; idx += TT) {
+        const int i = idx % N, j = idx / N;
+        const Cx<double> v = H[sw<NP>(i, j)];
+        W[sw<NP>(i, j)] = cx<double>(-v.x, -v.y);
+      }
+      team_sync<TT>(team);
+      if (!team_posdef<NP, TT>(W, N, 0.0, tt, team)) caus_num = fmax(0.0, team_lmax<NP, TT>(H, N, tt, S, team, true));
+      team_sync<TT>(team);
     }
   }
   double caus = 0;
@@ -410,8 +446,7 @@ __global__ void __launch_bounds__(BPC* Tile<NP>::TT) residual_kernel(ResidualArg
     Y[sw<NP>(i, j)] = pi * cx<double>(g.x - gt.x, g.y + gt.y);
   }
   team_sync<TT>(team);
-  if (hermitian_part<NP, TT>(Y, one, H, N, tt, S, team)) psd = fmax(psd, psd_ratio<NP, TT>(H, N, tt, S, team));
-  else psd = INFINITY;
+  psd = fmax(psd, psd_of<NP, TT>(Y, one, H, N, tt, S, team));
 
   // ---- Gamma = i (S> - S<), its positivity, r_A ---------------------------------
   __syncthreads();
@@ -424,8 +459,7 @@ __global__ void __launch_bounds__(BPC* Tile<NP>::TT) residual_kernel(ResidualArg
     X[sw<NP>(i, j)] = pi * cx<double>(g.x - l.x, g.y - l.y);
   }
   team_sync<TT>(team);
-  if (hermitian_part<NP, TT>(X, one, H, N, tt, S, team)) psd = fmax(psd, psd_ratio<NP, TT>(H, N, tt, S, team));
-  else psd = INFINITY;
+  psd = fmax(psd, psd_of<NP, TT>(X, one, H, N, tt, S, team));
   team_matmul<double, double, NP>(G, X, W, N, tt, false);  // W = G Gam
   team_sync<TT>(team);
   team_matmul<double, double, NP>(W, G, H, N, tt, true);   // H = G Gam G^H
@@ -448,10 +482,7 @@ __global__ void __launch_bounds__(BPC* Tile<NP>::TT) residual_kernel(ResidualArg
     team_sync<TT>(team);
     team_matmul<double, double, NP>(W, G, Y, N, tt, true);
     team_sync<TT>(team);
-    if (hermitian_part<NP, TT>(Y, which == 0 ? mi : pi, H, N, tt, S, team))
-      psd = fmax(psd, psd_ratio<NP, TT>(H, N, tt, S, team));
-    else
-      psd = INFINITY;
+    psd = fmax(psd, psd_of<NP, TT>(Y, which == 0 ? mi : pi, H, N, tt, S, team));
   }
 
   // ---- G< : positivity and r_K against the candidate lesser self-energy ----------
@@ -459,8 +490,7 @@ __global__ void __launch_bounds__(BPC* Tile<NP>::TT) residual_kernel(ResidualArg
   load_tile<RS, NP, BPC>(p.GL, bX, e0, m, NE, Nk, N);
   load_tile<RS, NP, BPC>(p.SLc, bY, e0, m, NE, Nk, N);
   __syncthreads();
-  if (hermitian_part<NP, TT>(X, mi, H, N, tt, S, team)) psd = fmax(psd, psd_ratio<NP, TT>(H, N, tt, S, team));
-  else psd = INFINITY;
+  psd = fmax(psd, psd_of<NP, TT>(X, mi, H, N, tt, S, team));
   team_matmul<double, double, NP>(G, Y, W, N, tt, false);
   team_sync<TT>(team);
   team_matmul<double, double, NP>(W, G, H, N, tt, true);
@@ -478,8 +508,7 @@ __global__ void __launch_bounds__(BPC* Tile<NP>::TT) residual_kernel(ResidualArg
   __syncthreads();
   load_tile<RS, NP, BPC>(p.GG, bX, e0, m, NE, Nk, N);
   __syncthreads();
-  if (hermitian_part<NP, TT>(X, pi, H, N, tt, S, team)) psd = fmax(psd, psd_ratio<NP, TT>(H, N, tt, S, team));
-  else psd = INFINITY;
+  psd = fmax(psd, psd_of<NP, TT>(X, pi, H, N, tt, S, team));
 
   if (tt == 0 && live) {
     double* o = p.block_out + 7 * ((size_t)e + (size_t)NE * m);

@@ -18,6 +18,10 @@ int launch_paired_coefficients(const double* trL, const double* trG, int gs, dou
                                int* status, cudaStream_t st, double realness_limit = 1e-10);
 int launch_normalize_pair(int precision, size_t n, void* GL, void* GG, const double* coeffs, cudaStream_t st);
 int launch_sum_fields(int precision, size_t n, const void* const* src, int count, void* out, cudaStream_t st);
+constexpr int kMaxMixFields = 32;
+size_t residual_mix_multi_partial_doubles(int nf);
+int launch_residual_mix_multi(int precision, size_t n, const void* const* old, void* const* cand, int nf,
+                              double alpha, double* partial, double* out, cudaStream_t st);
 int launch_residual_mix(int precision, size_t n, const void* old, void* new_, double alpha, double* partial,
                         double* out2, cudaStream_t st);
 int launch_combine(const double* partial, int count, int K, double* out, cudaStream_t st);

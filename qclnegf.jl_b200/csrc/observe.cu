@@ -86,28 +86,41 @@ __global__ void population_partial_kernel(int NE, int Nk, int N, const double* _
 // Combines partials into the final scalars:
 //   out[0] = Jbar, out[1] = Im of the complex flux (diagnostic),
 //   out[2 + a] = p_a.
+// One CTA per quantity (current, then each population), fixed-order sums.
 __global__ void observables_combine_kernel(int N, int ncta, const double* cur, const double* pop, int gs, double target,
                                            double* out) {
-  // fixed order, single thread per quantity
-  const int q = threadIdx.x;
+  const int q = blockIdx.x;  // 0: current, 1 + a: population a
+  const double* src = q == 0 ? cur : pop + 2 * (size_t)(q - 1) * ncta;
+  double re = 0, im = 0;
+  for (int c = threadIdx.x; c < ncta; c += blockDim.x) {
+    re += src[2 * c];
+    im += src[2 * c + 1];
+  }
+  __shared__ double red[2][32];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    re += __shfl_xor_sync(0xffffffffu, re, o);
+    im += __shfl_xor_sync(0xffffffffu, im, o);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    red[0][threadIdx.x >> 5] = re;
+    red[1][threadIdx.x >> 5] = im;
+  }
+  __syncthreads();
+  if (threadIdx.x != 0) return;
+  re = 0;
+  im = 0;
+  for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
+    re += red[0][w];
+    im += red[1][w];
+  }
   const double pre = gs / (2.0 * M_PI);
   if (q == 0) {
-    double re = 0, im = 0;
-    for (int c = 0; c < ncta; ++c) {
-      re += cur[2 * c];
-      im += cur[2 * c + 1];
-    }
     out[0] = pre * re;
     out[1] = pre * im;
-  }
-  for (int a = q; a < N; a += blockDim.x) {
-    double re = 0, im = 0;
-    for (int c = 0; c < ncta; ++c) {
-      re += pop[2 * ((size_t)a * ncta + c)];
-      im += pop[2 * ((size_t)a * ncta + c) + 1];
-    }
+  } else {
     // -i pre (re + i im) = pre (im - i re): real part = pre * im
-    out[2 + a] = pre * im / target;
+    out[1 + q] = pre * im / target;
   }
 }
 
@@ -132,7 +145,7 @@ int launch_observables(int precision, int NE, int Nk, int N, const double* wE, c
     population_partial_kernel<float><<<dim3(OBS_CTAS, N), OBS_THREADS, 0, st>>>(NE, Nk, N, wE, wk,
                                                                                 (const Cx<float>*)GL, pop);
   }
-  observables_combine_kernel<<<1, 64, 0, st>>>(N, OBS_CTAS, cur, pop, gs, target, out);
+  observables_combine_kernel<<<1 + N, 128, 0, st>>>(N, OBS_CTAS, cur, pop, gs, target, out);
   QCL_LAUNCH_CHECK("observables");
   return QCL_OK;
 }

@@ -262,6 +262,87 @@ int launch_residual_mix(int precision, size_t n, const void* old, void* new_, do
   return QCL_OK;
 }
 
+// All state/candidate field pairs of an iteration in one launch: blockIdx.y
+// selects the field, MIX_CTAS CTAs per field write (|new - old|^2, |new|^2)
+// partials and mix new <- (1 - alpha) old + alpha new in place.
+constexpr int MIX_CTAS = 64;
+template <typename R> struct MixFields {
+  const Cx<R>* old[kMaxMixFields];
+  Cx<R>* cand[kMaxMixFields];
+};
+
+template <typename R>
+__global__ void __launch_bounds__(REDUCE_THREADS) residual_mix_multi_kernel(size_t n, MixFields<R> f, double alpha,
+                                                                            double* partial) {
+  const Cx<R>* __restrict__ old = f.old[blockIdx.y];
+  Cx<R>* __restrict__ new_ = f.cand[blockIdx.y];
+  double v[2] = {0, 0};
+  const R al = (R)alpha, be = (R)(1.0 - alpha);
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    const Cx<R> o = old[i], c = new_[i];
+    const double dx = (double)c.x - o.x, dy = (double)c.y - o.y;
+    const double d2 = dx * dx + dy * dy, n2 = (double)c.x * c.x + (double)c.y * c.y;
+    if (isfinite(d2) && isfinite(n2) && isfinite((double)o.x) && isfinite((double)o.y)) {
+      v[0] += d2;
+      v[1] += n2;
+    } else {
+      v[0] = INFINITY;
+    }
+    if (alpha > 0) new_[i] = cx<R>(be * o.x + al * c.x, be * o.y + al * c.y);
+  }
+  block_sum<2>(v);
+  if (threadIdx.x == 0) {
+    double* pp = partial + 2 * ((size_t)blockIdx.y * gridDim.x + blockIdx.x);
+    pp[0] = v[0];
+    pp[1] = v[1];
+  }
+}
+
+// One CTA per segment: out[2 s + k] = sum_c partial[s][c][k], fixed order.
+__global__ void combine_segments_kernel(const double* partial, int count, double* out) {
+  const double* seg = partial + 2 * (size_t)blockIdx.x * count;
+  double v[2] = {0, 0};
+  for (int i = threadIdx.x; i < count; i += blockDim.x) {
+    v[0] += seg[2 * i];
+    v[1] += seg[2 * i + 1];
+  }
+  block_sum<2>(v);
+  if (threadIdx.x == 0) {
+    out[2 * blockIdx.x] = v[0];
+    out[2 * blockIdx.x + 1] = v[1];
+  }
+}
+
+size_t residual_mix_multi_partial_doubles(int nf) { return 2 * (size_t)MIX_CTAS * nf; }
+
+int launch_residual_mix_multi(int precision, size_t n, const void* const* old, void* const* cand, int nf,
+                              double alpha, double* partial, double* out, cudaStream_t st) {
+  if (nf <= 0) return QCL_OK;
+  if (nf > kMaxMixFields) {
+    set_last_error("residual_mix: %d fields exceed %d", nf, kMaxMixFields);
+    return QCL_ARG;
+  }
+  const dim3 grid(MIX_CTAS, nf);
+  if (precision == QCL_C128) {
+    MixFields<double> f{};
+    for (int i = 0; i < nf; ++i) {
+      f.old[i] = (const Cx<double>*)old[i];
+      f.cand[i] = (Cx<double>*)cand[i];
+    }
+    residual_mix_multi_kernel<double><<<grid, REDUCE_THREADS, 0, st>>>(n, f, alpha, partial);
+  } else {
+    MixFields<float> f{};
+    for (int i = 0; i < nf; ++i) {
+      f.old[i] = (const Cx<float>*)old[i];
+      f.cand[i] = (Cx<float>*)cand[i];
+    }
+    residual_mix_multi_kernel<float><<<grid, REDUCE_THREADS, 0, st>>>(n, f, alpha, partial);
+  }
+  combine_segments_kernel<<<nf, REDUCE_THREADS, 0, st>>>(partial, MIX_CTAS, out);
+  QCL_LAUNCH_CHECK("residual_mix_multi");
+  return QCL_OK;
+}
+
 int launch_combine(const double* partial, int count, int K, double* out, cudaStream_t st) {
   switch (K) {
     case 1: combine_partials<1><<<1, REDUCE_THREADS, 0, st>>>(partial, count, out); break;

@@ -558,14 +558,24 @@ __global__ void residual_reduce_kernel(long long blocks, const double* __restric
   }
 }
 
+// One warp per quantity, fixed-order lane sums then a fixed shuffle tree.
 __global__ void residual_final_kernel(int ncta, const double* partial, double* out) {
+  const int k = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  __shared__ double v[7];
+  const bool is_max = k == 0 || k >= 5;
+  double a = 0;
+  for (int c = lane; c < ncta; c += 32) {
+    const double q = partial[7 * c + k];
+    a = is_max ? fmax(a, q) + (isnan(q) ? INFINITY : 0.0) : a + q;
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    const double q = __shfl_xor_sync(0xffffffffu, a, o);
+    a = is_max ? fmax(a, q) : a + q;
+  }
+  if (lane == 0) v[k] = a;
+  __syncthreads();
   if (threadIdx.x != 0) return;
-  double v[7] = {0, 0, 0, 0, 0, 0, 0};
-  for (int c = 0; c < ncta; ++c)
-    for (int k = 0; k < 7; ++k) {
-      const double q = partial[7 * c + k];
-      v[k] = (k == 0 || k >= 5) ? fmax(v[k], q) : v[k] + q;
-    }
   out[0] = v[0];
   out[1] = (isfinite(v[1]) && isfinite(v[2])) ? sqrt(v[1]) / (sqrt(v[2]) + 1e-14) : INFINITY;
   out[2] = (isfinite(v[3]) && isfinite(v[4])) ? sqrt(v[3]) / (sqrt(v[4]) + 1e-14) : INFINITY;
@@ -720,7 +730,7 @@ int launch_residual_suite(int precision, int NE, int Nk, int N, const double* ep
   if (s) return s;
   double* partial = work + 7 * (size_t)NE * Nk;
   residual_reduce_kernel<<<RES_CTAS, 256, 0, st>>>((long long)NE * Nk, work, partial);
-  residual_final_kernel<<<1, 32, 0, st>>>(RES_CTAS, partial, out5);
+  residual_final_kernel<<<1, 7 * 32, 0, st>>>(RES_CTAS, partial, out5);
   QCL_LAUNCH_CHECK("residual_reduce");
   return QCL_OK;
 }

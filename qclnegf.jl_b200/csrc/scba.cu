@@ -89,6 +89,7 @@ struct ScbaCtx {
   // reductions
   Cx<double>*trL = nullptr, *trG = nullptr;
   double* rpartial = nullptr;
+  double* mpartial = nullptr;  // per-field partials of the fused residual + mixing
   double* reswork = nullptr;
   double* obspartial = nullptr;
   double* scal = nullptr;
@@ -182,6 +183,7 @@ void scba_destroy(ScbaCtx* c) {
   cudaFree(c->trL);
   cudaFree(c->trG);
   cudaFree(c->rpartial);
+  cudaFree(c->mpartial);
   cudaFree(c->reswork);
   cudaFree(c->obspartial);
   cudaFree(c->scal);
@@ -301,6 +303,7 @@ int scba_create(const qcl_scba_problem* p, const qcl_mechanism* mechs, ScbaCtx**
   TRY(dalloc((void**)&c->trL, (size_t)c->NE * c->Nk * 16));
   TRY(dalloc((void**)&c->trG, (size_t)c->NE * c->Nk * 16));
   TRY(dalloc((void**)&c->rpartial, kReduceCtas * 2 * sizeof(double)));
+  TRY(dalloc((void**)&c->mpartial, residual_mix_multi_partial_doubles(3 * (c->M + 2)) * sizeof(double)));
   TRY(dalloc((void**)&c->reswork, residual_work_doubles(c->NE, c->Nk) * sizeof(double)));
   TRY(dalloc((void**)&c->obspartial, observables_partial_doubles(c->N) * sizeof(double)));
   TRY(dalloc((void**)&c->scal, SC_TOTAL * sizeof(double)));
@@ -433,11 +436,16 @@ static int iteration_body(ScbaCtx* c, std::vector<void*>& state, std::vector<voi
     return s;
   // per-family residual + speculative linear mixing into the candidate buffers
   const int F = c->M + 2;
+  const void* olds[kMaxMixFields];
+  void* cands[kMaxMixFields];
   for (int f = 0; f < F; ++f)
-    for (int k = 0; k < 3; ++k)
-      if ((s = launch_residual_mix(sp, c->nfield, field_of(state, f, k), field_of(cand, f, k), c->alpha, c->rpartial,
-                                   c->scal + SC_FAM + 2 * (3 * f + k), c->st)))
-        return s;
+    for (int k = 0; k < 3; ++k) {
+      olds[3 * f + k] = field_of(state, f, k);
+      cands[3 * f + k] = field_of(cand, f, k);
+    }
+  if ((s = launch_residual_mix_multi(sp, c->nfield, olds, cands, 3 * F, c->alpha, c->mpartial, c->scal + SC_FAM,
+                                     c->st)))
+    return s;
   QCL_CUDA_CHECK(cudaMemcpyAsync(c->scal_h, c->scal, SC_TOTAL * sizeof(double), cudaMemcpyDeviceToHost, c->st));
   return QCL_OK;
 }

@@ -39,6 +39,11 @@ E0_EV = 0.1
 # bytes per block = read Sigma^R, Sigma^< + write G^R, G^< = 4 * 16 N^2.
 FLOP_PER_BLOCK = 24 * NB ** 3
 BYTES_PER_BLOCK = 4 * 16 * NB * NB
+# DRAM bytes (read + write) of one Dyson launch, from the ncu capture of
+# `bench.py --capture dyson` (N_k = 8, a quarter of the blocks: 604.4 MB read,
+# 562.4 MB written) scaled by 4 to the bench launch; traffic grows with the
+# block count.
+DYSON_TRAFFIC_BYTES = 4 * (604.39e6 + 562.44e6)
 
 
 def parse():
@@ -48,6 +53,8 @@ def parse():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-extras", action="store_true", help="skip the variant and SCBA side measurements")
+    ap.add_argument("--capture", choices=["dyson", "hilbert", "scba"],
+                    help="run one small case of a kernel for an ncu capture (2 launches) and exit")
     return ap.parse_args()
 
 
@@ -392,7 +399,9 @@ def run_gpu(args):
                                f"FFT Hilbert of Gamma (L = 8192, {ncols} columns)",
                    "l2": "inputs larger than L2 (each field 1.2 GB)", "parallelism": f"replicas x{ws}"},
         "roofline": {"bound": "hbm", "achieved": achieved_gbs, "peak": peak, "unit": "GB/s",
-                     "frac": achieved_gbs / peak, "traffic": None, "kernel": "dyson_keldysh_kernel",
+                     "frac": achieved_gbs / peak, "traffic": DYSON_TRAFFIC_BYTES,
+                     "traffic_source": "ncu dram__bytes_read+write of the N_k = 8 capture x 4",
+                     "algorithmic_bytes": BYTES_PER_BLOCK * NE * NK, "kernel": "dyson_keldysh_kernel",
                      "kernel_ms": dyson_ms, "peak_kind": peak_kind,
                      "fp64_tflops": achieved_tflops, "fp64_nominal_tflops": fp64_nominal,
                      "fp64_frac_of_nominal": achieved_tflops / fp64_nominal},
@@ -486,8 +495,60 @@ def extras(torch, dev, L, _lib):
     return out
 
 
+def run_capture(kind):
+    """Small cases for ncu: the same kernels as the timed step on a quarter of
+    the momenta (dyson: N_E x N_k = 4096 x 8, N_b = 24, c128, G^R + G^<), 4096
+    Hilbert columns at L = 8192, or 3 tutorial SCBA iterations."""
+    import torch
+
+    from qclb200 import _lib
+
+    L = _lib.lib()
+    dev = torch.device("cuda", 0)
+    P = ctypes.c_void_p
+    sp = P(torch.cuda.current_stream(dev).cuda_stream)
+    eps, wE = grids()
+    eps_d = torch.tensor(eps, dtype=torch.float64, device=dev)
+    if kind == "dyson":
+        global NK
+        NK = 8
+        hf, SR, SL, _ = device_inputs(torch, dev, NB, seed=1, cdt=torch.complex128)
+        GR, GL = torch.empty_like(SR), torch.empty_like(SR)
+        st = torch.zeros(2, dtype=torch.int32, device=dev)
+        for _ in range(2):
+            _lib.check(L.qcl_dev_dyson_keldysh(sp, _lib.QCL_C128, NE, NK, NB, P(eps_d.data_ptr()), 0.0,
+                                               P(hf.data_ptr()), P(SR.data_ptr()), P(SL.data_ptr()), None,
+                                               P(GR.data_ptr()), P(GL.data_ptr()), None, None, None, None,
+                                               P(st.data_ptr())))
+    elif kind == "hilbert":
+        ncols = 4096
+        g = torch.Generator(device=dev)
+        g.manual_seed(1)
+        Gam = torch.randn((ncols, NE), dtype=torch.complex128, device=dev, generator=g)
+        Lam = torch.empty_like(Gam)
+        wE_d = torch.tensor(wE, dtype=torch.float64, device=dev)
+        for _ in range(2):
+            _lib.check(L.qcl_dev_fft_hilbert_transform(sp, _lib.QCL_C128, NE, ncols, float(eps[1] - eps[0]),
+                                                       P(wE_d.data_ptr()), P(Gam.data_ptr()), P(Lam.data_ptr()),
+                                                       None))
+    else:
+        from qclb200.problem import tutorial_problem
+        from qclb200.scba import ProductionSCBA
+
+        s = ProductionSCBA(tutorial_problem(), precision="c128")
+        s.seed()
+        for _ in range(3):
+            s.step()
+        s.close()
+    torch.cuda.synchronize()
+    print("ok", kind)
+
+
 def main():
     args = parse()
+    if args.capture:
+        run_capture(args.capture)
+        return
     if args.impl == "reference":
         run_reference(args)
     else:

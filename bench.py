@@ -231,6 +231,22 @@ def dist_init(args):
     return None, 0, 1
 
 
+def max_over_ranks(dist, value, device=None):
+    """The slowest rank's time: the job is done when every replica is."""
+    if not dist:
+        return value
+    import torch
+
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_rate(ws, units_per_rank, ms):
+    """Whole-job throughput: units of all ranks over the slowest rank's time."""
+    return ws * units_per_rank / (ms / 1e3)
+
+
 def run_reference(args):
     dist, rank, ws = dist_init(args)
     if rank != 0:
@@ -337,11 +353,8 @@ def run_gpu(args):
     total_ms = t0.elapsed_time(t1)
     dyson_ms = sum(a.elapsed_time(b) for a, b in ev) / args.steps
     step_ms = total_ms / args.steps
-    if dist:
-        tt = torch.tensor([step_ms], device=dev)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        step_ms = float(tt.item())
-    value = ws * NE * NK / (step_ms / 1e3)
+    step_ms = max_over_ranks(dist, step_ms, dev)
+    value = job_rate(ws, NE * NK, step_ms)
     gpu_launches = launches[0]
 
     # ---- end to end through the host-buffer C ABI (pinned host arrays) ------------
@@ -374,12 +387,9 @@ def run_gpu(args):
             e2e_step()
         torch.cuda.synchronize()
         e2e_ms = (time.perf_counter() - t) / k * 1e3
-        if dist:
-            tt = torch.tensor([e2e_ms], device=dev)
-            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-            e2e_ms = float(tt.item())
+        e2e_ms = max_over_ranks(dist, e2e_ms, dev)
         fb = NE * NK * NB * NB * 16
-        e2e = {"value": ws * NE * NK / (e2e_ms / 1e3), "unit": "solves/s", "h2d_bytes_per_step": 3 * fb,
+        e2e = {"value": job_rate(ws, NE * NK, e2e_ms), "unit": "solves/s", "h2d_bytes_per_step": 3 * fb,
                "d2h_bytes_per_step": 3 * fb, "ms_per_step": e2e_ms,
                "path": "qcl_dyson_keldysh + qcl_fft_hilbert_transform with pinned host buffers"}
         # parity of this very run: GPU G^< equals the device-resident result

@@ -431,12 +431,37 @@ int qcl_static_contraction(int precision, const qcl_mechanism* op, int NE, int N
   }
   const size_t nb = field_elems(NE, Nk, Nb) * cbytes(sp);
   if ((s = dwk.upload(wk, Nk * sizeof(double)))) return s;
+  DevBuf st;
+  if ((s = st.upload(nullptr, 2 * sizeof(int)))) return s;
+  QCL_CUDA_CHECK(cudaMemset(st.p, 0, 2 * sizeof(int)));
+  float* bhi = nullptr;
+  float* blo = nullptr;
+  struct TcFree {
+    float** a;
+    float** b;
+    ~TcFree() {
+      cudaFree(*a);
+      cudaFree(*b);
+    }
+  } tc_free{&bhi, &blo};
+  if (op->kind == QCL_KERNEL_DENSE && sp == QCL_C64) {  // complex64: tensor-core operand
+    if ((s = tc_build_operator(Nk * (int)N2, Nk, mat.p, (const double*)dwk.p, &bhi, &blo, 0))) return s;
+    k.tc_bhi = bhi;
+    k.tc_blo = blo;
+    k.status = (int*)st.p;
+  }
   if ((s = dG.upload(G, nb))) return s;
   if ((s = dS.upload(beta != 0.0 ? S : nullptr, nb))) return s;
   if ((s = work.alloc(contraction_work_elems(k, NE, Nk, Nb) * cbytes(sp)))) return s;
   if ((s = launch_contraction(sp, k, NE, Nk, Nb, (const double*)dwk.p, dG.p, dS.p, alpha * op->q, beta, work.p, 0)))
     return s;
   QCL_CUDA_CHECK(cudaDeviceSynchronize());
+  int hst[2] = {0, 0};
+  QCL_CUDA_CHECK(cudaMemcpy(hst, st.p, sizeof(hst), cudaMemcpyDeviceToHost));
+  if (hst[0]) {
+    set_last_error("static contraction: device wait gave up (status %d at tile %d)", hst[0], hst[1]);
+    return hst[0];
+  }
   return dS.download(S);
 }
 

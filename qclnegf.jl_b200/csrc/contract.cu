@@ -236,6 +236,9 @@ static int contraction_t(const KernelOpDev& op, int NE, int Nk, int N, const dou
   }
   if (op.kind == QCL_KERNEL_DENSE) {
     const int Nc = Nk * N2;
+    if (sizeof(R) == 4 && op.tc_bhi)  // complex64 fields: tensor cores (3xTF32)
+      return launch_tc_dense_contraction(NE, Nc, op.tc_bhi, op.tc_blo, Gv, Sv, alpha_q, beta, (float*)work,
+                                         op.status, st);
     GemmArgs<R> g{};
     g.M = NE; g.Nout = Nc; g.K = Nc; g.batch = 1;
     g.A = G; g.lda = NEl; g.wk = wk; g.wk_mod = Nk;
@@ -280,6 +283,7 @@ static int contraction_t(const KernelOpDev& op, int NE, int Nk, int N, const dou
 
 size_t contraction_work_elems(const KernelOpDev& op, int NE, int Nk, int N) {
   if (op.kind == QCL_KERNEL_MOMENTUM_INDEPENDENT) return (size_t)NE * N * N;
+  if (op.kind == QCL_KERNEL_DENSE && op.tc_bhi) return (tc_a_work_floats(NE, Nk * N * N) + 1) / 2;  // complex64 units
   if (op.kind == QCL_KERNEL_IFR) return 2 * (size_t)NE * op.J * Nk;
   return 0;
 }

@@ -42,8 +42,14 @@ struct Mech {
   void* left = nullptr;
   void* right = nullptr;
   void* radial = nullptr;
+  float* tc_bhi = nullptr;  // dense operator prepared for the tensor cores (complex64 fields)
+  float* tc_blo = nullptr;
+  int* status = nullptr;
   KernelOpDev view() const {
     KernelOpDev k;
+    k.tc_bhi = tc_bhi;
+    k.tc_blo = tc_blo;
+    k.status = status;
     k.kind = kind;
     k.J = J;
     k.block = block;
@@ -170,6 +176,8 @@ void scba_destroy(ScbaCtx* c) {
     cudaFree(m.left);
     cudaFree(m.right);
     cudaFree(m.radial);
+    cudaFree(m.tc_bhi);
+    cudaFree(m.tc_blo);
   }
   for (void* p : c->state) cudaFree(p);
   for (void* p : c->cand) cudaFree(p);
@@ -276,6 +284,8 @@ int scba_create(const qcl_scba_problem* p, const qcl_mechanism* mechs, ScbaCtx**
     } else if (q.kind == QCL_KERNEL_DENSE) {
       const size_t nc = (size_t)c->Nk * N2;
       TRY(upload_op(c, &d.matrix, q.matrix, nc * nc));
+      if (c->precision != QCL_C128)
+        TRY(tc_build_operator((int)nc, c->Nk, d.matrix, c->wk, &d.tc_bhi, &d.tc_blo, c->st));
     } else if (q.kind == QCL_KERNEL_IFR) {
       if (q.J < 1) TRY((set_last_error("IFR operator needs J >= 1"), QCL_ARG));
       TRY(upload_op(c, &d.left, q.left, (size_t)N2 * q.J));
@@ -313,6 +323,7 @@ int scba_create(const qcl_scba_problem* p, const qcl_mechanism* mechs, ScbaCtx**
   }
   TRY(dalloc((void**)&c->status, 2 * sizeof(int)));
   QCL_CUDA_CHECK(cudaMemsetAsync(c->status, 0, 2 * sizeof(int), c->st));
+  for (auto& m : c->mech) m.status = c->status;
   QCL_CUDA_CHECK(cudaMemsetAsync(c->scal, 0, SC_TOTAL * sizeof(double), c->st));
   TRY(prepare_hilbert_tables(c->hil, c->NE, de, c->precision));
   TRY(ensure_partial(c->hil, (long long)c->Nk * N2));

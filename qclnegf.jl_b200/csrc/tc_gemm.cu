@@ -1,0 +1,380 @@
+// Dense self-energy contraction on the 5th-generation tensor cores (complex64
+// fields; the mixed and c64 precisions).
+//
+// Reference: _production_static_contraction! for a dense operator
+// (numerics/optimized/production_operators.jl:402-465):
+//   S[e,(m,a,b)] = beta S + alpha q sum_(m',c,d) M[(m,a,b),(m',c,d)] wk[m'] G[e,(m',c,d)].
+//
+// The complex product is one real GEMM.  With k = (m',c,d), j = (m,a,b) and
+// interleaved real indices kk = 2k + {0: Re, 1: Im}, nn = 2j + {0, 1}:
+//   A[e][kk]  = G[e,k] parts                       (M = N_E rows, K-contiguous)
+//   B[nn][kk] = wk * [[Re M, -Im M], [Im M, Re M]]  (built once per operator)
+//   S[e,j] = alpha q (C[e][2j] + i C[e][2j+1]) + beta S[e,j],  C = A B^T.
+// Both operands are split into TF32 parts x = hi + lo (hi = tf32(x),
+// lo = tf32(x - hi)) and C accumulates A_hi B_hi + A_hi B_lo + A_lo B_hi in
+// FP32 (the 3xTF32 scheme: ~FP32 accuracy at tensor-core rate).
+//
+// Kernel: one CTA of 256 threads per 128 x 256 output tile, 1 CTA per SM.
+// K advances in blocks of 32 (one 128-byte swizzle row per operand row);
+// all threads stage a block with cp.async into 1024-byte aligned,
+// 128B-swizzled K-major tiles (two stages); thread 0 issues the 3 x 4
+// tcgen05.mma (M=128, N=256, K=8, kind::tf32) of a block into one of two
+// tensor-memory accumulators (128 lanes x 256 FP32 columns each) and commits
+// them to the stage's mbarrier.
+//
+// Accumulation: the tensor core's FP32 accumulation truncates (measured here:
+// a relative bias of about -0.17 ulp per accumulate, -6.6e-5 after K = 8192).
+// So every K block starts a fresh accumulator, and while the tensor core
+// fills one buffer the 8 warps read the other (tcgen05.ld, warp w: lanes
+// 32 (w % 4) .. + 31, columns 128 (w / 4) .. + 127) and add it to per-thread
+// FP32 running sums with IEEE rounding; an mbarrier (256 arrivals) hands the
+// buffer back.  Each truncated chain is then 12 accumulates long.
+// Every wait is bounded: a wait that gives up records QCL_TIMEOUT, the CTA
+// then waits (bounded) for its own MMAs, releases its tensor memory and ends.
+#include "kernels.cuh"
+
+namespace qcl {
+
+constexpr int TC_BM = 128, TC_BN = 256, TC_BK = 32, TC_THREADS = 256;
+constexpr int TC_A_BYTES = TC_BM * TC_BK * 4;   // 16 KiB per A part
+constexpr int TC_B_BYTES = TC_BN * TC_BK * 4;   // 32 KiB per B part
+constexpr int TC_STAGE_BYTES = 2 * TC_A_BYTES + 2 * TC_B_BYTES;
+constexpr int TC_SMEM_BYTES = 2 * TC_STAGE_BYTES + 1024 + 64;  // + alignment + barriers
+constexpr uint32_t TC_TMEM_COLS = 512;  // two 256-column accumulators
+constexpr long long TC_WAIT_LIMIT = 1ll << 22;  // try_wait rounds (~1 s) before a wait gives up
+
+// UMMA shared-memory descriptor, K-major, 128-byte swizzle: start address
+// (>> 4), leading byte offset 1 (unused for swizzled K-major), stride byte
+// offset 1024 B between 8-row groups (>> 4), descriptor version 1, swizzle
+// mode 2 (128B).
+__device__ __forceinline__ uint64_t umma_desc_k_sw128(uint32_t saddr) {
+  return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)1 << 16) | ((uint64_t)64 << 32) | ((uint64_t)1 << 46) |
+         ((uint64_t)2 << 61);
+}
+// Instruction descriptor: D f32, A/B tf32, both K-major, N = 256, M = 128.
+constexpr uint32_t TC_IDESC = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(TC_BN >> 3) << 17) |
+                              ((uint32_t)(TC_BM >> 4) << 24);
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+// Bounded parity wait; returns false if it gave up.
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
+  for (long long i = 0; i < TC_WAIT_LIMIT; ++i) {
+    uint32_t done;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+        : "=r"(done)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+
+__device__ __forceinline__ void tc_mma(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t accumulate) {
+  asm volatile(
+      "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+      " tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n}" ::"r"(tmem_d),
+      "l"(adesc), "l"(bdesc), "r"(TC_IDESC), "r"(accumulate), "r"(0), "r"(0), "r"(0), "r"(0)
+      : "memory");
+}
+__device__ __forceinline__ void tc_commit(uint32_t bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar) : "memory");
+}
+
+// Copies one K block (32 floats per row) of `rows` rows of a K-contiguous
+// matrix (row stride ld floats) into a 128B-swizzled tile: row r, 16-byte
+// chunk c lands at r * 128 + ((c ^ (r & 7)) << 4).
+__device__ __forceinline__ void stage_rows(uint32_t tile, const float* __restrict__ src, long long ld, int rows) {
+  const int chunks = rows * 8;
+  for (int i = threadIdx.x; i < chunks; i += TC_THREADS) {
+    const int r = i >> 3, c = i & 7;
+    const float* g = src + (long long)r * ld + c * 4;
+    const uint32_t d = tile + r * 128 + ((c ^ (r & 7)) << 4);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(g) : "memory");
+  }
+}
+
+struct TcArgs {
+  int M;        // rows of C actually stored (N_E)
+  int Ncols;    // real columns of C actually stored (2 Nc)
+  int Kpad;     // padded real K (multiple of 32)
+  const float* Ahi;  // [Mpad][Kpad]
+  const float* Alo;
+  const float* Bhi;  // [Npad][Kpad]
+  const float* Blo;
+  Cx<float>* S;      // S[e + NE j], j < Ncols / 2
+  int NE;
+  double alpha, beta;
+  int* status;
+};
+
+__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
+}
+
+// Reads this thread's 32 columns [c, c + 32) of tensor-memory lane row `trow`.
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&v)[32]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+      "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+      : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]), "=r"(v[8]),
+        "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15]), "=r"(v[16]),
+        "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]), "=r"(v[22]), "=r"(v[23]), "=r"(v[24]),
+        "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
+      : "r"(taddr));
+}
+
+__global__ void __launch_bounds__(TC_THREADS, 1) tc_gemm_kernel(TcArgs p) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const uint32_t raw = smem_u32(smem_raw);
+  const uint32_t base = (raw + 1023u) & ~1023u;  // 1024-byte aligned tiles
+  unsigned char* gbase = smem_raw + (base - raw);
+  // barriers after the two stages: mma_done[2] (tcgen05.commit), acc_empty[2] (256 readers)
+  const uint32_t bars = base + 2 * TC_STAGE_BYTES;
+  const uint32_t mma_done = bars, acc_empty = bars + 16;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(gbase + 2 * TC_STAGE_BYTES + 32);
+  __shared__ int s_fail;
+
+  const int m0 = blockIdx.x * TC_BM, n0 = blockIdx.y * TC_BN;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (threadIdx.x == 0) {
+    mbar_init(mma_done, 1);
+    mbar_init(mma_done + 8, 1);
+    mbar_init(acc_empty, TC_THREADS);
+    mbar_init(acc_empty + 8, TC_THREADS);
+    s_fail = 0;
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                 "r"(TC_TMEM_COLS)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = *tmem_slot;
+  // this thread's accumulator rows / columns
+  const uint32_t tlane = (uint32_t)((warp & 3) * 32) << 16;
+  const int cbase = (warp >> 2) * 128;
+  float sum[128];
+#pragma unroll
+  for (int i = 0; i < 128; ++i) sum[i] = 0.0f;
+
+  const int nkb = p.Kpad / TC_BK;
+  const float* Ahi = p.Ahi + (long long)m0 * p.Kpad;
+  const float* Alo = p.Alo + (long long)m0 * p.Kpad;
+  const float* Bhi = p.Bhi + (long long)n0 * p.Kpad;
+  const float* Blo = p.Blo + (long long)n0 * p.Kpad;
+  bool ok = true;
+  // adds accumulator buffer of block kb into the running sums and hands it back
+  auto drain = [&](int kb) {
+    const int b = kb & 1;
+    if (!mbar_wait(mma_done + 8 * b, (uint32_t)((kb >> 1) & 1))) {
+      ok = false;
+      return;
+    }
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t taddr = tmem + tlane + (uint32_t)(b * TC_BN + cbase);
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+      uint32_t v[32];
+      tmem_ld32(taddr + c * 32, v);
+      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+      for (int i = 0; i < 32; ++i) sum[c * 32 + i] += __uint_as_float(v[i]);
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    mbar_arrive(acc_empty + 8 * b);
+  };
+  for (int kb = 0; kb < nkb; ++kb) {
+    const int s = kb & 1;
+    const uint32_t st = base + s * TC_STAGE_BYTES;
+    const uint32_t tAh = st, tAl = st + TC_A_BYTES, tBh = st + 2 * TC_A_BYTES, tBl = tBh + TC_B_BYTES;
+    // stage s was last read by the MMAs of block kb-2, drained (waited) at iteration kb-1
+    if (__syncthreads_or(!ok)) {
+      ok = false;  // every thread leaves; none waits for blocks that were never issued
+      break;
+    }
+    const long long koff = (long long)kb * TC_BK;
+    stage_rows(tAh, Ahi + koff, p.Kpad, TC_BM);
+    stage_rows(tAl, Alo + koff, p.Kpad, TC_BM);
+    stage_rows(tBh, Bhi + koff, p.Kpad, TC_BN);
+    stage_rows(tBl, Blo + koff, p.Kpad, TC_BN);
+    asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // generic writes -> tensor-core reads
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      // accumulator buffer s was read out (block kb-2) by every thread at iteration kb-1
+      bool free_ok = kb < 2 || mbar_wait(acc_empty + 8 * s, (uint32_t)(((kb - 2) >> 1) & 1));
+      if (free_ok) {
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        const uint32_t dacc = tmem + (uint32_t)(s * TC_BN);
+#pragma unroll
+        for (int ks = 0; ks < TC_BK / 8; ++ks) {  // K = 8 tf32 = 32 bytes per MMA
+          const uint32_t off = ks * 32;
+          const uint64_t ah = umma_desc_k_sw128(tAh + off), al = umma_desc_k_sw128(tAl + off);
+          const uint64_t bh = umma_desc_k_sw128(tBh + off), bl = umma_desc_k_sw128(tBl + off);
+          tc_mma(dacc, ah, bh, ks > 0 ? 1u : 0u);
+          tc_mma(dacc, ah, bl, 1u);
+          tc_mma(dacc, al, bh, 1u);
+        }
+      } else {
+        ok = false;
+      }
+      tc_commit(mma_done + 8 * s);  // arrives even when nothing was issued, so no reader waits for good
+    }
+    if (kb >= 1) drain(kb - 1);  // overlaps the tensor core's work on block kb
+  }
+  if (ok && nkb > 0) drain(nkb - 1);
+  if (!ok) {
+    s_fail = 1;
+    if (threadIdx.x == 0) record_status(p.status, QCL_TIMEOUT, (long long)blockIdx.x + 65536ll * blockIdx.y);
+  }
+  __syncthreads();
+  if (s_fail && nkb > 0) {
+    // let the MMAs already issued drain (bounded) before the memory is released
+    const int last = nkb - 1;
+    mbar_wait(mma_done + 8 * (last & 1), (uint32_t)((last >> 1) & 1));
+  }
+
+  if (!s_fail) {
+    const int e = m0 + (warp & 3) * 32 + lane;
+    const float al = (float)p.alpha, be = (float)p.beta;
+    if (e < p.M) {
+#pragma unroll
+      for (int q = 0; q < 64; ++q) {
+        const int nn = n0 + cbase + 2 * q;
+        if (nn >= p.Ncols) continue;
+        Cx<float>* dst = p.S + (size_t)e + (size_t)p.NE * (size_t)(nn >> 1);
+        const float re = al * sum[2 * q], im = al * sum[2 * q + 1];
+        if (p.beta == 0.0) {
+          *dst = cx<float>(re, im);
+        } else {
+          const Cx<float> o = *dst;
+          *dst = cx<float>(be * o.x + re, be * o.y + im);
+        }
+      }
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TC_TMEM_COLS) : "memory");
+}
+
+// ---------------------------------------------------------------------------
+// Operand preparation
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ float tf32_round(float x) {
+  uint32_t r;
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+  return __uint_as_float(r);
+}
+
+// A[e][2k + c] = part c of G[e + NE k] for k < Nc (zero in the padding),
+// split into tf32 hi / lo; a 32 x 32 (e, kk) tile is transposed through
+// shared memory so that both the E-fastest reads and the K-contiguous writes
+// are coalesced.
+__global__ void tc_split_a_kernel(int NE, int Nc, int Mpad, int Kpad, const Cx<float>* __restrict__ G,
+                                  float* __restrict__ Ahi, float* __restrict__ Alo) {
+  __shared__ float tile[32][33];
+  const int e0 = blockIdx.x * 32, kk0 = blockIdx.y * 32;
+  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;  // 32 x 8 threads
+  for (int r = ty; r < 32; r += 8) {
+    // read: row kk = kk0 + r (fixed k, component), column e = e0 + tx (coalesced along e)
+    const int kk = kk0 + r, e = e0 + tx;
+    float v = 0.0f;
+    const int k = kk >> 1;
+    if (e < NE && k < Nc) {
+      const Cx<float> g = G[(size_t)e + (size_t)NE * k];
+      v = (kk & 1) ? g.y : g.x;
+    }
+    tile[r][tx] = v;
+  }
+  __syncthreads();
+  for (int r = ty; r < 32; r += 8) {
+    const int e = e0 + r, kk = kk0 + tx;
+    if (e >= Mpad || kk >= Kpad) continue;
+    const float x = tile[tx][r];
+    const float hi = tf32_round(x);
+    const size_t idx = (size_t)e * Kpad + kk;
+    Ahi[idx] = hi;
+    Alo[idx] = tf32_round(x - hi);
+  }
+}
+
+// B[2j + c'][2k + c] from the complex operator M (column-major Nc x Nc,
+// complex64) and the momentum weights wk[k % Nk]:
+//   [[Re, -Im], [Im, Re]] * w  (rows c' = 0 real part of the output, 1 imaginary).
+__global__ void tc_build_b_kernel(int Nc, int Nk, int Npad, int Kpad, const Cx<float>* __restrict__ Mop,
+                                  const double* __restrict__ wk, float* __restrict__ Bhi, float* __restrict__ Blo) {
+  const long long n = (long long)Npad * Kpad;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const int nn = (int)(i / Kpad), kk = (int)(i % Kpad);
+    const int j = nn >> 1, k = kk >> 1;
+    float v = 0.0f;
+    if (j < Nc && k < Nc) {
+      const Cx<float> m = Mop[(size_t)j + (size_t)Nc * k];
+      const float w = (float)wk[k % Nk];
+      const int cp = nn & 1, c = kk & 1;
+      const float val = (cp == c) ? m.x : (cp == 0 ? -m.y : m.y);
+      v = w * val;
+    }
+    const float hi = tf32_round(v);
+    Bhi[i] = hi;
+    Blo[i] = tf32_round(v - hi);
+  }
+}
+
+int tc_dims(int NE, int Nc, int* Mpad, int* Npad, int* Kpad) {
+  *Mpad = (NE + TC_BM - 1) / TC_BM * TC_BM;
+  *Npad = (2 * Nc + TC_BN - 1) / TC_BN * TC_BN;
+  *Kpad = (2 * Nc + TC_BK - 1) / TC_BK * TC_BK;
+  return QCL_OK;
+}
+
+size_t tc_a_work_floats(int NE, int Nc) {
+  int Mpad, Npad, Kpad;
+  tc_dims(NE, Nc, &Mpad, &Npad, &Kpad);
+  return 2 * (size_t)Mpad * Kpad;
+}
+
+int tc_build_operator(int Nc, int Nk, const void* Mop_c64, const double* wk, float** Bhi, float** Blo,
+                      cudaStream_t st) {
+  int Mpad, Npad, Kpad;
+  tc_dims(1, Nc, &Mpad, &Npad, &Kpad);
+  const size_t n = (size_t)Npad * Kpad;
+  QCL_CUDA_CHECK(cudaMalloc(Bhi, n * sizeof(float)));
+  QCL_CUDA_CHECK(cudaMalloc(Blo, n * sizeof(float)));
+  tc_build_b_kernel<<<148 * 8, 256, 0, st>>>(Nc, Nk, Npad, Kpad, (const Cx<float>*)Mop_c64, wk, *Bhi, *Blo);
+  QCL_LAUNCH_CHECK("tc_build_b_kernel");
+  return QCL_OK;
+}
+
+int launch_tc_dense_contraction(int NE, int Nc, const float* Bhi, const float* Blo, const void* G, void* S,
+                                double alpha, double beta, float* awork, int* status, cudaStream_t st) {
+  int Mpad, Npad, Kpad;
+  tc_dims(NE, Nc, &Mpad, &Npad, &Kpad);
+  float* Ahi = awork;
+  float* Alo = awork + (size_t)Mpad * Kpad;
+  dim3 sg((Mpad + 31) / 32, (Kpad + 31) / 32);
+  tc_split_a_kernel<<<sg, 256, 0, st>>>(NE, Nc, Mpad, Kpad, (const Cx<float>*)G, Ahi, Alo);
+  QCL_LAUNCH_CHECK("tc_split_a_kernel");
+  static bool configured = false;
+  if (!configured) {
+    QCL_CUDA_CHECK(cudaFuncSetAttribute(tc_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM_BYTES));
+    configured = true;
+  }
+  TcArgs a{NE, 2 * Nc, Kpad, Ahi, Alo, Bhi, Blo, (Cx<float>*)S, NE, alpha, beta, status};
+  dim3 grid(Mpad / TC_BM, Npad / TC_BN);
+  tc_gemm_kernel<<<grid, TC_THREADS, TC_SMEM_BYTES, st>>>(a);
+  QCL_LAUNCH_CHECK("tc_gemm_kernel");
+  return QCL_OK;
+}
+
+}  // namespace qcl

@@ -281,3 +281,42 @@ def test_batched_hermitian_eigvals_match_numpy(gpu_ops, n):
     got = gpu_ops.hermitian_eigvals(H)
     ref = np.linalg.eigvalsh(H)
     assert np.max(np.abs(got - ref)) <= 1e-12 * np.max(np.abs(ref))
+
+
+@pytest.mark.parametrize("NE,Nk,Nb,beta", [(37, 4, 4, 0.0), (200, 3, 3, 1.0), (129, 5, 4, 0.5)])
+def test_dense_contraction_tensor_cores_c64(gpu_ops, orc, NE, Nk, Nb, beta):
+    # complex64 dense contraction on tcgen05 (3xTF32, FP32 accumulation) against
+    # the FP64 literal six-index map; ragged N_E and N_k N_b^2 exercise the
+    # zero padding of the 128 x 256 x 32 tiles
+    from qclb200.problem import small_problem
+
+    pr = small_problem(NE=NE, Nk=Nk, Nb=Nb, mechanisms=("impurity",))
+    mech = pr.mechanisms[0]
+    rng = np.random.default_rng(NE + Nk)
+    G = _rand_field(rng, pr.shape)
+    S0 = _rand_field(rng, pr.shape)
+    got = gpu_ops.production_static_contraction(mech, G, pr.wk, alpha=1.3, beta=beta, S=S0, precision="c64")
+    lit = orc.contraction_literal(mech.literal_kernel(pr.Nk, pr.Nb), G, pr.wk, 1.3 * mech.q) + beta * S0
+    assert got.dtype == np.complex64
+    assert approx_err(got, lit) < 2e-6
+
+
+def test_dense_contraction_tensor_cores_no_accumulation_bias(gpu_ops):
+    # a long positive sum (K = 2 N_k N_b^2 = 2048 real terms) exposes any
+    # truncation bias of the tensor-core accumulation: the mean signed relative
+    # error must stay at the FP32 rounding level, not grow with K
+    from qclb200.problem import Mechanism
+
+    rng = np.random.default_rng(17)
+    NE, Nk, Nb = 256, 16, 8
+    Nc = Nk * Nb * Nb
+    M = rng.uniform(0.0, 1.0, (Nc, Nc)) + 0j
+    G = rng.uniform(0.0, 1.0, (NE, Nk, Nb, Nb)).astype(np.complex64).astype(np.complex128)
+    G = np.asfortranarray(G)
+    mech = Mechanism("impurity", "dense", 1.0, matrix=np.asfortranarray(M))
+    got = gpu_ops.production_static_contraction(mech, G, np.ones(Nk), precision="c64")
+    got = got.reshape(NE, Nc, order="F").astype(np.complex128)
+    ref = G.reshape(NE, Nc, order="F") @ M.astype(np.complex64).astype(np.complex128).T
+    rel = (got.real - ref.real) / ref.real
+    assert abs(float(np.mean(rel))) < 1e-6
+    assert float(np.max(np.abs(rel))) < 3e-6

@@ -53,7 +53,7 @@ def parse():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-extras", action="store_true", help="skip the variant and SCBA side measurements")
-    ap.add_argument("--capture", choices=["dyson", "hilbert", "scba"],
+    ap.add_argument("--capture", choices=["dyson", "hilbert", "scba", "tcgemm"],
                     help="run one small case of a kernel for an ncu capture (2 launches) and exit")
     return ap.parse_args()
 
@@ -486,7 +486,12 @@ def extras(torch, dev, L, _lib):
     for precision in ("c128", "mixed"):
         solver = ProductionSCBA(pr, precision=precision, use_graph=True)
         solver.seed()
-        rows = [solver.step() for _ in range(3)]
+        rows = []
+        for it in range(3):
+            try:
+                rows.append(solver.step())
+            except Exception as ex:  # noqa: BLE001
+                raise RuntimeError(f"tutorial SCBA ({precision}) iteration {it}: {ex!r}") from ex
         torch.cuda.synchronize()
         t = time.perf_counter()
         n = 27
@@ -502,7 +507,44 @@ def extras(torch, dev, L, _lib):
             res[precision]["J_rel_err_vs_fp64"] = max(abs(a - b) / abs(a) for a, b in zip(Jref, J))
         solver.close()
     out["scba_tutorial_N12_30iter"] = res
+    try:
+        out["scba_all_mechanisms"] = scba_all_mechanisms(torch)
+    except Exception as ex:  # noqa: BLE001
+        import traceback
+
+        out["scba_all_mechanisms"] = {"error": repr(ex), "where": traceback.format_exc(limit=4)[-600:]}
     return out
+
+
+def scba_all_mechanisms(torch, NE_=1024, Nk_=32, Nb_=16, warm=2, timed=4):
+    """SCBA iterations/s with every scattering mechanism (LO with its four
+    shifts, acoustic, impurity, IFR, alloy): plain FP64 against mixed
+    precision (complex64 storage, FP64 elimination and reductions, dense
+    contractions on the tensor cores in 3xTF32), and the largest relative
+    difference of the current density J over the same iterations."""
+    import numpy as np
+    from qclb200.problem import small_problem
+    from qclb200.scba import ProductionSCBA
+
+    pr = small_problem(NE=NE_, Nk=Nk_, Nb=Nb_, mechanisms=("LO", "acoustic", "impurity", "IFR", "alloy"))
+    res, J = {}, {}
+    for precision in ("c128", "mixed"):
+        solver = ProductionSCBA(pr, precision=precision, use_graph=True)
+        solver.seed()
+        rows = [solver.step() for _ in range(warm)]
+        torch.cuda.synchronize()
+        t = time.perf_counter()
+        for _ in range(timed):
+            rows.append(solver.step())
+        sec = (time.perf_counter() - t) / timed
+        J[precision] = np.array([r["J"] for r in rows])
+        res[precision] = {"iter_per_s": 1.0 / sec, "ms_per_iter": sec * 1e3}
+        solver.close()
+    res["mixed_speedup_vs_fp64"] = res["mixed"]["iter_per_s"] / res["c128"]["iter_per_s"]
+    res["J_rel_err_mixed_vs_fp64"] = float(np.max(np.abs(J["mixed"] - J["c128"]) / np.abs(J["c128"])))
+    res["config"] = (f"N_E x N_k = {NE_} x {Nk_}, N_b = {Nb_}, LO+acoustic+impurity+IFR+alloy, "
+                     f"{warm} + {timed} timed iterations per precision, CUDA graph on, roundoff check on")
+    return res
 
 
 def run_capture(kind):
@@ -541,6 +583,22 @@ def run_capture(kind):
             _lib.check(L.qcl_dev_fft_hilbert_transform(sp, _lib.QCL_C128, NE, ncols, float(eps[1] - eps[0]),
                                                        P(wE_d.data_ptr()), P(Gam.data_ptr()), P(Lam.data_ptr()),
                                                        None))
+    elif kind == "tcgemm":
+        # complex64 dense contraction on the tensor cores: N_E = 1024 rows,
+        # N_k N_b^2 = 16 x 16^2 = 4096 complex columns (a 1024 x 8192 x 8192
+        # real GEMM in 3xTF32)
+        import numpy as np
+        from qclb200 import operators
+        from qclb200.problem import Mechanism
+
+        rng = np.random.default_rng(1)
+        ne, nk, nb = 1024, 16, 16
+        nc = nk * nb * nb
+        M = np.asfortranarray(rng.standard_normal((nc, nc)) + 1j * rng.standard_normal((nc, nc)))
+        G = np.asfortranarray(rng.standard_normal((ne, nk, nb, nb)) + 1j * rng.standard_normal((ne, nk, nb, nb)))
+        mech = Mechanism("impurity", "dense", 1.0, matrix=M)
+        for _ in range(2):
+            operators.production_static_contraction(mech, G, np.ones(nk), precision="c64")
     else:
         from qclb200.problem import tutorial_problem
         from qclb200.scba import ProductionSCBA

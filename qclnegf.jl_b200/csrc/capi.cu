@@ -219,9 +219,12 @@ int qcl_dyson_keldysh(int precision, int NE, int Nk, int Nb, const double* eps, 
   if (traceL && sigL && (s = P.trL.ensure(nb * 16))) return s;
   if (traceG && sigG && (s = P.trG.ensure(nb * 16))) return s;
   if ((s = P.status.ensure(2 * sizeof(int)))) return s;
-  QCL_CUDA_CHECK(cudaMemcpy(P.eps.p, eps, NE * sizeof(double), cudaMemcpyHostToDevice));
-  QCL_CUDA_CHECK(cudaMemcpy(P.h.p, h, (size_t)Nk * Nb * Nb * 16, cudaMemcpyHostToDevice));
-  QCL_CUDA_CHECK(cudaMemset(P.status.p, 0, 2 * sizeof(int)));
+  // on the pipeline's own (non-blocking) streams: legacy-stream copies and
+  // memsets would not be ordered before the slab kernels
+  QCL_CUDA_CHECK(cudaMemcpyAsync(P.eps.p, eps, NE * sizeof(double), cudaMemcpyHostToDevice, P.st[0]));
+  QCL_CUDA_CHECK(cudaMemcpyAsync(P.h.p, h, (size_t)Nk * Nb * Nb * 16, cudaMemcpyHostToDevice, P.st[0]));
+  QCL_CUDA_CHECK(cudaMemsetAsync(P.status.p, 0, 2 * sizeof(int), P.st[0]));
+  QCL_CUDA_CHECK(cudaStreamSynchronize(P.st[0]));
   // momentum slabs of ~64 MiB per field, round-robin over three streams so
   // that the upload of one slab, the kernel of the previous one and the
   // download of the one before overlap
@@ -309,7 +312,8 @@ static int hilbert_host(int precision, int NE, size_t ncols, const double* eps, 
   if (out_gam && (s = P.gam.ensure(nf))) return s;
   if (verify && (s = ensure_partial(t, (long long)ncols))) return s;
   if ((s = P.sum.ensure(2 * sizeof(double)))) return s;
-  QCL_CUDA_CHECK(cudaMemcpy(P.wE.p, wE, NE * sizeof(double), cudaMemcpyHostToDevice));
+  QCL_CUDA_CHECK(cudaMemcpyAsync(P.wE.p, wE, NE * sizeof(double), cudaMemcpyHostToDevice, P.st[0]));
+  QCL_CUDA_CHECK(cudaStreamSynchronize(P.st[0]));
   // column slabs of ~64 MiB, three streams
   size_t cs = std::max<size_t>(1, (64u << 20) / ((size_t)NE * es));
   cs = std::min(cs, ncols);

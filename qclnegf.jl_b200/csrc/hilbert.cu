@@ -445,6 +445,9 @@ template <typename R> static int upload_cx(void** dst, const std::vector<double>
   for (size_t i = 0; i < re.size(); ++i) h[i] = cx<R>((R)re[i], (R)im[i]);
   QCL_CUDA_CHECK(cudaMalloc(dst, h.size() * sizeof(Cx<R>)));
   QCL_CUDA_CHECK(cudaMemcpy(*dst, h.data(), h.size() * sizeof(Cx<R>), cudaMemcpyHostToDevice));
+  // the tables are read by kernels on non-blocking streams, which are not
+  // ordered after this legacy-stream copy: wait until it has landed
+  QCL_CUDA_CHECK(cudaDeviceSynchronize());
   return QCL_OK;
 }
 

@@ -120,16 +120,20 @@ static int dalloc(void** p, size_t bytes) {
   if (e != cudaSuccess) return cuda_status(e, "cudaMalloc (SCBA context)");
   return QCL_OK;
 }
-template <typename T> static int dupload(T** p, const void* host, size_t bytes) {
+// Uploads go on the context's stream: the context's kernels run on a
+// non-blocking stream, which a plain cudaMemcpy (legacy stream; from pageable
+// memory it may return before the DMA has landed) would not order them after.
+template <typename T> static int dupload(T** p, const void* host, size_t bytes, cudaStream_t st) {
   int s = dalloc((void**)p, bytes);
   if (s) return s;
-  QCL_CUDA_CHECK(cudaMemcpy(*p, host, bytes, cudaMemcpyHostToDevice));
+  QCL_CUDA_CHECK(cudaMemcpyAsync(*p, host, bytes, cudaMemcpyHostToDevice, st));
+  QCL_CUDA_CHECK(cudaStreamSynchronize(st));  // the host buffer may be a temporary
   return QCL_OK;
 }
 
 static int upload_op(ScbaCtx* c, void** dst, const void* host_c128, size_t n) {
   void* tmp = nullptr;
-  int s = dupload(&tmp, host_c128, n * 16);
+  int s = dupload(&tmp, host_c128, n * 16, c->st);
   if (s) return s;
   if ((s = dalloc(dst, n * (c->precision == QCL_C128 ? 16 : 8)))) {
     cudaFree(tmp);
@@ -147,10 +151,10 @@ static int build_plan(ScbaCtx* c, DevShift& d, double delta) {
   std::vector<unsigned char> v(c->NE);
   int s = build_shift_plan_host(c->NE, c->eps_h.data(), delta, l.data(), r.data(), th.data(), v.data());
   if (s) return s;
-  if ((s = dupload(&d.left, l.data(), c->NE * sizeof(int)))) return s;
-  if ((s = dupload(&d.right, r.data(), c->NE * sizeof(int)))) return s;
-  if ((s = dupload(&d.theta, th.data(), c->NE * sizeof(double)))) return s;
-  return dupload(&d.valid, v.data(), c->NE);
+  if ((s = dupload(&d.left, l.data(), c->NE * sizeof(int), c->st))) return s;
+  if ((s = dupload(&d.right, r.data(), c->NE * sizeof(int), c->st))) return s;
+  if ((s = dupload(&d.theta, th.data(), c->NE * sizeof(double), c->st))) return s;
+  return dupload(&d.valid, v.data(), c->NE, c->st);
 }
 
 void scba_destroy(ScbaCtx* c) {
@@ -258,12 +262,12 @@ int scba_create(const qcl_scba_problem* p, const qcl_mechanism* mechs, ScbaCtx**
     cudaError_t e = cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking);
     if (e != cudaSuccess) TRY(cuda_status(e, "cudaStreamCreate"));
   }
-  TRY(dupload(&c->eps, p->eps, c->NE * sizeof(double)));
-  TRY(dupload(&c->wE, p->wE, c->NE * sizeof(double)));
-  TRY(dupload(&c->wk, p->wk, c->Nk * sizeof(double)));
-  TRY(dupload(&c->h, p->h, (size_t)c->Nk * c->N * c->N * 16));
-  TRY(dupload(&c->Tp, p->Tplus, (size_t)c->N * c->N * 16));
-  TRY(dupload(&c->Tm, p->Tminus, (size_t)c->N * c->N * 16));
+  TRY(dupload(&c->eps, p->eps, c->NE * sizeof(double), c->st));
+  TRY(dupload(&c->wE, p->wE, c->NE * sizeof(double), c->st));
+  TRY(dupload(&c->wk, p->wk, c->Nk * sizeof(double), c->st));
+  TRY(dupload(&c->h, p->h, (size_t)c->Nk * c->N * c->N * 16, c->st));
+  TRY(dupload(&c->Tp, p->Tplus, (size_t)c->N * c->N * 16, c->st));
+  TRY(dupload(&c->Tm, p->Tminus, (size_t)c->N * c->N * 16, c->st));
   TRY(build_plan(c, c->shift[0], +c->Ep));
   TRY(build_plan(c, c->shift[1], -c->Ep));
   TRY(build_plan(c, c->shift[2], +c->hw_LO));
@@ -694,8 +698,8 @@ int scba_upload(ScbaCtx* c, int which, const void* host) {
     c->pending_commit = false;
   }
   std::vector<void*>& st = c->parity == 0 ? c->state : c->cand;
+  QCL_CUDA_CHECK(cudaMemcpyAsync(st[idx], host, c->fbytes, cudaMemcpyHostToDevice, c->st));
   QCL_CUDA_CHECK(cudaStreamSynchronize(c->st));
-  QCL_CUDA_CHECK(cudaMemcpy(st[idx], host, c->fbytes, cudaMemcpyHostToDevice));
   c->seeded = true;
   return QCL_OK;
 }

@@ -191,23 +191,29 @@ __global__ void __launch_bounds__(TC_THREADS, 1) tc_gemm_kernel(TcArgs p) {
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     mbar_arrive(acc_empty + 8 * b);
   };
+  auto load_block = [&](int kb) {
+    const uint32_t st = base + (kb & 1) * TC_STAGE_BYTES;
+    const long long koff = (long long)kb * TC_BK;
+    stage_rows(st, Ahi + koff, p.Kpad, TC_BM);
+    stage_rows(st + TC_A_BYTES, Alo + koff, p.Kpad, TC_BM);
+    stage_rows(st + 2 * TC_A_BYTES, Bhi + koff, p.Kpad, TC_BN);
+    stage_rows(st + 2 * TC_A_BYTES + TC_B_BYTES, Blo + koff, p.Kpad, TC_BN);
+    asm volatile("cp.async.commit_group;" ::: "memory");
+  };
+  // Software pipeline: the copies of block kb+1 are issued as soon as the
+  // MMAs of block kb-1 (the last reader of that stage) retire, i.e. while the
+  // tensor core works on block kb.
+  if (nkb > 0) load_block(0);
   for (int kb = 0; kb < nkb; ++kb) {
     const int s = kb & 1;
     const uint32_t st = base + s * TC_STAGE_BYTES;
     const uint32_t tAh = st, tAl = st + TC_A_BYTES, tBh = st + 2 * TC_A_BYTES, tBl = tBh + TC_B_BYTES;
-    // stage s was last read by the MMAs of block kb-2, drained (waited) at iteration kb-1
+    asm volatile("cp.async.wait_group 0;" ::: "memory");          // block kb has landed
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // generic writes -> tensor-core reads
     if (__syncthreads_or(!ok)) {
       ok = false;  // every thread leaves; none waits for blocks that were never issued
       break;
     }
-    const long long koff = (long long)kb * TC_BK;
-    stage_rows(tAh, Ahi + koff, p.Kpad, TC_BM);
-    stage_rows(tAl, Alo + koff, p.Kpad, TC_BM);
-    stage_rows(tBh, Bhi + koff, p.Kpad, TC_BN);
-    stage_rows(tBl, Blo + koff, p.Kpad, TC_BN);
-    asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;" ::: "memory");
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // generic writes -> tensor-core reads
-    __syncthreads();
     if (threadIdx.x == 0) {
       // accumulator buffer s was read out (block kb-2) by every thread at iteration kb-1
       bool free_ok = kb < 2 || mbar_wait(acc_empty + 8 * s, (uint32_t)(((kb - 2) >> 1) & 1));
@@ -228,7 +234,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1) tc_gemm_kernel(TcArgs p) {
       }
       tc_commit(mma_done + 8 * s);  // arrives even when nothing was issued, so no reader waits for good
     }
-    if (kb >= 1) drain(kb - 1);  // overlaps the tensor core's work on block kb
+    if (kb >= 1) drain(kb - 1);  // waits for the MMAs of block kb-1, reads their accumulator
+    if (ok && kb + 1 < nkb) load_block(kb + 1);  // into the stage block kb-1 has released
   }
   if (ok && nkb > 0) drain(nkb - 1);
   if (!ok) {

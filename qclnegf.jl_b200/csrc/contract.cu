@@ -212,6 +212,161 @@ template <typename R> static int launch_gemm(const GemmArgs<R>& a, cudaStream_t 
 }
 
 // ---------------------------------------------------------------------------
+// Dense complex128 contraction on the FP64 tensor path (mma.sync m8n8k4 f64):
+//   C[e, j] = alpha sum_k A[e + lda k] w[k % wmod] B[j + ldb k] + beta C[e + ldc j].
+// CTA: 8 warps, 128 (e) x 32 (j) outputs; warp (wm, wn) owns rows 32 wm ..
+// + 31 and columns 16 wn .. + 15 as 4 x 2 tiles of 8 x 8, each accumulated as
+// four real products (Re C += Ar Br - Ai Bi, Im C += Ar Bi + Ai Br).  K
+// advances by 16 through two cp.async stages; shared rows are padded to a
+// stride of 2 (mod 8) 16-byte units so the fragment loads of a quarter warp
+// hit 8 distinct bank groups.  Fragment layouts (m8n8k4, f64): A lane l holds
+// (l / 4, l % 4), B holds (l % 4, l / 4), C holds (l / 4, 2 (l % 4) + i).
+// ---------------------------------------------------------------------------
+constexpr int DM_BM = 128, DM_BN = 32, DM_BK = 16, DM_THREADS = 256;
+constexpr int DM_APAD = DM_BM + 2, DM_BPAD = DM_BN + 2;
+constexpr size_t DM_SMEM = (2 * DM_BK * DM_APAD + 2 * DM_BK * DM_BPAD) * sizeof(Cx<double>) + 2 * DM_BK * sizeof(double);
+
+struct DmArgs {
+  int M, N, K;
+  const Cx<double>* A;
+  long long lda;
+  const double* w;
+  int wmod;
+  const Cx<double>* B;
+  long long ldb;
+  Cx<double>* C;
+  long long ldc;
+  double alpha, beta;
+};
+
+__device__ __forceinline__ void dm_cp16(Cx<double>* dst, const Cx<double>* src, bool valid) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(d), "l"(src), "r"(valid ? 16 : 0) : "memory");
+}
+__device__ __forceinline__ void dmma(double (&c)[2], double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+               : "+d"(c[0]), "+d"(c[1])
+               : "d"(a), "d"(b));
+}
+
+__global__ void __launch_bounds__(DM_THREADS, 2) dmma_dense_kernel(DmArgs p) {
+  extern __shared__ __align__(16) unsigned char dm_raw[];
+  Cx<double>* As = reinterpret_cast<Cx<double>*>(dm_raw);   // [2][DM_BK][DM_APAD]
+  Cx<double>* Bs = As + 2 * DM_BK * DM_APAD;                 // [2][DM_BK][DM_BPAD]
+  double* ws = reinterpret_cast<double*>(Bs + 2 * DM_BK * DM_BPAD);  // [2][DM_BK]
+  const int m0 = blockIdx.x * DM_BM, n0 = blockIdx.y * DM_BN;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int wm = warp & 3, wn = warp >> 2;
+  const int lr = lane >> 2, lc = lane & 3;
+  double cr[4][2][2], ci[4][2][2];
+#pragma unroll
+  for (int t = 0; t < 4; ++t)
+#pragma unroll
+    for (int u = 0; u < 2; ++u) cr[t][u][0] = cr[t][u][1] = ci[t][u][0] = ci[t][u][1] = 0.0;
+
+  const int nkb = (p.K + DM_BK - 1) / DM_BK;
+  auto load = [&](int kb, int s) {
+    const int k0 = kb * DM_BK;
+    Cx<double>* as = As + s * DM_BK * DM_APAD;
+    Cx<double>* bs = Bs + s * DM_BK * DM_BPAD;
+#pragma unroll
+    for (int i = threadIdx.x; i < DM_BK * DM_BM; i += DM_THREADS) {
+      const int kk = i / DM_BM, el = i % DM_BM;
+      const int k = k0 + kk, e = m0 + el;
+      const bool ok = k < p.K && e < p.M;
+      dm_cp16(as + kk * DM_APAD + el, ok ? p.A + (size_t)e + (size_t)p.lda * k : p.A, ok);
+    }
+#pragma unroll
+    for (int i = threadIdx.x; i < DM_BK * DM_BN; i += DM_THREADS) {
+      const int kk = i / DM_BN, jl = i % DM_BN;
+      const int k = k0 + kk, j = n0 + jl;
+      const bool ok = k < p.K && j < p.N;
+      dm_cp16(bs + kk * DM_BPAD + jl, ok ? p.B + (size_t)j + (size_t)p.ldb * k : p.B, ok);
+    }
+    if (threadIdx.x < DM_BK) {
+      const int k = k0 + threadIdx.x;
+      ws[s * DM_BK + threadIdx.x] = (k < p.K && p.w) ? p.w[k % p.wmod] : 1.0;
+    }
+    asm volatile("cp.async.commit_group;" ::: "memory");
+  };
+
+  load(0, 0);
+  for (int kb = 0; kb < nkb; ++kb) {
+    const int s = kb & 1;
+    if (kb + 1 < nkb) {
+      load(kb + 1, s ^ 1);  // stage s^1 was released by the barrier at the end of iteration kb-1
+      asm volatile("cp.async.wait_group 1;" ::: "memory");
+    } else {
+      asm volatile("cp.async.wait_group 0;" ::: "memory");
+    }
+    __syncthreads();
+    const Cx<double>* as = As + s * DM_BK * DM_APAD;
+    const Cx<double>* bs = Bs + s * DM_BK * DM_BPAD;
+#pragma unroll
+    for (int c = 0; c < DM_BK / 4; ++c) {
+      const int kk = 4 * c + lc;
+      const double w = ws[s * DM_BK + kk];
+      double ar[4], ai[4], nai[4], br[2], bi[2];
+#pragma unroll
+      for (int t = 0; t < 4; ++t) {
+        const Cx<double> a = as[kk * DM_APAD + wm * 32 + t * 8 + lr];
+        ar[t] = a.x * w;
+        ai[t] = a.y * w;
+        nai[t] = -ai[t];
+      }
+#pragma unroll
+      for (int u = 0; u < 2; ++u) {
+        const Cx<double> b = bs[kk * DM_BPAD + wn * 16 + u * 8 + lr];
+        br[u] = b.x;
+        bi[u] = b.y;
+      }
+#pragma unroll
+      for (int t = 0; t < 4; ++t)
+#pragma unroll
+        for (int u = 0; u < 2; ++u) {
+          dmma(cr[t][u], ar[t], br[u]);
+          dmma(cr[t][u], nai[t], bi[u]);
+          dmma(ci[t][u], ar[t], bi[u]);
+          dmma(ci[t][u], ai[t], br[u]);
+        }
+    }
+    __syncthreads();  // every warp is done with stage s before it is refilled
+  }
+#pragma unroll
+  for (int t = 0; t < 4; ++t) {
+    const int e = m0 + wm * 32 + t * 8 + lr;
+    if (e >= p.M) continue;
+#pragma unroll
+    for (int u = 0; u < 2; ++u)
+#pragma unroll
+      for (int i = 0; i < 2; ++i) {
+        const int j = n0 + wn * 16 + u * 8 + 2 * lc + i;
+        if (j >= p.N) continue;
+        Cx<double>* dst = p.C + (size_t)e + (size_t)p.ldc * j;
+        const double vr = p.alpha * cr[t][u][i], vi = p.alpha * ci[t][u][i];
+        if (p.beta == 0.0) {
+          *dst = cx<double>(vr, vi);
+        } else {
+          const Cx<double> o = *dst;
+          *dst = cx<double>(p.beta * o.x + vr, p.beta * o.y + vi);
+        }
+      }
+  }
+}
+
+static int launch_dmma_dense(const DmArgs& a, cudaStream_t st) {
+  static bool configured = false;
+  if (!configured) {
+    QCL_CUDA_CHECK(cudaFuncSetAttribute(dmma_dense_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)DM_SMEM));
+    configured = true;
+  }
+  dim3 grid((a.M + DM_BM - 1) / DM_BM, (a.N + DM_BN - 1) / DM_BN);
+  dmma_dense_kernel<<<grid, DM_THREADS, DM_SMEM, st>>>(a);
+  QCL_LAUNCH_CHECK("dmma_dense_kernel");
+  return QCL_OK;
+}
+
+// ---------------------------------------------------------------------------
 // Contraction dispatch
 // ---------------------------------------------------------------------------
 template <typename R>
@@ -239,6 +394,11 @@ static int contraction_t(const KernelOpDev& op, int NE, int Nk, int N, const dou
     if (sizeof(R) == 4 && op.tc_bhi)  // complex64 fields: tensor cores (3xTF32)
       return launch_tc_dense_contraction(NE, Nc, op.tc_bhi, op.tc_blo, Gv, Sv, alpha_q, beta, (float*)work,
                                          op.status, st);
+    if (sizeof(R) == 8) {  // complex128: FP64 tensor path (DMMA)
+      DmArgs d{NE, Nc, Nc, (const Cx<double>*)Gv, NEl, wk, Nk, (const Cx<double>*)op.matrix, Nc, (Cx<double>*)Sv, NEl,
+               alpha_q, beta};
+      return launch_dmma_dense(d, st);
+    }
     GemmArgs<R> g{};
     g.M = NE; g.Nout = Nc; g.K = Nc; g.batch = 1;
     g.A = G; g.lda = NEl; g.wk = wk; g.wk_mod = Nk;

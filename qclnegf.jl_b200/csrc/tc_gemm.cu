@@ -234,8 +234,11 @@ __global__ void __launch_bounds__(TC_THREADS, 1) tc_gemm_kernel(TcArgs p) {
       }
       tc_commit(mma_done + 8 * s);  // arrives even when nothing was issued, so no reader waits for good
     }
-    if (kb >= 1) drain(kb - 1);  // waits for the MMAs of block kb-1, reads their accumulator
-    if (ok && kb + 1 < nkb) load_block(kb + 1);  // into the stage block kb-1 has released
+    // once the MMAs of block kb-1 retire, their stage takes the copies of block
+    // kb+1 (issued before the accumulator read-out, so they land sooner)
+    if (kb >= 1 && !mbar_wait(mma_done + 8 * ((kb - 1) & 1), (uint32_t)(((kb - 1) >> 1) & 1))) ok = false;
+    if (ok && kb + 1 < nkb) load_block(kb + 1);
+    if (kb >= 1) drain(kb - 1);  // reads the accumulator of block kb-1
   }
   if (ok && nkb > 0) drain(nkb - 1);
   if (!ok) {

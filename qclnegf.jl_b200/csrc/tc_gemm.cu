@@ -31,25 +31,34 @@
 // buffer back.  Each truncated chain is then 12 accumulates long.
 // Every wait is bounded: a wait that gives up records QCL_TIMEOUT, the CTA
 // then waits (bounded) for its own MMAs, releases its tensor memory and ends.
+#include <cuda.h>  // CUtensorMap (the encoder is reached through cudaGetDriverEntryPoint)
+
+#include <mutex>
+
 #include "kernels.cuh"
 
 namespace qcl {
 
-constexpr int TC_BM = 128, TC_BN = 256, TC_BK = 32, TC_THREADS = 256;
-constexpr int TC_A_BYTES = TC_BM * TC_BK * 4;   // 16 KiB per A part
-constexpr int TC_B_BYTES = TC_BN * TC_BK * 4;   // 32 KiB per B part
+constexpr int TC_BM = 128, TC_BN = 256, TC_BK = 16;
+constexpr int TC_STAGES = 4;      // operand stages: the producer runs up to 3 blocks ahead
+constexpr int TC_ACC_KB = 2;      // K blocks per tensor-memory accumulation (12 MMAs)
+constexpr int TC_DRAIN_WARPS = 8; // warps that read accumulators out and write the tile
+constexpr int TC_THREADS = 32 * (TC_DRAIN_WARPS + 2);  // + producer warp + MMA warp
+constexpr int TC_A_BYTES = TC_BM * TC_BK * 4;   // 8 KiB per A part
+constexpr int TC_B_BYTES = TC_BN * TC_BK * 4;   // 16 KiB per B part
 constexpr int TC_STAGE_BYTES = 2 * TC_A_BYTES + 2 * TC_B_BYTES;
-constexpr int TC_SMEM_BYTES = 2 * TC_STAGE_BYTES + 1024 + 64;  // + alignment + barriers
+constexpr int TC_BAR_BYTES = 128;
+constexpr int TC_SMEM_BYTES = TC_STAGES * TC_STAGE_BYTES + 1024 + TC_BAR_BYTES;
 constexpr uint32_t TC_TMEM_COLS = 512;  // two 256-column accumulators
 constexpr long long TC_WAIT_LIMIT = 1ll << 22;  // try_wait rounds (~1 s) before a wait gives up
 
-// UMMA shared-memory descriptor, K-major, 128-byte swizzle: start address
-// (>> 4), leading byte offset 1 (unused for swizzled K-major), stride byte
-// offset 1024 B between 8-row groups (>> 4), descriptor version 1, swizzle
-// mode 2 (128B).
-__device__ __forceinline__ uint64_t umma_desc_k_sw128(uint32_t saddr) {
-  return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)1 << 16) | ((uint64_t)64 << 32) | ((uint64_t)1 << 46) |
-         ((uint64_t)2 << 61);
+// UMMA shared-memory descriptor, K-major, 64-byte swizzle (the layout TMA
+// writes with CU_TENSOR_MAP_SWIZZLE_64B): start address (>> 4), leading byte
+// offset 1 (unused for swizzled K-major), stride byte offset 512 B between
+// 8-row groups (>> 4), descriptor version 1, swizzle mode 4 (64B).
+__device__ __forceinline__ uint64_t umma_desc_k_sw64(uint32_t saddr) {
+  return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)1 << 16) | ((uint64_t)32 << 32) | ((uint64_t)1 << 46) |
+         ((uint64_t)4 << 61);
 }
 // Instruction descriptor: D f32, A/B tf32, both K-major, N = 256, M = 128.
 constexpr uint32_t TC_IDESC = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(TC_BN >> 3) << 17) |
@@ -59,6 +68,12 @@ __device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)_
 
 __device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
   asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
 }
 // Bounded parity wait; returns false if it gave up.
 __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
@@ -74,6 +89,15 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
   return false;
 }
 
+// 2D tiled TMA load (no multicast) of the box at (x = K offset, y = row).
+__device__ __forceinline__ void tma_load(uint32_t dst, const CUtensorMap* map, int x, int y, uint32_t bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::
+          "r"(dst),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(bar)
+      : "memory");
+}
+
 __device__ __forceinline__ void tc_mma(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t accumulate) {
   asm volatile(
       "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
@@ -85,38 +109,7 @@ __device__ __forceinline__ void tc_commit(uint32_t bar) {
   asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar) : "memory");
 }
 
-// Copies one K block (32 floats per row) of `rows` rows of a K-contiguous
-// matrix (row stride ld floats) into a 128B-swizzled tile: row r, 16-byte
-// chunk c lands at r * 128 + ((c ^ (r & 7)) << 4).
-__device__ __forceinline__ void stage_rows(uint32_t tile, const float* __restrict__ src, long long ld, int rows) {
-  const int chunks = rows * 8;
-  for (int i = threadIdx.x; i < chunks; i += TC_THREADS) {
-    const int r = i >> 3, c = i & 7;
-    const float* g = src + (long long)r * ld + c * 4;
-    const uint32_t d = tile + r * 128 + ((c ^ (r & 7)) << 4);
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(g) : "memory");
-  }
-}
-
-struct TcArgs {
-  int M;        // rows of C actually stored (N_E)
-  int Ncols;    // real columns of C actually stored (2 Nc)
-  int Kpad;     // padded real K (multiple of 32)
-  const float* Ahi;  // [Mpad][Kpad]
-  const float* Alo;
-  const float* Bhi;  // [Npad][Kpad]
-  const float* Blo;
-  Cx<float>* S;      // S[e + NE j], j < Ncols / 2
-  int NE;
-  double alpha, beta;
-  int* status;
-};
-
-__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
-  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
-}
-
-// Reads this thread's 32 columns [c, c + 32) of tensor-memory lane row `trow`.
+// Reads 32 consecutive accumulator columns of this thread's lane.
 __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&v)[32]) {
   asm volatile(
       "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
@@ -128,27 +121,54 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&v)[32]) {
       : "r"(taddr));
 }
 
-__global__ void __launch_bounds__(TC_THREADS, 1) tc_gemm_kernel(TcArgs p) {
+struct TcMaps {  // TMA descriptors of the four operand parts (K-contiguous rows)
+  CUtensorMap ahi, alo, bhi, blo;
+};
+
+struct TcArgs {
+  int M;        // rows of C actually stored (N_E)
+  int Ncols;    // real columns of C actually stored (2 Nc)
+  int Kpad;     // padded real K (multiple of 32)
+  Cx<float>* S; // S[e + NE j], j < Ncols / 2
+  int NE;
+  double alpha, beta;
+  int* status;
+};
+
+// Warp roles: warps 0-7 read accumulators out (warp w: tensor-memory lanes
+// 32 (w % 4) .. + 31, columns 128 (w / 4) .. + 127) into FP32 running sums and
+// write the tile; warp 8 lane 0 streams the operand blocks with TMA; warp 9
+// lane 0 issues the MMAs (warp 9 also owns the tensor-memory allocation).
+// Hand-offs are mbarriers only: full[s] (TMA bytes), empty[s] (MMAs done
+// reading stage s), acc_full[b] (accumulation in buffer b done), acc_empty[b]
+// (256 readers done with buffer b).
+__global__ void __launch_bounds__(TC_THREADS, 1) tc_gemm_kernel(const __grid_constant__ TcMaps maps, TcArgs p) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const uint32_t raw = smem_u32(smem_raw);
-  const uint32_t base = (raw + 1023u) & ~1023u;  // 1024-byte aligned tiles
+  const uint32_t base = (raw + 1023u) & ~1023u;  // 1024-byte aligned stages
   unsigned char* gbase = smem_raw + (base - raw);
-  // barriers after the two stages: mma_done[2] (tcgen05.commit), acc_empty[2] (256 readers)
-  const uint32_t bars = base + 2 * TC_STAGE_BYTES;
-  const uint32_t mma_done = bars, acc_empty = bars + 16;
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(gbase + 2 * TC_STAGE_BYTES + 32);
-  __shared__ int s_fail;
+  const uint32_t bars = base + TC_STAGES * TC_STAGE_BYTES;
+  const uint32_t full = bars, empty = bars + 8 * TC_STAGES, acc_full = bars + 16 * TC_STAGES, acc_empty = acc_full + 16;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(gbase + TC_STAGES * TC_STAGE_BYTES + 16 * TC_STAGES + 32);
+  __shared__ volatile int s_fail;
 
   const int m0 = blockIdx.x * TC_BM, n0 = blockIdx.y * TC_BN;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int nkb = p.Kpad / TC_BK;
+  const int nch = (nkb + TC_ACC_KB - 1) / TC_ACC_KB;
   if (threadIdx.x == 0) {
-    mbar_init(mma_done, 1);
-    mbar_init(mma_done + 8, 1);
-    mbar_init(acc_empty, TC_THREADS);
-    mbar_init(acc_empty + 8, TC_THREADS);
+    for (int i = 0; i < TC_STAGES; ++i) {
+      mbar_init(full + 8 * i, 1);
+      mbar_init(empty + 8 * i, 1);
+    }
+    for (int i = 0; i < 2; ++i) {
+      mbar_init(acc_full + 8 * i, 1);
+      mbar_init(acc_empty + 8 * i, 32 * TC_DRAIN_WARPS);
+    }
     s_fail = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
-  if (warp == 0) {
+  if (warp == TC_DRAIN_WARPS + 1) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
                  "r"(TC_TMEM_COLS)
                  : "memory");
@@ -158,104 +178,100 @@ __global__ void __launch_bounds__(TC_THREADS, 1) tc_gemm_kernel(TcArgs p) {
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const uint32_t tmem = *tmem_slot;
-  // this thread's accumulator rows / columns
-  const uint32_t tlane = (uint32_t)((warp & 3) * 32) << 16;
-  const int cbase = (warp >> 2) * 128;
-  float sum[128];
-#pragma unroll
-  for (int i = 0; i < 128; ++i) sum[i] = 0.0f;
+  int issued = 0;  // MMA warp: blocks whose MMAs were issued and committed
 
-  const int nkb = p.Kpad / TC_BK;
-  const float* Ahi = p.Ahi + (long long)m0 * p.Kpad;
-  const float* Alo = p.Alo + (long long)m0 * p.Kpad;
-  const float* Bhi = p.Bhi + (long long)n0 * p.Kpad;
-  const float* Blo = p.Blo + (long long)n0 * p.Kpad;
-  bool ok = true;
-  // adds accumulator buffer of block kb into the running sums and hands it back
-  auto drain = [&](int kb) {
-    const int b = kb & 1;
-    if (!mbar_wait(mma_done + 8 * b, (uint32_t)((kb >> 1) & 1))) {
-      ok = false;
-      return;
+  if (warp == TC_DRAIN_WARPS) {
+    // ---- producer ---------------------------------------------------------
+    if (lane == 0) {
+      int loaded = 0;
+      for (int kb = 0; kb < nkb && !s_fail; ++kb) {
+        const int s = kb % TC_STAGES;
+        if (kb >= TC_STAGES && !mbar_wait(empty + 8 * s, (uint32_t)((kb / TC_STAGES - 1) & 1))) {
+          s_fail = 1;
+          break;
+        }
+        loaded = kb + 1;
+        const uint32_t st = base + s * TC_STAGE_BYTES;
+        mbar_expect_tx(full + 8 * s, TC_STAGE_BYTES);
+        tma_load(st, &maps.ahi, kb * TC_BK, m0, full + 8 * s);
+        tma_load(st + TC_A_BYTES, &maps.alo, kb * TC_BK, m0, full + 8 * s);
+        tma_load(st + 2 * TC_A_BYTES, &maps.bhi, kb * TC_BK, n0, full + 8 * s);
+        tma_load(st + 2 * TC_A_BYTES + TC_B_BYTES, &maps.blo, kb * TC_BK, n0, full + 8 * s);
+      }
+      // after a failure, let the copies in flight land (bounded) before the CTA ends
+      if (s_fail && loaded > 0) {
+        const int kl = loaded - 1;
+        mbar_wait(full + 8 * (kl % TC_STAGES), (uint32_t)((kl / TC_STAGES) & 1));
+      }
     }
-    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    const uint32_t taddr = tmem + tlane + (uint32_t)(b * TC_BN + cbase);
-#pragma unroll
-    for (int c = 0; c < 4; ++c) {
-      uint32_t v[32];
-      tmem_ld32(taddr + c * 32, v);
-      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-#pragma unroll
-      for (int i = 0; i < 32; ++i) sum[c * 32 + i] += __uint_as_float(v[i]);
-    }
-    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-    mbar_arrive(acc_empty + 8 * b);
-  };
-  auto load_block = [&](int kb) {
-    const uint32_t st = base + (kb & 1) * TC_STAGE_BYTES;
-    const long long koff = (long long)kb * TC_BK;
-    stage_rows(st, Ahi + koff, p.Kpad, TC_BM);
-    stage_rows(st + TC_A_BYTES, Alo + koff, p.Kpad, TC_BM);
-    stage_rows(st + 2 * TC_A_BYTES, Bhi + koff, p.Kpad, TC_BN);
-    stage_rows(st + 2 * TC_A_BYTES + TC_B_BYTES, Blo + koff, p.Kpad, TC_BN);
-    asm volatile("cp.async.commit_group;" ::: "memory");
-  };
-  // Software pipeline: the copies of block kb+1 are issued as soon as the
-  // MMAs of block kb-1 (the last reader of that stage) retire, i.e. while the
-  // tensor core works on block kb.
-  if (nkb > 0) load_block(0);
-  for (int kb = 0; kb < nkb; ++kb) {
-    const int s = kb & 1;
-    const uint32_t st = base + s * TC_STAGE_BYTES;
-    const uint32_t tAh = st, tAl = st + TC_A_BYTES, tBh = st + 2 * TC_A_BYTES, tBl = tBh + TC_B_BYTES;
-    asm volatile("cp.async.wait_group 0;" ::: "memory");          // block kb has landed
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // generic writes -> tensor-core reads
-    if (__syncthreads_or(!ok)) {
-      ok = false;  // every thread leaves; none waits for blocks that were never issued
-      break;
-    }
-    if (threadIdx.x == 0) {
-      // accumulator buffer s was read out (block kb-2) by every thread at iteration kb-1
-      bool free_ok = kb < 2 || mbar_wait(acc_empty + 8 * s, (uint32_t)(((kb - 2) >> 1) & 1));
-      if (free_ok) {
+  } else if (warp == TC_DRAIN_WARPS + 1) {
+    // ---- MMA issue --------------------------------------------------------
+    if (lane == 0) {
+      for (int kb = 0; kb < nkb && !s_fail; ++kb) {
+        const int s = kb % TC_STAGES, ch = kb / TC_ACC_KB, b = ch & 1;
+        const bool first = kb % TC_ACC_KB == 0, last = (kb % TC_ACC_KB == TC_ACC_KB - 1) || kb == nkb - 1;
+        if (!mbar_wait(full + 8 * s, (uint32_t)((kb / TC_STAGES) & 1)) ||
+            (first && ch >= 2 && !mbar_wait(acc_empty + 8 * b, (uint32_t)(((ch - 2) >> 1) & 1)))) {
+          s_fail = 1;
+          break;
+        }
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-        const uint32_t dacc = tmem + (uint32_t)(s * TC_BN);
+        const uint32_t st = base + s * TC_STAGE_BYTES;
+        const uint32_t tAh = st, tAl = st + TC_A_BYTES, tBh = st + 2 * TC_A_BYTES, tBl = tBh + TC_B_BYTES;
+        const uint32_t dacc = tmem + (uint32_t)(b * TC_BN);
 #pragma unroll
         for (int ks = 0; ks < TC_BK / 8; ++ks) {  // K = 8 tf32 = 32 bytes per MMA
           const uint32_t off = ks * 32;
-          const uint64_t ah = umma_desc_k_sw128(tAh + off), al = umma_desc_k_sw128(tAl + off);
-          const uint64_t bh = umma_desc_k_sw128(tBh + off), bl = umma_desc_k_sw128(tBl + off);
-          tc_mma(dacc, ah, bh, ks > 0 ? 1u : 0u);
+          const uint64_t ah = umma_desc_k_sw64(tAh + off), al = umma_desc_k_sw64(tAl + off);
+          const uint64_t bh = umma_desc_k_sw64(tBh + off), bl = umma_desc_k_sw64(tBl + off);
+          tc_mma(dacc, ah, bh, (first && ks == 0) ? 0u : 1u);
           tc_mma(dacc, ah, bl, 1u);
           tc_mma(dacc, al, bh, 1u);
         }
-      } else {
-        ok = false;
+        tc_commit(empty + 8 * s);
+        if (last) tc_commit(acc_full + 8 * b);
+        issued = kb + 1;
       }
-      tc_commit(mma_done + 8 * s);  // arrives even when nothing was issued, so no reader waits for good
+      // the tensor memory is released below: let every issued MMA finish (bounded)
+      if (issued > 0) {
+        const int kl = issued - 1;
+        mbar_wait(empty + 8 * (kl % TC_STAGES), (uint32_t)((kl / TC_STAGES) & 1));
+      }
     }
-    // once the MMAs of block kb-1 retire, their stage takes the copies of block
-    // kb+1 (issued before the accumulator read-out, so they land sooner)
-    if (kb >= 1 && !mbar_wait(mma_done + 8 * ((kb - 1) & 1), (uint32_t)(((kb - 1) >> 1) & 1))) ok = false;
-    if (ok && kb + 1 < nkb) load_block(kb + 1);
-    if (kb >= 1) drain(kb - 1);  // reads the accumulator of block kb-1
-  }
-  if (ok && nkb > 0) drain(nkb - 1);
-  if (!ok) {
-    s_fail = 1;
-    if (threadIdx.x == 0) record_status(p.status, QCL_TIMEOUT, (long long)blockIdx.x + 65536ll * blockIdx.y);
-  }
-  __syncthreads();
-  if (s_fail && nkb > 0) {
-    // let the MMAs already issued drain (bounded) before the memory is released
-    const int last = nkb - 1;
-    mbar_wait(mma_done + 8 * (last & 1), (uint32_t)((last >> 1) & 1));
-  }
-
-  if (!s_fail) {
+  } else {
+    // ---- accumulator read-out and epilogue --------------------------------
+    const uint32_t tlane = (uint32_t)((warp & 3) * 32) << 16;
+    const int cbase = (warp >> 2) * 128;
+    float sum[128];
+#pragma unroll
+    for (int i = 0; i < 128; ++i) sum[i] = 0.0f;
+    bool ok = true;
+    for (int ch = 0; ch < nch; ++ch) {
+      const int b = ch & 1;
+      // warp-uniform decision: the tensor-memory loads below are .sync.aligned
+      const bool stop = __any_sync(0xffffffffu, s_fail != 0);
+      const bool got = __all_sync(0xffffffffu, !stop && mbar_wait(acc_full + 8 * b, (uint32_t)((ch >> 1) & 1)));
+      if (!got) {
+        ok = false;
+        s_fail = 1;
+        break;
+      }
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      const uint32_t taddr = tmem + tlane + (uint32_t)(b * TC_BN + cbase);
+#pragma unroll
+      for (int c = 0; c < 4; ++c) {
+        uint32_t v[32];
+        tmem_ld32(taddr + c * 32, v);
+        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+        for (int i = 0; i < 32; ++i) sum[c * 32 + i] += __uint_as_float(v[i]);
+      }
+      asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+      mbar_arrive(acc_empty + 8 * b);
+    }
     const int e = m0 + (warp & 3) * 32 + lane;
-    const float al = (float)p.alpha, be = (float)p.beta;
-    if (e < p.M) {
+    if (ok && e < p.M) {
+      const float al = (float)p.alpha, be = (float)p.beta;
 #pragma unroll
       for (int q = 0; q < 64; ++q) {
         const int nn = n0 + cbase + 2 * q;
@@ -273,7 +289,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1) tc_gemm_kernel(TcArgs p) {
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
-  if (warp == 0)
+  if (threadIdx.x == 0 && s_fail) record_status(p.status, QCL_TIMEOUT, (long long)blockIdx.x + 65536ll * blockIdx.y);
+  if (warp == TC_DRAIN_WARPS + 1)
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TC_TMEM_COLS) : "memory");
 }
 
@@ -366,6 +383,44 @@ int tc_build_operator(int Nc, int Nk, const void* Mop_c64, const double* wk, flo
   return QCL_OK;
 }
 
+typedef CUresult (*TensorMapEncodeTiled)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                          const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                          CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+static TensorMapEncodeTiled tensor_map_encoder() {
+  static TensorMapEncodeTiled fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = (TensorMapEncodeTiled)f;
+  });
+  return fn;
+}
+
+// K-contiguous FP32 matrix [rows][Kpad] in boxes of TC_BK x box_rows, 64B swizzle.
+static int make_operand_map(CUtensorMap* m, const float* ptr, int rows, int Kpad, int box_rows) {
+  TensorMapEncodeTiled enc = tensor_map_encoder();
+  if (!enc) {
+    set_last_error("cuTensorMapEncodeTiled is not available from the driver");
+    return QCL_CUDA;
+  }
+  const cuuint64_t dims[2] = {(cuuint64_t)Kpad, (cuuint64_t)rows};
+  const cuuint64_t strides[1] = {(cuuint64_t)Kpad * sizeof(float)};
+  const cuuint32_t box[2] = {(cuuint32_t)TC_BK, (cuuint32_t)box_rows};
+  const cuuint32_t es[2] = {1, 1};
+  const CUresult r = enc(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, (void*)ptr, dims, strides, box, es,
+                         CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                         CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) {
+    set_last_error("cuTensorMapEncodeTiled failed (%d) for a %d x %d operand", (int)r, rows, Kpad);
+    return QCL_CUDA;
+  }
+  return QCL_OK;
+}
+
 int launch_tc_dense_contraction(int NE, int Nc, const float* Bhi, const float* Blo, const void* G, void* S,
                                 double alpha, double beta, float* awork, int* status, cudaStream_t st) {
   int Mpad, Npad, Kpad;
@@ -380,9 +435,15 @@ int launch_tc_dense_contraction(int NE, int Nc, const float* Bhi, const float* B
     QCL_CUDA_CHECK(cudaFuncSetAttribute(tc_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM_BYTES));
     configured = true;
   }
-  TcArgs a{NE, 2 * Nc, Kpad, Ahi, Alo, Bhi, Blo, (Cx<float>*)S, NE, alpha, beta, status};
+  TcMaps maps;
+  int s;
+  if ((s = make_operand_map(&maps.ahi, Ahi, Mpad, Kpad, TC_BM))) return s;
+  if ((s = make_operand_map(&maps.alo, Alo, Mpad, Kpad, TC_BM))) return s;
+  if ((s = make_operand_map(&maps.bhi, Bhi, Npad, Kpad, TC_BN))) return s;
+  if ((s = make_operand_map(&maps.blo, Blo, Npad, Kpad, TC_BN))) return s;
+  TcArgs a{NE, 2 * Nc, Kpad, (Cx<float>*)S, NE, alpha, beta, status};
   dim3 grid(Mpad / TC_BM, Npad / TC_BN);
-  tc_gemm_kernel<<<grid, TC_THREADS, TC_SMEM_BYTES, st>>>(a);
+  tc_gemm_kernel<<<grid, TC_THREADS, TC_SMEM_BYTES, st>>>(maps, a);
   QCL_LAUNCH_CHECK("tc_gemm_kernel");
   return QCL_OK;
 }

@@ -47,6 +47,7 @@ extern "C" {
 #define QCL_KERNEL_MOMENTUM_INDEPENDENT 0
 #define QCL_KERNEL_DENSE 1
 #define QCL_KERNEL_IFR 2
+#define QCL_KERNEL_LOW_RANK 3
 
 #define QCL_C128 0
 #define QCL_C64 1
@@ -130,6 +131,9 @@ int qcl_apply_energy_shift(int precision, int NE, size_t ncols, const double* ep
  *   QCL_KERNEL_MOMENTUM_INDEPENDENT  block  (N^2, N^2), rows (a,b), cols (c,d)
  *   QCL_KERNEL_DENSE                 matrix (Nk N^2)^2, rows (m,a,b), cols (m',c,d)
  *   QCL_KERNEL_IFR                   left (N^2, J), right (J, N^2), radial (Nk, Nk)
+ *   QCL_KERNEL_LOW_RANK              left (Nk N^2, J), right = right_adjoint (J, Nk N^2),
+ *                                    J = rank >= 1 (LowRankProductionKernel, built by
+ *                                    _low_rank_production_kernel, production_cache.jl:348-385)
  * q is the kernel scale q^K; is_LO selects the phonon-shifted contraction in
  * the SCBA loop. */
 typedef struct qcl_mechanism {
@@ -222,6 +226,23 @@ typedef struct qcl_scba_problem {
   int precision;      /* QCL_C128 / QCL_C64 / QCL_MIXED */
   int verify_roundoff;/* repeat each Hilbert transform at 2L */
   int nmech;          /* number of mechanisms, in _SCATTERING_MECHANISM_ORDER */
+  /* Model switches of AlgorithmOptions (algorithm_options.jl:19-39; checked
+   * as in _check_algorithm_options, :42-93), applied to every scattering
+   * candidate; 0 is the reference default.
+   *   self_energy_structure 0 :full, 1 :diagonal -- off-diagonal entries
+   *     zeroed (_diagonalize_blocks!, production_operators.jl:1208-1217);
+   *   transverse_momentum 0 :resolved, 1 :averaged -- wk-weighted mean over
+   *     k, sum(wk) > 0 required (_average_transverse_momentum!, :1219-1238);
+   *   retarded_real_part 0 :kramers_kronig, 1 :drop -- Sigma^R = -i Gamma/2,
+   *     no Hilbert transform (_retarded_self_energy_selected, :1174-1177);
+   *   elastic_retarded 0 :hilbert, 1 :direct_green -- Sigma^R = K[G^R] for
+   *     the elastic (non-LO) mechanisms unless the real part is dropped
+   *     (_scattering_candidate_production, :1306-1311); a truncated low-rank
+   *     operator is rejected with it, as the reference rejects the pair. */
+  int self_energy_structure;
+  int transverse_momentum;
+  int retarded_real_part;
+  int elastic_retarded;
 } qcl_scba_problem;
 
 /* One SCBAIteration row (domain/types.jl:908).  status: QCL_OK or

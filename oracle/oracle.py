@@ -77,6 +77,7 @@ def _declare(l):
         "orc_contraction_momentum_independent": (None, [I, I, I, P, P, P, D, D, P]),
         "orc_contraction_dense": (None, [I, I, I, P, P, P, D, D, P]),
         "orc_contraction_ifr": (None, [I, I, I, I, P, P, P, P, P, D, D, P]),
+        "orc_contraction_low_rank": (None, [I, I, I, I, P, P, P, P, D, D, P]),
         "orc_direct_hilbert": (None, [I, Z, P, P, P, P, I]),
         "orc_fft_hilbert": (I, [I, Z, P, P, P, P, I]),
         "orc_fft_hilbert_roundoff": (I, [I, Z, P, P, P, P, P]),
@@ -256,7 +257,8 @@ def contraction_literal(K, G, wk, q=1.0):
 
 def contraction(mech, G, wk, alpha=1.0, beta=0.0, S=None):
     """production_static_contraction for one factorised operator
-    (production_operators.jl:402-658): S = beta S + alpha q K[wk G]."""
+    (production_operators.jl:402-658, the LowRank method at :597-658):
+    S = beta S + alpha q K[wk G]."""
     G = _field(G)
     NE, Nk, Nb, _ = G.shape
     if S is None:
@@ -272,6 +274,10 @@ def contraction(mech, G, wk, alpha=1.0, beta=0.0, S=None):
         J = mech.left.shape[1]
         lib().orc_contraction_ifr(NE, Nk, Nb, J, _p(_field(mech.left)), _p(_field(mech.right)),
                                   _p(_field(mech.radial)), _p(G), _p(wk), aq, float(beta), _p(S))
+    elif mech.kind == "low_rank":
+        r = mech.left.shape[1]
+        lib().orc_contraction_low_rank(NE, Nk, Nb, r, _p(_field(mech.left)), _p(_field(mech.right)), _p(G),
+                                       _p(wk), aq, float(beta), _p(S))
     else:
         raise ValueError(mech.kind)
     return S
@@ -426,9 +432,42 @@ def seed_green(problem):
     return dict(GR=GR, GL=GL, GG=GG, scale=scale), mu
 
 
+def apply_scattering_model(problem, family):
+    """_apply_scattering_model! (production_operators.jl:1240-1256):
+    _diagonalize_blocks! (:1208-1217) then _average_transverse_momentum!
+    (:1219-1238), on every component of one family."""
+    out = []
+    for X in family:
+        X = np.array(X, dtype=np.complex128, order="F")
+        NE, Nk, Nb, _ = X.shape
+        if getattr(problem, "self_energy_structure", "full") == "diagonal":
+            for b in range(Nb):
+                for a in range(Nb):
+                    if a != b:
+                        X[:, :, a, b] = 0
+        if getattr(problem, "transverse_momentum", "resolved") == "averaged":
+            w = np.asarray(problem.wk, dtype=np.float64)
+            norm = float(np.sum(w))
+            if not norm > 0:
+                raise OracleError(4, "radial weights must have positive sum")
+            for b in range(Nb):
+                for a in range(Nb):
+                    v = np.zeros(NE, dtype=np.complex128)
+                    for m in range(Nk):
+                        v = v + w[m] * X[:, m, a, b]
+                    v = v / norm
+                    X[:, :, a, b] = v[:, None]
+        out.append(X)
+    return tuple(out)
+
+
 def scattering_candidate(problem, green, plans, verify=True):
     """_scattering_candidate_production (production_operators.jl:1258-1335)
-    with the thermal-LO branch of _production_lo_contraction (:1045-1163)."""
+    with the thermal-LO branch of _production_lo_contraction (:1045-1163),
+    the retarded closure of _retarded_self_energy_selected (:1165-1206) and
+    the model switches (:1240-1256)."""
+    drop = getattr(problem, "retarded_real_part", "kramers_kronig") == "drop"
+    direct = getattr(problem, "elastic_retarded", "hilbert") == "direct_green"
     out = {}
     roundoff = 0.0
     wk = problem.wk
@@ -442,12 +481,16 @@ def scattering_candidate(problem, green, plans, verify=True):
         else:
             SL = contraction(mech, green["GL"], wk)
             SG = contraction(mech, green["GG"], wk)
-        if verify:
+        if direct and not drop and mech.name != "LO":
+            SR = contraction(mech, green["GR"], wk)
+        elif drop:
+            SR = np.asfortranarray(-0.5j * (1j * (SG - SL)))
+        elif verify:
             SR, _, r = retarded_self_energy(SL, SG, problem.eps, problem.wE, return_roundoff=True)
             roundoff = max(roundoff, r)
         else:
             SR, _ = retarded_self_energy(SL, SG, problem.eps, problem.wE)
-        out[mech.name] = (SR, SL, SG)
+        out[mech.name] = apply_scattering_model(problem, (SR, SL, SG))
     return out, roundoff
 
 

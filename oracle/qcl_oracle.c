@@ -479,8 +479,9 @@ void orc_contraction_literal(int NE, int Nk, int Nb, const dc *K, const dc *G,
 
 /* MomentumIndependentProductionKernel contraction
  * (production_operators.jl:535-595): X[(c,d),e] = sum_m' wk G[e,m',c,d];
- * Y = B X with B[(a,b),(c,d)] = K[a,c,d,b]; S = beta S + alpha q Y broadcast
- * over m.  `block` is K[1,1,:,:,:,:] in (a,c,d,b) col-major order. */
+ * Y = B X with B[(a,b),(c,d)] = K[1,1,a,c,d,b]; S = beta S + alpha q Y
+ * broadcast over m.  `block` is B as an (N^2, N^2) column-major matrix, rows
+ * (a,b) and columns (c,d), first index fastest (production_cache.jl:396-399). */
 void orc_contraction_momentum_independent(int NE, int Nk, int Nb, const dc *block,
                                           const dc *G, const double *wk, double alpha_q,
                                           double beta, dc *S) {
@@ -502,7 +503,7 @@ void orc_contraction_momentum_independent(int NE, int Nk, int Nb, const dc *bloc
           dc s = 0;
           for (int d = 0; d < Nb; ++d)
             for (int c = 0; c < Nb; ++c)
-              s += block[a + (size_t)Nb * (c + (size_t)Nb * (d + (size_t)Nb * b))] * X[c + Nb * d];
+              s += block[(a + (size_t)Nb * b) + (size_t)N2 * (c + (size_t)Nb * d)] * X[c + Nb * d];
           Y[a + Nb * b] = s;
         }
       for (int b = 0; b < Nb; ++b)
@@ -533,6 +534,34 @@ void orc_contraction_dense(int NE, int Nk, int Nb, const dc *M, const dc *G,
       size_t ix = e + (size_t)NE * row;
       S[ix] = (beta == 0.0 ? 0.0 : beta * S[ix]) + alpha_q * s;
     }
+}
+
+/* LowRankProductionKernel contraction (production_operators.jl:597-658):
+ * S[e,q] = beta S + alpha q sum_r left[q,r] sum_q' right_adjoint[r,q']
+ *          wk[q' % Nk] G[e,q'], q = (m,a,b) with m fastest. */
+void orc_contraction_low_rank(int NE, int Nk, int Nb, int rank, const dc *left /* Nc x rank */,
+                              const dc *right /* rank x Nc */, const dc *G, const double *wk,
+                              double alpha_q, double beta, dc *S) {
+  size_t Nc = (size_t)Nk * Nb * Nb;
+#pragma omp parallel
+  {
+    dc *T = malloc(sizeof(dc) * (rank > 0 ? rank : 1));
+#pragma omp for schedule(static)
+    for (int e = 0; e < NE; ++e) {
+      for (int r = 0; r < rank; ++r) {
+        dc s = 0;
+        for (size_t q = 0; q < Nc; ++q) s += right[r + (size_t)rank * q] * wk[q % Nk] * G[e + (size_t)NE * q];
+        T[r] = s;
+      }
+      for (size_t q = 0; q < Nc; ++q) {
+        dc s = 0;
+        for (int r = 0; r < rank; ++r) s += left[q + Nc * r] * T[r];
+        size_t ix = e + (size_t)NE * q;
+        S[ix] = (beta == 0.0 ? 0.0 : beta * S[ix]) + alpha_q * s;
+      }
+    }
+    free(T);
+  }
 }
 
 /* _SeparableIFRProductionKernel contraction (production_operators.jl:467-533):

@@ -429,6 +429,16 @@ int qcl_static_contraction(int precision, const qcl_mechanism* op, int NE, int N
     k.left = le.p;
     k.right = ri.p;
     k.radial = ra.p;
+  } else if (op->kind == QCL_KERNEL_LOW_RANK) {
+    if (op->J < 1) {
+      set_last_error("low-rank operator needs rank J >= 1");
+      return QCL_ARG;
+    }
+    const size_t nc = (size_t)Nk * N2;
+    if ((s = upload_converted(sp, op->left, nc * op->J, le))) return s;
+    if ((s = upload_converted(sp, op->right, nc * op->J, ri))) return s;
+    k.left = le.p;
+    k.right = ri.p;
   } else {
     set_last_error("unknown kernel kind %d", op->kind);
     return QCL_ARG;

@@ -7,7 +7,8 @@
 //   momentum independent: X[e,(c,d)] = sum_m' wk G[e,m',c,d]; Y = B X;
 //                         S[e,m,(a,b)] broadcast over m;
 //   dense:                S[e,(m,a,b)] = sum_(m',c,d) M wk[m'] G[e,(m',c,d)];
-//   separable IFR:        S = left * (radial * (wk .* (right * G))).
+//   separable IFR:        S = left * (radial * (wk .* (right * G)));
+//   low rank:             S = left * (right_adjoint * (wk .* G)).
 // Every stage is one call of a tiled complex GEMM whose operand and output
 // index maps are strided views of the E-fastest fields: the energy axis is the
 // GEMM's M dimension, so all A loads and C stores are coalesced along E.
@@ -437,6 +438,36 @@ static int contraction_t(const KernelOpDev& op, int NE, int Nk, int N, const dou
     f.alpha = alpha_q; f.beta = beta;
     return launch_gemm<R>(f, st);
   }
+  if (op.kind == QCL_KERNEL_LOW_RANK) {
+    // LowRankProductionKernel (production_operators.jl:597-658):
+    //   T[e, r] = sum_q right_adjoint[r, q] wk[q % Nk] G[e, q]      (NE x rank)
+    //   S[e, q] = alpha q^K sum_r left[q, r] T[e, r] + beta S[e, q]
+    const int Nc = Nk * N2, r = op.J;
+    Cx<R>* T = (Cx<R>*)work;
+    int s;
+    if (sizeof(R) == 8) {
+      DmArgs d1{NE, r, Nc, (const Cx<double>*)Gv, NEl, wk, Nk, (const Cx<double>*)op.right, r, (Cx<double>*)work,
+                NEl, 1.0, 0.0};
+      if ((s = launch_dmma_dense(d1, st))) return s;
+      DmArgs d2{NE, Nc, r, (const Cx<double>*)work, NEl, nullptr, 1, (const Cx<double>*)op.left, Nc,
+                (Cx<double>*)Sv, NEl, alpha_q, beta};
+      return launch_dmma_dense(d2, st);
+    }
+    GemmArgs<R> g{};
+    g.M = NE; g.Nout = r; g.K = Nc; g.batch = 1;
+    g.A = G; g.lda = NEl; g.wk = wk; g.wk_mod = Nk;
+    g.B = (const Cx<R>*)op.right; g.ldb_j = 1; g.ldb_k = r;
+    g.C = T; g.ldc = NEl; g.bcast = 1;
+    g.alpha = 1.0; g.beta = 0.0;
+    if ((s = launch_gemm<R>(g, st))) return s;
+    GemmArgs<R> f{};
+    f.M = NE; f.Nout = Nc; f.K = r; f.batch = 1;
+    f.A = T; f.lda = NEl;
+    f.B = (const Cx<R>*)op.left; f.ldb_j = 1; f.ldb_k = Nc;
+    f.C = S; f.ldc = NEl; f.bcast = 1;
+    f.alpha = alpha_q; f.beta = beta;
+    return launch_gemm<R>(f, st);
+  }
   set_last_error("unknown kernel operator kind %d", op.kind);
   return QCL_ARG;
 }
@@ -445,6 +476,7 @@ size_t contraction_work_elems(const KernelOpDev& op, int NE, int Nk, int N) {
   if (op.kind == QCL_KERNEL_MOMENTUM_INDEPENDENT) return (size_t)NE * N * N;
   if (op.kind == QCL_KERNEL_DENSE && op.tc_bhi) return (tc_a_work_floats(NE, Nk * N * N) + 1) / 2;  // complex64 units
   if (op.kind == QCL_KERNEL_IFR) return 2 * (size_t)NE * op.J * Nk;
+  if (op.kind == QCL_KERNEL_LOW_RANK) return (size_t)NE * op.J;
   return 0;
 }
 

@@ -17,6 +17,10 @@ int launch_weighted_trace(int NE, int Nk, const void* tr, const double* wE, cons
 int launch_paired_coefficients(const double* trL, const double* trG, int gs, double target, double* coeffs,
                                int* status, cudaStream_t st, double realness_limit = 1e-10);
 int launch_normalize_pair(int precision, size_t n, void* GL, void* GG, const double* coeffs, cudaStream_t st);
+// scattering-model switches (model.cu)
+int launch_retarded_drop(int precision, size_t n, const void* SL, const void* SG, void* SR, cudaStream_t st);
+int launch_scattering_model(int precision, int NE, int Nk, int N, const double* wk, double norm, int diagonal,
+                            int averaged, void* const* fields, cudaStream_t st);
 int launch_sum_fields(int precision, size_t n, const void* const* src, int count, void* out, cudaStream_t st);
 constexpr int kMaxMixFields = 32;
 size_t residual_mix_multi_partial_doubles(int nf);
@@ -47,8 +51,8 @@ struct KernelOpDev {
   int J = 0;
   const void* block = nullptr;   // (N^2, N^2): rows (a,b), cols (c,d)
   const void* matrix = nullptr;  // (Nk N^2)^2: rows (m,a,b), cols (m',c,d)
-  const void* left = nullptr;    // (N^2, J)
-  const void* right = nullptr;   // (J, N^2)
+  const void* left = nullptr;    // IFR (N^2, J); low rank (Nk N^2, rank)
+  const void* right = nullptr;   // IFR (J, N^2); low rank right_adjoint (rank, Nk N^2)
   const void* radial = nullptr;  // (Nk, Nk)
   // dense operators, complex64 fields: tensor-core (3xTF32) operand prepared by
   // tc_build_operator; when set, the contraction runs on tcgen05

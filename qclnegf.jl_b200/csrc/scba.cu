@@ -76,6 +76,8 @@ enum {
 
 struct ScbaCtx {
   int NE, Nk, N, M, precision, gs, verify;
+  int diagonal = 0, averaged = 0, drop_real = 0, direct_green = 0;  // scattering-model switches
+  double wk_sum = 0;
   double Ep, hw_LO, N_LO, target, eta_seed, kBT, alpha, J0;
   size_t nfield, fbytes;
   cudaStream_t st = nullptr;
@@ -244,6 +246,10 @@ int scba_create(const qcl_scba_problem* p, const qcl_mechanism* mechs, ScbaCtx**
   c->kBT = p->kBT;
   c->alpha = p->alpha;
   c->J0 = p->J0;
+  c->diagonal = p->self_energy_structure;
+  c->averaged = p->transverse_momentum;
+  c->drop_real = p->retarded_real_part;
+  c->direct_green = p->elastic_retarded;
   c->nfield = field_elems(c->NE, c->Nk, c->N);
   c->fbytes = c->nfield * (c->precision == QCL_C128 ? 16 : 8);
   c->eps_h.assign(p->eps, p->eps + p->NE);
@@ -258,6 +264,20 @@ int scba_create(const qcl_scba_problem* p, const qcl_mechanism* mechs, ScbaCtx**
   } while (0)
   double de;
   TRY(check_uniform_grid(c->NE, p->eps, &de));
+  // _check_algorithm_options (algorithm_options.jl:42-93) for the model switches
+  for (int sw : {c->diagonal, c->averaged, c->drop_real, c->direct_green})
+    if (sw != 0 && sw != 1)
+      TRY((set_last_error("model switches (self_energy_structure, transverse_momentum, retarded_real_part, "
+                          "elastic_retarded) must be 0 or 1"),
+           QCL_ARG));
+  for (int m = 0; m < c->Nk; ++m) c->wk_sum += p->wk[m];
+  if (c->averaged && !(c->wk_sum > 0)) TRY((set_last_error("radial weights must have positive sum"), QCL_ARG));
+  if (c->direct_green && !c->drop_real)
+    for (int i = 0; i < c->M; ++i)
+      if (mechs[i].kind == QCL_KERNEL_LOW_RANK && mechs[i].J < c->Nk * c->N * c->N)
+        TRY((set_last_error("direct_green elastic retarded closure requires an untruncated kernel; a truncated "
+                            "low-rank operator does not preserve adjoints and positivity"),
+             QCL_ARG));
   {
     cudaError_t e = cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking);
     if (e != cudaSuccess) TRY(cuda_status(e, "cudaStreamCreate"));
@@ -295,6 +315,11 @@ int scba_create(const qcl_scba_problem* p, const qcl_mechanism* mechs, ScbaCtx**
       TRY(upload_op(c, &d.left, q.left, (size_t)N2 * q.J));
       TRY(upload_op(c, &d.right, q.right, (size_t)q.J * N2));
       TRY(upload_op(c, &d.radial, q.radial, (size_t)c->Nk * c->Nk));
+    } else if (q.kind == QCL_KERNEL_LOW_RANK) {
+      if (q.J < 1) TRY((set_last_error("low-rank operator needs rank J >= 1"), QCL_ARG));
+      const size_t nc = (size_t)c->Nk * N2;
+      TRY(upload_op(c, &d.left, q.left, nc * q.J));
+      TRY(upload_op(c, &d.right, q.right, (size_t)q.J * nc));
     } else {
       TRY((set_last_error("unknown kernel kind %d", q.kind), QCL_ARG));
     }
@@ -341,7 +366,8 @@ int scba_create(const qcl_scba_problem* p, const qcl_mechanism* mechs, ScbaCtx**
 // ---------------------------------------------------------------------------
 // Candidate maps (stream-ordered launches; no host synchronisation)
 // ---------------------------------------------------------------------------
-static int scattering_candidates(ScbaCtx* c, const void* GL, const void* GG, std::vector<void*>& dst, bool verify) {
+static int scattering_candidates(ScbaCtx* c, const void* GR, const void* GL, const void* GG, std::vector<void*>& dst,
+                                 bool verify) {
   int s;
   const int p = c->precision;
   // contractions run at storage precision (mixed: FP32 with FP64 k-sums)
@@ -371,10 +397,22 @@ static int scattering_candidates(ScbaCtx* c, const void* GL, const void* GG, std
       if ((s = launch_contraction(cp, op, c->NE, c->Nk, c->N, c->wk, GL, SL, m.q, 0.0, c->cwork, c->st))) return s;
       if ((s = launch_contraction(cp, op, c->NE, c->Nk, c->N, c->wk, GG, SG, m.q, 0.0, c->cwork, c->st))) return s;
     }
-    if ((s = launch_hilbert(c->hil, cp, ncols, c->wE, nullptr, SL, SG, nullptr, field_of(dst, i, 0), nullptr, verify,
-                            c->st)))
+    void* SR = field_of(dst, i, 0);
+    if (c->drop_real) {
+      // Sigma^R = -i Gamma / 2 (production_operators.jl:1174-1177); no roundoff estimate
+      if ((s = launch_retarded_drop(cp, c->nfield, SL, SG, SR, c->st))) return s;
+    } else if (c->direct_green && !m.is_LO) {
+      // elastic closure Sigma^R = K[G^R] (production_operators.jl:1311-1316)
+      if ((s = launch_contraction(cp, op, c->NE, c->Nk, c->N, c->wk, GR, SR, m.q, 0.0, c->cwork, c->st))) return s;
+    } else {
+      if ((s = launch_hilbert(c->hil, cp, ncols, c->wE, nullptr, SL, SG, nullptr, SR, nullptr, verify, c->st)))
+        return s;
+      if (verify && (s = launch_combine(c->hil.partial, (int)ncols, 2, c->scal + SC_ROUND + 2 * i, c->st))) return s;
+    }
+    // _apply_scattering_model! (production_operators.jl:1240-1256)
+    void* fam[3] = {SR, SL, SG};
+    if ((s = launch_scattering_model(cp, c->NE, c->Nk, c->N, c->wk, c->wk_sum, c->diagonal, c->averaged, fam, c->st)))
       return s;
-    if (verify && (s = launch_combine(c->hil.partial, (int)ncols, 2, c->scal + SC_ROUND + 2 * i, c->st))) return s;
   }
   return QCL_OK;
 }
@@ -427,7 +465,7 @@ static int iteration_body(ScbaCtx* c, std::vector<void*>& state, std::vector<voi
   int s;
   const int sp = c->precision == QCL_MIXED ? QCL_C64 : c->precision;
   if ((s = current_green(c, state))) return s;
-  if ((s = scattering_candidates(c, c->GL, c->GG, cand, c->verify != 0))) return s;
+  if ((s = scattering_candidates(c, c->GR, c->GL, c->GG, cand, c->verify != 0))) return s;
   if ((s = embedding_candidates(c, cand))) return s;
   // candidate total lesser for r_K
   {
@@ -534,7 +572,7 @@ int scba_seed(ScbaCtx* c, double* mu_out) {
   QCL_CUDA_CHECK(cudaMemcpyAsync(f_d, f.data(), c->NE * sizeof(double), cudaMemcpyHostToDevice, c->st));
   if ((s = launch_seed_green(sp, c->NE, c->Nk, c->N, c->GR, f_d, c->GL, c->GG, c->st))) return s;
   // initial candidates (no roundoff verification), straight into the state
-  if ((s = scattering_candidates(c, c->GL, c->GG, c->state, false))) return s;
+  if ((s = scattering_candidates(c, c->GR, c->GL, c->GG, c->state, false))) return s;
   if ((s = embedding_candidates(c, c->state))) return s;
   QCL_CUDA_CHECK(cudaStreamSynchronize(c->st));
   QCL_CUDA_CHECK(cudaMemcpy(hst, c->status, sizeof(hst), cudaMemcpyDeviceToHost));

@@ -83,13 +83,14 @@ end
 
 """`production_static_contraction(op, G, wᵏ, qᴷ)` for the factorised
 operators: `:momentum_independent` (block), `:dense` (matrix), `:ifr`
-(left, right, radial).  Arrays must stay rooted during the call."""
+(left, right, radial), `:low_rank` (left, right = right_adjoint of a
+`LowRankProductionKernel`).  Arrays must stay rooted during the call."""
 function production_static_contraction(kind::Symbol, arrays::NamedTuple, G::Array{ComplexF64,4},
                                        wᵏ::Vector{Float64}, qᴷ::Real; α::Real = 1, β::Real = 0,
                                        Σ::Array{ComplexF64,4} = zeros(ComplexF64, size(G)))
     NE, Nk, Nb, _ = size(G)
     k = kind === :momentum_independent ? 0 : kind === :dense ? 1 : kind === :ifr ? 2 :
-        throw(ArgumentError("unknown kernel kind $kind"))
+        kind === :low_rank ? 3 : throw(ArgumentError("unknown kernel kind $kind"))
     GC.@preserve arrays begin
         p(name) = haskey(arrays, name) ? pointer(getfield(arrays, name)) : Ptr{ComplexF64}(C_NULL)
         J = haskey(arrays, :left) ? size(arrays.left, 2) : 0
@@ -125,6 +126,10 @@ struct Problem
     Ep::Float64; hw_LO::Float64; N_LO::Float64
     gs::Cint; target::Float64; eta_seed::Float64; kBT::Float64; alpha::Float64; J0::Float64
     precision::Cint; verify_roundoff::Cint; nmech::Cint
+    # AlgorithmOptions model switches, 0 = default:
+    # self_energy_structure (:full/:diagonal), transverse_momentum (:resolved/:averaged),
+    # retarded_real_part (:kramers_kronig/:drop), elastic_retarded (:hilbert/:direct_green)
+    self_energy_structure::Cint; transverse_momentum::Cint; retarded_real_part::Cint; elastic_retarded::Cint
 end
 
 struct Row

@@ -143,7 +143,7 @@ class _Mechanism(ctypes.Structure):
                 ("right", ctypes.c_void_p), ("radial", ctypes.c_void_p)]
 
 
-_KIND = {"momentum_independent": 0, "dense": 1, "ifr": 2}
+_KIND = {"momentum_independent": 0, "dense": 1, "ifr": 2, "low_rank": 3}
 
 
 def mechanism_struct(mech):

@@ -52,12 +52,15 @@ class Mechanism:
     """One enabled scattering mechanism in its factorised operator form.
 
     kind:
-      * ``"momentum_independent"`` -- ``block`` is ``K[1,1,:,:,:,:]`` in
-        ``(a,c,d,b)`` order (``production_cache.jl:394-398``);
+      * ``"momentum_independent"`` -- ``block`` is the ``(Nb^2, Nb^2)``
+        matrix of ``K[1,1,a,c,d,b]`` with rows ``(a,b)`` and columns ``(c,d)``
+        (``production_cache.jl:396-399``);
       * ``"dense"`` -- ``matrix`` has rows ``(m,a,b)`` and columns
         ``(m',c,d)`` (``production_cache.jl:400-405``);
       * ``"ifr"`` -- ``left (Nb^2,J)``, ``right (J,Nb^2)``, ``radial (Nk,Nk)``
-        (``production_cache.jl:414-448``).
+        (``production_cache.jl:414-448``);
+      * ``"low_rank"`` -- ``left (Nk Nb^2, r)`` (U S), ``right (r, Nk Nb^2)``
+        (V^H) of the dense matrix (``production_cache.jl:348-385``).
     ``q`` is the kernel scale ``q^K`` (``kernels.jl:388-405``).
     """
 
@@ -69,18 +72,24 @@ class Mechanism:
     left: Optional[np.ndarray] = None
     right: Optional[np.ndarray] = None
     radial: Optional[np.ndarray] = None
+    residual: float = 0.0  # low rank: attained relative discarded singular-value norm
 
     def literal_kernel(self, Nk: int, Nb: int) -> np.ndarray:
         """The six-index tensor K[m,m',a,c,d,b] this operator represents."""
         K = np.zeros((Nk, Nk, Nb, Nb, Nb, Nb), dtype=np.complex128, order="F")
         if self.kind == "momentum_independent":
+            # block[(a,b),(c,d)] -> K[a,c,d,b]
+            blk = np.transpose(np.asarray(self.block).reshape((Nb, Nb, Nb, Nb), order="F"), (0, 2, 3, 1))
             for m in range(Nk):
                 for mp in range(Nk):
-                    K[m, mp] = self.block
+                    K[m, mp] = blk
         elif self.kind == "dense":
             # rows (m,a,b), cols (m',c,d), first index fastest
             M = self.matrix.reshape((Nk, Nb, Nb, Nk, Nb, Nb), order="F")
             # M[m,a,b,m',c,d] -> K[m,m',a,c,d,b]
+            K[...] = np.transpose(M, (0, 3, 1, 4, 5, 2))
+        elif self.kind == "low_rank":
+            M = (self.left @ self.right).reshape((Nk, Nb, Nb, Nk, Nb, Nb), order="F")
             K[...] = np.transpose(M, (0, 3, 1, 4, 5, 2))
         elif self.kind == "ifr":
             J = self.left.shape[1]
@@ -93,6 +102,71 @@ class Mechanism:
         else:
             raise ValueError(self.kind)
         return K
+
+
+def _is_momentum_independent(K: np.ndarray) -> bool:
+    """_is_momentum_independent (production_cache.jl:338-346): every (m, m')
+    slice of K equals K[1,1]."""
+    ref = K[0, 0]
+    return all(np.array_equal(K[m, mp], ref) for m in range(K.shape[0]) for mp in range(K.shape[1]))
+
+
+def low_rank_production_kernel(name: str, q: float, matrix: np.ndarray, relative_tolerance: float = 0.0,
+                               maximum_rank: int = 0) -> Mechanism:
+    """_low_rank_production_kernel (production_cache.jl:348-385): thin SVD of
+    the dense (m,a,b) x (m',c,d) matrix, truncated at the smallest rank whose
+    discarded singular values have norm <= tol * ||s||, capped at
+    ``maximum_rank`` (0 = no cap).  ``left = U_r diag(s_r)``, ``right =
+    V_r^H``.  Raises ValueError (the reference's ArgumentError) when the cap
+    cannot meet the tolerance.  ``.residual`` holds the attained relative
+    discarded norm."""
+    if not 0.0 <= relative_tolerance < 1.0:
+        raise ValueError("low_rank_relative_tolerance must lie in [0,1)")
+    if maximum_rank < 0:
+        raise ValueError("low_rank_maximum_rank cannot be negative")
+    U, sv, Vh = np.linalg.svd(np.asarray(matrix, dtype=np.complex128), full_matrices=False)
+    total = float(np.linalg.norm(sv))
+    cap = len(sv) if maximum_rank == 0 else min(maximum_rank, len(sv))
+    rank = len(sv)
+    if total > 0 and relative_tolerance > 0:
+        tail = float(np.sum(np.abs(sv) ** 2))
+        for cand in range(len(sv)):
+            tail -= float(abs(sv[cand]) ** 2)
+            rank = cand + 1
+            if math.sqrt(max(tail, 0.0)) <= relative_tolerance * total:
+                break
+    rank = min(rank, cap)
+    discarded = 0.0 if rank == len(sv) else float(np.linalg.norm(sv[rank:]))
+    residual = 0.0 if total == 0 else discarded / total
+    if not residual <= relative_tolerance + 64 * np.finfo(np.float64).eps:
+        raise ValueError(f"low_rank_maximum_rank={cap} cannot satisfy the requested relative tolerance "
+                         f"{relative_tolerance} (attained {residual})")
+    left = np.asfortranarray(U[:, :rank] * sv[:rank][None, :])
+    right = np.asfortranarray(Vh[:rank, :])
+    return Mechanism(name, "low_rank", q, left=left, right=right, residual=residual)
+
+
+def production_kernel(name: str, q: float, K: np.ndarray, contraction: str = "dense_blas",
+                      low_rank_relative_tolerance: float = 0.0, low_rank_maximum_rank: int = 0) -> Mechanism:
+    """_production_kernel (production_cache.jl:387-409): the factorised
+    operator of a six-index kernel K[m,m',a,c,d,b].  A momentum-independent K
+    becomes its (a,b) x (c,d) block; otherwise K is permuted to the (m,a,b) x
+    (m',c,d) matrix, dense or truncated (``contraction="low_rank"``).
+    ``contraction="literal"`` keeps the literal six-index map, which as a
+    linear map is that same dense matrix, so it is returned in dense form."""
+    if contraction not in ("literal", "dense_blas", "low_rank"):
+        raise ValueError("contraction must be :literal, :dense_blas, or :low_rank")
+    K = np.asarray(K, dtype=np.complex128)
+    Nk, Nk2, Nb, Nb2, Nb3, Nb4 = K.shape
+    if not (Nk == Nk2 and Nb == Nb2 == Nb3 == Nb4):
+        raise ValueError("kernel order must be (m,m',a,c,d,b)")
+    if contraction != "literal" and _is_momentum_independent(K):
+        return Mechanism(name, "momentum_independent", q, block=block_matrix(K[0, 0]))
+    # rows (m,a,b), cols (m',c,d): permute (m,m',a,c,d,b) -> (m,a,b,m',c,d)
+    matrix = np.transpose(K, (0, 2, 5, 1, 3, 4)).reshape((Nk * Nb * Nb, Nk * Nb * Nb), order="F")
+    if contraction == "low_rank":
+        return low_rank_production_kernel(name, q, matrix, low_rank_relative_tolerance, low_rank_maximum_rank)
+    return Mechanism(name, "dense", q, matrix=np.asfortranarray(matrix))
 
 
 @dataclasses.dataclass
@@ -117,6 +191,11 @@ class SCBAProblem:
     mechanisms: List[Mechanism]
     J0: float = J0_A_M2
     name: str = "problem"
+    # scattering-model switches of AlgorithmOptions (algorithm_options.jl:19-39)
+    self_energy_structure: str = "full"           # or "diagonal"
+    transverse_momentum: str = "resolved"         # or "averaged"
+    retarded_real_part: str = "kramers_kronig"    # or "drop"
+    elastic_retarded: str = "hilbert"             # or "direct_green"
 
     @property
     def shape(self):
@@ -188,8 +267,16 @@ def _localized_states(rng, Nb, Nz=96, length=3.0):
     return x, np.full(Nz, dx), chi
 
 
+def block_matrix(K4: np.ndarray) -> np.ndarray:
+    """The (Nb^2, Nb^2) operator of a momentum-independent kernel slice
+    K[a,c,d,b]: rows (a,b), columns (c,d), first index fastest
+    (production_cache.jl:396-399)."""
+    Nb = K4.shape[0]
+    return np.asfortranarray(np.transpose(K4, (0, 3, 1, 2)).reshape((Nb * Nb, Nb * Nb), order="F"))
+
+
 def acoustic_block(chi, wx, prefactor):
-    """Deformation-potential kernel block K[a,c,d,b] = P sum_g w chi_a chi_c
+    """Deformation-potential kernel slice K[a,c,d,b] = P sum_g w chi_a chi_c
     chi_d chi_b (acoustic_kernel, numerics/reference/kernels.jl:246-283, real
     basis functions) in (a,c,d,b) order."""
     K = prefactor * np.einsum("g,ga,gc,gd,gb->acdb", wx, chi, chi, chi, chi)
@@ -222,7 +309,7 @@ def tutorial_problem(seed: int = 1, NE: int = 400, Nk: int = 16, alpha: float = 
     K0 = (E0_EV * E_CHARGE) ** 2 * (L0_NM * 1e-9) ** 2
     K = acoustic_block(chi, wx, pref / K0)
     q = float(np.max(np.abs(K)))
-    mech = Mechanism("acoustic", "momentum_independent", q, block=np.asfortranarray(K / q))
+    mech = Mechanism("acoustic", "momentum_independent", q, block=block_matrix(K / q))
     # 4.5e14 m^-2 sheet doping (presets.jl:62) in solver units (x L0^2)
     target = 4.5e14 * (L0_NM * 1e-9) ** 2
     kBT = KB_EV * 50.0 / E0_EV
@@ -264,7 +351,7 @@ def small_problem(seed=3, NE=33, Nk=3, Nb=4, mechanisms=("acoustic",), alpha=0.3
             K = acoustic_block(chi, wx, 1.0)
             q = float(np.max(np.abs(K)))
             mechs.append(Mechanism(name, "momentum_independent", strength * (1.3 if name == "alloy" else 1.0),
-                                   block=np.asfortranarray(K / q)))
+                                   block=block_matrix(K / q)))
         elif name in ("LO", "impurity"):
             # sum_h R_h(m,m') F_h (x) F_h^* -- the LO/impurity covariance form
             # (kernels.jl:321-356) with synthetic form factors.

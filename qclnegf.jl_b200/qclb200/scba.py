@@ -26,7 +26,29 @@ class _Problem(ctypes.Structure):
                 ("Ep", ctypes.c_double), ("hw_LO", ctypes.c_double), ("N_LO", ctypes.c_double),
                 ("gs", ctypes.c_int), ("target", ctypes.c_double), ("eta_seed", ctypes.c_double),
                 ("kBT", ctypes.c_double), ("alpha", ctypes.c_double), ("J0", ctypes.c_double),
-                ("precision", ctypes.c_int), ("verify_roundoff", ctypes.c_int), ("nmech", ctypes.c_int)]
+                ("precision", ctypes.c_int), ("verify_roundoff", ctypes.c_int), ("nmech", ctypes.c_int),
+                ("self_energy_structure", ctypes.c_int), ("transverse_momentum", ctypes.c_int),
+                ("retarded_real_part", ctypes.c_int), ("elastic_retarded", ctypes.c_int)]
+
+
+# AlgorithmOptions model switches -> the C ABI's 0/1 codes (_check_algorithm_options,
+# algorithm_options.jl:42-93, rejects any other symbol with an ArgumentError)
+_SWITCHES = {
+    "self_energy_structure": ("full", "diagonal"),
+    "transverse_momentum": ("resolved", "averaged"),
+    "retarded_real_part": ("kramers_kronig", "drop"),
+    "elastic_retarded": ("hilbert", "direct_green"),
+}
+
+
+def _switch_codes(problem):
+    codes = []
+    for name, choices in _SWITCHES.items():
+        v = getattr(problem, name, choices[0])
+        if v not in choices:
+            raise ValueError(f"{name} must be :{choices[0]} or :{choices[1]}")
+        codes.append(choices.index(v))
+    return codes
 
 
 class Row(ctypes.Structure):
@@ -59,7 +81,7 @@ class ProductionSCBA:
         ptr = [ctypes.c_void_p(a.ctypes.data) for a in self._keep]
         self._p = _Problem(pr.NE, pr.Nk, pr.Nb, *ptr, float(pr.Ep), float(pr.hw_LO), float(pr.N_LO), int(pr.gs),
                            float(pr.target), float(pr.eta_seed), float(pr.kBT), float(pr.alpha), float(pr.J0),
-                           self.precision, 1 if verify_roundoff else 0, len(pr.mechanisms))
+                           self.precision, 1 if verify_roundoff else 0, len(pr.mechanisms), *_switch_codes(pr))
         self._mechs = [mechanism_struct(m) for m in pr.mechanisms]
         arr = (type(self._mechs[0]) * max(len(self._mechs), 1))(*self._mechs) if self._mechs else None
         self._marr = arr

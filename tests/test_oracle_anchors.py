@@ -167,7 +167,7 @@ def test_contractions_equal_literal_six_index_map(orc):
     M = np.transpose(K, (0, 2, 5, 1, 3, 4)).reshape((Nk * Nb * Nb, Nk * Nb * Nb), order="F")
     dense = orc.contraction(Mechanism("x", "dense", q, matrix=np.asfortranarray(M)), G, wk)
     assert approx(dense, direct, rtol=2e-14, atol=2e-14)
-    block = rng.standard_normal((Nb,) * 4) + 1j * rng.standard_normal((Nb,) * 4)
+    block = rng.standard_normal((Nb * Nb,) * 2) + 1j * rng.standard_normal((Nb * Nb,) * 2)
     mech = Mechanism("y", "momentum_independent", q, block=np.asfortranarray(block))
     Kind = mech.literal_kernel(Nk, Nb)
     np.testing.assert_allclose(orc.contraction(mech, G, wk), orc.contraction_literal(Kind, G, wk, q),

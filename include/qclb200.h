@@ -165,6 +165,22 @@ int qcl_residual_suite(int precision, int NE, int Nk, int Nb, const double* eps,
                        const void* GL, const void* GG, const void* SR, const void* SL, const void* SG,
                        const void* SLc, double* out);
 
+/* The condition_number and dyson_scale fields of GreenState
+ * (domain/types.jl:733-740) for a Dyson solve: per block D = (eps + i eta) I
+ * - h - SR, kappa = cond_2(D) = ||D||_2 ||D^-1||_2 (LAPACK cond via SVD in
+ * retarded_green, numerics/reference/greens.jl:38, and
+ * _retarded_green_production, production_operators.jl:1379) and the
+ * row-sum scale s.  GR must be the Dyson output for the same inputs (it is
+ * D^-1); SR may be NULL (zero); kappa / scale are (N_E, N_k) float64, either
+ * may be NULL. */
+int qcl_condition_number(int precision, int NE, int Nk, int Nb, const double* eps, double eta, const void* h,
+                         const void* SR, const void* GR, double* kappa, double* scale);
+
+/* A = i (GR - GR^H) per block: spectral_function (numerics/reference/
+ * greens.jl:50-57), the A field written by _green_state_production
+ * (production_operators.jl:1387-1415). */
+int qcl_spectral_function(int precision, int NE, int Nk, int Nb, const void* GR, void* A);
+
 /* Eigenvalues (unsorted) of `count` Hermitian n x n matrices stored back to
  * back (column-major complex128; the Hermitian part is used), n <= 48.
  * Replaces the per-block LAPACK zheev calls of the residual suite
@@ -281,6 +297,11 @@ int qcl_scba_download(qcl_scba* ctx, int which, void* host);
 int qcl_scba_upload(qcl_scba* ctx, int which, const void* host);
 /* Replay each iteration as one captured CUDA graph (default off). */
 int qcl_scba_use_graph(qcl_scba* ctx, int enable);
+/* The derived GreenState fields of the last Dyson solve (seed or step) --
+ * A (a field in the context's storage precision), condition_number and
+ * dyson_scale ((N_E, N_k) float64) -- as _green_state_production returns
+ * them (production_operators.jl:1387-1415).  Any output may be NULL. */
+int qcl_scba_green_state(qcl_scba* ctx, void* A, double* kappa, double* scale);
 
 #ifdef __cplusplus
 }

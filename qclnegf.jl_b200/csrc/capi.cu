@@ -136,6 +136,7 @@ int scba_populations(ScbaCtx* c, double* out);
 int scba_download(ScbaCtx* c, int which, void* host);
 int scba_upload(ScbaCtx* c, int which, const void* host);
 int scba_set_graph(ScbaCtx* c, int enable);
+int scba_green_state(ScbaCtx* c, void* A, double* kappa, double* scale);
 
 static int shift_plan_dev(int NE, const double* eps, double delta, DevBuf& l, DevBuf& r, DevBuf& th, DevBuf& v,
                           ShiftPlanDev* out) {
@@ -633,6 +634,68 @@ int qcl_scba_populations(qcl_scba* ctx, double* out) { return scba_populations((
 int qcl_scba_download(qcl_scba* ctx, int which, void* host) { return scba_download((ScbaCtx*)ctx, which, host); }
 int qcl_scba_upload(qcl_scba* ctx, int which, const void* host) { return scba_upload((ScbaCtx*)ctx, which, host); }
 int qcl_scba_use_graph(qcl_scba* ctx, int enable) { return scba_set_graph((ScbaCtx*)ctx, enable); }
+int qcl_scba_green_state(qcl_scba* ctx, void* A, double* kappa, double* scale) {
+  if (!ctx) {
+    set_last_error("ctx is required");
+    return QCL_ARG;
+  }
+  return scba_green_state((ScbaCtx*)ctx, A, kappa, scale);
+}
+
+int qcl_condition_number(int precision, int NE, int Nk, int Nb, const double* eps, double eta, const void* h,
+                         const void* SR, const void* GR, double* kappa, double* scale) {
+  if (int s = check_precision(precision)) return s;
+  if (NE <= 0 || Nk <= 0 || Nb <= 0) {
+    set_last_error("condition_number: non-positive dimension (%d,%d,%d)", NE, Nk, Nb);
+    return QCL_DIM;
+  }
+  if (!eps || !h || !GR || (!kappa && !scale)) {
+    set_last_error("condition_number: eps, h, GR and at least one of kappa / scale are required");
+    return QCL_ARG;
+  }
+  if (!isfinite(eta)) {
+    set_last_error("condition_number: eta must be finite");
+    return QCL_ARG;
+  }
+  const int sp = precision == QCL_MIXED ? QCL_C64 : precision;
+  const size_t nf = field_elems(NE, Nk, Nb) * cbytes(sp), nb = (size_t)NE * Nk * sizeof(double);
+  DevBuf de, dh, dS, dG, dk, ds;
+  int s;
+  if ((s = de.upload(eps, NE * sizeof(double)))) return s;
+  if ((s = dh.upload(h, (size_t)Nk * Nb * Nb * 16))) return s;
+  if (SR && (s = dS.upload(SR, nf))) return s;
+  if ((s = dG.upload(GR, nf))) return s;
+  if (kappa && (s = dk.alloc(nb))) return s;
+  if (scale && (s = ds.alloc(nb))) return s;
+  if ((s = launch_condition(sp, NE, Nk, Nb, (const double*)de.p, eta, dh.p, SR ? dS.p : nullptr, dG.p,
+                            (double*)dk.p, (double*)ds.p, 0)))
+    return s;
+  QCL_CUDA_CHECK(cudaDeviceSynchronize());
+  if (kappa && (s = dk.download(kappa))) return s;
+  if (scale && (s = ds.download(scale))) return s;
+  return QCL_OK;
+}
+
+int qcl_spectral_function(int precision, int NE, int Nk, int Nb, const void* GR, void* A) {
+  if (int s = check_precision(precision)) return s;
+  if (NE <= 0 || Nk <= 0 || Nb <= 0) {
+    set_last_error("spectral_function: non-positive dimension (%d,%d,%d)", NE, Nk, Nb);
+    return QCL_DIM;
+  }
+  if (!GR || !A || GR == A) {
+    set_last_error("spectral_function: distinct GR and A are required");
+    return QCL_ARG;
+  }
+  const int sp = precision == QCL_MIXED ? QCL_C64 : precision;
+  const size_t nf = field_elems(NE, Nk, Nb) * cbytes(sp);
+  DevBuf dG, dA;
+  int s;
+  if ((s = dG.upload(GR, nf))) return s;
+  if ((s = dA.alloc(nf))) return s;
+  if ((s = launch_spectral(sp, NE, Nk, Nb, dG.p, dA.p, 0))) return s;
+  QCL_CUDA_CHECK(cudaDeviceSynchronize());
+  return dA.download(A);
+}
 
 int qcl_retarded_self_energy(int precision, int NE, size_t ncols, const double* eps, const double* wE,
                              const void* SL, const void* SG, void* SR, void* Gam, double* roundoff) {

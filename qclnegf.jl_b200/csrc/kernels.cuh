@@ -17,6 +17,10 @@ int launch_weighted_trace(int NE, int Nk, const void* tr, const double* wE, cons
 int launch_paired_coefficients(const double* trL, const double* trG, int gs, double target, double* coeffs,
                                int* status, cudaStream_t st, double realness_limit = 1e-10);
 int launch_normalize_pair(int precision, size_t n, void* GL, void* GG, const double* coeffs, cudaStream_t st);
+// condition number / Dyson scale and the spectral function (residual.cu)
+int launch_condition(int precision, int NE, int Nk, int N, const double* eps, double eta, const void* h,
+                     const void* SR, const void* GR, double* kappa, double* scale, cudaStream_t st);
+int launch_spectral(int precision, int NE, int Nk, int N, const void* GR, void* A, cudaStream_t st);
 // scattering-model switches (model.cu)
 int launch_retarded_drop(int precision, size_t n, const void* SL, const void* SG, void* SR, cudaStream_t st);
 int launch_scattering_model(int precision, int NE, int Nk, int N, const double* wk, double norm, int diagonal,

@@ -673,6 +673,164 @@ int launch_eigvals(int n, long long count, const void* A, double* vals, cudaStre
   return QCL_OK;
 }
 
+// ---------------------------------------------------------------------------
+// Condition number and Dyson scale per (E,k) block: the condition_number and
+// dyson_scale fields of GreenState (domain/types.jl:733-740) as
+// retarded_green / _retarded_green_production write them
+// (numerics/reference/greens.jl:30-41, production_operators.jl:1362-1380):
+//   D = (eps_e + i eta) I - h_m - SigmaR_em,  s = max_a sum_b |D_ab|,
+//   kappa = cond_2(D) = ||D||_2 ||D^-1||_2.
+// D is rebuilt from the Dyson inputs and D^-1 is the G^R the Dyson kernel
+// produced for them.  The reference takes cond(D) from an SVD (zgesvd); here
+// each spectral norm is sqrt(lmax(X X^H)) by the tridiagonal multisection of
+// the residual suite.  Nothing in the SCBA loop reads kappa, so it is computed
+// on request only.
+// ---------------------------------------------------------------------------
+template <typename RS> struct CondArgs {
+  int NE, Nk, N;
+  const double* eps;
+  double eta;
+  const Cx<double>* h;
+  const Cx<RS>* SR;  // may be NULL (Sigma^R = 0)
+  const Cx<RS>* GR;
+  double* kappa;     // (N_E, N_k) or NULL
+  double* scale;     // (N_E, N_k) or NULL
+};
+
+template <typename RS, int NP, int BPC>
+__global__ void __launch_bounds__(BPC* Tile<NP>::TT) condition_kernel(CondArgs<RS> p) {
+  constexpr int TT = Tile<NP>::TT;
+  constexpr size_t MSZ = (size_t)NP * NP;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  Cx<double>* bG = reinterpret_cast<Cx<double>*>(smem_raw);
+  Cx<double>* bX = bG + BPC * MSZ;
+  Cx<double>* bH = bX + BPC * MSZ;
+  ResScratch<NP>* scr = reinterpret_cast<ResScratch<NP>*>(bH + BPC * MSZ);
+  const int N = p.N, NE = p.NE, Nk = p.Nk;
+  const int m = blockIdx.y, e0 = blockIdx.x * BPC;
+  const int team = threadIdx.x / TT, tt = threadIdx.x % TT;
+  const int e = e0 + team;
+  const bool live = e < NE;
+  Cx<double>* G = bG + team * MSZ;
+  Cx<double>* X = bX + team * MSZ;
+  Cx<double>* H = bH + team * MSZ;
+  ResScratch<NP>& S = scr[team];
+
+  load_tile<RS, NP, BPC>(p.GR, bG, e0, m, NE, Nk, N);
+  if (p.SR) load_tile<RS, NP, BPC>(p.SR, bX, e0, m, NE, Nk, N);
+  __syncthreads();
+  const double eps_e = live ? p.eps[e] : 0.0;
+  for (int idx = tt; idx < N * N; idx += TT) {
+    const int i = idx % N, j = idx / N;
+    const Cx<double> hv = p.h[(size_t)m + (size_t)Nk * ((size_t)i + (size_t)N * j)];
+    const Cx<double> sr = p.SR ? X[sw<NP>(i, j)] : cx<double>(0, 0);
+    Cx<double> d = cx<double>(-hv.x - sr.x, -hv.y - sr.y);
+    if (i == j) {
+      d.x += eps_e;
+      d.y += p.eta;
+    }
+    X[sw<NP>(i, j)] = d;
+  }
+  team_sync<TT>(team);
+  // s = max row sum |D_ab| (row a per thread, then a team max)
+  double rowmax = 0;
+  for (int a = tt; a < N; a += TT) {
+    double r = 0;
+    for (int b = 0; b < N; ++b) {
+      const Cx<double> d = X[sw<NP>(a, b)];
+      r += hypot(d.x, d.y);
+    }
+    rowmax = fmax(rowmax, r);
+  }
+  rowmax = team_max<TT>(rowmax, tt, S.red, team);
+  double kappa = 0;
+  if (p.kappa) {
+    team_matmul<double, double, NP>(X, X, H, N, tt, true);  // D D^H
+    team_sync<TT>(team);
+    const double lD = team_lmax<NP, TT>(H, N, tt, S, team, false);
+    team_sync<TT>(team);
+    team_matmul<double, double, NP>(G, G, H, N, tt, true);  // D^-1 D^-H
+    team_sync<TT>(team);
+    const double lG = team_lmax<NP, TT>(H, N, tt, S, team, false);
+    kappa = (isfinite(lD) && isfinite(lG)) ? sqrt(fmax(lD, 0.0)) * sqrt(fmax(lG, 0.0)) : INFINITY;
+  }
+  if (live && tt == 0) {
+    const size_t o = (size_t)e + (size_t)NE * m;
+    if (p.kappa) p.kappa[o] = kappa;
+    if (p.scale) p.scale[o] = rowmax;
+  }
+}
+
+template <typename RS, int NP, int BPC> static int launch_condition_t(const CondArgs<RS>& a, cudaStream_t st) {
+  constexpr int TT = Tile<NP>::TT;
+  constexpr size_t smem = 3 * (size_t)BPC * NP * NP * sizeof(Cx<double>) + BPC * sizeof(ResScratch<NP>);
+  static bool configured = false;
+  if (!configured) {
+    QCL_CUDA_CHECK(cudaFuncSetAttribute(condition_kernel<RS, NP, BPC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)smem));
+    configured = true;
+  }
+  dim3 grid((a.NE + BPC - 1) / BPC, a.Nk);
+  condition_kernel<RS, NP, BPC><<<grid, BPC * TT, smem, st>>>(a);
+  QCL_LAUNCH_CHECK("condition_kernel");
+  return QCL_OK;
+}
+
+template <typename RS> static int launch_condition_p(const CondArgs<RS>& a, cudaStream_t st) {
+  switch (padded_size(a.N)) {
+    case 8: return launch_condition_t<RS, 8, 8>(a, st);
+    case 16: return launch_condition_t<RS, 16, 4>(a, st);
+    case 24: return launch_condition_t<RS, 24, 4>(a, st);
+    case 32: return launch_condition_t<RS, 32, 2>(a, st);
+    case 48: return launch_condition_t<RS, 48, 1>(a, st);
+    default:
+      set_last_error("basis size N_b=%d exceeds the supported maximum 48", a.N);
+      return QCL_UNSUPPORTED;
+  }
+}
+
+int launch_condition(int precision, int NE, int Nk, int N, const double* eps, double eta, const void* h,
+                     const void* SR, const void* GR, double* kappa, double* scale, cudaStream_t st) {
+  if (precision == QCL_C128) {
+    CondArgs<double> a{NE, Nk, N, eps, eta, (const Cx<double>*)h, (const Cx<double>*)SR, (const Cx<double>*)GR,
+                       kappa, scale};
+    return launch_condition_p<double>(a, st);
+  }
+  CondArgs<float> a{NE, Nk, N, eps, eta, (const Cx<double>*)h, (const Cx<float>*)SR, (const Cx<float>*)GR, kappa,
+                    scale};
+  return launch_condition_p<float>(a, st);
+}
+
+// A = i (G^R - G^R^H) per block (spectral_function, numerics/reference/
+// greens.jl:50-57; the A field written by _green_state_production,
+// production_operators.jl:1387-1415).  One thread per element; the transposed
+// partner is read from the same (E,k) column, so both reads stay coalesced
+// along E.
+template <typename R>
+__global__ void spectral_kernel(int NE, int Nk, int N, const Cx<R>* __restrict__ GR, Cx<R>* __restrict__ A) {
+  const long long blocks = (long long)NE * Nk, n = blocks * N * N;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const long long em = i % blocks, ab = i / blocks;
+    const int a = (int)(ab % N), b = (int)(ab / N);
+    const Cx<R> g = GR[i], gt = GR[em + blocks * ((long long)b + (long long)N * a)];
+    const double dx = (double)g.x - (double)gt.x, dy = (double)g.y + (double)gt.y;  // G - G^H
+    A[i] = cx<R>((R)(-dy), (R)dx);                                                  // i (G - G^H)
+  }
+}
+
+int launch_spectral(int precision, int NE, int Nk, int N, const void* GR, void* A, cudaStream_t st) {
+  const long long n = (long long)NE * Nk * N * N;
+  long long g = (n + 255) / 256;
+  if (g > 148 * 16) g = 148 * 16;
+  if (g < 1) g = 1;
+  if (precision == QCL_C128)
+    spectral_kernel<double><<<(unsigned)g, 256, 0, st>>>(NE, Nk, N, (const Cx<double>*)GR, (Cx<double>*)A);
+  else
+    spectral_kernel<float><<<(unsigned)g, 256, 0, st>>>(NE, Nk, N, (const Cx<float>*)GR, (Cx<float>*)A);
+  QCL_LAUNCH_CHECK("spectral_kernel");
+  return QCL_OK;
+}
+
 constexpr int RES_CTAS = 148;
 
 size_t residual_work_doubles(int NE, int Nk) { return 7 * (size_t)NE * Nk + 7 * RES_CTAS; }

@@ -113,6 +113,8 @@ struct ScbaCtx {
   double Jprev = NAN;
   std::vector<double> pprev, pops;
   bool seeded = false;
+  bool have_green = false;  // GR holds the Dyson solution of (eps + i green_eta, h, tot[0])
+  double green_eta = 0;
 };
 
 static void* field_of(const std::vector<void*>& v, int f, int c) { return v[3 * f + c]; }
@@ -582,6 +584,8 @@ int scba_seed(ScbaCtx* c, double* mu_out) {
   }
   if (mu_out) *mu_out = mu;
   c->seeded = true;
+  c->have_green = true;
+  c->green_eta = c->eta_seed;
   c->nu = 0;
   c->pending_commit = false;
   c->Jprev = NAN;
@@ -624,6 +628,8 @@ int scba_step(ScbaCtx* c, qcl_scba_row* row) {
   }
   int s = run_body(c);
   if (s) return s;
+  c->have_green = true;
+  c->green_eta = 0.0;
   QCL_CUDA_CHECK(cudaStreamSynchronize(c->st));
   int hst[2];
   QCL_CUDA_CHECK(cudaMemcpy(hst, c->status, sizeof(hst), cudaMemcpyDeviceToHost));
@@ -739,6 +745,41 @@ int scba_upload(ScbaCtx* c, int which, const void* host) {
   QCL_CUDA_CHECK(cudaMemcpyAsync(st[idx], host, c->fbytes, cudaMemcpyHostToDevice, c->st));
   QCL_CUDA_CHECK(cudaStreamSynchronize(c->st));
   c->seeded = true;
+  return QCL_OK;
+}
+
+// The derived GreenState fields of the last Dyson solve (seed or step):
+// A = i (G^R - G^R^H), condition_number = cond_2(D), dyson_scale = s
+// (_green_state_production, production_operators.jl:1387-1415, with the
+// kappa / scale outputs of _retarded_green_production, :1337-1385).  Any
+// output may be NULL; A is a field in the context's storage precision,
+// kappa and scale are (N_E, N_k) float64.
+int scba_green_state(ScbaCtx* c, void* A_host, double* kappa, double* scale) {
+  if (!c->have_green) {
+    set_last_error("green_state: no Green state yet (call seed or step first)");
+    return QCL_ARG;
+  }
+  const int sp = c->precision == QCL_MIXED ? QCL_C64 : c->precision;
+  const size_t nb = (size_t)c->NE * c->Nk * sizeof(double);
+  struct Tmp {
+    void* p[3] = {nullptr, nullptr, nullptr};
+    ~Tmp() {
+      for (void* q : p)
+        if (q) cudaFree(q);
+    }
+  } t;
+  int s;
+  if (A_host && (s = dalloc(&t.p[0], c->fbytes))) return s;
+  if (kappa && (s = dalloc(&t.p[1], nb))) return s;
+  if (scale && (s = dalloc(&t.p[2], nb))) return s;
+  if (A_host && (s = launch_spectral(sp, c->NE, c->Nk, c->N, c->GR, t.p[0], c->st))) return s;
+  if ((kappa || scale) && (s = launch_condition(sp, c->NE, c->Nk, c->N, c->eps, c->green_eta, c->h, c->tot[0], c->GR,
+                                                (double*)t.p[1], (double*)t.p[2], c->st)))
+    return s;
+  if (A_host) QCL_CUDA_CHECK(cudaMemcpyAsync(A_host, t.p[0], c->fbytes, cudaMemcpyDeviceToHost, c->st));
+  if (kappa) QCL_CUDA_CHECK(cudaMemcpyAsync(kappa, t.p[1], nb, cudaMemcpyDeviceToHost, c->st));
+  if (scale) QCL_CUDA_CHECK(cudaMemcpyAsync(scale, t.p[2], nb, cudaMemcpyDeviceToHost, c->st));
+  QCL_CUDA_CHECK(cudaStreamSynchronize(c->st));
   return QCL_OK;
 }
 

@@ -103,6 +103,30 @@ function production_static_contraction(kind::Symbol, arrays::NamedTuple, G::Arra
     return Σ
 end
 
+"""`condition_number(ε, h, Gᴿ, Σᴿ; η)` → `(κD, scaleD)`: the condition_number
+and dyson_scale outputs of `_retarded_green_production` for the Dyson solve
+that produced `Gᴿ`."""
+function condition_number(ε::Vector{Float64}, h::Array{ComplexF64,3}, Gᴿ::Array{ComplexF64,4},
+                          Σᴿ::Union{Nothing,Array{ComplexF64,4}} = nothing; η::Real = 0.0)
+    NE, Nk, Nb, _ = size(Gᴿ)
+    κ = zeros(Float64, NE, Nk); s = zeros(Float64, NE, Nk)
+    check(ccall((:qcl_condition_number, libqcl), Cint,
+                (Cint, Cint, Cint, Cint, Ptr{Float64}, Float64, Ptr{ComplexF64}, Ptr{ComplexF64},
+                 Ptr{ComplexF64}, Ptr{Float64}, Ptr{Float64}),
+                QCL_C128, NE, Nk, Nb, ε, Float64(η), h,
+                Σᴿ === nothing ? Ptr{ComplexF64}(C_NULL) : Σᴿ, Gᴿ, κ, s))
+    return κ, s
+end
+
+"""`spectral_function(Gᴿ)` = i(Gᴿ − Gᴿ†) per block."""
+function spectral_function(Gᴿ::Array{ComplexF64,4})
+    NE, Nk, Nb, _ = size(Gᴿ)
+    A = similar(Gᴿ)
+    check(ccall((:qcl_spectral_function, libqcl), Cint,
+                (Cint, Cint, Cint, Cint, Ptr{ComplexF64}, Ptr{ComplexF64}), QCL_C128, NE, Nk, Nb, Gᴿ, A))
+    return A
+end
+
 """`production_residual_suite(ε, h, green, total, candidate)` →
 `(r_D, r_A, r_K, r_PSD, r_caus)`."""
 function production_residual_suite(ε, h, Gᴿ, Gˡ, Gᵍ, Σᴿ, Σˡ, Σᵍ, candidate_Σˡ)

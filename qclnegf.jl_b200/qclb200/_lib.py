@@ -128,6 +128,8 @@ def _declare(l):
         "qcl_residual_suite": (I, [I, I, I, I, P, P, P, P, P, P, P, P, P, P]),
         "qcl_selfenergy_residual": (I, [I, Z, P, P, P]),
         "qcl_hermitian_eigvals": (I, [I, Z, P, P]),
+        "qcl_condition_number": (I, [I, I, I, I, P, D, P, P, P, P, P]),
+        "qcl_spectral_function": (I, [I, I, I, I, P, P]),
         "qcl_dev_residual_suite_noalloc": (I, [P, I, I, I, I, P, P, P, P, P, P, P, P, P, P]),
         "qcl_current_populations": (I, [I, I, I, I, P, P, I, D, P, P, P, P, P]),
         "qcl_scba_create": (I, [P, P, P]),
@@ -139,6 +141,7 @@ def _declare(l):
         "qcl_scba_download": (I, [P, I, P]),
         "qcl_scba_upload": (I, [P, I, P]),
         "qcl_scba_use_graph": (I, [P, I]),
+        "qcl_scba_green_state": (I, [P, P, P, P]),
     }
     for name, (res, args) in sig.items():
         if hasattr(l, name):

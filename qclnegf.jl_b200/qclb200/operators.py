@@ -137,6 +137,33 @@ def retarded_self_energy_fft(SL, SG, eps, wE, *, precision="c128", return_roundo
     return (SR, Gam, r.value) if return_roundoff else (SR, Gam)
 
 
+def condition_number(eps, h, GR, SR=None, *, eta=0.0, precision="c128"):
+    """(kappa, scale): cond_2(D) and the Dyson row-sum scale per (E,k) block,
+    D = (eps + i eta) I - h - SR -- the condition_number / dyson_scale outputs
+    of _retarded_green_production (production_operators.jl:1337-1385).  GR is
+    the Dyson solution for the same inputs."""
+    p = _prec(precision)
+    GR = _field(GR, _CDT[p])
+    NE, Nk, Nb, _ = GR.shape
+    h = _field(h, np.complex128, (Nk, Nb, Nb))
+    SR = None if SR is None else _field(SR, _CDT[p], GR.shape)
+    kappa = np.zeros((NE, Nk), order="F")
+    scale = np.zeros((NE, Nk), order="F")
+    check(lib().qcl_condition_number(p, NE, Nk, Nb, _ptr(_real(eps)), float(eta), _ptr(h),
+                                     None if SR is None else _ptr(SR), _ptr(GR), _ptr(kappa), _ptr(scale)))
+    return kappa, scale
+
+
+def spectral_function(GR, *, precision="c128"):
+    """A = i (GR - GR^H) per block (spectral_function, numerics/reference/greens.jl:50-57)."""
+    p = _prec(precision)
+    GR = _field(GR, _CDT[p])
+    NE, Nk, Nb, _ = GR.shape
+    A = np.zeros_like(GR, order="F")
+    check(lib().qcl_spectral_function(p, NE, Nk, Nb, _ptr(GR), _ptr(A)))
+    return A
+
+
 class _Mechanism(ctypes.Structure):
     _fields_ = [("kind", ctypes.c_int), ("is_LO", ctypes.c_int), ("J", ctypes.c_int), ("q", ctypes.c_double),
                 ("block", ctypes.c_void_p), ("matrix", ctypes.c_void_p), ("left", ctypes.c_void_p),

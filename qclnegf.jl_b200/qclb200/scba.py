@@ -142,6 +142,18 @@ class ProductionSCBA:
     def green(self):
         return dict(GR=self.download(0), GL=self.download(1), GG=self.download(2))
 
+    def green_state(self):
+        """The derived GreenState fields of the last Dyson solve: A, the
+        condition numbers cond_2(D) and the Dyson scales, (N_E, N_k) each
+        (_green_state_production, production_operators.jl:1387-1415)."""
+        pr = self.problem
+        A = np.zeros(pr.shape, dtype=_CDT[self.precision], order="F")
+        kappa = np.zeros((pr.NE, pr.Nk), order="F")
+        scale = np.zeros((pr.NE, pr.Nk), order="F")
+        check(lib().qcl_scba_green_state(self._h, ctypes.c_void_p(A.ctypes.data), ctypes.c_void_p(kappa.ctypes.data),
+                                         ctypes.c_void_p(scale.ctypes.data)))
+        return dict(A=A, condition_number=kappa, dyson_scale=scale)
+
     def family(self, f):
         """(SigmaR, Sigma<, Sigma>) of family f: 0..M-1 mechanisms, M plus, M+1 minus."""
         return tuple(self.download(3 + 3 * f + c) for c in range(3))

@@ -187,13 +187,33 @@ int qcl_spectral_function(int precision, int NE, int Nk, int Nb, const void* GR,
  * (_production_hermitian_eigvals!, numerics/optimized/residuals.jl:311-353). */
 int qcl_hermitian_eigvals(int n, size_t count, const void* H, double* vals);
 
+/* The positivity witness of a residual-suite evaluation (_PositivityWitness,
+ * numerics/reference/positivity_diagnostics.jl:41-91): over the blocks in the
+ * reference's order (e slow, m fast) and the six matrices in kind order, the
+ * first with the largest ratio (production_residual_suite, residuals.jl:
+ * 662-726; _production_positivity_witness, :773-779).  matrix_kind: -1 none,
+ * 0 spectral A, 1 occupied -iG<, 2 unoccupied iG>, 3 broadening Gamma,
+ * 4 raw occupied -i G S< G^H, 5 raw unoccupied i G S> G^H; indices 0-based. */
+typedef struct qcl_psd_witness {
+  int matrix_kind;
+  int energy_index;
+  int momentum_index;
+  double minimum_eigenvalue, block_norm, floor, ratio, absolute_defect, relative_defect, backward_error,
+      hermiticity_defect, construction_scale;
+} qcl_psd_witness;
+
+/* qcl_residual_suite plus its positivity witness. */
+int qcl_residual_suite_witness(int precision, int NE, int Nk, int Nb, const double* eps, const void* h,
+                               const void* GR, const void* GL, const void* GG, const void* SR, const void* SL,
+                               const void* SG, const void* SLc, double* out, qcl_psd_witness* witness);
+
 /* Allocation-free residual suite on device arrays (no counterpart in the
  * reference).  For callers that cannot call cudaMalloc -- a host whose
  * device memory belongs to its own pool allocator, a fixed up-front device
  * budget, or a loop that must not risk the synchronisation of an allocation.
  * Same result as qcl_residual_suite (out: 5 doubles in device memory, written
  * asynchronously on `stream`); the per-block scratch is a fixed device array
- * of the library (about 14.7 MB per GPU, held until exit), so N_E * N_k must
+ * of the library (about 18.9 MB per GPU, held until exit), so N_E * N_k must
  * not exceed 262144 (QCL_UNSUPPORTED otherwise).  Calls share that array:
  * calls that overlap on the GPU race.  The first call on a device looks up
  * the array's address on that device; make it before any stream capture. */
@@ -302,6 +322,10 @@ int qcl_scba_use_graph(qcl_scba* ctx, int enable);
  * dyson_scale ((N_E, N_k) float64) -- as _green_state_production returns
  * them (production_operators.jl:1387-1415).  Any output may be NULL. */
 int qcl_scba_green_state(qcl_scba* ctx, void* A, double* kappa, double* scale);
+/* The positivity witness of the last step's residual suite (the witness of
+ * its SCBAIteration row, production_solver.jl:611-619), valid until the next
+ * step or seed. */
+int qcl_scba_witness(qcl_scba* ctx, qcl_psd_witness* witness);
 
 #ifdef __cplusplus
 }

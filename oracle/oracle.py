@@ -88,6 +88,7 @@ def _declare(l):
         "orc_mix": (None, [Z, P, P, D]),
         "orc_relative_change": (D, [Z, P, P]),
         "orc_residual_suite": (None, [I, I, I, P, P, P, P, P, P, P, P, P, P]),
+        "orc_residual_witness": (None, [I, I, I, P, P, P, P, P, P, P]),
         "orc_dyson_keldysh": (I, [I, I, I, P, P, P, P, P, P, P, P, P]),
     }
     for name, (res, args) in sig.items():
@@ -356,6 +357,27 @@ def residual_suite(eps, h, GR, GL, GG, total, candidate_SL):
                              _p(_field(GG)), _p(_field(SR)), _p(_field(SL)), _p(_field(SG)),
                              _p(_field(candidate_SL)), _p(out))
     return dict(rD=out[0], rA=out[1], rK=out[2], rPSD=out[3], rcaus=out[4])
+
+
+WITNESS_KINDS = ("spectral", "occupied", "unoccupied", "broadening", "raw_occupied", "raw_unoccupied")
+WITNESS_FIELDS = ("minimum_eigenvalue", "block_norm", "floor", "ratio", "absolute_defect", "relative_defect",
+                  "backward_error", "hermiticity_defect", "construction_scale")
+
+
+def residual_witness(GR, GL, GG, total):
+    """The positivity witness of production_residual_suite
+    (residuals.jl:662-779, positivity_diagnostics.jl:41-91): kind (or
+    "none"), 0-based e, m and the nine witness numbers."""
+    NE, Nk, Nb, _ = GR.shape
+    ikem = np.zeros(3, dtype=np.int32)
+    w = np.zeros(9)
+    _, SL, SG = total
+    lib().orc_residual_witness(NE, Nk, Nb, _p(_field(GR)), _p(_field(GL)), _p(_field(GG)), _p(_field(SL)),
+                               _p(_field(SG)), ikem.ctypes.data_as(ctypes.c_void_p), _p(w))
+    out = dict(zip(WITNESS_FIELDS, w.tolist()))
+    out.update(matrix_kind="none" if ikem[0] < 0 else WITNESS_KINDS[ikem[0]], energy_index=int(ikem[1]),
+               momentum_index=int(ikem[2]))
+    return out
 
 
 def dyson_keldysh(eps, h, SR, SL, SG=None):

@@ -918,6 +918,88 @@ static double negative_part(int n, const dc *X, dc factor, dc *H, double *vals) 
   return fmax(0.0, absolute - budget) / fmax(bn, 2.2250738585072014e-308);
 }
 
+/* One witness candidate (_positivity_witness, numerics/reference/
+ * positivity_diagnostics.jl:61-91) for the Hermitian part of f X: w[0..8] =
+ * minimum_eigenvalue, block_norm, floor, ratio, absolute_defect,
+ * relative_defect, backward_error, hermiticity_defect, construction_scale.
+ * Returns 0 when X is non-finite (no candidate). */
+static int witness_candidate(int n, const dc *X, dc f, dc *H, double *vals, double *w) {
+  double herm = 0;
+  for (int j = 0; j < n; ++j)
+    for (int i = 0; i < n; ++i) {
+      dc v = f * MAT(X, i, j, n), u = f * MAT(X, j, i, n);
+      if (!isfinite(creal(v)) || !isfinite(cimag(v))) return 0;
+      MAT(H, i, j, n) = 0.5 * (v + conj(u));
+      dc d = v - conj(u);
+      herm += creal(d * conj(d));
+    }
+  orc_hermitian_eigvals(n, H, vals);
+  double lmin = vals[0], bn = 0;
+  for (int i = 0; i < n; ++i) bn = fmax(bn, fabs(vals[i]));
+  double budget = 64.0 * n * 2.220446049250313e-16 * fmax(bn, 1.0);
+  double absolute = fmax(0.0, -lmin), den = fmax(bn, 2.2250738585072014e-308);
+  w[0] = lmin; w[1] = bn; w[2] = budget; w[3] = fmax(0.0, absolute - budget) / den;
+  w[4] = absolute; w[5] = absolute / den; w[6] = budget; w[7] = sqrt(herm) / 2; w[8] = 1.0;
+  return 1;
+}
+
+/* The positivity witness of production_residual_suite
+ * (numerics/optimized/residuals.jl:662-726 collecting per chunk,
+ * _production_positivity_witness :773-779 reducing): over the blocks in the
+ * reference's order (e slow, m fast; residuals.jl:126-131) and the matrices
+ * in the order spectral A, occupied -iG<, unoccupied iG>, broadening Gam,
+ * raw occupied -i G S< G^H, raw unoccupied i G S> G^H (kinds 0..5), the
+ * first candidate with the largest ratio.  A non-finite primary matrix
+ * (kinds 0..3) is a candidate of ratio Inf with NaN eigen data
+ * (_nonfinite_positivity_witness, positivity_diagnostics.jl:56-57); a
+ * non-finite raw product is not a candidate.  ikem = {kind, e, m} 0-based
+ * (kind -1: none), w as in witness_candidate.  Single-threaded. */
+void orc_residual_witness(int NE, int Nk, int Nb, const dc *GR, const dc *GL, const dc *GG, const dc *SLt,
+                          const dc *SGt, int *ikem, double *w) {
+  int n = Nb;
+  dc *G = malloc(sizeof(dc) * n * n), *X = malloc(sizeof(dc) * n * n), *H = malloc(sizeof(dc) * n * n);
+  dc *T1 = malloc(sizeof(dc) * n * n), *T2 = malloc(sizeof(dc) * n * n);
+  double *vals = malloc(sizeof(double) * n), cand[9];
+  const double empty[9] = {0.0, 0.0, 0.0, -1.0, 0.0, 0.0, 0.0, 0.0, 1.0};
+  const dc factors[6] = {1.0, -I, I, 1.0, -I, I};
+  for (int k = 0; k < 9; ++k) w[k] = empty[k];
+  ikem[0] = -1; ikem[1] = 0; ikem[2] = 0;
+  for (int e = 0; e < NE; ++e)
+    for (int m = 0; m < Nk; ++m) {
+      for (int b = 0; b < n; ++b)
+        for (int a = 0; a < n; ++a) MAT(G, a, b, n) = GR[IX(e, m, a, b)];
+      for (int kind = 0; kind < 6; ++kind) {
+        for (int b = 0; b < n; ++b)
+          for (int a = 0; a < n; ++a) {
+            size_t ix = IX(e, m, a, b);
+            dc v = 0;
+            if (kind == 0) v = I * (MAT(G, a, b, n) - conj(MAT(G, b, a, n)));
+            else if (kind == 1) v = GL[ix];
+            else if (kind == 2) v = GG[ix];
+            else if (kind == 3) v = I * (SGt[ix] - SLt[ix]);
+            else v = kind == 4 ? SLt[ix] : SGt[ix];
+            MAT(X, a, b, n) = v;
+          }
+        if (kind >= 4) {
+          matmul(n, G, X, 0, T1);
+          matmul(n, T1, G, 1, T2);
+          memcpy(X, T2, sizeof(dc) * n * n);
+        }
+        int ok = witness_candidate(n, X, factors[kind], H, vals, cand);
+        if (!ok) {
+          if (kind >= 4) continue;
+          const double nf[9] = {NAN, INFINITY, 1e-14, INFINITY, NAN, NAN, 1e-14, 0.0, 1.0};
+          memcpy(cand, nf, sizeof(nf));
+        }
+        if (cand[3] > w[3]) {
+          memcpy(w, cand, sizeof(cand));
+          ikem[0] = kind; ikem[1] = e; ikem[2] = m;
+        }
+      }
+    }
+  free(G); free(X); free(H); free(T1); free(T2); free(vals);
+}
+
 /* production_residual_suite (numerics/optimized/residuals.jl:537-770), with
  * the definitions of validation.jl:33-103.  out = {rD, rA, rK, rPSD, rcaus}.
  * A = i(GR - GR^H) is formed per block; Gam = i(SG_total - SL_total). */

@@ -137,6 +137,7 @@ int scba_download(ScbaCtx* c, int which, void* host);
 int scba_upload(ScbaCtx* c, int which, const void* host);
 int scba_set_graph(ScbaCtx* c, int enable);
 int scba_green_state(ScbaCtx* c, void* A, double* kappa, double* scale);
+int scba_witness(ScbaCtx* c, double* out12);
 
 static int shift_plan_dev(int NE, const double* eps, double delta, DevBuf& l, DevBuf& r, DevBuf& th, DevBuf& v,
                           ShiftPlanDev* out) {
@@ -510,9 +511,24 @@ int qcl_embedding_component(int precision, int NE, int Nk, int Nb, const double*
   return dS.download(S);
 }
 
-int qcl_residual_suite(int precision, int NE, int Nk, int Nb, const double* eps, const void* h, const void* GR,
-                       const void* GL, const void* GG, const void* SR, const void* SL, const void* SG,
-                       const void* SLc, double* out) {
+static void witness_from_doubles(const double* v, qcl_psd_witness* w) {
+  w->matrix_kind = (int)v[0];
+  w->energy_index = (int)v[1];
+  w->momentum_index = (int)v[2];
+  w->minimum_eigenvalue = v[3];
+  w->block_norm = v[4];
+  w->floor = v[5];
+  w->ratio = v[6];
+  w->absolute_defect = v[7];
+  w->relative_defect = v[8];
+  w->backward_error = v[9];
+  w->hermiticity_defect = v[10];
+  w->construction_scale = v[11];
+}
+
+static int residual_suite_host(int precision, int NE, int Nk, int Nb, const double* eps, const void* h,
+                               const void* GR, const void* GL, const void* GG, const void* SR, const void* SL,
+                               const void* SG, const void* SLc, double* out, qcl_psd_witness* witness) {
   if (int s = check_precision(precision)) return s;
   if (!eps || !h || !GR || !GL || !GG || !SR || !SL || !SG || !SLc || !out) {
     set_last_error("all residual-suite arrays are required");
@@ -536,8 +552,38 @@ int qcl_residual_suite(int precision, int NE, int Nk, int Nb, const double* eps,
   if ((s = launch_residual_suite(sp, NE, Nk, Nb, (const double*)de.p, dh.p, d[0].p, d[1].p, d[2].p, d[3].p, d[4].p,
                                  d[5].p, d[6].p, (double*)work.p, (double*)o.p, 0)))
     return s;
+  DevBuf wpart, wout;
+  if (witness) {
+    if ((s = wpart.alloc(residual_witness_partial_doubles() * sizeof(double)))) return s;
+    if ((s = wout.alloc(12 * sizeof(double)))) return s;
+    if ((s = launch_residual_witness(sp, NE, Nk, Nb, d[0].p, d[1].p, d[2].p, d[4].p, d[5].p, (const double*)work.p,
+                                     (double*)wpart.p, (double*)wout.p, 0)))
+      return s;
+  }
   QCL_CUDA_CHECK(cudaDeviceSynchronize());
-  return o.download(out);
+  if ((s = o.download(out))) return s;
+  if (witness) {
+    double v[12];
+    if ((s = wout.download(v))) return s;
+    witness_from_doubles(v, witness);
+  }
+  return QCL_OK;
+}
+
+int qcl_residual_suite(int precision, int NE, int Nk, int Nb, const double* eps, const void* h, const void* GR,
+                       const void* GL, const void* GG, const void* SR, const void* SL, const void* SG,
+                       const void* SLc, double* out) {
+  return residual_suite_host(precision, NE, Nk, Nb, eps, h, GR, GL, GG, SR, SL, SG, SLc, out, nullptr);
+}
+
+int qcl_residual_suite_witness(int precision, int NE, int Nk, int Nb, const double* eps, const void* h,
+                               const void* GR, const void* GL, const void* GG, const void* SR, const void* SL,
+                               const void* SG, const void* SLc, double* out, qcl_psd_witness* witness) {
+  if (!witness) {
+    set_last_error("residual_suite_witness: witness output is required");
+    return QCL_ARG;
+  }
+  return residual_suite_host(precision, NE, Nk, Nb, eps, h, GR, GL, GG, SR, SL, SG, SLc, out, witness);
 }
 
 int qcl_hermitian_eigvals(int n, size_t count, const void* H, double* vals) {
@@ -640,6 +686,17 @@ int qcl_scba_green_state(qcl_scba* ctx, void* A, double* kappa, double* scale) {
     return QCL_ARG;
   }
   return scba_green_state((ScbaCtx*)ctx, A, kappa, scale);
+}
+
+int qcl_scba_witness(qcl_scba* ctx, qcl_psd_witness* witness) {
+  if (!ctx || !witness) {
+    set_last_error("ctx and witness are required");
+    return QCL_ARG;
+  }
+  double v[12];
+  if (int s = scba_witness((ScbaCtx*)ctx, v)) return s;
+  witness_from_doubles(v, witness);
+  return QCL_OK;
 }
 
 int qcl_condition_number(int precision, int NE, int Nk, int Nb, const double* eps, double eta, const void* h,

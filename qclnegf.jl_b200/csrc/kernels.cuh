@@ -21,6 +21,11 @@ int launch_normalize_pair(int precision, size_t n, void* GL, void* GG, const dou
 int launch_condition(int precision, int NE, int Nk, int N, const double* eps, double eta, const void* h,
                      const void* SR, const void* GR, double* kappa, double* scale, cudaStream_t st);
 int launch_spectral(int precision, int NE, int Nk, int N, const void* GR, void* A, cudaStream_t st);
+// positivity witness of a residual-suite run (residual.cu)
+int launch_residual_witness(int precision, int NE, int Nk, int N, const void* GR, const void* GL, const void* GG,
+                            const void* SL, const void* SG, const double* work, double* partial, double* out12,
+                            cudaStream_t st);
+size_t residual_witness_partial_doubles();
 // scattering-model switches (model.cu)
 int launch_retarded_drop(int precision, size_t n, const void* SL, const void* SG, void* SR, cudaStream_t st);
 int launch_scattering_model(int precision, int NE, int Nk, int N, const double* wk, double norm, int diagonal,

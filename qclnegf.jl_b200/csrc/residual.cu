@@ -28,6 +28,10 @@
 
 namespace qcl {
 
+// Per-block outputs: r_D, r_A num/den, r_K num/den, r_PSD, r_caus, and the
+// block's positivity-witness ratio and matrix kind.
+constexpr int kResidualBlockDoubles = 9;
+
 template <typename RS> struct ResidualArgs {
   int NE, Nk, N;
   const double* eps;
@@ -39,7 +43,7 @@ template <typename RS> struct ResidualArgs {
   const Cx<RS>* SL;
   const Cx<RS>* SG;
   const Cx<RS>* SLc;  // candidate total lesser
-  double* block_out;  // 7 doubles per block
+  double* block_out;  // kResidualBlockDoubles per block
 };
 
 struct JacobiRot {
@@ -439,6 +443,19 @@ __global__ void __launch_bounds__(BPC* Tile<NP>::TT) residual_kernel(ResidualArg
 
   // ---- spectral function A and its positivity ---------------------------------
   double psd = 0;
+  // positivity witness of this block: the largest ratio over the six matrices,
+  // the lowest kind index on ties (kinds: 0 spectral, 1 occupied, 2
+  // unoccupied, 3 broadening, 4 raw occupied, 5 raw unoccupied); a
+  // non-finite raw product is not a witness candidate
+  double wr = -1.0, wk = -1.0;
+  auto witness = [&](double r, int kind) {
+    psd = fmax(psd, r);
+    if (kind >= 4 && !isfinite(r)) return;
+    if (r > wr || (r == wr && kind < wk)) {
+      wr = r;
+      wk = kind;
+    }
+  };
   for (int idx = tt; idx < N * N; idx += TT) {
     const int i = idx % N, j = idx / N;
     const Cx<double> g = G[sw<NP>(i, j)], gt = G[sw<NP>(j, i)];
@@ -446,7 +463,7 @@ __global__ void __launch_bounds__(BPC* Tile<NP>::TT) residual_kernel(ResidualArg
     Y[sw<NP>(i, j)] = pi * cx<double>(g.x - gt.x, g.y + gt.y);
   }
   team_sync<TT>(team);
-  psd = fmax(psd, psd_of<NP, TT>(Y, one, H, N, tt, S, team));
+  witness(psd_of<NP, TT>(Y, one, H, N, tt, S, team), 0);
 
   // ---- Gamma = i (S> - S<), its positivity, r_A ---------------------------------
   __syncthreads();
@@ -459,7 +476,7 @@ __global__ void __launch_bounds__(BPC* Tile<NP>::TT) residual_kernel(ResidualArg
     X[sw<NP>(i, j)] = pi * cx<double>(g.x - l.x, g.y - l.y);
   }
   team_sync<TT>(team);
-  psd = fmax(psd, psd_of<NP, TT>(X, one, H, N, tt, S, team));
+  witness(psd_of<NP, TT>(X, one, H, N, tt, S, team), 3);
   team_matmul<double, double, NP>(G, X, W, N, tt, false);  // W = G Gam
   team_sync<TT>(team);
   team_matmul<double, double, NP>(W, G, H, N, tt, true);   // H = G Gam G^H
@@ -482,7 +499,7 @@ __global__ void __launch_bounds__(BPC* Tile<NP>::TT) residual_kernel(ResidualArg
     team_sync<TT>(team);
     team_matmul<double, double, NP>(W, G, Y, N, tt, true);
     team_sync<TT>(team);
-    psd = fmax(psd, psd_of<NP, TT>(Y, which == 0 ? mi : pi, H, N, tt, S, team));
+    witness(psd_of<NP, TT>(Y, which == 0 ? mi : pi, H, N, tt, S, team), 4 + which);
   }
 
   // ---- G< : positivity and r_K against the candidate lesser self-energy ----------
@@ -490,7 +507,7 @@ __global__ void __launch_bounds__(BPC* Tile<NP>::TT) residual_kernel(ResidualArg
   load_tile<RS, NP, BPC>(p.GL, bX, e0, m, NE, Nk, N);
   load_tile<RS, NP, BPC>(p.SLc, bY, e0, m, NE, Nk, N);
   __syncthreads();
-  psd = fmax(psd, psd_of<NP, TT>(X, mi, H, N, tt, S, team));
+  witness(psd_of<NP, TT>(X, mi, H, N, tt, S, team), 1);
   team_matmul<double, double, NP>(G, Y, W, N, tt, false);
   team_sync<TT>(team);
   team_matmul<double, double, NP>(W, G, H, N, tt, true);
@@ -508,10 +525,10 @@ __global__ void __launch_bounds__(BPC* Tile<NP>::TT) residual_kernel(ResidualArg
   __syncthreads();
   load_tile<RS, NP, BPC>(p.GG, bX, e0, m, NE, Nk, N);
   __syncthreads();
-  psd = fmax(psd, psd_of<NP, TT>(X, pi, H, N, tt, S, team));
+  witness(psd_of<NP, TT>(X, pi, H, N, tt, S, team), 2);
 
   if (tt == 0 && live) {
-    double* o = p.block_out + 7 * ((size_t)e + (size_t)NE * m);
+    double* o = p.block_out + kResidualBlockDoubles * ((size_t)e + (size_t)NE * m);
     o[0] = rD;
     o[1] = isfinite(aNum) ? aNum : INFINITY;
     o[2] = isfinite(aDen) ? aDen : INFINITY;
@@ -519,6 +536,8 @@ __global__ void __launch_bounds__(BPC* Tile<NP>::TT) residual_kernel(ResidualArg
     o[4] = isfinite(kDen) ? kDen : INFINITY;
     o[5] = psd;
     o[6] = caus;
+    o[7] = wr;
+    o[8] = wk;
   }
 }
 
@@ -528,7 +547,7 @@ __global__ void residual_reduce_kernel(long long blocks, const double* __restric
   double mx[3] = {0, 0, 0}, sm[4] = {0, 0, 0, 0};
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < blocks;
        i += (long long)gridDim.x * blockDim.x) {
-    const double* o = bo + 7 * i;
+    const double* o = bo + kResidualBlockDoubles * i;
     mx[0] = fmax(mx[0], o[0]) + (isnan(o[0]) ? INFINITY : 0.0);
     sm[0] += o[1];
     sm[1] += o[2];
@@ -831,21 +850,243 @@ int launch_spectral(int precision, int NE, int Nk, int N, const void* GR, void* 
   return QCL_OK;
 }
 
+// ---------------------------------------------------------------------------
+// Positivity witness of the residual suite (_positivity_witness,
+// numerics/reference/positivity_diagnostics.jl:41-91, collected per chunk in
+// production_residual_suite, numerics/optimized/residuals.jl:662-726, and
+// reduced by _production_positivity_witness, :773-779).  The reference scans
+// the blocks in the order lin = m + N_k e (e slow, m fast; residuals.jl:
+// 126-131) and the six matrices in kind order, keeping the first strict
+// maximum of the ratio: the witness is the (block, kind) of largest ratio,
+// lowest lin and then lowest kind on ties.  The residual kernel leaves each
+// block's best (ratio, kind); a deterministic arg-max over the blocks picks
+// the witness block, and one CTA recomputes that block's matrix and its full
+// spectrum for the reported numbers.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ bool witness_better(double r, long long lin, double r2, long long lin2) {
+  return r > r2 || (r == r2 && lin < lin2);
+}
+
+__global__ void witness_reduce_kernel(long long blocks, int NE, int Nk, const double* __restrict__ bo, double* partial) {
+  double br = -2.0, bk = -1.0;
+  long long bl = 0x7fffffffffffffffll;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < blocks;
+       i += (long long)gridDim.x * blockDim.x) {
+    const double* o = bo + kResidualBlockDoubles * i;
+    const double r = isnan(o[7]) ? INFINITY : o[7];
+    const long long lin = i / NE + (long long)Nk * (i % NE);
+    if (witness_better(r, lin, br, bl)) {
+      br = r;
+      bl = lin;
+      bk = o[8];
+    }
+  }
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) {
+    const double r2 = __shfl_xor_sync(0xffffffffu, br, off);
+    const long long l2 = __shfl_xor_sync(0xffffffffu, bl, off);
+    const double k2 = __shfl_xor_sync(0xffffffffu, bk, off);
+    if (witness_better(r2, l2, br, bl)) {
+      br = r2;
+      bl = l2;
+      bk = k2;
+    }
+  }
+  __shared__ double sr[32], sk[32];
+  __shared__ long long sl[32];
+  const int w = threadIdx.x >> 5;
+  if ((threadIdx.x & 31) == 0) {
+    sr[w] = br;
+    sl[w] = bl;
+    sk[w] = bk;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int q = 1; q < (int)(blockDim.x >> 5); ++q)
+      if (witness_better(sr[q], sl[q], br, bl)) {
+        br = sr[q];
+        bl = sl[q];
+        bk = sk[q];
+      }
+    partial[3 * blockIdx.x + 0] = br;
+    partial[3 * blockIdx.x + 1] = (double)bl;
+    partial[3 * blockIdx.x + 2] = bk;
+  }
+}
+
+template <typename RS> struct WitnessArgs {
+  int NE, Nk, N, ncta;
+  const Cx<RS>* GR;
+  const Cx<RS>* GL;
+  const Cx<RS>* GG;
+  const Cx<RS>* SL;  // totals
+  const Cx<RS>* SG;
+  const double* partial;  // ncta x (ratio, lin, kind)
+  double* out;            // kind, e, m, then the nine witness numbers
+};
+
+template <typename RS, int NP>
+__global__ void __launch_bounds__(Tile<NP>::TT) witness_detail_kernel(WitnessArgs<RS> p) {
+  constexpr int TT = Tile<NP>::TT;
+  constexpr size_t MSZ = (size_t)NP * NP;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  Cx<double>* G = reinterpret_cast<Cx<double>*>(smem_raw);
+  Cx<double>* X = G + MSZ;
+  Cx<double>* Y = X + MSZ;
+  Cx<double>* H = Y + MSZ;
+  ResScratch<NP>& S = *reinterpret_cast<ResScratch<NP>*>(H + MSZ);
+  __shared__ double best[3];
+  const int tt = threadIdx.x, N = p.N;
+  if (tt == 0) {
+    double br = -2.0, bk = -1.0;
+    long long bl = 0x7fffffffffffffffll;
+    for (int c = 0; c < p.ncta; ++c) {
+      const double r = p.partial[3 * c];
+      const long long l = (long long)p.partial[3 * c + 1];
+      if (witness_better(r, l, br, bl)) {
+        br = r;
+        bl = l;
+        bk = p.partial[3 * c + 2];
+      }
+    }
+    best[0] = br;
+    best[1] = (double)bl;
+    best[2] = bk;
+  }
+  __syncthreads();
+  const int kind = (int)best[2];
+  if (kind < 0) {  // no block: the empty witness (positivity_diagnostics.jl:58-59)
+    if (tt == 0) {
+      const double v[12] = {-1, 0, 0, 0.0, 0.0, 0.0, -1.0, 0.0, 0.0, 0.0, 0.0, 1.0};
+      for (int i = 0; i < 12; ++i) p.out[i] = v[i];
+    }
+    return;
+  }
+  const long long lin = (long long)best[1];
+  const int e = (int)(lin / p.Nk), m = (int)(lin % p.Nk);
+  load_tile<RS, NP, 1>(p.GR, G, e, m, p.NE, p.Nk, N);
+  if (kind == 1) load_tile<RS, NP, 1>(p.GL, X, e, m, p.NE, p.Nk, N);
+  if (kind == 2) load_tile<RS, NP, 1>(p.GG, X, e, m, p.NE, p.Nk, N);
+  if (kind == 3 || kind == 4) load_tile<RS, NP, 1>(p.SL, Y, e, m, p.NE, p.Nk, N);
+  if (kind == 3) load_tile<RS, NP, 1>(p.SG, X, e, m, p.NE, p.Nk, N);
+  if (kind == 5) load_tile<RS, NP, 1>(p.SG, Y, e, m, p.NE, p.Nk, N);
+  __syncthreads();
+  const Cx<double> pi = cx<double>(0, 1);
+  if (kind == 0 || kind == 3) {
+    for (int idx = tt; idx < N * N; idx += TT) {
+      const int i = idx % N, j = idx / N;
+      Cx<double> v;
+      if (kind == 0) {
+        const Cx<double> g = G[sw<NP>(i, j)], gt = G[sw<NP>(j, i)];
+        v = pi * cx<double>(g.x - gt.x, g.y + gt.y);  // A = i (G - G^H)
+      } else {
+        const Cx<double> g = X[sw<NP>(i, j)], l = Y[sw<NP>(i, j)];
+        v = pi * cx<double>(g.x - l.x, g.y - l.y);  // Gam = i (S> - S<)
+      }
+      H[sw<NP>(i, j)] = v;
+    }
+    __syncthreads();
+    for (int idx = tt; idx < N * N; idx += TT) X[sw<NP>(idx % N, idx / N)] = H[sw<NP>(idx % N, idx / N)];
+  } else if (kind >= 4) {
+    team_matmul<double, double, NP>(G, Y, H, N, tt, false);  // G S
+    __syncthreads();
+    team_matmul<double, double, NP>(H, G, X, N, tt, true);   // G S G^H
+  }
+  __syncthreads();
+  const Cx<double> f = (kind == 1 || kind == 4) ? cx<double>(0, -1) : (kind == 2 || kind == 5) ? pi : cx<double>(1, 0);
+  double bad = 0, herm = 0;
+  for (int idx = tt; idx < N * N; idx += TT) {
+    const int i = idx % N, j = idx / N;
+    const Cx<double> v = f * X[sw<NP>(i, j)], u = f * X[sw<NP>(j, i)];
+    if (!isfinite(v.x) || !isfinite(v.y)) bad = 1;
+    H[sw<NP>(i, j)] = cx<double>(0.5 * (v.x + u.x), 0.5 * (v.y - u.y));
+    const double dx = v.x - u.x, dy = v.y + u.y;  // v - conj(u)
+    herm += dx * dx + dy * dy;
+  }
+  bad = team_max<TT>(bad, tt, S.red, 0);
+  herm = team_sum<TT>(herm, tt, S.red, 0);
+  if (bad != 0) {  // _nonfinite_positivity_witness (positivity_diagnostics.jl:56-57)
+    if (tt == 0) {
+      const double v[12] = {(double)kind, (double)e, (double)m, NAN, INFINITY, 1e-14, INFINITY, NAN, NAN, 1e-14, 0.0,
+                            1.0};
+      for (int i = 0; i < 12; ++i) p.out[i] = v[i];
+    }
+    return;
+  }
+  team_eigvals<NP, TT>(H, N, tt, S, 0);
+  if (tt == 0) {
+    double lmin = INFINITY, bn = 0;
+    bool fin = true;
+    for (int i = 0; i < N; ++i) {
+      const double l = S.vals[i];
+      fin = fin && isfinite(l);
+      lmin = fmin(lmin, l);
+      bn = fmax(bn, fabs(l));
+    }
+    double* o = p.out;
+    o[0] = kind;
+    o[1] = e;
+    o[2] = m;
+    if (!fin) {
+      const double v[9] = {NAN, INFINITY, 1e-14, INFINITY, NAN, NAN, 1e-14, 0.0, 1.0};
+      for (int i = 0; i < 9; ++i) o[3 + i] = v[i];
+      return;
+    }
+    const double budget = 64.0 * N * 2.220446049250313e-16 * fmax(bn, 1.0);
+    const double absolute = fmax(0.0, -lmin), den = fmax(bn, 2.2250738585072014e-308);
+    o[3] = lmin;
+    o[4] = bn;
+    o[5] = budget;
+    o[6] = fmax(0.0, absolute - budget) / den;
+    o[7] = absolute;
+    o[8] = absolute / den;
+    o[9] = budget;
+    o[10] = sqrt(herm) / 2;
+    o[11] = 1.0;
+  }
+}
+
+template <typename RS, int NP> static int launch_witness_detail_t(const WitnessArgs<RS>& a, cudaStream_t st) {
+  constexpr size_t smem = 4 * (size_t)NP * NP * sizeof(Cx<double>) + sizeof(ResScratch<NP>);
+  static bool configured = false;
+  if (!configured) {
+    QCL_CUDA_CHECK(cudaFuncSetAttribute(witness_detail_kernel<RS, NP>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)smem));
+    configured = true;
+  }
+  witness_detail_kernel<RS, NP><<<1, Tile<NP>::TT, smem, st>>>(a);
+  QCL_LAUNCH_CHECK("witness_detail_kernel");
+  return QCL_OK;
+}
+
+template <typename RS> static int launch_witness_detail_p(const WitnessArgs<RS>& a, cudaStream_t st) {
+  switch (padded_size(a.N)) {
+    case 8: return launch_witness_detail_t<RS, 8>(a, st);
+    case 16: return launch_witness_detail_t<RS, 16>(a, st);
+    case 24: return launch_witness_detail_t<RS, 24>(a, st);
+    case 32: return launch_witness_detail_t<RS, 32>(a, st);
+    case 48: return launch_witness_detail_t<RS, 48>(a, st);
+    default:
+      set_last_error("basis size N_b=%d exceeds the supported maximum 48", a.N);
+      return QCL_UNSUPPORTED;
+  }
+}
+
 constexpr int RES_CTAS = 148;
 
-size_t residual_work_doubles(int NE, int Nk) { return 7 * (size_t)NE * Nk + 7 * RES_CTAS; }
+size_t residual_work_doubles(int NE, int Nk) { return kResidualBlockDoubles * (size_t)NE * Nk + 7 * RES_CTAS; }
 
 // ---------------------------------------------------------------------------
 // Allocation-free variant.  Some callers cannot call cudaMalloc: a Julia
 // session whose device memory is owned by its own pool allocator, a host
 // application that reserves a fixed device budget up front, or a solver loop
 // that must not pay the device synchronisation an allocation can imply.  For
-// them the residual suite's scratch (7 doubles per (E,k) block plus 7 per
+// them the residual suite's scratch (9 doubles per (E,k) block plus 7 per
 // reduction CTA) lives in this file-scope device array instead.  Every GPU
-// that loads the library holds it (about 14.7 MB) until the process exits.
+// that loads the library holds it (about 18.9 MB) until the process exits.
 // ---------------------------------------------------------------------------
 constexpr long long kNoAllocMaxBlocks = 1ll << 18;  // N_E * N_k <= 262144
-static __device__ __align__(256) double g_residual_scratch[7 * kNoAllocMaxBlocks + 7 * 148];
+static __device__ __align__(256) double g_residual_scratch[kResidualBlockDoubles * kNoAllocMaxBlocks + 7 * 148];
 
 static std::mutex g_noalloc_mutex;
 static double* g_noalloc_ptr[64] = {nullptr};
@@ -886,12 +1127,34 @@ int launch_residual_suite(int precision, int NE, int Nk, int N, const double* ep
     s = launch_residual_p<float>(a, st);
   }
   if (s) return s;
-  double* partial = work + 7 * (size_t)NE * Nk;
+  double* partial = work + kResidualBlockDoubles * (size_t)NE * Nk;
   residual_reduce_kernel<<<RES_CTAS, 256, 0, st>>>((long long)NE * Nk, work, partial);
   residual_final_kernel<<<1, 7 * 32, 0, st>>>(RES_CTAS, partial, out5);
   QCL_LAUNCH_CHECK("residual_reduce");
   return QCL_OK;
 }
+
+// The witness of the residual suite whose per-block outputs are in `work`
+// (the same work array and fields as the launch_residual_suite call before
+// it).  out12: kind, e, m, then minimum_eigenvalue, block_norm, floor, ratio,
+// absolute_defect, relative_defect, backward_error, hermiticity_defect,
+// construction_scale.  Uses 3 * RES_CTAS doubles of `partial` scratch.
+int launch_residual_witness(int precision, int NE, int Nk, int N, const void* GR, const void* GL, const void* GG,
+                            const void* SL, const void* SG, const double* work, double* partial, double* out12,
+                            cudaStream_t st) {
+  witness_reduce_kernel<<<RES_CTAS, 256, 0, st>>>((long long)NE * Nk, NE, Nk, work, partial);
+  QCL_LAUNCH_CHECK("witness_reduce_kernel");
+  if (precision == QCL_C128) {
+    WitnessArgs<double> a{NE, Nk, N, RES_CTAS, (const Cx<double>*)GR, (const Cx<double>*)GL, (const Cx<double>*)GG,
+                          (const Cx<double>*)SL, (const Cx<double>*)SG, partial, out12};
+    return launch_witness_detail_p<double>(a, st);
+  }
+  WitnessArgs<float> a{NE, Nk, N, RES_CTAS, (const Cx<float>*)GR, (const Cx<float>*)GL, (const Cx<float>*)GG,
+                       (const Cx<float>*)SL, (const Cx<float>*)SG, partial, out12};
+  return launch_witness_detail_p<float>(a, st);
+}
+
+size_t residual_witness_partial_doubles() { return 3 * RES_CTAS; }
 
 }  // namespace qcl
 

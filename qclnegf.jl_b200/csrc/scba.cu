@@ -114,6 +114,7 @@ struct ScbaCtx {
   std::vector<double> pprev, pops;
   bool seeded = false;
   bool have_green = false;  // GR holds the Dyson solution of (eps + i green_eta, h, tot[0])
+  bool have_residual = false;  // reswork holds the per-block residual outputs of the last step
   double green_eta = 0;
 };
 
@@ -586,6 +587,7 @@ int scba_seed(ScbaCtx* c, double* mu_out) {
   c->seeded = true;
   c->have_green = true;
   c->green_eta = c->eta_seed;
+  c->have_residual = false;  // the seed used the residual scratch
   c->nu = 0;
   c->pending_commit = false;
   c->Jprev = NAN;
@@ -630,6 +632,7 @@ int scba_step(ScbaCtx* c, qcl_scba_row* row) {
   if (s) return s;
   c->have_green = true;
   c->green_eta = 0.0;
+  c->have_residual = true;
   QCL_CUDA_CHECK(cudaStreamSynchronize(c->st));
   int hst[2];
   QCL_CUDA_CHECK(cudaMemcpy(hst, c->status, sizeof(hst), cudaMemcpyDeviceToHost));
@@ -781,6 +784,30 @@ int scba_green_state(ScbaCtx* c, void* A_host, double* kappa, double* scale) {
   if (scale) QCL_CUDA_CHECK(cudaMemcpyAsync(scale, t.p[2], nb, cudaMemcpyDeviceToHost, c->st));
   QCL_CUDA_CHECK(cudaStreamSynchronize(c->st));
   return QCL_OK;
+}
+
+// Positivity witness of the last step's residual suite (SCBAIteration.witness,
+// production_solver.jl:611-619): reduced on request from the per-block
+// outputs the step left in the residual scratch.
+int scba_witness(ScbaCtx* c, double* out12) {
+  if (!c->have_residual) {
+    set_last_error("witness: no residual evaluation yet (call step first)");
+    return QCL_ARG;
+  }
+  const int sp = c->precision == QCL_MIXED ? QCL_C64 : c->precision;
+  double* dev = nullptr;
+  int s = dalloc((void**)&dev, (residual_witness_partial_doubles() + 12) * sizeof(double));
+  if (s) return s;
+  s = launch_residual_witness(sp, c->NE, c->Nk, c->N, c->GR, c->GL, c->GG, c->tot[1], c->tot[2], c->reswork, dev,
+                              dev + residual_witness_partial_doubles(), c->st);
+  if (!s) {
+    cudaError_t e = cudaMemcpyAsync(out12, dev + residual_witness_partial_doubles(), 12 * sizeof(double),
+                                    cudaMemcpyDeviceToHost, c->st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->st);
+    if (e != cudaSuccess) s = cuda_status(e, "witness download");
+  }
+  cudaFree(dev);
+  return s;
 }
 
 int scba_set_graph(ScbaCtx* c, int enable) {

@@ -126,6 +126,7 @@ def _declare(l):
         "qcl_static_contraction": (I, [I, P, I, I, I, P, D, D, P, P]),
         "qcl_embedding_component": (I, [I, I, I, I, P, D, P, P, P]),
         "qcl_residual_suite": (I, [I, I, I, I, P, P, P, P, P, P, P, P, P, P]),
+        "qcl_residual_suite_witness": (I, [I, I, I, I, P, P, P, P, P, P, P, P, P, P, P]),
         "qcl_selfenergy_residual": (I, [I, Z, P, P, P]),
         "qcl_hermitian_eigvals": (I, [I, Z, P, P]),
         "qcl_condition_number": (I, [I, I, I, I, P, D, P, P, P, P, P]),
@@ -142,6 +143,7 @@ def _declare(l):
         "qcl_scba_upload": (I, [P, I, P]),
         "qcl_scba_use_graph": (I, [P, I]),
         "qcl_scba_green_state": (I, [P, P, P, P]),
+        "qcl_scba_witness": (I, [P, P]),
     }
     for name, (res, args) in sig.items():
         if hasattr(l, name):

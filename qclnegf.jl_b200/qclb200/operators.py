@@ -227,9 +227,26 @@ def embedding_component(T, G, eps, delta, *, precision="c128"):
     return S
 
 
-def production_residual_suite(eps, h, GR, GL, GG, total, candidate_lesser, *, precision="c128"):
+WITNESS_KINDS = ("spectral", "occupied", "unoccupied", "broadening", "raw_occupied", "raw_unoccupied")
+
+
+class PsdWitness(ctypes.Structure):
+    """qcl_psd_witness: _PositivityWitness (positivity_diagnostics.jl:41-54)."""
+    _fields_ = [("matrix_kind", ctypes.c_int), ("energy_index", ctypes.c_int), ("momentum_index", ctypes.c_int)] + [
+        (n, ctypes.c_double) for n in ("minimum_eigenvalue", "block_norm", "floor", "ratio", "absolute_defect",
+                                       "relative_defect", "backward_error", "hermiticity_defect",
+                                       "construction_scale")]
+
+    def as_dict(self):
+        d = {n: getattr(self, n) for n, _ in self._fields_}
+        d["matrix_kind"] = "none" if self.matrix_kind < 0 else WITNESS_KINDS[self.matrix_kind]
+        return d
+
+
+def production_residual_suite(eps, h, GR, GL, GG, total, candidate_lesser, *, precision="c128",
+                              return_witness=False):
     """production_residual_suite (residuals.jl:537-770): dict r_D, r_A, r_K,
-    r_PSD, r_caus."""
+    r_PSD, r_caus (and the positivity witness as ``witness``)."""
     p = _prec(precision)
     cdt = _CDT[p]
     GR = _field(GR, cdt)
@@ -237,9 +254,16 @@ def production_residual_suite(eps, h, GR, GL, GG, total, candidate_lesser, *, pr
     NE, Nk, Nb, _ = shape
     arrs = [GR] + [_field(x, cdt, shape) for x in (GL, GG, total[0], total[1], total[2], candidate_lesser)]
     out = np.zeros(5)
-    check(lib().qcl_residual_suite(p, NE, Nk, Nb, _ptr(_real(eps)), _ptr(_field(h, np.complex128)),
-                                   *[_ptr(a) for a in arrs], _ptr(out)))
-    return dict(rD=out[0], rA=out[1], rK=out[2], rPSD=out[3], rcaus=out[4])
+    args = (p, NE, Nk, Nb, _ptr(_real(eps)), _ptr(_field(h, np.complex128)), *[_ptr(a) for a in arrs], _ptr(out))
+    w = PsdWitness()
+    if return_witness:
+        check(lib().qcl_residual_suite_witness(*args, ctypes.byref(w)))
+    else:
+        check(lib().qcl_residual_suite(*args))
+    res = dict(rD=out[0], rA=out[1], rK=out[2], rPSD=out[3], rcaus=out[4])
+    if return_witness:
+        res["witness"] = w.as_dict()
+    return res
 
 
 def production_selfenergy_residual(old, new, *, precision="c128"):

@@ -154,6 +154,14 @@ class ProductionSCBA:
                                          ctypes.c_void_p(scale.ctypes.data)))
         return dict(A=A, condition_number=kappa, dyson_scale=scale)
 
+    def witness(self):
+        """The positivity witness of the last step's residual suite."""
+        from .operators import PsdWitness
+
+        w = PsdWitness()
+        check(lib().qcl_scba_witness(self._h, ctypes.byref(w)))
+        return w.as_dict()
+
     def family(self, f):
         """(SigmaR, Sigma<, Sigma>) of family f: 0..M-1 mechanisms, M plus, M+1 minus."""
         return tuple(self.download(3 + 3 * f + c) for c in range(3))

@@ -279,6 +279,10 @@ typedef struct qcl_scba_problem {
   int transverse_momentum;
   int retarded_real_part;
   int elastic_retarded;
+  /* occupation_normalization 0 :paired_convex (_normalize_keldysh_pair!),
+   * 1 :scalar_lesser -- G< / lambda and G> = G^R - G^A + G<
+   * (production_state.jl:54-61). */
+  int occupation_normalization;
 } qcl_scba_problem;
 
 /* One SCBAIteration row (domain/types.jl:908).  status: QCL_OK or
@@ -288,6 +292,10 @@ typedef struct qcl_scba_row {
   int status;
   double r_D, r_A, r_K, r_Sigma, r_lambda, lambda, r_PSD, r_caus, r_roundoff;
   double r_J, r_pop, J, Jbar, number, holes, occupied_fraction, empty_fraction;
+  /* SCBAIteration's target_charge, normalized_charge (the number functional
+   * of the normalised G<) and lambda_change (NaN on the first row),
+   * production_solver.jl:607-610; raw_charge is `number`. */
+  double target_charge, normalized_charge, lambda_change;
 } qcl_scba_row;
 
 typedef struct qcl_scba qcl_scba;

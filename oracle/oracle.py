@@ -541,10 +541,18 @@ def current_green(problem, total):
     lam = number / problem.target
     if not (math.isfinite(lam) and lam > 0):
         raise OracleError(2, "kinetic eigenvalue must be positive")
+    if getattr(problem, "occupation_normalization", "paired_convex") == "scalar_lesser":
+        # production_state.jl:54-61: G< / lambda, G> = G^R - G^A + G<
+        GL = np.asfortranarray(GL / lam)
+        GG = np.asfortranarray((GR - np.conj(np.transpose(GR, (0, 1, 3, 2)))) + GL)
+        holes = -number_functional(GG, problem.wE, problem.wk, problem.gs)
+        return dict(GR=GR, GL=GL, GG=GG, scale=scale, number=number, holes=holes, a=1.0, c=0.0,
+                    normalized=number_functional(GL, problem.wE, problem.wk, problem.gs)), lam
     holes = -number_functional(GG, problem.wE, problem.wk, problem.gs)
     a, c, lam = paired_coefficients(number, holes, problem.target)
     normalize_pair(GL, GG, a, c)
-    return dict(GR=GR, GL=GL, GG=GG, scale=scale, number=number, holes=holes, a=a, c=c), lam
+    return dict(GR=GR, GL=GL, GG=GG, scale=scale, number=number, holes=holes, a=a, c=c,
+                normalized=number_functional(GL, problem.wE, problem.wk, problem.gs)), lam
 
 
 def make_plans(problem):
@@ -591,7 +599,9 @@ def scba(problem, iterations, verify=True, state=None, keep_state=False):
         rJ = math.inf if Jprev is None else abs(J - Jprev) / max(abs(J), abs(Jprev), 1e-12)
         rp = math.inf if pprev is None else float(np.linalg.norm(pops - pprev) / (np.linalg.norm(pops) + 1e-14))
         row = dict(nu=nu, lam=lam, rlam=abs(lam - 1), rSigma=rS, rround=rround, J=J, Jbar=Jbar,
-                   populations=pops, rJ=rJ, rpop=rp, number=green["number"], holes=green["holes"], **res)
+                   populations=pops, rJ=rJ, rpop=rp, number=green["number"], holes=green["holes"],
+                   target=problem.target, normalized=green["normalized"],
+                   lambda_change=math.nan if not history else lam - history[-1]["lam"], **res)
         history.append(row)
         a = problem.alpha
         for m in problem.mechanisms:

@@ -15,7 +15,9 @@ int launch_dyson_keldysh(int precision, int NE, int Nk, int N, const double* eps
 int launch_weighted_trace(int NE, int Nk, const void* tr, const double* wE, const double* wk, double* partial,
                           double* out, cudaStream_t st);
 int launch_paired_coefficients(const double* trL, const double* trG, int gs, double target, double* coeffs,
-                               int* status, cudaStream_t st, double realness_limit = 1e-10);
+                               int* status, cudaStream_t st, double realness_limit = 1e-10, int scalar = 0);
+int launch_scalar_lesser(int precision, int NE, int Nk, int N, const void* GR, void* GL, void* GG,
+                         const double* coeffs, cudaStream_t st);
 int launch_normalize_pair(int precision, size_t n, void* GL, void* GG, const double* coeffs, cudaStream_t st);
 // condition number / Dyson scale and the spectral function (residual.cu)
 int launch_condition(int precision, int NE, int Nk, int N, const double* eps, double eta, const void* h,

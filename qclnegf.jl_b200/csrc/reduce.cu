@@ -95,10 +95,12 @@ int launch_weighted_trace(int NE, int Nk, const void* tr, const double* wE, cons
 //   N = Re[-i gs/(2pi) trL] = gs/(2pi) Im trL,  H = -Re[-i gs/(2pi) trG]
 // coeffs = (a, c, lambda, N, H); status gets QCL_DOMAIN / QCL_ARG.
 // The realness check of number_functional (greens.jl:100-110) is applied to
-// both functionals.
+// both functionals.  scalar != 0 is the occupation_normalization =
+// :scalar_lesser comparator (production_state.jl:54-61): only N and lambda
+// are checked (the reference never forms H there), a = 1, c = 0.
 // ---------------------------------------------------------------------------
 __global__ void paired_coefficients_kernel(const double* trL, const double* trG, int gs, double target,
-                                           double limit, double* coeffs, int* status) {
+                                           double limit, double* coeffs, int* status, int scalar) {
   if (threadIdx.x != 0 || blockIdx.x != 0) return;
   const double pre = gs / (2.0 * M_PI);
   // -i * pre * (x + i y) = pre * (y - i x)
@@ -108,9 +110,18 @@ __global__ void paired_coefficients_kernel(const double* trL, const double* trG,
   coeffs[3] = number;
   coeffs[4] = holes;
   int code = 0;
-  if (!(fabs(Nim) <= limit * fmax(fabs(Nre), 1.0)) || !(fabs(Gim) <= limit * fmax(fabs(Gre), 1.0)))
+  if (!(fabs(Nim) <= limit * fmax(fabs(Nre), 1.0)) ||
+      (!scalar && !(fabs(Gim) <= limit * fmax(fabs(Gre), 1.0))))
     code = QCL_DOMAIN;
   double a = 1, c = 0, lam = number / target;
+  if (scalar) {
+    if (!code && !(isfinite(lam) && lam > 0)) code = QCL_DOMAIN;
+    if (code && status) record_status(status, code, -1);
+    coeffs[0] = 1.0;
+    coeffs[1] = 0.0;
+    coeffs[2] = lam;
+    return;
+  }
   if (!code) {
     if (!(isfinite(target) && target > 0)) code = QCL_ARG;
     else if (!(isfinite(lam) && lam > 0)) code = QCL_DOMAIN;
@@ -140,8 +151,8 @@ __global__ void paired_coefficients_kernel(const double* trL, const double* trG,
 // numerical_invariants.jl:5) for complex128 fields; complex64 fields carry
 // ~1e-7 relative rounding in every diagonal element, so their limit is 1e-5.
 int launch_paired_coefficients(const double* trL, const double* trG, int gs, double target, double* coeffs,
-                               int* status, cudaStream_t st, double realness_limit) {
-  paired_coefficients_kernel<<<1, 32, 0, st>>>(trL, trG, gs, target, realness_limit, coeffs, status);
+                               int* status, cudaStream_t st, double realness_limit, int scalar) {
+  paired_coefficients_kernel<<<1, 32, 0, st>>>(trL, trG, gs, target, realness_limit, coeffs, status, scalar);
   QCL_LAUNCH_CHECK("paired_coefficients");
   return QCL_OK;
 }
@@ -158,6 +169,24 @@ __global__ void normalize_pair_kernel(size_t n, Cx<R>* __restrict__ GL, Cx<R>* _
   }
 }
 
+// occupation_normalization = :scalar_lesser (production_state.jl:54-61 with
+// the greater component of _green_state_production, production_operators.jl:
+// 1405-1409): G< <- G< / lambda, G> <- (G^R - G^R^H) + G<.
+template <typename R>
+__global__ void scalar_lesser_kernel(int NE, int Nk, int N, const Cx<R>* __restrict__ GR, Cx<R>* __restrict__ GL,
+                                     Cx<R>* __restrict__ GG, const double* __restrict__ coeffs) {
+  const double lam = coeffs[2];
+  const long long blocks = (long long)NE * Nk, n = blocks * N * N;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const long long em = i % blocks, ab = i / blocks;
+    const int a = (int)(ab % N), b = (int)(ab / N);
+    const Cx<R> l = GL[i], g = GR[i], gt = GR[em + blocks * ((long long)b + (long long)N * a)];
+    const double lx = (double)l.x / lam, ly = (double)l.y / lam;
+    GL[i] = cx<R>((R)lx, (R)ly);
+    GG[i] = cx<R>((R)(((double)g.x - (double)gt.x) + lx), (R)(((double)g.y + (double)gt.y) + ly));
+  }
+}
+
 static unsigned grid_for(size_t n, int threads) {
   size_t g = (n + threads - 1) / threads;
   const size_t cap = 148 * 16;
@@ -170,6 +199,19 @@ int launch_normalize_pair(int precision, size_t n, void* GL, void* GG, const dou
   else
     normalize_pair_kernel<float><<<grid_for(n, 256), 256, 0, st>>>(n, (Cx<float>*)GL, (Cx<float>*)GG, coeffs);
   QCL_LAUNCH_CHECK("normalize_pair");
+  return QCL_OK;
+}
+
+int launch_scalar_lesser(int precision, int NE, int Nk, int N, const void* GR, void* GL, void* GG,
+                         const double* coeffs, cudaStream_t st) {
+  const size_t n = (size_t)NE * Nk * N * N;
+  if (precision == QCL_C128)
+    scalar_lesser_kernel<double><<<grid_for(n, 256), 256, 0, st>>>(NE, Nk, N, (const Cx<double>*)GR, (Cx<double>*)GL,
+                                                                    (Cx<double>*)GG, coeffs);
+  else
+    scalar_lesser_kernel<float><<<grid_for(n, 256), 256, 0, st>>>(NE, Nk, N, (const Cx<float>*)GR, (Cx<float>*)GL,
+                                                                   (Cx<float>*)GG, coeffs);
+  QCL_LAUNCH_CHECK("scalar_lesser");
   return QCL_OK;
 }
 

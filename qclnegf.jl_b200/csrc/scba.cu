@@ -77,6 +77,7 @@ enum {
 struct ScbaCtx {
   int NE, Nk, N, M, precision, gs, verify;
   int diagonal = 0, averaged = 0, drop_real = 0, direct_green = 0;  // scattering-model switches
+  int scalar_lesser = 0;                                             // occupation_normalization
   double wk_sum = 0;
   double Ep, hw_LO, N_LO, target, eta_seed, kBT, alpha, J0;
   size_t nfield, fbytes;
@@ -111,6 +112,7 @@ struct ScbaCtx {
   bool pending_commit = false;
   int nu = 0;
   double Jprev = NAN;
+  double lam_prev = NAN;
   std::vector<double> pprev, pops;
   bool seeded = false;
   bool have_green = false;  // GR holds the Dyson solution of (eps + i green_eta, h, tot[0])
@@ -253,6 +255,7 @@ int scba_create(const qcl_scba_problem* p, const qcl_mechanism* mechs, ScbaCtx**
   c->averaged = p->transverse_momentum;
   c->drop_real = p->retarded_real_part;
   c->direct_green = p->elastic_retarded;
+  c->scalar_lesser = p->occupation_normalization;
   c->nfield = field_elems(c->NE, c->Nk, c->N);
   c->fbytes = c->nfield * (c->precision == QCL_C128 ? 16 : 8);
   c->eps_h.assign(p->eps, p->eps + p->NE);
@@ -268,10 +271,10 @@ int scba_create(const qcl_scba_problem* p, const qcl_mechanism* mechs, ScbaCtx**
   double de;
   TRY(check_uniform_grid(c->NE, p->eps, &de));
   // _check_algorithm_options (algorithm_options.jl:42-93) for the model switches
-  for (int sw : {c->diagonal, c->averaged, c->drop_real, c->direct_green})
+  for (int sw : {c->diagonal, c->averaged, c->drop_real, c->direct_green, c->scalar_lesser})
     if (sw != 0 && sw != 1)
       TRY((set_last_error("model switches (self_energy_structure, transverse_momentum, retarded_real_part, "
-                          "elastic_retarded) must be 0 or 1"),
+                          "elastic_retarded, occupation_normalization) must be 0 or 1"),
            QCL_ARG));
   for (int m = 0; m < c->Nk; ++m) c->wk_sum += p->wk[m];
   if (c->averaged && !(c->wk_sum > 0)) TRY((set_last_error("radial weights must have positive sum"), QCL_ARG));
@@ -456,9 +459,10 @@ static int current_green(ScbaCtx* c, const std::vector<void*>& fam) {
   if ((s = launch_weighted_trace(c->NE, c->Nk, c->trL, c->wE, c->wk, c->rpartial, c->scal + SC_TRL, c->st))) return s;
   if ((s = launch_weighted_trace(c->NE, c->Nk, c->trG, c->wE, c->wk, c->rpartial, c->scal + SC_TRG, c->st))) return s;
   if ((s = launch_paired_coefficients(c->scal + SC_TRL, c->scal + SC_TRG, c->gs, c->target, c->scal + SC_COEF,
-                                      c->status, c->st, c->precision == QCL_C128 ? 1e-10 : 1e-5)))
+                                      c->status, c->st, c->precision == QCL_C128 ? 1e-10 : 1e-5, c->scalar_lesser)))
     return s;
   const int sp = c->precision == QCL_MIXED ? QCL_C64 : c->precision;
+  if (c->scalar_lesser) return launch_scalar_lesser(sp, c->NE, c->Nk, c->N, c->GR, c->GL, c->GG, c->scal + SC_COEF, c->st);
   return launch_normalize_pair(sp, c->nfield, c->GL, c->GG, c->scal + SC_COEF, c->st);
 }
 
@@ -591,6 +595,7 @@ int scba_seed(ScbaCtx* c, double* mu_out) {
   c->nu = 0;
   c->pending_commit = false;
   c->Jprev = NAN;
+  c->lam_prev = NAN;
   c->pprev.clear();
   return QCL_OK;
 }
@@ -646,6 +651,13 @@ int scba_step(ScbaCtx* c, qcl_scba_row* row) {
   row->holes = h[SC_COEF + 4];
   row->occupied_fraction = h[SC_COEF + 0];
   row->empty_fraction = h[SC_COEF + 1];
+  row->target_charge = c->target;
+  // number functional of the normalised G< (production_solver.jl:609): a N + c H
+  // for the paired transfer (N(G>) = -H), N / lambda for the scalar comparator
+  row->normalized_charge = c->scalar_lesser ? row->number / row->lambda
+                                            : row->occupied_fraction * row->number +
+                                                  row->empty_fraction * row->holes;
+  row->lambda_change = isnan(c->lam_prev) ? NAN : row->lambda - c->lam_prev;
   row->r_D = h[SC_RES + 0];
   row->r_A = h[SC_RES + 1];
   row->r_K = h[SC_RES + 2];
@@ -682,6 +694,7 @@ int scba_step(ScbaCtx* c, qcl_scba_row* row) {
   }
   row->status = hst[0];
   c->Jprev = row->J;
+  c->lam_prev = row->lambda;
   c->pprev = c->pops;
   c->pending_commit = true;
   if (hst[0] == QCL_SINGULAR) {

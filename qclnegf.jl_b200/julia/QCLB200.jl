@@ -154,6 +154,7 @@ struct Problem
     # self_energy_structure (:full/:diagonal), transverse_momentum (:resolved/:averaged),
     # retarded_real_part (:kramers_kronig/:drop), elastic_retarded (:hilbert/:direct_green)
     self_energy_structure::Cint; transverse_momentum::Cint; retarded_real_part::Cint; elastic_retarded::Cint
+    occupation_normalization::Cint  # :paired_convex / :scalar_lesser
 end
 
 struct Row
@@ -162,6 +163,7 @@ struct Row
     r_PSD::Float64; r_caus::Float64; r_roundoff::Float64; r_J::Float64; r_pop::Float64
     J::Float64; Jbar::Float64; number::Float64; holes::Float64
     occupied_fraction::Float64; empty_fraction::Float64
+    target_charge::Float64; normalized_charge::Float64; lambda_change::Float64
 end
 
 mutable struct Solver

@@ -196,6 +196,7 @@ class SCBAProblem:
     transverse_momentum: str = "resolved"         # or "averaged"
     retarded_real_part: str = "kramers_kronig"    # or "drop"
     elastic_retarded: str = "hilbert"             # or "direct_green"
+    occupation_normalization: str = "paired_convex"  # or "scalar_lesser"
 
     @property
     def shape(self):

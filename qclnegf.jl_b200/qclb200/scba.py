@@ -28,7 +28,8 @@ class _Problem(ctypes.Structure):
                 ("kBT", ctypes.c_double), ("alpha", ctypes.c_double), ("J0", ctypes.c_double),
                 ("precision", ctypes.c_int), ("verify_roundoff", ctypes.c_int), ("nmech", ctypes.c_int),
                 ("self_energy_structure", ctypes.c_int), ("transverse_momentum", ctypes.c_int),
-                ("retarded_real_part", ctypes.c_int), ("elastic_retarded", ctypes.c_int)]
+                ("retarded_real_part", ctypes.c_int), ("elastic_retarded", ctypes.c_int),
+                ("occupation_normalization", ctypes.c_int)]
 
 
 # AlgorithmOptions model switches -> the C ABI's 0/1 codes (_check_algorithm_options,
@@ -38,6 +39,7 @@ _SWITCHES = {
     "transverse_momentum": ("resolved", "averaged"),
     "retarded_real_part": ("kramers_kronig", "drop"),
     "elastic_retarded": ("hilbert", "direct_green"),
+    "occupation_normalization": ("paired_convex", "scalar_lesser"),
 }
 
 
@@ -55,7 +57,8 @@ class Row(ctypes.Structure):
     _fields_ = [("nu", ctypes.c_int), ("status", ctypes.c_int)] + [
         (n, ctypes.c_double) for n in ("r_D", "r_A", "r_K", "r_Sigma", "r_lambda", "lambda_", "r_PSD", "r_caus",
                                        "r_roundoff", "r_J", "r_pop", "J", "Jbar", "number", "holes",
-                                       "occupied_fraction", "empty_fraction")]
+                                       "occupied_fraction", "empty_fraction", "target_charge",
+                                       "normalized_charge", "lambda_change")]
 
     def as_dict(self):
         d = {n: getattr(self, n) for n, _ in self._fields_}

@@ -10,6 +10,7 @@ defining properties.  GPU: the device SCBA loop with each switch against the
 oracle's SCBA, every history metric within 1e-9.
 """
 import dataclasses
+import math
 
 import numpy as np
 import pytest
@@ -128,11 +129,28 @@ def test_switch_properties_on_oracle_candidates(orc):
             assert approx_err(SR, orc.contraction(m, green["GR"], base.wk)) == 0.0
 
 
+def test_scalar_lesser_normalisation_on_oracle(orc):
+    """occupation_normalization = :scalar_lesser (production_state.jl:54-61):
+    N(G<) equals the target and G> = G^R - G^A + G<."""
+    pr = _small(occupation_normalization="scalar_lesser")
+    plans = orc.make_plans(pr)
+    green, _ = orc.seed_green(pr)
+    scattering, _ = orc.scattering_candidate(pr, green, plans, verify=False)
+    plus, minus = orc.embedding_candidate(pr, green, plans)
+    g, lam = orc.current_green(pr, orc.total_family(pr, scattering, plus, minus))
+    assert g["normalized"] == pytest.approx(pr.target, rel=1e-12)
+    GR = g["GR"]
+    assert approx_err(g["GG"], GR - np.conj(np.transpose(GR, (0, 1, 3, 2))) + g["GL"]) < 1e-15
+    paired = _small()
+    gp, lp = orc.current_green(paired, orc.total_family(paired, scattering, plus, minus))
+    assert lp == lam and gp["normalized"] == pytest.approx(pr.target, rel=1e-12)
+
+
 def test_switch_codes_validate_symbols():
     from qclb200.scba import _switch_codes
 
-    assert _switch_codes(_small()) == [0, 0, 0, 0]
-    assert _switch_codes(_small(self_energy_structure="diagonal", elastic_retarded="direct_green")) == [1, 0, 0, 1]
+    assert _switch_codes(_small()) == [0, 0, 0, 0, 0]
+    assert _switch_codes(_small(self_energy_structure="diagonal", elastic_retarded="direct_green")) == [1, 0, 0, 1, 0]
     with pytest.raises(ValueError, match="transverse_momentum"):
         _switch_codes(_small(transverse_momentum="mean"))
 
@@ -147,6 +165,7 @@ SWITCH_CASES = [
     dict(retarded_real_part="drop"),
     dict(elastic_retarded="direct_green"),
     dict(self_energy_structure="diagonal", transverse_momentum="averaged", elastic_retarded="direct_green"),
+    dict(occupation_normalization="scalar_lesser"),
 ]
 
 
@@ -166,6 +185,13 @@ def test_scba_with_model_switches_matches_oracle(gpu_ops, orc, switches):
         np.testing.assert_allclose(rg["populations"], ro["populations"], rtol=1e-9, atol=1e-13)
         if switches.get("retarded_real_part") == "drop":
             assert rg["r_roundoff"] == 0.0
+        assert rg["target_charge"] == pr.target
+        assert rg["normalized_charge"] == pytest.approx(ro["normalized"], rel=1e-9)
+        assert rg["normalized_charge"] == pytest.approx(pr.target, rel=1e-9)
+        if ro["nu"] == 1:
+            assert math.isnan(rg["lambda_change"])
+        else:
+            assert rg["lambda_change"] == pytest.approx(ro["lambda_change"], rel=1e-6, abs=1e-12)
 
 
 @pytest.mark.gpu

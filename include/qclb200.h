@@ -323,6 +323,16 @@ int qcl_scba_populations(qcl_scba* ctx, double* out);
  * component c (0 R, 1 <, 2 >) of the current state. */
 int qcl_scba_download(qcl_scba* ctx, int which, void* host);
 int qcl_scba_upload(qcl_scba* ctx, int which, const void* host);
+/* A new operating point of a bias or temperature sweep on the same context
+ * (retarget_problem + retarget_production_cache, composition/
+ * operating_point.jl:25-170): the +-Ep shift plans are rebuilt for the new
+ * period drop Ep, and the Hartree Hamiltonian h ((Nk, Nb, Nb) complex128),
+ * the LO occupation N_LO, kBT and the kernel scales q (nmech doubles, e.g.
+ * the acoustic q^K proportional to the lattice temperature) are replaced
+ * where given (h, q may be NULL).  Kernel operators, grids and the state stay
+ * resident: the next step continues from the last unmixed state (warm
+ * start); the row history (r_J, r_pop, lambda_change, nu) restarts. */
+int qcl_scba_retarget(qcl_scba* ctx, double Ep, double N_LO, double kBT, const void* h, const double* q);
 /* Replay each iteration as one captured CUDA graph (default off). */
 int qcl_scba_use_graph(qcl_scba* ctx, int enable);
 /* The derived GreenState fields of the last Dyson solve (seed or step) --

@@ -138,6 +138,7 @@ int scba_upload(ScbaCtx* c, int which, const void* host);
 int scba_set_graph(ScbaCtx* c, int enable);
 int scba_green_state(ScbaCtx* c, void* A, double* kappa, double* scale);
 int scba_witness(ScbaCtx* c, double* out12);
+int scba_retarget(ScbaCtx* c, double Ep, double N_LO, double kBT, const void* h, const double* q);
 
 static int shift_plan_dev(int NE, const double* eps, double delta, DevBuf& l, DevBuf& r, DevBuf& th, DevBuf& v,
                           ShiftPlanDev* out) {
@@ -686,6 +687,14 @@ int qcl_scba_green_state(qcl_scba* ctx, void* A, double* kappa, double* scale) {
     return QCL_ARG;
   }
   return scba_green_state((ScbaCtx*)ctx, A, kappa, scale);
+}
+
+int qcl_scba_retarget(qcl_scba* ctx, double Ep, double N_LO, double kBT, const void* h, const double* q) {
+  if (!ctx) {
+    set_last_error("ctx is required");
+    return QCL_ARG;
+  }
+  return scba_retarget((ScbaCtx*)ctx, Ep, N_LO, kBT, h, q);
 }
 
 int qcl_scba_witness(qcl_scba* ctx, qcl_psd_witness* witness) {

@@ -164,6 +164,21 @@ static int build_plan(ScbaCtx* c, DevShift& d, double delta) {
   return dupload(&d.valid, v.data(), c->NE, c->st);
 }
 
+// Rebuilds a shift plan into its existing device arrays.
+static int refill_plan(ScbaCtx* c, DevShift& d, double delta) {
+  std::vector<int> l(c->NE), r(c->NE);
+  std::vector<double> th(c->NE);
+  std::vector<unsigned char> v(c->NE);
+  int s = build_shift_plan_host(c->NE, c->eps_h.data(), delta, l.data(), r.data(), th.data(), v.data());
+  if (s) return s;
+  QCL_CUDA_CHECK(cudaMemcpyAsync(d.left, l.data(), c->NE * sizeof(int), cudaMemcpyHostToDevice, c->st));
+  QCL_CUDA_CHECK(cudaMemcpyAsync(d.right, r.data(), c->NE * sizeof(int), cudaMemcpyHostToDevice, c->st));
+  QCL_CUDA_CHECK(cudaMemcpyAsync(d.theta, th.data(), c->NE * sizeof(double), cudaMemcpyHostToDevice, c->st));
+  QCL_CUDA_CHECK(cudaMemcpyAsync(d.valid, v.data(), c->NE, cudaMemcpyHostToDevice, c->st));
+  QCL_CUDA_CHECK(cudaStreamSynchronize(c->st));  // the host vectors are temporaries
+  return QCL_OK;
+}
+
 void scba_destroy(ScbaCtx* c) {
   if (!c) return;
   if (c->st) cudaStreamSynchronize(c->st);
@@ -821,6 +836,53 @@ int scba_witness(ScbaCtx* c, double* out12) {
   }
   cudaFree(dev);
   return s;
+}
+
+// A new operating point on the same cache (retarget_problem +
+// retarget_production_cache, composition/operating_point.jl:25-170): the
+// +-Ep shift plans are rebuilt for the new field, h (the new Hartree
+// Hamiltonian), N_LO, kBT and the kernel scales q^K are replaced where given;
+// the kernel operators, grids, LO plans and the state stay resident, so the
+// next step continues from the last (unmixed) state as a warm start.  The
+// per-run history (r_J, r_pop, lambda_change, iteration count) restarts, and
+// captured iteration graphs are rebuilt (they hold the old scalars).
+int scba_retarget(ScbaCtx* c, double Ep, double N_LO, double kBT, const void* h, const double* q) {
+  if (!isfinite(Ep) || !isfinite(N_LO) || N_LO < 0 || !(kBT > 0) || !isfinite(kBT)) {
+    set_last_error("retarget: Ep, N_LO >= 0 and kBT > 0 must be finite");
+    return QCL_ARG;
+  }
+  if (q)
+    for (int i = 0; i < c->M; ++i)
+      if (!isfinite(q[i])) {
+        set_last_error("retarget: kernel scale q[%d] is not finite", i);
+        return QCL_ARG;
+      }
+  QCL_CUDA_CHECK(cudaStreamSynchronize(c->st));
+  int s;
+  if ((s = refill_plan(c, c->shift[0], +Ep))) return s;
+  if ((s = refill_plan(c, c->shift[1], -Ep))) return s;
+  if (h) {
+    QCL_CUDA_CHECK(cudaMemcpyAsync(c->h, h, (size_t)c->Nk * c->N * c->N * 16, cudaMemcpyHostToDevice, c->st));
+    QCL_CUDA_CHECK(cudaStreamSynchronize(c->st));
+  }
+  c->Ep = Ep;
+  c->N_LO = N_LO;
+  c->kBT = kBT;
+  if (q)
+    for (int i = 0; i < c->M; ++i) c->mech[i].q = q[i];
+  for (int g = 0; g < 2; ++g)
+    if (c->graph[g]) {
+      cudaGraphExecDestroy(c->graph[g]);
+      c->graph[g] = nullptr;
+    }
+  c->pending_commit = false;  // keep the unmixed state of the last step
+  c->nu = 0;
+  c->Jprev = NAN;
+  c->lam_prev = NAN;
+  c->pprev.clear();
+  c->have_green = false;
+  c->have_residual = false;
+  return QCL_OK;
 }
 
 int scba_set_graph(ScbaCtx* c, int enable) {

@@ -144,6 +144,7 @@ def _declare(l):
         "qcl_scba_use_graph": (I, [P, I]),
         "qcl_scba_green_state": (I, [P, P, P, P]),
         "qcl_scba_witness": (I, [P, P]),
+        "qcl_scba_retarget": (I, [P, D, D, D, P, P]),
     }
     for name, (res, args) in sig.items():
         if hasattr(l, name):

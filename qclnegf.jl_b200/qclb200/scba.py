@@ -157,6 +157,32 @@ class ProductionSCBA:
                                          ctypes.c_void_p(scale.ctypes.data)))
         return dict(A=A, condition_number=kappa, dyson_scale=scale)
 
+    def retarget(self, *, Ep=None, N_LO=None, kBT=None, h=None, q=None):
+        """A new operating point on the resident cache and state
+        (retarget_problem + retarget_production_cache,
+        composition/operating_point.jl:25-170).  Unspecified values are kept;
+        self.problem is replaced by the retargeted copy."""
+        import dataclasses
+
+        pr = self.problem
+        mechs = list(pr.mechanisms)
+        if q is not None:
+            q = [float(v) for v in q]
+            if len(q) != len(mechs):
+                raise ValueError("one kernel scale per mechanism is required")
+            mechs = [dataclasses.replace(m, q=v) for m, v in zip(mechs, q)]
+        new = dataclasses.replace(pr, Ep=pr.Ep if Ep is None else float(Ep),
+                                  N_LO=pr.N_LO if N_LO is None else float(N_LO),
+                                  kBT=pr.kBT if kBT is None else float(kBT),
+                                  h=pr.h if h is None else _c(h), mechanisms=mechs)
+        harr = None if h is None else _c(h)
+        qarr = None if q is None else np.ascontiguousarray(q, dtype=np.float64)
+        check(lib().qcl_scba_retarget(self._h, float(new.Ep), float(new.N_LO), float(new.kBT),
+                                      None if harr is None else ctypes.c_void_p(harr.ctypes.data),
+                                      None if qarr is None else ctypes.c_void_p(qarr.ctypes.data)))
+        self.problem = new
+        return new
+
     def witness(self):
         """The positivity witness of the last step's residual suite."""
         from .operators import PsdWitness

@@ -119,3 +119,32 @@ def test_scba_terminal_state_is_unmixed_and_resumable(gpu_ops):
     assert r4["J"] == pytest.approx(rows_full[3]["J"], rel=1e-12)
     for s in (full, part, resumed):
         s.close()
+
+
+def test_scba_retarget_warm_start_matches_oracle(gpu_ops, orc):
+    """A bias/temperature sweep point on a resident context (retarget_problem +
+    retarget_production_cache, composition/operating_point.jl:25-170): the
+    new +-Ep plans, h, N_LO and q^K act on the last unmixed state; the oracle
+    restarted from that state with the retargeted problem gives the same rows."""
+    import dataclasses
+
+    from qclb200.problem import small_problem
+    from qclb200.scba import ProductionSCBA
+
+    pr = small_problem(NE=41, Nk=3, Nb=4, mechanisms=("LO", "acoustic", "impurity", "IFR", "alloy"))
+    s = ProductionSCBA(pr, use_graph=True)
+    s.seed()
+    s.run(3)
+    rng = np.random.default_rng(12)
+    dh = 0.01 * (rng.standard_normal((pr.Nb, pr.Nb)) + 1j * rng.standard_normal((pr.Nb, pr.Nb)))
+    h2 = np.asfortranarray(pr.h + (dh + dh.conj().T)[None, :, :])
+    q2 = [m.q * (1.25 if m.name == "acoustic" else 1.0) for m in pr.mechanisms]
+    pr2 = s.retarget(Ep=0.37, N_LO=0.3, kBT=0.25, h=h2, q=q2)
+    M = len(pr.mechanisms)
+    state = dict(scattering={m.name: s.family(i) for i, m in enumerate(pr.mechanisms)}, plus=s.family(M),
+                 minus=s.family(M + 1))
+    hist_g = s.run(3)
+    s.close()
+    hist_o, _ = orc.scba(pr2, 3, state=state)
+    assert math.isinf(hist_g[0]["r_J"])
+    _compare(hist_o, hist_g)

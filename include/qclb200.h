@@ -283,7 +283,31 @@ typedef struct qcl_scba_problem {
    * 1 :scalar_lesser -- G< / lambda and G> = G^R - G^A + G<
    * (production_state.jl:54-61). */
   int occupation_normalization;
+  /* mixing 0 :linear (alpha), 1 :anderson -- bounded-history Anderson
+   * acceleration with the exact causality guard and its linear fallback
+   * (_anderson_mix!, numerics/optimized/production_mixing.jl:224-317); the
+   * three parameters as in AlgorithmOptions (depth 1..8 here; the reference
+   * defaults are 5, 1.0, 1e-12). */
+  int mixing;
+  int anderson_history_depth;
+  double anderson_damping;
+  double anderson_regularization;
 } qcl_scba_problem;
+
+/* Mixer diagnostics of the last step (the metrics _anderson_mix! reports,
+ * production_mixing.jl:283-298).  reset_reason: 0 none, 1 residual_increase,
+ * 2 coefficient_solve, 3 coefficient_bound, 4 causality_guard;
+ * guard_first_failure: 1-based block index (family, e, m; m fastest) of the
+ * first guard failure, 0 if none. */
+typedef struct qcl_anderson_info {
+  int history_depth;
+  int reset_reason;
+  int acceleration_accepted;
+  int fallback;
+  int guard_failure_code;
+  long long guard_first_failure;
+  double coefficients_l1;
+} qcl_anderson_info;
 
 /* One SCBAIteration row (domain/types.jl:908).  status: QCL_OK or
  * QCL_NONFINITE (the :nonfinite_metrics exit). */
@@ -333,6 +357,15 @@ int qcl_scba_upload(qcl_scba* ctx, int which, const void* host);
  * resident: the next step continues from the last unmixed state (warm
  * start); the row history (r_J, r_pop, lambda_change, nu) restarts. */
 int qcl_scba_retarget(qcl_scba* ctx, double Ep, double N_LO, double kBT, const void* h, const double* q);
+/* The causality / Keldysh guard of a set of self-energy families
+ * (_anderson_guard / _anderson_block_failure!, numerics/optimized/
+ * production_mixing.jl:48-118): fields = nfam x (SigmaR, Sigma<, Sigma>).
+ * first_failure = 1-based index of the first failing block over (family, e,
+ * m), m fastest, 0 if all pass; code = the reference's failure code 1..5. */
+int qcl_anderson_guard(int precision, int NE, int Nk, int Nb, int nfam, const void* const* fields,
+                       long long* first_failure, int* code);
+/* Anderson mixer diagnostics of the last step (all zero for linear mixing). */
+int qcl_scba_mixer_info(qcl_scba* ctx, qcl_anderson_info* info);
 /* Replay each iteration as one captured CUDA graph (default off). */
 int qcl_scba_use_graph(qcl_scba* ctx, int enable);
 /* The derived GreenState fields of the last Dyson solve (seed or step) --

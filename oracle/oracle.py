@@ -564,6 +564,159 @@ def make_plans(problem):
     }
 
 
+# --------------------------------------------------------------------------
+# Anderson mixing (numerics/optimized/production_mixing.jl:1-317)
+# --------------------------------------------------------------------------
+_EPS = float(np.finfo(np.float64).eps)
+_TINY = float(np.finfo(np.float64).tiny)
+
+
+def _anderson_inner(left, right):
+    """_anderson_inner (production_mixing.jl:129-138): sum of Re <a, b> over
+    families and components, column-major order."""
+    v = 0.0
+    for fa, fb in zip(left, right):
+        for a, b in zip(fa, fb):
+            v += float(np.real(np.vdot(np.ravel(a, order="F"), np.ravel(b, order="F"))))
+    return v
+
+
+def anderson_coefficients(gram, regularization):
+    """_anderson_coefficients (production_mixing.jl:155-180).  Raises
+    ValueError where the reference throws ArgumentError."""
+    count = gram.shape[0]
+    if count == 1:
+        return np.ones(1)
+    g = np.array(gram, dtype=np.float64)
+    scale = max(float(np.max(np.abs(np.diag(g)))), _EPS)
+    g[np.diag_indices(count)] += regularization * scale
+    values, vectors = np.linalg.eigh(g / scale)
+    cutoff = max(regularization, math.sqrt(_EPS))
+    projected = vectors.T @ np.ones(count)
+    weights = np.array([projected[i] / values[i] if values[i] > cutoff else 0.0 for i in range(count)])
+    coef = vectors @ weights
+    denom = float(np.sum(coef))
+    if not (math.isfinite(denom) and abs(denom) > _EPS):
+        raise ValueError("Anderson history is rank deficient")
+    coef = coef / denom
+    if not np.all(np.isfinite(coef)):
+        raise ValueError("Anderson coefficient solve produced non-finite values")
+    return coef
+
+
+def anderson_block_failure(R, L, G):
+    """_anderson_block_failure! (production_mixing.jl:48-96): 0 or the code."""
+    n = R.shape[0]
+    if not np.all(np.isfinite(R)):
+        return 1
+    Hm = (R - R.conj().T) / 2j
+    nR = np.linalg.norm(R, 2)
+    if not np.linalg.eigvalsh(0.5 * (Hm + Hm.conj().T)).max() <= 64 * _EPS * max(nR, _TINY):
+        return 2
+    if not (np.all(np.isfinite(L)) and np.all(np.isfinite(G))):
+        return 1
+    for X, f in ((L, -1j), (G, 1j)):
+        F = f * X
+        budget = 64 * n * _EPS * max(np.linalg.norm(F, 2), 1.0)
+        if not np.linalg.norm(F - F.conj().T) / 2 <= budget:
+            return 3
+        if not np.linalg.eigvalsh(0.5 * (F + F.conj().T)).min() >= -budget:
+            return 4
+    diff = R - R.conj().T - (G - L)
+    budget = 64 * n * _EPS * max(nR, np.linalg.norm(L, 2), np.linalg.norm(G, 2), 1.0)
+    if not np.linalg.norm(diff) <= budget:
+        return 5
+    return 0
+
+
+def anderson_guard(families):
+    """_anderson_guard (production_mixing.jl:98-118): (passed, first failing
+    1-based index over (family, e, m) with m fastest, code)."""
+    for fi, (R, L, G) in enumerate(families):
+        NE, Nk = R.shape[0], R.shape[1]
+        for e in range(NE):
+            for m in range(Nk):
+                code = anderson_block_failure(R[e, m], L[e, m], G[e, m])
+                if code:
+                    return False, fi * NE * Nk + e * Nk + m + 1, code
+    return True, 0, 0
+
+
+class AndersonMixer:
+    """The _AndersonWorkspace history with _anderson_append! and
+    _anderson_mix! (production_mixing.jl:184-317)."""
+
+    def __init__(self, depth=5, damping=1.0, regularization=1e-12):
+        self.depth, self.damping, self.regularization = depth, damping, regularization
+        self.states, self.residuals = [], []
+        self.gram = np.zeros((0, 0))
+        self.info = {}
+
+    def clear(self):
+        self.states, self.residuals = [], []
+        self.gram = np.zeros((0, 0))
+
+    def append(self, state, candidate):
+        prior = None if not self.residuals else float(self.gram[-1, -1])
+        if len(self.states) >= self.depth:
+            self.states.pop(0)
+            self.residuals.pop(0)
+            self.gram = self.gram[1:, 1:]
+        saved = [tuple(np.array(c, order="F") for c in f) for f in state]
+        residual = [tuple(np.asfortranarray(cand[c] - st[c]) for c in range(3)) for st, cand in zip(state, candidate)]
+        rn = _anderson_inner(residual, residual)
+        reset = prior is not None and rn > (1 + 64 * _EPS) * max(prior, _TINY)
+        if reset:
+            self.clear()
+        count = len(self.states) + 1
+        gram = np.zeros((count, count))
+        if count > 1:
+            gram[:-1, :-1] = self.gram
+        for i in range(count - 1):
+            gram[i, -1] = gram[-1, i] = _anderson_inner(self.residuals[i], residual)
+        gram[-1, -1] = rn
+        self.gram = gram
+        self.states.append(saved)
+        self.residuals.append(residual)
+        return reset
+
+    def mix(self, state, candidate, alpha):
+        reset = self.append(state, candidate)
+        reason = "residual_increase" if reset else "none"
+        try:
+            coef = anderson_coefficients(self.gram, self.regularization)
+        except ValueError:
+            reason = "coefficient_solve"
+            coef = np.r_[np.zeros(len(self.residuals) - 1), 1.0]
+        if np.sum(np.abs(coef)) > 10 or not np.all(np.isfinite(coef)):
+            reason = "coefficient_bound"
+            coef = np.r_[np.zeros(len(self.residuals) - 1), 1.0]
+        d = alpha * self.damping
+        out = []
+        for fi in range(len(state)):
+            comps = []
+            for c in range(3):
+                v = np.zeros_like(self.states[0][fi][c])
+                for h in range(len(coef)):
+                    v = v + coef[h] * (self.states[h][fi][c] + d * self.residuals[h][fi][c])
+                comps.append(np.asfortranarray(v))
+            out.append(tuple(comps))
+        depth = len(self.states)
+        passed, first, code = anderson_guard(out)
+        accepted = passed and int(np.count_nonzero(coef)) > 1
+        if not passed:
+            x, r = self.states[-1], self.residuals[-1]
+            out = [tuple(np.asfortranarray(x[fi][c] + d * r[fi][c]) for c in range(3)) for fi in range(len(state))]
+            self.clear()
+            reason = "causality_guard"
+            if not anderson_guard(out)[0]:
+                raise OracleError(2, "convex Anderson fallback is not admissible; inspect raw self-energies")
+        self.info = dict(history_depth=depth, reset_reason=reason, coefficients_l1=float(np.sum(np.abs(coef))),
+                         acceleration_accepted=accepted, guard_first_failure=first, guard_failure_code=code,
+                         fallback=not passed)
+        return out
+
+
 def scba(problem, iterations, verify=True, state=None, keep_state=False):
     """Run `iterations` SCBA steps (solve_scba, scba.jl:142-354, with the
     production operators).  Returns (history, state)."""
@@ -577,6 +730,10 @@ def scba(problem, iterations, verify=True, state=None, keep_state=False):
     history = []
     Jprev = None
     pprev = None
+    mixer = None
+    if getattr(problem, "mixing", "linear") == "anderson":
+        mixer = AndersonMixer(problem.anderson_history_depth, problem.anderson_damping,
+                              problem.anderson_regularization)
     for nu in range(1, iterations + 1):
         total = total_family(problem, scattering, plus, minus)
         green, lam = current_green(problem, total)
@@ -604,6 +761,17 @@ def scba(problem, iterations, verify=True, state=None, keep_state=False):
                    lambda_change=math.nan if not history else lam - history[-1]["lam"], **res)
         history.append(row)
         a = problem.alpha
+        if mixer is not None:
+            names = [m.name for m in problem.mechanisms]
+            st = [scattering[n] for n in names] + [plus, minus]
+            cd = [cand_sc[n] for n in names] + [cplus, cminus]
+            mixed = mixer.mix(st, cd, a)
+            row["mixer"] = dict(mixer.info)
+            for i, n in enumerate(names):
+                scattering[n] = mixed[i]
+            plus, minus = mixed[-2], mixed[-1]
+            Jprev, pprev = J, pops
+            continue
         for m in problem.mechanisms:
             scattering[m.name] = tuple(np.asfortranarray((1 - a) * scattering[m.name][c] + a * cand_sc[m.name][c])
                                        for c in range(3))

@@ -139,6 +139,7 @@ int scba_set_graph(ScbaCtx* c, int enable);
 int scba_green_state(ScbaCtx* c, void* A, double* kappa, double* scale);
 int scba_witness(ScbaCtx* c, double* out12);
 int scba_retarget(ScbaCtx* c, double Ep, double N_LO, double kBT, const void* h, const double* q);
+int scba_mixer_info(ScbaCtx* c, qcl_anderson_info* out);
 
 static int shift_plan_dev(int NE, const double* eps, double delta, DevBuf& l, DevBuf& r, DevBuf& th, DevBuf& v,
                           ShiftPlanDev* out) {
@@ -695,6 +696,51 @@ int qcl_scba_retarget(qcl_scba* ctx, double Ep, double N_LO, double kBT, const v
     return QCL_ARG;
   }
   return scba_retarget((ScbaCtx*)ctx, Ep, N_LO, kBT, h, q);
+}
+
+int qcl_anderson_guard(int precision, int NE, int Nk, int Nb, int nfam, const void* const* fields,
+                       long long* first_failure, int* code) {
+  if (int s = check_precision(precision)) return s;
+  if (NE <= 0 || Nk <= 0 || Nb <= 0 || nfam < 1 || nfam > kMaxMixFields / 3) {
+    set_last_error("anderson_guard: bad dimensions (%d,%d,%d) or family count %d", NE, Nk, Nb, nfam);
+    return QCL_DIM;
+  }
+  if (!fields || !first_failure || !code) {
+    set_last_error("anderson_guard: fields and outputs are required");
+    return QCL_ARG;
+  }
+  const int sp = precision == QCL_MIXED ? QCL_C64 : precision;
+  const size_t nb = field_elems(NE, Nk, Nb) * cbytes(sp);
+  std::vector<DevBuf> d(3 * nfam);
+  void* ptr[kMaxMixFields];
+  int s;
+  for (int i = 0; i < 3 * nfam; ++i) {
+    if (!fields[i]) {
+      set_last_error("anderson_guard: field %d is NULL", i);
+      return QCL_ARG;
+    }
+    if ((s = d[i].upload(fields[i], nb))) return s;
+    ptr[i] = d[i].p;
+  }
+  DevBuf meta;
+  if ((s = meta.alloc(sizeof(AndersonMeta)))) return s;
+  if ((s = launch_anderson_reset((AndersonMeta*)meta.p, 0))) return s;
+  if ((s = launch_anderson_guard(sp, NE, Nk, Nb, ptr, nfam, (AndersonMeta*)meta.p, 0, 0))) return s;
+  QCL_CUDA_CHECK(cudaDeviceSynchronize());
+  AndersonMeta h;
+  QCL_CUDA_CHECK(cudaMemcpy(&h, meta.p, sizeof(h), cudaMemcpyDeviceToHost));
+  const bool failed = h.guard_key != ~0ull;
+  *first_failure = failed ? (long long)(h.guard_key >> 3) : 0;
+  *code = failed ? (int)(h.guard_key & 7ull) : 0;
+  return QCL_OK;
+}
+
+int qcl_scba_mixer_info(qcl_scba* ctx, qcl_anderson_info* info) {
+  if (!ctx || !info) {
+    set_last_error("ctx and info are required");
+    return QCL_ARG;
+  }
+  return scba_mixer_info((ScbaCtx*)ctx, info);
 }
 
 int qcl_scba_witness(qcl_scba* ctx, qcl_psd_witness* witness) {

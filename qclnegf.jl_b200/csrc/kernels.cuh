@@ -28,6 +28,38 @@ int launch_residual_witness(int precision, int NE, int Nk, int N, const void* GR
                             const void* SL, const void* SG, const double* work, double* partial, double* out12,
                             cudaStream_t st);
 size_t residual_witness_partial_doubles();
+// Anderson mixing (anderson.cu; guard in residual.cu).  Device-resident mixer
+// state, so that an iteration stays one stream-ordered launch sequence.
+constexpr int kAndersonMaxDepth = 8;
+struct AndersonMeta {
+  int count;   // history entries; logical entry j is ring slot (head + j) % depth
+  int head;
+  int slot;    // ring slot of this step's entry
+  int reason;  // 0 none, 1 residual_increase, 2 coefficient_solve, 3 coefficient_bound, 4 causality_guard
+  int fallback;    // the guard rejected the accelerated state; linear fallback applied
+  int accepted;    // accelerated state accepted with more than one non-zero coefficient
+  int used;        // history entries the mix used
+  int guard_code;  // code of the first failing block of the first guard pass (0 none)
+  unsigned long long guard_key;   // (1-based first failing index << 3) | code of the current pass
+  unsigned long long guard_first; // 1-based first failing index of the first pass (0 none)
+  double prior;    // <R_last, R_last> before this step (< 0: empty history)
+  double l1;       // sum |coefficients|
+  double gram[kAndersonMaxDepth * kAndersonMaxDepth];
+  double coef[kAndersonMaxDepth];
+  double dots[kAndersonMaxDepth + 1];
+};
+size_t anderson_partial_doubles(int nf);
+int launch_anderson_reset(AndersonMeta* m, cudaStream_t st);
+int launch_anderson_plan(AndersonMeta* m, int depth, cudaStream_t st);
+int launch_anderson_append(int precision, size_t n, const void* const* state, const void* const* cand, int nf,
+                           void* Xh, void* Rh, int depth, AndersonMeta* meta, double* partial, double* fam_out,
+                           cudaStream_t st);
+int launch_anderson_coefficients(AndersonMeta* m, int depth, double regularization, cudaStream_t st);
+int launch_anderson_mix(int precision, size_t n, void* const* out, int nf, const void* Xh, const void* Rh, int depth,
+                        const AndersonMeta* m, double damping, int fallback, cudaStream_t st);
+int launch_anderson_after_guard(AndersonMeta* m, int pass, int* status, cudaStream_t st);
+int launch_anderson_guard(int precision, int NE, int Nk, int N, void* const* fields, int nfam, AndersonMeta* m,
+                          int pass, cudaStream_t st);
 // scattering-model switches (model.cu)
 int launch_retarded_drop(int precision, size_t n, const void* SL, const void* SG, void* SR, cudaStream_t st);
 int launch_scattering_model(int precision, int NE, int Nk, int N, const double* wk, double norm, int diagonal,

@@ -1072,6 +1072,226 @@ template <typename RS> static int launch_witness_detail_p(const WitnessArgs<RS>&
   }
 }
 
+// ---------------------------------------------------------------------------
+// Causality / Keldysh guard of an Anderson-mixed state
+// (_anderson_block_failure!, numerics/optimized/production_mixing.jl:48-96),
+// per block of every family, n = N_b:
+//   1  a non-finite entry in Sigma^R, Sigma< or Sigma>;
+//   2  lmax(Im_H Sigma^R) > 64 eps max(||Sigma^R||_2, floatmin);
+//   3  ||fX - (fX)^H||_F / 2 > b(X), 4  lmin(Herm fX) < -b(X), for (X, f) =
+//      (Sigma<, -i), (Sigma>, i), b(X) = 64 n eps max(||X||_2, 1);
+//   5  ||Sigma^R - Sigma^R^H - (Sigma> - Sigma<)||_F > 64 n eps max(||Sigma^R||_2,
+//      ||Sigma<||_2, ||Sigma>||_2, 1).
+// Every test first tries a sufficient condition that needs no spectrum:
+// LDL^T certificates for the sign tests, and max |entry| <= ||X||_2 for the
+// budgets; the exact spectral norms and extreme eigenvalues (tridiagonal
+// multisection) are computed only for blocks those do not settle.  The first
+// failing block in the reference's order (family, e, m; m fastest) is kept
+// with its code by one atomicMin on (index << 3 | code).
+// ---------------------------------------------------------------------------
+constexpr int kGuardMaxFamilies = kMaxMixFields / 3;
+template <typename RS> struct GuardArgs {
+  int NE, Nk, N, nfam, pass;
+  const Cx<RS>* f[3 * kGuardMaxFamilies];
+  AndersonMeta* meta;
+};
+
+template <int NP, int TT>
+__device__ double team_maxabs(const Cx<double>* X, int N, int tt, ResScratch<NP>& S, int team) {
+  double a = 0;
+  for (int idx = tt; idx < N * N; idx += TT) {
+    const Cx<double> v = X[sw<NP>(idx % N, idx / N)];
+    a = fmax(a, hypot(v.x, v.y));
+  }
+  return team_max<TT>(a, tt, S.red, team);
+}
+
+// ||X||_2 = sqrt(lmax(X X^H)); W is scratch.
+template <int NP, int TT>
+__device__ double team_norm2(const Cx<double>* X, Cx<double>* W, int N, int tt, ResScratch<NP>& S, int team) {
+  team_matmul<double, double, NP>(X, X, W, N, tt, true);
+  team_sync<TT>(team);
+  return sqrt(fmax(team_lmax<NP, TT>(W, N, tt, S, team, false), 0.0));
+}
+
+template <typename RS, int NP, int BPC>
+__global__ void __launch_bounds__(BPC* Tile<NP>::TT) anderson_guard_kernel(GuardArgs<RS> p) {
+  if (p.pass == 1 && !p.meta->fallback) return;
+  constexpr int TT = Tile<NP>::TT;
+  constexpr size_t MSZ = (size_t)NP * NP;
+  constexpr double eps = 2.220446049250313e-16;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  Cx<double>* bR = reinterpret_cast<Cx<double>*>(smem_raw);
+  Cx<double>* bL = bR + BPC * MSZ;
+  Cx<double>* bG = bL + BPC * MSZ;
+  Cx<double>* bH = bG + BPC * MSZ;
+  Cx<double>* bW = bH + BPC * MSZ;
+  ResScratch<NP>* scr = reinterpret_cast<ResScratch<NP>*>(bW + BPC * MSZ);
+  const int N = p.N, NE = p.NE, Nk = p.Nk, fam = blockIdx.z;
+  const int m = blockIdx.y, e0 = blockIdx.x * BPC;
+  const int team = threadIdx.x / TT, tt = threadIdx.x % TT;
+  const int e = e0 + team;
+  const bool live = e < NE;
+  Cx<double>* R = bR + team * MSZ;
+  Cx<double>* L = bL + team * MSZ;
+  Cx<double>* G = bG + team * MSZ;
+  Cx<double>* H = bH + team * MSZ;
+  Cx<double>* W = bW + team * MSZ;
+  ResScratch<NP>& S = scr[team];
+  load_tile<RS, NP, BPC>(p.f[3 * fam + 0], bR, e0, m, NE, Nk, N);
+  load_tile<RS, NP, BPC>(p.f[3 * fam + 1], bL, e0, m, NE, Nk, N);
+  load_tile<RS, NP, BPC>(p.f[3 * fam + 2], bG, e0, m, NE, Nk, N);
+  __syncthreads();
+  int code = 0;
+  // finiteness of the three blocks (code 1; the reference tests Sigma^R first)
+  double badR = 0, badLG = 0;
+  for (int idx = tt; idx < N * N; idx += TT) {
+    const int i = idx % N, j = idx / N;
+    const Cx<double> r = R[sw<NP>(i, j)], l = L[sw<NP>(i, j)], g = G[sw<NP>(i, j)];
+    if (!isfinite(r.x) || !isfinite(r.y)) badR = 1;
+    if (!isfinite(l.x) || !isfinite(l.y) || !isfinite(g.x) || !isfinite(g.y)) badLG = 1;
+  }
+  badR = team_max<TT>(badR, tt, S.red, team);
+  badLG = team_max<TT>(badLG, tt, S.red, team);
+  double nR = -1;  // ||Sigma^R||_2 once computed
+  if (badR != 0) code = 1;
+  if (!code) {  // code 2: causality of Sigma^R
+    for (int idx = tt; idx < N * N; idx += TT) {
+      const int i = idx % N, j = idx / N;
+      const Cx<double> a = R[sw<NP>(i, j)], b = R[sw<NP>(j, i)];
+      // -(a - conj b) / (2i) = -Im_H
+      W[sw<NP>(i, j)] = cx<double>(-0.5 * (a.y + b.y), 0.5 * (a.x - b.x));
+    }
+    team_sync<TT>(team);
+    if (!team_posdef<NP, TT>(W, N, 0.0, tt, team)) {
+      team_sync<TT>(team);
+      for (int idx = tt; idx < N * N; idx += TT) {
+        const int i = idx % N, j = idx / N;
+        const Cx<double> a = R[sw<NP>(i, j)], b = R[sw<NP>(j, i)];
+        H[sw<NP>(i, j)] = cx<double>(0.5 * (a.y + b.y), -0.5 * (a.x - b.x));  // Im_H
+      }
+      team_sync<TT>(team);
+      const double lmax = team_lmax<NP, TT>(H, N, tt, S, team, false);
+      team_sync<TT>(team);
+      nR = team_norm2<NP, TT>(R, W, N, tt, S, team);
+      if (!(lmax <= 64 * eps * fmax(nR, 2.2250738585072014e-308))) code = 2;
+    }
+    team_sync<TT>(team);
+  }
+  if (!code && badLG != 0) code = 1;
+  for (int which = 0; which < 2 && !code; ++which) {  // codes 3, 4
+    const Cx<double>* X = which == 0 ? L : G;
+    const double fs = which == 0 ? -1.0 : 1.0;  // f = fs * i
+    double dF2 = 0, amax = 0;
+    for (int idx = tt; idx < N * N; idx += TT) {
+      const int i = idx % N, j = idx / N;
+      const Cx<double> a = X[sw<NP>(i, j)], b = X[sw<NP>(j, i)];
+      const Cx<double> v = cx<double>(-fs * a.y, fs * a.x), u = cx<double>(-fs * b.y, fs * b.x);
+      H[sw<NP>(i, j)] = cx<double>(0.5 * (v.x + u.x), 0.5 * (v.y - u.y));
+      const double dx = v.x - u.x, dy = v.y + u.y;
+      dF2 += dx * dx + dy * dy;
+      amax = fmax(amax, hypot(a.x, a.y));
+    }
+    dF2 = team_sum<TT>(dF2, tt, S.red, team);
+    amax = team_max<TT>(amax, tt, S.red, team);
+    const double herm = sqrt(dF2) / 2;
+    const double blo = 64.0 * N * eps * fmax(amax, 1.0);  // amax <= ||X||_2
+    team_sync<TT>(team);
+    if (herm <= blo && team_posdef<NP, TT>(H, N, blo, tt, team)) continue;
+    team_sync<TT>(team);
+    const double budget = 64.0 * N * eps * fmax(team_norm2<NP, TT>(X, W, N, tt, S, team), 1.0);
+    team_sync<TT>(team);
+    if (!(herm <= budget)) {
+      code = 3;
+      break;
+    }
+    for (int idx = tt; idx < N * N; idx += TT) {
+      const int i = idx % N, j = idx / N;
+      const Cx<double> a = X[sw<NP>(i, j)], b = X[sw<NP>(j, i)];
+      const Cx<double> v = cx<double>(-fs * a.y, fs * a.x), u = cx<double>(-fs * b.y, fs * b.x);
+      H[sw<NP>(i, j)] = cx<double>(0.5 * (v.x + u.x), 0.5 * (v.y - u.y));
+    }
+    team_sync<TT>(team);
+    team_tridiagonalize<NP, TT>(H, N, tt, S, team);
+    double lmin = INFINITY;
+    bool fin = true;
+    for (int i = 0; i < N; ++i) fin = fin && isfinite(S.d[i]) && (i + 1 >= N || isfinite(S.e2[i]));
+    if (fin) lmin = tri_eig(S.d, S.e2, N, 1);
+    team_sync<TT>(team);
+    if (!(lmin >= -budget)) code = 4;
+  }
+  if (!code) {  // code 5: Keldysh identity
+    double dF2 = 0, amax = 0;
+    for (int idx = tt; idx < N * N; idx += TT) {
+      const int i = idx % N, j = idx / N;
+      const Cx<double> a = R[sw<NP>(i, j)], b = R[sw<NP>(j, i)], l = L[sw<NP>(i, j)], g = G[sw<NP>(i, j)];
+      const double dx = (a.x - b.x) - (g.x - l.x), dy = (a.y + b.y) - (g.y - l.y);
+      dF2 += dx * dx + dy * dy;
+      amax = fmax(amax, fmax(hypot(a.x, a.y), fmax(hypot(l.x, l.y), hypot(g.x, g.y))));
+    }
+    dF2 = team_sum<TT>(dF2, tt, S.red, team);
+    amax = team_max<TT>(amax, tt, S.red, team);
+    const double dF = sqrt(dF2);
+    if (!(dF <= 64.0 * N * eps * fmax(amax, 1.0))) {
+      team_sync<TT>(team);
+      if (nR < 0) nR = team_norm2<NP, TT>(R, W, N, tt, S, team);
+      team_sync<TT>(team);
+      const double nL = team_norm2<NP, TT>(L, W, N, tt, S, team);
+      team_sync<TT>(team);
+      const double nG = team_norm2<NP, TT>(G, W, N, tt, S, team);
+      if (!(dF <= 64.0 * N * eps * fmax(fmax(nR, fmax(nL, nG)), 1.0))) code = 5;
+    }
+  }
+  if (code && live && tt == 0) {
+    const unsigned long long idx = (unsigned long long)fam * NE * Nk + (unsigned long long)e * Nk + m + 1;
+    atomicMin(&p.meta->guard_key, (idx << 3) | (unsigned long long)code);
+  }
+}
+
+template <typename RS, int NP, int BPC> static int launch_guard_t(const GuardArgs<RS>& a, cudaStream_t st) {
+  constexpr int TT = Tile<NP>::TT;
+  constexpr size_t smem = 5 * (size_t)BPC * NP * NP * sizeof(Cx<double>) + BPC * sizeof(ResScratch<NP>);
+  static bool configured = false;
+  if (!configured) {
+    QCL_CUDA_CHECK(cudaFuncSetAttribute(anderson_guard_kernel<RS, NP, BPC>,
+                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    configured = true;
+  }
+  dim3 grid((a.NE + BPC - 1) / BPC, a.Nk, a.nfam);
+  anderson_guard_kernel<RS, NP, BPC><<<grid, BPC * TT, smem, st>>>(a);
+  QCL_LAUNCH_CHECK("anderson_guard_kernel");
+  return QCL_OK;
+}
+
+template <typename RS> static int launch_guard_p(const GuardArgs<RS>& a, cudaStream_t st) {
+  switch (padded_size(a.N)) {
+    case 8: return launch_guard_t<RS, 8, 8>(a, st);
+    case 16: return launch_guard_t<RS, 16, 4>(a, st);
+    case 24: return launch_guard_t<RS, 24, 2>(a, st);
+    case 32: return launch_guard_t<RS, 32, 1>(a, st);
+    case 48: return launch_guard_t<RS, 48, 1>(a, st);
+    default:
+      set_last_error("basis size N_b=%d exceeds the supported maximum 48", a.N);
+      return QCL_UNSUPPORTED;
+  }
+}
+
+int launch_anderson_guard(int precision, int NE, int Nk, int N, void* const* fields, int nfam, AndersonMeta* m,
+                          int pass, cudaStream_t st) {
+  if (nfam < 1 || nfam > kGuardMaxFamilies) {
+    set_last_error("anderson guard: %d families out of range", nfam);
+    return QCL_ARG;
+  }
+  if (precision == QCL_C128) {
+    GuardArgs<double> a{NE, Nk, N, nfam, pass, {}, m};
+    for (int i = 0; i < 3 * nfam; ++i) a.f[i] = (const Cx<double>*)fields[i];
+    return launch_guard_p<double>(a, st);
+  }
+  GuardArgs<float> a{NE, Nk, N, nfam, pass, {}, m};
+  for (int i = 0; i < 3 * nfam; ++i) a.f[i] = (const Cx<float>*)fields[i];
+  return launch_guard_p<float>(a, st);
+}
+
 constexpr int RES_CTAS = 148;
 
 size_t residual_work_doubles(int NE, int Nk) { return kResidualBlockDoubles * (size_t)NE * Nk + 7 * RES_CTAS; }

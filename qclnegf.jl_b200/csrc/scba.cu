@@ -78,6 +78,13 @@ struct ScbaCtx {
   int NE, Nk, N, M, precision, gs, verify;
   int diagonal = 0, averaged = 0, drop_real = 0, direct_green = 0;  // scattering-model switches
   int scalar_lesser = 0;                                             // occupation_normalization
+  // Anderson mixing (mixing = :anderson): device history and mixer state
+  int mixing = 0, and_depth = 5;
+  double and_damping = 1.0, and_reg = 1e-12;
+  void *Xh = nullptr, *Rh = nullptr;
+  AndersonMeta* ameta = nullptr;
+  AndersonMeta* ameta_h = nullptr;  // pinned copy, read after each step
+  double* apartial = nullptr;
   double wk_sum = 0;
   double Ep, hw_LO, N_LO, target, eta_seed, kBT, alpha, J0;
   size_t nfield, fbytes;
@@ -223,6 +230,11 @@ void scba_destroy(ScbaCtx* c) {
   cudaFree(c->scal);
   cudaFreeHost(c->scal_h);
   cudaFree(c->status);
+  cudaFree(c->Xh);
+  cudaFree(c->Rh);
+  cudaFree(c->ameta);
+  cudaFree(c->apartial);
+  if (c->ameta_h) cudaFreeHost(c->ameta_h);
   free_hilbert_tables(c->hil);
   if (c->st) cudaStreamDestroy(c->st);
   delete c;
@@ -271,6 +283,10 @@ int scba_create(const qcl_scba_problem* p, const qcl_mechanism* mechs, ScbaCtx**
   c->drop_real = p->retarded_real_part;
   c->direct_green = p->elastic_retarded;
   c->scalar_lesser = p->occupation_normalization;
+  c->mixing = p->mixing;
+  c->and_depth = p->anderson_history_depth;
+  c->and_damping = p->anderson_damping;
+  c->and_reg = p->anderson_regularization;
   c->nfield = field_elems(c->NE, c->Nk, c->N);
   c->fbytes = c->nfield * (c->precision == QCL_C128 ? 16 : 8);
   c->eps_h.assign(p->eps, p->eps + p->NE);
@@ -291,6 +307,17 @@ int scba_create(const qcl_scba_problem* p, const qcl_mechanism* mechs, ScbaCtx**
       TRY((set_last_error("model switches (self_energy_structure, transverse_momentum, retarded_real_part, "
                           "elastic_retarded, occupation_normalization) must be 0 or 1"),
            QCL_ARG));
+  if (c->mixing != 0 && c->mixing != 1) TRY((set_last_error("mixing must be 0 (:linear) or 1 (:anderson)"), QCL_ARG));
+  if (c->mixing) {  // _check_algorithm_options (algorithm_options.jl:84-91)
+    if (c->and_depth < 1) TRY((set_last_error("anderson_history_depth must be positive"), QCL_ARG));
+    if (c->and_depth > kAndersonMaxDepth)
+      TRY((set_last_error("anderson_history_depth %d exceeds the supported maximum %d", c->and_depth,
+                          kAndersonMaxDepth),
+           QCL_UNSUPPORTED));
+    if (!(c->and_damping > 0 && c->and_damping <= 1)) TRY((set_last_error("anderson_damping must lie in (0,1]"), QCL_ARG));
+    if (!(c->and_reg >= 0) || !isfinite(c->and_reg))
+      TRY((set_last_error("anderson_regularization cannot be negative"), QCL_ARG));
+  }
   for (int m = 0; m < c->Nk; ++m) c->wk_sum += p->wk[m];
   if (c->averaged && !(c->wk_sum > 0)) TRY((set_last_error("radial weights must have positive sum"), QCL_ARG));
   if (c->direct_green && !c->drop_real)
@@ -375,6 +402,17 @@ int scba_create(const qcl_scba_problem* p, const qcl_mechanism* mechs, ScbaCtx**
   QCL_CUDA_CHECK(cudaMemsetAsync(c->status, 0, 2 * sizeof(int), c->st));
   for (auto& m : c->mech) m.status = c->status;
   QCL_CUDA_CHECK(cudaMemsetAsync(c->scal, 0, SC_TOTAL * sizeof(double), c->st));
+  if (c->mixing) {
+    const size_t nf = 3 * (size_t)(c->M + 2);
+    TRY(dalloc(&c->Xh, (size_t)c->and_depth * nf * c->fbytes));
+    TRY(dalloc(&c->Rh, (size_t)c->and_depth * nf * c->fbytes));
+    TRY(dalloc((void**)&c->ameta, sizeof(AndersonMeta)));
+    TRY(dalloc((void**)&c->apartial, anderson_partial_doubles((int)nf) * sizeof(double)));
+    cudaError_t e = cudaMallocHost((void**)&c->ameta_h, sizeof(AndersonMeta));
+    if (e != cudaSuccess) TRY(cuda_status(e, "cudaMallocHost"));
+    memset(c->ameta_h, 0, sizeof(AndersonMeta));
+    TRY(launch_anderson_reset(c->ameta, c->st));
+  }
   TRY(prepare_hilbert_tables(c->hil, c->NE, de, c->precision));
   TRY(ensure_partial(c->hil, (long long)c->Nk * N2));
 #undef TRY
@@ -518,9 +556,27 @@ static int iteration_body(ScbaCtx* c, std::vector<void*>& state, std::vector<voi
       olds[3 * f + k] = field_of(state, f, k);
       cands[3 * f + k] = field_of(cand, f, k);
     }
-  if ((s = launch_residual_mix_multi(sp, c->nfield, olds, cands, 3 * F, c->alpha, c->mpartial, c->scal + SC_FAM,
-                                     c->st)))
+  if (c->mixing) {
+    // Anderson mixing with the causality guard (production_mixing.jl:224-317)
+    const int nf = 3 * F;
+    if ((s = launch_anderson_plan(c->ameta, c->and_depth, c->st))) return s;
+    if ((s = launch_anderson_append(sp, c->nfield, olds, (const void* const*)cands, nf, c->Xh, c->Rh, c->and_depth,
+                                    c->ameta, c->apartial, c->scal + SC_FAM, c->st)))
+      return s;
+    if ((s = launch_anderson_coefficients(c->ameta, c->and_depth, c->and_reg, c->st))) return s;
+    const double damping = c->alpha * c->and_damping;
+    for (int pass = 0; pass < 2; ++pass) {  // pass 1 (linear fallback) runs only if pass 0's guard failed
+      if ((s = launch_anderson_mix(sp, c->nfield, cands, nf, c->Xh, c->Rh, c->and_depth, c->ameta, damping, pass,
+                                   c->st)))
+        return s;
+      if ((s = launch_anderson_guard(sp, c->NE, c->Nk, c->N, cands, F, c->ameta, pass, c->st))) return s;
+      if ((s = launch_anderson_after_guard(c->ameta, pass, c->status, c->st))) return s;
+    }
+    QCL_CUDA_CHECK(cudaMemcpyAsync(c->ameta_h, c->ameta, sizeof(AndersonMeta), cudaMemcpyDeviceToHost, c->st));
+  } else if ((s = launch_residual_mix_multi(sp, c->nfield, olds, cands, 3 * F, c->alpha, c->mpartial,
+                                            c->scal + SC_FAM, c->st))) {
     return s;
+  }
   QCL_CUDA_CHECK(cudaMemcpyAsync(c->scal_h, c->scal, SC_TOTAL * sizeof(double), cudaMemcpyDeviceToHost, c->st));
   return QCL_OK;
 }
@@ -607,6 +663,10 @@ int scba_seed(ScbaCtx* c, double* mu_out) {
   c->have_green = true;
   c->green_eta = c->eta_seed;
   c->have_residual = false;  // the seed used the residual scratch
+  if (c->mixing) {
+    if ((s = launch_anderson_reset(c->ameta, c->st))) return s;
+    QCL_CUDA_CHECK(cudaStreamSynchronize(c->st));
+  }
   c->nu = 0;
   c->pending_commit = false;
   c->Jprev = NAN;
@@ -720,7 +780,10 @@ int scba_step(ScbaCtx* c, qcl_scba_row* row) {
   }
   if (hst[0] == QCL_DOMAIN) {
     c->pending_commit = false;
-    set_last_error("paired number normalisation rejected the raw occupation");
+    if (c->mixing && c->ameta_h->fallback)
+      set_last_error("convex Anderson fallback is not admissible; inspect raw self-energies (block %d)", hst[1]);
+    else
+      set_last_error("paired number normalisation rejected the raw occupation");
     return QCL_DOMAIN;
   }
   const double m[] = {row->r_D, row->r_A, row->r_K, row->r_Sigma, row->r_lambda, row->r_PSD, row->r_caus,
@@ -773,6 +836,10 @@ int scba_upload(ScbaCtx* c, int which, const void* host) {
     c->pending_commit = false;
   }
   std::vector<void*>& st = c->parity == 0 ? c->state : c->cand;
+  if (c->mixing) {  // a replaced state starts a new Anderson history
+    int s = launch_anderson_reset(c->ameta, c->st);
+    if (s) return s;
+  }
   QCL_CUDA_CHECK(cudaMemcpyAsync(st[idx], host, c->fbytes, cudaMemcpyHostToDevice, c->st));
   QCL_CUDA_CHECK(cudaStreamSynchronize(c->st));
   c->seeded = true;
@@ -882,6 +949,26 @@ int scba_retarget(ScbaCtx* c, double Ep, double N_LO, double kBT, const void* h,
   c->pprev.clear();
   c->have_green = false;
   c->have_residual = false;
+  if (c->mixing) {  // a new operating point starts a new Anderson history
+    if ((s = launch_anderson_reset(c->ameta, c->st))) return s;
+    QCL_CUDA_CHECK(cudaStreamSynchronize(c->st));
+  }
+  return QCL_OK;
+}
+
+// Mixer diagnostics of the last step (the SolverMetric list of _anderson_mix!,
+// production_mixing.jl:283-298).
+int scba_mixer_info(ScbaCtx* c, qcl_anderson_info* out) {
+  memset(out, 0, sizeof(*out));
+  if (!c->mixing) return QCL_OK;
+  const AndersonMeta& m = *c->ameta_h;
+  out->history_depth = m.used;
+  out->reset_reason = m.reason;
+  out->coefficients_l1 = m.l1;
+  out->acceleration_accepted = m.accepted;
+  out->fallback = m.fallback;
+  out->guard_first_failure = (long long)m.guard_first;
+  out->guard_failure_code = m.guard_code;
   return QCL_OK;
 }
 

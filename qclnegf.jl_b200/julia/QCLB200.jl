@@ -155,6 +155,8 @@ struct Problem
     # retarded_real_part (:kramers_kronig/:drop), elastic_retarded (:hilbert/:direct_green)
     self_energy_structure::Cint; transverse_momentum::Cint; retarded_real_part::Cint; elastic_retarded::Cint
     occupation_normalization::Cint  # :paired_convex / :scalar_lesser
+    mixing::Cint                    # :linear / :anderson
+    anderson_history_depth::Cint; anderson_damping::Float64; anderson_regularization::Float64
 end
 
 struct Row

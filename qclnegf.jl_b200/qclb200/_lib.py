@@ -145,6 +145,8 @@ def _declare(l):
         "qcl_scba_green_state": (I, [P, P, P, P]),
         "qcl_scba_witness": (I, [P, P]),
         "qcl_scba_retarget": (I, [P, D, D, D, P, P]),
+        "qcl_scba_mixer_info": (I, [P, P]),
+        "qcl_anderson_guard": (I, [I, I, I, I, I, P, P, P]),
     }
     for name, (res, args) in sig.items():
         if hasattr(l, name):

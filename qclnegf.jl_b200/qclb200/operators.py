@@ -227,6 +227,22 @@ def embedding_component(T, G, eps, delta, *, precision="c128"):
     return S
 
 
+def anderson_guard(families, *, precision="c128"):
+    """_anderson_guard (production_mixing.jl:98-118) on a list of
+    (SigmaR, Sigma<, Sigma>) families: (passed, first failing 1-based block
+    index over (family, e, m) with m fastest, failure code)."""
+    p = _prec(precision)
+    cdt = _CDT[p]
+    shape = np.shape(families[0][0])
+    NE, Nk, Nb, _ = shape
+    arrs = [_field(x, cdt, shape) for fam in families for x in fam]
+    ptrs = (ctypes.c_void_p * len(arrs))(*[a.ctypes.data for a in arrs])
+    first = ctypes.c_longlong()
+    code = ctypes.c_int()
+    check(lib().qcl_anderson_guard(p, NE, Nk, Nb, len(families), ptrs, ctypes.byref(first), ctypes.byref(code)))
+    return first.value == 0, int(first.value), int(code.value)
+
+
 WITNESS_KINDS = ("spectral", "occupied", "unoccupied", "broadening", "raw_occupied", "raw_unoccupied")
 
 

@@ -197,6 +197,10 @@ class SCBAProblem:
     retarded_real_part: str = "kramers_kronig"    # or "drop"
     elastic_retarded: str = "hilbert"             # or "direct_green"
     occupation_normalization: str = "paired_convex"  # or "scalar_lesser"
+    mixing: str = "linear"                        # or "anderson"
+    anderson_history_depth: int = 5
+    anderson_damping: float = 1.0
+    anderson_regularization: float = 1e-12
 
     @property
     def shape(self):

@@ -29,7 +29,19 @@ class _Problem(ctypes.Structure):
                 ("precision", ctypes.c_int), ("verify_roundoff", ctypes.c_int), ("nmech", ctypes.c_int),
                 ("self_energy_structure", ctypes.c_int), ("transverse_momentum", ctypes.c_int),
                 ("retarded_real_part", ctypes.c_int), ("elastic_retarded", ctypes.c_int),
-                ("occupation_normalization", ctypes.c_int)]
+                ("occupation_normalization", ctypes.c_int), ("mixing", ctypes.c_int),
+                ("anderson_history_depth", ctypes.c_int), ("anderson_damping", ctypes.c_double),
+                ("anderson_regularization", ctypes.c_double)]
+
+
+class AndersonInfo(ctypes.Structure):
+    _fields_ = [("history_depth", ctypes.c_int), ("reset_reason", ctypes.c_int),
+                ("acceleration_accepted", ctypes.c_int), ("fallback", ctypes.c_int),
+                ("guard_failure_code", ctypes.c_int), ("guard_first_failure", ctypes.c_longlong),
+                ("coefficients_l1", ctypes.c_double)]
+
+
+RESET_REASONS = ("none", "residual_increase", "coefficient_solve", "coefficient_bound", "causality_guard")
 
 
 # AlgorithmOptions model switches -> the C ABI's 0/1 codes (_check_algorithm_options,
@@ -40,6 +52,7 @@ _SWITCHES = {
     "retarded_real_part": ("kramers_kronig", "drop"),
     "elastic_retarded": ("hilbert", "direct_green"),
     "occupation_normalization": ("paired_convex", "scalar_lesser"),
+    "mixing": ("linear", "anderson"),
 }
 
 
@@ -84,7 +97,9 @@ class ProductionSCBA:
         ptr = [ctypes.c_void_p(a.ctypes.data) for a in self._keep]
         self._p = _Problem(pr.NE, pr.Nk, pr.Nb, *ptr, float(pr.Ep), float(pr.hw_LO), float(pr.N_LO), int(pr.gs),
                            float(pr.target), float(pr.eta_seed), float(pr.kBT), float(pr.alpha), float(pr.J0),
-                           self.precision, 1 if verify_roundoff else 0, len(pr.mechanisms), *_switch_codes(pr))
+                           self.precision, 1 if verify_roundoff else 0, len(pr.mechanisms), *_switch_codes(pr),
+                           int(getattr(pr, "anderson_history_depth", 5)), float(getattr(pr, "anderson_damping", 1.0)),
+                           float(getattr(pr, "anderson_regularization", 1e-12)))
         self._mechs = [mechanism_struct(m) for m in pr.mechanisms]
         arr = (type(self._mechs[0]) * max(len(self._mechs), 1))(*self._mechs) if self._mechs else None
         self._marr = arr
@@ -182,6 +197,14 @@ class ProductionSCBA:
                                       None if qarr is None else ctypes.c_void_p(qarr.ctypes.data)))
         self.problem = new
         return new
+
+    def mixer_info(self):
+        """Anderson mixer diagnostics of the last step."""
+        info = AndersonInfo()
+        check(lib().qcl_scba_mixer_info(self._h, ctypes.byref(info)))
+        d = {n: getattr(info, n) for n, _ in info._fields_}
+        d["reset_reason"] = RESET_REASONS[info.reset_reason]
+        return d
 
     def witness(self):
         """The positivity witness of the last step's residual suite."""

@@ -149,8 +149,9 @@ def test_scalar_lesser_normalisation_on_oracle(orc):
 def test_switch_codes_validate_symbols():
     from qclb200.scba import _switch_codes
 
-    assert _switch_codes(_small()) == [0, 0, 0, 0, 0]
-    assert _switch_codes(_small(self_energy_structure="diagonal", elastic_retarded="direct_green")) == [1, 0, 0, 1, 0]
+    assert _switch_codes(_small()) == [0, 0, 0, 0, 0, 0]
+    assert _switch_codes(_small(self_energy_structure="diagonal", elastic_retarded="direct_green")) == [1, 0, 0, 1, 0,
+                                                                                                         0]
     with pytest.raises(ValueError, match="transverse_momentum"):
         _switch_codes(_small(transverse_momentum="mean"))
 

@@ -181,6 +181,14 @@ int qcl_condition_number(int precision, int NE, int Nk, int Nb, const double* ep
  * (production_operators.jl:1387-1415). */
 int qcl_spectral_function(int precision, int NE, int Nk, int Nb, const void* GR, void* A);
 
+/* Integrated coherences rho_ab = sum_{m,e} wE_e wk_m G<_{e,m,a,b} (Nb x Nb,
+ * complex128, column-major): the `integrated` matrix of
+ * _electron_density_bar (physics/observables.jl:1-22) from which the outer
+ * Poisson loop forms n(z) = g_s/(2 pi) Re(-i chi(z) rho chi(z)^H)
+ * (production_solver.jl:1043). */
+int qcl_density_matrix(int precision, int NE, int Nk, int Nb, const double* wE, const double* wk, const void* GL,
+                       void* rho);
+
 /* Eigenvalues (unsorted) of `count` Hermitian n x n matrices stored back to
  * back (column-major complex128; the Hermitian part is used), n <= 48.
  * Replaces the per-block LAPACK zheev calls of the residual suite
@@ -364,6 +372,8 @@ int qcl_scba_retarget(qcl_scba* ctx, double Ep, double N_LO, double kBT, const v
  * m), m fastest, 0 if all pass; code = the reference's failure code 1..5. */
 int qcl_anderson_guard(int precision, int NE, int Nk, int Nb, int nfam, const void* const* fields,
                        long long* first_failure, int* code);
+/* qcl_density_matrix of the last Dyson solve (seed or step) of a context. */
+int qcl_scba_density_matrix(qcl_scba* ctx, void* rho);
 /* Anderson mixer diagnostics of the last step (all zero for linear mixing). */
 int qcl_scba_mixer_info(qcl_scba* ctx, qcl_anderson_info* info);
 /* Replay each iteration as one captured CUDA graph (default off). */

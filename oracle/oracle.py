@@ -565,6 +565,87 @@ def make_plans(problem):
 
 
 # --------------------------------------------------------------------------
+# Outer Hartree-Poisson loop (numerics/optimized/production_solver.jl:993-1151)
+# --------------------------------------------------------------------------
+def density_matrix(GL, wE, wk):
+    """integrated[a,b] = sum_m sum_e wE_e wk_m G<[e,m,a,b] in the reference's
+    loop order (_electron_density_bar, physics/observables.jl:1-22)."""
+    NE, Nk, Nb, _ = GL.shape
+    out = np.zeros((Nb, Nb), dtype=np.complex128)
+    W = np.outer(np.asarray(wE), np.asarray(wk))
+    for b in range(Nb):
+        for a in range(Nb):
+            out[a, b] = np.sum(W * GL[:, :, a, b])
+    return out
+
+
+def poisson_solve(st, nbar):
+    """solve_periodic_poisson (numerics/reference/poisson.jl:41-65) with
+    build_poisson_matrix (:12-28): returns (U, zeta, r_P, neutrality)."""
+    N = len(st.x)
+    dx = st.wx[0]
+    e = np.asarray(st.eps_r, dtype=np.float64)
+    L = np.zeros((N, N))
+    for g in range(N):
+        gp, gm = (g + 1) % N, (g - 1) % N
+        fg = 2 * e[g] * e[gp] / (e[g] + e[gp])
+        fm = 2 * e[gm] * e[g] / (e[gm] + e[g])
+        L[g, g] = (fm + fg) / dx ** 2
+        L[g, gm] = -fm / dx ** 2
+        L[g, gp] = -fg / dx ** 2
+    ND2D = float(np.dot(st.wx, st.ND))
+    neutrality = abs(float(np.dot(st.wx, st.ND - nbar))) / ND2D
+    b = -st.lambda_P * (st.ND - nbar)
+    sP = float(np.max(np.sum(np.abs(L), axis=1)))
+    v = np.full(N, 1 / math.sqrt(N))
+    B = np.block([[L / sP, v[:, None]], [v[None, :], np.zeros((1, 1))]])
+    ans = np.linalg.solve(B, np.r_[b / sP, 0.0])
+    U = ans[:N]
+    rP = float(np.linalg.norm(L @ U - b) / (np.linalg.norm(b) + st.lambda_P * 1e-14))
+    return U, float(ans[N]), rP, neutrality
+
+
+def outer_loop(problem, st, max_poisson, inner_iterations, alpha_P=0.3):
+    """The outer loop of solve_production (production_solver.jl:993-1151)
+    with a fixed inner iteration count, every inner solve warm-started from
+    the previous terminal state."""
+    import dataclasses as _dc
+
+    Nz = len(st.x)
+    U = np.zeros(Nz)
+    rows = []
+    state = None
+    nprev = Jprev = pprev = None
+    ND2D, Lp = float(np.dot(st.wx, st.ND)), float(np.sum(st.wx))
+    for mu in range(1, max_poisson + 1):
+        Nb = st.H0.shape[0]
+        static = st.H0 - st.F * (st.Z - st.z0 * np.eye(Nb)) + st.Phi.conj().T @ np.diag(U) @ st.Phi
+        h = np.zeros((len(st.kappa), Nb, Nb), dtype=np.complex128, order="F")
+        for m, k in enumerate(st.kappa):
+            h[m] = static + st.Cbar * k * k * st.Minv
+        pr = _dc.replace(problem, h=h)
+        hist, state = scba(pr, inner_iterations, state=state, keep_state=True, terminal=True)
+        green = state["green"]
+        rho = density_matrix(green["GL"], pr.wE, pr.wk)
+        nbar = pr.gs / (2 * math.pi) * np.real(-1j * np.einsum("ga,ab,gb->g", st.chi, rho, np.conj(st.chi)))
+        cand, zeta, rP, rneutral = poisson_solve(st, nbar)
+        rU = float(np.max(np.abs(cand - U)))
+        rn = math.inf if nprev is None else float(math.sqrt(np.sum(st.wx * (nbar - nprev) ** 2)) / (ND2D / math.sqrt(Lp)))
+        jp = current(pr, state["plus"][2], state["plus"][1], green["GL"], green["GG"])
+        jm = current(pr, state["minus"][2], state["minus"][1], green["GL"], green["GG"])
+        rJ = abs(jp + jm) / max(abs(jp), abs(jm), 1e-12)
+        J = jp * pr.J0
+        pops = hist[-1]["populations"]
+        rJc = math.inf if Jprev is None else abs(J - Jprev) / max(abs(J), abs(Jprev), 1e-12)
+        rpop = math.inf if pprev is None else float(np.linalg.norm(pops - pprev) / (np.linalg.norm(pops) + 1e-14))
+        rows.append(dict(mu=mu, r_P=rP, r_U=rU, r_n=rn, r_neutral=rneutral, r_J=rJ, r_Jchange=rJc,
+                         r_population=rpop, zeta=zeta, J=J, populations=pops, n=nbar, inner=hist))
+        U = (1 - alpha_P) * U + alpha_P * cand
+        nprev, Jprev, pprev = nbar, J, pops
+    return rows
+
+
+# --------------------------------------------------------------------------
 # Anderson mixing (numerics/optimized/production_mixing.jl:1-317)
 # --------------------------------------------------------------------------
 _EPS = float(np.finfo(np.float64).eps)
@@ -717,9 +798,11 @@ class AndersonMixer:
         return out
 
 
-def scba(problem, iterations, verify=True, state=None, keep_state=False):
+def scba(problem, iterations, verify=True, state=None, keep_state=False, terminal=False):
     """Run `iterations` SCBA steps (solve_scba, scba.jl:142-354, with the
-    production operators).  Returns (history, state)."""
+    production operators).  Returns (history, state).  With `terminal` the
+    last iteration is the solver's terminal row: its families stay unmixed
+    (the state a warm-started solve continues from)."""
     plans = make_plans(problem)
     if state is None:
         green, mu = seed_green(problem)
@@ -761,6 +844,8 @@ def scba(problem, iterations, verify=True, state=None, keep_state=False):
                    lambda_change=math.nan if not history else lam - history[-1]["lam"], **res)
         history.append(row)
         a = problem.alpha
+        if terminal and nu == iterations:
+            break
         if mixer is not None:
             names = [m.name for m in problem.mechanisms]
             st = [scattering[n] for n in names] + [plus, minus]

@@ -140,6 +140,7 @@ int scba_green_state(ScbaCtx* c, void* A, double* kappa, double* scale);
 int scba_witness(ScbaCtx* c, double* out12);
 int scba_retarget(ScbaCtx* c, double Ep, double N_LO, double kBT, const void* h, const double* q);
 int scba_mixer_info(ScbaCtx* c, qcl_anderson_info* out);
+int scba_density_matrix(ScbaCtx* c, void* out);
 
 static int shift_plan_dev(int NE, const double* eps, double delta, DevBuf& l, DevBuf& r, DevBuf& th, DevBuf& v,
                           ShiftPlanDev* out) {
@@ -733,6 +734,39 @@ int qcl_anderson_guard(int precision, int NE, int Nk, int Nb, int nfam, const vo
   *first_failure = failed ? (long long)(h.guard_key >> 3) : 0;
   *code = failed ? (int)(h.guard_key & 7ull) : 0;
   return QCL_OK;
+}
+
+int qcl_scba_density_matrix(qcl_scba* ctx, void* rho) {
+  if (!ctx || !rho) {
+    set_last_error("ctx and rho are required");
+    return QCL_ARG;
+  }
+  return scba_density_matrix((ScbaCtx*)ctx, rho);
+}
+
+int qcl_density_matrix(int precision, int NE, int Nk, int Nb, const double* wE, const double* wk, const void* GL,
+                       void* rho) {
+  if (int s = check_precision(precision)) return s;
+  if (NE <= 0 || Nk <= 0 || Nb <= 0) {
+    set_last_error("density_matrix: non-positive dimension (%d,%d,%d)", NE, Nk, Nb);
+    return QCL_DIM;
+  }
+  if (!wE || !wk || !GL || !rho) {
+    set_last_error("density_matrix: wE, wk, GL and rho are required");
+    return QCL_ARG;
+  }
+  const int sp = precision == QCL_MIXED ? QCL_C64 : precision;
+  DevBuf dwE, dwk, dG, dr;
+  int s;
+  if ((s = dwE.upload(wE, NE * sizeof(double)))) return s;
+  if ((s = dwk.upload(wk, Nk * sizeof(double)))) return s;
+  if ((s = dG.upload(GL, field_elems(NE, Nk, Nb) * cbytes(sp)))) return s;
+  if ((s = dr.alloc(2 * (size_t)Nb * Nb * sizeof(double)))) return s;
+  if ((s = launch_density_matrix(sp, NE, Nk, Nb, dG.p, (const double*)dwE.p, (const double*)dwk.p, (double*)dr.p,
+                                 0)))
+    return s;
+  QCL_CUDA_CHECK(cudaDeviceSynchronize());
+  return dr.download(rho);
 }
 
 int qcl_scba_mixer_info(qcl_scba* ctx, qcl_anderson_info* info) {

@@ -16,6 +16,8 @@ int launch_weighted_trace(int NE, int Nk, const void* tr, const double* wE, cons
                           double* out, cudaStream_t st);
 int launch_paired_coefficients(const double* trL, const double* trG, int gs, double target, double* coeffs,
                                int* status, cudaStream_t st, double realness_limit = 1e-10, int scalar = 0);
+int launch_density_matrix(int precision, int NE, int Nk, int N, const void* GL, const double* wE, const double* wk,
+                          double* out, cudaStream_t st);
 int launch_scalar_lesser(int precision, int NE, int Nk, int N, const void* GR, void* GL, void* GG,
                          const double* coeffs, cudaStream_t st);
 int launch_normalize_pair(int precision, size_t n, void* GL, void* GG, const double* coeffs, cudaStream_t st);

@@ -216,6 +216,42 @@ int launch_scalar_lesser(int precision, int NE, int Nk, int N, const void* GR, v
 }
 
 // ---------------------------------------------------------------------------
+// Integrated coherence matrix rho_ab = sum_{m,e} wE_e wk_m G<_{e,m,a,b}
+// (the `integrated` array of _electron_density_bar, physics/observables.jl:
+// 1-22): one CTA per (a, b), whose N_E N_k entries are contiguous in the
+// E-fastest layout; fixed-order sum.
+// ---------------------------------------------------------------------------
+template <typename R>
+__global__ void __launch_bounds__(REDUCE_THREADS)
+    density_matrix_kernel(int NE, int Nk, const Cx<R>* __restrict__ GL, const double* __restrict__ wE,
+                          const double* __restrict__ wk, double* out) {
+  const long long blocks = (long long)NE * Nk;
+  const Cx<R>* g = GL + (size_t)blockIdx.x * blocks;
+  double v[2] = {0, 0};
+  for (long long i = threadIdx.x; i < blocks; i += blockDim.x) {
+    const double w = wE[i % NE] * wk[i / NE];
+    const Cx<R> z = g[i];
+    v[0] += w * (double)z.x;
+    v[1] += w * (double)z.y;
+  }
+  block_sum<2>(v);
+  if (threadIdx.x == 0) {
+    out[2 * blockIdx.x] = v[0];
+    out[2 * blockIdx.x + 1] = v[1];
+  }
+}
+
+int launch_density_matrix(int precision, int NE, int Nk, int N, const void* GL, const double* wE, const double* wk,
+                          double* out, cudaStream_t st) {
+  if (precision == QCL_C128)
+    density_matrix_kernel<double><<<N * N, REDUCE_THREADS, 0, st>>>(NE, Nk, (const Cx<double>*)GL, wE, wk, out);
+  else
+    density_matrix_kernel<float><<<N * N, REDUCE_THREADS, 0, st>>>(NE, Nk, (const Cx<float>*)GL, wE, wk, out);
+  QCL_LAUNCH_CHECK("density_matrix");
+  return QCL_OK;
+}
+
+// ---------------------------------------------------------------------------
 // Sum of up to 8 fields (component-wise totals, _total_family_production,
 // production_operators.jl:1447-1473): out = sum_j src[j].
 // ---------------------------------------------------------------------------

@@ -956,6 +956,28 @@ int scba_retarget(ScbaCtx* c, double Ep, double N_LO, double kBT, const void* h,
   return QCL_OK;
 }
 
+// rho_ab = sum wE wk G<_ab of the last Dyson solve (the electron-density
+// coherences the outer Poisson loop projects on the position grid,
+// _electron_density_bar, physics/observables.jl:1-22).  out: N x N complex128.
+int scba_density_matrix(ScbaCtx* c, void* out) {
+  if (!c->have_green) {
+    set_last_error("density_matrix: no Green state yet (call seed or step first)");
+    return QCL_ARG;
+  }
+  const int sp = c->precision == QCL_MIXED ? QCL_C64 : c->precision;
+  double* d = nullptr;
+  int s = dalloc((void**)&d, 2 * (size_t)c->N * c->N * sizeof(double));
+  if (s) return s;
+  s = launch_density_matrix(sp, c->NE, c->Nk, c->N, c->GL, c->wE, c->wk, d, c->st);
+  if (!s) {
+    cudaError_t e = cudaMemcpyAsync(out, d, 2 * (size_t)c->N * c->N * sizeof(double), cudaMemcpyDeviceToHost, c->st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->st);
+    if (e != cudaSuccess) s = cuda_status(e, "density_matrix download");
+  }
+  cudaFree(d);
+  return s;
+}
+
 // Mixer diagnostics of the last step (the SolverMetric list of _anderson_mix!,
 // production_mixing.jl:283-298).
 int scba_mixer_info(ScbaCtx* c, qcl_anderson_info* out) {

@@ -147,6 +147,8 @@ def _declare(l):
         "qcl_scba_retarget": (I, [P, D, D, D, P, P]),
         "qcl_scba_mixer_info": (I, [P, P]),
         "qcl_anderson_guard": (I, [I, I, I, I, I, P, P, P]),
+        "qcl_scba_density_matrix": (I, [P, P]),
+        "qcl_density_matrix": (I, [I, I, I, I, P, P, P, P]),
     }
     for name, (res, args) in sig.items():
         if hasattr(l, name):

@@ -198,6 +198,13 @@ class ProductionSCBA:
         self.problem = new
         return new
 
+    def density_matrix(self):
+        """rho_ab = sum wE wk G<_ab of the last Dyson solve (N_b x N_b)."""
+        n = self.problem.Nb
+        rho = np.zeros((n, n), dtype=np.complex128, order="F")
+        check(lib().qcl_scba_density_matrix(self._h, ctypes.c_void_p(rho.ctypes.data)))
+        return rho
+
     def mixer_info(self):
         """Anderson mixer diagnostics of the last step."""
         info = AndersonInfo()

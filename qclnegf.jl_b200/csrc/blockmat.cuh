@@ -129,6 +129,83 @@ __device__ __forceinline__ void team_matmul(const Cx<RS>* A, const Cx<RS>* B, Cx
   team_store_regs<RS, RM, NP>(C, acc, tt);
 }
 
+// ---------------------------------------------------------------------------
+// FP64 tensor-core (DMMA, mma.sync m8n8k4 f64) version of the team matmul for
+// complex128 tiles.  The NP x NP product is cut into (NP/8)^2 tiles of 8 x 8;
+// warp w of the team owns tile rows w, w + NW, ...  Each complex product is
+// four real DMMAs (Re C += Ar Br - Ai Bi, Im C += Ar Bi + Ai Br), and K
+// advances by 4 with entries past N read as zero.  Fragment layouts (PTX
+// m8n8k4 .f64): A lane l holds (l/4, l%4), B holds (l%4, l/4), C holds
+// (l/4, 2 (l%4) + i).  One DMMA issue does the 256 FMAs of 8 DFMA issues
+// per lane.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void dmma_f64(double (&c)[2], double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+               : "+d"(c[0]), "+d"(c[1])
+               : "d"(a), "d"(b));
+}
+
+template <int NP, int TT> struct DmmaTile {
+  static constexpr int NT = NP / 8, NW = TT / 32, RPW = (NT + NW - 1) / NW;
+  double re[RPW][NT][2], im[RPW][NT][2];
+};
+
+template <int NP, int TT>
+__device__ __forceinline__ void team_matmul_dmma(const Cx<double>* A, const Cx<double>* B, DmmaTile<NP, TT>& acc,
+                                                 int N, int tt, bool adjB) {
+  constexpr int NT = DmmaTile<NP, TT>::NT, NW = DmmaTile<NP, TT>::NW, RPW = DmmaTile<NP, TT>::RPW;
+  const int warp = tt >> 5, lane = tt & 31, lr = lane >> 2, lc = lane & 3;
+#pragma unroll
+  for (int r = 0; r < RPW; ++r)
+#pragma unroll
+    for (int j = 0; j < NT; ++j) acc.re[r][j][0] = acc.re[r][j][1] = acc.im[r][j][0] = acc.im[r][j][1] = 0.0;
+  for (int k0 = 0; k0 < N; k0 += 4) {
+    const int k = k0 + lc;
+    const bool kin = k < N;
+    double ar[RPW], ai[RPW], nai[RPW], br[NT], bi[NT];
+#pragma unroll
+    for (int r = 0; r < RPW; ++r) {
+      const bool rin = warp + r * NW < NT;  // warp-uniform
+      const Cx<double> a = kin && rin ? A[sw<NP>((warp + r * NW) * 8 + lr, k)] : cx<double>(0, 0);
+      ar[r] = a.x;
+      ai[r] = a.y;
+      nai[r] = -a.y;
+    }
+#pragma unroll
+    for (int j = 0; j < NT; ++j) {
+      Cx<double> b = cx<double>(0, 0);
+      if (kin) b = adjB ? conj(B[sw<NP>(j * 8 + lr, k)]) : B[sw<NP>(k, j * 8 + lr)];
+      br[j] = b.x;
+      bi[j] = b.y;
+    }
+#pragma unroll
+    for (int r = 0; r < RPW; ++r)
+#pragma unroll
+      for (int j = 0; j < NT; ++j) {
+        if (RPW * NW != NT && warp + r * NW >= NT) continue;  // warp-uniform: no tile row here
+        dmma_f64(acc.re[r][j], ar[r], br[j]);
+        dmma_f64(acc.re[r][j], nai[r], bi[j]);
+        dmma_f64(acc.im[r][j], ar[r], bi[j]);
+        dmma_f64(acc.im[r][j], ai[r], br[j]);
+      }
+  }
+}
+
+template <int NP, int TT>
+__device__ __forceinline__ void team_store_dmma(Cx<double>* C, const DmmaTile<NP, TT>& acc, int tt) {
+  constexpr int NT = DmmaTile<NP, TT>::NT, NW = DmmaTile<NP, TT>::NW, RPW = DmmaTile<NP, TT>::RPW;
+  const int warp = tt >> 5, lane = tt & 31, lr = lane >> 2, lc = lane & 3;
+#pragma unroll
+  for (int r = 0; r < RPW; ++r) {
+    if (RPW * NW != NT && warp + r * NW >= NT) continue;
+#pragma unroll
+    for (int j = 0; j < NT; ++j)
+#pragma unroll
+      for (int i = 0; i < 2; ++i)
+        C[sw<NP>((warp + r * NW) * 8 + lr, j * 8 + 2 * lc + i)] = cx<double>(acc.re[r][j][i], acc.im[r][j][i]);
+  }
+}
+
 // Cooperative, coalesced copy of BPC consecutive-energy blocks between a
 // global field (E fastest) and the per-block shared matrices.
 template <typename RG_, typename RS, int NP, int BPC>

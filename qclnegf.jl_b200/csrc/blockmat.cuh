@@ -120,14 +120,6 @@ __device__ __forceinline__ void team_store_regs(Cx<RS>* C, const MatTile<RM, NP>
     for (int u = 0; u < TC; ++u) C[sw<NP>(rg * TR + t, cg * TC + u)] = cvt<RS>(acc.v[t][u]);
 }
 
-// C = A * B (adjB = false) or C = A * B^H (adjB = true); C distinct from A, B.
-template <typename RS, typename RM, int NP>
-__device__ __forceinline__ void team_matmul(const Cx<RS>* A, const Cx<RS>* B, Cx<RS>* C, int N, int tt,
-                                            bool adjB) {
-  MatTile<RM, NP> acc;
-  team_matmul_regs<RS, RM, NP>(A, B, acc, N, tt, adjB);
-  team_store_regs<RS, RM, NP>(C, acc, tt);
-}
 
 // ---------------------------------------------------------------------------
 // FP64 tensor-core (DMMA, mma.sync m8n8k4 f64) version of the team matmul for
@@ -203,6 +195,22 @@ __device__ __forceinline__ void team_store_dmma(Cx<double>* C, const DmmaTile<NP
 #pragma unroll
       for (int i = 0; i < 2; ++i)
         C[sw<NP>((warp + r * NW) * 8 + lr, j * 8 + 2 * lc + i)] = cx<double>(acc.re[r][j][i], acc.im[r][j][i]);
+  }
+}
+
+// C = A * B (adjB = false) or C = A * B^H (adjB = true); C distinct from A, B.
+// complex128 tiles go through the FP64 tensor path (DMMA).
+template <typename RS, typename RM, int NP>
+__device__ __forceinline__ void team_matmul(const Cx<RS>* A, const Cx<RS>* B, Cx<RS>* C, int N, int tt,
+                                            bool adjB) {
+  if constexpr (sizeof(RS) == 8 && sizeof(RM) == 8) {
+    DmmaTile<NP, Tile<NP>::TT> acc;
+    team_matmul_dmma<NP, Tile<NP>::TT>((const Cx<double>*)A, (const Cx<double>*)B, acc, N, tt, adjB);
+    team_store_dmma<NP, Tile<NP>::TT>((Cx<double>*)C, acc, tt);
+  } else {
+    MatTile<RM, NP> acc;
+    team_matmul_regs<RS, RM, NP>(A, B, acc, N, tt, adjB);
+    team_store_regs<RS, RM, NP>(C, acc, tt);
   }
 }
 

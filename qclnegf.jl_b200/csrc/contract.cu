@@ -59,6 +59,54 @@ int launch_shift(int precision, int NE, long long ncols, const ShiftPlanDev& pla
   return QCL_OK;
 }
 
+// Y = a X(eps + d1) + b X(eps + d2): two shifts of the same field combined in
+// one pass (the linear combination the thermal-LO self-energy contracts,
+// production_operators.jl:1107-1163, formed before the contraction).
+template <typename R>
+__global__ void shift_pair_kernel(int NE, long long ncols, ShiftPlanDev p1, ShiftPlanDev p2, double a, double b,
+                                  const Cx<R>* __restrict__ X, Cx<R>* __restrict__ Y) {
+  const long long n = (long long)NE * ncols;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const int e = (int)(i % NE);
+    const long long base = i - e;
+    double vx = 0, vy = 0;
+#pragma unroll
+    for (int s = 0; s < 2; ++s) {
+      const ShiftPlanDev& pl = s == 0 ? p1 : p2;
+      const double c = s == 0 ? a : b;
+      if (!pl.valid[e]) continue;
+      const int l = pl.left[e], r = pl.right[e];
+      const double th = pl.theta[e];
+      double ux, uy;
+      if (l == r || th == 0.0) {
+        const Cx<R> q = X[base + l];
+        ux = q.x;
+        uy = q.y;
+      } else {
+        const Cx<R> ql = X[base + l], qr = X[base + r];
+        ux = (1 - th) * ql.x + th * qr.x;
+        uy = (1 - th) * ql.y + th * qr.y;
+      }
+      vx += c * ux;
+      vy += c * uy;
+    }
+    Y[i] = cx<R>((R)vx, (R)vy);
+  }
+}
+
+int launch_shift_pair(int precision, int NE, long long ncols, const ShiftPlanDev& p1, const ShiftPlanDev& p2, double a,
+                      double b, const void* X, void* Y, cudaStream_t st) {
+  const long long n = (long long)NE * ncols;
+  if (precision == QCL_C128)
+    shift_pair_kernel<double><<<grid_cap(n, 256), 256, 0, st>>>(NE, ncols, p1, p2, a, b, (const Cx<double>*)X,
+                                                               (Cx<double>*)Y);
+  else
+    shift_pair_kernel<float><<<grid_cap(n, 256), 256, 0, st>>>(NE, ncols, p1, p2, a, b, (const Cx<float>*)X,
+                                                              (Cx<float>*)Y);
+  QCL_LAUNCH_CHECK("shift_pair_kernel");
+  return QCL_OK;
+}
+
 // build_shift_plan (production_cache.jl:258-290), 0-based, on the host.
 int build_shift_plan_host(int NE, const double* eps, double delta, int* left, int* right, double* theta,
                           unsigned char* valid) {

@@ -89,6 +89,8 @@ int build_shift_plan_host(int NE, const double* eps, double delta, int* left, in
                           unsigned char* valid);
 int launch_shift(int precision, int NE, long long ncols, const ShiftPlanDev& plan, const void* X, void* Y,
                  cudaStream_t st);
+int launch_shift_pair(int precision, int NE, long long ncols, const ShiftPlanDev& p1, const ShiftPlanDev& p2, double a,
+                      double b, const void* X, void* Y, cudaStream_t st);
 
 // Device view of a factorised kernel operator (arrays in the field precision).
 struct KernelOpDev {

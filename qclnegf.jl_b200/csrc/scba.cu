@@ -438,20 +438,19 @@ static int scattering_candidates(ScbaCtx* c, const void* GR, const void* GL, con
     void* SL = field_of(dst, i, 1);
     void* SG = field_of(dst, i, 2);
     if (m.is_LO) {
-      // _production_lo_contraction, thermal branch (production_operators.jl:1045-1163)
+      // _production_lo_contraction, thermal branch (production_operators.jl:1045-1163):
+      //   Sigma< = (N+1) K[G<(E+hw)] + N K[G<(E-hw)],  Sigma> = (N+1) K[G>(E-hw)] + N K[G>(E+hw)].
+      // K is linear, so each is one contraction of the combined shifted field,
+      // K[(N+1) G(E+-hw) + N G(E-+hw)]: two dense maps instead of four.
       const double n = c->N_LO;
-      if ((s = launch_shift(cp, c->NE, ncols, c->shift[2].view(), GL, c->tmp, c->st))) return s;
-      if ((s = launch_contraction(cp, op, c->NE, c->Nk, c->N, c->wk, c->tmp, SL, (n + 1) * m.q, 0.0, c->cwork, c->st)))
+      if ((s = launch_shift_pair(cp, c->NE, ncols, c->shift[2].view(), c->shift[3].view(), n + 1, n, GL, c->tmp,
+                                 c->st)))
         return s;
-      if ((s = launch_shift(cp, c->NE, ncols, c->shift[3].view(), GL, c->tmp, c->st))) return s;
-      if ((s = launch_contraction(cp, op, c->NE, c->Nk, c->N, c->wk, c->tmp, SL, n * m.q, 1.0, c->cwork, c->st)))
+      if ((s = launch_contraction(cp, op, c->NE, c->Nk, c->N, c->wk, c->tmp, SL, m.q, 0.0, c->cwork, c->st))) return s;
+      if ((s = launch_shift_pair(cp, c->NE, ncols, c->shift[3].view(), c->shift[2].view(), n + 1, n, GG, c->tmp,
+                                 c->st)))
         return s;
-      if ((s = launch_shift(cp, c->NE, ncols, c->shift[3].view(), GG, c->tmp, c->st))) return s;
-      if ((s = launch_contraction(cp, op, c->NE, c->Nk, c->N, c->wk, c->tmp, SG, (n + 1) * m.q, 0.0, c->cwork, c->st)))
-        return s;
-      if ((s = launch_shift(cp, c->NE, ncols, c->shift[2].view(), GG, c->tmp, c->st))) return s;
-      if ((s = launch_contraction(cp, op, c->NE, c->Nk, c->N, c->wk, c->tmp, SG, n * m.q, 1.0, c->cwork, c->st)))
-        return s;
+      if ((s = launch_contraction(cp, op, c->NE, c->Nk, c->N, c->wk, c->tmp, SG, m.q, 0.0, c->cwork, c->st))) return s;
     } else {
       if ((s = launch_contraction(cp, op, c->NE, c->Nk, c->N, c->wk, GL, SL, m.q, 0.0, c->cwork, c->st))) return s;
       if ((s = launch_contraction(cp, op, c->NE, c->Nk, c->N, c->wk, GG, SG, m.q, 0.0, c->cwork, c->st))) return s;

@@ -181,6 +181,30 @@ int qcl_condition_number(int precision, int NE, int Nk, int Nb, const double* ep
  * (production_operators.jl:1387-1415). */
 int qcl_spectral_function(int precision, int NE, int Nk, int Nb, const void* GR, void* A);
 
+/* Dense kernel operators assembled on the device from angular node weights.
+ * The reference's momentum-dependent kernels are angular averages over
+ * phi_r = 2 pi (r-1) / N_phi of a transfer-momentum kernel C(q) (the exact
+ * LO phonon kernel, lo_phonon_kernel, numerics/reference/kernels.jl:321-356;
+ * the tabulated lookup of numerics/optimized/kernels.jl:205-217, 303-320),
+ * which makes K(m,m') = sum_t W[(m,m'),t] X_t for node weights W (host-formed
+ * angular means, N_k^2 x T, column-major, (m,m') index m + N_k m') and node
+ * tensors X_t:
+ *   QCL_ASSEMBLE_RANK1: X_t = F_t (x) conj(F_t), X = F (T x N_b^2 complex128,
+ *                       F[t + T (a + N_b c)]);
+ *   QCL_ASSEMBLE_TABLE: X_t the (N_b^2 x N_b^2) pair covariance at table node t,
+ *                       X[(a + N_b c) + N_b^2 (b + N_b d) + N_b^4 t].
+ * Output: the production dense matrix (rows (m,a,b), columns (m',c,d);
+ * _production_kernel, production_cache.jl:400-405) normalised by
+ * qK = max |K| (build_kernels, kernels.jl:393-403); a zero or non-finite
+ * kernel is left unnormalised and reported through qK. */
+#define QCL_ASSEMBLE_RANK1 0
+#define QCL_ASSEMBLE_TABLE 1
+int qcl_assemble_kernel(int form, int Nk, int Nb, int T, const double* W, const void* X, void* matrix, double* qK);
+/* Device-array variant on `stream`; work holds (296 + 1) doubles and receives
+ * qK in its last entry. */
+int qcl_dev_assemble_kernel(void* stream, int form, int Nk, int Nb, int T, const double* W, const void* X,
+                            void* matrix, double* work);
+
 /* Integrated coherences rho_ab = sum_{m,e} wE_e wk_m G<_{e,m,a,b} (Nb x Nb,
  * complex128, column-major): the `integrated` matrix of
  * _electron_density_bar (physics/observables.jl:1-22) from which the outer
@@ -333,7 +357,9 @@ typedef struct qcl_scba_row {
 typedef struct qcl_scba qcl_scba;
 
 /* Allocates the device state and uploads grids, h, T+-, shift plans and
- * kernel operators (build_production_cache, production_cache.jl:759-840). */
+ * kernel operators (build_production_cache, production_cache.jl:759-840).
+ * The operator arrays of `mechanisms` may be host or device memory (e.g. a
+ * dense operator from qcl_dev_assemble_kernel); they are copied. */
 int qcl_scba_create(const qcl_scba_problem* problem, const qcl_mechanism* mechanisms, qcl_scba** out);
 void qcl_scba_destroy(qcl_scba* ctx);
 /* Equilibrium seed + initial candidates (_seed_green_production,

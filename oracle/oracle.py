@@ -565,6 +565,85 @@ def make_plans(problem):
 
 
 # --------------------------------------------------------------------------
+# Kernel builders (numerics/reference/kernels.jl, numerics/optimized/kernels.jl)
+# --------------------------------------------------------------------------
+def lo_kernel_literal(F, qz, wqz, kappa, Nphi, qscreen, prefactor, L0=1.0):
+    """lo_phonon_kernel (kernels.jl:321-356) with _angular_average_kernel
+    (:5-19): K[m,m',a,c,d,b] = prefactor/N_phi sum_phi sum_h f_h(q) F[h,a,c]
+    conj(F[h,b,d]), f_h = wqz_h L0 / (2 pi (q^2 + qz_h^2 + qs^2))."""
+    Nq, Nb, _ = F.shape
+    Nk = len(kappa)
+    K = np.zeros((Nk, Nk, Nb, Nb, Nb, Nb), dtype=np.complex128)
+    outer = [np.einsum("ac,bd->acdb", F[h], np.conj(F[h])) for h in range(Nq)]
+    for m in range(Nk):
+        for mp in range(Nk):
+            acc = np.zeros((Nb, Nb, Nb, Nb), dtype=np.complex128)
+            for r in range(Nphi):
+                phi = 2 * math.pi * r / Nphi
+                q = math.sqrt(max(kappa[m] ** 2 + kappa[mp] ** 2 - 2 * kappa[m] * kappa[mp] * math.cos(phi), 0.0))
+                Ksi = np.zeros_like(acc)
+                for h in range(Nq):
+                    Ksi += wqz[h] * L0 / (2 * math.pi * (q * q + qz[h] ** 2 + qscreen ** 2)) * outer[h]
+                acc += prefactor * Ksi
+            K[m, mp] = acc / Nphi
+    return K
+
+
+def lookup_block(nodes, values, q):
+    """_lookup_block (numerics/optimized/kernels.jl:205-217)."""
+    qlo, qhi = nodes[0], nodes[-1]
+    tol = 64 * _EPS * max(abs(qlo), abs(qhi), 1.0)
+    if not (qlo - tol <= q <= qhi + tol):
+        raise ValueError("lookup query lies outside the tabulated interval")
+    qc = min(max(q, qlo), qhi)
+    if qc == qhi:
+        return values[-1]
+    j = min(max(int(np.searchsorted(nodes, qc, side="right")) - 1, 0), len(nodes) - 2)
+    th = (qc - nodes[j]) / (nodes[j + 1] - nodes[j])
+    return (1 - th) * values[j] + th * values[j + 1]
+
+
+def assemble_lookup_kernel(nodes, values, kappa, Nphi):
+    """_assemble_lookup_kernel (numerics/optimized/kernels.jl:303-320):
+    values[t] are (a,c,d,b) blocks."""
+    Nk = len(kappa)
+    Nb = values[0].shape[0]
+    K = np.zeros((Nk, Nk, Nb, Nb, Nb, Nb), dtype=np.complex128)
+    for m in range(Nk):
+        for mp in range(Nk):
+            acc = np.zeros((Nb,) * 4, dtype=np.complex128)
+            for r in range(Nphi):
+                phi = 2 * math.pi * r / Nphi
+                q = math.sqrt(max(kappa[m] ** 2 + kappa[mp] ** 2 - 2 * kappa[m] * kappa[mp] * math.cos(phi), 0.0))
+                acc = acc + lookup_block(nodes, values, q)
+            K[m, mp] = acc / Nphi
+    return K
+
+
+def impurity_block_literal(q, chi, x, wx, donor_weights, q_s, pre):
+    """kernel_at_q of impurity_kernel (kernels.jl:117-141) as an (a,c,d,b)
+    block: sum over donor cells of w_D V[a,c] conj(V[b,d]),
+    V[a,c] = pre/(q + q_s) sum_g wx conj(chi_ga) exp(-q |x_g - x_D|) chi_gc."""
+    Nb = chi.shape[1]
+    Ksi = np.zeros((Nb,) * 4, dtype=np.complex128)
+    for D in range(len(x)):
+        if donor_weights[D] == 0:
+            continue
+        V = np.zeros((Nb, Nb), dtype=np.complex128)
+        for a in range(Nb):
+            for c in range(Nb):
+                V[a, c] = pre / (q + q_s) * np.sum(wx * np.conj(chi[:, a]) * np.exp(-q * np.abs(x - x[D])) * chi[:, c])
+        Ksi += donor_weights[D] * np.einsum("ac,bd->acdb", V, np.conj(V))
+    return Ksi
+
+
+def normalize_kernel(K):
+    """build_kernels scaling (kernels.jl:393-403): (K / q, q), q = max |K|."""
+    q = float(np.max(np.abs(K)))
+    return K / q, q
+
+
+# --------------------------------------------------------------------------
 # Outer Hartree-Poisson loop (numerics/optimized/production_solver.jl:993-1151)
 # --------------------------------------------------------------------------
 def density_matrix(GL, wE, wk):

@@ -769,6 +769,48 @@ int qcl_density_matrix(int precision, int NE, int Nk, int Nb, const double* wE, 
   return dr.download(rho);
 }
 
+static int check_assembly(int form, int Nk, int Nb, int T) {
+  if (form != QCL_ASSEMBLE_RANK1 && form != QCL_ASSEMBLE_TABLE) {
+    set_last_error("kernel assembly: unknown form %d", form);
+    return QCL_ARG;
+  }
+  if (Nk <= 0 || Nb <= 0 || T <= 0) {
+    set_last_error("kernel assembly: non-positive dimension (Nk=%d, Nb=%d, T=%d)", Nk, Nb, T);
+    return QCL_DIM;
+  }
+  return QCL_OK;
+}
+
+int qcl_dev_assemble_kernel(void* stream, int form, int Nk, int Nb, int T, const double* W, const void* X,
+                            void* matrix, double* work) {
+  if (int s = check_assembly(form, Nk, Nb, T)) return s;
+  if (!W || !X || !matrix || !work) {
+    set_last_error("kernel assembly: W, X, matrix and work are required");
+    return QCL_ARG;
+  }
+  return launch_assemble_kernel(form, Nk, Nb, T, W, X, matrix, work, (cudaStream_t)stream);
+}
+
+int qcl_assemble_kernel(int form, int Nk, int Nb, int T, const double* W, const void* X, void* matrix, double* qK) {
+  if (int s = check_assembly(form, Nk, Nb, T)) return s;
+  if (!W || !X || !matrix || !qK) {
+    set_last_error("kernel assembly: W, X, matrix and qK are required");
+    return QCL_ARG;
+  }
+  const size_t N2 = (size_t)Nb * Nb, Nc = (size_t)Nk * N2;
+  const size_t xelems = form == QCL_ASSEMBLE_RANK1 ? (size_t)T * N2 : (size_t)T * N2 * N2;
+  DevBuf dW, dX, dM, work;
+  int s;
+  if ((s = dW.upload(W, (size_t)Nk * Nk * T * sizeof(double)))) return s;
+  if ((s = dX.upload(X, xelems * 16))) return s;
+  if ((s = dM.alloc(Nc * Nc * 16))) return s;
+  if ((s = work.alloc(assemble_work_doubles() * sizeof(double)))) return s;
+  if ((s = launch_assemble_kernel(form, Nk, Nb, T, (const double*)dW.p, dX.p, dM.p, (double*)work.p, 0))) return s;
+  QCL_CUDA_CHECK(cudaDeviceSynchronize());
+  QCL_CUDA_CHECK(cudaMemcpy(qK, (double*)work.p + assemble_work_doubles() - 1, sizeof(double), cudaMemcpyDeviceToHost));
+  return dM.download(matrix);
+}
+
 int qcl_scba_mixer_info(qcl_scba* ctx, qcl_anderson_info* info) {
   if (!ctx || !info) {
     set_last_error("ctx and info are required");

@@ -62,6 +62,10 @@ int launch_anderson_mix(int precision, size_t n, void* const* out, int nf, const
 int launch_anderson_after_guard(AndersonMeta* m, int pass, int* status, cudaStream_t st);
 int launch_anderson_guard(int precision, int NE, int Nk, int N, void* const* fields, int nfam, AndersonMeta* m,
                           int pass, cudaStream_t st);
+// dense kernel operators from angular node weights (kbuild.cu)
+size_t assemble_work_doubles();
+int launch_assemble_kernel(int form, int Nk, int Nb, int T, const double* W, const void* X, void* out, double* work,
+                           cudaStream_t st);
 // scattering-model switches (model.cu)
 int launch_retarded_drop(int precision, size_t n, const void* SL, const void* SG, void* SR, cudaStream_t st);
 int launch_scattering_model(int precision, int NE, int Nk, int N, const double* wk, double norm, int diagonal,

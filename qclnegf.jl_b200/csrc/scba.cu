@@ -137,10 +137,12 @@ static int dalloc(void** p, size_t bytes) {
 // Uploads go on the context's stream: the context's kernels run on a
 // non-blocking stream, which a plain cudaMemcpy (legacy stream; from pageable
 // memory it may return before the DMA has landed) would not order them after.
+// The source may be host or device memory (unified addressing picks the
+// direction), so operators assembled on the device need no host round trip.
 template <typename T> static int dupload(T** p, const void* host, size_t bytes, cudaStream_t st) {
   int s = dalloc((void**)p, bytes);
   if (s) return s;
-  QCL_CUDA_CHECK(cudaMemcpyAsync(*p, host, bytes, cudaMemcpyHostToDevice, st));
+  QCL_CUDA_CHECK(cudaMemcpyAsync(*p, host, bytes, cudaMemcpyDefault, st));
   QCL_CUDA_CHECK(cudaStreamSynchronize(st));  // the host buffer may be a temporary
   return QCL_OK;
 }

@@ -149,6 +149,8 @@ def _declare(l):
         "qcl_anderson_guard": (I, [I, I, I, I, I, P, P, P]),
         "qcl_scba_density_matrix": (I, [P, P]),
         "qcl_density_matrix": (I, [I, I, I, I, P, P, P, P]),
+        "qcl_assemble_kernel": (I, [I, I, I, I, P, P, P, P]),
+        "qcl_dev_assemble_kernel": (I, [P, I, I, I, I, P, P, P, P]),
     }
     for name, (res, args) in sig.items():
         if hasattr(l, name):

@@ -181,12 +181,15 @@ def mechanism_struct(mech):
     def arr(a):
         if a is None:
             return None
+        if hasattr(a, "__cuda_array_interface__"):  # device array (complex128, column-major): passed as is
+            keep.append(a)
+            return ctypes.c_void_p(a.__cuda_array_interface__["data"][0])
         a = np.asfortranarray(np.asarray(a, dtype=np.complex128))
         keep.append(a)
         return ctypes.c_void_p(a.ctypes.data)
 
     s = _Mechanism(_KIND[mech.kind], 1 if mech.name == "LO" else 0,
-                   0 if mech.left is None else int(mech.left.shape[1]), float(mech.q),
+                   0 if mech.left is None else int(np.shape(mech.left)[1]), float(mech.q),
                    arr(mech.block), arr(mech.matrix), arr(mech.left), arr(mech.right), arr(mech.radial))
     s._keep = keep
     return s

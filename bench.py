@@ -53,7 +53,7 @@ def parse():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-extras", action="store_true", help="skip the variant and SCBA side measurements")
-    ap.add_argument("--capture", choices=["dyson", "hilbert", "scba", "tcgemm"],
+    ap.add_argument("--capture", choices=["dyson", "hilbert", "scba", "tcgemm", "scba_all_mixed", "scba_all_c128"],
                     help="run one small case of a kernel for an ncu capture (2 launches) and exit")
     return ap.parse_args()
 
@@ -599,6 +599,19 @@ def run_capture(kind):
         mech = Mechanism("impurity", "dense", 1.0, matrix=M)
         for _ in range(2):
             operators.production_static_contraction(mech, G, np.ones(nk), precision="c64")
+    elif kind.startswith("scba_all"):
+        # the all-mechanism SCBA workload of the extras (N_E x N_k = 1024 x 32,
+        # N_b = 16, LO + acoustic + impurity + IFR + alloy): seed + 3 eager
+        # iterations, for a per-kernel launch list of an iteration
+        from qclb200.problem import small_problem
+        from qclb200.scba import ProductionSCBA
+
+        pr = small_problem(NE=1024, Nk=32, Nb=16, mechanisms=("LO", "acoustic", "impurity", "IFR", "alloy"))
+        s = ProductionSCBA(pr, precision="mixed" if kind.endswith("mixed") else "c128", use_graph=False)
+        s.seed()
+        for _ in range(3):
+            s.step()
+        s.close()
     else:
         from qclb200.problem import tutorial_problem
         from qclb200.scba import ProductionSCBA

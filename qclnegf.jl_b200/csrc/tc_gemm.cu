@@ -39,17 +39,22 @@
 
 namespace qcl {
 
-constexpr int TC_BM = 128, TC_BN = 256, TC_BK = 16;
+constexpr int TC_BM = 128, TC_BN = 256, TC_BK = 16;  // TC_BN: the widest tile (operand padding)
 constexpr int TC_STAGES = 4;      // operand stages: the producer runs up to 3 blocks ahead
 constexpr int TC_ACC_KB = 2;      // K blocks per tensor-memory accumulation (12 MMAs)
 constexpr int TC_DRAIN_WARPS = 8; // warps that read accumulators out and write the tile
 constexpr int TC_THREADS = 32 * (TC_DRAIN_WARPS + 2);  // + producer warp + MMA warp
 constexpr int TC_A_BYTES = TC_BM * TC_BK * 4;   // 8 KiB per A part
-constexpr int TC_B_BYTES = TC_BN * TC_BK * 4;   // 16 KiB per B part
-constexpr int TC_STAGE_BYTES = 2 * TC_A_BYTES + 2 * TC_B_BYTES;
 constexpr int TC_BAR_BYTES = 128;
-constexpr int TC_SMEM_BYTES = TC_STAGES * TC_STAGE_BYTES + 1024 + TC_BAR_BYTES;
-constexpr uint32_t TC_TMEM_COLS = 512;  // two 256-column accumulators
+constexpr uint32_t TC_TMEM_COLS = 512;  // two accumulators of up to 256 columns
+// Per tile width BN (the N of one MMA): B part bytes, stage bytes, shared memory.
+template <int BN> struct TcShape {
+  static constexpr int B_BYTES = BN * TC_BK * 4;
+  static constexpr int STAGE_BYTES = 2 * TC_A_BYTES + 2 * B_BYTES;
+  static constexpr int SMEM_BYTES = TC_STAGES * STAGE_BYTES + 1024 + TC_BAR_BYTES;
+  static constexpr int CH = BN / 2;                   // accumulator columns per drain warp
+  static constexpr int LDW = CH % 32 == 0 ? 32 : 16;  // tensor-memory load width
+};
 constexpr long long TC_WAIT_LIMIT = 1ll << 22;  // try_wait rounds (~1 s) before a wait gives up
 
 // UMMA shared-memory descriptor, K-major, 64-byte swizzle (the layout TMA
@@ -60,9 +65,10 @@ __device__ __forceinline__ uint64_t umma_desc_k_sw64(uint32_t saddr) {
   return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)1 << 16) | ((uint64_t)32 << 32) | ((uint64_t)1 << 46) |
          ((uint64_t)4 << 61);
 }
-// Instruction descriptor: D f32, A/B tf32, both K-major, N = 256, M = 128.
-constexpr uint32_t TC_IDESC = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(TC_BN >> 3) << 17) |
-                              ((uint32_t)(TC_BM >> 4) << 24);
+// Instruction descriptor: D f32, A/B tf32, both K-major, N = BN, M = 128.
+template <int BN> __device__ __forceinline__ constexpr uint32_t tc_idesc() {
+  return (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(BN >> 3) << 17) | ((uint32_t)(TC_BM >> 4) << 24);
+}
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
@@ -98,17 +104,26 @@ __device__ __forceinline__ void tma_load(uint32_t dst, const CUtensorMap* map, i
       : "memory");
 }
 
-__device__ __forceinline__ void tc_mma(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t accumulate) {
+__device__ __forceinline__ void tc_mma(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                       uint32_t accumulate) {
   asm volatile(
       "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
       " tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n}" ::"r"(tmem_d),
-      "l"(adesc), "l"(bdesc), "r"(TC_IDESC), "r"(accumulate), "r"(0), "r"(0), "r"(0), "r"(0)
+      "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate), "r"(0), "r"(0), "r"(0), "r"(0)
       : "memory");
 }
 __device__ __forceinline__ void tc_commit(uint32_t bar) {
   asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar) : "memory");
 }
 
+// Reads 16 consecutive accumulator columns of this thread's lane.
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&v)[16]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+      : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]), "=r"(v[8]),
+        "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
+      : "r"(taddr));
+}
 // Reads 32 consecutive accumulator columns of this thread's lane.
 __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&v)[32]) {
   asm volatile(
@@ -142,7 +157,10 @@ struct TcArgs {
 // Hand-offs are mbarriers only: full[s] (TMA bytes), empty[s] (MMAs done
 // reading stage s), acc_full[b] (accumulation in buffer b done), acc_empty[b]
 // (256 readers done with buffer b).
+template <int BN>
 __global__ void __launch_bounds__(TC_THREADS, 1) tc_gemm_kernel(const __grid_constant__ TcMaps maps, TcArgs p) {
+  using S = TcShape<BN>;
+  constexpr int TC_STAGE_BYTES = S::STAGE_BYTES, TC_B_BYTES = S::B_BYTES;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const uint32_t raw = smem_u32(smem_raw);
   const uint32_t base = (raw + 1023u) & ~1023u;  // 1024-byte aligned stages
@@ -152,7 +170,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) tc_gemm_kernel(const __grid_con
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(gbase + TC_STAGES * TC_STAGE_BYTES + 16 * TC_STAGES + 32);
   __shared__ volatile int s_fail;
 
-  const int m0 = blockIdx.x * TC_BM, n0 = blockIdx.y * TC_BN;
+  const int m0 = blockIdx.x * TC_BM, n0 = blockIdx.y * BN;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int nkb = p.Kpad / TC_BK;
   const int nch = (nkb + TC_ACC_KB - 1) / TC_ACC_KB;
@@ -218,15 +236,16 @@ __global__ void __launch_bounds__(TC_THREADS, 1) tc_gemm_kernel(const __grid_con
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
         const uint32_t st = base + s * TC_STAGE_BYTES;
         const uint32_t tAh = st, tAl = st + TC_A_BYTES, tBh = st + 2 * TC_A_BYTES, tBl = tBh + TC_B_BYTES;
-        const uint32_t dacc = tmem + (uint32_t)(b * TC_BN);
+        const uint32_t dacc = tmem + (uint32_t)(b * BN);
+        constexpr uint32_t idesc = tc_idesc<BN>();
 #pragma unroll
         for (int ks = 0; ks < TC_BK / 8; ++ks) {  // K = 8 tf32 = 32 bytes per MMA
           const uint32_t off = ks * 32;
           const uint64_t ah = umma_desc_k_sw64(tAh + off), al = umma_desc_k_sw64(tAl + off);
           const uint64_t bh = umma_desc_k_sw64(tBh + off), bl = umma_desc_k_sw64(tBl + off);
-          tc_mma(dacc, ah, bh, (first && ks == 0) ? 0u : 1u);
-          tc_mma(dacc, ah, bl, 1u);
-          tc_mma(dacc, al, bh, 1u);
+          tc_mma(dacc, ah, bh, idesc, (first && ks == 0) ? 0u : 1u);
+          tc_mma(dacc, ah, bl, idesc, 1u);
+          tc_mma(dacc, al, bh, idesc, 1u);
         }
         tc_commit(empty + 8 * s);
         if (last) tc_commit(acc_full + 8 * b);
@@ -240,11 +259,12 @@ __global__ void __launch_bounds__(TC_THREADS, 1) tc_gemm_kernel(const __grid_con
     }
   } else {
     // ---- accumulator read-out and epilogue --------------------------------
+    constexpr int CH = S::CH, LDW = S::LDW;
     const uint32_t tlane = (uint32_t)((warp & 3) * 32) << 16;
-    const int cbase = (warp >> 2) * 128;
-    float sum[128];
+    const int cbase = (warp >> 2) * CH;
+    float sum[CH];
 #pragma unroll
-    for (int i = 0; i < 128; ++i) sum[i] = 0.0f;
+    for (int i = 0; i < CH; ++i) sum[i] = 0.0f;
     bool ok = true;
     for (int ch = 0; ch < nch; ++ch) {
       const int b = ch & 1;
@@ -257,14 +277,15 @@ __global__ void __launch_bounds__(TC_THREADS, 1) tc_gemm_kernel(const __grid_con
         break;
       }
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-      const uint32_t taddr = tmem + tlane + (uint32_t)(b * TC_BN + cbase);
+      const uint32_t taddr = tmem + tlane + (uint32_t)(b * BN + cbase);
 #pragma unroll
-      for (int c = 0; c < 4; ++c) {
-        uint32_t v[32];
-        tmem_ld32(taddr + c * 32, v);
+      for (int c = 0; c < CH / LDW; ++c) {
+        uint32_t v[LDW];
+        if constexpr (LDW == 32) tmem_ld32(taddr + c * 32, v);
+        else tmem_ld16(taddr + c * 16, v);
         asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 #pragma unroll
-        for (int i = 0; i < 32; ++i) sum[c * 32 + i] += __uint_as_float(v[i]);
+        for (int i = 0; i < LDW; ++i) sum[c * LDW + i] += __uint_as_float(v[i]);
       }
       asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
       mbar_arrive(acc_empty + 8 * b);
@@ -273,7 +294,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) tc_gemm_kernel(const __grid_con
     if (ok && e < p.M) {
       const float al = (float)p.alpha, be = (float)p.beta;
 #pragma unroll
-      for (int q = 0; q < 64; ++q) {
+      for (int q = 0; q < CH / 2; ++q) {
         const int nn = n0 + cbase + 2 * q;
         if (nn >= p.Ncols) continue;
         Cx<float>* dst = p.S + (size_t)e + (size_t)p.NE * (size_t)(nn >> 1);
@@ -421,6 +442,41 @@ static int make_operand_map(CUtensorMap* m, const float* ptr, int rows, int Kpad
   return QCL_OK;
 }
 
+// Tile width for an output of Ncols real columns: of 256 and 224 the one
+// whose tiles fill the most of their waves over the 148 SMs (one CTA per SM),
+// weighted by the share of the last tile that is padding; ties go to the
+// wider tile (fewer operand bytes per flop).  (192-wide tiles spill the drain
+// registers.)
+static int tc_pick_bn(int mtiles, int Ncols) {
+  const int cand[2] = {256, 224};
+  int best = 256;
+  double best_eff = -1;
+  for (int bn : cand) {
+    const int nt = (Ncols + bn - 1) / bn;
+    const long long tiles = (long long)mtiles * nt;
+    const long long waves = (tiles + 147) / 148;
+    const double eff = (double)tiles / (double)(waves * 148) * ((double)Ncols / ((double)nt * bn));
+    if (eff > best_eff + 1e-9) {
+      best_eff = eff;
+      best = bn;
+    }
+  }
+  return best;
+}
+
+template <int BN> static int launch_tc_t(const TcMaps& maps, const TcArgs& a, int mtiles, cudaStream_t st) {
+  static bool configured = false;
+  if (!configured) {
+    QCL_CUDA_CHECK(cudaFuncSetAttribute(tc_gemm_kernel<BN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        TcShape<BN>::SMEM_BYTES));
+    configured = true;
+  }
+  dim3 grid(mtiles, (a.Ncols + BN - 1) / BN);
+  tc_gemm_kernel<BN><<<grid, TC_THREADS, TcShape<BN>::SMEM_BYTES, st>>>(maps, a);
+  QCL_LAUNCH_CHECK("tc_gemm_kernel");
+  return QCL_OK;
+}
+
 int launch_tc_dense_contraction(int NE, int Nc, const float* Bhi, const float* Blo, const void* G, void* S,
                                 double alpha, double beta, float* awork, int* status, cudaStream_t st) {
   int Mpad, Npad, Kpad;
@@ -430,22 +486,18 @@ int launch_tc_dense_contraction(int NE, int Nc, const float* Bhi, const float* B
   dim3 sg((Mpad + 31) / 32, (Kpad + 31) / 32);
   tc_split_a_kernel<<<sg, 256, 0, st>>>(NE, Nc, Mpad, Kpad, (const Cx<float>*)G, Ahi, Alo);
   QCL_LAUNCH_CHECK("tc_split_a_kernel");
-  static bool configured = false;
-  if (!configured) {
-    QCL_CUDA_CHECK(cudaFuncSetAttribute(tc_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM_BYTES));
-    configured = true;
-  }
+  const int mtiles = Mpad / TC_BM;
+  const int bn = tc_pick_bn(mtiles, 2 * Nc);
   TcMaps maps;
   int s;
   if ((s = make_operand_map(&maps.ahi, Ahi, Mpad, Kpad, TC_BM))) return s;
   if ((s = make_operand_map(&maps.alo, Alo, Mpad, Kpad, TC_BM))) return s;
-  if ((s = make_operand_map(&maps.bhi, Bhi, Npad, Kpad, TC_BN))) return s;
-  if ((s = make_operand_map(&maps.blo, Blo, Npad, Kpad, TC_BN))) return s;
+  // B rows past Npad (the last tile of a narrower width) read the zero fill
+  if ((s = make_operand_map(&maps.bhi, Bhi, Npad, Kpad, bn))) return s;
+  if ((s = make_operand_map(&maps.blo, Blo, Npad, Kpad, bn))) return s;
   TcArgs a{NE, 2 * Nc, Kpad, (Cx<float>*)S, NE, alpha, beta, status};
-  dim3 grid(Mpad / TC_BM, Npad / TC_BN);
-  tc_gemm_kernel<<<grid, TC_THREADS, TC_SMEM_BYTES, st>>>(maps, a);
-  QCL_LAUNCH_CHECK("tc_gemm_kernel");
-  return QCL_OK;
+  if (bn == 224) return launch_tc_t<224>(maps, a, mtiles, st);
+  return launch_tc_t<256>(maps, a, mtiles, st);
 }
 
 }  // namespace qcl

@@ -620,7 +620,7 @@ template <typename RS, int NP, int BPC> static int launch_residual_t(const Resid
 template <typename RS> static int launch_residual_p(const ResidualArgs<RS>& a, cudaStream_t st) {
   switch (padded_size(a.N)) {
     case 8: return launch_residual_t<RS, 8, 8>(a, st);
-    case 16: return launch_residual_t<RS, 16, 4>(a, st);
+    case 16: return launch_residual_t<RS, 16, 2>(a, st);
     case 24: return launch_residual_t<RS, 24, 2>(a, st);
     case 32: return launch_residual_t<RS, 32, 1>(a, st);
     case 48: return launch_residual_t<RS, 48, 1>(a, st);

@@ -392,6 +392,26 @@ def run_gpu(args):
         e2e = {"value": job_rate(ws, NE * NK, e2e_ms), "unit": "solves/s", "h2d_bytes_per_step": 3 * fb,
                "d2h_bytes_per_step": 3 * fb, "ms_per_step": e2e_ms,
                "path": "qcl_dyson_keldysh + qcl_fft_hilbert_transform with pinned host buffers"}
+        # the link bound of this path: one field each way at once over PCIe
+        # (pinned buffers, two streams), times the 3 fields each way of a step
+        dbuf = torch.empty_like(SR)
+        s_in, s_out = torch.cuda.Stream(dev), torch.cuda.Stream(dev)
+
+        def both_ways():
+            with torch.cuda.stream(s_in):
+                dbuf.copy_(hSR, non_blocking=True)
+            with torch.cuda.stream(s_out):
+                hGR.copy_(SR, non_blocking=True)
+            torch.cuda.synchronize()
+
+        both_ways()
+        t = time.perf_counter()
+        for _ in range(2):
+            both_ways()
+        link_ms = 3 * (time.perf_counter() - t) / 2 * 1e3
+        e2e["link_bound_ms_per_step"] = link_ms
+        e2e["frac_of_link_bound"] = link_ms / e2e_ms
+        del dbuf
         # parity of this very run: GPU G^< equals the device-resident result
         diff = float((hGL.to(dev) - GL).abs().max().item())
         e2e["max_abs_diff_vs_device_run"] = diff

@@ -129,14 +129,6 @@ template <typename R> struct SmemOut {
   Cx<R>* buf;
   __device__ __forceinline__ void operator()(int t, Cx<R> v) const { buf[fpad(t)] = v; }
 };
-// conj(v * K[t]) into shared memory: the spectrum product, conjugated so that
-// the next forward transform computes the inverse one (IFFT(X) = conj(FFT(conj X)) / L).
-template <typename R> struct SpectrumOut {
-  Cx<R>* buf;
-  const Cx<R>* __restrict__ K;
-  __device__ __forceinline__ void operator()(int t, Cx<R> v) const { buf[fpad(t)] = conj(v * ldg_cx(K + t)); }
-};
-
 // v * W_{2H}^k for compile-time k (H a power of two, 2H <= 16).
 template <typename R, int H, int k> __device__ __forceinline__ Cx<R> w2h_mul(Cx<R> d) {
   switch ((k * 8 / H) & 15) {
@@ -161,10 +153,44 @@ template <typename R, int H> struct ZeroHiStage<R, H, 0> {
   __device__ __forceinline__ static void run(Cx<R>*) {}
 };
 
+// Twiddles of a pass (radix RADIX, stride NS): v[r] *= W_L^{k c r}, r = 1 ..
+// RADIX-1, k = j mod NS, c = L / (NS RADIX).
+// complex128: w_1 = W_L^{k c} from the length-L table and its powers by binary
+// powering (products of at most four factors, so the twiddle error stays a
+// few ulps).  complex64: every power read from the pass's own table seg[(r-1)
+// NS + k] (correctly rounded, and contiguous in k so a warp's loads coalesce);
+// a few FP32 ulps of twiddle error would otherwise be the largest term of the
+// transform error (about twice the table form's).
+template <typename R, int L, int RADIX, int NS>
+__device__ __forceinline__ Cx<R> first_twiddle(int k, const Cx<R>* __restrict__ tw, const Cx<R>* __restrict__ seg) {
+  if constexpr (sizeof(R) == 4) return ldg_cx(seg + k);
+  return ldg_cx(tw + k * (L / (NS * RADIX)));
+}
+template <typename R, int L, int RADIX, int NS>
+__device__ __forceinline__ void apply_twiddles(Cx<R>* v, Cx<R> w1, int k, const Cx<R>* __restrict__ seg) {
+  if constexpr (sizeof(R) == 4) {
+    v[1] = v[1] * w1;
+#pragma unroll
+    for (int r = 2; r < RADIX; ++r) v[r] = v[r] * ldg_cx(seg + (r - 1) * NS + k);
+  } else {
+    Cx<R> w[RADIX];
+    w[1] = w1;
+#pragma unroll
+    for (int r = 2; r < RADIX; ++r) {
+      const int hi = (r & (r - 1)) ? (r & (r - 1)) : r / 2;  // r = hi + lo, hi >= lo
+      w[r] = w[hi] * w[r - hi];
+    }
+#pragma unroll
+    for (int r = 1; r < RADIX; ++r) v[r] = v[r] * w[r];
+  }
+}
+
 // One mixed-radix Stockham pass (natural-order output after all passes).
 // ZHI: the inputs of slots r >= RADIX/2 are known to be zero (the padding).
+// tw: W_L^t, t < L; seg: this pass's complex64 twiddle table (null otherwise).
 template <typename R, int L, int RADIX, int NS, bool ZHI, typename In, typename Out>
-__device__ __forceinline__ void stockham_pass(const In& in, const Out& out, const Cx<R>* __restrict__ tw) {
+__device__ __forceinline__ void stockham_pass(const In& in, const Out& out, const Cx<R>* __restrict__ tw,
+                                              const Cx<R>* __restrict__ seg) {
   const int tid = threadIdx.x;
   constexpr int T = FftPlan<L>::T;
   constexpr int NB = L / RADIX;
@@ -178,7 +204,7 @@ __device__ __forceinline__ void stockham_pass(const In& in, const Out& out, cons
 #pragma unroll
     for (int q = 0; q < Q; ++q) {
       const int j = tid + q * T;
-      w1[q] = ldg_cx(tw + (j < NB ? (j % NS) * (L / (NS * RADIX)) : 0));
+      w1[q] = first_twiddle<R, L, RADIX, NS>(j < NB ? j % NS : 0, tw, seg);
     }
   }
   Cx<R> v[Q][RADIX];
@@ -196,19 +222,7 @@ __device__ __forceinline__ void stockham_pass(const In& in, const Out& out, cons
     const int j = tid + q * T;
     if (j < NB) {
       const int k = j % NS;
-      if (NS > 1) {
-        // w_r = w_1^r by binary powering (products of at most four factors, so
-        // the twiddle error stays a few ulps) instead of RADIX - 1 table loads.
-        Cx<R> w[RADIX];
-        w[1] = w1[q];
-#pragma unroll
-        for (int r = 2; r < RADIX; ++r) {
-          const int hi = (r & (r - 1)) ? (r & (r - 1)) : r / 2;  // r = hi + lo, hi >= lo
-          w[r] = w[hi] * w[r - hi];
-        }
-#pragma unroll
-        for (int r = 1; r < RADIX; ++r) v[q][r] = v[q][r] * w[r];
-      }
+      if (NS > 1) apply_twiddles<R, L, RADIX, NS>(v[q], w1[q], k, seg);
       if (ZHI) {
         ZeroHiStage<R, RADIX / 2, RADIX / 2>::run(v[q]);
         DifStage<R, RADIX, RADIX / 4>::run(v[q]);
@@ -223,38 +237,112 @@ __device__ __forceinline__ void stockham_pass(const In& in, const Out& out, cons
   __syncthreads();
 }
 
-// Forward FFT of length L: first pass reads through `in`, last pass writes
-// through `out`, the passes between work in place on `buf` (padded indexing).
-// ZHI: the input is zero on [L/2, L) (the zero padding of the convolution).
-template <typename R, int L, bool ZHI, typename In, typename Out>
-__device__ __forceinline__ void fft_run(const In& in, const Out& out, Cx<R>* buf, const Cx<R>* tw) {
-  static_assert(L >= 64 && L <= 16384, "unsupported FFT length");
-  const SmemIn<R> si{buf};
-  const SmemOut<R> so{buf};
-  if constexpr (L == 64) {
-    stockham_pass<R, L, 16, 1, ZHI>(in, so, tw);
-    stockham_pass<R, L, 4, 16, false>(si, out, tw);
-  } else if constexpr (L == 128) {
-    stockham_pass<R, L, 16, 1, ZHI>(in, so, tw);
-    stockham_pass<R, L, 8, 16, false>(si, out, tw);
-  } else if constexpr (L == 256) {
-    stockham_pass<R, L, 16, 1, ZHI>(in, so, tw);
-    stockham_pass<R, L, 16, 16, false>(si, out, tw);
-  } else if constexpr (L <= 2048) {
-    // small radix first: with the zero half pruned it is a plain copy
-    stockham_pass<R, L, L / 256, 1, ZHI>(in, so, tw);
-    stockham_pass<R, L, 16, L / 256, false>(si, so, tw);
-    stockham_pass<R, L, 16, L / 16, false>(si, out, tw);
-  } else if constexpr (L == 4096) {
-    stockham_pass<R, L, 16, 1, ZHI>(in, so, tw);
-    stockham_pass<R, L, 16, 16, false>(si, so, tw);
-    stockham_pass<R, L, 16, 256, false>(si, out, tw);
-  } else {
-    stockham_pass<R, L, L / 4096, 1, ZHI>(in, so, tw);
-    stockham_pass<R, L, 16, L / 4096, false>(si, so, tw);
-    stockham_pass<R, L, 16, L / 256, false>(si, so, tw);
-    stockham_pass<R, L, 16, L / 16, false>(si, out, tw);
+// Pass plan of the length-L convolution: the forward transform is a first
+// pass of radix S = L / 16^P (2 <= S <= 16) followed by P radix-16 passes,
+// the inverse runs the same radices in reverse order.  The last forward pass
+// (NS = L/16) and the first inverse pass (NS = 1) touch the same indices
+// j + r L/16 in the same thread, so they run as one register-resident pass
+// with the spectrum product between them (spectrum_pass).
+constexpr int conv_passes(int L) {
+  int p = 0;
+  while (L > 16) {
+    L /= 16;
+    ++p;
   }
+  return p;
+}
+
+// complex64 pass tables, in pass order: the forward radix-16 passes (NS = S
+// 16^i, i < P; the last is the fused one), the inverse radix-16 passes (NS =
+// 16^i, 1 <= i < P), the final radix-S pass (NS = L/S); a pass's table is
+// (RADIX - 1) NS entries.  Offsets in entries:
+constexpr int conv_fwd_seg(int L, int i) {  // S (16^i - 1)
+  const int P = conv_passes(L);
+  int off = 0, ns = L >> (4 * P);
+  for (int t = 0; t < i; ++t, ns *= 16) off += 15 * ns;
+  return off;
+}
+constexpr int conv_inv_seg(int L, int i) {  // (L - S) + 16^i - 16
+  const int P = conv_passes(L);
+  int off = L - (L >> (4 * P)), ns = 16;
+  for (int t = 1; t < i; ++t, ns *= 16) off += 15 * ns;
+  return off;
+}
+constexpr int conv_table_entries(int L) {  // 2L - S - 16
+  return conv_inv_seg(L, conv_passes(L)) + ((L >> (4 * conv_passes(L))) - 1) * (L / (L >> (4 * conv_passes(L))));
+}
+
+template <typename R, int L, int NS, int COUNT> struct Radix16Passes {
+  __device__ __forceinline__ static void run(Cx<R>* buf, const Cx<R>* tw, const Cx<R>* seg) {
+    stockham_pass<R, L, 16, NS, false>(SmemIn<R>{buf}, SmemOut<R>{buf}, tw, seg);
+    Radix16Passes<R, L, NS * 16, COUNT - 1>::run(buf, tw, seg ? seg + 15 * NS : nullptr);
+  }
+};
+template <typename R, int L, int NS> struct Radix16Passes<R, L, NS, 0> {
+  __device__ __forceinline__ static void run(Cx<R>*, const Cx<R>*, const Cx<R>*) {}
+};
+
+// Last radix-16 pass of the forward transform, times K and conjugated (so
+// that the next forward transform computes the inverse one: IFFT(X) =
+// conj(FFT(conj X)) / L), and the first radix-16 pass of that transform.
+template <typename R, int L>
+__device__ __forceinline__ void spectrum_pass(Cx<R>* buf, const Cx<R>* __restrict__ K, const Cx<R>* __restrict__ tw,
+                                              const Cx<R>* __restrict__ seg) {
+  constexpr int T = FftPlan<L>::T;
+  constexpr int NB = L / 16;
+  constexpr int Q = (NB + T - 1) / T;
+  const int tid = threadIdx.x;
+  Cx<R> w1[Q];
+#pragma unroll
+  for (int q = 0; q < Q; ++q) {
+    const int j = tid + q * T;
+    w1[q] = first_twiddle<R, L, 16, NB>(j < NB ? j : 0, tw, seg);  // NS = L/16: W_L^j
+  }
+  Cx<R> v[Q][16];
+#pragma unroll
+  for (int q = 0; q < Q; ++q) {
+    const int j = tid + q * T;
+    if (j < NB) {
+#pragma unroll
+      for (int r = 0; r < 16; ++r) v[q][r] = buf[fpad(j + r * NB)];
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int q = 0; q < Q; ++q) {
+    const int j = tid + q * T;
+    if (j < NB) {
+      apply_twiddles<R, L, 16, NB>(v[q], w1[q], j, seg);
+      DifStage<R, 16, 8>::run(v[q]);
+      // forward output j + r NB is v[bitrev(r)]; it is input r of the next pass
+      Cx<R> u[16];
+#pragma unroll
+      for (int r = 0; r < 16; ++r) u[r] = conj(v[q][bitrev<16>(r)] * ldg_cx(K + j + r * NB));
+      DifStage<R, 16, 8>::run(u);
+#pragma unroll
+      for (int r = 0; r < 16; ++r) buf[fpad(16 * j + r)] = u[bitrev<16>(r)];
+    }
+  }
+  __syncthreads();
+}
+
+// conj(L * IFFT(FFT(x) .* K)) for a field read through `in` (ZHI: zero on
+// [L/2, L)), written through `out`; `buf` holds the padded column, `twt` the
+// complex64 pass tables (null for complex128).
+template <typename R, int L, bool ZHI, typename In, typename Out>
+__device__ __forceinline__ void convolve_run(const In& in, const Cx<R>* K, const Out& out, Cx<R>* buf,
+                                             const Cx<R>* tw, const Cx<R>* twt) {
+  static_assert(L >= 64 && L <= 16384, "unsupported FFT length");
+  constexpr int P = conv_passes(L);
+  constexpr int S = L >> (4 * P);
+  static_assert(S >= 2 && S <= 16, "first-pass radix");
+  static_assert(conv_table_entries(L) == 2 * L - S - 16, "pass-table layout");
+  const bool t = twt != nullptr;
+  stockham_pass<R, L, S, 1, ZHI>(in, SmemOut<R>{buf}, tw, nullptr);
+  Radix16Passes<R, L, S, P - 1>::run(buf, tw, t ? twt + conv_fwd_seg(L, 0) : nullptr);
+  spectrum_pass<R, L>(buf, K, tw, t ? twt + conv_fwd_seg(L, P - 1) : nullptr);
+  Radix16Passes<R, L, 16, P - 1>::run(buf, tw, t ? twt + conv_inv_seg(L, 1) : nullptr);
+  stockham_pass<R, L, S, L / S, false>(SmemIn<R>{buf}, out, tw, t ? twt + conv_inv_seg(L, P) : nullptr);
 }
 
 template <typename R> struct HilbertArgs {
@@ -273,6 +361,9 @@ template <typename R> struct HilbertArgs {
   const Cx<R>* twist; // W_2L^n, n < L
   double* partial;    // per column (|y2L - yL|^2, |yL|^2), or null
   double scale_out;   // 1 / L
+  const Cx<R>* ksplit;  // [FFT_L(kernel)[2j], j < L/2 | FFT_L(kernel)[2j+1], j < L/2]
+  const Cx<R>* twh;     // W_{L/2}^t, t < L/2
+  const Cx<R>* twt;     // complex64 pass twiddle tables (null for complex128)
 };
 
 template <typename R>
@@ -290,12 +381,12 @@ template <typename R> struct FieldIn {
   static constexpr bool kShared = false;
   const HilbertArgs<R>* p;
   size_t base;
-  bool twist;
+  const Cx<R>* twist;  // per-sample phase, or null
   __device__ __forceinline__ Cx<R> operator()(int e) const {
     if (e >= p->NE) return cx<R>(0, 0);
     Cx<R> g = gamma_at(*p, base + e);
     if (twist) {
-      g = g * ldg_cx(p->twist + e);
+      g = g * ldg_cx(twist + e);
     } else if (p->GamOut) {
       p->GamOut[base + e] = g;
     }
@@ -321,38 +412,48 @@ template <typename R> struct ResultOut {
   }
 };
 
+// Registers are capped (128 per thread for complex128, 96 for complex64) so
+// that the register file holds as many CTAs as the shared memory does.
+template <typename R, int T> constexpr int hilbert_min_blocks() {
+  return 65536 / ((sizeof(R) == 8 ? 128 : 96) * T) < 1 ? 1 : 65536 / ((sizeof(R) == 8 ? 128 : 96) * T);
+}
+// Shared memory of the one-pass kernel: the padded column, plus (with
+// verification) the length-L results y_L[e + NE - 1] kept for the comparison.
+template <typename R, int L, bool VERIFY> constexpr size_t hilbert_smem_bytes() {
+  return (size_t)(L + L / 16 + (VERIFY ? L / 2 : 0)) * sizeof(Cx<R>);
+}
+
 template <typename R, int L, bool VERIFY>
-__global__ void __launch_bounds__(FftPlan<L>::T) hilbert_kernel(HilbertArgs<R> p) {
+__global__ void __launch_bounds__(FftPlan<L>::T, (hilbert_min_blocks<R, FftPlan<L>::T>()))
+    hilbert_kernel(HilbertArgs<R> p) {
   constexpr int T = FftPlan<L>::T;
-  constexpr int PER = (L / 2 + T - 1) / T;  // outputs per thread (NE <= L/2 + 1)
+  constexpr int PER = (L / 2 + T - 1) / T;  // outputs per thread (NE <= L/2)
   extern __shared__ __align__(16) unsigned char smem_raw[];
   Cx<R>* buf = reinterpret_cast<Cx<R>*>(smem_raw);
   const long long col = blockIdx.x + (long long)blockIdx.y * gridDim.x;
   if (col >= p.ncols) return;
   const int NE = p.NE;
   const size_t base = (size_t)col * NE;
-  const SmemIn<R> si{buf};
   const SmemOut<R> so{buf};
 
-  // forward transform of the padded column, times the kernel spectrum
-  fft_run<R, L, true>(FieldIn<R>{&p, base, false}, SpectrumOut<R>{buf, p.khat}, buf, p.tw);
   if constexpr (!VERIFY) {
-    // inverse transform, results written from registers
-    fft_run<R, L, false>(si, ResultOut<R>{&p, base}, buf, p.tw);
+    // results written from registers by the last pass
+    convolve_run<R, L, true>(FieldIn<R>{&p, base, nullptr}, p.khat, ResultOut<R>{&p, base}, buf, p.tw, p.twt);
     return;
   }
-  fft_run<R, L, false>(si, so, buf, p.tw);
-  Cx<R> lam[PER];
+  convolve_run<R, L, true>(FieldIn<R>{&p, base, nullptr}, p.khat, so, buf, p.tw, p.twt);
+  // y_L of this thread's outputs, kept in shared memory (read back by the
+  // same thread) instead of registers across the second transform
+  Cx<R>* lam = buf + (L + L / 16);
   const R sc = (R)p.scale_out;
 #pragma unroll
   for (int q = 0; q < PER; ++q) {
     const int e = threadIdx.x + q * T;
-    if (e < NE) lam[q] = sc * conj(buf[fpad(e + NE - 1)]);
+    if (e < NE) lam[e] = sc * conj(buf[fpad(e + NE - 1)]);
   }
   __syncthreads();
   // ---- odd-frequency half of the length-2L transform -------------------------
-  fft_run<R, L, true>(FieldIn<R>{&p, base, true}, SpectrumOut<R>{buf, p.kodd}, buf, p.tw);
-  fft_run<R, L, false>(si, so, buf, p.tw);
+  convolve_run<R, L, true>(FieldIn<R>{&p, base, p.twist}, p.kodd, so, buf, p.tw, p.twt);
   double dsum = 0, lsum = 0;
 #pragma unroll
   for (int q = 0; q < PER; ++q) {
@@ -360,15 +461,16 @@ __global__ void __launch_bounds__(FftPlan<L>::T) hilbert_kernel(HilbertArgs<R> p
     if (e < NE) {
       const int n = e + NE - 1;
       Cx<R> yo = sc * (conj(buf[fpad(n)]) * conj(p.twist[n]));
+      const Cx<R> yl = lam[e];
       // y_2L - y_L = (y_L + yo)/2 - y_L = (yo - y_L)/2
-      Cx<R> d = (R)0.5 * (yo - lam[q]);
+      Cx<R> d = (R)0.5 * (yo - yl);
       dsum += (double)d.x * d.x + (double)d.y * d.y;
-      lsum += (double)lam[q].x * lam[q].x + (double)lam[q].y * lam[q].y;
+      lsum += (double)yl.x * yl.x + (double)yl.y * yl.y;
       if (p.SR) {
         Cx<R> g = gamma_at(p, base + e);
-        p.SR[base + e] = cx<R>(lam[q].x + (R)0.5 * g.y, lam[q].y - (R)0.5 * g.x);
+        p.SR[base + e] = cx<R>(yl.x + (R)0.5 * g.y, yl.y - (R)0.5 * g.x);
       } else {
-        p.Lam[base + e] = lam[q];
+        p.Lam[base + e] = yl;
       }
     }
   }
@@ -393,6 +495,74 @@ __global__ void __launch_bounds__(FftPlan<L>::T) hilbert_kernel(HilbertArgs<R> p
     p.partial[2 * col] = a;
     p.partial[2 * col + 1] = b;
   }
+}
+
+// ---------------------------------------------------------------------------
+// Even/odd frequency halves in sequence (no verification).
+//
+// The padded field is zero on [L/2, L), so its length-L spectrum splits into
+//   X[2j]   = FFT_{L/2}(x)[j],   X[2j+1] = FFT_{L/2}(x W_L^n)[j],
+// and with Y = X K_hat the length-L inverse transform is
+//   y[n] = (ye[n'] + (-1)^s W_L^{-n'} yo[n']) / L,   n = n' + s L/2,
+// ye, yo the unnormalised length-L/2 inverse transforms of Y[2j], Y[2j+1].
+// One CTA transforms the even half, parks conj(ye) of the wanted outputs in
+// the output array, then transforms the odd half and completes each output
+// in the same thread that parked it.  The column buffer is L/2 long, so two
+// columns share an SM where one length-L column filled it.  Arithmetic is
+// that of the one-pass kernel, minus the zero-pruned radix-2 pass of the
+// inverse transform.  The output must not alias the input (the field is read
+// again for the odd half).
+// ---------------------------------------------------------------------------
+// Output slot of padded index t in [0, L/2): n = t or t + L/2, whichever lies
+// in [NE - 1, 2 NE - 2] (at most one does, since NE <= L/2); -1 if neither.
+template <int LH> __device__ __forceinline__ int half_slot(int t, int NE) {
+  const int n = t >= NE - 1 ? t : t + LH;
+  const int e = n - (NE - 1);
+  return e < NE ? e : -1;
+}
+template <typename R, int LH> struct ParkOut {
+  const HilbertArgs<R>* p;
+  size_t base;
+  __device__ __forceinline__ void operator()(int t, Cx<R> v) const {
+    const int e = half_slot<LH>(t, p->NE);
+    if (e < 0) return;
+    (p->SR ? p->SR : p->Lam)[base + e] = v;
+  }
+};
+template <typename R, int LH> struct CompleteOut {
+  const HilbertArgs<R>* p;
+  size_t base;
+  __device__ __forceinline__ void operator()(int t, Cx<R> v) const {
+    const int NE = p->NE;
+    const int e = half_slot<LH>(t, NE);
+    if (e < 0) return;
+    Cx<R>* dst = p->SR ? p->SR : p->Lam;
+    const Cx<R> a = dst[base + e];  // parked by this thread in the even half
+    const Cx<R> d = v * ldg_cx(p->tw + t);
+    const Cx<R> y = t < NE - 1 ? a - d : a + d;
+    const R sc = (R)p->scale_out;
+    const Cx<R> lam = cx<R>(sc * y.x, -sc * y.y);
+    if (p->SR) {
+      const Cx<R> g = gamma_at(*p, base + e);
+      p->SR[base + e] = cx<R>(lam.x + (R)0.5 * g.y, lam.y - (R)0.5 * g.x);
+    } else {
+      p->Lam[base + e] = lam;
+    }
+  }
+};
+
+template <typename R, int LH>
+__global__ void __launch_bounds__(FftPlan<LH>::T, (hilbert_min_blocks<R, FftPlan<LH>::T>()))
+    hilbert_halves_kernel(HilbertArgs<R> p) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  Cx<R>* buf = reinterpret_cast<Cx<R>*>(smem_raw);
+  const long long col = blockIdx.x + (long long)blockIdx.y * gridDim.x;
+  if (col >= p.ncols) return;
+  const size_t base = (size_t)col * p.NE;
+  convolve_run<R, LH, false>(FieldIn<R>{&p, base, nullptr}, p.ksplit, ParkOut<R, LH>{&p, base}, buf, p.twh,
+                             nullptr);
+  convolve_run<R, LH, false>(FieldIn<R>{&p, base, p.tw}, p.ksplit + LH, CompleteOut<R, LH>{&p, base}, buf,
+                             p.twh, nullptr);
 }
 
 // ---------------------------------------------------------------------------
@@ -436,6 +606,9 @@ void free_hilbert_tables(HilbertTables& t) {
   cudaFree(t.kodd);
   cudaFree(t.tw);
   cudaFree(t.twist);
+  cudaFree(t.ksplit);
+  cudaFree(t.twh);
+  cudaFree(t.twt);
   cudaFree(t.partial);
   t = HilbertTables();
 }
@@ -493,7 +666,8 @@ int prepare_hilbert_tables(HilbertTables& t, int NE, double de, int precision) {
   }
   host_fft(kr, ki);
   host_fft(kr2, ki2);
-  std::vector<double> kor(L), koi(L), twr(L), twi(L), tsr(L), tsi(L);
+  const int LH = L / 2;
+  std::vector<double> kor(L), koi(L), twr(L), twi(L), tsr(L), tsi(L), ksr(L), ksi(L), thr(LH), thi(LH);
   for (int k = 0; k < L; ++k) {
     kor[k] = kr2[2 * k + 1];
     koi[k] = ki2[2 * k + 1];
@@ -501,6 +675,13 @@ int prepare_hilbert_tables(HilbertTables& t, int NE, double de, int precision) {
     twi[k] = -sin(2.0 * M_PI * k / L);
     tsr[k] = cos(M_PI * k / L);
     tsi[k] = -sin(M_PI * k / L);
+    const int j = k >> 1, r = k & 1;  // even spectrum first, then odd
+    ksr[r * LH + j] = kr[k];
+    ksi[r * LH + j] = ki[k];
+  }
+  for (int k = 0; k < LH; ++k) {
+    thr[k] = cos(2.0 * M_PI * k / LH);
+    thi[k] = -sin(2.0 * M_PI * k / LH);
   }
   int st;
   if (storage == QCL_C128) {
@@ -508,11 +689,36 @@ int prepare_hilbert_tables(HilbertTables& t, int NE, double de, int precision) {
     if ((st = upload_cx<double>(&t.kodd, kor, koi))) return st;
     if ((st = upload_cx<double>(&t.tw, twr, twi))) return st;
     if ((st = upload_cx<double>(&t.twist, tsr, tsi))) return st;
+    if ((st = upload_cx<double>(&t.ksplit, ksr, ksi))) return st;
+    if ((st = upload_cx<double>(&t.twh, thr, thi))) return st;
   } else {
     if ((st = upload_cx<float>(&t.khat, kr, ki))) return st;
     if ((st = upload_cx<float>(&t.kodd, kor, koi))) return st;
     if ((st = upload_cx<float>(&t.tw, twr, twi))) return st;
     if ((st = upload_cx<float>(&t.twist, tsr, tsi))) return st;
+    if ((st = upload_cx<float>(&t.ksplit, ksr, ksi))) return st;
+    if ((st = upload_cx<float>(&t.twh, thr, thi))) return st;
+    // pass twiddle tables (the order and offsets of conv_fwd_seg / conv_inv_seg)
+    int P = 0;
+    for (int x = L; x > 16; x /= 16) ++P;
+    const int S = L >> (4 * P);
+    std::vector<double> pr, pi;
+    auto seg = [&](int radix, int ns) {
+      for (int r = 1; r < radix; ++r)
+        for (int k = 0; k < ns; ++k) {
+          const long long m = (long long)k * (L / (ns * radix)) * r;  // < L
+          pr.push_back(cos(2.0 * M_PI * (double)m / L));
+          pi.push_back(-sin(2.0 * M_PI * (double)m / L));
+        }
+    };
+    for (int i = 0, ns = S; i < P; ++i, ns *= 16) seg(16, ns);
+    for (int i = 1, ns = 16; i < P; ++i, ns *= 16) seg(16, ns);
+    seg(S, L / S);
+    if (pr.size() != (size_t)(2 * L - S - 16)) {
+      set_last_error("internal: FFT pass-table size %zu for L = %d", pr.size(), L);
+      return QCL_UNSUPPORTED;
+    }
+    if ((st = upload_cx<float>(&t.twt, pr, pi))) return st;
   }
   t.NE = NE;
   t.L = L;
@@ -532,7 +738,7 @@ int ensure_partial(HilbertTables& t, long long ncols) {
 
 template <typename R, int L, bool VERIFY> static int launch_hilbert_LV(const HilbertArgs<R>& a, cudaStream_t st) {
   constexpr int T = FftPlan<L>::T;
-  constexpr size_t smem = (size_t)(L + L / 16) * sizeof(Cx<R>);
+  constexpr size_t smem = hilbert_smem_bytes<R, L, VERIFY>();
   static bool configured = false;
   if (!configured) {
     QCL_CUDA_CHECK(cudaFuncSetAttribute(hilbert_kernel<R, L, VERIFY>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -545,22 +751,47 @@ template <typename R, int L, bool VERIFY> static int launch_hilbert_LV(const Hil
   QCL_LAUNCH_CHECK("hilbert_kernel");
   return QCL_OK;
 }
-template <typename R, int L> static int launch_hilbert_L(const HilbertArgs<R>& a, cudaStream_t st) {
-  return a.partial ? launch_hilbert_LV<R, L, true>(a, st) : launch_hilbert_LV<R, L, false>(a, st);
+template <typename R, int LH> static int launch_hilbert_halves(const HilbertArgs<R>& a, cudaStream_t st) {
+  constexpr int T = FftPlan<LH>::T;
+  constexpr size_t smem = (size_t)(LH + LH / 16) * sizeof(Cx<R>);
+  static bool configured = false;
+  if (!configured) {
+    QCL_CUDA_CHECK(cudaFuncSetAttribute(hilbert_halves_kernel<R, LH>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)smem));
+    configured = true;
+  }
+  const long long nc = a.ncols;
+  dim3 grid((unsigned)(nc < 65535 ? nc : 65535), (unsigned)((nc + 65534) / 65535));
+  hilbert_halves_kernel<R, LH><<<grid, T, smem, st>>>(a);
+  QCL_LAUNCH_CHECK("hilbert_halves_kernel");
+  return QCL_OK;
 }
 
-template <typename R> static int launch_hilbert_t(const HilbertArgs<R>& a, int L, cudaStream_t st) {
+// The half-length form is used for the complex128 transform whose length-L
+// column fills an SM's shared memory (L = 8192; at L = 4096 two columns
+// already share an SM and the one-pass kernel is faster).
+template <typename R, int L> constexpr bool kHilbertHalves = sizeof(R) == 8 && L == 8192;
+
+template <typename R, int L> static int launch_hilbert_L(const HilbertArgs<R>& a, bool halves, cudaStream_t st) {
+  if (a.partial) return launch_hilbert_LV<R, L, true>(a, st);
+  if constexpr (kHilbertHalves<R, L>) {
+    if (halves) return launch_hilbert_halves<R, L / 2>(a, st);
+  }
+  return launch_hilbert_LV<R, L, false>(a, st);
+}
+
+template <typename R> static int launch_hilbert_t(const HilbertArgs<R>& a, int L, bool halves, cudaStream_t st) {
   switch (L) {
-    case 64: return launch_hilbert_L<R, 64>(a, st);
-    case 128: return launch_hilbert_L<R, 128>(a, st);
-    case 256: return launch_hilbert_L<R, 256>(a, st);
-    case 512: return launch_hilbert_L<R, 512>(a, st);
-    case 1024: return launch_hilbert_L<R, 1024>(a, st);
-    case 2048: return launch_hilbert_L<R, 2048>(a, st);
-    case 4096: return launch_hilbert_L<R, 4096>(a, st);
-    case 8192: return launch_hilbert_L<R, 8192>(a, st);
+    case 64: return launch_hilbert_L<R, 64>(a, halves, st);
+    case 128: return launch_hilbert_L<R, 128>(a, halves, st);
+    case 256: return launch_hilbert_L<R, 256>(a, halves, st);
+    case 512: return launch_hilbert_L<R, 512>(a, halves, st);
+    case 1024: return launch_hilbert_L<R, 1024>(a, halves, st);
+    case 2048: return launch_hilbert_L<R, 2048>(a, halves, st);
+    case 4096: return launch_hilbert_L<R, 4096>(a, halves, st);
+    case 8192: return launch_hilbert_L<R, 8192>(a, halves, st);
     case 16384:
-      if constexpr (sizeof(R) == 4) return launch_hilbert_L<R, 16384>(a, st);
+      if constexpr (sizeof(R) == 4) return launch_hilbert_L<R, 16384>(a, halves, st);
       [[fallthrough]];
     default:
       set_last_error("unsupported FFT length %d", L);
@@ -579,6 +810,19 @@ int launch_hilbert(HilbertTables& t, int precision, long long ncols, const doubl
     if (s) return s;
   }
   if (ncols <= 0) return QCL_OK;
+  // the half-length kernel reads the field twice: not used when the output
+  // overlaps it ...
+  const size_t bytes = (size_t)ncols * t.NE * (precision == QCL_C128 ? 16 : 8);
+  const char* out = (const char*)(SR ? SR : Lam);
+  auto overlaps = [&](const void* in) {
+    const char* c = (const char*)in;
+    return c && c < out + bytes && out < c + bytes;
+  };
+  // ... nor below two columns per SM, where the one-pass kernel's 2x wider
+  // CTAs finish a column sooner
+  int dev = 0, sms = 148;
+  if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const bool halves = ncols >= 2LL * sms && !overlaps(Gam) && !overlaps(SL) && !overlaps(SG);
   if (precision == QCL_C128) {
     HilbertArgs<double> a{t.NE,
                           ncols,
@@ -594,8 +838,11 @@ int launch_hilbert(HilbertTables& t, int precision, long long ncols, const doubl
                           (const Cx<double>*)t.tw,
                           (const Cx<double>*)t.twist,
                           verify ? t.partial + 2 * partial_offset : nullptr,
-                          1.0 / t.L};
-    return launch_hilbert_t<double>(a, t.L, st);
+                          1.0 / t.L,
+                          (const Cx<double>*)t.ksplit,
+                          (const Cx<double>*)t.twh,
+                          nullptr};
+    return launch_hilbert_t<double>(a, t.L, halves, st);
   }
   HilbertArgs<float> a{t.NE,
                        ncols,
@@ -611,8 +858,11 @@ int launch_hilbert(HilbertTables& t, int precision, long long ncols, const doubl
                        (const Cx<float>*)t.tw,
                        (const Cx<float>*)t.twist,
                        verify ? t.partial + 2 * partial_offset : nullptr,
-                       1.0 / t.L};
-  return launch_hilbert_t<float>(a, t.L, st);
+                       1.0 / t.L,
+                       (const Cx<float>*)t.ksplit,
+                       (const Cx<float>*)t.twh,
+                       (const Cx<float>*)t.twt};
+  return launch_hilbert_t<float>(a, t.L, halves, st);
 }
 
 }  // namespace qcl

@@ -138,6 +138,9 @@ struct HilbertTables {
   void* kodd = nullptr;
   void* tw = nullptr;
   void* twist = nullptr;
+  void* ksplit = nullptr;
+  void* twh = nullptr;
+  void* twt = nullptr;
   double* partial = nullptr;
   long long partial_cols = 0;
 };

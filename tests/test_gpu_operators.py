@@ -77,7 +77,7 @@ def test_dyson_singular_block_raises(gpu_ops):
         gpu_ops.retarded_green(eps, h, SR2)
 
 
-@pytest.mark.parametrize("NE", [37, 64, 400, 1000, 2048, 4096])
+@pytest.mark.parametrize("NE", [37, 64, 400, 1000, 1025, 2048, 3001, 4096])
 def test_fft_hilbert_c128_matches_direct_pv(gpu_ops, orc, NE):
     rng = np.random.default_rng(NE)
     ncols = 6
@@ -98,6 +98,39 @@ def test_fft_hilbert_c128_matches_direct_pv(gpu_ops, orc, NE):
     Lam2 = gpu_ops.fft_hilbert_transform(G, eps, w)
     assert approx_err(Lam2, direct) < 2e-13
     assert np.max(np.abs(Lam2 - Lam)) <= 1e-13 * max(np.max(np.abs(Lam)), 1.0)
+
+
+@pytest.mark.parametrize("NE", [1500, 4096])
+def test_fft_hilbert_in_place_on_device(gpu_ops, orc, NE):
+    """Lam == Gam through the device entry: the transform of the original
+    field (the half-length kernel, which reads the field twice, is not used
+    for an overlapping output)."""
+    import ctypes
+
+    import torch
+    from qclb200 import _lib
+
+    rng = np.random.default_rng(NE + 1)
+    ncols = 5
+    eps = np.linspace(-1.3, 0.9, NE)
+    w = np.full(NE, eps[1] - eps[0])
+    G = rng.standard_normal((ncols, NE)) + 1j * rng.standard_normal((ncols, NE))
+    dev = torch.device("cuda", 0)
+    buf = torch.tensor(G, dtype=torch.complex128, device=dev)
+    sep = torch.empty_like(buf)
+    wd = torch.tensor(w, dtype=torch.float64, device=dev)
+    P = ctypes.c_void_p
+    st = P(torch.cuda.current_stream().cuda_stream)
+    L = _lib.lib()
+    de = float(eps[1] - eps[0])
+    _lib.check(L.qcl_dev_fft_hilbert_transform(st, _lib.QCL_C128, NE, ncols, de, P(wd.data_ptr()),
+                                               P(buf.data_ptr()), P(sep.data_ptr()), None))
+    _lib.check(L.qcl_dev_fft_hilbert_transform(st, _lib.QCL_C128, NE, ncols, de, P(wd.data_ptr()),
+                                               P(buf.data_ptr()), P(buf.data_ptr()), None))
+    torch.cuda.synchronize()
+    direct = orc.direct_hilbert(np.asfortranarray(G.T), eps, w)
+    assert approx_err(sep.cpu().numpy().T, direct) < 2e-13
+    assert approx_err(buf.cpu().numpy().T, direct) < 2e-13
 
 
 @pytest.mark.parametrize("NE", [400, 4096])

@@ -25,7 +25,9 @@ def _compare(hist_o, hist_g, rtol=1e-9):
         for k in KEYS:
             a, b = ro[k], rg[GPU_KEYS[k]]
             scale = max(abs(a), abs(b))
-            tol = rtol * scale + (1e-14 if k in ("rD",) else 1e-15)
+            # r_D and r_A sit at roundoff (~1e-16..1e-15): their values depend
+            # on the summation / FFT pass order, so they get a 1e-14 floor
+            tol = rtol * scale + (1e-14 if k in ("rD", "rA") else 1e-15)
             assert abs(a - b) <= tol, (ro["nu"], k, a, b)
         np.testing.assert_allclose(rg["populations"], ro["populations"], rtol=1e-9, atol=1e-13)
         assert rg["r_PSD"] == pytest.approx(ro["rPSD"], abs=1e-12)

@@ -182,7 +182,8 @@ def test_scba_with_model_switches_matches_oracle(gpu_ops, orc, switches):
     for ro, rg in zip(hist_o, hist_g):
         for ko, kg in (("J", "J"), ("rSigma", "r_Sigma"), ("lam", "lam"), ("rK", "r_K"), ("rA", "r_A")):
             a, b = ro[ko], rg[kg]
-            assert abs(a - b) <= 1e-9 * max(abs(a), abs(b)) + 1e-15, (ro["nu"], ko, a, b)
+            floor = 1e-14 if ko == "rA" else 1e-15  # r_A sits at roundoff
+            assert abs(a - b) <= 1e-9 * max(abs(a), abs(b)) + floor, (ro["nu"], ko, a, b)
         np.testing.assert_allclose(rg["populations"], ro["populations"], rtol=1e-9, atol=1e-13)
         if switches.get("retarded_real_part") == "drop":
             assert rg["r_roundoff"] == 0.0

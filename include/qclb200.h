@@ -109,7 +109,8 @@ int qcl_fft_hilbert_transform(int precision, int NE, size_t ncols, const double*
 
 /* Device variant (asynchronous on `stream`): de is the uniform energy
  * spacing, wE a device array.  If roundoff_sums != NULL it receives (device,
- * 2 doubles) sum |Lam_2L - Lam_L|^2 and sum |Lam_L|^2. */
+ * 2 doubles) sum |Lam_2L - Lam_L|^2 and sum |Lam_L|^2.  Lam may be Gam (in
+ * place). */
 int qcl_dev_fft_hilbert_transform(void* stream, int precision, int NE, size_t ncols, double de, const double* wE,
                                   const void* Gam, void* Lam, double* roundoff_sums);
 

@@ -556,7 +556,7 @@ def scba_all_mechanisms(torch, NE_=1024, Nk_=32, Nb_=16, warm=2, timed=7):
     """SCBA iterations/s with every scattering mechanism (LO with its four
     shifts, acoustic, impurity, IFR, alloy): plain FP64 against mixed
     precision (complex64 storage, FP64 elimination and reductions, dense
-    contractions on the tensor cores in 3xTF32), and the largest relative
+    contractions on the tensor cores as scaled FP16 hi/lo pairs), and the largest relative
     difference of the current density J over the same iterations."""
     import numpy as np
     from qclb200.problem import small_problem
@@ -627,7 +627,7 @@ def run_capture(kind):
     elif kind == "tcgemm":
         # complex64 dense contraction on the tensor cores: N_E = 1024 rows,
         # N_k N_b^2 = 16 x 16^2 = 4096 complex columns (a 1024 x 8192 x 8192
-        # real GEMM in 3xTF32)
+        # real GEMM of scaled FP16 hi/lo pairs, three MMA passes)
         import numpy as np
         from qclb200 import operators
         from qclb200.problem import Mechanism

@@ -453,20 +453,14 @@ int qcl_static_contraction(int precision, const qcl_mechanism* op, int NE, int N
   DevBuf st;
   if ((s = st.upload(nullptr, 2 * sizeof(int)))) return s;
   QCL_CUDA_CHECK(cudaMemset(st.p, 0, 2 * sizeof(int)));
-  float* bhi = nullptr;
-  float* blo = nullptr;
+  void* bop = nullptr;
   struct TcFree {
-    float** a;
-    float** b;
-    ~TcFree() {
-      cudaFree(*a);
-      cudaFree(*b);
-    }
-  } tc_free{&bhi, &blo};
+    void** a;
+    ~TcFree() { cudaFree(*a); }
+  } tc_free{&bop};
   if (op->kind == QCL_KERNEL_DENSE && sp == QCL_C64) {  // complex64: tensor-core operand
-    if ((s = tc_build_operator(Nk * (int)N2, Nk, mat.p, (const double*)dwk.p, &bhi, &blo, 0))) return s;
-    k.tc_bhi = bhi;
-    k.tc_blo = blo;
+    if ((s = tc_build_operator(Nk * (int)N2, Nk, mat.p, (const double*)dwk.p, &bop, 0))) return s;
+    k.tc_bop = bop;
     k.status = (int*)st.p;
   }
   if ((s = dG.upload(G, nb))) return s;

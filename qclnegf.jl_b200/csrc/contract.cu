@@ -440,9 +440,8 @@ static int contraction_t(const KernelOpDev& op, int NE, int Nk, int N, const dou
   }
   if (op.kind == QCL_KERNEL_DENSE) {
     const int Nc = Nk * N2;
-    if (sizeof(R) == 4 && op.tc_bhi)  // complex64 fields: tensor cores (3xTF32)
-      return launch_tc_dense_contraction(NE, Nc, op.tc_bhi, op.tc_blo, Gv, Sv, alpha_q, beta, (float*)work,
-                                         op.status, st);
+    if (sizeof(R) == 4 && op.tc_bop)  // complex64 fields: tensor cores (scaled FP16 hi/lo)
+      return launch_tc_dense_contraction(NE, Nc, op.tc_bop, Gv, Sv, alpha_q, beta, (float*)work, op.status, st);
     if (sizeof(R) == 8) {  // complex128: FP64 tensor path (DMMA)
       DmArgs d{NE, Nc, Nc, (const Cx<double>*)Gv, NEl, wk, Nk, (const Cx<double>*)op.matrix, Nc, (Cx<double>*)Sv, NEl,
                alpha_q, beta};
@@ -522,7 +521,7 @@ static int contraction_t(const KernelOpDev& op, int NE, int Nk, int N, const dou
 
 size_t contraction_work_elems(const KernelOpDev& op, int NE, int Nk, int N) {
   if (op.kind == QCL_KERNEL_MOMENTUM_INDEPENDENT) return (size_t)NE * N * N;
-  if (op.kind == QCL_KERNEL_DENSE && op.tc_bhi) return (tc_a_work_floats(NE, Nk * N * N) + 1) / 2;  // complex64 units
+  if (op.kind == QCL_KERNEL_DENSE && op.tc_bop) return (tc_a_work_floats(NE, Nk * N * N) + 1) / 2;  // complex64 units
   if (op.kind == QCL_KERNEL_IFR) return 2 * (size_t)NE * op.J * Nk;
   if (op.kind == QCL_KERNEL_LOW_RANK) return (size_t)NE * op.J;
   return 0;

@@ -105,19 +105,17 @@ struct KernelOpDev {
   const void* left = nullptr;    // IFR (N^2, J); low rank (Nk N^2, rank)
   const void* right = nullptr;   // IFR (J, N^2); low rank right_adjoint (rank, Nk N^2)
   const void* radial = nullptr;  // (Nk, Nk)
-  // dense operators, complex64 fields: tensor-core (3xTF32) operand prepared by
-  // tc_build_operator; when set, the contraction runs on tcgen05
-  const float* tc_bhi = nullptr;
-  const float* tc_blo = nullptr;
+  // dense operators, complex64 fields: tensor-core operand (scaled FP16 hi/lo
+  // pair) prepared by tc_build_operator; when set, the contraction runs on tcgen05
+  const void* tc_bop = nullptr;
   int* status = nullptr;  // device status word for bounded-wait timeouts
 };
 size_t contraction_work_elems(const KernelOpDev& op, int NE, int Nk, int N);
 // tensor-core dense contraction (tc_gemm.cu)
-int tc_build_operator(int Nc, int Nk, const void* Mop_c64, const double* wk, float** Bhi, float** Blo,
-                      cudaStream_t st);
+int tc_build_operator(int Nc, int Nk, const void* Mop_c64, const double* wk, void** Bop, cudaStream_t st);
 size_t tc_a_work_floats(int NE, int Nc);
-int launch_tc_dense_contraction(int NE, int Nc, const float* Bhi, const float* Blo, const void* G, void* S,
-                                double alpha, double beta, float* awork, int* status, cudaStream_t st);
+int launch_tc_dense_contraction(int NE, int Nc, const void* Bop, const void* G, void* S, double alpha, double beta,
+                                float* awork, int* status, cudaStream_t st);
 int launch_contraction(int precision, const KernelOpDev& op, int NE, int Nk, int N, const double* wk, const void* G,
                        void* S, double alpha_q, double beta, void* work, cudaStream_t st);
 

@@ -42,13 +42,11 @@ struct Mech {
   void* left = nullptr;
   void* right = nullptr;
   void* radial = nullptr;
-  float* tc_bhi = nullptr;  // dense operator prepared for the tensor cores (complex64 fields)
-  float* tc_blo = nullptr;
+  void* tc_bop = nullptr;  // dense operator prepared for the tensor cores (complex64 fields)
   int* status = nullptr;
   KernelOpDev view() const {
     KernelOpDev k;
-    k.tc_bhi = tc_bhi;
-    k.tc_blo = tc_blo;
+    k.tc_bop = tc_bop;
     k.status = status;
     k.kind = kind;
     k.J = J;
@@ -211,8 +209,7 @@ void scba_destroy(ScbaCtx* c) {
     cudaFree(m.left);
     cudaFree(m.right);
     cudaFree(m.radial);
-    cudaFree(m.tc_bhi);
-    cudaFree(m.tc_blo);
+    cudaFree(m.tc_bop);
   }
   for (void* p : c->state) cudaFree(p);
   for (void* p : c->cand) cudaFree(p);
@@ -359,7 +356,7 @@ int scba_create(const qcl_scba_problem* p, const qcl_mechanism* mechs, ScbaCtx**
       const size_t nc = (size_t)c->Nk * N2;
       TRY(upload_op(c, &d.matrix, q.matrix, nc * nc));
       if (c->precision != QCL_C128)
-        TRY(tc_build_operator((int)nc, c->Nk, d.matrix, c->wk, &d.tc_bhi, &d.tc_blo, c->st));
+        TRY(tc_build_operator((int)nc, c->Nk, d.matrix, c->wk, &d.tc_bop, c->st));
     } else if (q.kind == QCL_KERNEL_IFR) {
       if (q.J < 1) TRY((set_last_error("IFR operator needs J >= 1"), QCL_ARG));
       TRY(upload_op(c, &d.left, q.left, (size_t)N2 * q.J));

@@ -10,28 +10,34 @@
 //   A[e][kk]  = G[e,k] parts                       (M = N_E rows, K-contiguous)
 //   B[nn][kk] = wk * [[Re M, -Im M], [Im M, Re M]]  (built once per operator)
 //   S[e,j] = alpha q (C[e][2j] + i C[e][2j+1]) + beta S[e,j],  C = A B^T.
-// Both operands are split into TF32 parts x = hi + lo (hi = tf32(x),
-// lo = tf32(x - hi)) and C accumulates A_hi B_hi + A_hi B_lo + A_lo B_hi in
-// FP32 (the 3xTF32 scheme: ~FP32 accuracy at tensor-core rate).
 //
-// Kernel: one CTA of 256 threads per 128 x 256 output tile, 1 CTA per SM.
-// K advances in blocks of 32 (one 128-byte swizzle row per operand row);
-// all threads stage a block with cp.async into 1024-byte aligned,
-// 128B-swizzled K-major tiles (two stages); thread 0 issues the 3 x 4
-// tcgen05.mma (M=128, N=256, K=8, kind::tf32) of a block into one of two
-// tensor-memory accumulators (128 lanes x 256 FP32 columns each) and commits
-// them to the stage's mbarrier.
+// Operands: FP16 pairs.  Each row of A is scaled by a power of two s_e so
+// that its largest entry lies in [2^13, 2^14), B by one power of two s_B, and
+// every value is split into x = hi + lo with hi = fp16(x), lo = fp16(x - hi)
+// (11 + 11 significant bits, as TF32 hi/lo).  C accumulates A_hi B_hi +
+// A_hi B_lo + A_lo B_hi in FP32 (relative error ~3 * 2^-22 per product; a
+// value below 2^-28 of its row maximum keeps an absolute error under 2^-38
+// of it) and the epilogue divides by s_e s_B (exact).  Against TF32 hi/lo the
+// operands are half the bytes and the MMA rate is twice as high.
 //
-// Accumulation: the tensor core's FP32 accumulation truncates (measured here:
-// a relative bias of about -0.17 ulp per accumulate, -6.6e-5 after K = 8192).
-// So every K block starts a fresh accumulator, and while the tensor core
-// fills one buffer the 8 warps read the other (tcgen05.ld, warp w: lanes
-// 32 (w % 4) .. + 31, columns 128 (w / 4) .. + 127) and add it to per-thread
-// FP32 running sums with IEEE rounding; an mbarrier (256 arrivals) hands the
-// buffer back.  Each truncated chain is then 12 accumulates long.
+// Kernel: one CTA of 320 threads per 128 x BN output tile (BN = 256 or 224),
+// 1 CTA per SM.  K advances in blocks of 32 (one 64-byte swizzle row per
+// operand row).  Warp 8 streams the blocks with TMA into a 4-stage ring of
+// 64B-swizzled K-major tiles; warp 9 issues the 3 x 2 tcgen05.mma (M = 128,
+// N = BN, K = 16, kind::f16) of a block into one of two tensor-memory
+// accumulators (128 lanes x BN FP32 columns each).
+//
+// Accumulation: the tensor core's FP32 accumulation truncates (measured: a
+// relative bias of about -0.17 ulp per accumulate).  So every second K block
+// starts a fresh accumulator, and while the tensor core fills one buffer the
+// 8 drain warps read the other (tcgen05.ld, warp w: lanes 32 (w % 4) .. + 31,
+// columns BN/2 (w / 4) .. ) and add it to per-thread FP32 running sums with
+// IEEE rounding; an mbarrier (256 arrivals) hands the buffer back.  Each
+// truncated chain is then 12 MMAs long.
 // Every wait is bounded: a wait that gives up records QCL_TIMEOUT, the CTA
 // then waits (bounded) for its own MMAs, releases its tensor memory and ends.
 #include <cuda.h>  // CUtensorMap (the encoder is reached through cudaGetDriverEntryPoint)
+#include <cuda_fp16.h>
 
 #include <mutex>
 
@@ -39,17 +45,17 @@
 
 namespace qcl {
 
-constexpr int TC_BM = 128, TC_BN = 256, TC_BK = 16;  // TC_BN: the widest tile (operand padding)
+constexpr int TC_BM = 128, TC_BN = 256, TC_BK = 32;  // TC_BN: the widest tile (operand padding); TC_BK fp16
 constexpr int TC_STAGES = 4;      // operand stages: the producer runs up to 3 blocks ahead
 constexpr int TC_ACC_KB = 2;      // K blocks per tensor-memory accumulation (12 MMAs)
 constexpr int TC_DRAIN_WARPS = 8; // warps that read accumulators out and write the tile
 constexpr int TC_THREADS = 32 * (TC_DRAIN_WARPS + 2);  // + producer warp + MMA warp
-constexpr int TC_A_BYTES = TC_BM * TC_BK * 4;   // 8 KiB per A part
+constexpr int TC_A_BYTES = TC_BM * TC_BK * 2;   // 8 KiB per A part
 constexpr int TC_BAR_BYTES = 128;
 constexpr uint32_t TC_TMEM_COLS = 512;  // two accumulators of up to 256 columns
 // Per tile width BN (the N of one MMA): B part bytes, stage bytes, shared memory.
 template <int BN> struct TcShape {
-  static constexpr int B_BYTES = BN * TC_BK * 4;
+  static constexpr int B_BYTES = BN * TC_BK * 2;
   static constexpr int STAGE_BYTES = 2 * TC_A_BYTES + 2 * B_BYTES;
   static constexpr int SMEM_BYTES = TC_STAGES * STAGE_BYTES + 1024 + TC_BAR_BYTES;
   static constexpr int CH = BN / 2;                   // accumulator columns per drain warp
@@ -65,9 +71,9 @@ __device__ __forceinline__ uint64_t umma_desc_k_sw64(uint32_t saddr) {
   return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)1 << 16) | ((uint64_t)32 << 32) | ((uint64_t)1 << 46) |
          ((uint64_t)4 << 61);
 }
-// Instruction descriptor: D f32, A/B tf32, both K-major, N = BN, M = 128.
+// Instruction descriptor (kind::f16): D f32, A/B f16, both K-major, N = BN, M = 128.
 template <int BN> __device__ __forceinline__ constexpr uint32_t tc_idesc() {
-  return (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(BN >> 3) << 17) | ((uint32_t)(TC_BM >> 4) << 24);
+  return (1u << 4) | (0u << 7) | (0u << 10) | ((uint32_t)(BN >> 3) << 17) | ((uint32_t)(TC_BM >> 4) << 24);
 }
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
@@ -108,7 +114,7 @@ __device__ __forceinline__ void tc_mma(uint32_t tmem_d, uint64_t adesc, uint64_t
                                        uint32_t accumulate) {
   asm volatile(
       "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
-      " tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n}" ::"r"(tmem_d),
+      " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n}" ::"r"(tmem_d),
       "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate), "r"(0), "r"(0), "r"(0), "r"(0)
       : "memory");
 }
@@ -143,10 +149,12 @@ struct TcMaps {  // TMA descriptors of the four operand parts (K-contiguous rows
 struct TcArgs {
   int M;        // rows of C actually stored (N_E)
   int Ncols;    // real columns of C actually stored (2 Nc)
-  int Kpad;     // padded real K (multiple of 32)
+  int Kpad;     // padded real K (multiple of TC_BK)
   Cx<float>* S; // S[e + NE j], j < Ncols / 2
   int NE;
   double alpha, beta;
+  const float* ainv;  // 1 / s_e per row of A
+  const float* binv;  // 1 / s_B (device scalar)
   int* status;
 };
 
@@ -239,7 +247,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) tc_gemm_kernel(const __grid_con
         const uint32_t dacc = tmem + (uint32_t)(b * BN);
         constexpr uint32_t idesc = tc_idesc<BN>();
 #pragma unroll
-        for (int ks = 0; ks < TC_BK / 8; ++ks) {  // K = 8 tf32 = 32 bytes per MMA
+        for (int ks = 0; ks < TC_BK / 16; ++ks) {  // K = 16 fp16 = 32 bytes per MMA
           const uint32_t off = ks * 32;
           const uint64_t ah = umma_desc_k_sw64(tAh + off), al = umma_desc_k_sw64(tAl + off);
           const uint64_t bh = umma_desc_k_sw64(tBh + off), bl = umma_desc_k_sw64(tBl + off);
@@ -292,13 +300,16 @@ __global__ void __launch_bounds__(TC_THREADS, 1) tc_gemm_kernel(const __grid_con
     }
     const int e = m0 + (warp & 3) * 32 + lane;
     if (ok && e < p.M) {
-      const float al = (float)p.alpha, be = (float)p.beta;
+      // undo the operand scales (powers of two) and apply alpha in FP64, so that
+      // no intermediate under- or overflows: one rounding to FP32, as before
+      const double al = p.alpha * (double)p.ainv[e] * (double)__ldg(p.binv);
+      const float be = (float)p.beta;
 #pragma unroll
       for (int q = 0; q < CH / 2; ++q) {
         const int nn = n0 + cbase + 2 * q;
         if (nn >= p.Ncols) continue;
         Cx<float>* dst = p.S + (size_t)e + (size_t)p.NE * (size_t)(nn >> 1);
-        const float re = al * sum[2 * q], im = al * sum[2 * q + 1];
+        const float re = (float)(al * (double)sum[2 * q]), im = (float)(al * (double)sum[2 * q + 1]);
         if (p.beta == 0.0) {
           *dst = cx<float>(re, im);
         } else {
@@ -318,18 +329,53 @@ __global__ void __launch_bounds__(TC_THREADS, 1) tc_gemm_kernel(const __grid_con
 // ---------------------------------------------------------------------------
 // Operand preparation
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ float tf32_round(float x) {
-  uint32_t r;
-  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
-  return __uint_as_float(r);
+// Power-of-two scale that takes a largest magnitude mx into [2^13, 2^14)
+// (1 for zero or non-finite mx; the exponent is clamped to keep the scale and
+// its inverse normal FP32 numbers).
+__device__ __forceinline__ float tc_scale_for(float mx) {
+  if (!(mx > 0.0f) || !isfinite(mx)) return 1.0f;
+  int ex;
+  frexpf(mx, &ex);  // mx = f 2^ex, f in [0.5, 1)
+  const int sh = min(max(14 - ex, -120), 120);
+  return ldexpf(1.0f, sh);
+}
+// x = hi + lo in FP16 (x already scaled); x - hi is exact in FP32.
+__device__ __forceinline__ void split_f16(float x, __half& hi, __half& lo) {
+  hi = __float2half_rn(x);
+  lo = __float2half_rn(x - __half2float(hi));
 }
 
-// A[e][2k + c] = part c of G[e + NE k] for k < Nc (zero in the padding),
-// split into tf32 hi / lo; a 32 x 32 (e, kk) tile is transposed through
+// Row scales of A: s_e from max_kk |A[e][kk]| (rows past N_E: 1); ainv = 1 / s_e.
+// 32 rows per CTA, coalesced along e.
+__global__ void tc_row_scale_kernel(int NE, int Nc, int Mpad, const Cx<float>* __restrict__ G,
+                                    float* __restrict__ ascale, float* __restrict__ ainv) {
+  __shared__ float red[8][32];
+  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;  // 32 x 8 threads
+  const int e = blockIdx.x * 32 + tx;
+  float mx = 0.0f;
+  if (e < NE)
+    for (int k = ty; k < Nc; k += 8) {
+      const Cx<float> g = G[(size_t)e + (size_t)NE * k];
+      mx = fmaxf(mx, fmaxf(fabsf(g.x), fabsf(g.y)));  // fmaxf drops NaN: caught below
+      if (!isfinite(g.x) || !isfinite(g.y)) mx = INFINITY;
+    }
+  red[ty][tx] = mx;
+  __syncthreads();
+  if (ty == 0 && e < Mpad) {
+    for (int q = 1; q < 8; ++q) mx = fmaxf(mx, red[q][tx]);
+    const float sc = tc_scale_for(mx);
+    ascale[e] = sc;
+    ainv[e] = 1.0f / sc;
+  }
+}
+
+// A[e][2k + c] = s_e * part c of G[e + NE k] for k < Nc (zero in the padding),
+// split into fp16 hi / lo; a 32 x 32 (e, kk) tile is transposed through
 // shared memory so that both the E-fastest reads and the K-contiguous writes
 // are coalesced.
 __global__ void tc_split_a_kernel(int NE, int Nc, int Mpad, int Kpad, const Cx<float>* __restrict__ G,
-                                  float* __restrict__ Ahi, float* __restrict__ Alo) {
+                                  const float* __restrict__ ascale, __half* __restrict__ Ahi,
+                                  __half* __restrict__ Alo) {
   __shared__ float tile[32][33];
   const int e0 = blockIdx.x * 32, kk0 = blockIdx.y * 32;
   const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;  // 32 x 8 threads
@@ -340,7 +386,7 @@ __global__ void tc_split_a_kernel(int NE, int Nc, int Mpad, int Kpad, const Cx<f
     const int k = kk >> 1;
     if (e < NE && k < Nc) {
       const Cx<float> g = G[(size_t)e + (size_t)NE * k];
-      v = (kk & 1) ? g.y : g.x;
+      v = ((kk & 1) ? g.y : g.x) * ascale[e];
     }
     tile[r][tx] = v;
   }
@@ -348,34 +394,49 @@ __global__ void tc_split_a_kernel(int NE, int Nc, int Mpad, int Kpad, const Cx<f
   for (int r = ty; r < 32; r += 8) {
     const int e = e0 + r, kk = kk0 + tx;
     if (e >= Mpad || kk >= Kpad) continue;
-    const float x = tile[tx][r];
-    const float hi = tf32_round(x);
     const size_t idx = (size_t)e * Kpad + kk;
-    Ahi[idx] = hi;
-    Alo[idx] = tf32_round(x - hi);
+    split_f16(tile[tx][r], Ahi[idx], Alo[idx]);
   }
 }
 
 // B[2j + c'][2k + c] from the complex operator M (column-major Nc x Nc,
 // complex64) and the momentum weights wk[k % Nk]:
 //   [[Re, -Im], [Im, Re]] * w  (rows c' = 0 real part of the output, 1 imaginary).
+__device__ __forceinline__ float tc_b_value(int nn, int kk, int Nc, int Nk, const Cx<float>* __restrict__ Mop,
+                                            const double* __restrict__ wk) {
+  const int j = nn >> 1, k = kk >> 1;
+  if (j >= Nc || k >= Nc) return 0.0f;
+  const Cx<float> m = Mop[(size_t)j + (size_t)Nc * k];
+  const float w = (float)wk[k % Nk];
+  const int cp = nn & 1, c = kk & 1;
+  const float val = (cp == c) ? m.x : (cp == 0 ? -m.y : m.y);
+  return w * val;
+}
+// max |B| into *mxbits (non-negative FP32 bits order as unsigned integers;
+// a non-finite entry gives +inf).
+__global__ void tc_b_maxabs_kernel(int Nc, int Nk, const Cx<float>* __restrict__ Mop,
+                                   const double* __restrict__ wk, unsigned* __restrict__ mxbits) {
+  const long long n = (long long)Nc * Nc;
+  float mx = 0.0f;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const Cx<float> m = Mop[i];
+    const float w = fabsf((float)wk[(i / Nc) % Nk]);
+    const float a = fmaxf(fabsf(m.x), fabsf(m.y)) * w;
+    mx = isfinite(a) ? fmaxf(mx, a) : INFINITY;
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+  if ((threadIdx.x & 31) == 0) atomicMax(mxbits, __float_as_uint(mx));
+}
 __global__ void tc_build_b_kernel(int Nc, int Nk, int Npad, int Kpad, const Cx<float>* __restrict__ Mop,
-                                  const double* __restrict__ wk, float* __restrict__ Bhi, float* __restrict__ Blo) {
+                                  const double* __restrict__ wk, const unsigned* __restrict__ mxbits,
+                                  __half* __restrict__ Bhi, __half* __restrict__ Blo, float* __restrict__ binv) {
+  const float sc = tc_scale_for(__uint_as_float(*mxbits));
+  if (blockIdx.x == 0 && threadIdx.x == 0) *binv = 1.0f / sc;
   const long long n = (long long)Npad * Kpad;
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
     const int nn = (int)(i / Kpad), kk = (int)(i % Kpad);
-    const int j = nn >> 1, k = kk >> 1;
-    float v = 0.0f;
-    if (j < Nc && k < Nc) {
-      const Cx<float> m = Mop[(size_t)j + (size_t)Nc * k];
-      const float w = (float)wk[k % Nk];
-      const int cp = nn & 1, c = kk & 1;
-      const float val = (cp == c) ? m.x : (cp == 0 ? -m.y : m.y);
-      v = w * val;
-    }
-    const float hi = tf32_round(v);
-    Bhi[i] = hi;
-    Blo[i] = tf32_round(v - hi);
+    split_f16(sc * tc_b_value(nn, kk, Nc, Nk, Mop, wk), Bhi[i], Blo[i]);
   }
 }
 
@@ -386,20 +447,30 @@ int tc_dims(int NE, int Nc, int* Mpad, int* Npad, int* Kpad) {
   return QCL_OK;
 }
 
+// A work area, in floats: fp16 hi and lo (Mpad x Kpad each), then the row
+// scales and their inverses (Mpad each).
 size_t tc_a_work_floats(int NE, int Nc) {
   int Mpad, Npad, Kpad;
   tc_dims(NE, Nc, &Mpad, &Npad, &Kpad);
-  return 2 * (size_t)Mpad * Kpad;
+  return (size_t)Mpad * Kpad + 2 * (size_t)Mpad;
 }
 
-int tc_build_operator(int Nc, int Nk, const void* Mop_c64, const double* wk, float** Bhi, float** Blo,
-                      cudaStream_t st) {
+// Prepared operator: one allocation holding 1 / s_B (256 bytes reserved), the
+// max-|B| word, then B_hi and B_lo (Npad x Kpad fp16 each).  *Bop receives it.
+int tc_build_operator(int Nc, int Nk, const void* Mop_c64, const double* wk, void** Bop, cudaStream_t st) {
   int Mpad, Npad, Kpad;
   tc_dims(1, Nc, &Mpad, &Npad, &Kpad);
   const size_t n = (size_t)Npad * Kpad;
-  QCL_CUDA_CHECK(cudaMalloc(Bhi, n * sizeof(float)));
-  QCL_CUDA_CHECK(cudaMalloc(Blo, n * sizeof(float)));
-  tc_build_b_kernel<<<148 * 8, 256, 0, st>>>(Nc, Nk, Npad, Kpad, (const Cx<float>*)Mop_c64, wk, *Bhi, *Blo);
+  QCL_CUDA_CHECK(cudaMalloc(Bop, 256 + 2 * n * sizeof(__half)));
+  char* b = (char*)*Bop;
+  float* binv = (float*)b;
+  unsigned* mxbits = (unsigned*)(b + 16);
+  __half* Bhi = (__half*)(b + 256);
+  QCL_CUDA_CHECK(cudaMemsetAsync(mxbits, 0, sizeof(unsigned), st));
+  tc_b_maxabs_kernel<<<148 * 4, 256, 0, st>>>(Nc, Nk, (const Cx<float>*)Mop_c64, wk, mxbits);
+  QCL_LAUNCH_CHECK("tc_b_maxabs_kernel");
+  tc_build_b_kernel<<<148 * 8, 256, 0, st>>>(Nc, Nk, Npad, Kpad, (const Cx<float>*)Mop_c64, wk, mxbits, Bhi,
+                                             Bhi + n, binv);
   QCL_LAUNCH_CHECK("tc_build_b_kernel");
   return QCL_OK;
 }
@@ -421,18 +492,18 @@ static TensorMapEncodeTiled tensor_map_encoder() {
   return fn;
 }
 
-// K-contiguous FP32 matrix [rows][Kpad] in boxes of TC_BK x box_rows, 64B swizzle.
-static int make_operand_map(CUtensorMap* m, const float* ptr, int rows, int Kpad, int box_rows) {
+// K-contiguous FP16 matrix [rows][Kpad] in boxes of TC_BK x box_rows, 64B swizzle.
+static int make_operand_map(CUtensorMap* m, const __half* ptr, int rows, int Kpad, int box_rows) {
   TensorMapEncodeTiled enc = tensor_map_encoder();
   if (!enc) {
     set_last_error("cuTensorMapEncodeTiled is not available from the driver");
     return QCL_CUDA;
   }
   const cuuint64_t dims[2] = {(cuuint64_t)Kpad, (cuuint64_t)rows};
-  const cuuint64_t strides[1] = {(cuuint64_t)Kpad * sizeof(float)};
+  const cuuint64_t strides[1] = {(cuuint64_t)Kpad * sizeof(__half)};
   const cuuint32_t box[2] = {(cuuint32_t)TC_BK, (cuuint32_t)box_rows};
   const cuuint32_t es[2] = {1, 1};
-  const CUresult r = enc(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, (void*)ptr, dims, strides, box, es,
+  const CUresult r = enc(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT16, 2, (void*)ptr, dims, strides, box, es,
                          CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                          CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   if (r != CUDA_SUCCESS) {
@@ -477,15 +548,22 @@ template <int BN> static int launch_tc_t(const TcMaps& maps, const TcArgs& a, in
   return QCL_OK;
 }
 
-int launch_tc_dense_contraction(int NE, int Nc, const float* Bhi, const float* Blo, const void* G, void* S,
-                                double alpha, double beta, float* awork, int* status, cudaStream_t st) {
+int launch_tc_dense_contraction(int NE, int Nc, const void* Bop, const void* G, void* S, double alpha, double beta,
+                                float* awork, int* status, cudaStream_t st) {
   int Mpad, Npad, Kpad;
   tc_dims(NE, Nc, &Mpad, &Npad, &Kpad);
-  float* Ahi = awork;
-  float* Alo = awork + (size_t)Mpad * Kpad;
+  __half* Ahi = (__half*)awork;
+  __half* Alo = Ahi + (size_t)Mpad * Kpad;
+  float* ascale = (float*)(Alo + (size_t)Mpad * Kpad);
+  float* ainv = ascale + Mpad;
+  tc_row_scale_kernel<<<Mpad / 32, 256, 0, st>>>(NE, Nc, Mpad, (const Cx<float>*)G, ascale, ainv);
+  QCL_LAUNCH_CHECK("tc_row_scale_kernel");
   dim3 sg((Mpad + 31) / 32, (Kpad + 31) / 32);
-  tc_split_a_kernel<<<sg, 256, 0, st>>>(NE, Nc, Mpad, Kpad, (const Cx<float>*)G, Ahi, Alo);
+  tc_split_a_kernel<<<sg, 256, 0, st>>>(NE, Nc, Mpad, Kpad, (const Cx<float>*)G, ascale, Ahi, Alo);
   QCL_LAUNCH_CHECK("tc_split_a_kernel");
+  const char* b = (const char*)Bop;
+  const __half* Bhi = (const __half*)(b + 256);
+  const __half* Blo = Bhi + (size_t)Npad * Kpad;
   const int mtiles = Mpad / TC_BM;
   const int bn = tc_pick_bn(mtiles, 2 * Nc);
   TcMaps maps;
@@ -495,7 +573,7 @@ int launch_tc_dense_contraction(int NE, int Nc, const float* Bhi, const float* B
   // B rows past Npad (the last tile of a narrower width) read the zero fill
   if ((s = make_operand_map(&maps.bhi, Bhi, Npad, Kpad, bn))) return s;
   if ((s = make_operand_map(&maps.blo, Blo, Npad, Kpad, bn))) return s;
-  TcArgs a{NE, 2 * Nc, Kpad, (Cx<float>*)S, NE, alpha, beta, status};
+  TcArgs a{NE, 2 * Nc, Kpad, (Cx<float>*)S, NE, alpha, beta, ainv, (const float*)b, status};
   if (bn == 224) return launch_tc_t<224>(maps, a, mtiles, st);
   return launch_tc_t<256>(maps, a, mtiles, st);
 }

@@ -318,9 +318,9 @@ def test_batched_hermitian_eigvals_match_numpy(gpu_ops, n):
 
 @pytest.mark.parametrize("NE,Nk,Nb,beta", [(37, 4, 4, 0.0), (200, 3, 3, 1.0), (129, 5, 4, 0.5)])
 def test_dense_contraction_tensor_cores_c64(gpu_ops, orc, NE, Nk, Nb, beta):
-    # complex64 dense contraction on tcgen05 (3xTF32, FP32 accumulation) against
-    # the FP64 literal six-index map; ragged N_E and N_k N_b^2 exercise the
-    # zero padding of the 128 x 256 x 32 tiles
+    # complex64 dense contraction on tcgen05 (scaled FP16 hi/lo operands, FP32
+    # accumulation) against the FP64 literal six-index map; ragged N_E and
+    # N_k N_b^2 exercise the zero padding of the 128 x 256 x 32 tiles
     from qclb200.problem import small_problem
 
     pr = small_problem(NE=NE, Nk=Nk, Nb=Nb, mechanisms=("impurity",))
@@ -332,6 +332,29 @@ def test_dense_contraction_tensor_cores_c64(gpu_ops, orc, NE, Nk, Nb, beta):
     lit = orc.contraction_literal(mech.literal_kernel(pr.Nk, pr.Nb), G, pr.wk, 1.3 * mech.q) + beta * S0
     assert got.dtype == np.complex64
     assert approx_err(got, lit) < 2e-6
+
+
+def test_dense_contraction_tensor_cores_dynamic_range(gpu_ops, orc):
+    # FP16 operand pairs need the per-row scale of the field and the operator
+    # scale: rows from 1e-15 to 1e20, entries spread over 1e6 inside a row, an
+    # operator scaled by 1e-9 (outputs stay normal FP32 numbers, >= ~1e-27);
+    # every row keeps its FP32-level relative error
+    from qclb200.problem import small_problem
+
+    pr = small_problem(NE=150, Nk=3, Nb=4, mechanisms=("impurity",))
+    mech = pr.mechanisms[0]
+    mech.matrix = np.asfortranarray(mech.matrix * 1e-9)
+    rng = np.random.default_rng(99)
+    G = _rand_field(rng, pr.shape)
+    G *= 10.0 ** rng.uniform(-6.0, 0.0, G.shape)
+    G *= (10.0 ** rng.uniform(-15.0, 20.0, pr.NE))[:, None, None, None]
+    G = np.asfortranarray(G)
+    got = gpu_ops.production_static_contraction(mech, G, pr.wk, precision="c64").astype(np.complex128)
+    lit = orc.contraction_literal(mech.literal_kernel(pr.Nk, pr.Nb), G, pr.wk, mech.q)
+    d = (got - lit).reshape(pr.NE, -1)
+    rel = np.linalg.norm(d, axis=1) / np.linalg.norm(lit.reshape(pr.NE, -1), axis=1)
+    assert np.all(np.isfinite(got))
+    assert float(np.max(rel)) < 2e-6
 
 
 def test_dense_contraction_tensor_cores_no_accumulation_bias(gpu_ops):

@@ -412,10 +412,12 @@ template <typename R> struct ResultOut {
   }
 };
 
-// Registers are capped (128 per thread for complex128, 96 for complex64) so
-// that the register file holds as many CTAs as the shared memory does.
-template <typename R, int T> constexpr int hilbert_min_blocks() {
-  return 65536 / ((sizeof(R) == 8 ? 128 : 96) * T) < 1 ? 1 : 65536 / ((sizeof(R) == 8 ? 128 : 96) * T);
+// Registers are capped (128 per thread for complex128; 64 for complex64, 96
+// with verification, which spills at 64) so that the register file holds as
+// many CTAs as the shared memory does.
+template <typename R, bool VERIFY> constexpr int hilbert_reg_cap() { return sizeof(R) == 8 ? 128 : (VERIFY ? 96 : 64); }
+template <typename R, int T, bool VERIFY = false> constexpr int hilbert_min_blocks() {
+  return 65536 / (hilbert_reg_cap<R, VERIFY>() * T) < 1 ? 1 : 65536 / (hilbert_reg_cap<R, VERIFY>() * T);
 }
 // Shared memory of the one-pass kernel: the padded column, plus (with
 // verification) the length-L results y_L[e + NE - 1] kept for the comparison.
@@ -424,7 +426,7 @@ template <typename R, int L, bool VERIFY> constexpr size_t hilbert_smem_bytes() 
 }
 
 template <typename R, int L, bool VERIFY>
-__global__ void __launch_bounds__(FftPlan<L>::T, (hilbert_min_blocks<R, FftPlan<L>::T>()))
+__global__ void __launch_bounds__(FftPlan<L>::T, (hilbert_min_blocks<R, FftPlan<L>::T, VERIFY>()))
     hilbert_kernel(HilbertArgs<R> p) {
   constexpr int T = FftPlan<L>::T;
   constexpr int PER = (L / 2 + T - 1) / T;  // outputs per thread (NE <= L/2)

@@ -345,48 +345,52 @@ __device__ __forceinline__ void split_f16(float x, __half& hi, __half& lo) {
   lo = __float2half_rn(x - __half2float(hi));
 }
 
-// Row scales of A: s_e from max_kk |A[e][kk]| (rows past N_E: 1); ainv = 1 / s_e.
-// 32 rows per CTA, coalesced along e.
-__global__ void tc_row_scale_kernel(int NE, int Nc, int Mpad, const Cx<float>* __restrict__ G,
-                                    float* __restrict__ ascale, float* __restrict__ ainv) {
+// Row maxima of A: max_kk |A[e][kk]| into rowmax[e] as FP32 bits (non-negative
+// values order as unsigned integers; a non-finite entry gives +inf), which
+// the caller zeroes first.  A CTA covers 32 rows x 256 values of k (coalesced
+// along e); the atomic maximum is independent of the order.
+__global__ void tc_row_max_kernel(int NE, int Nc, const Cx<float>* __restrict__ G, unsigned* __restrict__ rowmax) {
   __shared__ float red[8][32];
   const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;  // 32 x 8 threads
   const int e = blockIdx.x * 32 + tx;
+  const int k0 = blockIdx.y * 256, k1 = min(Nc, k0 + 256);
   float mx = 0.0f;
   if (e < NE)
-    for (int k = ty; k < Nc; k += 8) {
+    for (int k = k0 + ty; k < k1; k += 8) {
       const Cx<float> g = G[(size_t)e + (size_t)NE * k];
-      mx = fmaxf(mx, fmaxf(fabsf(g.x), fabsf(g.y)));  // fmaxf drops NaN: caught below
-      if (!isfinite(g.x) || !isfinite(g.y)) mx = INFINITY;
+      const float a = fmaxf(fabsf(g.x), fabsf(g.y));
+      mx = (isfinite(g.x) && isfinite(g.y)) ? fmaxf(mx, a) : INFINITY;
     }
   red[ty][tx] = mx;
   __syncthreads();
-  if (ty == 0 && e < Mpad) {
+  if (ty == 0 && e < NE) {
     for (int q = 1; q < 8; ++q) mx = fmaxf(mx, red[q][tx]);
-    const float sc = tc_scale_for(mx);
-    ascale[e] = sc;
-    ainv[e] = 1.0f / sc;
+    atomicMax(rowmax + e, __float_as_uint(mx));
   }
 }
 
 // A[e][2k + c] = s_e * part c of G[e + NE k] for k < Nc (zero in the padding),
-// split into fp16 hi / lo; a 32 x 32 (e, kk) tile is transposed through
-// shared memory so that both the E-fastest reads and the K-contiguous writes
-// are coalesced.
+// split into fp16 hi / lo, s_e from the row maximum (rows past N_E: 1); the
+// first column of CTAs also writes ainv[e] = 1 / s_e.  A 32 x 32 (e, kk)
+// tile is transposed through shared memory so that both the E-fastest reads
+// and the K-contiguous writes are coalesced.
 __global__ void tc_split_a_kernel(int NE, int Nc, int Mpad, int Kpad, const Cx<float>* __restrict__ G,
-                                  const float* __restrict__ ascale, __half* __restrict__ Ahi,
-                                  __half* __restrict__ Alo) {
+                                  const unsigned* __restrict__ rowmax, __half* __restrict__ Ahi,
+                                  __half* __restrict__ Alo, float* __restrict__ ainv) {
   __shared__ float tile[32][33];
   const int e0 = blockIdx.x * 32, kk0 = blockIdx.y * 32;
   const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;  // 32 x 8 threads
+  const int er = e0 + tx;  // this thread's row in the read phase
+  const float sc = er < NE ? tc_scale_for(__uint_as_float(rowmax[er])) : 1.0f;
+  if (blockIdx.y == 0 && ty == 0 && er < Mpad) ainv[er] = 1.0f / sc;
   for (int r = ty; r < 32; r += 8) {
     // read: row kk = kk0 + r (fixed k, component), column e = e0 + tx (coalesced along e)
-    const int kk = kk0 + r, e = e0 + tx;
+    const int kk = kk0 + r;
     float v = 0.0f;
     const int k = kk >> 1;
-    if (e < NE && k < Nc) {
-      const Cx<float> g = G[(size_t)e + (size_t)NE * k];
-      v = ((kk & 1) ? g.y : g.x) * ascale[e];
+    if (er < NE && k < Nc) {
+      const Cx<float> g = G[(size_t)er + (size_t)NE * k];
+      v = ((kk & 1) ? g.y : g.x) * sc;
     }
     tile[r][tx] = v;
   }
@@ -448,7 +452,7 @@ int tc_dims(int NE, int Nc, int* Mpad, int* Npad, int* Kpad) {
 }
 
 // A work area, in floats: fp16 hi and lo (Mpad x Kpad each), then the row
-// scales and their inverses (Mpad each).
+// maxima (FP32 bits) and the inverse row scales (Mpad each).
 size_t tc_a_work_floats(int NE, int Nc) {
   int Mpad, Npad, Kpad;
   tc_dims(NE, Nc, &Mpad, &Npad, &Kpad);
@@ -554,12 +558,13 @@ int launch_tc_dense_contraction(int NE, int Nc, const void* Bop, const void* G, 
   tc_dims(NE, Nc, &Mpad, &Npad, &Kpad);
   __half* Ahi = (__half*)awork;
   __half* Alo = Ahi + (size_t)Mpad * Kpad;
-  float* ascale = (float*)(Alo + (size_t)Mpad * Kpad);
-  float* ainv = ascale + Mpad;
-  tc_row_scale_kernel<<<Mpad / 32, 256, 0, st>>>(NE, Nc, Mpad, (const Cx<float>*)G, ascale, ainv);
-  QCL_LAUNCH_CHECK("tc_row_scale_kernel");
+  unsigned* rowmax = (unsigned*)(Alo + (size_t)Mpad * Kpad);
+  float* ainv = (float*)(rowmax + Mpad);
+  QCL_CUDA_CHECK(cudaMemsetAsync(rowmax, 0, (size_t)Mpad * sizeof(unsigned), st));
+  tc_row_max_kernel<<<dim3(Mpad / 32, (Nc + 255) / 256), 256, 0, st>>>(NE, Nc, (const Cx<float>*)G, rowmax);
+  QCL_LAUNCH_CHECK("tc_row_max_kernel");
   dim3 sg((Mpad + 31) / 32, (Kpad + 31) / 32);
-  tc_split_a_kernel<<<sg, 256, 0, st>>>(NE, Nc, Mpad, Kpad, (const Cx<float>*)G, ascale, Ahi, Alo);
+  tc_split_a_kernel<<<sg, 256, 0, st>>>(NE, Nc, Mpad, Kpad, (const Cx<float>*)G, rowmax, Ahi, Alo, ainv);
   QCL_LAUNCH_CHECK("tc_split_a_kernel");
   const char* b = (const char*)Bop;
   const __half* Bhi = (const __half*)(b + 256);

@@ -59,6 +59,20 @@ template <int NP> struct ResScratch {
   Cx<double> u[NP], w[NP];
 };
 
+// Visits the (i, j), i, j < N, of an NP x NP tile: team thread tt takes the
+// padded indices tt, tt + TT, ... (compile-time trip count and index split,
+// no runtime division).
+template <int NP, int TT, typename F> __device__ __forceinline__ void tile_for(int N, int tt, F&& f) {
+#pragma unroll 1
+  for (int q = 0; q < (NP * NP + TT - 1) / TT; ++q) {
+    const int idx = tt + q * TT;
+    if (idx < NP * NP) {
+      const int i = idx % NP, j = idx / NP;
+      if (i < N && j < N) f(i, j);
+    }
+  }
+}
+
 // Team sum of two doubles (fixed order).
 template <int TT>
 __device__ __forceinline__ void team_sum2(double& a, double& b, int tt, double* scratch, int team) {
@@ -158,12 +172,11 @@ template <int NP, int TT>
 __device__ bool hermitian_part(const Cx<double>* X, Cx<double> f, Cx<double>* H, int N, int tt, ResScratch<NP>& S,
                                int team) {
   double bad = 0;
-  for (int idx = tt; idx < N * N; idx += TT) {
-    const int i = idx % N, j = idx / N;
+  tile_for<NP, TT>(N, tt, [&](int i, int j) {
     const Cx<double> v = f * X[sw<NP>(i, j)], w = f * X[sw<NP>(j, i)];
     if (!isfinite(v.x) || !isfinite(v.y) || !isfinite(w.x) || !isfinite(w.y)) bad = 1;
     H[sw<NP>(i, j)] = cx<double>(0.5 * (v.x + w.x), 0.5 * (v.y - w.y));
-  }
+  });
   bad = team_max<TT>(bad, tt, S.red, team);
   team_sync<TT>(team);  // H complete for every thread of the team
   return bad == 0;
@@ -284,18 +297,22 @@ __device__ double tri_eig(const double* d, const double* e2, int N, int kth) {
 // eigenvalues themselves.
 template <int NP, int TT>
 __device__ bool team_posdef(Cx<double>* H, int N, double shift, int tt, int team) {
+  // TT / NP threads per row (rows past the tile's thread count idle): thread
+  // (i, h) updates entries j = k + 1 + h, k + 1 + h + R, ... <= i of row i
+  constexpr int R = TT / NP >= 1 ? TT / NP : 1;
+  const int i = tt % NP, h = tt / NP;
   for (int k = 0; k < N; ++k) {
     const double dk = H[sw<NP>(k, k)].x + shift;
     if (!(dk > 0)) return false;  // team-uniform: every thread read the same pivot
     const double inv = 1.0 / dk;
-    const int m = N - k - 1;
-    for (int idx = tt; idx < m * m; idx += TT) {
-      const int i = k + 1 + idx % m, j = k + 1 + idx / m;
-      if (i < j) continue;
-      const Cx<double> a = H[sw<NP>(i, k)], b = H[sw<NP>(j, k)];
-      Cx<double>& h = H[sw<NP>(i, j)];
-      const Cx<double> t = a * conj(b);
-      h = cx<double>(h.x - inv * t.x, h.y - inv * t.y);
+    if (h < R && i > k && i < N) {
+      const Cx<double> a = H[sw<NP>(i, k)];
+      for (int j = k + 1 + h; j <= i; j += R) {
+        const Cx<double> b = H[sw<NP>(j, k)];
+        Cx<double>& hij = H[sw<NP>(i, j)];
+        const Cx<double> t = a * conj(b);
+        hij = cx<double>(hij.x - inv * t.x, hij.y - inv * t.y);
+      }
     }
     team_sync<TT>(team);
   }
@@ -379,24 +396,22 @@ __global__ void __launch_bounds__(BPC* Tile<NP>::TT) residual_kernel(ResidualArg
   double caus_num = 0;
   {
     double bad = 0;
-    for (int idx = tt; idx < N * N; idx += TT) {
-      const int i = idx % N, j = idx / N;
+    tile_for<NP, TT>(N, tt, [&](int i, int j) {
       const Cx<double> a = X[sw<NP>(i, j)], b = X[sw<NP>(j, i)];
       if (!isfinite(a.x) || !isfinite(a.y)) bad = 1;
       // (a - conj(b)) / (2i)
       const double dx = a.x - b.x, dy = a.y + b.y;
       H[sw<NP>(i, j)] = cx<double>(0.5 * dy, -0.5 * dx);
-    }
+    });
     bad = team_max<TT>(bad, tt, S.red, team);
     if (bad != 0) {
       caus_num = INFINITY;
     } else {
       // the causal case, -Im_H SR positive definite, is settled by one LDL^T
-      for (int idx = tt; idx < N * N; idx += TT) {
-        const int i = idx % N, j = idx / N;
+      tile_for<NP, TT>(N, tt, [&](int i, int j) {
         const Cx<double> v = H[sw<NP>(i, j)];
         W[sw<NP>(i, j)] = cx<double>(-v.x, -v.y);
-      }
+      });
       team_sync<TT>(team);
       if (!team_posdef<NP, TT>(W, N, 0.0, tt, team)) caus_num = fmax(0.0, team_lmax<NP, TT>(H, N, tt, S, team, true));
       team_sync<TT>(team);
@@ -415,8 +430,7 @@ __global__ void __launch_bounds__(BPC* Tile<NP>::TT) residual_kernel(ResidualArg
 
   // ---- r_D -------------------------------------------------------------------
   double nD = 0, nG = 0;
-  for (int idx = tt; idx < N * N; idx += TT) {
-    const int i = idx % N, j = idx / N;
+  tile_for<NP, TT>(N, tt, [&](int i, int j) {
     const Cx<double> hv = p.h[(size_t)m + (size_t)Nk * ((size_t)i + (size_t)N * j)];
     Cx<double> d = X[sw<NP>(i, j)];
     d = cx<double>(-hv.x - d.x, -hv.y - d.y);
@@ -425,18 +439,17 @@ __global__ void __launch_bounds__(BPC* Tile<NP>::TT) residual_kernel(ResidualArg
     nD += d.x * d.x + d.y * d.y;
     const Cx<double> g = G[sw<NP>(i, j)];
     nG += g.x * g.x + g.y * g.y;
-  }
+  });
   team_sum2<TT>(nD, nG, tt, S.red, team);
   team_sync<TT>(team);
   team_matmul<double, double, NP>(X, G, W, N, tt, false);
   team_sync<TT>(team);
   double nR = 0;
-  for (int idx = tt; idx < N * N; idx += TT) {
-    const int i = idx % N, j = idx / N;
+  tile_for<NP, TT>(N, tt, [&](int i, int j) {
     Cx<double> v = W[sw<NP>(i, j)];
     if (i == j) v.x -= 1;
     nR += v.x * v.x + v.y * v.y;
-  }
+  });
   nR = team_sum<TT>(nR, tt, S.red, team);
   double rD = sqrt(nR) / (sqrt(nD) * sqrt(nG) + sqrt((double)N));
   if (!isfinite(rD)) rD = INFINITY;
@@ -456,12 +469,11 @@ __global__ void __launch_bounds__(BPC* Tile<NP>::TT) residual_kernel(ResidualArg
       wk = kind;
     }
   };
-  for (int idx = tt; idx < N * N; idx += TT) {
-    const int i = idx % N, j = idx / N;
+  tile_for<NP, TT>(N, tt, [&](int i, int j) {
     const Cx<double> g = G[sw<NP>(i, j)], gt = G[sw<NP>(j, i)];
     // A = i (G - G^H)
     Y[sw<NP>(i, j)] = pi * cx<double>(g.x - gt.x, g.y + gt.y);
-  }
+  });
   team_sync<TT>(team);
   witness(psd_of<NP, TT>(Y, one, H, N, tt, S, team), 0);
 
@@ -470,11 +482,10 @@ __global__ void __launch_bounds__(BPC* Tile<NP>::TT) residual_kernel(ResidualArg
   load_tile<RS, NP, BPC>(p.SG, bX, e0, m, NE, Nk, N);
   load_tile<RS, NP, BPC>(p.SL, bW, e0, m, NE, Nk, N);
   __syncthreads();
-  for (int idx = tt; idx < N * N; idx += TT) {
-    const int i = idx % N, j = idx / N;
+  tile_for<NP, TT>(N, tt, [&](int i, int j) {
     const Cx<double> g = X[sw<NP>(i, j)], l = W[sw<NP>(i, j)];
     X[sw<NP>(i, j)] = pi * cx<double>(g.x - l.x, g.y - l.y);
-  }
+  });
   team_sync<TT>(team);
   witness(psd_of<NP, TT>(X, one, H, N, tt, S, team), 3);
   team_matmul<double, double, NP>(G, X, W, N, tt, false);  // W = G Gam
@@ -482,12 +493,11 @@ __global__ void __launch_bounds__(BPC* Tile<NP>::TT) residual_kernel(ResidualArg
   team_matmul<double, double, NP>(W, G, H, N, tt, true);   // H = G Gam G^H
   team_sync<TT>(team);
   double aNum = 0, aDen = 0;
-  for (int idx = tt; idx < N * N; idx += TT) {
-    const int i = idx % N, j = idx / N;
+  tile_for<NP, TT>(N, tt, [&](int i, int j) {
     const Cx<double> a = Y[sw<NP>(i, j)], q = H[sw<NP>(i, j)];
     aNum += (a.x - q.x) * (a.x - q.x) + (a.y - q.y) * (a.y - q.y);
     aDen += a.x * a.x + a.y * a.y;
-  }
+  });
   team_sum2<TT>(aNum, aDen, tt, S.red, team);
 
   // ---- raw Keldysh products -i G S< G^H, i G S> G^H ------------------------------
@@ -513,12 +523,11 @@ __global__ void __launch_bounds__(BPC* Tile<NP>::TT) residual_kernel(ResidualArg
   team_matmul<double, double, NP>(W, G, H, N, tt, true);
   team_sync<TT>(team);
   double kNum = 0, kDen = 0;
-  for (int idx = tt; idx < N * N; idx += TT) {
-    const int i = idx % N, j = idx / N;
+  tile_for<NP, TT>(N, tt, [&](int i, int j) {
     const Cx<double> a = X[sw<NP>(i, j)], q = H[sw<NP>(i, j)];
     kNum += (a.x - q.x) * (a.x - q.x) + (a.y - q.y) * (a.y - q.y);
     kDen += a.x * a.x + a.y * a.y;
-  }
+  });
   team_sum2<TT>(kNum, kDen, tt, S.red, team);
 
   // ---- G> positivity ---------------------------------------------------------------

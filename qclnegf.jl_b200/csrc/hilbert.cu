@@ -412,10 +412,10 @@ template <typename R> struct ResultOut {
   }
 };
 
-// Registers are capped (128 per thread for complex128; 64 for complex64, 96
+// Registers are capped (128 per thread for complex128; 64 for complex64, 80
 // with verification, which spills at 64) so that the register file holds as
 // many CTAs as the shared memory does.
-template <typename R, bool VERIFY> constexpr int hilbert_reg_cap() { return sizeof(R) == 8 ? 128 : (VERIFY ? 96 : 64); }
+template <typename R, bool VERIFY> constexpr int hilbert_reg_cap() { return sizeof(R) == 8 ? 128 : (VERIFY ? 80 : 64); }
 template <typename R, int T, bool VERIFY = false> constexpr int hilbert_min_blocks() {
   return 65536 / (hilbert_reg_cap<R, VERIFY>() * T) < 1 ? 1 : 65536 / (hilbert_reg_cap<R, VERIFY>() * T);
 }

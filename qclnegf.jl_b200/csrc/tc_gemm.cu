@@ -286,14 +286,26 @@ __global__ void __launch_bounds__(TC_THREADS, 1) tc_gemm_kernel(const __grid_con
       }
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
       const uint32_t taddr = tmem + tlane + (uint32_t)(b * BN + cbase);
+      // up to 64 columns in flight per wait (2 waits per buffer instead of CH / LDW)
+      constexpr int NL = CH / LDW, GL = 64 / LDW;
 #pragma unroll
-      for (int c = 0; c < CH / LDW; ++c) {
-        uint32_t v[LDW];
-        if constexpr (LDW == 32) tmem_ld32(taddr + c * 32, v);
-        else tmem_ld16(taddr + c * 16, v);
+      for (int c0 = 0; c0 < NL; c0 += GL) {
+        uint32_t v[GL][LDW];
+#pragma unroll
+        for (int g = 0; g < GL; ++g) {
+          if (c0 + g < NL) {
+            if constexpr (LDW == 32) tmem_ld32(taddr + (c0 + g) * 32, v[g]);
+            else tmem_ld16(taddr + (c0 + g) * 16, v[g]);
+          }
+        }
         asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 #pragma unroll
-        for (int i = 0; i < LDW; ++i) sum[c * LDW + i] += __uint_as_float(v[i]);
+        for (int g = 0; g < GL; ++g) {
+          if (c0 + g < NL) {
+#pragma unroll
+            for (int i = 0; i < LDW; ++i) sum[(c0 + g) * LDW + i] += __uint_as_float(v[g][i]);
+          }
+        }
       }
       asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
       mbar_arrive(acc_empty + 8 * b);

@@ -208,6 +208,22 @@ def cpu_rate(m_count=4, reps=1, warm=0):
     return NE * m_count / sec, sec
 
 
+def cpu_scba_tutorial(iters=2):
+    """ms per SCBA iteration of the CPU port (the oracle's SCBA loop: C kernels
+    with OpenMP) on the tutorial-scale problem (N_E x N_k = 400 x 16, N_b = 12,
+    roundoff check on), after a seed and one iteration."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    sys.path.insert(0, os.path.join(ROOT, "qclnegf.jl_b200"))
+    import oracle as orc
+    from qclb200.problem import tutorial_problem
+
+    pr = tutorial_problem()
+    _, st = orc.scba(pr, 1, keep_state=True)
+    t0 = time.perf_counter()
+    orc.scba(pr, iters, state=st)
+    return (time.perf_counter() - t0) / iters * 1e3
+
+
 def cores():
     try:
         return len(os.sched_getaffinity(0))
@@ -445,6 +461,10 @@ def run_gpu(args):
             line["cpu_baseline"] = {"value": rate, "unit": "solves/s", "cores": cores(), "kind": "port",
                                     "sample": f"the full batch ({NK} momenta x {NE} energies), median of 3 "
                                               f"after 1 warm-up, {sec:.2f} s per batch"}
+            line["cpu_baseline"]["scba_tutorial_N12"] = {
+                "ms_per_iter": cpu_scba_tutorial(), "kind": "port", "cores": cores(),
+                "sample": "2 SCBA iterations of the tutorial problem (N_E x N_k = 400 x 16, N_b = 12, roundoff "
+                          "check on) after a seed and 1 iteration; compare extras.scba_tutorial_N12_30iter"}
         except Exception as ex:  # noqa: BLE001
             line["cpu_baseline"] = {"value": None, "error": str(ex)}
     line["clocks"] = clk.summary()

@@ -326,6 +326,22 @@ __device__ __forceinline__ void spectrum_pass(Cx<R>* buf, const Cx<R>* __restric
   __syncthreads();
 }
 
+// Pulls this thread's kernel-spectrum entries of the spectrum pass (K[j + r
+// L/16], r < 16) toward L1 ahead of use, without holding registers.  Used in
+// complex64, where it took the N_E = 1024 transform from 0.297 to 0.248 ms
+// (with verification); complex128 measured no gain.
+template <typename R, int L> __device__ __forceinline__ void prefetch_spectrum(const Cx<R>* K) {
+  constexpr int T = FftPlan<L>::T, NB = L / 16, Q = (NB + T - 1) / T;
+#pragma unroll
+  for (int q = 0; q < Q; ++q) {
+    const int j = threadIdx.x + q * T;
+    if (j < NB) {
+#pragma unroll
+      for (int r = 0; r < 16; ++r) asm volatile("prefetch.global.L1 [%0];" ::"l"(K + j + r * NB));
+    }
+  }
+}
+
 // conj(L * IFFT(FFT(x) .* K)) for a field read through `in` (ZHI: zero on
 // [L/2, L)), written through `out`; `buf` holds the padded column, `twt` the
 // complex64 pass tables (null for complex128).
@@ -339,6 +355,7 @@ __device__ __forceinline__ void convolve_run(const In& in, const Cx<R>* K, const
   static_assert(conv_table_entries(L) == 2 * L - S - 16, "pass-table layout");
   const bool t = twt != nullptr;
   stockham_pass<R, L, S, 1, ZHI>(in, SmemOut<R>{buf}, tw, nullptr);
+  if constexpr (sizeof(R) == 4) prefetch_spectrum<R, L>(K);
   Radix16Passes<R, L, S, P - 1>::run(buf, tw, t ? twt + conv_fwd_seg(L, 0) : nullptr);
   spectrum_pass<R, L>(buf, K, tw, t ? twt + conv_fwd_seg(L, P - 1) : nullptr);
   Radix16Passes<R, L, 16, P - 1>::run(buf, tw, t ? twt + conv_inv_seg(L, 1) : nullptr);

@@ -22,17 +22,29 @@ template <typename R> struct SandwichArgs {
 template <typename R, int NP, int BPC>
 __device__ __forceinline__ void load_shifted(const Cx<R>* __restrict__ X, const ShiftPlanDev& plan, Cx<R>* bufs,
                                              int e0, int m, int NE, int Nk, int N) {
-  const int total = BPC * N * N;
-  for (int i = threadIdx.x; i < total; i += blockDim.x) {
-    const int eloc = i % BPC, el = i / BPC;
-    const int a = el % N, b = el / N;
-    const int e = e0 + eloc;
+  // blockDim.x is a multiple of BPC, so each thread serves one energy of the
+  // CTA: its interpolation plan is read once; the padded tile index is split
+  // at compile time (entries past N are left as they are, as before)
+  const int eloc = threadIdx.x % BPC;
+  const int e = e0 + eloc;
+  const bool ok = e < NE && plan.valid[e];
+  int l = 0, r = 0;
+  double th = 0.0;
+  if (ok) {
+    l = plan.left[e];
+    r = plan.right[e];
+    th = plan.theta[e];
+  }
+  const bool two = l != r && th != 0.0;
+  const size_t base = (size_t)NE * m, cstride = (size_t)NE * Nk;
+  for (int i = threadIdx.x; i < BPC * NP * NP; i += blockDim.x) {
+    const int el = i / BPC;
+    const int a = el % NP, b = el / NP;
+    if (a >= N || b >= N) continue;
     Cx<R> v = cx<R>(0, 0);
-    if (e < NE && plan.valid[e]) {
-      const size_t col = (size_t)NE * ((size_t)m + (size_t)Nk * ((size_t)a + (size_t)N * b));
-      const int l = plan.left[e], r = plan.right[e];
-      const double th = plan.theta[e];
-      if (l == r || th == 0.0) {
+    if (ok) {
+      const size_t col = base + cstride * ((size_t)a + (size_t)N * b);
+      if (!two) {
         v = X[col + l];
       } else {
         const Cx<R> u = X[col + l], w = X[col + r];

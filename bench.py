@@ -481,8 +481,10 @@ def run_gpu(args):
 
 
 def extras(torch, dev, L, _lib):
-    """Side measurements: complex64 / mixed Dyson, N_b = 48, and SCBA
-    iterations/s of the tutorial-scale problem (FP64 vs mixed, J error)."""
+    """Side measurements: the operator batch (Dyson + Keldysh, and the L = 8192
+    Hilbert transform of every column) in complex64 / mixed and at N_b = 48,
+    and SCBA iterations/s of the tutorial-scale problem (FP64 vs mixed, J
+    error)."""
     import numpy as np
 
     P = ctypes.c_void_p
@@ -504,17 +506,37 @@ def extras(torch, dev, L, _lib):
                                                P(SR.data_ptr()), P(SL.data_ptr()), None, P(GR.data_ptr()),
                                                P(GL.data_ptr()), None, None, None, None, P(st.data_ptr())))
 
-        for _ in range(3):
-            call()
-        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        a.record(s)
-        for _ in range(5):
-            call()
-        b.record(s)
-        torch.cuda.synchronize()
-        ms = a.elapsed_time(b) / 5
-        out[name] = {"dyson_keldysh_ms": ms, "solves_per_s": NE * NK / (ms / 1e3)}
-        del SR, SL, GR, GL
+        # the batch's Hilbert transform at the storage precision: Gamma of every
+        # (m, a, b) column, L = 8192
+        hprec = _lib.QCL_C128 if prec == _lib.QCL_C128 else _lib.QCL_C64
+        ncols = NK * N * N
+        g = torch.Generator(device=dev)
+        g.manual_seed(5)
+        Gam = torch.randn((ncols, NE), dtype=cdt, device=dev, generator=g)
+        Lam = torch.empty_like(Gam)
+        wE_d = torch.tensor(wE, dtype=torch.float64, device=dev)
+
+        def hilbert():
+            _lib.check(L.qcl_dev_fft_hilbert_transform(sp, hprec, NE, ncols, float(eps[1] - eps[0]),
+                                                       P(wE_d.data_ptr()), P(Gam.data_ptr()), P(Lam.data_ptr()),
+                                                       None))
+
+        times = {}
+        for key, fn in (("dyson_keldysh_ms", call), ("hilbert_ms", hilbert)):
+            for _ in range(3):
+                fn()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(s)
+            for _ in range(5):
+                fn()
+            b.record(s)
+            torch.cuda.synchronize()
+            times[key] = a.elapsed_time(b) / 5
+        ms = times["dyson_keldysh_ms"]
+        out[name] = {"dyson_keldysh_ms": ms, "solves_per_s": NE * NK / (ms / 1e3), "hilbert_ms": times["hilbert_ms"],
+                     "step_solves_per_s": NE * NK / ((ms + times["hilbert_ms"]) / 1e3),
+                     "hilbert_columns": ncols}
+        del SR, SL, GR, GL, Gam, Lam
         torch.cuda.empty_cache()
     # SCBA iterations/s at tutorial scale
     from qclb200.problem import tutorial_problem

@@ -10,11 +10,15 @@
 // and _retarded_self_energy_fft_production (:842-884):
 //   Gam = i (S> - S<),  SR = Lam - i Gam / 2.
 //
-// B200 mapping: one CTA per column (m, a, b).  The whole padded column lives
-// in shared memory (L <= 8192 complex128 = 136 KiB padded), the two FFTs are
-// radix-16 Stockham passes with the butterflies in registers, the kernel
-// spectrum is read from L2, and the inputs are read once and the outputs
-// written once (E is the contiguous axis, so every load/store is coalesced).
+// B200 mapping: one CTA per column (m, a, b).  The padded column lives in
+// shared memory, the two FFTs are Stockham passes (radix 16 after a first
+// pass of radix L / 16^P) with the butterflies in registers, the last forward
+// pass, the spectrum product and the first inverse pass run as one register
+// pass, the kernel spectrum is read from L2, and the inputs are read once and
+// the outputs written once (E is the contiguous axis, so every load/store is
+// coalesced).  The complex128 L = 8192 transform runs as two half-length
+// transforms (even / odd frequencies) in a 68 KiB buffer, so that two columns
+// share an SM (hilbert_halves_kernel).
 //
 // Roundoff verification (fft_parallel.jl:279-290 runs a second transform at
 // length 2L).  Because the input is zero beyond N_E <= L/2 + 1 and only

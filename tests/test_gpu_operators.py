@@ -100,6 +100,43 @@ def test_fft_hilbert_c128_matches_direct_pv(gpu_ops, orc, NE):
     assert np.max(np.abs(Lam2 - Lam)) <= 1e-13 * max(np.max(np.abs(Lam)), 1.0)
 
 
+@pytest.mark.parametrize("NE", [2049, 3001, 4096])
+def test_fft_hilbert_half_length_path_matches_oracle(gpu_ops, orc, NE):
+    """L = 8192 complex128 with at least two columns per SM runs as two
+    half-length transforms (even / odd frequencies): every column against the
+    oracle's FFT convolution, some against the direct principal-value sum, and
+    against the one-CTA kernel (the roundoff rerun) to rounding."""
+    rng = np.random.default_rng(NE + 7)
+    ncols = 300
+    eps = np.linspace(-1.3, 0.9, NE)
+    w = np.full(NE, eps[1] - eps[0])
+    w[[0, -1]] /= 2
+    G = np.asfortranarray(rng.standard_normal((NE, ncols)) + 1j * rng.standard_normal((NE, ncols)))
+    Lam = gpu_ops.fft_hilbert_transform(G, eps, w)
+    assert approx_err(Lam, orc.fft_hilbert(G, eps, w)) < 2e-13
+    sub = [0, 1, 150, ncols - 1]
+    assert approx_err(Lam[:, sub], orc.direct_hilbert(np.asfortranarray(G[:, sub]), eps, w)) < 2e-13
+    Lam2, r = gpu_ops.fft_hilbert_transform(G, eps, w, return_roundoff=True)
+    assert r < 1e-12
+    assert np.max(np.abs(Lam2 - Lam)) <= 1e-13 * np.max(np.abs(Lam))
+
+
+def test_retarded_self_energy_half_length_path(gpu_ops, orc):
+    # the fused Gamma = i (S> - S<), SR = Lam - i Gamma / 2 through the
+    # half-length kernel (N_E = 2500, L = 8192, 300 columns)
+    rng = np.random.default_rng(0xFF72)
+    NE, Nk, Nb = 2500, 3, 10
+    eps = np.linspace(-1.3, 0.9, NE)
+    w = np.full(NE, eps[1] - eps[0])
+    w[[0, -1]] /= 2
+    SL = np.asfortranarray(rng.standard_normal((NE, Nk, Nb, Nb)) + 1j * rng.standard_normal((NE, Nk, Nb, Nb)))
+    SG = np.asfortranarray(rng.standard_normal((NE, Nk, Nb, Nb)) + 1j * rng.standard_normal((NE, Nk, Nb, Nb)))
+    SR, Gam = gpu_ops.retarded_self_energy_fft(SL, SG, eps, w)
+    oSR, oGam = orc.retarded_self_energy(SL, SG, eps, w, method="fft")
+    assert np.array_equal(Gam, oGam)
+    assert approx_err(SR, oSR) < 2e-13
+
+
 @pytest.mark.parametrize("NE", [1500, 4096])
 def test_fft_hilbert_in_place_on_device(gpu_ops, orc, NE):
     """Lam == Gam through the device entry: the transform of the original

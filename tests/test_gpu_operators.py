@@ -394,6 +394,26 @@ def test_dense_contraction_tensor_cores_dynamic_range(gpu_ops, orc):
     assert float(np.max(rel)) < 2e-6
 
 
+def test_dense_contraction_tensor_cores_wide_tile(gpu_ops):
+    # N_E = 4736 (37 row tiles) x 1024 real columns: 256-wide tiles fill one
+    # wave of 148 exactly, so the tile-width choice takes the 256 variant
+    from qclb200.problem import Mechanism
+
+    rng = np.random.default_rng(23)
+    NE, Nk, Nb = 4736, 2, 16
+    Nc = Nk * Nb * Nb
+    M = rng.standard_normal((Nc, Nc)) + 1j * rng.standard_normal((Nc, Nc))
+    G = rng.standard_normal((NE, Nk, Nb, Nb)) + 1j * rng.standard_normal((NE, Nk, Nb, Nb))
+    wk = np.array([0.7, 1.3])
+    mech = Mechanism("impurity", "dense", 0.9, matrix=np.asfortranarray(M))
+    got = gpu_ops.production_static_contraction(mech, np.asfortranarray(G), wk, precision="c64")
+    Gf = G.astype(np.complex64).astype(np.complex128).reshape(NE, Nc, order="F")
+    Mf = M.astype(np.complex64).astype(np.complex128)
+    wq = np.array([wk[q % Nk] for q in range(Nc)])  # column q = m' + Nk (c + Nb d)
+    ref = 0.9 * (Gf * wq[None, :]) @ Mf.T
+    assert approx_err(got.reshape(NE, Nc, order="F"), ref) < 2e-6
+
+
 def test_dense_contraction_tensor_cores_no_accumulation_bias(gpu_ops):
     # a long positive sum (K = 2 N_k N_b^2 = 2048 real terms) exposes any
     # truncation bias of the tensor-core accumulation: the mean signed relative

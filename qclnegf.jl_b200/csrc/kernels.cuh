@@ -154,6 +154,11 @@ int launch_residual_suite(int precision, int NE, int Nk, int N, const double* ep
                           const void* GL, const void* GG, const void* SR, const void* SL, const void* SG,
                           const void* SLc, double* work, double* out5, cudaStream_t st);
 size_t residual_work_doubles(int NE, int Nk);
+enum { RES_PART_ALL = 0, RES_PART_MAIN = 1, RES_PART_RK = 2 };
+int launch_residual_blocks(int precision, int part, int NE, int Nk, int N, const double* eps, const void* h,
+                           const void* GR, const void* GL, const void* GG, const void* SR, const void* SL,
+                           const void* SG, const void* SLc, double* work, cudaStream_t st);
+int launch_residual_reduce(int NE, int Nk, double* work, double* out5, cudaStream_t st);
 int launch_eigvals(int n, long long count, const void* A, double* vals, cudaStream_t st);
 size_t observables_partial_doubles(int N);
 int launch_observables(int precision, int NE, int Nk, int N, const double* wE, const double* wk, const void* SG,

@@ -44,6 +44,7 @@ template <typename RS> struct ResidualArgs {
   const Cx<RS>* SG;
   const Cx<RS>* SLc;  // candidate total lesser
   double* block_out;  // kResidualBlockDoubles per block
+  int part;           // RES_PART_ALL, RES_PART_MAIN (all but r_K) or RES_PART_RK (r_K only)
 };
 
 struct JacobiRot {
@@ -387,6 +388,31 @@ __global__ void __launch_bounds__(BPC* Tile<NP>::TT) residual_kernel(ResidualArg
   ResScratch<NP>& S = scr[team];
   const Cx<double> one = cx<double>(1, 0), mi = cx<double>(0, -1), pi = cx<double>(0, 1);
 
+  if (p.part == RES_PART_RK) {  // launch-uniform
+    // r_K alone: ||G< - G S<_cand G^H||^2 and ||G<||^2 of this block
+    load_tile<RS, NP, BPC>(p.GR, bG, e0, m, NE, Nk, N);
+    load_tile<RS, NP, BPC>(p.GL, bX, e0, m, NE, Nk, N);
+    load_tile<RS, NP, BPC>(p.SLc, bY, e0, m, NE, Nk, N);
+    __syncthreads();
+    team_matmul<double, double, NP>(G, Y, W, N, tt, false);
+    team_sync<TT>(team);
+    team_matmul<double, double, NP>(W, G, H, N, tt, true);
+    team_sync<TT>(team);
+    double kNum = 0, kDen = 0;
+    tile_for<NP, TT>(N, tt, [&](int i, int j) {
+      const Cx<double> a = X[sw<NP>(i, j)], q = H[sw<NP>(i, j)];
+      kNum += (a.x - q.x) * (a.x - q.x) + (a.y - q.y) * (a.y - q.y);
+      kDen += a.x * a.x + a.y * a.y;
+    });
+    team_sum2<TT>(kNum, kDen, tt, S.red, team);
+    if (tt == 0 && live) {
+      double* o = p.block_out + kResidualBlockDoubles * ((size_t)e + (size_t)NE * m);
+      o[3] = isfinite(kNum) ? kNum : INFINITY;
+      o[4] = isfinite(kDen) ? kDen : INFINITY;
+    }
+    return;
+  }
+
   load_tile<RS, NP, BPC>(p.GR, bG, e0, m, NE, Nk, N);
   load_tile<RS, NP, BPC>(p.SR, bX, e0, m, NE, Nk, N);
   __syncthreads();
@@ -514,21 +540,24 @@ __global__ void __launch_bounds__(BPC* Tile<NP>::TT) residual_kernel(ResidualArg
 
   // ---- G< : positivity and r_K against the candidate lesser self-energy ----------
   __syncthreads();
+  const bool with_rk = p.part == RES_PART_ALL;  // launch-uniform
   load_tile<RS, NP, BPC>(p.GL, bX, e0, m, NE, Nk, N);
-  load_tile<RS, NP, BPC>(p.SLc, bY, e0, m, NE, Nk, N);
+  if (with_rk) load_tile<RS, NP, BPC>(p.SLc, bY, e0, m, NE, Nk, N);
   __syncthreads();
   witness(psd_of<NP, TT>(X, mi, H, N, tt, S, team), 1);
-  team_matmul<double, double, NP>(G, Y, W, N, tt, false);
-  team_sync<TT>(team);
-  team_matmul<double, double, NP>(W, G, H, N, tt, true);
-  team_sync<TT>(team);
   double kNum = 0, kDen = 0;
-  tile_for<NP, TT>(N, tt, [&](int i, int j) {
-    const Cx<double> a = X[sw<NP>(i, j)], q = H[sw<NP>(i, j)];
-    kNum += (a.x - q.x) * (a.x - q.x) + (a.y - q.y) * (a.y - q.y);
-    kDen += a.x * a.x + a.y * a.y;
-  });
-  team_sum2<TT>(kNum, kDen, tt, S.red, team);
+  if (with_rk) {
+    team_matmul<double, double, NP>(G, Y, W, N, tt, false);
+    team_sync<TT>(team);
+    team_matmul<double, double, NP>(W, G, H, N, tt, true);
+    team_sync<TT>(team);
+    tile_for<NP, TT>(N, tt, [&](int i, int j) {
+      const Cx<double> a = X[sw<NP>(i, j)], q = H[sw<NP>(i, j)];
+      kNum += (a.x - q.x) * (a.x - q.x) + (a.y - q.y) * (a.y - q.y);
+      kDen += a.x * a.x + a.y * a.y;
+    });
+    team_sum2<TT>(kNum, kDen, tt, S.red, team);
+  }
 
   // ---- G> positivity ---------------------------------------------------------------
   __syncthreads();
@@ -541,8 +570,10 @@ __global__ void __launch_bounds__(BPC* Tile<NP>::TT) residual_kernel(ResidualArg
     o[0] = rD;
     o[1] = isfinite(aNum) ? aNum : INFINITY;
     o[2] = isfinite(aDen) ? aDen : INFINITY;
-    o[3] = isfinite(kNum) ? kNum : INFINITY;
-    o[4] = isfinite(kDen) ? kDen : INFINITY;
+    if (with_rk) {
+      o[3] = isfinite(kNum) ? kNum : INFINITY;
+      o[4] = isfinite(kDen) ? kDen : INFINITY;
+    }
     o[5] = psd;
     o[6] = caus;
     o[7] = wr;
@@ -1340,27 +1371,43 @@ static int noalloc_scratch(double** out) {
   return QCL_OK;
 }
 
-int launch_residual_suite(int precision, int NE, int Nk, int N, const double* eps, const void* h, const void* GR,
-                          const void* GL, const void* GG, const void* SR, const void* SL, const void* SG,
-                          const void* SLc, double* work, double* out5, cudaStream_t st) {
-  int s;
+// Per-block pass of the residual suite (part: RES_PART_ALL, or the two halves
+// RES_PART_MAIN and RES_PART_RK, which write disjoint per-block slots and may
+// run concurrently).
+int launch_residual_blocks(int precision, int part, int NE, int Nk, int N, const double* eps, const void* h,
+                           const void* GR, const void* GL, const void* GG, const void* SR, const void* SL,
+                           const void* SG, const void* SLc, double* work, cudaStream_t st) {
+  if (part != RES_PART_ALL && part != RES_PART_MAIN && part != RES_PART_RK) {
+    set_last_error("residual suite: unknown part %d", part);
+    return QCL_ARG;
+  }
   if (precision == QCL_C128) {
     ResidualArgs<double> a{NE, Nk, N, eps, (const Cx<double>*)h, (const Cx<double>*)GR, (const Cx<double>*)GL,
                            (const Cx<double>*)GG, (const Cx<double>*)SR, (const Cx<double>*)SL,
-                           (const Cx<double>*)SG, (const Cx<double>*)SLc, work};
-    s = launch_residual_p<double>(a, st);
-  } else {
-    ResidualArgs<float> a{NE, Nk, N, eps, (const Cx<double>*)h, (const Cx<float>*)GR, (const Cx<float>*)GL,
-                          (const Cx<float>*)GG, (const Cx<float>*)SR, (const Cx<float>*)SL, (const Cx<float>*)SG,
-                          (const Cx<float>*)SLc, work};
-    s = launch_residual_p<float>(a, st);
+                           (const Cx<double>*)SG, (const Cx<double>*)SLc, work, part};
+    return launch_residual_p<double>(a, st);
   }
-  if (s) return s;
+  ResidualArgs<float> a{NE, Nk, N, eps, (const Cx<double>*)h, (const Cx<float>*)GR, (const Cx<float>*)GL,
+                        (const Cx<float>*)GG, (const Cx<float>*)SR, (const Cx<float>*)SL, (const Cx<float>*)SG,
+                        (const Cx<float>*)SLc, work, part};
+  return launch_residual_p<float>(a, st);
+}
+
+// Fixed-order reduction of the per-block outputs in `work` into out5.
+int launch_residual_reduce(int NE, int Nk, double* work, double* out5, cudaStream_t st) {
   double* partial = work + kResidualBlockDoubles * (size_t)NE * Nk;
   residual_reduce_kernel<<<RES_CTAS, 256, 0, st>>>((long long)NE * Nk, work, partial);
   residual_final_kernel<<<1, 7 * 32, 0, st>>>(RES_CTAS, partial, out5);
   QCL_LAUNCH_CHECK("residual_reduce");
   return QCL_OK;
+}
+
+int launch_residual_suite(int precision, int NE, int Nk, int N, const double* eps, const void* h, const void* GR,
+                          const void* GL, const void* GG, const void* SR, const void* SL, const void* SG,
+                          const void* SLc, double* work, double* out5, cudaStream_t st) {
+  int s = launch_residual_blocks(precision, RES_PART_ALL, NE, Nk, N, eps, h, GR, GL, GG, SR, SL, SG, SLc, work, st);
+  if (s) return s;
+  return launch_residual_reduce(NE, Nk, work, out5, st);
 }
 
 // The witness of the residual suite whose per-block outputs are in `work`

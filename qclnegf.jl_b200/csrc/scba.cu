@@ -112,6 +112,8 @@ struct ScbaCtx {
   HilbertTables hil;
   // graph of one iteration (two parities: state/cand swap)
   cudaGraphExec_t graph[2] = {nullptr, nullptr};
+  cudaStream_t st2 = nullptr;  // side stream of an iteration (forked from st, joined back)
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   bool use_graph = false;
   int parity = 0;
   bool pending_commit = false;
@@ -235,6 +237,9 @@ void scba_destroy(ScbaCtx* c) {
   cudaFree(c->apartial);
   if (c->ameta_h) cudaFreeHost(c->ameta_h);
   free_hilbert_tables(c->hil);
+  if (c->ev_fork) cudaEventDestroy(c->ev_fork);
+  if (c->ev_join) cudaEventDestroy(c->ev_join);
+  if (c->st2) cudaStreamDestroy(c->st2);
   if (c->st) cudaStreamDestroy(c->st);
   delete c;
 }
@@ -327,6 +332,11 @@ int scba_create(const qcl_scba_problem* p, const qcl_mechanism* mechs, ScbaCtx**
              QCL_ARG));
   {
     cudaError_t e = cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking);
+    if (e != cudaSuccess) TRY(cuda_status(e, "cudaStreamCreate"));
+    // the residual suite's G-only part runs beside the candidate construction
+    e = cudaStreamCreateWithFlags(&c->st2, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming);
     if (e != cudaSuccess) TRY(cuda_status(e, "cudaStreamCreate"));
   }
   TRY(dupload(&c->eps, p->eps, c->NE * sizeof(double), c->st));
@@ -523,6 +533,16 @@ static int iteration_body(ScbaCtx* c, std::vector<void*>& state, std::vector<voi
   int s;
   const int sp = c->precision == QCL_MIXED ? QCL_C64 : c->precision;
   if ((s = current_green(c, state))) return s;
+  // Everything of the residual suite except r_K needs only G and the totals:
+  // it runs on the side stream while the candidates are built; r_K follows the
+  // candidate total lesser, and the fixed-order reduction waits for both (the
+  // two parts write disjoint per-block slots).
+  QCL_CUDA_CHECK(cudaEventRecord(c->ev_fork, c->st));
+  QCL_CUDA_CHECK(cudaStreamWaitEvent(c->st2, c->ev_fork, 0));
+  if ((s = launch_residual_blocks(c->precision, RES_PART_MAIN, c->NE, c->Nk, c->N, c->eps, c->h, c->GR, c->GL, c->GG,
+                                  c->tot[0], c->tot[1], c->tot[2], nullptr, c->reswork, c->st2)))
+    return s;
+  QCL_CUDA_CHECK(cudaEventRecord(c->ev_join, c->st2));
   if ((s = scattering_candidates(c, c->GR, c->GL, c->GG, cand, c->verify != 0))) return s;
   if ((s = embedding_candidates(c, cand))) return s;
   // candidate total lesser for r_K
@@ -532,9 +552,11 @@ static int iteration_body(ScbaCtx* c, std::vector<void*>& state, std::vector<voi
     for (int f = 0; f < F; ++f) src[f] = field_of(cand, f, 1);
     if ((s = launch_sum_fields(sp, c->nfield, src, F, c->candSL, c->st))) return s;
   }
-  if ((s = launch_residual_suite(c->precision, c->NE, c->Nk, c->N, c->eps, c->h, c->GR, c->GL, c->GG, c->tot[0],
-                                 c->tot[1], c->tot[2], c->candSL, c->reswork, c->scal + SC_RES, c->st)))
+  if ((s = launch_residual_blocks(c->precision, RES_PART_RK, c->NE, c->Nk, c->N, c->eps, c->h, c->GR, c->GL, c->GG,
+                                  c->tot[0], c->tot[1], c->tot[2], c->candSL, c->reswork, c->st)))
     return s;
+  QCL_CUDA_CHECK(cudaStreamWaitEvent(c->st, c->ev_join, 0));
+  if ((s = launch_residual_reduce(c->NE, c->Nk, c->reswork, c->scal + SC_RES, c->st))) return s;
   // embedding-total residual (before the plus/minus candidates are mixed over)
   for (int k = 0; k < 3; ++k)
     if ((s = launch_residual_pair(sp, c->nfield, field_of(state, c->M, k), field_of(state, c->M + 1, k),

@@ -182,20 +182,26 @@ template <typename R> struct GemmArgs {
   double alpha, beta;
 };
 
-constexpr int GE = 64, GJ = 32, GK = 16, GT = 256;
+constexpr int GK = 16;
 
-template <typename R> __global__ void __launch_bounds__(GT) gemm_kernel(GemmArgs<R> p) {
+// Output tile GE x GJ per CTA of GT threads: a 16 x (GT / 16) thread grid,
+// each thread GE/16 x GJ/(GT/16) outputs.  Two shapes: 64 x 32 (256 threads)
+// and, when that gives fewer than two CTAs per SM, 32 x 16 (128 threads) --
+// the same per-output arithmetic and summation order, more CTAs in flight.
+template <typename R, int GE, int GJ, int GT> __global__ void __launch_bounds__(GT) gemm_kernel(GemmArgs<R> p) {
+  constexpr int TJ = GT / 16, NI = GE / 16, NU = GJ / TJ;
+  static_assert(GE % 16 == 0 && GJ % TJ == 0, "tile shape");
   __shared__ Cx<R> As[GK][GE];
   __shared__ Cx<R> Bs[GK][GJ];
   const int b = blockIdx.z;
   const int e0 = blockIdx.x * GE, j0 = blockIdx.y * GJ;
   const int te = threadIdx.x % 16, tj = threadIdx.x / 16;
   const double wbb = p.wb ? p.wb[b] : 1.0;
-  Cx<R> acc[4][2];
+  Cx<R> acc[NI][NU];
 #pragma unroll
-  for (int i = 0; i < 4; ++i)
+  for (int i = 0; i < NI; ++i)
 #pragma unroll
-    for (int u = 0; u < 2; ++u) acc[i][u] = cx<R>(0, 0);
+    for (int u = 0; u < NU; ++u) acc[i][u] = cx<R>(0, 0);
   for (int k0 = 0; k0 < p.K; k0 += GK) {
     for (int idx = threadIdx.x; idx < GE * GK; idx += GT) {
       const int el = idx % GE, kl = idx / GE;
@@ -218,25 +224,25 @@ template <typename R> __global__ void __launch_bounds__(GT) gemm_kernel(GemmArgs
     __syncthreads();
 #pragma unroll
     for (int kl = 0; kl < GK; ++kl) {
-      Cx<R> a[4], bb[2];
+      Cx<R> a[NI], bb[NU];
 #pragma unroll
-      for (int i = 0; i < 4; ++i) a[i] = As[kl][te + 16 * i];
+      for (int i = 0; i < NI; ++i) a[i] = As[kl][te + 16 * i];
 #pragma unroll
-      for (int u = 0; u < 2; ++u) bb[u] = Bs[kl][tj + 16 * u];
+      for (int u = 0; u < NU; ++u) bb[u] = Bs[kl][tj + TJ * u];
 #pragma unroll
-      for (int i = 0; i < 4; ++i)
+      for (int i = 0; i < NI; ++i)
 #pragma unroll
-        for (int u = 0; u < 2; ++u) cfma(acc[i][u], a[i], bb[u]);
+        for (int u = 0; u < NU; ++u) cfma(acc[i][u], a[i], bb[u]);
     }
     __syncthreads();
   }
 #pragma unroll
-  for (int i = 0; i < 4; ++i) {
+  for (int i = 0; i < NI; ++i) {
     const int e = e0 + te + 16 * i;
     if (e >= p.M) continue;
 #pragma unroll
-    for (int u = 0; u < 2; ++u) {
-      const int j = j0 + tj + 16 * u;
+    for (int u = 0; u < NU; ++u) {
+      const int j = j0 + tj + TJ * u;
       if (j >= p.Nout) continue;
       const double vx = p.alpha * (double)acc[i][u].x, vy = p.alpha * (double)acc[i][u].y;
       for (int r = 0; r < p.bcast; ++r) {
@@ -254,8 +260,14 @@ template <typename R> __global__ void __launch_bounds__(GT) gemm_kernel(GemmArgs
 
 template <typename R> static int launch_gemm(const GemmArgs<R>& a, cudaStream_t st) {
   if (a.M <= 0 || a.Nout <= 0 || a.batch <= 0) return QCL_OK;
-  dim3 grid((a.M + GE - 1) / GE, (a.Nout + GJ - 1) / GJ, a.batch);
-  gemm_kernel<R><<<grid, GT, 0, st>>>(a);
+  const long long big = (long long)((a.M + 63) / 64) * ((a.Nout + 31) / 32) * a.batch;
+  if (big >= 2 * 148) {
+    dim3 grid((a.M + 63) / 64, (a.Nout + 31) / 32, a.batch);
+    gemm_kernel<R, 64, 32, 256><<<grid, 256, 0, st>>>(a);
+  } else {
+    dim3 grid((a.M + 31) / 32, (a.Nout + 15) / 16, a.batch);
+    gemm_kernel<R, 32, 16, 128><<<grid, 128, 0, st>>>(a);
+  }
   QCL_LAUNCH_CHECK("gemm_kernel");
   return QCL_OK;
 }

@@ -373,8 +373,7 @@ __global__ void __launch_bounds__(BPC* Tile<NP>::TT) residual_kernel(ResidualArg
   Cx<double>* bX = bG + BPC * MSZ;
   Cx<double>* bW = bX + BPC * MSZ;
   Cx<double>* bH = bW + BPC * MSZ;
-  Cx<double>* bY = bH + BPC * MSZ;
-  ResScratch<NP>* scr = reinterpret_cast<ResScratch<NP>*>(bY + BPC * MSZ);
+  ResScratch<NP>* scr = reinterpret_cast<ResScratch<NP>*>(bH + BPC * MSZ);
   const int N = p.N, NE = p.NE, Nk = p.Nk;
   const int m = blockIdx.y, e0 = blockIdx.x * BPC;
   const int team = threadIdx.x / TT, tt = threadIdx.x % TT;
@@ -384,7 +383,6 @@ __global__ void __launch_bounds__(BPC* Tile<NP>::TT) residual_kernel(ResidualArg
   Cx<double>* X = bX + team * MSZ;
   Cx<double>* W = bW + team * MSZ;
   Cx<double>* H = bH + team * MSZ;
-  Cx<double>* Y = bY + team * MSZ;
   ResScratch<NP>& S = scr[team];
   const Cx<double> one = cx<double>(1, 0), mi = cx<double>(0, -1), pi = cx<double>(0, 1);
 
@@ -392,15 +390,15 @@ __global__ void __launch_bounds__(BPC* Tile<NP>::TT) residual_kernel(ResidualArg
     // r_K alone: ||G< - G S<_cand G^H||^2 and ||G<||^2 of this block
     load_tile<RS, NP, BPC>(p.GR, bG, e0, m, NE, Nk, N);
     load_tile<RS, NP, BPC>(p.GL, bX, e0, m, NE, Nk, N);
-    load_tile<RS, NP, BPC>(p.SLc, bY, e0, m, NE, Nk, N);
+    load_tile<RS, NP, BPC>(p.SLc, bW, e0, m, NE, Nk, N);
     __syncthreads();
-    team_matmul<double, double, NP>(G, Y, W, N, tt, false);
+    team_matmul<double, double, NP>(G, W, H, N, tt, false);  // H = G S<_cand
     team_sync<TT>(team);
-    team_matmul<double, double, NP>(W, G, H, N, tt, true);
+    team_matmul<double, double, NP>(H, G, W, N, tt, true);   // W = H G^H
     team_sync<TT>(team);
     double kNum = 0, kDen = 0;
     tile_for<NP, TT>(N, tt, [&](int i, int j) {
-      const Cx<double> a = X[sw<NP>(i, j)], q = H[sw<NP>(i, j)];
+      const Cx<double> a = X[sw<NP>(i, j)], q = W[sw<NP>(i, j)];
       kNum += (a.x - q.x) * (a.x - q.x) + (a.y - q.y) * (a.y - q.y);
       kDen += a.x * a.x + a.y * a.y;
     });
@@ -495,32 +493,33 @@ __global__ void __launch_bounds__(BPC* Tile<NP>::TT) residual_kernel(ResidualArg
       wk = kind;
     }
   };
+  // four tiles per team: G (G^R), X, W, H; X keeps A = i (G - G^H) (D is no
+  // longer needed after r_D) until r_A is formed
   tile_for<NP, TT>(N, tt, [&](int i, int j) {
     const Cx<double> g = G[sw<NP>(i, j)], gt = G[sw<NP>(j, i)];
-    // A = i (G - G^H)
-    Y[sw<NP>(i, j)] = pi * cx<double>(g.x - gt.x, g.y + gt.y);
+    X[sw<NP>(i, j)] = pi * cx<double>(g.x - gt.x, g.y + gt.y);
   });
   team_sync<TT>(team);
-  witness(psd_of<NP, TT>(Y, one, H, N, tt, S, team), 0);
+  witness(psd_of<NP, TT>(X, one, H, N, tt, S, team), 0);
 
   // ---- Gamma = i (S> - S<), its positivity, r_A ---------------------------------
   __syncthreads();
-  load_tile<RS, NP, BPC>(p.SG, bX, e0, m, NE, Nk, N);
-  load_tile<RS, NP, BPC>(p.SL, bW, e0, m, NE, Nk, N);
+  load_tile<RS, NP, BPC>(p.SG, bW, e0, m, NE, Nk, N);
+  load_tile<RS, NP, BPC>(p.SL, bH, e0, m, NE, Nk, N);
   __syncthreads();
   tile_for<NP, TT>(N, tt, [&](int i, int j) {
-    const Cx<double> g = X[sw<NP>(i, j)], l = W[sw<NP>(i, j)];
-    X[sw<NP>(i, j)] = pi * cx<double>(g.x - l.x, g.y - l.y);
+    const Cx<double> g = W[sw<NP>(i, j)], l = H[sw<NP>(i, j)];
+    W[sw<NP>(i, j)] = pi * cx<double>(g.x - l.x, g.y - l.y);
   });
   team_sync<TT>(team);
-  witness(psd_of<NP, TT>(X, one, H, N, tt, S, team), 3);
-  team_matmul<double, double, NP>(G, X, W, N, tt, false);  // W = G Gam
+  witness(psd_of<NP, TT>(W, one, H, N, tt, S, team), 3);
+  team_matmul<double, double, NP>(G, W, H, N, tt, false);  // H = G Gam
   team_sync<TT>(team);
-  team_matmul<double, double, NP>(W, G, H, N, tt, true);   // H = G Gam G^H
+  team_matmul<double, double, NP>(H, G, W, N, tt, true);   // W = G Gam G^H
   team_sync<TT>(team);
   double aNum = 0, aDen = 0;
   tile_for<NP, TT>(N, tt, [&](int i, int j) {
-    const Cx<double> a = Y[sw<NP>(i, j)], q = H[sw<NP>(i, j)];
+    const Cx<double> a = X[sw<NP>(i, j)], q = W[sw<NP>(i, j)];
     aNum += (a.x - q.x) * (a.x - q.x) + (a.y - q.y) * (a.y - q.y);
     aDen += a.x * a.x + a.y * a.y;
   });
@@ -533,26 +532,26 @@ __global__ void __launch_bounds__(BPC* Tile<NP>::TT) residual_kernel(ResidualArg
     __syncthreads();
     team_matmul<double, double, NP>(G, X, W, N, tt, false);
     team_sync<TT>(team);
-    team_matmul<double, double, NP>(W, G, Y, N, tt, true);
+    team_matmul<double, double, NP>(W, G, X, N, tt, true);
     team_sync<TT>(team);
-    witness(psd_of<NP, TT>(Y, which == 0 ? mi : pi, H, N, tt, S, team), 4 + which);
+    witness(psd_of<NP, TT>(X, which == 0 ? mi : pi, H, N, tt, S, team), 4 + which);
   }
 
   // ---- G< : positivity and r_K against the candidate lesser self-energy ----------
   __syncthreads();
   const bool with_rk = p.part == RES_PART_ALL;  // launch-uniform
   load_tile<RS, NP, BPC>(p.GL, bX, e0, m, NE, Nk, N);
-  if (with_rk) load_tile<RS, NP, BPC>(p.SLc, bY, e0, m, NE, Nk, N);
+  if (with_rk) load_tile<RS, NP, BPC>(p.SLc, bW, e0, m, NE, Nk, N);
   __syncthreads();
   witness(psd_of<NP, TT>(X, mi, H, N, tt, S, team), 1);
   double kNum = 0, kDen = 0;
   if (with_rk) {
-    team_matmul<double, double, NP>(G, Y, W, N, tt, false);
+    team_matmul<double, double, NP>(G, W, H, N, tt, false);
     team_sync<TT>(team);
-    team_matmul<double, double, NP>(W, G, H, N, tt, true);
+    team_matmul<double, double, NP>(H, G, W, N, tt, true);
     team_sync<TT>(team);
     tile_for<NP, TT>(N, tt, [&](int i, int j) {
-      const Cx<double> a = X[sw<NP>(i, j)], q = H[sw<NP>(i, j)];
+      const Cx<double> a = X[sw<NP>(i, j)], q = W[sw<NP>(i, j)];
       kNum += (a.x - q.x) * (a.x - q.x) + (a.y - q.y) * (a.y - q.y);
       kDen += a.x * a.x + a.y * a.y;
     });
@@ -644,7 +643,8 @@ __global__ void residual_final_kernel(int ncta, const double* partial, double* o
 
 template <typename RS, int NP, int BPC> static int launch_residual_t(const ResidualArgs<RS>& a, cudaStream_t st) {
   constexpr int TT = Tile<NP>::TT;
-  constexpr size_t smem = 5 * (size_t)BPC * NP * NP * sizeof(Cx<double>) + BPC * sizeof(ResScratch<NP>);
+  // four tiles per team (G, X, W, H) and the scratch
+  constexpr size_t smem = 4 * (size_t)BPC * NP * NP * sizeof(Cx<double>) + BPC * sizeof(ResScratch<NP>);
   static bool configured = false;
   if (!configured) {
     QCL_CUDA_CHECK(cudaFuncSetAttribute(residual_kernel<RS, NP, BPC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -1290,6 +1290,7 @@ __global__ void __launch_bounds__(BPC* Tile<NP>::TT) anderson_guard_kernel(Guard
 
 template <typename RS, int NP, int BPC> static int launch_guard_t(const GuardArgs<RS>& a, cudaStream_t st) {
   constexpr int TT = Tile<NP>::TT;
+  // five tiles per team (R, L, G, H, W) and the scratch
   constexpr size_t smem = 5 * (size_t)BPC * NP * NP * sizeof(Cx<double>) + BPC * sizeof(ResScratch<NP>);
   static bool configured = false;
   if (!configured) {

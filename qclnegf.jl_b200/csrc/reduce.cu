@@ -269,6 +269,23 @@ template <typename R> __global__ void sum_fields_kernel(SumArgs<R> p) {
     p.out[i] = v;
   }
 }
+// complex64 with 16-byte aligned fields and even n: two elements per 16-byte
+// access (the same per-element sums)
+__global__ void sum_fields_pair_kernel(SumArgs<float> p) {
+  const size_t n2 = p.n / 2;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n2; i += (size_t)gridDim.x * blockDim.x) {
+    float4 v = reinterpret_cast<const float4*>(p.src[0])[i];
+    for (int j = 1; j < p.count; ++j) {
+      const float4 w = reinterpret_cast<const float4*>(p.src[j])[i];
+      v.x += w.x;
+      v.y += w.y;
+      v.z += w.z;
+      v.w += w.w;
+    }
+    reinterpret_cast<float4*>(p.out)[i] = v;
+  }
+}
+static bool aligned16(const void* q) { return ((uintptr_t)q & 15u) == 0; }
 
 int launch_sum_fields(int precision, size_t n, const void* const* src, int count, void* out, cudaStream_t st) {
   if (count < 1 || count > 8) {
@@ -284,11 +301,16 @@ int launch_sum_fields(int precision, size_t n, const void* const* src, int count
     sum_fields_kernel<double><<<grid_for(n, 256), 256, 0, st>>>(a);
   } else {
     SumArgs<float> a;
-    for (int j = 0; j < count; ++j) a.src[j] = (const Cx<float>*)src[j];
+    bool pairs = n % 2 == 0 && aligned16(out);
+    for (int j = 0; j < count; ++j) {
+      a.src[j] = (const Cx<float>*)src[j];
+      pairs = pairs && aligned16(src[j]);
+    }
     a.count = count;
     a.out = (Cx<float>*)out;
     a.n = n;
-    sum_fields_kernel<float><<<grid_for(n, 256), 256, 0, st>>>(a);
+    if (pairs) sum_fields_pair_kernel<<<grid_for(n / 2, 256), 256, 0, st>>>(a);
+    else sum_fields_kernel<float><<<grid_for(n, 256), 256, 0, st>>>(a);
   }
   QCL_LAUNCH_CHECK("sum_fields");
   return QCL_OK;
@@ -376,6 +398,43 @@ __global__ void __launch_bounds__(REDUCE_THREADS) residual_mix_multi_kernel(size
   }
 }
 
+// complex64 with 16-byte aligned fields and even n: two elements per 16-byte
+// access, each with the arithmetic of residual_mix_multi_kernel.
+__global__ void __launch_bounds__(REDUCE_THREADS) residual_mix_multi_pair_kernel(size_t n, MixFields<float> f,
+                                                                                double alpha, double* partial) {
+  const float4* __restrict__ old = reinterpret_cast<const float4*>(f.old[blockIdx.y]);
+  float4* __restrict__ new_ = reinterpret_cast<float4*>(f.cand[blockIdx.y]);
+  double v[2] = {0, 0};
+  const float al = (float)alpha, be = (float)(1.0 - alpha);
+  const size_t n2 = n / 2;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n2; i += (size_t)gridDim.x * blockDim.x) {
+    const float4 o4 = old[i], c4 = new_[i];
+    const Cx<float> os[2] = {cx<float>(o4.x, o4.y), cx<float>(o4.z, o4.w)};
+    const Cx<float> cs[2] = {cx<float>(c4.x, c4.y), cx<float>(c4.z, c4.w)};
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const Cx<float> o = os[h], c = cs[h];
+      const double dx = (double)c.x - o.x, dy = (double)c.y - o.y;
+      const double d2 = dx * dx + dy * dy, n2v = (double)c.x * c.x + (double)c.y * c.y;
+      if (isfinite(d2) && isfinite(n2v) && isfinite((double)o.x) && isfinite((double)o.y)) {
+        v[0] += d2;
+        v[1] += n2v;
+      } else {
+        v[0] = INFINITY;
+      }
+    }
+    if (alpha > 0)
+      new_[i] = make_float4(be * os[0].x + al * cs[0].x, be * os[0].y + al * cs[0].y, be * os[1].x + al * cs[1].x,
+                            be * os[1].y + al * cs[1].y);
+  }
+  block_sum<2>(v);
+  if (threadIdx.x == 0) {
+    double* pp = partial + 2 * ((size_t)blockIdx.y * gridDim.x + blockIdx.x);
+    pp[0] = v[0];
+    pp[1] = v[1];
+  }
+}
+
 // One CTA per segment: out[2 s + k] = sum_c partial[s][c][k], fixed order.
 __global__ void combine_segments_kernel(const double* partial, int count, double* out) {
   const double* seg = partial + 2 * (size_t)blockIdx.x * count;
@@ -410,11 +469,14 @@ int launch_residual_mix_multi(int precision, size_t n, const void* const* old, v
     residual_mix_multi_kernel<double><<<grid, REDUCE_THREADS, 0, st>>>(n, f, alpha, partial);
   } else {
     MixFields<float> f{};
+    bool pairs = n % 2 == 0;
     for (int i = 0; i < nf; ++i) {
       f.old[i] = (const Cx<float>*)old[i];
       f.cand[i] = (Cx<float>*)cand[i];
+      pairs = pairs && aligned16(old[i]) && aligned16(cand[i]);
     }
-    residual_mix_multi_kernel<float><<<grid, REDUCE_THREADS, 0, st>>>(n, f, alpha, partial);
+    if (pairs) residual_mix_multi_pair_kernel<<<grid, REDUCE_THREADS, 0, st>>>(n, f, alpha, partial);
+    else residual_mix_multi_kernel<float><<<grid, REDUCE_THREADS, 0, st>>>(n, f, alpha, partial);
   }
   combine_segments_kernel<<<nf, REDUCE_THREADS, 0, st>>>(partial, MIX_CTAS, out);
   QCL_LAUNCH_CHECK("residual_mix_multi");

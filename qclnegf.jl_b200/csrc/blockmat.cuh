@@ -88,7 +88,10 @@ template <typename RM, int NP> struct MatTile {
 template <typename RS, typename RM, int NP>
 __device__ __forceinline__ void team_matmul_regs(const Cx<RS>* A, const Cx<RS>* B, MatTile<RM, NP>& acc, int N,
                                                  int tt, bool adjB) {
-  constexpr int TR = Tile<NP>::TR, TC = Tile<NP>::TC, RG = NP / TR;
+  // thread (rg, cg) owns rows rg + RG t and columns cg + CG u: the rows a warp
+  // reads together differ in their low three bits, so the swizzled column walk
+  // of A (and of B^H) is free of bank conflicts
+  constexpr int TR = Tile<NP>::TR, TC = Tile<NP>::TC, RG = NP / TR, CG = NP / TC;
   const int rg = tt % RG, cg = tt / RG;
 #pragma unroll
   for (int t = 0; t < TR; ++t)
@@ -97,10 +100,10 @@ __device__ __forceinline__ void team_matmul_regs(const Cx<RS>* A, const Cx<RS>* 
   for (int l = 0; l < N; ++l) {
     Cx<RM> a[TR], b[TC];
 #pragma unroll
-    for (int t = 0; t < TR; ++t) a[t] = cvt<RM>(A[sw<NP>(rg * TR + t, l)]);
+    for (int t = 0; t < TR; ++t) a[t] = cvt<RM>(A[sw<NP>(rg + RG * t, l)]);
 #pragma unroll
     for (int u = 0; u < TC; ++u) {
-      const int j = cg * TC + u;
+      const int j = cg + CG * u;
       b[u] = adjB ? conj(cvt<RM>(B[sw<NP>(j, l)])) : cvt<RM>(B[sw<NP>(l, j)]);
     }
 #pragma unroll
@@ -112,12 +115,12 @@ __device__ __forceinline__ void team_matmul_regs(const Cx<RS>* A, const Cx<RS>* 
 
 template <typename RS, typename RM, int NP>
 __device__ __forceinline__ void team_store_regs(Cx<RS>* C, const MatTile<RM, NP>& acc, int tt) {
-  constexpr int TR = Tile<NP>::TR, TC = Tile<NP>::TC, RG = NP / TR;
+  constexpr int TR = Tile<NP>::TR, TC = Tile<NP>::TC, RG = NP / TR, CG = NP / TC;
   const int rg = tt % RG, cg = tt / RG;
 #pragma unroll
   for (int t = 0; t < TR; ++t)
 #pragma unroll
-    for (int u = 0; u < TC; ++u) C[sw<NP>(rg * TR + t, cg * TC + u)] = cvt<RS>(acc.v[t][u]);
+    for (int u = 0; u < TC; ++u) C[sw<NP>(rg + RG * t, cg + CG * u)] = cvt<RS>(acc.v[t][u]);
 }
 
 

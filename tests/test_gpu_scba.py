@@ -78,6 +78,24 @@ def test_scba_tutorial_reduced_precision_current(gpu_ops, precision):
     s2.close()
 
 
+def test_scba_all_mechanisms_mixed_current_within_target(gpu_ops):
+    """The mixed-precision target: with every mechanism on (dense LO and
+    impurity maps on the tensor cores as scaled FP16 pairs, FP32 FFT Hilbert
+    with the roundoff check), J of each iteration within 1e-6 relative of the
+    FP64 device run."""
+    from qclb200.problem import small_problem
+    from qclb200.scba import solve_scba_production
+
+    pr = small_problem(NE=256, Nk=8, Nb=16, mechanisms=("LO", "acoustic", "impurity", "IFR", "alloy"))
+    ref, s1 = solve_scba_production(pr, 6)
+    got, s2 = solve_scba_production(pr, 6, precision="mixed")
+    s1.close()
+    s2.close()
+    for a, b in zip(ref, got):
+        assert abs(a["J"] - b["J"]) <= 1e-6 * abs(a["J"]), (a["J"], b["J"])
+        assert abs(a["lam"] - b["lam"]) <= 1e-6
+
+
 def test_scba_graph_replay_is_identical(gpu_ops):
     from qclb200.problem import small_problem
     from qclb200.scba import solve_scba_production

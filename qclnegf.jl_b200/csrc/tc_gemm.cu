@@ -415,19 +415,6 @@ __global__ void tc_split_a_kernel(int NE, int Nc, int Mpad, int Kpad, const Cx<f
   }
 }
 
-// B[2j + c'][2k + c] from the complex operator M (column-major Nc x Nc,
-// complex64) and the momentum weights wk[k % Nk]:
-//   [[Re, -Im], [Im, Re]] * w  (rows c' = 0 real part of the output, 1 imaginary).
-__device__ __forceinline__ float tc_b_value(int nn, int kk, int Nc, int Nk, const Cx<float>* __restrict__ Mop,
-                                            const double* __restrict__ wk) {
-  const int j = nn >> 1, k = kk >> 1;
-  if (j >= Nc || k >= Nc) return 0.0f;
-  const Cx<float> m = Mop[(size_t)j + (size_t)Nc * k];
-  const float w = (float)wk[k % Nk];
-  const int cp = nn & 1, c = kk & 1;
-  const float val = (cp == c) ? m.x : (cp == 0 ? -m.y : m.y);
-  return w * val;
-}
 // max |B| into *mxbits (non-negative FP32 bits order as unsigned integers;
 // a non-finite entry gives +inf).
 __global__ void tc_b_maxabs_kernel(int Nc, int Nk, const Cx<float>* __restrict__ Mop,
@@ -444,15 +431,34 @@ __global__ void tc_b_maxabs_kernel(int Nc, int Nk, const Cx<float>* __restrict__
   for (int o = 16; o > 0; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
   if ((threadIdx.x & 31) == 0) atomicMax(mxbits, __float_as_uint(mx));
 }
-__global__ void tc_build_b_kernel(int Nc, int Nk, int Npad, int Kpad, const Cx<float>* __restrict__ Mop,
+// B[2j + c'][2k + c] from the complex operator M (column-major Nc x Nc,
+// complex64) and the momentum weights wk[k % Nk]:
+//   s_B [[Re, -Im], [Im, Re]] * w  (rows c' = 0 real part of the output, 1 imaginary),
+// as fp16 hi / lo.  One CTA per 32 (j) x 16 (k) tile of M: M is read
+// coalesced along j into shared memory, B written coalesced along its K axis
+// (each M entry feeds a 2 x 2 block of B; the padding past Nc is zero).
+__global__ void tc_build_b_kernel(int Nc, int Nk, int Kpad, const Cx<float>* __restrict__ Mop,
                                   const double* __restrict__ wk, const unsigned* __restrict__ mxbits,
                                   __half* __restrict__ Bhi, __half* __restrict__ Blo, float* __restrict__ binv) {
+  __shared__ Cx<float> tile[16][33];  // [k][j]
   const float sc = tc_scale_for(__uint_as_float(*mxbits));
-  if (blockIdx.x == 0 && threadIdx.x == 0) *binv = 1.0f / sc;
-  const long long n = (long long)Npad * Kpad;
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
-    const int nn = (int)(i / Kpad), kk = (int)(i % Kpad);
-    split_f16(sc * tc_b_value(nn, kk, Nc, Nk, Mop, wk), Bhi[i], Blo[i]);
+  if (blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0) *binv = 1.0f / sc;
+  const int j0 = blockIdx.x * 32, k0 = blockIdx.y * 16;
+  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;  // 32 x 8 threads
+  for (int r = ty; r < 16; r += 8) {
+    const int j = j0 + tx, k = k0 + r;
+    tile[r][tx] = (j < Nc && k < Nc) ? Mop[(size_t)j + (size_t)Nc * k] : cx<float>(0, 0);
+  }
+  __syncthreads();
+  // 64 rows x 32 columns of B: thread column kk = 2 k0 + tx, rows in steps of 8
+  const int kk = 2 * k0 + tx, kl = tx >> 1, c = tx & 1, k = k0 + kl;
+  const float w = k < Nc ? (float)wk[k % Nk] : 0.0f;
+  for (int rr = ty; rr < 64; rr += 8) {
+    const int nn = 2 * j0 + rr, jl = rr >> 1, cp = rr & 1;
+    const Cx<float> m = tile[kl][jl];
+    const float val = (cp == c) ? m.x : (cp == 0 ? -m.y : m.y);
+    const size_t i = (size_t)nn * Kpad + kk;
+    split_f16(sc * (w * val), Bhi[i], Blo[i]);
   }
 }
 
@@ -485,8 +491,8 @@ int tc_build_operator(int Nc, int Nk, const void* Mop_c64, const double* wk, voi
   QCL_CUDA_CHECK(cudaMemsetAsync(mxbits, 0, sizeof(unsigned), st));
   tc_b_maxabs_kernel<<<148 * 4, 256, 0, st>>>(Nc, Nk, (const Cx<float>*)Mop_c64, wk, mxbits);
   QCL_LAUNCH_CHECK("tc_b_maxabs_kernel");
-  tc_build_b_kernel<<<148 * 8, 256, 0, st>>>(Nc, Nk, Npad, Kpad, (const Cx<float>*)Mop_c64, wk, mxbits, Bhi,
-                                             Bhi + n, binv);
+  tc_build_b_kernel<<<dim3(Npad / 64, Kpad / 32), 256, 0, st>>>(Nc, Nk, Kpad, (const Cx<float>*)Mop_c64, wk, mxbits,
+                                                                 Bhi, Bhi + n, binv);
   QCL_LAUNCH_CHECK("tc_build_b_kernel");
   return QCL_OK;
 }

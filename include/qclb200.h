@@ -48,6 +48,7 @@ extern "C" {
 #define QCL_KERNEL_DENSE 1
 #define QCL_KERNEL_IFR 2
 #define QCL_KERNEL_LOW_RANK 3
+#define QCL_KERNEL_SEPARABLE_SUM 4
 
 #define QCL_C128 0
 #define QCL_C64 1
@@ -135,6 +136,20 @@ int qcl_apply_energy_shift(int precision, int NE, size_t ncols, const double* ep
  *   QCL_KERNEL_LOW_RANK              left (Nk N^2, J), right = right_adjoint (J, Nk N^2),
  *                                    J = rank >= 1 (LowRankProductionKernel, built by
  *                                    _low_rank_production_kernel, production_cache.jl:348-385)
+ *   QCL_KERNEL_SEPARABLE_SUM         radial (Nk, Nk, J), block (N^2, N^2, J) -- rows (a,b),
+ *                                    cols (c,d) per term: K(m,m') = sum_i radial_i(m,m') block_i,
+ *                                    J >= 1 terms.  The Kronecker-sum form of the
+ *                                    momentum-dependent kernels: the exact LO kernel
+ *                                    sum_h R_h(m,m') F_h (x) conj F_h (lo_phonon_kernel,
+ *                                    numerics/reference/kernels.jl:321-356) and the tabulated
+ *                                    kernels sum_t W_t(m,m') C(q_t) (numerics/optimized/
+ *                                    kernels.jl:303-320) are such sums; a host-side
+ *                                    compression keeps J small.  The SeparableIFR operator
+ *                                    (production_operators.jl:467-533) is the J = 1 case.
+ *                                    The contraction costs 8 J N_k N^4 N_E real flop per map
+ *                                    against 8 N_k^2 N^4 N_E for the dense matrix, and the
+ *                                    operator holds (N_k^2 + N^4) J entries instead of
+ *                                    (N_k N^2)^2.
  * q is the kernel scale q^K; is_LO selects the phonon-shifted contraction in
  * the SCBA loop. */
 typedef struct qcl_mechanism {
@@ -325,7 +340,32 @@ typedef struct qcl_scba_problem {
   int anderson_history_depth;
   double anderson_damping;
   double anderson_regularization;
+  /* Execution budget of the memory preflight in bytes (ProductionOptions.
+   * memory_budget_bytes, production_contracts.jl:143-165); 0 = the device's
+   * free memory when the context is created.  qcl_scba_create refuses with
+   * QCL_NOMEM, before any allocation, when the estimated peak exceeds it
+   * (build_production_cache, numerics/optimized/production_cache.jl:764-770). */
+  size_t memory_budget_bytes;
+  /* 1: a QCL_C64 / QCL_MIXED context that reserves complex128 fields and
+   * keeps complex128 operator copies, so that qcl_scba_promote can finish the
+   * solve in FP64 (mixed-precision iterations, then FP64 refinement of the
+   * fixed point); 0 otherwise. */
+  int refinement;
 } qcl_scba_problem;
+
+/* Device-memory estimate of qcl_scba_create (bytes): the SCBA fields (state
+ * and candidate families, G, totals, scratch fields), the operators (with the
+ * tensor-core operands and refinement copies), the contraction / reduction /
+ * FFT workspace, the Anderson history, their sum (resident) and the peak
+ * during creation (resident plus the largest complex128 staging copy of an
+ * operator array).  The role of _estimate_production_memory
+ * (numerics/optimized/production_cache.jl:475-668) for this library's own
+ * allocation plan. */
+typedef struct qcl_memory_estimate {
+  size_t fields, operators, workspace, anderson, resident, peak;
+} qcl_memory_estimate;
+int qcl_scba_estimate_memory(const qcl_scba_problem* problem, const qcl_mechanism* mechanisms,
+                             qcl_memory_estimate* out);
 
 /* Mixer diagnostics of the last step (the metrics _anderson_mix! reports,
  * production_mixing.jl:283-298).  reset_reason: 0 none, 1 residual_increase,
@@ -403,6 +443,17 @@ int qcl_anderson_guard(int precision, int NE, int Nk, int Nb, int nfam, const vo
 int qcl_scba_density_matrix(qcl_scba* ctx, void* rho);
 /* Anderson mixer diagnostics of the last step (all zero for linear mixing). */
 int qcl_scba_mixer_info(qcl_scba* ctx, qcl_anderson_info* info);
+/* FP64 refinement: switches a context created with refinement = 1 from
+ * QCL_C64 / QCL_MIXED to QCL_C128 for the steps that follow.  The current
+ * state (with the last step's mixing committed) is converted exactly to
+ * complex128 and the next step continues from it; operators switch to their
+ * complex128 copies; the Anderson history restarts.  The north-star scheme
+ * "FP32 bulk, FP64 refinement of the fixed point": iterate in mixed precision
+ * until r_Sigma reaches its FP32 floor, then converge in FP64 (no reference
+ * counterpart: the reference has no reduced precision,
+ * application/algorithm_registry.jl:226-240).  QCL_ARG if the context was
+ * not created for refinement; a no-op on a QCL_C128 context. */
+int qcl_scba_promote(qcl_scba* ctx);
 /* Replay each iteration as one captured CUDA graph (default off). */
 int qcl_scba_use_graph(qcl_scba* ctx, int enable);
 /* The derived GreenState fields of the last Dyson solve (seed or step) --

@@ -275,6 +275,14 @@ def contraction(mech, G, wk, alpha=1.0, beta=0.0, S=None):
         J = mech.left.shape[1]
         lib().orc_contraction_ifr(NE, Nk, Nb, J, _p(_field(mech.left)), _p(_field(mech.right)),
                                   _p(_field(mech.radial)), _p(G), _p(wk), aq, float(beta), _p(S))
+    elif mech.kind == "separable_sum":
+        # The reference has no Kronecker-sum operator: its contraction of the
+        # same kernel is the dense BLAS map (production_operators.jl:402-465)
+        # of the permuted six-index tensor (_production_kernel,
+        # production_cache.jl:400-405), which is what is evaluated here.
+        K = mech.literal_kernel(Nk, Nb)
+        M = np.transpose(K, (0, 2, 5, 1, 3, 4)).reshape((Nk * Nb * Nb, Nk * Nb * Nb), order="F")
+        lib().orc_contraction_dense(NE, Nk, Nb, _p(_field(M)), _p(G), _p(wk), aq, float(beta), _p(S))
     elif mech.kind == "low_rank":
         r = mech.left.shape[1]
         lib().orc_contraction_low_rank(NE, Nk, Nb, r, _p(_field(mech.left)), _p(_field(mech.right)), _p(G),

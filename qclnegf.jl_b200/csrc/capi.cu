@@ -139,6 +139,8 @@ int scba_set_graph(ScbaCtx* c, int enable);
 int scba_green_state(ScbaCtx* c, void* A, double* kappa, double* scale);
 int scba_witness(ScbaCtx* c, double* out12);
 int scba_retarget(ScbaCtx* c, double Ep, double N_LO, double kBT, const void* h, const double* q);
+int scba_estimate_memory(const qcl_scba_problem* p, const qcl_mechanism* mechs, size_t out[6]);
+int scba_promote(ScbaCtx* c);
 int scba_mixer_info(ScbaCtx* c, qcl_anderson_info* out);
 int scba_density_matrix(ScbaCtx* c, void* out);
 
@@ -444,6 +446,15 @@ int qcl_static_contraction(int precision, const qcl_mechanism* op, int NE, int N
     if ((s = upload_converted(sp, op->right, nc * op->J, ri))) return s;
     k.left = le.p;
     k.right = ri.p;
+  } else if (op->kind == QCL_KERNEL_SEPARABLE_SUM) {
+    if (op->J < 1) {
+      set_last_error("separable-sum operator needs J >= 1 terms");
+      return QCL_ARG;
+    }
+    if ((s = upload_converted(sp, op->radial, (size_t)Nk * Nk * op->J, ra))) return s;
+    if ((s = upload_converted(sp, op->block, N2 * N2 * op->J, blk))) return s;
+    k.radial = ra.p;
+    k.block = blk.p;
   } else {
     set_last_error("unknown kernel kind %d", op->kind);
     return QCL_ARG;
@@ -461,6 +472,24 @@ int qcl_static_contraction(int precision, const qcl_mechanism* op, int NE, int N
   if (op->kind == QCL_KERNEL_DENSE && sp == QCL_C64) {  // complex64: tensor-core operand
     if ((s = tc_build_operator(Nk * (int)N2, Nk, mat.p, (const double*)dwk.p, &bop, 0))) return s;
     k.tc_bop = bop;
+    k.status = (int*)st.p;
+  }
+  std::vector<void*> chunk_ops;  // separable sum, complex64: one tensor-core operand per term chunk
+  struct ChunkFree {
+    std::vector<void*>* v;
+    ~ChunkFree() {
+      for (void* q : *v) cudaFree(q);
+    }
+  } chunk_free{&chunk_ops};
+  if (op->kind == QCL_KERNEL_SEPARABLE_SUM && sp == QCL_C64) {
+    for (int i0 = 0; i0 < op->J; i0 += kSepChunk) {
+      const int jc = std::min(kSepChunk, op->J - i0);
+      void* b = nullptr;
+      s = tc_build_operator2((int)N2, jc * (int)N2, 1, (const Cx<float>*)blk.p + N2 * N2 * i0, nullptr, &b, 0);
+      if (b) chunk_ops.push_back(b);
+      if (s) return s;
+    }
+    k.tc_chunks = chunk_ops.data();
     k.status = (int*)st.p;
   }
   if ((s = dG.upload(G, nb))) return s;
@@ -691,6 +720,32 @@ int qcl_scba_retarget(qcl_scba* ctx, double Ep, double N_LO, double kBT, const v
     return QCL_ARG;
   }
   return scba_retarget((ScbaCtx*)ctx, Ep, N_LO, kBT, h, q);
+}
+
+int qcl_scba_estimate_memory(const qcl_scba_problem* problem, const qcl_mechanism* mechanisms,
+                             qcl_memory_estimate* out) {
+  if (!problem || !out || (problem->nmech > 0 && !mechanisms)) {
+    set_last_error("problem, mechanisms and out are required");
+    return QCL_ARG;
+  }
+  size_t v[6];
+  int s = scba_estimate_memory(problem, mechanisms, v);
+  if (s) return s;
+  out->fields = v[0];
+  out->operators = v[1];
+  out->workspace = v[2];
+  out->anderson = v[3];
+  out->resident = v[4];
+  out->peak = v[5];
+  return QCL_OK;
+}
+
+int qcl_scba_promote(qcl_scba* ctx) {
+  if (!ctx) {
+    set_last_error("ctx is required");
+    return QCL_ARG;
+  }
+  return scba_promote((ScbaCtx*)ctx);
 }
 
 int qcl_anderson_guard(int precision, int NE, int Nk, int Nb, int nfam, const void* const* fields,

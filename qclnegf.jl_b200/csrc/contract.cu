@@ -8,7 +8,9 @@
 //                         S[e,m,(a,b)] broadcast over m;
 //   dense:                S[e,(m,a,b)] = sum_(m',c,d) M wk[m'] G[e,(m',c,d)];
 //   separable IFR:        S = left * (radial * (wk .* (right * G)));
-//   low rank:             S = left * (right_adjoint * (wk .* G)).
+//   low rank:             S = left * (right_adjoint * (wk .* G));
+//   separable sum:        S[e,m,(a,b)] = sum_i sum_(c,d) block_i[(a,b),(c,d)]
+//                                        sum_m' radial_i[m,m'] wk[m'] G[e,m',c,d].
 // Every stage is one call of a tiled complex GEMM whose operand and output
 // index maps are strided views of the E-fastest fields: the energy axis is the
 // GEMM's M dimension, so all A loads and C stores are coalesced along E.
@@ -527,6 +529,58 @@ static int contraction_t(const KernelOpDev& op, int NE, int Nk, int N, const dou
     f.alpha = alpha_q; f.beta = beta;
     return launch_gemm<R>(f, st);
   }
+  if (op.kind == QCL_KERNEL_SEPARABLE_SUM) {
+    // K(m,m') = sum_i radial_i(m,m') block_i: a Kronecker sum of J terms (the
+    // exact LO form sum_h R_h(m,m') F_h (x) conj F_h of lo_phonon_kernel,
+    // numerics/reference/kernels.jl:321-356, and the tabulated kernels of
+    // numerics/optimized/kernels.jl:303-320, compressed on the host).  Per
+    // chunk of up to kSepChunk terms:
+    //   stage 1 (term i, batch (c,d)):  Z_i[e + NE m + NE Nk (c,d)] =
+    //            sum_m' radial_i[m + Nk m'] wk[m'] G[e + NE m' + NE Nk (c,d)]
+    //   stage 2 (one GEMM over the chunk, K = (c,d,i)):
+    //            S[(e,m), (a,b)] = alpha q sum_k Z[(e,m), k] block[(a,b), k] + beta S
+    // The rows of stage 2 are the (e, m) pairs, contiguous in the E-fastest
+    // layout, so S and Z are plain column-major (NE Nk) x N^2 matrices.
+    const int J = op.J;
+    const long long Mr = NEl * Nk;                // stage-2 rows
+    const size_t zfield = (size_t)Mr * N2;        // one intermediate field
+    Cx<R>* Z = (Cx<R>*)work;
+    const int jmax = J < kSepChunk ? J : kSepChunk;  // terms per chunk
+    float* awork = (float*)((char*)work + (size_t)jmax * zfield * sizeof(Cx<R>));
+    int s;
+    for (int c = 0, i0 = 0; i0 < J; ++c, i0 += kSepChunk) {
+      const int jc = min(kSepChunk, J - i0);
+      for (int i = i0; i < i0 + jc; ++i) {
+        GemmArgs<R> g{};
+        g.M = NE; g.Nout = Nk; g.K = Nk; g.batch = N2;
+        g.A = G; g.lda = NEl; g.a_b = Mr; g.wk = wk; g.wk_mod = Nk;
+        g.B = (const Cx<R>*)op.radial + (size_t)Nk * Nk * i; g.ldb_j = 1; g.ldb_k = Nk; g.b_b = 0;
+        g.C = Z + zfield * (i - i0); g.ldc = NEl; g.c_b = Mr; g.bcast = 1;
+        g.alpha = 1.0; g.beta = 0.0;
+        if ((s = launch_gemm<R>(g, st))) return s;
+      }
+      const double bc = c == 0 ? beta : 1.0;
+      const Cx<R>* blk = (const Cx<R>*)op.block + (size_t)N2 * N2 * i0;
+      if (sizeof(R) == 8) {
+        DmArgs d{(int)Mr, N2, jc * N2, (const Cx<double>*)Z, Mr, nullptr, 1, (const Cx<double>*)blk, N2,
+                 (Cx<double>*)Sv, Mr, alpha_q, bc};
+        if ((s = launch_dmma_dense(d, st))) return s;
+      } else if (op.tc_chunks) {
+        if ((s = launch_tc_contraction2((int)Mr, N2, jc * N2, op.tc_chunks[c], Z, Sv, alpha_q, bc, awork, op.status,
+                                        st)))
+          return s;
+      } else {
+        GemmArgs<R> f{};
+        f.M = (int)Mr; f.Nout = N2; f.K = jc * N2; f.batch = 1;
+        f.A = Z; f.lda = Mr;
+        f.B = blk; f.ldb_j = 1; f.ldb_k = N2;
+        f.C = S; f.ldc = Mr; f.bcast = 1;
+        f.alpha = alpha_q; f.beta = bc;
+        if ((s = launch_gemm<R>(f, st))) return s;
+      }
+    }
+    return QCL_OK;
+  }
   set_last_error("unknown kernel operator kind %d", op.kind);
   return QCL_ARG;
 }
@@ -536,6 +590,14 @@ size_t contraction_work_elems(const KernelOpDev& op, int NE, int Nk, int N) {
   if (op.kind == QCL_KERNEL_DENSE && op.tc_bop) return (tc_a_work_floats(NE, Nk * N * N) + 1) / 2;  // complex64 units
   if (op.kind == QCL_KERNEL_IFR) return 2 * (size_t)NE * op.J * Nk;
   if (op.kind == QCL_KERNEL_LOW_RANK) return (size_t)NE * op.J;
+  if (op.kind == QCL_KERNEL_SEPARABLE_SUM) {
+    // kSepChunk intermediate fields (field precision), then for complex64
+    // tensor-core chunks the stage-2 A operand (floats) in complex64 units
+    const int jmax = op.J < kSepChunk ? op.J : kSepChunk;
+    const size_t zf = (size_t)jmax * NE * Nk * N * N;
+    if (op.tc_chunks) return zf + (tc_a_work_floats2(NE * Nk, jmax * N * N) + 1) / 2;
+    return zf;
+  }
   return 0;
 }
 

@@ -104,16 +104,28 @@ struct KernelOpDev {
   const void* matrix = nullptr;  // (Nk N^2)^2: rows (m,a,b), cols (m',c,d)
   const void* left = nullptr;    // IFR (N^2, J); low rank (Nk N^2, rank)
   const void* right = nullptr;   // IFR (J, N^2); low rank right_adjoint (rank, Nk N^2)
-  const void* radial = nullptr;  // (Nk, Nk)
+  const void* radial = nullptr;  // IFR (Nk, Nk); separable sum (Nk, Nk, J)
   // dense operators, complex64 fields: tensor-core operand (scaled FP16 hi/lo
   // pair) prepared by tc_build_operator; when set, the contraction runs on tcgen05
   const void* tc_bop = nullptr;
+  // separable sums, complex64 fields: one prepared operand per chunk of
+  // kSepChunk terms (host array of device pointers)
+  const void* const* tc_chunks = nullptr;
   int* status = nullptr;  // device status word for bounded-wait timeouts
 };
+// Terms of a separable-sum operator contracted per stage-2 GEMM: the
+// intermediate of a chunk holds kSepChunk fields.
+constexpr int kSepChunk = 8;
+inline int sep_chunks(int J) { return (J + kSepChunk - 1) / kSepChunk; }
 size_t contraction_work_elems(const KernelOpDev& op, int NE, int Nk, int N);
 // tensor-core dense contraction (tc_gemm.cu)
 int tc_build_operator(int Nc, int Nk, const void* Mop_c64, const double* wk, void** Bop, cudaStream_t st);
+int tc_build_operator2(int Nout, int Kc, int Nk, const void* Mop_c64, const double* wk, void** Bop, cudaStream_t st);
 size_t tc_a_work_floats(int NE, int Nc);
+size_t tc_a_work_floats2(int M, int Kc);
+size_t tc_operator_bytes(int Nout, int Kc);
+int launch_tc_contraction2(int M, int Nout, int Kc, const void* Bop, const void* A, void* S, double alpha,
+                           double beta, float* awork, int* status, cudaStream_t st);
 int launch_tc_dense_contraction(int NE, int Nc, const void* Bop, const void* G, void* S, double alpha, double beta,
                                 float* awork, int* status, cudaStream_t st);
 int launch_contraction(int precision, const KernelOpDev& op, int NE, int Nk, int N, const double* wk, const void* G,
@@ -171,5 +183,6 @@ int launch_seed_green(int precision, int NE, int Nk, int N, const void* GR, cons
 int launch_residual_pair(int precision, size_t n, const void* o1, const void* o2, const void* n1, const void* n2,
                          double* partial, double* out2, cudaStream_t st);
 int launch_convert(int precision, size_t n, const void* in_c128, void* out, cudaStream_t st);
+int launch_promote(size_t n, const void* in_c64, void* out_c128, cudaStream_t st);
 
 }  // namespace qcl

@@ -141,4 +141,19 @@ int launch_convert(int precision, size_t n, const void* in_c128, void* out, cuda
   return QCL_OK;
 }
 
+// complex64 -> complex128 (exact): the FP64 refinement of a mixed-precision
+// state.
+__global__ void promote_kernel(size_t n, const Cx<float>* __restrict__ in, Cx<double>* __restrict__ out) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    const Cx<float> v = in[i];
+    out[i] = cx<double>((double)v.x, (double)v.y);
+  }
+}
+
+int launch_promote(size_t n, const void* in_c64, void* out_c128, cudaStream_t st) {
+  promote_kernel<<<gcap((long long)n, 256), 256, 0, st>>>(n, (const Cx<float>*)in_c64, (Cx<double>*)out_c128);
+  QCL_LAUNCH_CHECK("promote");
+  return QCL_OK;
+}
+
 }  // namespace qcl

@@ -43,10 +43,14 @@ struct Mech {
   void* right = nullptr;
   void* radial = nullptr;
   void* tc_bop = nullptr;  // dense operator prepared for the tensor cores (complex64 fields)
+  // complex128 copies of the operator arrays (refinement contexts): swapped in by promote
+  void *block64 = nullptr, *matrix64 = nullptr, *left64 = nullptr, *right64 = nullptr, *radial64 = nullptr;
+  std::vector<void*> tc_chunks;  // separable sum: tensor-core operand per term chunk (complex64 fields)
   int* status = nullptr;
   KernelOpDev view() const {
     KernelOpDev k;
     k.tc_bop = tc_bop;
+    k.tc_chunks = tc_chunks.empty() ? nullptr : tc_chunks.data();
     k.status = status;
     k.kind = kind;
     k.J = J;
@@ -74,6 +78,7 @@ enum {
 
 struct ScbaCtx {
   int NE, Nk, N, M, precision, gs, verify;
+  int refinement = 0;  // FP64-sized state and complex128 operator copies for qcl_scba_promote
   int diagonal = 0, averaged = 0, drop_real = 0, direct_green = 0;  // scattering-model switches
   int scalar_lesser = 0;                                             // occupation_normalization
   // Anderson mixing (mixing = :anderson): device history and mixer state
@@ -85,7 +90,9 @@ struct ScbaCtx {
   double* apartial = nullptr;
   double wk_sum = 0;
   double Ep, hw_LO, N_LO, target, eta_seed, kBT, alpha, J0;
-  size_t nfield, fbytes;
+  double de = 0;  // uniform energy spacing (FFT tables)
+  size_t nfield, fbytes;  // elements per field, bytes per field at the active precision
+  size_t fcap = 0;        // allocated bytes per field (complex128 size in refinement contexts)
   cudaStream_t st = nullptr;
   // grids and operators
   double *eps = nullptr, *wE = nullptr, *wk = nullptr;
@@ -100,6 +107,7 @@ struct ScbaCtx {
   void* candSL = nullptr;
   void* tmp = nullptr;
   void* cwork = nullptr;
+  size_t cwork_bytes = 0;
   // reductions
   Cx<double>*trL = nullptr, *trG = nullptr;
   double* rpartial = nullptr;
@@ -147,17 +155,24 @@ template <typename T> static int dupload(T** p, const void* host, size_t bytes, 
   return QCL_OK;
 }
 
-static int upload_op(ScbaCtx* c, void** dst, const void* host_c128, size_t n) {
+// Uploads an operator array in the context's precision; a refinement context
+// of reduced precision also keeps the complex128 array (*keep64) for promote.
+static int upload_op(ScbaCtx* c, void** dst, const void* host_c128, size_t n, void** keep64 = nullptr) {
   void* tmp = nullptr;
   int s = dupload(&tmp, host_c128, n * 16, c->st);
   if (s) return s;
-  if ((s = dalloc(dst, n * (c->precision == QCL_C128 ? 16 : 8)))) {
+  if (c->precision == QCL_C128) {
+    *dst = tmp;
+    return QCL_OK;
+  }
+  if ((s = dalloc(dst, n * 8))) {
     cudaFree(tmp);
     return s;
   }
   s = launch_convert(c->precision, n, tmp, *dst, c->st);
   cudaStreamSynchronize(c->st);
-  cudaFree(tmp);
+  if (c->refinement && keep64) *keep64 = tmp;
+  else cudaFree(tmp);
   return s;
 }
 
@@ -212,6 +227,8 @@ void scba_destroy(ScbaCtx* c) {
     cudaFree(m.right);
     cudaFree(m.radial);
     cudaFree(m.tc_bop);
+    for (void* q : m.tc_chunks) cudaFree(q);
+    for (void* q : {m.block64, m.matrix64, m.left64, m.right64, m.radial64}) cudaFree(q);
   }
   for (void* p : c->state) cudaFree(p);
   for (void* p : c->cand) cudaFree(p);
@@ -244,6 +261,93 @@ void scba_destroy(ScbaCtx* c) {
   delete c;
 }
 
+// ---------------------------------------------------------------------------
+// Memory preflight (the estimate and refusal of build_production_cache,
+// numerics/optimized/production_cache.jl:475-668, 764-770): the device bytes
+// scba_create allocates, computed before the first allocation.
+// ---------------------------------------------------------------------------
+struct MemPlan {
+  size_t fields = 0, operators = 0, workspace = 0, anderson = 0, transient = 0;
+  size_t resident() const { return fields + operators + workspace + anderson; }
+  size_t peak() const { return resident() + transient; }
+};
+
+// Element counts of a mechanism's operator arrays (as uploaded).
+static std::vector<size_t> op_arrays(const qcl_mechanism& q, int Nk, int N) {
+  const size_t N2 = (size_t)N * N, nc = (size_t)Nk * N2, J = q.J > 0 ? (size_t)q.J : 0;
+  switch (q.kind) {
+    case QCL_KERNEL_MOMENTUM_INDEPENDENT: return {N2 * N2};
+    case QCL_KERNEL_DENSE: return {nc * nc};
+    case QCL_KERNEL_IFR: return {N2 * J, J * N2, (size_t)Nk * Nk};
+    case QCL_KERNEL_LOW_RANK: return {nc * J, J * nc};
+    case QCL_KERNEL_SEPARABLE_SUM: return {(size_t)Nk * Nk * J, N2 * N2 * J};
+    default: return {};
+  }
+}
+
+// Contraction scratch elements of a mechanism at one precision.
+static size_t op_work_elems(const qcl_mechanism& q, int precision, int NE, int Nk, int N) {
+  KernelOpDev k;
+  k.kind = q.kind;
+  k.J = q.J;
+  static const void* dummy[1] = {nullptr};
+  if (precision != QCL_C128) {  // the tensor-core operands exist
+    if (q.kind == QCL_KERNEL_DENSE) k.tc_bop = dummy;
+    if (q.kind == QCL_KERNEL_SEPARABLE_SUM) k.tc_chunks = dummy;
+  }
+  return contraction_work_elems(k, NE, Nk, N);
+}
+
+static int plan_memory(const qcl_scba_problem* p, const qcl_mechanism* mechs, MemPlan* mp) {
+  *mp = MemPlan();
+  if (!p || p->NE < 2 || p->Nk < 1 || p->Nb < 1 || p->nmech < 0 || p->nmech > 5) {
+    set_last_error("memory estimate: invalid dimensions or mechanism count");
+    return QCL_DIM;
+  }
+  const int NE = p->NE, Nk = p->Nk, N = p->Nb, M = p->nmech;
+  const bool c128 = p->precision == QCL_C128;
+  const size_t esz = c128 ? 16 : 8, nfield = field_elems(NE, Nk, N);
+  const size_t fcap = nfield * (p->refinement ? 16 : esz);
+  mp->fields = (size_t)(6 * (M + 2) + 8) * fcap;  // state + candidate families, G x 3, totals x 3, candSL, tmp
+  size_t cwork = 0;
+  for (int i = 0; i < M; ++i) {
+    const qcl_mechanism& q = mechs[i];
+    for (size_t n : op_arrays(q, Nk, N)) {
+      mp->operators += n * esz;
+      if (!c128 && p->refinement) mp->operators += n * 16;  // kept complex128 copy
+      mp->transient = std::max(mp->transient, c128 ? (size_t)0 : n * 16);  // staging copy
+    }
+    const int N2 = N * N;
+    if (!c128 && q.kind == QCL_KERNEL_DENSE) mp->operators += tc_operator_bytes(Nk * N2, Nk * N2);
+    if (!c128 && q.kind == QCL_KERNEL_SEPARABLE_SUM)
+      for (int i0 = 0; i0 < q.J; i0 += kSepChunk) mp->operators += tc_operator_bytes(N2, std::min(kSepChunk, q.J - i0) * N2);
+    cwork = std::max(cwork, op_work_elems(q, p->precision, NE, Nk, N) * esz);
+    if (p->refinement && !c128) cwork = std::max(cwork, op_work_elems(q, QCL_C128, NE, Nk, N) * 16);
+  }
+  const int L = next_pow2(2 * NE - 1);
+  mp->workspace = cwork + 2 * (size_t)NE * Nk * 16 + (size_t)kReduceCtas * 2 * 8 +
+                  residual_mix_multi_partial_doubles(3 * (M + 2)) * 8 + residual_work_doubles(NE, Nk) * 8 +
+                  observables_partial_doubles(N) * 8 + 4096 /* scalars, status */ +
+                  (size_t)16 * 16 * L /* FFT tables */ + (size_t)Nk * N * N * 2 * 8 /* per-column partials */;
+  if (p->mixing)
+    mp->anderson = 2 * (size_t)p->anderson_history_depth * 3 * (M + 2) * fcap +
+                   anderson_partial_doubles(3 * (M + 2)) * 8 + sizeof(AndersonMeta);
+  return QCL_OK;
+}
+
+int scba_estimate_memory(const qcl_scba_problem* p, const qcl_mechanism* mechs, size_t out[6]) {
+  MemPlan mp;
+  int s = plan_memory(p, mechs, &mp);
+  if (s) return s;
+  out[0] = mp.fields;
+  out[1] = mp.operators;
+  out[2] = mp.workspace;
+  out[3] = mp.anderson;
+  out[4] = mp.resident();
+  out[5] = mp.peak();
+  return QCL_OK;
+}
+
 int scba_create(const qcl_scba_problem* p, const qcl_mechanism* mechs, ScbaCtx** out) {
   *out = nullptr;
   if (!p || p->NE < 2 || p->Nk < 1 || p->Nb < 1) {
@@ -266,7 +370,32 @@ int scba_create(const qcl_scba_problem* p, const qcl_mechanism* mechs, ScbaCtx**
     set_last_error("unknown precision %d", p->precision);
     return QCL_ARG;
   }
+  if (p->refinement && p->precision == QCL_C128) {
+    set_last_error("refinement applies to a reduced-precision context (QCL_C64 or QCL_MIXED)");
+    return QCL_ARG;
+  }
+  {
+    // preflight: refuse before the first allocation (build_production_cache,
+    // production_cache.jl:764-770)
+    MemPlan mp;
+    int s0 = plan_memory(p, mechs, &mp);
+    if (s0) return s0;
+    size_t budget = p->memory_budget_bytes;
+    if (budget == 0) {
+      size_t fr = 0, tot = 0;
+      cudaError_t e = cudaMemGetInfo(&fr, &tot);
+      if (e != cudaSuccess) return cuda_status(e, "cudaMemGetInfo");
+      budget = fr;
+    }
+    if (mp.peak() > budget) {
+      set_last_error("estimated peak device memory %zu bytes exceeds the execution budget %zu bytes (fields %zu, "
+                     "operators %zu, workspace %zu, Anderson history %zu, staging %zu)",
+                     mp.peak(), budget, mp.fields, mp.operators, mp.workspace, mp.anderson, mp.transient);
+      return QCL_NOMEM;
+    }
+  }
   ScbaCtx* c = new ScbaCtx();
+  c->refinement = p->refinement;
   c->NE = p->NE;
   c->Nk = p->Nk;
   c->N = p->Nb;
@@ -293,6 +422,7 @@ int scba_create(const qcl_scba_problem* p, const qcl_mechanism* mechs, ScbaCtx**
   c->and_reg = p->anderson_regularization;
   c->nfield = field_elems(c->NE, c->Nk, c->N);
   c->fbytes = c->nfield * (c->precision == QCL_C128 ? 16 : 8);
+  c->fcap = c->refinement ? c->nfield * 16 : c->fbytes;
   c->eps_h.assign(p->eps, p->eps + p->NE);
   c->wE_h.assign(p->wE, p->wE + p->NE);
   int s;
@@ -305,6 +435,7 @@ int scba_create(const qcl_scba_problem* p, const qcl_mechanism* mechs, ScbaCtx**
   } while (0)
   double de;
   TRY(check_uniform_grid(c->NE, p->eps, &de));
+  c->de = de;
   // _check_algorithm_options (algorithm_options.jl:42-93) for the model switches
   for (int sw : {c->diagonal, c->averaged, c->drop_real, c->direct_green, c->scalar_lesser})
     if (sw != 0 && sw != 1)
@@ -361,41 +492,60 @@ int scba_create(const qcl_scba_problem* p, const qcl_mechanism* mechs, ScbaCtx**
     c->mech.push_back(m);
     Mech& d = c->mech.back();
     if (q.kind == QCL_KERNEL_MOMENTUM_INDEPENDENT) {
-      TRY(upload_op(c, &d.block, q.block, (size_t)N2 * N2));
+      TRY(upload_op(c, &d.block, q.block, (size_t)N2 * N2, &d.block64));
     } else if (q.kind == QCL_KERNEL_DENSE) {
       const size_t nc = (size_t)c->Nk * N2;
-      TRY(upload_op(c, &d.matrix, q.matrix, nc * nc));
+      TRY(upload_op(c, &d.matrix, q.matrix, nc * nc, &d.matrix64));
       if (c->precision != QCL_C128)
         TRY(tc_build_operator((int)nc, c->Nk, d.matrix, c->wk, &d.tc_bop, c->st));
     } else if (q.kind == QCL_KERNEL_IFR) {
       if (q.J < 1) TRY((set_last_error("IFR operator needs J >= 1"), QCL_ARG));
-      TRY(upload_op(c, &d.left, q.left, (size_t)N2 * q.J));
-      TRY(upload_op(c, &d.right, q.right, (size_t)q.J * N2));
-      TRY(upload_op(c, &d.radial, q.radial, (size_t)c->Nk * c->Nk));
+      TRY(upload_op(c, &d.left, q.left, (size_t)N2 * q.J, &d.left64));
+      TRY(upload_op(c, &d.right, q.right, (size_t)q.J * N2, &d.right64));
+      TRY(upload_op(c, &d.radial, q.radial, (size_t)c->Nk * c->Nk, &d.radial64));
     } else if (q.kind == QCL_KERNEL_LOW_RANK) {
       if (q.J < 1) TRY((set_last_error("low-rank operator needs rank J >= 1"), QCL_ARG));
       const size_t nc = (size_t)c->Nk * N2;
-      TRY(upload_op(c, &d.left, q.left, nc * q.J));
-      TRY(upload_op(c, &d.right, q.right, (size_t)q.J * nc));
+      TRY(upload_op(c, &d.left, q.left, nc * q.J, &d.left64));
+      TRY(upload_op(c, &d.right, q.right, (size_t)q.J * nc, &d.right64));
+    } else if (q.kind == QCL_KERNEL_SEPARABLE_SUM) {
+      if (q.J < 1) TRY((set_last_error("separable-sum operator needs J >= 1 terms"), QCL_ARG));
+      TRY(upload_op(c, &d.radial, q.radial, (size_t)c->Nk * c->Nk * q.J, &d.radial64));
+      TRY(upload_op(c, &d.block, q.block, (size_t)N2 * N2 * q.J, &d.block64));
+      if (c->precision != QCL_C128)
+        for (int i0 = 0; i0 < q.J; i0 += kSepChunk) {
+          const int jc = std::min(kSepChunk, q.J - i0);
+          void* b = nullptr;
+          s = tc_build_operator2(N2, jc * N2, 1, (const Cx<float>*)d.block + (size_t)N2 * N2 * i0, nullptr, &b, c->st);
+          if (b) d.tc_chunks.push_back(b);
+          TRY(s);
+        }
     } else {
       TRY((set_last_error("unknown kernel kind %d", q.kind), QCL_ARG));
     }
-    cwork = std::max(cwork, contraction_work_elems(d.view(), c->NE, c->Nk, c->N));
+    cwork = std::max(cwork, contraction_work_elems(d.view(), c->NE, c->Nk, c->N) * (c->precision == QCL_C128 ? 16 : 8));
+    if (c->refinement) {  // the complex128 contraction after promote
+      KernelOpDev k64;
+      k64.kind = d.kind;
+      k64.J = d.J;
+      cwork = std::max(cwork, contraction_work_elems(k64, c->NE, c->Nk, c->N) * 16);
+    }
   }
   const int F = c->M + 2;
   c->state.assign(3 * F, nullptr);
   c->cand.assign(3 * F, nullptr);
   for (int i = 0; i < 3 * F; ++i) {
-    TRY(dalloc(&c->state[i], c->fbytes));
-    TRY(dalloc(&c->cand[i], c->fbytes));
+    TRY(dalloc(&c->state[i], c->fcap));
+    TRY(dalloc(&c->cand[i], c->fcap));
   }
-  TRY(dalloc(&c->GR, c->fbytes));
-  TRY(dalloc(&c->GL, c->fbytes));
-  TRY(dalloc(&c->GG, c->fbytes));
-  for (auto& t : c->tot) TRY(dalloc(&t, c->fbytes));
-  TRY(dalloc(&c->candSL, c->fbytes));
-  TRY(dalloc(&c->tmp, c->fbytes));
-  TRY(dalloc(&c->cwork, cwork * (c->precision == QCL_C128 ? 16 : 8)));
+  TRY(dalloc(&c->GR, c->fcap));
+  TRY(dalloc(&c->GL, c->fcap));
+  TRY(dalloc(&c->GG, c->fcap));
+  for (auto& t : c->tot) TRY(dalloc(&t, c->fcap));
+  TRY(dalloc(&c->candSL, c->fcap));
+  TRY(dalloc(&c->tmp, c->fcap));
+  TRY(dalloc(&c->cwork, cwork));
+  c->cwork_bytes = cwork;
   TRY(dalloc((void**)&c->trL, (size_t)c->NE * c->Nk * 16));
   TRY(dalloc((void**)&c->trG, (size_t)c->NE * c->Nk * 16));
   TRY(dalloc((void**)&c->rpartial, kReduceCtas * 2 * sizeof(double)));
@@ -413,8 +563,8 @@ int scba_create(const qcl_scba_problem* p, const qcl_mechanism* mechs, ScbaCtx**
   QCL_CUDA_CHECK(cudaMemsetAsync(c->scal, 0, SC_TOTAL * sizeof(double), c->st));
   if (c->mixing) {
     const size_t nf = 3 * (size_t)(c->M + 2);
-    TRY(dalloc(&c->Xh, (size_t)c->and_depth * nf * c->fbytes));
-    TRY(dalloc(&c->Rh, (size_t)c->and_depth * nf * c->fbytes));
+    TRY(dalloc(&c->Xh, (size_t)c->and_depth * nf * c->fcap));
+    TRY(dalloc(&c->Rh, (size_t)c->and_depth * nf * c->fcap));
     TRY(dalloc((void**)&c->ameta, sizeof(AndersonMeta)));
     TRY(dalloc((void**)&c->apartial, anderson_partial_doubles((int)nf) * sizeof(double)));
     cudaError_t e = cudaMallocHost((void**)&c->ameta_h, sizeof(AndersonMeta));
@@ -1018,6 +1168,66 @@ int scba_set_graph(ScbaCtx* c, int enable) {
   c->use_graph = enable != 0;
   return QCL_OK;
 }
+
+// Switches a refinement context (QCL_MIXED or QCL_C64 storage) to complex128
+// for the iterations that follow: the FP64 refinement of a reduced-precision
+// fixed point.  The current state families (with the last step's mixing
+// committed) are converted exactly to complex128, the operators switch to the
+// complex128 copies kept at creation, the FFT tables are rebuilt and the
+// captured graphs and the Anderson history are dropped.  The next step
+// continues from the same state; the row history (r_J, r_pop) continues.
+int scba_promote(ScbaCtx* c) {
+  if (!c->refinement) {
+    set_last_error("promote: the context was not created with refinement enabled");
+    return QCL_ARG;
+  }
+  if (c->precision == QCL_C128) return QCL_OK;
+  QCL_CUDA_CHECK(cudaStreamSynchronize(c->st));
+  if (c->pending_commit) {
+    c->parity ^= 1;
+    c->pending_commit = false;
+  }
+  int s;
+  std::vector<void*>& st = c->parity == 0 ? c->state : c->cand;
+  for (void*& f : st) {  // state field -> tmp (complex128), then swap the buffers
+    if ((s = launch_promote(c->nfield, f, c->tmp, c->st))) return s;
+    std::swap(f, c->tmp);
+  }
+  for (auto& m : c->mech) {
+    auto swap_in = [](void*& cur, void*& keep) {
+      if (keep) {
+        cudaFree(cur);
+        cur = keep;
+        keep = nullptr;
+      }
+    };
+    swap_in(m.block, m.block64);
+    swap_in(m.matrix, m.matrix64);
+    swap_in(m.left, m.left64);
+    swap_in(m.right, m.right64);
+    swap_in(m.radial, m.radial64);
+    cudaFree(m.tc_bop);
+    m.tc_bop = nullptr;
+    for (void* q : m.tc_chunks) cudaFree(q);
+    m.tc_chunks.clear();
+  }
+  c->precision = QCL_C128;
+  c->fbytes = c->nfield * 16;
+  if ((s = prepare_hilbert_tables(c->hil, c->NE, c->de, QCL_C128))) return s;
+  if ((s = ensure_partial(c->hil, (long long)c->Nk * c->N * c->N))) return s;
+  for (int g = 0; g < 2; ++g)
+    if (c->graph[g]) {
+      cudaGraphExecDestroy(c->graph[g]);
+      c->graph[g] = nullptr;
+    }
+  if (c->mixing && (s = launch_anderson_reset(c->ameta, c->st))) return s;
+  c->have_green = false;
+  c->have_residual = false;
+  QCL_CUDA_CHECK(cudaStreamSynchronize(c->st));
+  return QCL_OK;
+}
+
+int scba_precision(ScbaCtx* c) { return c->precision; }
 
 cudaStream_t scba_stream(ScbaCtx* c) { return c->st; }
 

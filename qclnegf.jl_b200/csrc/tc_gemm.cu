@@ -416,14 +416,15 @@ __global__ void tc_split_a_kernel(int NE, int Nc, int Mpad, int Kpad, const Cx<f
 }
 
 // max |B| into *mxbits (non-negative FP32 bits order as unsigned integers;
-// a non-finite entry gives +inf).
-__global__ void tc_b_maxabs_kernel(int Nc, int Nk, const Cx<float>* __restrict__ Mop,
+// a non-finite entry gives +inf).  Mop is column-major Nout x Kc; column k
+// carries the weight wk[k % Nk] (no weight if wk is NULL).
+__global__ void tc_b_maxabs_kernel(int Nout, int Kc, int Nk, const Cx<float>* __restrict__ Mop,
                                    const double* __restrict__ wk, unsigned* __restrict__ mxbits) {
-  const long long n = (long long)Nc * Nc;
+  const long long n = (long long)Nout * Kc;
   float mx = 0.0f;
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
     const Cx<float> m = Mop[i];
-    const float w = fabsf((float)wk[(i / Nc) % Nk]);
+    const float w = wk ? fabsf((float)wk[(i / Nout) % Nk]) : 1.0f;
     const float a = fmaxf(fabsf(m.x), fabsf(m.y)) * w;
     mx = isfinite(a) ? fmaxf(mx, a) : INFINITY;
   }
@@ -431,13 +432,13 @@ __global__ void tc_b_maxabs_kernel(int Nc, int Nk, const Cx<float>* __restrict__
   for (int o = 16; o > 0; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
   if ((threadIdx.x & 31) == 0) atomicMax(mxbits, __float_as_uint(mx));
 }
-// B[2j + c'][2k + c] from the complex operator M (column-major Nc x Nc,
-// complex64) and the momentum weights wk[k % Nk]:
+// B[2j + c'][2k + c] from the complex operator M (column-major Nout x Kc,
+// complex64) and the momentum weights wk[k % Nk] (1 if wk is NULL):
 //   s_B [[Re, -Im], [Im, Re]] * w  (rows c' = 0 real part of the output, 1 imaginary),
 // as fp16 hi / lo.  One CTA per 32 (j) x 16 (k) tile of M: M is read
 // coalesced along j into shared memory, B written coalesced along its K axis
-// (each M entry feeds a 2 x 2 block of B; the padding past Nc is zero).
-__global__ void tc_build_b_kernel(int Nc, int Nk, int Kpad, const Cx<float>* __restrict__ Mop,
+// (each M entry feeds a 2 x 2 block of B; the padding past Nout / Kc is zero).
+__global__ void tc_build_b_kernel(int Nout, int Kc, int Nk, int Kpad, const Cx<float>* __restrict__ Mop,
                                   const double* __restrict__ wk, const unsigned* __restrict__ mxbits,
                                   __half* __restrict__ Bhi, __half* __restrict__ Blo, float* __restrict__ binv) {
   __shared__ Cx<float> tile[16][33];  // [k][j]
@@ -447,12 +448,12 @@ __global__ void tc_build_b_kernel(int Nc, int Nk, int Kpad, const Cx<float>* __r
   const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;  // 32 x 8 threads
   for (int r = ty; r < 16; r += 8) {
     const int j = j0 + tx, k = k0 + r;
-    tile[r][tx] = (j < Nc && k < Nc) ? Mop[(size_t)j + (size_t)Nc * k] : cx<float>(0, 0);
+    tile[r][tx] = (j < Nout && k < Kc) ? Mop[(size_t)j + (size_t)Nout * k] : cx<float>(0, 0);
   }
   __syncthreads();
   // 64 rows x 32 columns of B: thread column kk = 2 k0 + tx, rows in steps of 8
   const int kk = 2 * k0 + tx, kl = tx >> 1, c = tx & 1, k = k0 + kl;
-  const float w = k < Nc ? (float)wk[k % Nk] : 0.0f;
+  const float w = k < Kc ? (wk ? (float)wk[k % Nk] : 1.0f) : 0.0f;
   for (int rr = ty; rr < 64; rr += 8) {
     const int nn = 2 * j0 + rr, jl = rr >> 1, cp = rr & 1;
     const Cx<float> m = tile[kl][jl];
@@ -462,26 +463,34 @@ __global__ void tc_build_b_kernel(int Nc, int Nk, int Kpad, const Cx<float>* __r
   }
 }
 
+// Padded extents of a C[M x Nout] = A[M x Kc] B^T product (complex counts;
+// real extents twice that), in whole tiles.
+static void tc_dims2(int M, int Nout, int Kc, int* Mpad, int* Npad, int* Kpad) {
+  *Mpad = (M + TC_BM - 1) / TC_BM * TC_BM;
+  *Npad = (2 * Nout + TC_BN - 1) / TC_BN * TC_BN;
+  *Kpad = (2 * Kc + TC_BK - 1) / TC_BK * TC_BK;
+}
 int tc_dims(int NE, int Nc, int* Mpad, int* Npad, int* Kpad) {
-  *Mpad = (NE + TC_BM - 1) / TC_BM * TC_BM;
-  *Npad = (2 * Nc + TC_BN - 1) / TC_BN * TC_BN;
-  *Kpad = (2 * Nc + TC_BK - 1) / TC_BK * TC_BK;
+  tc_dims2(NE, Nc, Nc, Mpad, Npad, Kpad);
   return QCL_OK;
 }
 
 // A work area, in floats: fp16 hi and lo (Mpad x Kpad each), then the row
 // maxima (FP32 bits) and the inverse row scales (Mpad each).
-size_t tc_a_work_floats(int NE, int Nc) {
+size_t tc_a_work_floats2(int M, int Kc) {
   int Mpad, Npad, Kpad;
-  tc_dims(NE, Nc, &Mpad, &Npad, &Kpad);
+  tc_dims2(M, 1, Kc, &Mpad, &Npad, &Kpad);
   return (size_t)Mpad * Kpad + 2 * (size_t)Mpad;
 }
+size_t tc_a_work_floats(int NE, int Nc) { return tc_a_work_floats2(NE, Nc); }
 
 // Prepared operator: one allocation holding 1 / s_B (256 bytes reserved), the
 // max-|B| word, then B_hi and B_lo (Npad x Kpad fp16 each).  *Bop receives it.
-int tc_build_operator(int Nc, int Nk, const void* Mop_c64, const double* wk, void** Bop, cudaStream_t st) {
+// Mop is column-major Nout x Kc (complex64); wk (may be NULL) weights column
+// k by wk[k % Nk].
+int tc_build_operator2(int Nout, int Kc, int Nk, const void* Mop_c64, const double* wk, void** Bop, cudaStream_t st) {
   int Mpad, Npad, Kpad;
-  tc_dims(1, Nc, &Mpad, &Npad, &Kpad);
+  tc_dims2(1, Nout, Kc, &Mpad, &Npad, &Kpad);
   const size_t n = (size_t)Npad * Kpad;
   QCL_CUDA_CHECK(cudaMalloc(Bop, 256 + 2 * n * sizeof(__half)));
   char* b = (char*)*Bop;
@@ -489,12 +498,21 @@ int tc_build_operator(int Nc, int Nk, const void* Mop_c64, const double* wk, voi
   unsigned* mxbits = (unsigned*)(b + 16);
   __half* Bhi = (__half*)(b + 256);
   QCL_CUDA_CHECK(cudaMemsetAsync(mxbits, 0, sizeof(unsigned), st));
-  tc_b_maxabs_kernel<<<148 * 4, 256, 0, st>>>(Nc, Nk, (const Cx<float>*)Mop_c64, wk, mxbits);
+  tc_b_maxabs_kernel<<<148 * 4, 256, 0, st>>>(Nout, Kc, Nk, (const Cx<float>*)Mop_c64, wk, mxbits);
   QCL_LAUNCH_CHECK("tc_b_maxabs_kernel");
-  tc_build_b_kernel<<<dim3(Npad / 64, Kpad / 32), 256, 0, st>>>(Nc, Nk, Kpad, (const Cx<float>*)Mop_c64, wk, mxbits,
-                                                                 Bhi, Bhi + n, binv);
+  tc_build_b_kernel<<<dim3(Npad / 64, Kpad / 32), 256, 0, st>>>(Nout, Kc, Nk, Kpad, (const Cx<float>*)Mop_c64, wk,
+                                                                 mxbits, Bhi, Bhi + n, binv);
   QCL_LAUNCH_CHECK("tc_build_b_kernel");
   return QCL_OK;
+}
+// Bytes of a prepared operand (tc_build_operator2).
+size_t tc_operator_bytes(int Nout, int Kc) {
+  int Mpad, Npad, Kpad;
+  tc_dims2(1, Nout, Kc, &Mpad, &Npad, &Kpad);
+  return 256 + 2 * (size_t)Npad * Kpad * sizeof(__half);
+}
+int tc_build_operator(int Nc, int Nk, const void* Mop_c64, const double* wk, void** Bop, cudaStream_t st) {
+  return tc_build_operator2(Nc, Nc, Nk, Mop_c64, wk, Bop, st);
 }
 
 typedef CUresult (*TensorMapEncodeTiled)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
@@ -570,25 +588,28 @@ template <int BN> static int launch_tc_t(const TcMaps& maps, const TcArgs& a, in
   return QCL_OK;
 }
 
-int launch_tc_dense_contraction(int NE, int Nc, const void* Bop, const void* G, void* S, double alpha, double beta,
-                                float* awork, int* status, cudaStream_t st) {
+// C = A B^T on the tensor cores for complex64 operands:
+//   S[e + M j] = alpha sum_k A[e + M k] Bop[j, k] + beta S[e + M j],
+// e < M, j < Nout, k < Kc; Bop prepared by tc_build_operator2(Nout, Kc, ...).
+int launch_tc_contraction2(int M, int Nout, int Kc, const void* Bop, const void* A, void* S, double alpha,
+                           double beta, float* awork, int* status, cudaStream_t st) {
   int Mpad, Npad, Kpad;
-  tc_dims(NE, Nc, &Mpad, &Npad, &Kpad);
+  tc_dims2(M, Nout, Kc, &Mpad, &Npad, &Kpad);
   __half* Ahi = (__half*)awork;
   __half* Alo = Ahi + (size_t)Mpad * Kpad;
   unsigned* rowmax = (unsigned*)(Alo + (size_t)Mpad * Kpad);
   float* ainv = (float*)(rowmax + Mpad);
   QCL_CUDA_CHECK(cudaMemsetAsync(rowmax, 0, (size_t)Mpad * sizeof(unsigned), st));
-  tc_row_max_kernel<<<dim3(Mpad / 32, (Nc + 255) / 256), 256, 0, st>>>(NE, Nc, (const Cx<float>*)G, rowmax);
+  tc_row_max_kernel<<<dim3(Mpad / 32, (Kc + 255) / 256), 256, 0, st>>>(M, Kc, (const Cx<float>*)A, rowmax);
   QCL_LAUNCH_CHECK("tc_row_max_kernel");
   dim3 sg((Mpad + 31) / 32, (Kpad + 31) / 32);
-  tc_split_a_kernel<<<sg, 256, 0, st>>>(NE, Nc, Mpad, Kpad, (const Cx<float>*)G, rowmax, Ahi, Alo, ainv);
+  tc_split_a_kernel<<<sg, 256, 0, st>>>(M, Kc, Mpad, Kpad, (const Cx<float>*)A, rowmax, Ahi, Alo, ainv);
   QCL_LAUNCH_CHECK("tc_split_a_kernel");
   const char* b = (const char*)Bop;
   const __half* Bhi = (const __half*)(b + 256);
   const __half* Blo = Bhi + (size_t)Npad * Kpad;
   const int mtiles = Mpad / TC_BM;
-  const int bn = tc_pick_bn(mtiles, 2 * Nc);
+  const int bn = tc_pick_bn(mtiles, 2 * Nout);
   TcMaps maps;
   int s;
   if ((s = make_operand_map(&maps.ahi, Ahi, Mpad, Kpad, TC_BM))) return s;
@@ -596,9 +617,14 @@ int launch_tc_dense_contraction(int NE, int Nc, const void* Bop, const void* G, 
   // B rows past Npad (the last tile of a narrower width) read the zero fill
   if ((s = make_operand_map(&maps.bhi, Bhi, Npad, Kpad, bn))) return s;
   if ((s = make_operand_map(&maps.blo, Blo, Npad, Kpad, bn))) return s;
-  TcArgs a{NE, 2 * Nc, Kpad, (Cx<float>*)S, NE, alpha, beta, ainv, (const float*)b, status};
+  TcArgs a{M, 2 * Nout, Kpad, (Cx<float>*)S, M, alpha, beta, ainv, (const float*)b, status};
   if (bn == 224) return launch_tc_t<224>(maps, a, mtiles, st);
   return launch_tc_t<256>(maps, a, mtiles, st);
+}
+
+int launch_tc_dense_contraction(int NE, int Nc, const void* Bop, const void* G, void* S, double alpha, double beta,
+                                float* awork, int* status, cudaStream_t st) {
+  return launch_tc_contraction2(NE, Nc, Nc, Bop, G, S, alpha, beta, awork, status, st);
 }
 
 }  // namespace qcl

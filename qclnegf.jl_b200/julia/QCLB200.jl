@@ -157,6 +157,12 @@ struct Problem
     occupation_normalization::Cint  # :paired_convex / :scalar_lesser
     mixing::Cint                    # :linear / :anderson
     anderson_history_depth::Cint; anderson_damping::Float64; anderson_regularization::Float64
+    memory_budget_bytes::Csize_t    # preflight budget (ProductionOptions.memory_budget_bytes); 0 = free memory
+    refinement::Cint                # 1: a mixed context that can finish in FP64 (promote!)
+end
+
+struct MemoryEstimate
+    fields::Csize_t; operators::Csize_t; workspace::Csize_t; anderson::Csize_t; resident::Csize_t; peak::Csize_t
 end
 
 struct Row
@@ -181,6 +187,17 @@ function create(problem::Problem, mechanisms::Vector{Mechanism}, keep::Vector{An
     finalizer(x -> ccall((:qcl_scba_destroy, libqcl), Cvoid, (Ptr{Cvoid},), x.handle), s)
     return s
 end
+
+# _estimate_production_memory / build_production_cache's refusal (production_cache.jl:475-668, 764-770)
+function estimate_memory(problem::Problem, mechanisms::Vector{Mechanism})
+    out = Ref{MemoryEstimate}()
+    check(ccall((:qcl_scba_estimate_memory, libqcl), Cint, (Ref{Problem}, Ptr{Mechanism}, Ref{MemoryEstimate}),
+                problem, mechanisms, out))
+    return out[]
+end
+
+# FP64 refinement of a mixed-precision state (a context created with refinement = 1)
+promote!(s::Solver) = check(ccall((:qcl_scba_promote, libqcl), Cint, (Ptr{Cvoid},), s.handle))
 
 seed!(s::Solver) = (μ = Ref(0.0); check(ccall((:qcl_scba_seed, libqcl), Cint, (Ptr{Cvoid}, Ref{Float64}), s.handle, μ)); μ[])
 

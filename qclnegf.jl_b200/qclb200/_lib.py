@@ -71,6 +71,12 @@ class CudaError(QCLError):
     pass
 
 
+class MemoryBudgetError(ArgumentError):
+    """QCL_NOMEM: the memory preflight refused the context (the ArgumentError
+    of build_production_cache, numerics/optimized/production_cache.jl:
+    764-770) or a device allocation failed."""
+
+
 _EXC = {
     QCL_SINGULAR: SingularException,
     QCL_DOMAIN: DomainError,
@@ -79,7 +85,7 @@ _EXC = {
     QCL_NONFINITE: NonFiniteMetrics,
     QCL_UNSUPPORTED: UnsupportedError,
     QCL_CUDA: CudaError,
-    QCL_NOMEM: CudaError,
+    QCL_NOMEM: MemoryBudgetError,
     QCL_TIMEOUT: QCLError,
 }
 
@@ -145,6 +151,8 @@ def _declare(l):
         "qcl_scba_green_state": (I, [P, P, P, P]),
         "qcl_scba_witness": (I, [P, P]),
         "qcl_scba_retarget": (I, [P, D, D, D, P, P]),
+        "qcl_scba_estimate_memory": (I, [P, P, P]),
+        "qcl_scba_promote": (I, [P]),
         "qcl_scba_mixer_info": (I, [P, P]),
         "qcl_anderson_guard": (I, [I, I, I, I, I, P, P, P]),
         "qcl_scba_density_matrix": (I, [P, P]),

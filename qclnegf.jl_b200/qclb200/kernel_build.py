@@ -173,3 +173,118 @@ def table_kernel_operator(name: str, nodes, covariances, kappa, Nphi: int) -> Me
     X = np.transpose(C, (1, 2, 0))  # [(a,c), (b,d), t] column-major
     W = lookup_weights(nodes, kappa, Nphi)
     return assemble_operator(name, TABLE, len(kappa), Nb, W, X)
+
+
+def impurity_pair_factors(q, chi, x, wx, donor_weights, q_s, prefactor_scale: float):
+    """The factors of the screened ionised-donor covariance at one transfer
+    momentum q: C(q) = V diag(w_D) V^H with V[(a,c), D] as in
+    impurity_pair_covariance (_production_impurity_evaluator,
+    numerics/optimized/kernels.jl:122-158).  Returns (V, w_D) over the doped
+    cells only."""
+    chi = np.asarray(chi, dtype=np.complex128)
+    Nb = chi.shape[1]
+    donors = np.nonzero(np.asarray(donor_weights))[0]
+    if len(donors) == 0:
+        raise ValueError("impurity kernel has no ionized donors")
+    pair = (np.asarray(wx)[:, None, None] * np.conj(chi)[:, :, None] * chi[:, None, :]).reshape(
+        (len(x), Nb * Nb), order="F")  # [g, a + Nb c]
+    dist = np.abs(np.asarray(x)[:, None] - np.asarray(x)[donors][None, :])
+    V = prefactor_scale / (q + q_s) * (pair.T @ np.exp(-q * dist))
+    return V, np.asarray(donor_weights, dtype=np.float64)[donors]
+
+
+def separable_sum_operator(name: str, W, V, d=None, rtol: float = 1e-15, max_terms: int = 0) -> Mechanism:
+    """Kronecker-sum form K(m, m') = q sum_i radial_i(m, m') block_i of a
+    kernel given by angular node weights and node tensors,
+
+        K[m, m', a, c, d, b] = sum_t W[(m, m'), t] X_t[(a, c), (b, d)],
+        X_t = V_t diag(d) V_t^H                       (pair layout),
+
+    which covers both of the reference's momentum-dependent kernels: the
+    exact LO kernel (lo_phonon_kernel, numerics/reference/kernels.jl:321-356:
+    X_h = F_h (x) conj F_h, V_h = vec F_h, d = 1, W = lo_weights) and the
+    tabulated kernels (_assemble_lookup_kernel, numerics/optimized/
+    kernels.jl:303-320: X_t = C(q_t), W = lookup_weights; the impurity
+    covariance C = V diag(w_D) V^H, impurity_pair_factors).
+
+    W: (N_k^2, T) (row m + N_k m'); V: (T, N_b^2, D) with pair index
+    a + N_b c; d: (D,) non-negative (default ones).
+
+    The compression is exact up to the singular values it drops, which are
+    all below `rtol` of the largest (in the norm of the N_k^2 x N_b^4
+    unfolding of K):
+      1. Q = orthonormal basis of the columns sqrt(d_j) V_t[:, j] (SVD);
+         then X_t = Q Y_t Q^H with Y_t (k x k) -- no N_b^4-sized array;
+      2. QR of the k^2 x T matrix of the vec(Y_t)^H: W Y = (W R^H) Q_Y^H;
+      3. SVD of W R^H (N_k^2 x T) gives the terms.
+    The smooth transfer-momentum dependence of these kernels makes J small
+    (about 20-30 terms at rtol 1e-15 for the LO and impurity kernels of a
+    32-state basis on a 64-point momentum grid) where the dense operator has
+    (N_k N_b^2)^2 entries.  q is max_(m,m') sum_i |radial_i(m,m')| max|block_i|
+    (an upper bound of max|K|; only the product q K enters the map).
+    `max_terms` (0 = none) caps J; ValueError if the cap drops a term above
+    rtol."""
+    W = np.asarray(W)
+    V = np.asarray(V, dtype=np.complex128)
+    if V.ndim == 2:
+        V = V[:, :, None]
+    T, N2, D = V.shape
+    n1 = W.shape[0]
+    Nk, Nb = int(round(math.sqrt(n1))), int(round(math.sqrt(N2)))
+    if Nk * Nk != n1 or Nb * Nb != N2 or W.shape[1] != T:
+        raise ValueError("W must be (N_k^2, T) and V (T, N_b^2, D)")
+    d = np.ones(D) if d is None else np.asarray(d, dtype=np.float64)
+    if d.shape != (D,) or np.any(d < 0) or not np.all(np.isfinite(d)):
+        raise ValueError("node weights d must be D finite non-negative numbers")
+    A = (V * np.sqrt(d)[None, None, :]).transpose(1, 0, 2).reshape(N2, T * D)  # columns sqrt(d_j) V_t[:, j]
+    U, sA, _ = np.linalg.svd(A, full_matrices=False)
+    if not (sA.size and sA[0] > 0 and np.isfinite(sA[0])):
+        raise ValueError(f"kernel {name} is zero or non-finite")
+    k = int(np.count_nonzero(sA > sA[0] * 1e-17))
+    Q = U[:, :k]
+    Bt = np.ascontiguousarray((Q.conj().T @ A).reshape(k, T, D).transpose(1, 0, 2))  # (T, k, D): Q^H sqrt(d) V_t
+    Y = Bt @ np.conj(np.transpose(Bt, (0, 2, 1)))  # Y_t = B_t B_t^H, (T, k, k)
+    del Bt
+    Yflat = np.transpose(Y, (0, 2, 1)).reshape(T, k * k)  # column-major vec of each Y_t
+    del Y
+    QY, RY = np.linalg.qr(np.conj(Yflat.T))  # Yflat = RY^H QY^H, QY orthonormal columns (k^2 x T)
+    del Yflat
+    P, Sig, Zh = np.linalg.svd(W @ np.conj(RY.T), full_matrices=False)  # K-unfolding = P Sig (Zh QY^H)
+    if not (Sig.size and Sig[0] > 0 and np.isfinite(Sig[0])):
+        raise ValueError(f"kernel {name} is zero or non-finite")
+    R = int(np.count_nonzero(Sig > Sig[0] * rtol))
+    if max_terms and R > max_terms:
+        raise ValueError(f"{name}: {R} terms exceed max_terms={max_terms} at rtol={rtol}")
+    rho = Zh[:R] @ np.conj(QY.T)  # (R, k^2): vec Y^(i)
+    del QY
+    radial = np.empty((Nk, Nk, R), dtype=np.complex128, order="F")
+    block = np.empty((N2, N2, R), dtype=np.complex128, order="F")
+    for i in range(R):
+        Yi = rho[i].reshape((k, k), order="F")
+        Pi = (Q @ Yi @ Q.conj().T).reshape((Nb, Nb, Nb, Nb), order="F")  # [a, c, b, d]
+        blk = np.transpose(Pi, (0, 2, 1, 3)).reshape((N2, N2), order="F")  # rows a + Nb b, cols c + Nb d
+        mx = float(np.max(np.abs(blk)))
+        block[:, :, i] = blk / mx
+        radial[:, :, i] = (P[:, i] * (Sig[i] * mx)).reshape((Nk, Nk), order="F")
+    q = float(np.max(np.sum(np.abs(radial), axis=2)))
+    if not (q > 0 and math.isfinite(q)):
+        raise ValueError(f"kernel {name} has scale {q}: zero or non-finite")
+    mech = Mechanism(name, "separable_sum", q, block=block, radial=np.asfortranarray(radial / q))
+    mech.residual = float(Sig[R] / Sig[0]) if R < len(Sig) else 0.0
+    return mech
+
+
+def exact_node_kernel(W, V, d=None) -> np.ndarray:
+    """The literal six-index K[m, m', a, c, d, b] = sum_t W[(m, m'), t]
+    (V_t diag(d) V_t^H)[(a, c), (b, d)] on the host (small sizes; tests)."""
+    W = np.asarray(W)
+    V = np.asarray(V, dtype=np.complex128)
+    if V.ndim == 2:
+        V = V[:, :, None]
+    T, N2, D = V.shape
+    Nk, Nb = int(round(math.sqrt(W.shape[0]))), int(round(math.sqrt(N2)))
+    d = np.ones(D) if d is None else np.asarray(d, dtype=np.float64)
+    X = np.einsum("tpj,j,tqj->tpq", V, d, V.conj())  # [t, (a,c), (b,d)]
+    K = np.tensordot(W, X, axes=(1, 0))  # [(m,m'), (a,c), (b,d)]
+    K = K.reshape((Nk, Nk, Nb, Nb, Nb, Nb), order="F")  # [m, m', a, c, b, d]
+    return np.asfortranarray(np.transpose(K, (0, 1, 2, 3, 5, 4)))

@@ -170,7 +170,7 @@ class _Mechanism(ctypes.Structure):
                 ("right", ctypes.c_void_p), ("radial", ctypes.c_void_p)]
 
 
-_KIND = {"momentum_independent": 0, "dense": 1, "ifr": 2, "low_rank": 3}
+_KIND = {"momentum_independent": 0, "dense": 1, "ifr": 2, "low_rank": 3, "separable_sum": 4}
 
 
 def mechanism_struct(mech):
@@ -188,8 +188,11 @@ def mechanism_struct(mech):
         keep.append(a)
         return ctypes.c_void_p(a.ctypes.data)
 
-    s = _Mechanism(_KIND[mech.kind], 1 if mech.name == "LO" else 0,
-                   0 if mech.left is None else int(np.shape(mech.left)[1]), float(mech.q),
+    if mech.kind == "separable_sum":
+        J = int(np.shape(mech.radial)[2])
+    else:
+        J = 0 if mech.left is None else int(np.shape(mech.left)[1])
+    s = _Mechanism(_KIND[mech.kind], 1 if mech.name == "LO" else 0, J, float(mech.q),
                    arr(mech.block), arr(mech.matrix), arr(mech.left), arr(mech.right), arr(mech.radial))
     s._keep = keep
     return s

@@ -60,7 +60,11 @@ class Mechanism:
       * ``"ifr"`` -- ``left (Nb^2,J)``, ``right (J,Nb^2)``, ``radial (Nk,Nk)``
         (``production_cache.jl:414-448``);
       * ``"low_rank"`` -- ``left (Nk Nb^2, r)`` (U S), ``right (r, Nk Nb^2)``
-        (V^H) of the dense matrix (``production_cache.jl:348-385``).
+        (V^H) of the dense matrix (``production_cache.jl:348-385``);
+      * ``"separable_sum"`` -- ``radial (Nk, Nk, J)`` and ``block (Nb^2, Nb^2,
+        J)`` (rows ``(a,b)``, columns ``(c,d)``): ``K(m,m') = sum_i
+        radial_i(m,m') block_i``, the Kronecker-sum form of the momentum
+        dependent kernels (``kernel_build.separable_sum_operator``).
     ``q`` is the kernel scale ``q^K`` (``kernels.jl:388-405``).
     """
 
@@ -91,6 +95,10 @@ class Mechanism:
         elif self.kind == "low_rank":
             M = (self.left @ self.right).reshape((Nk, Nb, Nb, Nk, Nb, Nb), order="F")
             K[...] = np.transpose(M, (0, 3, 1, 4, 5, 2))
+        elif self.kind == "separable_sum":
+            J = self.radial.shape[2]
+            blk = np.asarray(self.block).reshape((Nb, Nb, Nb, Nb, J), order="F")  # [a,b,c,d,i]
+            K[...] = np.einsum("mni,abcdi->mnacdb", np.asarray(self.radial), blk)
         elif self.kind == "ifr":
             J = self.left.shape[1]
             L = self.left.reshape((Nb, Nb, J), order="F")  # [a,b,j]
@@ -418,3 +426,136 @@ def operator_batch_hamiltonian(N: int, Nk: int, seed: int = 7):
         h[m] = h0 + Cbar * kappa[m] ** 2 * np.eye(N)
     eps, wE = energy_grid(-0.05 / E0_EV, 0.35 / E0_EV, 4096)
     return h, wk, kappa
+
+
+# GaAs / Al0.15Ga0.85As constants used by the full-physics synthetic structure
+# (presets.jl:45-47, 76-78; SI).
+_EPS0 = 8.8541878128e-12
+_KB_J = 1.380649e-23
+_GAAS_EPS_INF, _GAAS_EPS_S = 10.89, 12.9
+_GAAS_RHO, _GAAS_VS, _GAAS_XI_EV = 5317.0, 5220.0, 7.0
+
+
+def _period_basis(rng, periods, states, layers_nm, dz_nm=0.5):
+    """Real, normalised, localised basis functions chi[g, a] (a = period *
+    states + s) on a cell-centred grid over `periods` periods of the layer
+    stack, in solver units (x / L0, sum_g wx chi^2 = 1); also the interface
+    coordinates (layer edges, the period seam included once per period)."""
+    Lp = sum(layers_nm) / L0_NM
+    nz = int(round(sum(layers_nm) / dz_nm))
+    dx = Lp / nz
+    x = (np.arange(periods * nz) + 0.5) * dx
+    chi = np.zeros((len(x), periods * states))
+    for p in range(periods):
+        centres = p * Lp + Lp * (np.arange(states) + 0.5) / states + 0.03 * Lp * rng.standard_normal(states)
+        widths = Lp * (0.10 + 0.12 * rng.random(states))
+        for s in range(states):
+            a = p * states + s
+            u = (x - centres[s]) / widths[s]
+            chi[:, a] = np.exp(-0.5 * u ** 2) * (1 + 0.4 * np.sin((1 + s % 3) * math.pi * u))
+    chi /= np.sqrt((chi ** 2).sum(axis=0) * dx)[None, :]
+    edges = np.cumsum(layers_nm) / L0_NM
+    interfaces = np.array([p * Lp + e for p in range(periods) for e in np.concatenate(([0.0], edges[:-1]))])
+    return x, np.full(len(x), dx), chi, interfaces
+
+
+def full_physics_problem(seed: int = 11, NE: int = 2048, Nk: int = 64, periods: int = 4, states: int = 8,
+                         Nqz: int = 401, Nphi: int = 64, lookup_nodes: int = 129, rtol: float = 1e-15,
+                         alpha: float = 0.5, bias_mV: float = 50.0) -> SCBAProblem:
+    """Full-physics-shaped SCBA structure: a supercell of `periods` periods x
+    `states` localised states (N_b = 32 by default) of the GaAs /
+    Al0.15Ga0.85As stack 4.0 / 8.5 / 2.0 / 16.0 nm, N_E = 2048 energies over
+    [-0.25, 0.40] eV, N_k = 64 momenta on 0-80 meV kinetic energy, T = 100 K,
+    with all five mechanisms built from the basis functions:
+
+    * LO phonon (36.7 meV): the exact screened Froehlich kernel
+      (lo_phonon_kernel, numerics/reference/kernels.jl:321-356) on N_qz = 401
+      longitudinal nodes (|q_z| <= 10 nm^-1) and N_phi = 64 angles, as a
+      separable sum;
+    * acoustic deformation potential (Xi = 7 eV, kernels.jl:246-283) and
+      alloy disorder (kernels.jl:285-319), momentum independent;
+    * ionised impurities, 2D sheet doping 3e10 cm^-2 per period in the 4 nm
+      layer: the tabulated screened covariance (numerics/optimized/
+      kernels.jl:122-158, 303-320) on `lookup_nodes` nodes, as a separable sum;
+    * interface roughness (Delta = 0.1 nm, Lambda = 8 nm) at every layer edge
+      (interface_roughness_kernel, kernels.jl:176-244), separable.
+
+    The basis functions, level scheme and couplings are synthetic and seeded;
+    the kernels follow the reference formulas with these basis functions.
+    `rtol` is the compression tolerance of the separable sums."""
+    from .kernel_build import (impurity_pair_factors, lo_form_factors, lo_weights, lookup_weights,
+                               separable_sum_operator, transfer_momenta)
+
+    rng = np.random.default_rng(seed)
+    Nb = periods * states
+    layers = [4.0, 8.5, 2.0, 16.0]
+    Ep = bias_mV * 1e-3 / E0_EV
+    eps, wE = energy_grid(-0.25 / E0_EV, 0.40 / E0_EV, NE)
+    Cbar = _kinetic_coefficient()
+    kmax = math.sqrt(0.080 / E0_EV / Cbar)
+    kappa, wk = momentum_grid(kmax, Nk)
+    levels = list(np.linspace(0.0, 0.24, states) + 0.004 * rng.standard_normal(states))
+    h0, Tplus, mix = _supercell(rng, periods, states, levels, Ep, 0.004)
+    h = np.zeros((Nk, Nb, Nb), dtype=np.complex128, order="F")
+    for m in range(Nk):
+        h[m] = h0 + Cbar * kappa[m] ** 2 * (np.eye(Nb) + mix)
+    x, wx, chi, interfaces = _period_basis(rng, periods, states, layers)
+    L0 = L0_NM * 1e-9
+    K0 = (E0_EV * E_CHARGE) ** 2 * L0 ** 2
+    T_K = 100.0
+    hw = 0.0367
+    mechs = []
+    # LO: prefactor e^2 hbar w / (2 eps0) (1/eps_inf - 1/eps_s) L0 / K0 (kernels.jl:340-355)
+    pre_lo = E_CHARGE ** 2 * hw * E_CHARGE / (2 * _EPS0) * (1 / _GAAS_EPS_INF - 1 / _GAAS_EPS_S) * L0 / K0
+    qz = np.linspace(-10.0 * L0_NM, 10.0 * L0_NM, Nqz)
+    wqz = np.full(Nqz, qz[1] - qz[0])
+    F = lo_form_factors(chi, x, wx, qz).reshape((Nqz, Nb * Nb), order="F")
+    W = lo_weights(kappa, Nphi, qz, wqz, qscreen=0.05 * L0_NM, prefactor=pre_lo)
+    mechs.append(separable_sum_operator("LO", W, F, rtol=rtol))
+    # acoustic: Xi^2 kB T / (rho v_s^2) / (L0 K0) sum_g w chi^4 (kernels.jl:262-283)
+    pre_ac = (_GAAS_XI_EV * E_CHARGE) ** 2 * _KB_J * T_K / (_GAAS_RHO * _GAAS_VS ** 2) / L0 / K0
+    Kac = acoustic_block(chi, wx, pre_ac)
+    q = float(np.max(np.abs(Kac)))
+    mechs.append(Mechanism("acoustic", "momentum_independent", q, block=block_matrix(Kac / q)))
+    # impurity: 3e10 cm^-2 per period over the cells of each period's first (4 nm) layer
+    Lp = sum(layers) / L0_NM
+    doped = ((x % Lp) < layers[0] / L0_NM)
+    sheet = 3e14 * L0 ** 2  # N_D L0^2 per period
+    donor_w = np.where(doped, wx, 0.0)
+    donor_w *= sheet * periods / donor_w.sum()
+    pre_imp = math.sqrt(E_CHARGE ** 4 / (2 * _EPS0 * _GAAS_EPS_S) ** 2 / K0)  # V in sqrt(K0) units
+    qmax = float(transfer_momenta(kappa, Nphi).max())
+    nodes = qmax * (np.arange(lookup_nodes) / (lookup_nodes - 1)) ** 2
+    qs_imp = 0.1 * L0_NM
+    VD = [impurity_pair_factors(qn, chi, x, wx, donor_w, qs_imp, pre_imp) for qn in nodes]
+    mechs.append(separable_sum_operator("impurity", lookup_weights(nodes, kappa, Nphi), np.array([v for v, _ in VD]),
+                                        VD[0][1], rtol=rtol))
+    # IFR: D_j[a,c] = dEc chi_a(z_j) chi_c(z_j); block = sum_j D_j (x) conj D_j; radial = angular
+    # mean of pi Delta^2 Lambda^2 exp(-q^2 Lambda^2 / 4) (interface_roughness_kernel, kernels.jl:176-244)
+    dEc = 0.831 * 0.15 / E0_EV
+    u = np.array([[np.interp(z, x, chi[:, a]) for a in range(Nb)] for z in interfaces])  # (J, Nb)
+    Jn = len(interfaces)
+    left = np.zeros((Nb * Nb, Jn), dtype=np.complex128)
+    for j in range(Jn):
+        left[:, j] = (dEc * np.outer(u[j], u[j])).reshape(Nb * Nb, order="F")
+    right = np.asfortranarray(left.conj().T)
+    Delta, Lam = 0.1 / L0_NM, 8.0 / L0_NM
+    qt = transfer_momenta(kappa, Nphi)
+    radial = (math.pi * Delta ** 2 * Lam ** 2 * np.exp(-qt ** 2 * Lam ** 2 / 4).mean(axis=2)).astype(np.complex128)
+    qifr = float(np.max(np.abs(radial))) * float(np.max(np.abs(left @ right)))
+    mechs.append(Mechanism("IFR", "ifr", qifr, left=np.asfortranarray(left), right=right,
+                           radial=np.asfortranarray(radial / qifr)))
+    # alloy: Omega dV^2 x(1 - x) in the barriers (kernels.jl:285-319), Omega = a^3 / 4, dV = 0.6 eV
+    xal = np.where(np.isin(np.floor((x % Lp) / (Lp / 4)).astype(int), [1, 3]), 0.15, 0.0)
+    pre_al = (0.565e-9) ** 3 / 4 * (0.6 * E_CHARGE) ** 2 / L0 / K0
+    Kal = acoustic_block(chi, wx * xal * (1 - xal), pre_al)
+    q = float(np.max(np.abs(Kal)))
+    mechs.append(Mechanism("alloy", "momentum_independent", q, block=block_matrix(Kal / q)))
+    kBT = KB_EV * T_K / E0_EV
+    target = 3e14 * L0 ** 2 * periods
+    return SCBAProblem(
+        NE=NE, Nk=Nk, Nb=Nb, eps=eps, wE=wE, wk=wk, h=h, Tplus=np.asfortranarray(Tplus),
+        Tminus=np.asfortranarray(Tplus.conj().T), Ep=Ep * periods, hw_LO=hw / E0_EV,
+        N_LO=1.0 / math.expm1(hw / (KB_EV * T_K)), gs=2, target=target, kBT=kBT,
+        eta_seed=0.0005 / E0_EV, alpha=alpha, mechanisms=mechs, name=f"full_physics_N{Nb}",
+    )

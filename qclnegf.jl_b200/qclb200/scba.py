@@ -31,7 +31,12 @@ class _Problem(ctypes.Structure):
                 ("retarded_real_part", ctypes.c_int), ("elastic_retarded", ctypes.c_int),
                 ("occupation_normalization", ctypes.c_int), ("mixing", ctypes.c_int),
                 ("anderson_history_depth", ctypes.c_int), ("anderson_damping", ctypes.c_double),
-                ("anderson_regularization", ctypes.c_double)]
+                ("anderson_regularization", ctypes.c_double), ("memory_budget_bytes", ctypes.c_size_t),
+                ("refinement", ctypes.c_int)]
+
+
+class MemoryEstimate(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_size_t) for n in ("fields", "operators", "workspace", "anderson", "resident", "peak")]
 
 
 class AndersonInfo(ctypes.Structure):
@@ -88,9 +93,23 @@ class ProductionSCBA:
     ``ProductionCache`` + state; calls on one context must be serialised,
     like the reference's plans, fft_parallel.jl:16-17)."""
 
-    def __init__(self, problem, precision="c128", verify_roundoff=True, use_graph=False):
+    def __init__(self, problem, precision="c128", verify_roundoff=True, use_graph=False, refinement=False,
+                 memory_budget_bytes=0):
+        """refinement: a reduced-precision context that can finish in FP64
+        (``promote``); memory_budget_bytes: the preflight budget (0 = the
+        device's free memory); a context above it raises MemoryBudgetError
+        before any allocation."""
         self.problem = problem
         self.precision = _prec(precision)
+        self._p, self._marr = self._structs(problem, verify_roundoff, refinement, memory_budget_bytes)
+        h = ctypes.c_void_p()
+        check(lib().qcl_scba_create(ctypes.byref(self._p), self._marr, ctypes.byref(h)))
+        self._h = h
+        if use_graph:
+            check(lib().qcl_scba_use_graph(self._h, 1))
+        self.mu = None
+
+    def _structs(self, problem, verify_roundoff, refinement, memory_budget_bytes):
         pr = problem
         self._keep = [np.ascontiguousarray(pr.eps, dtype=np.float64), np.ascontiguousarray(pr.wE, dtype=np.float64),
                       np.ascontiguousarray(pr.wk, dtype=np.float64), _c(pr.h), _c(pr.Tplus), _c(pr.Tminus)]
@@ -99,16 +118,11 @@ class ProductionSCBA:
                            float(pr.target), float(pr.eta_seed), float(pr.kBT), float(pr.alpha), float(pr.J0),
                            self.precision, 1 if verify_roundoff else 0, len(pr.mechanisms), *_switch_codes(pr),
                            int(getattr(pr, "anderson_history_depth", 5)), float(getattr(pr, "anderson_damping", 1.0)),
-                           float(getattr(pr, "anderson_regularization", 1e-12)))
+                           float(getattr(pr, "anderson_regularization", 1e-12)), int(memory_budget_bytes),
+                           1 if refinement else 0)
         self._mechs = [mechanism_struct(m) for m in pr.mechanisms]
         arr = (type(self._mechs[0]) * max(len(self._mechs), 1))(*self._mechs) if self._mechs else None
-        self._marr = arr
-        h = ctypes.c_void_p()
-        check(lib().qcl_scba_create(ctypes.byref(self._p), arr, ctypes.byref(h)))
-        self._h = h
-        if use_graph:
-            check(lib().qcl_scba_use_graph(self._h, 1))
-        self.mu = None
+        return self._p, arr
 
     def close(self):
         if getattr(self, "_h", None):
@@ -120,6 +134,12 @@ class ProductionSCBA:
             self.close()
         except Exception:
             pass
+
+    def promote(self):
+        """Finish in FP64: the state converts exactly to complex128 and the
+        following steps run in complex128 (a refinement context only)."""
+        check(lib().qcl_scba_promote(self._h))
+        self.precision = _prec("c128")
 
     def seed(self):
         mu = ctypes.c_double()
@@ -224,6 +244,18 @@ class ProductionSCBA:
     def family(self, f):
         """(SigmaR, Sigma<, Sigma>) of family f: 0..M-1 mechanisms, M plus, M+1 minus."""
         return tuple(self.download(3 + 3 * f + c) for c in range(3))
+
+
+def estimate_memory(problem, precision="c128", refinement=False, verify_roundoff=True):
+    """The device bytes a context for `problem` would allocate
+    (qcl_scba_estimate_memory): fields, operators, workspace, anderson,
+    resident, peak."""
+    tmp = ProductionSCBA.__new__(ProductionSCBA)
+    tmp.precision = _prec(precision)
+    p, arr = tmp._structs(problem, verify_roundoff, refinement, 0)
+    est = MemoryEstimate()
+    check(lib().qcl_scba_estimate_memory(ctypes.byref(p), arr, ctypes.byref(est)))
+    return {n: int(getattr(est, n)) for n, _ in est._fields_}
 
 
 def solve_scba_production(problem, iterations, *, precision="c128", verify_roundoff=True, tol_sigma=-1.0,

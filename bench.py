@@ -184,24 +184,31 @@ def cpu_inputs(N, m_count, seed):
 # ---------------------------------------------------------------------------
 # CPU path (the reference algorithm on the host cores: the oracle port)
 # ---------------------------------------------------------------------------
-def cpu_step(orc, eps, wE, h, SR, SL, Gam):
-    orc.dyson_keldysh(eps, h, SR, SL)
-    orc.fft_hilbert(Gam, eps, wE)
+def cpu_step(orc, eps, wE, h, SR, SL, Gam, threads):
+    """One step of the reference's production path on the host cores:
+    LAPACK inverse + lesser sandwich per (E, k) block, pocketfft Hilbert of
+    every column (the oracle's production restatements)."""
+    orc.production_green_lapack(eps, h, SR, SL, threads=threads)
+    orc.production_fft_hilbert_pocketfft(Gam, eps, wE, threads=threads)
 
 
-def cpu_rate(m_count=4, reps=1, warm=0):
-    """Green solves/s of the CPU port on m_count momenta (all energies)."""
+CPU_KIND_DETAIL = ("port of the reference production path: per-block inverse and products with LAPACK/BLAS "
+                   "(numpy, OpenBLAS), zero-padded FFT Hilbert with pocketfft (scipy.fft), threads over slabs")
+
+
+def cpu_rate(m_count=NK, reps=1, warm=0):
+    """Green solves/s of the CPU baseline on m_count momenta (all energies)."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as orc
 
     eps, wE = grids()
     h, SR, SL, Gam = cpu_inputs(NB, m_count, seed=11)
     for _ in range(warm):
-        cpu_step(orc, eps, wE, h, SR, SL, Gam)
+        cpu_step(orc, eps, wE, h, SR, SL, Gam, cores())
     t = []
     for _ in range(reps):
         t0 = time.perf_counter()
-        cpu_step(orc, eps, wE, h, SR, SL, Gam)
+        cpu_step(orc, eps, wE, h, SR, SL, Gam, cores())
         t.append(time.perf_counter() - t0)
     t.sort()
     sec = t[len(t) // 2]
@@ -222,6 +229,51 @@ def cpu_scba_tutorial(iters=2):
     t0 = time.perf_counter()
     orc.scba(pr, iters, state=st)
     return (time.perf_counter() - t0) / iters * 1e3
+
+
+def sampled_parity(torch, eps, wE, h, SR, SL, GR, GL, Gam, Lam, nblk=64, ncol=32, seed=0):
+    """Parity of a benchmarked batch against the oracle on a fixed random
+    sample: `nblk` (e, k) blocks of G^R and G^< (oracle retarded_green /
+    keldysh_green on the same, possibly complex64-rounded, inputs) and `ncol`
+    Hilbert columns (oracle fft_hilbert).  Device fields are Julia-layout
+    tensors of shape (N, N, N_k, N_E); Gam / Lam are (columns, N_E).  Returns
+    the largest relative errors (Julia isapprox norm)."""
+    import numpy as np
+
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as orc
+
+    rng = np.random.default_rng(seed)
+    N, nk, ne = SR.shape[1], SR.shape[2], SR.shape[3]
+    es = torch.as_tensor(rng.integers(0, ne, nblk), device=SR.device)
+    ms = torch.as_tensor(rng.integers(0, nk, nblk), device=SR.device)
+
+    def blocks(X):  # (nblk, a, b) complex128 on the host
+        return X[:, :, ms, es].permute(2, 1, 0).to(torch.complex128).cpu().numpy()
+
+    sr, sl, gr, gl = (blocks(X) for X in (SR, SL, GR, GL))
+
+    def rel(x, y):
+        d = max(np.linalg.norm(x), np.linalg.norm(y))
+        return 0.0 if d == 0 else float(np.linalg.norm(x - y) / d)
+
+    eg, el = 0.0, 0.0
+    for i in range(nblk):
+        e, m = int(es[i]), int(ms[i])
+        f = lambda a: np.asfortranarray(a.reshape((1, 1, N, N)))
+        oGR = orc.retarded_green(eps[e:e + 1], np.asfortranarray(h[m:m + 1]), f(sr[i]))[0]
+        oGL = orc.keldysh_green(oGR, f(sl[i]))
+        eg = max(eg, rel(gr[i], oGR[0, 0]))
+        el = max(el, rel(gl[i], oGL[0, 0]))
+    cols = torch.as_tensor(rng.integers(0, Gam.shape[0] if Gam.dim() == 2 else Gam.numel() // ne, ncol),
+                           device=Gam.device)
+    G2, L2 = Gam.reshape(-1, ne), Lam.reshape(-1, ne)
+    gam = np.asfortranarray(G2[cols].to(torch.complex128).cpu().numpy().T)
+    lam = L2[cols].to(torch.complex128).cpu().numpy().T
+    olam = orc.fft_hilbert(gam, eps, wE)
+    eh = max(rel(lam[:, j], olam[:, j]) for j in range(ncol))
+    return {"GR_max_rel_err": eg, "GL_max_rel_err": el, "hilbert_max_rel_err": eh, "blocks": nblk,
+            "hilbert_columns": ncol, "oracle": "oracle.retarded_green / keldysh_green / fft_hilbert (FP64)"}
 
 
 def cores():
@@ -269,28 +321,28 @@ def run_reference(args):
         if dist:
             dist.destroy_process_group()
         return
-    m_count = 8  # a bounded sample of 8 of the 32 momenta (all 4096 energies) per step
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as orc
 
     eps, wE = grids()
-    h, SR, SL, Gam = cpu_inputs(NB, m_count, seed=11)
+    h, SR, SL, Gam = cpu_inputs(NB, NK, seed=11)  # the full batch: 32 momenta x 4096 energies
+    th = cores()
     for _ in range(args.warmup):
-        cpu_step(orc, eps, wE, h, SR, SL, Gam)
+        cpu_step(orc, eps, wE, h, SR, SL, Gam, th)
     t0 = time.perf_counter()
     for _ in range(args.steps):
-        cpu_step(orc, eps, wE, h, SR, SL, Gam)
+        cpu_step(orc, eps, wE, h, SR, SL, Gam, th)
     sec = (time.perf_counter() - t0) / args.steps
-    rate = NE * m_count / sec
-    full_ms = NE * NK / rate * 1e3
-    sample = f"{m_count} of {NK} momenta x {NE} energies per step (Dyson+Keldysh and the Hilbert columns of those momenta)"
+    rate = NE * NK / sec
+    full_ms = sec * 1e3
+    sample = f"the full batch ({NK} momenta x {NE} energies, {NK * NB * NB} Hilbert columns) every step; {CPU_KIND_DETAIL}"
     line = {
         "impl": "reference", "metric": "(E,k) Green solves/s", "value": rate, "unit": "solves/s",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": full_ms,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64 (complex128)",
         "data": "synthetic", "config": {"workload": f"operator batch N_E x N_k = {NE} x {NK}, N_b = {NB}, "
                                                     "Dyson + Keldysh G^< + FFT Hilbert (L = 8192)"},
-        "cpu_baseline": {"value": rate, "unit": "solves/s", "cores": cores(), "kind": "port", "sample": sample},
+        "cpu_baseline": {"value": rate, "unit": "solves/s", "cores": th, "kind": "port", "sample": sample},
         "e2e": {"value": rate, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -433,6 +485,11 @@ def run_gpu(args):
         e2e["max_abs_diff_vs_device_run"] = diff
         del hSR, hSL, hGam, hGR, hGL, hLam
 
+    try:
+        parity = sampled_parity(torch, eps, wE, hf.cpu().numpy().reshape((NB, NB, NK)).transpose(2, 1, 0), SR, SL,
+                                GR, GL, Gam, Lam)
+    except Exception as ex:  # noqa: BLE001
+        parity = {"error": repr(ex)}
     peak, peak_kind = measured_peaks()
     achieved_gbs = BYTES_PER_BLOCK * NE * NK / (dyson_ms / 1e3) / 1e9
     achieved_tflops = FLOP_PER_BLOCK * NE * NK / (dyson_ms / 1e3) / 1e12
@@ -453,6 +510,7 @@ def run_gpu(args):
                      "fp64_frac_of_nominal": achieved_tflops / fp64_nominal},
         "gpu_launches": gpu_launches,
         "e2e": e2e,
+        "parity": parity,
     }
     # ---- CPU baseline on the host cores (rank 0, N = 1) ------------------------------
     if ws == 1:
@@ -460,7 +518,7 @@ def run_gpu(args):
             rate, sec = cpu_rate(m_count=NK, reps=3, warm=1)
             line["cpu_baseline"] = {"value": rate, "unit": "solves/s", "cores": cores(), "kind": "port",
                                     "sample": f"the full batch ({NK} momenta x {NE} energies), median of 3 "
-                                              f"after 1 warm-up, {sec:.2f} s per batch"}
+                                              f"after 1 warm-up, {sec:.2f} s per batch; {CPU_KIND_DETAIL}"}
             line["cpu_baseline"]["scba_tutorial_N12"] = {
                 "ms_per_iter": cpu_scba_tutorial(), "kind": "port", "cores": cores(),
                 "sample": "2 SCBA iterations of the tutorial problem (N_E x N_k = 400 x 16, N_b = 12, roundoff "
@@ -536,6 +594,11 @@ def extras(torch, dev, L, _lib):
         out[name] = {"dyson_keldysh_ms": ms, "solves_per_s": NE * NK / (ms / 1e3), "hilbert_ms": times["hilbert_ms"],
                      "step_solves_per_s": NE * NK / ((ms + times["hilbert_ms"]) / 1e3),
                      "hilbert_columns": ncols}
+        try:
+            hh = hf.cpu().numpy().reshape((N, N, NK)).transpose(2, 1, 0)
+            out[name]["parity"] = sampled_parity(torch, eps, wE, hh, SR, SL, GR, GL, Gam, Lam, seed=N + prec)
+        except Exception as ex:  # noqa: BLE001
+            out[name]["parity"] = {"error": repr(ex)}
         del SR, SL, GR, GL, Gam, Lam
         torch.cuda.empty_cache()
     # SCBA iterations/s at tutorial scale

@@ -58,6 +58,12 @@ extern "C" {
 int qcl_version(void);
 /* Message of the last failing call on this thread ("" if none). */
 const char* qcl_last_error(void);
+/* The k of the last QCL_SINGULAR failure on this thread: 0 for a block whose
+ * row-sum scale is zero or non-finite, else the 1-based index of the first
+ * zero pivot of the block's partial-pivoting elimination (LAPACK getrf's
+ * info) -- the argument of the reference's SingularException(k)
+ * (numerics/optimized/production_operators.jl:39, 94, 1372). */
+int qcl_last_singular_pivot(void);
 /* Largest supported basis size N_b. */
 int qcl_max_basis(void);
 
@@ -264,7 +270,9 @@ int qcl_residual_suite_witness(int precision, int NE, int Nk, int Nb, const doub
  * of the library (about 18.9 MB per GPU, held until exit), so N_E * N_k must
  * not exceed 262144 (QCL_UNSUPPORTED otherwise).  Calls share that array:
  * calls that overlap on the GPU race.  The first call on a device looks up
- * the array's address on that device; make it before any stream capture. */
+ * the array's address on that device; make it before any stream capture.
+ * After a device reset (cudaDeviceReset) that address is stale: do not call
+ * the entry point again in that process. */
 int qcl_dev_residual_suite_noalloc(void* stream, int precision, int NE, int Nk, int Nb, const double* eps,
                                    const void* h, const void* GR, const void* GL, const void* GG, const void* SR,
                                    const void* SL, const void* SG, const void* SLc, double* out);

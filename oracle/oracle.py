@@ -952,3 +952,70 @@ def scba(problem, iterations, verify=True, state=None, keep_state=False, termina
         Jprev, pprev = J, pops
     out_state = dict(scattering=scattering, plus=plus, minus=minus, green=green) if keep_state else None
     return history, out_state
+
+
+# --------------------------------------------------------------------------
+# The reference's production path on the host cores with library arithmetic
+# (the CPU baseline of the benchmark): LAPACK through numpy (OpenBLAS) for
+# the per-block inverse and products, pocketfft (scipy.fft) for the Hilbert
+# transform, threads over independent slabs as the :threads backend of
+# ProductionOptions (production_contracts.jl:113-121).
+# --------------------------------------------------------------------------
+def production_green_lapack(eps, h, SR, SL, threads=1, chunk=512):
+    """_retarded_green_production (production_operators.jl:1337-1385: row-sum
+    scale s, G = inv(D/s)/s with LAPACK) fused with the lesser sandwich of
+    _current_green_production (production_state.jl:29-47).  The condition
+    number kappa (an SVD per block) is not formed, as on the device.
+    Returns (GR, GL) in the Julia layout."""
+    import concurrent.futures
+
+    eps = np.asarray(eps, dtype=np.float64)
+    h = np.asarray(h)
+    NE, Nk, N, _ = SR.shape
+    GR = np.empty(SR.shape, dtype=np.complex128, order="F")
+    GL = np.empty(SR.shape, dtype=np.complex128, order="F")
+    eye = np.eye(N)
+
+    def work(task):
+        m, e0 = task
+        e1 = min(NE, e0 + chunk)
+        D = eps[e0:e1, None, None] * eye - h[m][None] - SR[e0:e1, m]
+        s = np.max(np.sum(np.abs(D), axis=2), axis=1)[:, None, None]
+        G = np.linalg.inv(D / s) / s
+        GR[e0:e1, m] = G
+        GL[e0:e1, m] = G @ SL[e0:e1, m] @ np.conj(np.swapaxes(G, -1, -2))
+
+    tasks = [(m, e0) for m in range(Nk) for e0 in range(0, NE, chunk)]
+    with concurrent.futures.ThreadPoolExecutor(max(1, threads)) as ex:
+        list(ex.map(work, tasks))
+    return GR, GL
+
+
+def production_fft_hilbert_pocketfft(Gam, eps, wE, threads=1, chunk=512):
+    """production_fft_hilbert_transform (fft_parallel.jl:168-291): per column
+    the weighted field zero-padded to L = nextpow2(2 N_E - 1), multiplied in
+    Fourier space by the spectrum of k[lag + N_E - 1] = 1 / (2 pi lag de),
+    output y[e + N_E - 1]; columns in chunks, each chunk's FFTs over
+    `threads` workers."""
+    import scipy.fft
+
+    Gam = np.asarray(Gam)
+    NE = Gam.shape[0]
+    cols = Gam.reshape((NE, -1), order="F")
+    ncols = cols.shape[1]
+    L = 1 << (2 * NE - 2).bit_length()
+    de = float(eps[1] - eps[0])
+    kern = np.zeros(L, dtype=np.complex128)
+    lag = np.arange(-(NE - 1), NE)
+    nz = lag != 0
+    kern[lag[nz] + NE - 1] = 1.0 / (2 * math.pi * lag[nz] * de)
+    khat = scipy.fft.fft(kern)
+    out = np.empty((NE, ncols), dtype=np.complex128, order="F")
+    w = np.asarray(wE, dtype=np.float64)
+    for c0 in range(0, ncols, chunk):
+        c1 = min(ncols, c0 + chunk)
+        buf = np.zeros((c1 - c0, L), dtype=np.complex128)
+        buf[:, :NE] = (cols[:, c0:c1] * w[:, None]).T
+        y = scipy.fft.ifft(scipy.fft.fft(buf, axis=1, workers=threads) * khat[None, :], axis=1, workers=threads)
+        out[:, c0:c1] = y[:, NE - 1:2 * NE - 1].T
+    return out.reshape(Gam.shape, order="F")

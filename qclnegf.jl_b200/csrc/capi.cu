@@ -20,6 +20,15 @@ void set_last_error(const char* fmt, ...) {
   va_end(ap);
 }
 
+static thread_local int g_singular_pivot = 0;
+
+int singular_status(const char* what, int where) {
+  const int block = (int)(where / kSingularPivotSpan), k = (int)(where % kSingularPivotSpan);
+  g_singular_pivot = k;
+  set_last_error("%s: singular block (linear block index %d, SingularException(%d))", what, block, k);
+  return QCL_SINGULAR;
+}
+
 int cuda_status(cudaError_t e, const char* where) {
   set_last_error("CUDA error %s (%s) at %s", cudaGetErrorName(e), cudaGetErrorString(e), where);
   if (e == cudaErrorMemoryAllocation) return QCL_NOMEM;
@@ -74,10 +83,7 @@ static int read_status(const int* dstatus, const char* what) {
   int h[2] = {0, 0};
   cudaError_t e = cudaMemcpy(h, dstatus, sizeof(h), cudaMemcpyDeviceToHost);
   if (e != cudaSuccess) return cuda_status(e, what);
-  if (h[0] == QCL_SINGULAR) {
-    set_last_error("%s: singular block (linear block index %d)", what, h[1]);
-    return QCL_SINGULAR;
-  }
+  if (h[0] == QCL_SINGULAR) return singular_status(what, h[1]);
   if (h[0] != 0) {
     set_last_error("%s: device status %d at %d", what, h[0], h[1]);
     return h[0];
@@ -181,6 +187,7 @@ extern "C" {
 
 int qcl_version(void) { return 100; }
 const char* qcl_last_error(void) { return g_last_error; }
+int qcl_last_singular_pivot(void) { return g_singular_pivot; }
 int qcl_max_basis(void) { return 48; }
 
 int qcl_dev_dyson_keldysh(void* stream, int precision, int NE, int Nk, int Nb, const double* eps, double eta,

@@ -126,8 +126,15 @@ __device__ __forceinline__ void record_status(int* status, int code, long long w
   if (atomicCAS(status, 0, code) == 0) status[1] = (int)where;
 }
 
+// A QCL_SINGULAR status stores block * kSingularPivotSpan + k, k the index of
+// SingularException(k) (0: zero scale; else the 1-based first zero pivot).
+constexpr long long kSingularPivotSpan = 64;
+
 // Host-side error plumbing --------------------------------------------------
 void set_last_error(const char* fmt, ...);
+// Records a QCL_SINGULAR device status word (block * 64 + k) for
+// qcl_last_singular_pivot and formats the message; returns QCL_SINGULAR.
+int singular_status(const char* what, int where);
 int cuda_status(cudaError_t e, const char* where);
 
 #define QCL_CUDA_CHECK(expr)                                   \

@@ -186,6 +186,7 @@ __global__ void __launch_bounds__(BPC* Tile<NP>::TT, (dyson_min_ctas<RS, RL, NP,
   // row at the end instead of to the whole pivot row at every step.
   bool used = !has_row;
   bool singular = !scale_ok;
+  int zstep = -1;  // first step without a non-zero pivot (the k of SingularException(k) is zstep + 1)
   int mystep = row;
   Cx<RL> myrc = cx<RL>(1, 0);
   const int lane = threadIdx.x & 31;
@@ -212,6 +213,7 @@ __global__ void __launch_bounds__(BPC* Tile<NP>::TT, (dyson_min_ctas<RS, RL, NP,
         const int best = 63 - (int)(key & 63u);
         const bool zero = pivot_key_zero(key);
         singular |= zero;
+        if (zero && zstep < 0) zstep = k;
         if (tt == 0) S.pivrow[k] = best;
         Cx<RL> f = wk;
         if (CPR > 1) {
@@ -254,7 +256,11 @@ __global__ void __launch_bounds__(BPC* Tile<NP>::TT, (dyson_min_ctas<RS, RL, NP,
     }
   }
   team_sync<TT>(team);
-  if (singular && live && tt == 0) record_status(p.status, QCL_SINGULAR, (long long)e + (long long)NE * m);
+  // where = block * 64 + k: k = 0 for a zero or non-finite row-sum scale, else the 1-based first zero
+  // pivot (LAPACK getrf's info), as SingularException(k) in production_operators.jl:39, 94, 1372
+  if (singular && live && tt == 0)
+    record_status(p.status, QCL_SINGULAR,
+                  ((long long)e + (long long)NE * m) * kSingularPivotSpan + (scale_ok ? zstep + 1 : 0));
   // inverse(D/s)[step][pivrow[k']] = w[k'] / pivot(step);  GR = that / s
   if (has_row) {
     const Cx<RL> rs = inv_s * myrc;

@@ -1347,13 +1347,18 @@ size_t residual_work_doubles(int NE, int Nk) { return kResidualBlockDoubles * (s
 // that loads the library holds it (about 18.9 MB) until the process exits.
 // ---------------------------------------------------------------------------
 constexpr long long kNoAllocMaxBlocks = 1ll << 18;  // N_E * N_k <= 262144
-static __device__ __align__(256) double g_residual_scratch[kResidualBlockDoubles * kNoAllocMaxBlocks + 7 * 148];
+// the layout of residual_work_doubles(N_E, N_k) at N_E * N_k = kNoAllocMaxBlocks
+constexpr long long kNoAllocScratchDoubles = kResidualBlockDoubles * kNoAllocMaxBlocks + 7ll * RES_CTAS;
+static __device__ __align__(256) double g_residual_scratch[kNoAllocScratchDoubles];
 
 static std::mutex g_noalloc_mutex;
 static double* g_noalloc_ptr[64] = {nullptr};
 
 // Device address of the scratch array on the current device, resolved once
-// per device (host code cannot use the symbol itself as an address).
+// per device (host code cannot use the symbol itself as an address).  The
+// address stays valid for the life of the device context: after a
+// cudaDeviceReset (CUDA.jl's device_reset!) every device pointer held by the
+// library is stale, this one included, and the entry point must not be used.
 static int noalloc_scratch(double** out) {
   int dev = 0;
   QCL_CUDA_CHECK(cudaGetDevice(&dev));
@@ -1463,6 +1468,10 @@ extern "C" int qcl_dev_residual_suite_noalloc(void* stream, int precision, int N
   if (!eps || !h || !GR || !GL || !GG || !SR || !SL || !SG || !SLc || !out) {
     set_last_error("residual_suite_noalloc: all arrays are required");
     return QCL_ARG;
+  }
+  if ((long long)residual_work_doubles(NE, Nk) > kNoAllocScratchDoubles) {  // holds by the block limit above
+    set_last_error("residual_suite_noalloc: scratch layout exceeds the fixed array");
+    return QCL_UNSUPPORTED;
   }
   double* scratch = nullptr;
   int s = noalloc_scratch(&scratch);

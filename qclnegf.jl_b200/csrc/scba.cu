@@ -773,6 +773,7 @@ int scba_seed(ScbaCtx* c, double* mu_out) {
   QCL_CUDA_CHECK(cudaStreamSynchronize(c->st));
   int hst[2];
   QCL_CUDA_CHECK(cudaMemcpy(hst, c->status, sizeof(hst), cudaMemcpyDeviceToHost));
+  if (hst[0] == QCL_SINGULAR) return singular_status("seed Dyson solve", hst[1]);
   if (hst[0]) {
     set_last_error("seed Dyson solve failed (status %d at block %d)", hst[0], hst[1]);
     return hst[0];
@@ -945,8 +946,7 @@ int scba_step(ScbaCtx* c, qcl_scba_row* row) {
   if (hst[0] == QCL_SINGULAR) {
     // a Dyson failure carries no partial state (production_solver.jl:447-469)
     c->pending_commit = false;
-    set_last_error("singular Dyson block (linear block index %d)", hst[1]);
-    return QCL_SINGULAR;
+    return singular_status("SCBA Dyson solve", hst[1]);
   }
   if (hst[0] == QCL_DOMAIN) {
     c->pending_commit = false;

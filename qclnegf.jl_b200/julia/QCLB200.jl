@@ -24,10 +24,13 @@ const QCL_MIXED = Cint(2)
 function check(status::Cint)
     status == 0 && return nothing
     msg = unsafe_string(ccall((:qcl_last_error, libqcl), Cstring, ()))
-    status == 1 && throw(SingularException(0))
+    # the index of the failing pivot, as _production_inverse! reports LAPACK's info
+    status == 1 && throw(SingularException(Int(ccall((:qcl_last_singular_pivot, libqcl), Cint, ()))))
     status == 2 && throw(DomainError(msg))
     status == 3 && throw(DimensionMismatch(msg))
     status == 4 && throw(ArgumentError(msg))
+    # the memory preflight refuses as build_production_cache does (production_cache.jl:764-770)
+    status == 8 && throw(ArgumentError(msg))
     error("qclb200 status $status: $msg")
 end
 

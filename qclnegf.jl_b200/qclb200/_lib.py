@@ -44,7 +44,11 @@ class QCLError(RuntimeError):
 
 
 class SingularException(QCLError):
-    """Reference: LinearAlgebra.SingularException (production_operators.jl:39,94)."""
+    """Reference: LinearAlgebra.SingularException (production_operators.jl:39,94);
+    ``k`` is its index: 0 for a zero row-sum scale, else the 1-based first
+    zero pivot (qcl_last_singular_pivot)."""
+
+    k = 0
 
 
 class DomainError(QCLError, ValueError):
@@ -153,6 +157,7 @@ def _declare(l):
         "qcl_scba_retarget": (I, [P, D, D, D, P, P]),
         "qcl_scba_estimate_memory": (I, [P, P, P]),
         "qcl_scba_promote": (I, [P]),
+        "qcl_last_singular_pivot": (I, []),
         "qcl_scba_mixer_info": (I, [P, P]),
         "qcl_anderson_guard": (I, [I, I, I, I, I, P, P, P]),
         "qcl_scba_density_matrix": (I, [P, P]),
@@ -177,5 +182,8 @@ def declare(name, res, args):
 def check(status):
     if status != QCL_OK:
         msg = lib().qcl_last_error().decode(errors="replace")
-        raise _EXC.get(status, QCLError)(status, msg or f"qclb200 status {status}")
+        exc = _EXC.get(status, QCLError)(status, msg or f"qclb200 status {status}")
+        if status == QCL_SINGULAR:
+            exc.k = int(lib().qcl_last_singular_pivot())
+        raise exc
     return status

@@ -67,14 +67,24 @@ def test_dyson_singular_block_raises(gpu_ops):
     SR = np.zeros((5, 1, 3, 3), dtype=complex, order="F")
     SR[:, 0] = np.diag([0.0, 0.0, 0.0])
     # eps[0] = 0 with h = 0 and SR = 0 gives D = 0: scale 0 -> SingularException(0)
-    with pytest.raises(SingularException):
+    with pytest.raises(SingularException) as ex:
         gpu_ops.retarded_green(eps, h, SR)
-    # a rank-deficient (but non-zero) block
+    assert ex.value.k == 0
+    # a rank-deficient (but non-zero) block: D = ones(3, 3), whose first
+    # elimination step leaves a zero column -> LAPACK getrf info = 2
     SR2 = np.zeros((5, 1, 3, 3), dtype=complex, order="F")
     for e in range(5):
         SR2[e, 0] = eps[e] * np.eye(3) - np.ones((3, 3))
-    with pytest.raises(SingularException):
+    with pytest.raises(SingularException) as ex:
         gpu_ops.retarded_green(eps, h, SR2)
+    assert ex.value.k == 2
+    # D = diag(1, 2, 0) at every energy: the third pivot is zero -> info = 3
+    SR3 = np.zeros((5, 1, 3, 3), dtype=complex, order="F")
+    for e in range(5):
+        SR3[e, 0] = eps[e] * np.eye(3) - np.diag([1.0, 2.0, 0.0])
+    with pytest.raises(SingularException) as ex:
+        gpu_ops.retarded_green(eps, h, SR3)
+    assert ex.value.k == 3
 
 
 @pytest.mark.parametrize("NE", [37, 64, 400, 1000, 1025, 2048, 3001, 4096])

@@ -462,6 +462,21 @@ int qcl_scba_mixer_info(qcl_scba* ctx, qcl_anderson_info* info);
  * application/algorithm_registry.jl:226-240).  QCL_ARG if the context was
  * not created for refinement; a no-op on a QCL_C128 context. */
 int qcl_scba_promote(qcl_scba* ctx);
+/* Phase telemetry (the :phase_begin / :phase_end SolverEvents of
+ * ProductionOptions.phase_timing, application/production_telemetry.jl:81-200,
+ * emitted at production_solver.jl:438-590 and production_iteration.jl:1-65):
+ * with telemetry on, CUDA events at the phase boundaries of every iteration
+ * (event-record nodes inside a captured graph) give the device time of each
+ * phase.  qcl_scba_phase_times writes the last step's times in milliseconds
+ * for the QCL_PHASES phases in this order -- dyson, candidate_scattering,
+ * candidate_embedding, candidate_assembly, residuals, observables, mixing --
+ * and the last seed's :initialization time.  Phases run back to back on the
+ * context's stream except that the G-only part of the residual suite runs on
+ * a side stream during the candidate phases; "residuals" is the time from the
+ * candidate total to the end of the reduction. */
+#define QCL_PHASES 7
+int qcl_scba_use_telemetry(qcl_scba* ctx, int enable);
+int qcl_scba_phase_times(qcl_scba* ctx, double* ms, double* initialization_ms);
 /* Replay each iteration as one captured CUDA graph (default off). */
 int qcl_scba_use_graph(qcl_scba* ctx, int enable);
 /* The derived GreenState fields of the last Dyson solve (seed or step) --

@@ -147,6 +147,8 @@ int scba_witness(ScbaCtx* c, double* out12);
 int scba_retarget(ScbaCtx* c, double Ep, double N_LO, double kBT, const void* h, const double* q);
 int scba_estimate_memory(const qcl_scba_problem* p, const qcl_mechanism* mechs, size_t out[6]);
 int scba_promote(ScbaCtx* c);
+int scba_set_telemetry(ScbaCtx* c, int enable);
+int scba_phase_times(ScbaCtx* c, double* ms, double* init_ms);
 int scba_mixer_info(ScbaCtx* c, qcl_anderson_info* out);
 int scba_density_matrix(ScbaCtx* c, void* out);
 
@@ -745,6 +747,22 @@ int qcl_scba_estimate_memory(const qcl_scba_problem* problem, const qcl_mechanis
   out->resident = v[4];
   out->peak = v[5];
   return QCL_OK;
+}
+
+int qcl_scba_use_telemetry(qcl_scba* ctx, int enable) {
+  if (!ctx) {
+    set_last_error("ctx is required");
+    return QCL_ARG;
+  }
+  return scba_set_telemetry((ScbaCtx*)ctx, enable);
+}
+
+int qcl_scba_phase_times(qcl_scba* ctx, double* ms, double* initialization_ms) {
+  if (!ctx) {
+    set_last_error("ctx is required");
+    return QCL_ARG;
+  }
+  return scba_phase_times((ScbaCtx*)ctx, ms, initialization_ms);
 }
 
 int qcl_scba_promote(qcl_scba* ctx) {

@@ -76,6 +76,11 @@ enum {
   SC_TOTAL = SC_ROUND + 5 * 2
 };
 
+// Phases of an iteration, in the reference's names (production_solver.jl:438-590,
+// production_iteration.jl:1-65): dyson, candidate_scattering, candidate_embedding,
+// candidate_assembly, residuals, observables, mixing.
+constexpr int kPhases = 7;
+
 struct ScbaCtx {
   int NE, Nk, N, M, precision, gs, verify;
   int refinement = 0;  // FP64-sized state and complex128 operator copies for qcl_scba_promote
@@ -123,6 +128,12 @@ struct ScbaCtx {
   cudaStream_t st2 = nullptr;  // side stream of an iteration (forked from st, joined back)
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   bool use_graph = false;
+  // phase telemetry: device time between CUDA events at the phase boundaries of an
+  // iteration (the :phase_begin / :phase_end events of production_telemetry.jl:81-200)
+  bool telemetry = false;
+  cudaEvent_t pev[kPhases + 1] = {};
+  double phase_ms[kPhases] = {};
+  double init_ms = 0;
   int parity = 0;
   bool pending_commit = false;
   int nu = 0;
@@ -254,6 +265,8 @@ void scba_destroy(ScbaCtx* c) {
   cudaFree(c->apartial);
   if (c->ameta_h) cudaFreeHost(c->ameta_h);
   free_hilbert_tables(c->hil);
+  for (auto& e : c->pev)
+    if (e) cudaEventDestroy(e);
   if (c->ev_fork) cudaEventDestroy(c->ev_fork);
   if (c->ev_join) cudaEventDestroy(c->ev_join);
   if (c->st2) cudaStreamDestroy(c->st2);
@@ -679,10 +692,20 @@ static int current_green(ScbaCtx* c, const std::vector<void*>& fam) {
 
 // Everything of one iteration after the state is fixed; writes candidates into
 // `cand`, mixed values into `cand` as well (speculatively) and all scalars.
+// Marks the end of phase i - 1 / start of phase i (an event-record node when
+// the iteration is captured into a graph).
+static int phase_mark(ScbaCtx* c, int i) {
+  if (!c->telemetry) return QCL_OK;
+  QCL_CUDA_CHECK(cudaEventRecordWithFlags(c->pev[i], c->st, cudaEventRecordExternal));
+  return QCL_OK;
+}
+
 static int iteration_body(ScbaCtx* c, std::vector<void*>& state, std::vector<void*>& cand) {
   int s;
   const int sp = c->precision == QCL_MIXED ? QCL_C64 : c->precision;
+  if ((s = phase_mark(c, 0))) return s;
   if ((s = current_green(c, state))) return s;
+  if ((s = phase_mark(c, 1))) return s;
   // Everything of the residual suite except r_K needs only G and the totals:
   // it runs on the side stream while the candidates are built; r_K follows the
   // candidate total lesser, and the fixed-order reduction waits for both (the
@@ -694,7 +717,9 @@ static int iteration_body(ScbaCtx* c, std::vector<void*>& state, std::vector<voi
     return s;
   QCL_CUDA_CHECK(cudaEventRecord(c->ev_join, c->st2));
   if ((s = scattering_candidates(c, c->GR, c->GL, c->GG, cand, c->verify != 0))) return s;
+  if ((s = phase_mark(c, 2))) return s;
   if ((s = embedding_candidates(c, cand))) return s;
+  if ((s = phase_mark(c, 3))) return s;
   // candidate total lesser for r_K
   {
     const void* src[8];
@@ -702,6 +727,7 @@ static int iteration_body(ScbaCtx* c, std::vector<void*>& state, std::vector<voi
     for (int f = 0; f < F; ++f) src[f] = field_of(cand, f, 1);
     if ((s = launch_sum_fields(sp, c->nfield, src, F, c->candSL, c->st))) return s;
   }
+  if ((s = phase_mark(c, 4))) return s;
   if ((s = launch_residual_blocks(c->precision, RES_PART_RK, c->NE, c->Nk, c->N, c->eps, c->h, c->GR, c->GL, c->GG,
                                   c->tot[0], c->tot[1], c->tot[2], c->candSL, c->reswork, c->st)))
     return s;
@@ -713,10 +739,12 @@ static int iteration_body(ScbaCtx* c, std::vector<void*>& state, std::vector<voi
                                   field_of(cand, c->M, k), field_of(cand, c->M + 1, k), c->rpartial,
                                   c->scal + SC_EMB + 2 * k, c->st)))
       return s;
+  if ((s = phase_mark(c, 5))) return s;
   // J from the (unmixed) plus family and the state's G
   if ((s = launch_observables(sp, c->NE, c->Nk, c->N, c->wE, c->wk, field_of(state, c->M, 2), field_of(state, c->M, 1),
                               c->GL, c->GG, c->gs, c->target, c->obspartial, c->scal + SC_OBS, c->st)))
     return s;
+  if ((s = phase_mark(c, 6))) return s;
   // per-family residual + speculative linear mixing into the candidate buffers
   const int F = c->M + 2;
   const void* olds[kMaxMixFields];
@@ -747,6 +775,7 @@ static int iteration_body(ScbaCtx* c, std::vector<void*>& state, std::vector<voi
                                             c->scal + SC_FAM, c->st))) {
     return s;
   }
+  if ((s = phase_mark(c, 7))) return s;
   QCL_CUDA_CHECK(cudaMemcpyAsync(c->scal_h, c->scal, SC_TOTAL * sizeof(double), cudaMemcpyDeviceToHost, c->st));
   return QCL_OK;
 }
@@ -761,6 +790,7 @@ static double fermi(double e, double mu, double kBT) {
 int scba_seed(ScbaCtx* c, double* mu_out) {
   int s;
   const int sp = c->precision == QCL_MIXED ? QCL_C64 : c->precision;
+  if (c->telemetry) QCL_CUDA_CHECK(cudaEventRecord(c->pev[0], c->st));
   // Dyson with eta_seed and Sigma = 0 (cand fields used as scratch zeros)
   QCL_CUDA_CHECK(cudaMemsetAsync(c->tot[0], 0, c->fbytes, c->st));
   if ((s = launch_dyson_keldysh(c->precision, c->NE, c->Nk, c->N, c->eps, c->eta_seed, c->h, c->tot[0], nullptr,
@@ -830,6 +860,13 @@ int scba_seed(ScbaCtx* c, double* mu_out) {
     return hst[0];
   }
   if (mu_out) *mu_out = mu;
+  if (c->telemetry) {  // :initialization (seed + initial candidates)
+    QCL_CUDA_CHECK(cudaEventRecord(c->pev[1], c->st));
+    QCL_CUDA_CHECK(cudaEventSynchronize(c->pev[1]));
+    float ms = 0;
+    QCL_CUDA_CHECK(cudaEventElapsedTime(&ms, c->pev[0], c->pev[1]));
+    c->init_ms = ms;
+  }
   c->seeded = true;
   c->have_green = true;
   c->green_eta = c->eta_seed;
@@ -885,6 +922,12 @@ int scba_step(ScbaCtx* c, qcl_scba_row* row) {
   c->green_eta = 0.0;
   c->have_residual = true;
   QCL_CUDA_CHECK(cudaStreamSynchronize(c->st));
+  if (c->telemetry)
+    for (int i = 0; i < kPhases; ++i) {
+      float ms = 0;
+      QCL_CUDA_CHECK(cudaEventElapsedTime(&ms, c->pev[i], c->pev[i + 1]));
+      c->phase_ms[i] = ms;
+    }
   int hst[2];
   QCL_CUDA_CHECK(cudaMemcpy(hst, c->status, sizeof(hst), cudaMemcpyDeviceToHost));
   const double* h = c->scal_h;
@@ -1166,6 +1209,31 @@ int scba_mixer_info(ScbaCtx* c, qcl_anderson_info* out) {
 
 int scba_set_graph(ScbaCtx* c, int enable) {
   c->use_graph = enable != 0;
+  return QCL_OK;
+}
+
+// Phase telemetry on / off; captured graphs are rebuilt (they hold the marks or not).
+int scba_set_telemetry(ScbaCtx* c, int enable) {
+  QCL_CUDA_CHECK(cudaStreamSynchronize(c->st));
+  if (enable && !c->pev[0])
+    for (auto& e : c->pev) QCL_CUDA_CHECK(cudaEventCreate(&e));
+  c->telemetry = enable != 0;
+  for (int g = 0; g < 2; ++g)
+    if (c->graph[g]) {
+      cudaGraphExecDestroy(c->graph[g]);
+      c->graph[g] = nullptr;
+    }
+  return QCL_OK;
+}
+
+int scba_phase_times(ScbaCtx* c, double* ms, double* init_ms) {
+  if (!c->telemetry) {
+    set_last_error("phase_times: telemetry is off");
+    return QCL_ARG;
+  }
+  if (ms)
+    for (int i = 0; i < kPhases; ++i) ms[i] = c->phase_ms[i];
+  if (init_ms) *init_ms = c->init_ms;
   return QCL_OK;
 }
 

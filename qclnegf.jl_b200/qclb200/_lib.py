@@ -157,6 +157,8 @@ def _declare(l):
         "qcl_scba_retarget": (I, [P, D, D, D, P, P]),
         "qcl_scba_estimate_memory": (I, [P, P, P]),
         "qcl_scba_promote": (I, [P]),
+        "qcl_scba_use_telemetry": (I, [P, I]),
+        "qcl_scba_phase_times": (I, [P, P, P]),
         "qcl_last_singular_pivot": (I, []),
         "qcl_scba_mixer_info": (I, [P, P]),
         "qcl_anderson_guard": (I, [I, I, I, I, I, P, P, P]),

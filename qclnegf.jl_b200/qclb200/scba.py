@@ -48,6 +48,11 @@ class AndersonInfo(ctypes.Structure):
 
 RESET_REASONS = ("none", "residual_increase", "coefficient_solve", "coefficient_bound", "causality_guard")
 
+# The per-iteration phases of solve_scba_production (production_solver.jl:438-590,
+# production_iteration.jl:1-65), in the order qcl_scba_phase_times reports them.
+PHASES = ("dyson", "candidate_scattering", "candidate_embedding", "candidate_assembly", "residuals", "observables",
+          "mixing")
+
 
 # AlgorithmOptions model switches -> the C ABI's 0/1 codes (_check_algorithm_options,
 # algorithm_options.jl:42-93, rejects any other symbol with an ArgumentError)
@@ -94,11 +99,12 @@ class ProductionSCBA:
     like the reference's plans, fft_parallel.jl:16-17)."""
 
     def __init__(self, problem, precision="c128", verify_roundoff=True, use_graph=False, refinement=False,
-                 memory_budget_bytes=0):
+                 memory_budget_bytes=0, telemetry=False):
         """refinement: a reduced-precision context that can finish in FP64
         (``promote``); memory_budget_bytes: the preflight budget (0 = the
         device's free memory); a context above it raises MemoryBudgetError
-        before any allocation."""
+        before any allocation; telemetry: per-phase device times in every
+        row (``phase_ms``) and ``initialization_ms`` after the seed."""
         self.problem = problem
         self.precision = _prec(precision)
         self._p, self._marr = self._structs(problem, verify_roundoff, refinement, memory_budget_bytes)
@@ -107,7 +113,20 @@ class ProductionSCBA:
         self._h = h
         if use_graph:
             check(lib().qcl_scba_use_graph(self._h, 1))
+        self.telemetry = bool(telemetry)
+        if telemetry:
+            check(lib().qcl_scba_use_telemetry(self._h, 1))
         self.mu = None
+        self.initialization_ms = None
+
+    def phase_times(self):
+        """{phase: device ms} of the last step, and the seed's
+        :initialization time (the phase_begin / phase_end pairs of
+        production_telemetry.jl:81-200)."""
+        ms = np.zeros(len(PHASES))
+        init = ctypes.c_double()
+        check(lib().qcl_scba_phase_times(self._h, ctypes.c_void_p(ms.ctypes.data), ctypes.byref(init)))
+        return dict(zip(PHASES, ms.tolist())), init.value
 
     def _structs(self, problem, verify_roundoff, refinement, memory_budget_bytes):
         pr = problem
@@ -145,6 +164,8 @@ class ProductionSCBA:
         mu = ctypes.c_double()
         check(lib().qcl_scba_seed(self._h, ctypes.byref(mu)))
         self.mu = mu.value
+        if self.telemetry:
+            self.initialization_ms = self.phase_times()[1]
         return self.mu
 
     def step(self):
@@ -152,6 +173,8 @@ class ProductionSCBA:
         check(lib().qcl_scba_step(self._h, ctypes.byref(r)))
         d = r.as_dict()
         d["populations"] = self.populations()
+        if self.telemetry:
+            d["phase_ms"] = self.phase_times()[0]
         return d
 
     def run(self, iterations, tol_sigma=-1.0):

@@ -139,3 +139,34 @@ def test_refined_mixed_run_reaches_the_fp64_fixed_point(gpu_ops):
     assert len(rr) < len(rf)  # the FP64 phase starts from the mixed fixed point
     f.close()
     m.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("use_graph", [False, True])
+def test_phase_telemetry_times_every_phase(gpu_ops, use_graph):
+    """Per-phase device times under the reference's phase names
+    (production_telemetry.jl:81-200): every phase has a non-negative time,
+    their sum is within the step's wall time, and telemetry leaves the
+    iteration's results unchanged."""
+    import time
+
+    from qclb200.problem import small_problem
+    from qclb200.scba import PHASES, ProductionSCBA
+
+    pr = small_problem(NE=41, Nk=3, Nb=4, mechanisms=("LO", "acoustic", "IFR"))
+    a = ProductionSCBA(pr, precision="c128", use_graph=use_graph, telemetry=True)
+    b = ProductionSCBA(pr, precision="c128", use_graph=use_graph)
+    a.seed()
+    b.seed()
+    assert a.initialization_ms is not None and a.initialization_ms > 0
+    for _ in range(3):
+        t = time.perf_counter()
+        ra = a.step()
+        wall_ms = (time.perf_counter() - t) * 1e3
+        rb = b.step()
+        assert set(ra["phase_ms"]) == set(PHASES)
+        assert all(v >= 0 for v in ra["phase_ms"].values())
+        assert sum(ra["phase_ms"].values()) <= wall_ms
+        assert ra["J"] == rb["J"] and ra["r_Sigma"] == rb["r_Sigma"]
+    a.close()
+    b.close()

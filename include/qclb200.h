@@ -489,6 +489,14 @@ int qcl_scba_green_state(qcl_scba* ctx, void* A, double* kappa, double* scale);
  * step or seed. */
 int qcl_scba_witness(qcl_scba* ctx, qcl_psd_witness* witness);
 
+/* Test hook (no counterpart in the reference): the number of polling rounds
+ * after which a main-loop wait of the tensor-core contraction kernel gives up
+ * on the current device (0: at once; negative: the default, about 1 s).  A
+ * wait that gives up records QCL_TIMEOUT in the call's status; the kernel then
+ * waits with the full limit for its copies and MMAs in flight, frees its
+ * tensor memory and returns, so the context stays usable. */
+int qcl_debug_set_wait_limit(long long rounds);
+
 #ifdef __cplusplus
 }
 #endif

@@ -765,6 +765,8 @@ int qcl_scba_phase_times(qcl_scba* ctx, double* ms, double* initialization_ms) {
   return scba_phase_times((ScbaCtx*)ctx, ms, initialization_ms);
 }
 
+int qcl_debug_set_wait_limit(long long rounds) { return tc_set_wait_limit(rounds); }
+
 int qcl_scba_promote(qcl_scba* ctx) {
   if (!ctx) {
     set_last_error("ctx is required");

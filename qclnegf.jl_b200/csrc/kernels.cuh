@@ -124,6 +124,7 @@ int tc_build_operator2(int Nout, int Kc, int Nk, const void* Mop_c64, const doub
 size_t tc_a_work_floats(int NE, int Nc);
 size_t tc_a_work_floats2(int M, int Kc);
 size_t tc_operator_bytes(int Nout, int Kc);
+int tc_set_wait_limit(long long rounds);
 int launch_tc_contraction2(int M, int Nout, int Kc, const void* Bop, const void* A, void* S, double alpha,
                            double beta, float* awork, int* status, cudaStream_t st);
 int launch_tc_dense_contraction(int NE, int Nc, const void* Bop, const void* G, void* S, double alpha, double beta,

@@ -62,6 +62,10 @@ template <int BN> struct TcShape {
   static constexpr int LDW = CH % 32 == 0 ? 32 : 16;  // tensor-memory load width
 };
 constexpr long long TC_WAIT_LIMIT = 1ll << 22;  // try_wait rounds (~1 s) before a wait gives up
+// Rounds of the main-loop waits (producer, MMA issuer, accumulator drain).  The
+// waits after a failure (in-flight copies and MMAs) always use TC_WAIT_LIMIT.
+// qcl_debug_set_wait_limit lowers it so that a test can take the timeout path.
+__device__ long long g_tc_main_wait_limit = TC_WAIT_LIMIT;
 
 // UMMA shared-memory descriptor, K-major, 64-byte swizzle (the layout TMA
 // writes with CU_TENSOR_MAP_SWIZZLE_64B): start address (>> 4), leading byte
@@ -88,8 +92,8 @@ __device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
 }
 // Bounded parity wait; returns false if it gave up.
-__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
-  for (long long i = 0; i < TC_WAIT_LIMIT; ++i) {
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, long long limit = TC_WAIT_LIMIT) {
+  for (long long i = 0; i < limit; ++i) {
     uint32_t done;
     asm volatile(
         "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
@@ -182,6 +186,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) tc_gemm_kernel(const __grid_con
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int nkb = p.Kpad / TC_BK;
   const int nch = (nkb + TC_ACC_KB - 1) / TC_ACC_KB;
+  const long long lim = g_tc_main_wait_limit;
   if (threadIdx.x == 0) {
     for (int i = 0; i < TC_STAGES; ++i) {
       mbar_init(full + 8 * i, 1);
@@ -205,14 +210,14 @@ __global__ void __launch_bounds__(TC_THREADS, 1) tc_gemm_kernel(const __grid_con
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const uint32_t tmem = *tmem_slot;
   int issued = 0;  // MMA warp: blocks whose MMAs were issued and committed
+  int loaded = 0;  // producer: blocks whose TMA copies were issued
 
   if (warp == TC_DRAIN_WARPS) {
     // ---- producer ---------------------------------------------------------
     if (lane == 0) {
-      int loaded = 0;
       for (int kb = 0; kb < nkb && !s_fail; ++kb) {
         const int s = kb % TC_STAGES;
-        if (kb >= TC_STAGES && !mbar_wait(empty + 8 * s, (uint32_t)((kb / TC_STAGES - 1) & 1))) {
+        if (kb >= TC_STAGES && !mbar_wait(empty + 8 * s, (uint32_t)((kb / TC_STAGES - 1) & 1), lim)) {
           s_fail = 1;
           break;
         }
@@ -224,11 +229,6 @@ __global__ void __launch_bounds__(TC_THREADS, 1) tc_gemm_kernel(const __grid_con
         tma_load(st + 2 * TC_A_BYTES, &maps.bhi, kb * TC_BK, n0, full + 8 * s);
         tma_load(st + 2 * TC_A_BYTES + TC_B_BYTES, &maps.blo, kb * TC_BK, n0, full + 8 * s);
       }
-      // after a failure, let the copies in flight land (bounded) before the CTA ends
-      if (s_fail && loaded > 0) {
-        const int kl = loaded - 1;
-        mbar_wait(full + 8 * (kl % TC_STAGES), (uint32_t)((kl / TC_STAGES) & 1));
-      }
     }
   } else if (warp == TC_DRAIN_WARPS + 1) {
     // ---- MMA issue --------------------------------------------------------
@@ -236,8 +236,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1) tc_gemm_kernel(const __grid_con
       for (int kb = 0; kb < nkb && !s_fail; ++kb) {
         const int s = kb % TC_STAGES, ch = kb / TC_ACC_KB, b = ch & 1;
         const bool first = kb % TC_ACC_KB == 0, last = (kb % TC_ACC_KB == TC_ACC_KB - 1) || kb == nkb - 1;
-        if (!mbar_wait(full + 8 * s, (uint32_t)((kb / TC_STAGES) & 1)) ||
-            (first && ch >= 2 && !mbar_wait(acc_empty + 8 * b, (uint32_t)(((ch - 2) >> 1) & 1)))) {
+        if (!mbar_wait(full + 8 * s, (uint32_t)((kb / TC_STAGES) & 1), lim) ||
+            (first && ch >= 2 && !mbar_wait(acc_empty + 8 * b, (uint32_t)(((ch - 2) >> 1) & 1), lim))) {
           s_fail = 1;
           break;
         }
@@ -278,7 +278,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) tc_gemm_kernel(const __grid_con
       const int b = ch & 1;
       // warp-uniform decision: the tensor-memory loads below are .sync.aligned
       const bool stop = __any_sync(0xffffffffu, s_fail != 0);
-      const bool got = __all_sync(0xffffffffu, !stop && mbar_wait(acc_full + 8 * b, (uint32_t)((ch >> 1) & 1)));
+      const bool got = __all_sync(0xffffffffu, !stop && mbar_wait(acc_full + 8 * b, (uint32_t)((ch >> 1) & 1), lim));
       if (!got) {
         ok = false;
         s_fail = 1;
@@ -336,6 +336,14 @@ __global__ void __launch_bounds__(TC_THREADS, 1) tc_gemm_kernel(const __grid_con
   if (threadIdx.x == 0 && s_fail) record_status(p.status, QCL_TIMEOUT, (long long)blockIdx.x + 65536ll * blockIdx.y);
   if (warp == TC_DRAIN_WARPS + 1)
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TC_TMEM_COLS) : "memory");
+  // After a failure (s_fail is final past the barrier above) copies may still be
+  // in flight into this CTA's shared memory: the producer waits (full limit) for
+  // the last TC_STAGES loads, one per stage at its latest phase, before the CTA
+  // ends (a phase the MMA warp already consumed has completed: its wait returns
+  // at once).  Without a failure every load was consumed by an MMA.
+  if (warp == TC_DRAIN_WARPS && lane == 0 && s_fail)
+    for (int kl = loaded > TC_STAGES ? loaded - TC_STAGES : 0; kl < loaded; ++kl)
+      mbar_wait(full + 8 * (kl % TC_STAGES), (uint32_t)((kl / TC_STAGES) & 1));
 }
 
 // ---------------------------------------------------------------------------
@@ -620,6 +628,15 @@ int launch_tc_contraction2(int M, int Nout, int Kc, const void* Bop, const void*
   TcArgs a{M, 2 * Nout, Kpad, (Cx<float>*)S, M, alpha, beta, ainv, (const float*)b, status};
   if (bn == 224) return launch_tc_t<224>(maps, a, mtiles, st);
   return launch_tc_t<256>(maps, a, mtiles, st);
+}
+
+// Sets the main-loop wait limit of the tensor-core kernels on the current
+// device (rounds of mbarrier.try_wait; 0 makes every main-loop wait give up at
+// once; a negative value restores the default).
+int tc_set_wait_limit(long long rounds) {
+  const long long v = rounds >= 0 ? rounds : TC_WAIT_LIMIT;
+  QCL_CUDA_CHECK(cudaMemcpyToSymbol(g_tc_main_wait_limit, &v, sizeof(v)));
+  return QCL_OK;
 }
 
 int launch_tc_dense_contraction(int NE, int Nc, const void* Bop, const void* G, void* S, double alpha, double beta,

@@ -489,6 +489,26 @@ int qcl_scba_green_state(qcl_scba* ctx, void* A, double* kappa, double* scale);
  * step or seed. */
 int qcl_scba_witness(qcl_scba* ctx, qcl_psd_witness* witness);
 
+/* Autotuner (the reference sets the analogous execution knobs by hand:
+ * ProductionOptions.energy_chunk / hilbert_columns / worker_count,
+ * numerics/optimized/production_contracts.jl:143-165).  qcl_autotune times
+ * every compiled CTA shape of the Dyson + Keldysh kernel -- the number of
+ * (E, k) blocks per CTA, which sets threads, shared memory and registers per
+ * CTA -- for one basis class (N_b padded to 8, 16, 24, 32 or 48) and
+ * precision on a synthetic NE x Nk batch; every later Dyson launch of that
+ * class in the process uses the fastest.  qcl_autotune_reset restores the
+ * built-in choices; qcl_tuned_dyson_bpc reports the one in use. */
+typedef struct qcl_tune_result {
+  int dyson_bpc;   /* chosen blocks per CTA */
+  int default_bpc; /* the built-in choice */
+  int candidates;  /* number of candidates timed */
+  int bpc[4];      /* the candidates */
+  float ms[4];     /* mean device time per launch of each candidate */
+} qcl_tune_result;
+int qcl_autotune(int precision, int Nb, int NE, int Nk, qcl_tune_result* out);
+int qcl_autotune_reset(void);
+int qcl_tuned_dyson_bpc(int precision, int Nb);
+
 /* Test hook (no counterpart in the reference): the number of polling rounds
  * after which a main-loop wait of the tensor-core contraction kernel gives up
  * on the current device (0: at once; negative: the default, about 1 s).  A

@@ -18,6 +18,8 @@
 // shared-memory tiled matmuls with TRxTC register tiles per thread.  Shared
 // memory rows are XOR-swizzled on the low three column bits so that column
 // walks hit distinct banks.
+#include <mutex>
+
 #include "blockmat.cuh"
 
 namespace qcl {
@@ -356,15 +358,93 @@ int padded_size(int N) {
   return 0;
 }
 
+// ---------------------------------------------------------------------------
+// CTA shape: blocks per CTA (BPC).  Each padded size has a few compiled
+// candidates (the search space of the autotuner, autotune_dyson in
+// autotune.cu); the default is the measured choice of the operator batch,
+// and a tuned choice per (precision, padded size) replaces it once the
+// autotuner has run.
+// ---------------------------------------------------------------------------
+static int np_index(int NP) { return NP == 8 ? 0 : NP == 16 ? 1 : NP == 24 ? 2 : NP == 32 ? 3 : NP == 48 ? 4 : -1; }
+static int prec_index(int precision) { return precision == QCL_C128 ? 0 : precision == QCL_MIXED ? 1 : 2; }
+static int g_tuned_bpc[3][5] = {};  // 0: not tuned
+static std::mutex g_tune_mutex;
+
+int dyson_bpc_candidates(int NP, int* out) {
+  static const int c8[] = {8, 16, 32}, c16[] = {2, 4, 8}, c24[] = {1, 2, 4}, c32[] = {1, 2}, c48[] = {1, 2};
+  const int* c = nullptr;
+  int n = 0;
+  switch (NP) {
+    case 8: c = c8; n = 3; break;
+    case 16: c = c16; n = 3; break;
+    case 24: c = c24; n = 3; break;
+    case 32: c = c32; n = 2; break;
+    case 48: c = c48; n = 2; break;
+    default: return 0;
+  }
+  for (int i = 0; i < n; ++i) out[i] = c[i];
+  return n;
+}
+
+int dyson_default_bpc(int precision, int NP) {
+  const bool wide = precision == QCL_C128;  // FP64 storage: half the blocks per CTA
+  switch (NP) {
+    case 8: return 16;
+    case 16: return wide ? 4 : 8;
+    case 24: return wide ? 2 : 4;
+    case 32: return wide ? 1 : 2;
+    case 48: return 1;
+    default: return 0;
+  }
+}
+
+int dyson_bpc(int precision, int NP) {
+  std::lock_guard<std::mutex> lock(g_tune_mutex);
+  const int i = np_index(NP);
+  if (i < 0) return 0;
+  const int t = g_tuned_bpc[prec_index(precision)][i];
+  return t ? t : dyson_default_bpc(precision, NP);
+}
+
+void dyson_set_bpc(int precision, int NP, int bpc) {
+  std::lock_guard<std::mutex> lock(g_tune_mutex);
+  const int i = np_index(NP);
+  if (i >= 0) g_tuned_bpc[prec_index(precision)][i] = bpc;
+}
+
+template <typename RS, typename RL, typename RM, int NP>
+static int launch_dyson_np(const DysonArgs<RS>& a, int bpc, cudaStream_t st) {
+  if constexpr (NP == 8) {
+    if (bpc == 8) return launch_dyson_t<RS, RL, RM, 8, 8>(a, st);
+    if (bpc == 32) return launch_dyson_t<RS, RL, RM, 8, 32>(a, st);
+    return launch_dyson_t<RS, RL, RM, 8, 16>(a, st);
+  } else if constexpr (NP == 16) {
+    if (bpc == 2) return launch_dyson_t<RS, RL, RM, 16, 2>(a, st);
+    if (bpc == 8) return launch_dyson_t<RS, RL, RM, 16, 8>(a, st);
+    return launch_dyson_t<RS, RL, RM, 16, 4>(a, st);
+  } else if constexpr (NP == 24) {
+    if (bpc == 1) return launch_dyson_t<RS, RL, RM, 24, 1>(a, st);
+    if (bpc == 4) return launch_dyson_t<RS, RL, RM, 24, 4>(a, st);
+    return launch_dyson_t<RS, RL, RM, 24, 2>(a, st);
+  } else if constexpr (NP == 32) {
+    if (bpc == 2) return launch_dyson_t<RS, RL, RM, 32, 2>(a, st);
+    return launch_dyson_t<RS, RL, RM, 32, 1>(a, st);
+  } else {
+    if (bpc == 2) return launch_dyson_t<RS, RL, RM, 48, 2>(a, st);
+    return launch_dyson_t<RS, RL, RM, 48, 1>(a, st);
+  }
+}
+
 template <typename RS, typename RL, typename RM>
-static int launch_dyson_prec(const DysonArgs<RS>& a, cudaStream_t st) {
-  constexpr bool wide = sizeof(RS) == 8;  // FP64 storage: half the blocks per CTA
-  switch (padded_size(a.N)) {
-    case 8: return launch_dyson_t<RS, RL, RM, 8, 16>(a, st);
-    case 16: return launch_dyson_t<RS, RL, RM, 16, wide ? 4 : 8>(a, st);
-    case 24: return launch_dyson_t<RS, RL, RM, 24, wide ? 2 : 4>(a, st);
-    case 32: return launch_dyson_t<RS, RL, RM, 32, wide ? 1 : 2>(a, st);
-    case 48: return launch_dyson_t<RS, RL, RM, 48, 1>(a, st);
+static int launch_dyson_prec(const DysonArgs<RS>& a, int precision, int bpc_override, cudaStream_t st) {
+  const int NP = padded_size(a.N);
+  const int bpc = bpc_override > 0 ? bpc_override : dyson_bpc(precision, NP);
+  switch (NP) {
+    case 8: return launch_dyson_np<RS, RL, RM, 8>(a, bpc, st);
+    case 16: return launch_dyson_np<RS, RL, RM, 16>(a, bpc, st);
+    case 24: return launch_dyson_np<RS, RL, RM, 24>(a, bpc, st);
+    case 32: return launch_dyson_np<RS, RL, RM, 32>(a, bpc, st);
+    case 48: return launch_dyson_np<RS, RL, RM, 48>(a, bpc, st);
     default:
       set_last_error("basis size N_b=%d exceeds the supported maximum 48", a.N);
       return QCL_UNSUPPORTED;
@@ -375,6 +455,14 @@ int launch_dyson_keldysh(int precision, int NE, int Nk, int N, const double* eps
                          const void* sigR, const void* sigL, const void* sigG, void* GR, void* GL, void* GG,
                          double* scale, void* traceL, void* traceG, int* status, cudaStream_t st, int m0,
                          int mcount) {
+  return launch_dyson_keldysh_bpc(precision, NE, Nk, N, eps, eta, h, sigR, sigL, sigG, GR, GL, GG, scale, traceL,
+                                  traceG, status, st, m0, mcount, 0);
+}
+
+int launch_dyson_keldysh_bpc(int precision, int NE, int Nk, int N, const double* eps, double eta, const void* h,
+                             const void* sigR, const void* sigL, const void* sigG, void* GR, void* GL, void* GG,
+                             double* scale, void* traceL, void* traceG, int* status, cudaStream_t st, int m0,
+                             int mcount, int bpc) {
   if (mcount < 0) mcount = Nk - m0;
   if (m0 < 0 || mcount <= 0 || m0 + mcount > Nk) {
     set_last_error("dyson_keldysh: momentum slab [%d, %d) outside [0, %d)", m0, m0 + mcount, Nk);
@@ -388,13 +476,13 @@ int launch_dyson_keldysh(int precision, int NE, int Nk, int N, const double* eps
     DysonArgs<double> a{NE, Nk, N, m0, eps, eta, (const Cx<double>*)h, (const Cx<double>*)sigR,
                         (const Cx<double>*)sigL, (const Cx<double>*)sigG, (Cx<double>*)GR, (Cx<double>*)GL,
                         (Cx<double>*)GG, scale, (Cx<double>*)traceL, (Cx<double>*)traceG, status, mcount};
-    return launch_dyson_prec<double, double, double>(a, st);
+    return launch_dyson_prec<double, double, double>(a, precision, bpc, st);
   }
   DysonArgs<float> a{NE, Nk, N, m0, eps, eta, (const Cx<double>*)h, (const Cx<float>*)sigR,
                      (const Cx<float>*)sigL, (const Cx<float>*)sigG, (Cx<float>*)GR, (Cx<float>*)GL,
                      (Cx<float>*)GG, scale, (Cx<double>*)traceL, (Cx<double>*)traceG, status, mcount};
-  if (precision == QCL_MIXED) return launch_dyson_prec<float, double, float>(a, st);
-  if (precision == QCL_C64) return launch_dyson_prec<float, float, float>(a, st);
+  if (precision == QCL_MIXED) return launch_dyson_prec<float, double, float>(a, precision, bpc, st);
+  if (precision == QCL_C64) return launch_dyson_prec<float, float, float>(a, precision, bpc, st);
   set_last_error("unknown precision %d", precision);
   return QCL_ARG;
 }

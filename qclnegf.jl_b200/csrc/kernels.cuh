@@ -12,6 +12,16 @@ int launch_dyson_keldysh(int precision, int NE, int Nk, int N, const double* eps
                          double* scale, void* traceL, void* traceG, int* status, cudaStream_t st, int m0 = 0,
                          int mcount = -1);
 
+int launch_dyson_keldysh_bpc(int precision, int NE, int Nk, int N, const double* eps, double eta, const void* h,
+                             const void* sigR, const void* sigL, const void* sigG, void* GR, void* GL, void* GG,
+                             double* scale, void* traceL, void* traceG, int* status, cudaStream_t st, int m0,
+                             int mcount, int bpc);
+// Dyson CTA shapes (blocks per CTA): candidates, default, current (tuned or default), set
+int dyson_bpc_candidates(int NP, int* out);
+int dyson_default_bpc(int precision, int NP);
+int dyson_bpc(int precision, int NP);
+void dyson_set_bpc(int precision, int NP, int bpc);
+
 int launch_weighted_trace(int NE, int Nk, const void* tr, const double* wE, const double* wk, double* partial,
                           double* out, cudaStream_t st);
 int launch_paired_coefficients(const double* trL, const double* trG, int gs, double target, double* coeffs,

@@ -161,6 +161,9 @@ def _declare(l):
         "qcl_scba_phase_times": (I, [P, P, P]),
         "qcl_last_singular_pivot": (I, []),
         "qcl_debug_set_wait_limit": (I, [ctypes.c_longlong]),
+        "qcl_autotune": (I, [I, I, I, I, P]),
+        "qcl_autotune_reset": (I, []),
+        "qcl_tuned_dyson_bpc": (I, [I, I]),
         "qcl_scba_mixer_info": (I, [P, P]),
         "qcl_anderson_guard": (I, [I, I, I, I, I, P, P, P]),
         "qcl_scba_density_matrix": (I, [P, P]),

@@ -323,3 +323,28 @@ def hermitian_eigvals(H):
     vals = np.zeros((stack.shape[0], n))
     check(lib().qcl_hermitian_eigvals(n, stack.shape[0], _ptr(cm), _ptr(vals)))
     return np.sort(vals, axis=1).reshape(H.shape[:-1])
+
+
+class TuneResult(ctypes.Structure):
+    _fields_ = [("dyson_bpc", ctypes.c_int), ("default_bpc", ctypes.c_int), ("candidates", ctypes.c_int),
+                ("bpc", ctypes.c_int * 4), ("ms", ctypes.c_float * 4)]
+
+
+def autotune(Nb, *, precision="c128", NE=1024, Nk=8):
+    """qcl_autotune: time every compiled CTA shape (blocks per CTA) of the
+    Dyson + Keldysh kernel for the basis class of Nb on a synthetic NE x Nk
+    batch; later launches of that class in this process use the fastest.
+    Returns {"chosen", "default", "ms": {bpc: ms}}."""
+    r = TuneResult()
+    check(lib().qcl_autotune(_prec(precision), int(Nb), int(NE), int(Nk), ctypes.byref(r)))
+    return {"chosen": r.dyson_bpc, "default": r.default_bpc,
+            "ms": {int(r.bpc[i]): float(r.ms[i]) for i in range(r.candidates)}}
+
+
+def autotune_reset():
+    """Restore the built-in CTA shapes."""
+    check(lib().qcl_autotune_reset())
+
+
+def tuned_dyson_bpc(Nb, *, precision="c128"):
+    return int(lib().qcl_tuned_dyson_bpc(_prec(precision), int(Nb)))

@@ -199,4 +199,4 @@ def test_scba_with_separable_operators_matches_dense_oracle(gpu_ops, orc, precis
     solver.close()
     for ro, rg in zip(hist_o, hist_g):
         assert abs(rg["J"] - ro["J"]) <= tol * abs(ro["J"])
-        assert abs(rg["r_Sigma"] - ro["r_Sigma"]) <= max(tol, 1e-6) * abs(ro["r_Sigma"]) + 1e-12
+        assert abs(rg["r_Sigma"] - ro["rSigma"]) <= max(tol, 1e-6) * abs(ro["rSigma"]) + 1e-12

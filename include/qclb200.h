@@ -489,6 +489,29 @@ int qcl_scba_green_state(qcl_scba* ctx, void* A, double* kappa, double* scale);
  * step or seed. */
 int qcl_scba_witness(qcl_scba* ctx, qcl_psd_witness* witness);
 
+/* Batched sweep of independent operating points: a bias sweep, or points of
+ * different structures (basis sizes, energy grids).  The reference solves
+ * operating points one after another, re-using basis and kernels across
+ * biases (retarget_problem + retarget_production_cache, composition/
+ * operating_point.jl:25-170).  Here the points that fit the memory budget
+ * together (each point's qcl_scba_estimate_memory peak; 0 = the device's
+ * free memory) are resident at once, and one iteration of all resident
+ * points is one CUDA graph launch whose child graphs (the points' captured
+ * iterations) run concurrently.  A point leaves when r_Sigma <= tol_sigma, on
+ * a failure or non-finite row, or after max_iter steps, and the next pending
+ * point takes its memory.  qcl_sweep_create copies the problem and mechanism
+ * structs (not the arrays they point to, which must stay valid until
+ * qcl_sweep_run returns).  qcl_sweep_run fills, per point, its last row and
+ * its iteration count; stats (may be NULL) receives 5 doubles: wall seconds,
+ * total iterations, graph launches, largest number of resident points,
+ * parent-graph builds. */
+typedef struct qcl_sweep qcl_sweep;
+int qcl_sweep_create(int npoints, const qcl_scba_problem* problems, const qcl_mechanism* const* mechanisms,
+                     size_t memory_budget_bytes, qcl_sweep** out);
+int qcl_sweep_run(qcl_sweep* sweep, int max_iter, double tol_sigma, qcl_scba_row* last_rows, int* iterations,
+                  double* stats);
+void qcl_sweep_destroy(qcl_sweep* sweep);
+
 /* Autotuner (the reference sets the analogous execution knobs by hand:
  * ProductionOptions.energy_chunk / hilbert_columns / worker_count,
  * numerics/optimized/production_contracts.jl:143-165).  qcl_autotune times

@@ -147,6 +147,11 @@ int scba_witness(ScbaCtx* c, double* out12);
 int scba_retarget(ScbaCtx* c, double Ep, double N_LO, double kBT, const void* h, const double* q);
 int scba_estimate_memory(const qcl_scba_problem* p, const qcl_mechanism* mechs, size_t out[6]);
 int scba_promote(ScbaCtx* c);
+struct Sweep;
+int sweep_create(int n, const qcl_scba_problem* problems, const qcl_mechanism* const* mechanisms, size_t budget,
+                 Sweep** out);
+int sweep_run(Sweep* sw, int max_iter, double tol, qcl_scba_row* last, int* iters, double* stats);
+void sweep_destroy(Sweep* sw);
 int scba_set_telemetry(ScbaCtx* c, int enable);
 int scba_phase_times(ScbaCtx* c, double* ms, double* init_ms);
 int scba_mixer_info(ScbaCtx* c, qcl_anderson_info* out);
@@ -764,6 +769,26 @@ int qcl_scba_phase_times(qcl_scba* ctx, double* ms, double* initialization_ms) {
   }
   return scba_phase_times((ScbaCtx*)ctx, ms, initialization_ms);
 }
+
+int qcl_sweep_create(int npoints, const qcl_scba_problem* problems, const qcl_mechanism* const* mechanisms,
+                     size_t memory_budget_bytes, qcl_sweep** out) {
+  if (!out) {
+    set_last_error("out is required");
+    return QCL_ARG;
+  }
+  return sweep_create(npoints, problems, mechanisms, memory_budget_bytes, (Sweep**)out);
+}
+
+int qcl_sweep_run(qcl_sweep* sweep, int max_iter, double tol_sigma, qcl_scba_row* last_rows, int* iterations,
+                  double* stats) {
+  if (!sweep || !last_rows || !iterations || max_iter < 1) {
+    set_last_error("sweep, last_rows, iterations and max_iter >= 1 are required");
+    return QCL_ARG;
+  }
+  return sweep_run((Sweep*)sweep, max_iter, tol_sigma, last_rows, iterations, stats);
+}
+
+void qcl_sweep_destroy(qcl_sweep* sweep) { sweep_destroy((Sweep*)sweep); }
 
 int qcl_debug_set_wait_limit(long long rounds) { return tc_set_wait_limit(rounds); }
 

@@ -20,6 +20,8 @@
 #include <string.h>
 
 #include <algorithm>
+#include <chrono>
+#include <map>
 #include <vector>
 
 #include "kernels.cuh"
@@ -125,6 +127,7 @@ struct ScbaCtx {
   HilbertTables hil;
   // graph of one iteration (two parities: state/cand swap)
   cudaGraphExec_t graph[2] = {nullptr, nullptr};
+  cudaGraph_t gtpl[2] = {nullptr, nullptr};  // the captured iterations (child graphs of a batched sweep)
   cudaStream_t st2 = nullptr;  // side stream of an iteration (forked from st, joined back)
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   bool use_graph = false;
@@ -147,6 +150,8 @@ struct ScbaCtx {
 };
 
 static void* field_of(const std::vector<void*>& v, int f, int c) { return v[3 * f + c]; }
+int scba_step_launch(ScbaCtx* c, cudaGraph_t* child);
+int scba_step_finish(ScbaCtx* c, qcl_scba_row* row);
 
 static int dalloc(void** p, size_t bytes) {
   cudaError_t e = cudaMalloc(p, bytes > 0 ? bytes : 16);
@@ -219,6 +224,8 @@ void scba_destroy(ScbaCtx* c) {
   if (c->st) cudaStreamSynchronize(c->st);
   for (int g = 0; g < 2; ++g)
     if (c->graph[g]) cudaGraphExecDestroy(c->graph[g]);
+  for (int g = 0; g < 2; ++g)
+    if (c->gtpl[g]) cudaGraphDestroy(c->gtpl[g]);
   cudaFree(c->eps);
   cudaFree(c->wE);
   cudaFree(c->wk);
@@ -883,7 +890,23 @@ int scba_seed(ScbaCtx* c, double* mu_out) {
   return QCL_OK;
 }
 
-static int run_body(ScbaCtx* c) {
+// Drops the captured iteration graphs (they hold the context's current
+// scalars, precision and telemetry marks).
+static void drop_graphs(ScbaCtx* c) {
+  for (int g = 0; g < 2; ++g) {
+    if (c->graph[g]) cudaGraphExecDestroy(c->graph[g]);
+    if (c->gtpl[g]) cudaGraphDestroy(c->gtpl[g]);
+    c->graph[g] = nullptr;
+    c->gtpl[g] = nullptr;
+  }
+}
+
+// Enqueues one iteration.  With `child` non-null and a captured iteration
+// available, the iteration is not launched: *child receives its graph, for
+// the caller to launch as a node of a larger graph (a batched sweep);
+// otherwise *child is null and the iteration is on the context's stream.
+static int run_body(ScbaCtx* c, cudaGraph_t* child) {
+  if (child) *child = nullptr;
   std::vector<void*>& st = c->parity == 0 ? c->state : c->cand;
   std::vector<void*>& cd = c->parity == 0 ? c->cand : c->state;
   // graphs are captured once every kernel has been launched (and configured) eagerly
@@ -899,8 +922,15 @@ static int run_body(ScbaCtx* c) {
     }
     if (e != cudaSuccess) return cuda_status(e, "cudaStreamEndCapture");
     e = cudaGraphInstantiate(&c->graph[c->parity], g, 0);
-    cudaGraphDestroy(g);
-    if (e != cudaSuccess) return cuda_status(e, "cudaGraphInstantiate");
+    if (e != cudaSuccess) {
+      cudaGraphDestroy(g);
+      return cuda_status(e, "cudaGraphInstantiate");
+    }
+    c->gtpl[c->parity] = g;
+  }
+  if (child) {
+    *child = c->gtpl[c->parity];
+    return QCL_OK;
   }
   QCL_CUDA_CHECK(cudaGraphLaunch(c->graph[c->parity], c->st));
   return QCL_OK;
@@ -908,6 +938,14 @@ static int run_body(ScbaCtx* c) {
 
 // One SCBA iteration.  Commits the previous iteration's mixing first.
 int scba_step(ScbaCtx* c, qcl_scba_row* row) {
+  int s = scba_step_launch(c, nullptr);
+  if (s) return s;
+  return scba_step_finish(c, row);
+}
+
+// First half of a step: commit, then enqueue the iteration (or hand its
+// captured graph to the caller through `child`, see run_body).
+int scba_step_launch(ScbaCtx* c, cudaGraph_t* child) {
   if (!c->seeded) {
     set_last_error("scba_step before scba_seed");
     return QCL_ARG;
@@ -916,8 +954,14 @@ int scba_step(ScbaCtx* c, qcl_scba_row* row) {
     c->parity ^= 1;
     c->pending_commit = false;
   }
-  int s = run_body(c);
-  if (s) return s;
+  return run_body(c, child);
+}
+
+// Second half of a step: once the iteration has run (on the context's stream
+// or inside the caller's graph, whose stream the caller has synchronised),
+// read its scalars into the row and apply the reference's status handling.
+int scba_step_finish(ScbaCtx* c, qcl_scba_row* row) {
+  int s;
   c->have_green = true;
   c->green_eta = 0.0;
   c->have_residual = true;
@@ -1150,11 +1194,7 @@ int scba_retarget(ScbaCtx* c, double Ep, double N_LO, double kBT, const void* h,
   c->kBT = kBT;
   if (q)
     for (int i = 0; i < c->M; ++i) c->mech[i].q = q[i];
-  for (int g = 0; g < 2; ++g)
-    if (c->graph[g]) {
-      cudaGraphExecDestroy(c->graph[g]);
-      c->graph[g] = nullptr;
-    }
+  drop_graphs(c);
   c->pending_commit = false;  // keep the unmixed state of the last step
   c->nu = 0;
   c->Jprev = NAN;
@@ -1218,11 +1258,7 @@ int scba_set_telemetry(ScbaCtx* c, int enable) {
   if (enable && !c->pev[0])
     for (auto& e : c->pev) QCL_CUDA_CHECK(cudaEventCreate(&e));
   c->telemetry = enable != 0;
-  for (int g = 0; g < 2; ++g)
-    if (c->graph[g]) {
-      cudaGraphExecDestroy(c->graph[g]);
-      c->graph[g] = nullptr;
-    }
+  drop_graphs(c);
   return QCL_OK;
 }
 
@@ -1283,11 +1319,7 @@ int scba_promote(ScbaCtx* c) {
   c->fbytes = c->nfield * 16;
   if ((s = prepare_hilbert_tables(c->hil, c->NE, c->de, QCL_C128))) return s;
   if ((s = ensure_partial(c->hil, (long long)c->Nk * c->N * c->N))) return s;
-  for (int g = 0; g < 2; ++g)
-    if (c->graph[g]) {
-      cudaGraphExecDestroy(c->graph[g]);
-      c->graph[g] = nullptr;
-    }
+  drop_graphs(c);
   if (c->mixing && (s = launch_anderson_reset(c->ameta, c->st))) return s;
   c->have_green = false;
   c->have_residual = false;
@@ -1298,5 +1330,202 @@ int scba_promote(ScbaCtx* c) {
 int scba_precision(ScbaCtx* c) { return c->precision; }
 
 cudaStream_t scba_stream(ScbaCtx* c) { return c->st; }
+
+// ---------------------------------------------------------------------------
+// Batched sweep of independent operating points (bias points of a sweep,
+// structures of different sizes).  The reference solves operating points one
+// after another, re-using basis and kernels (retarget_problem +
+// retarget_production_cache, composition/operating_point.jl:25-170).  Here
+// every point is a context; the points that fit the memory budget together
+// (the preflight estimate of each) are resident at once, and one iteration of
+// all of them is ONE graph launch: a parent graph whose child nodes are the
+// points' captured iterations, which the GPU runs concurrently.  A point
+// leaves when it converges (r_Sigma <= tol), fails, or reaches max_iter; the
+// next pending point takes its memory.  The parent graph is rebuilt when the
+// resident set changes and otherwise alternates between the two parities.
+// ---------------------------------------------------------------------------
+struct SweepPoint {
+  qcl_scba_problem problem;
+  std::vector<qcl_mechanism> mechs;
+};
+
+struct Sweep {
+  std::vector<SweepPoint> points;
+  size_t budget = 0;
+  cudaStream_t st = nullptr;
+};
+
+void sweep_destroy(Sweep* sw) {
+  if (!sw) return;
+  if (sw->st) cudaStreamDestroy(sw->st);
+  delete sw;
+}
+
+int sweep_create(int n, const qcl_scba_problem* problems, const qcl_mechanism* const* mechanisms, size_t budget,
+                 Sweep** out) {
+  *out = nullptr;
+  if (n < 1 || !problems || !mechanisms) {
+    set_last_error("sweep: at least one point with its problem and mechanisms is required");
+    return QCL_ARG;
+  }
+  Sweep* sw = new Sweep();
+  sw->budget = budget;
+  for (int i = 0; i < n; ++i) {
+    SweepPoint pt;
+    pt.problem = problems[i];
+    if (pt.problem.nmech > 0 && !mechanisms[i]) {
+      sweep_destroy(sw);
+      set_last_error("sweep: point %d has no mechanism array", i);
+      return QCL_ARG;
+    }
+    pt.mechs.assign(mechanisms[i], mechanisms[i] + std::max(pt.problem.nmech, 0));
+    MemPlan mp;
+    int s = plan_memory(&pt.problem, pt.mechs.data(), &mp);
+    if (s) {
+      sweep_destroy(sw);
+      return s;
+    }
+    sw->points.push_back(pt);
+  }
+  cudaError_t e = cudaStreamCreateWithFlags(&sw->st, cudaStreamNonBlocking);
+  if (e != cudaSuccess) {
+    sweep_destroy(sw);
+    return cuda_status(e, "cudaStreamCreate (sweep)");
+  }
+  *out = sw;
+  return QCL_OK;
+}
+
+// stats: [0] wall seconds, [1] total iterations, [2] parent-graph launches,
+// [3] largest number of resident points, [4] parent-graph builds.
+int sweep_run(Sweep* sw, int max_iter, double tol, qcl_scba_row* last, int* iters, double* stats) {
+  const int n = (int)sw->points.size();
+  size_t budget = sw->budget;
+  if (budget == 0) {
+    size_t fr = 0, tot = 0;
+    QCL_CUDA_CHECK(cudaMemGetInfo(&fr, &tot));
+    budget = fr;
+  }
+  struct Active {
+    int idx;
+    ScbaCtx* ctx;
+    size_t bytes;
+  };
+  std::vector<Active> active;
+  std::vector<size_t> peak(n);
+  for (int i = 0; i < n; ++i) {
+    MemPlan mp;
+    plan_memory(&sw->points[i].problem, sw->points[i].mechs.data(), &mp);
+    peak[i] = mp.peak();
+    if (peak[i] > budget) {
+      set_last_error("sweep: point %d alone needs %zu bytes, over the budget %zu", i, peak[i], budget);
+      return QCL_NOMEM;
+    }
+    iters[i] = 0;
+    memset(&last[i], 0, sizeof(qcl_scba_row));
+  }
+  auto t0 = std::chrono::steady_clock::now();
+  double launches = 0, builds = 0, total_iters = 0, max_resident = 0;
+  int next = 0;
+  size_t used = 0;
+  std::map<std::vector<std::pair<void*, int>>, cudaGraphExec_t> parents;
+  auto clear_parents = [&]() {
+    for (auto& kv : parents) cudaGraphExecDestroy(kv.second);
+    parents.clear();
+  };
+  auto fail = [&](int s) {
+    clear_parents();
+    for (auto& a : active) scba_destroy(a.ctx);
+    return s;
+  };
+  while (next < n || !active.empty()) {
+    // admit pending points while they fit
+    bool changed = false;
+    while (next < n && used + peak[next] <= budget) {
+      qcl_scba_problem p = sw->points[next].problem;
+      p.memory_budget_bytes = budget - used;
+      ScbaCtx* c = nullptr;
+      int s = scba_create(&p, sw->points[next].mechs.data(), &c);
+      if (s) return fail(s);
+      c->use_graph = true;
+      if ((s = scba_seed(c, nullptr))) {
+        scba_destroy(c);
+        return fail(s);
+      }
+      active.push_back({next, c, peak[next]});
+      used += peak[next];
+      ++next;
+      changed = true;
+    }
+    if (changed) clear_parents();
+    max_resident = std::max(max_resident, (double)active.size());
+    // one iteration of every resident point
+    std::vector<cudaGraph_t> kids;
+    std::vector<std::pair<void*, int>> key;
+    for (auto& a : active) {
+      cudaGraph_t g = nullptr;
+      int s = scba_step_launch(a.ctx, &g);
+      if (s) return fail(s);
+      if (g) {
+        kids.push_back(g);
+        key.push_back({(void*)a.ctx, a.ctx->parity});
+      }
+    }
+    if (!kids.empty()) {
+      auto it = parents.find(key);
+      if (it == parents.end()) {
+        cudaGraph_t parent;
+        QCL_CUDA_CHECK(cudaGraphCreate(&parent, 0));
+        for (cudaGraph_t g : kids) {
+          cudaGraphNode_t node;
+          cudaError_t e = cudaGraphAddChildGraphNode(&node, parent, nullptr, 0, g);
+          if (e != cudaSuccess) {
+            cudaGraphDestroy(parent);
+            return fail(cuda_status(e, "cudaGraphAddChildGraphNode"));
+          }
+        }
+        cudaGraphExec_t ex;
+        cudaError_t e = cudaGraphInstantiate(&ex, parent, 0);
+        cudaGraphDestroy(parent);
+        if (e != cudaSuccess) return fail(cuda_status(e, "cudaGraphInstantiate (sweep)"));
+        it = parents.emplace(key, ex).first;
+        builds += 1;
+      }
+      cudaError_t e = cudaGraphLaunch(it->second, sw->st);
+      if (e == cudaSuccess) e = cudaStreamSynchronize(sw->st);
+      if (e != cudaSuccess) return fail(cuda_status(e, "sweep iteration"));
+      launches += 1;
+    }
+    // rows; converged, failed or exhausted points leave
+    std::vector<Active> keep;
+    for (auto& a : active) {
+      qcl_scba_row row;
+      int s = scba_step_finish(a.ctx, &row);
+      iters[a.idx] += 1;
+      total_iters += 1;
+      last[a.idx] = row;
+      const bool done = s != QCL_OK || row.status != QCL_OK || row.r_Sigma <= tol || iters[a.idx] >= max_iter;
+      if (s != QCL_OK) last[a.idx].status = s;
+      if (done) {
+        scba_destroy(a.ctx);
+        used -= a.bytes;
+        changed = true;
+      } else {
+        keep.push_back(a);
+      }
+    }
+    active.swap(keep);
+    if (changed) clear_parents();
+  }
+  clear_parents();
+  if (stats) {
+    stats[0] = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    stats[1] = total_iters;
+    stats[2] = launches;
+    stats[3] = max_resident;
+    stats[4] = builds;
+  }
+  return QCL_OK;
+}
 
 }  // namespace qcl

@@ -162,6 +162,9 @@ def _declare(l):
         "qcl_last_singular_pivot": (I, []),
         "qcl_debug_set_wait_limit": (I, [ctypes.c_longlong]),
         "qcl_autotune": (I, [I, I, I, I, P]),
+        "qcl_sweep_create": (I, [I, P, P, Z, P]),
+        "qcl_sweep_run": (I, [P, I, D, P, P, P]),
+        "qcl_sweep_destroy": (None, [P]),
         "qcl_autotune_reset": (I, []),
         "qcl_tuned_dyson_bpc": (I, [I, I]),
         "qcl_scba_mixer_info": (I, [P, P]),

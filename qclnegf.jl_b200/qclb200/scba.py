@@ -287,3 +287,54 @@ def solve_scba_production(problem, iterations, *, precision="c128", verify_round
     s = ProductionSCBA(problem, precision=precision, verify_roundoff=verify_roundoff, use_graph=use_graph)
     s.seed()
     return s.run(iterations, tol_sigma), s
+
+
+class BatchedSweep:
+    """A batched sweep of independent operating points (qcl_sweep_*): the
+    points that fit the memory budget together are resident at once and one
+    iteration of all of them is one CUDA graph launch (their captured
+    iterations as child graphs).  The reference solves a bias sweep point by
+    point, re-using basis and kernels (retarget_problem,
+    composition/operating_point.jl:25-170)."""
+
+    def __init__(self, problems, precision="mixed", verify_roundoff=True, memory_budget_bytes=0):
+        self.problems = list(problems)
+        self._holders = []
+        structs, mech_arrays = [], []
+        for pr in self.problems:
+            h = ProductionSCBA.__new__(ProductionSCBA)
+            h.precision = _prec(precision)
+            p, arr = h._structs(pr, verify_roundoff, False, 0)
+            self._holders.append((h, p, arr))
+            structs.append(p)
+            mech_arrays.append(arr)
+        n = len(structs)
+        self._parr = (_Problem * n)(*structs)
+        self._marr = (ctypes.c_void_p * n)(*[ctypes.cast(a, ctypes.c_void_p) if a is not None else None
+                                               for a in mech_arrays])
+        handle = ctypes.c_void_p()
+        check(lib().qcl_sweep_create(n, ctypes.byref(self._parr), ctypes.byref(self._marr),
+                                     int(memory_budget_bytes), ctypes.byref(handle)))
+        self._h = handle
+
+    def run(self, max_iter, tol_sigma=-1.0):
+        """Runs every point; returns (last rows, iteration counts, stats)."""
+        n = len(self.problems)
+        rows = (Row * n)()
+        iters = (ctypes.c_int * n)()
+        stats = (ctypes.c_double * 5)()
+        check(lib().qcl_sweep_run(self._h, int(max_iter), float(tol_sigma), ctypes.byref(rows), ctypes.byref(iters),
+                                  ctypes.byref(stats)))
+        st = dict(zip(("wall_s", "iterations", "graph_launches", "max_resident", "graph_builds"), list(stats)))
+        return [r.as_dict() for r in rows], list(iters), st
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().qcl_sweep_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

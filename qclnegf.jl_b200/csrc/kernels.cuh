@@ -195,5 +195,6 @@ int launch_residual_pair(int precision, size_t n, const void* o1, const void* o2
                          double* partial, double* out2, cudaStream_t st);
 int launch_convert(int precision, size_t n, const void* in_c128, void* out, cudaStream_t st);
 int launch_promote(size_t n, const void* in_c64, void* out_c128, cudaStream_t st);
+int launch_antihermitian_part(int NE, int Nk, int N, void* X, cudaStream_t st);
 
 }  // namespace qcl

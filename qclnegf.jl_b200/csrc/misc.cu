@@ -150,6 +150,36 @@ __global__ void promote_kernel(size_t n, const Cx<float>* __restrict__ in, Cx<do
   }
 }
 
+// X <- (X - X^H) / 2 per (e, m) block of a complex128 field, in place: one
+// thread per unordered pair (a <= b).
+__global__ void antihermitian_kernel(int NE, int Nk, int N, Cx<double>* X) {
+  const long long blocks = (long long)NE * Nk, pairs = (long long)N * (N + 1) / 2;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < blocks * pairs;
+       i += (long long)gridDim.x * blockDim.x) {
+    const long long blk = i % blocks;
+    int q = (int)(i / blocks), b = 0;
+    while (q >= N - b) {  // pair index -> (a, b), a >= b
+      q -= N - b;
+      ++b;
+    }
+    const int a = b + q;
+    Cx<double>* pab = X + blk + blocks * ((long long)a + (long long)N * b);
+    Cx<double>* pba = X + blk + blocks * ((long long)b + (long long)N * a);
+    const Cx<double> u = *pab, v = *pba;
+    // (X - X^H)_ab / 2 = (u - conj v) / 2, and (X - X^H)_ba = -conj of it
+    const Cx<double> w = cx<double>(0.5 * (u.x - v.x), 0.5 * (u.y + v.y));
+    *pab = w;
+    *pba = cx<double>(-w.x, w.y);
+  }
+}
+
+int launch_antihermitian_part(int NE, int Nk, int N, void* X, cudaStream_t st) {
+  const long long n = (long long)NE * Nk * N * (N + 1) / 2;
+  antihermitian_kernel<<<gcap(n, 256), 256, 0, st>>>(NE, Nk, N, (Cx<double>*)X);
+  QCL_LAUNCH_CHECK("antihermitian");
+  return QCL_OK;
+}
+
 int launch_promote(size_t n, const void* in_c64, void* out_c128, cudaStream_t st) {
   promote_kernel<<<gcap((long long)n, 256), 256, 0, st>>>(n, (const Cx<float>*)in_c64, (Cx<double>*)out_c128);
   QCL_LAUNCH_CHECK("promote");

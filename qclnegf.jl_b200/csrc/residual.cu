@@ -1159,7 +1159,10 @@ __global__ void __launch_bounds__(BPC* Tile<NP>::TT) anderson_guard_kernel(Guard
   if (p.pass == 1 && !p.meta->fallback) return;
   constexpr int TT = Tile<NP>::TT;
   constexpr size_t MSZ = (size_t)NP * NP;
-  constexpr double eps = 2.220446049250313e-16;
+  // unit roundoff of the storage precision: the budgets of the reference
+  // (64 n eps ||X||, production_mixing.jl:48-118) scaled to the fields that
+  // are actually stored (complex64 fields carry FP32 rounding in every entry)
+  constexpr double eps = sizeof(RS) == 8 ? 2.220446049250313e-16 : 1.1920928955078125e-07;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   Cx<double>* bR = reinterpret_cast<Cx<double>*>(smem_raw);
   Cx<double>* bL = bR + BPC * MSZ;

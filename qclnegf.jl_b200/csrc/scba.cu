@@ -703,7 +703,12 @@ static int current_green(ScbaCtx* c, const std::vector<void*>& fam) {
 // the iteration is captured into a graph).
 static int phase_mark(ScbaCtx* c, int i) {
   if (!c->telemetry) return QCL_OK;
-  QCL_CUDA_CHECK(cudaEventRecordWithFlags(c->pev[i], c->st, cudaEventRecordExternal));
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  QCL_CUDA_CHECK(cudaStreamIsCapturing(c->st, &cs));
+  if (cs == cudaStreamCaptureStatusActive)  // an event-record node of the captured iteration
+    QCL_CUDA_CHECK(cudaEventRecordWithFlags(c->pev[i], c->st, cudaEventRecordExternal));
+  else
+    QCL_CUDA_CHECK(cudaEventRecord(c->pev[i], c->st));
   return QCL_OK;
 }
 
@@ -1293,9 +1298,16 @@ int scba_promote(ScbaCtx* c) {
   }
   int s;
   std::vector<void*>& st = c->parity == 0 ? c->state : c->cand;
-  for (void*& f : st) {  // state field -> tmp (complex128), then swap the buffers
+  for (size_t i = 0; i < st.size(); ++i) {  // state field -> tmp (complex128), then swap the buffers
+    void*& f = st[i];
     if ((s = launch_promote(c->nfield, f, c->tmp, c->st))) return s;
     std::swap(f, c->tmp);
+    // Sigma< and Sigma> are anti-Hermitian (i times Hermitian) per block; the
+    // reduced-precision iterations computed the (a,b) and (b,a) entries apart,
+    // so they are only anti-Hermitian to FP32 rounding, which the FP64 checks
+    // of the iterations that follow (the realness of the number functional,
+    // 1e-10) would reject.  The promoted state keeps their anti-Hermitian part.
+    if (i % 3 != 0 && (s = launch_antihermitian_part(c->NE, c->Nk, c->N, f, c->st))) return s;
   }
   for (auto& m : c->mech) {
     auto swap_in = [](void*& cur, void*& keep) {

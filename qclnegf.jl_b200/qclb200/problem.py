@@ -461,7 +461,9 @@ def _period_basis(rng, periods, states, layers_nm, dz_nm=0.5):
 
 def full_physics_problem(seed: int = 11, NE: int = 2048, Nk: int = 64, periods: int = 4, states: int = 8,
                          Nqz: int = 401, Nphi: int = 64, lookup_nodes: int = 129, rtol: float = 1e-15,
-                         alpha: float = 0.5, bias_mV: float = 50.0) -> SCBAProblem:
+                         alpha: float = 0.5, bias_mV: float = 50.0,
+                         mechanisms=("LO", "acoustic", "impurity", "IFR", "alloy"),
+                         kernels=None) -> SCBAProblem:
     """Full-physics-shaped SCBA structure: a supercell of `periods` periods x
     `states` localised states (N_b = 32 by default) of the GaAs /
     Al0.15Ga0.85As stack 4.0 / 8.5 / 2.0 / 16.0 nm, N_E = 2048 energies over
@@ -482,7 +484,12 @@ def full_physics_problem(seed: int = 11, NE: int = 2048, Nk: int = 64, periods: 
 
     The basis functions, level scheme and couplings are synthetic and seeded;
     the kernels follow the reference formulas with these basis functions.
-    `rtol` is the compression tolerance of the separable sums."""
+    `rtol` is the compression tolerance of the separable sums.  `mechanisms`
+    selects the mechanisms (in the reference order); `kernels` (the
+    mechanism list of an earlier call with the same seed, structure and N_k)
+    is reused as is -- the kernels do not depend on the bias or the energy
+    grid, as retarget_problem keeps them (composition/operating_point.jl:
+    25-150)."""
     from .kernel_build import (impurity_pair_factors, lo_form_factors, lo_weights, lookup_weights,
                                separable_sum_operator, transfer_momenta)
 
@@ -505,18 +512,21 @@ def full_physics_problem(seed: int = 11, NE: int = 2048, Nk: int = 64, periods: 
     T_K = 100.0
     hw = 0.0367
     mechs = []
+    want = set(mechanisms)
     # LO: prefactor e^2 hbar w / (2 eps0) (1/eps_inf - 1/eps_s) L0 / K0 (kernels.jl:340-355)
     pre_lo = E_CHARGE ** 2 * hw * E_CHARGE / (2 * _EPS0) * (1 / _GAAS_EPS_INF - 1 / _GAAS_EPS_S) * L0 / K0
     qz = np.linspace(-10.0 * L0_NM, 10.0 * L0_NM, Nqz)
     wqz = np.full(Nqz, qz[1] - qz[0])
-    F = lo_form_factors(chi, x, wx, qz).reshape((Nqz, Nb * Nb), order="F")
-    W = lo_weights(kappa, Nphi, qz, wqz, qscreen=0.05 * L0_NM, prefactor=pre_lo)
-    mechs.append(separable_sum_operator("LO", W, F, rtol=rtol))
+    if kernels is None and "LO" in want:
+        F = lo_form_factors(chi, x, wx, qz).reshape((Nqz, Nb * Nb), order="F")
+        W = lo_weights(kappa, Nphi, qz, wqz, qscreen=0.05 * L0_NM, prefactor=pre_lo)
+        mechs.append(separable_sum_operator("LO", W, F, rtol=rtol))
     # acoustic: Xi^2 kB T / (rho v_s^2) / (L0 K0) sum_g w chi^4 (kernels.jl:262-283)
     pre_ac = (_GAAS_XI_EV * E_CHARGE) ** 2 * _KB_J * T_K / (_GAAS_RHO * _GAAS_VS ** 2) / L0 / K0
-    Kac = acoustic_block(chi, wx, pre_ac)
-    q = float(np.max(np.abs(Kac)))
-    mechs.append(Mechanism("acoustic", "momentum_independent", q, block=block_matrix(Kac / q)))
+    if kernels is None and "acoustic" in want:
+        Kac = acoustic_block(chi, wx, pre_ac)
+        q = float(np.max(np.abs(Kac)))
+        mechs.append(Mechanism("acoustic", "momentum_independent", q, block=block_matrix(Kac / q)))
     # impurity: 3e10 cm^-2 per period over the cells of each period's first (4 nm) layer
     Lp = sum(layers) / L0_NM
     doped = ((x % Lp) < layers[0] / L0_NM)
@@ -527,9 +537,10 @@ def full_physics_problem(seed: int = 11, NE: int = 2048, Nk: int = 64, periods: 
     qmax = float(transfer_momenta(kappa, Nphi).max())
     nodes = qmax * (np.arange(lookup_nodes) / (lookup_nodes - 1)) ** 2
     qs_imp = 0.1 * L0_NM
-    VD = [impurity_pair_factors(qn, chi, x, wx, donor_w, qs_imp, pre_imp) for qn in nodes]
-    mechs.append(separable_sum_operator("impurity", lookup_weights(nodes, kappa, Nphi), np.array([v for v, _ in VD]),
-                                        VD[0][1], rtol=rtol))
+    if kernels is None and "impurity" in want:
+        VD = [impurity_pair_factors(qn, chi, x, wx, donor_w, qs_imp, pre_imp) for qn in nodes]
+        mechs.append(separable_sum_operator("impurity", lookup_weights(nodes, kappa, Nphi),
+                                            np.array([v for v, _ in VD]), VD[0][1], rtol=rtol))
     # IFR: D_j[a,c] = dEc chi_a(z_j) chi_c(z_j); block = sum_j D_j (x) conj D_j; radial = angular
     # mean of pi Delta^2 Lambda^2 exp(-q^2 Lambda^2 / 4) (interface_roughness_kernel, kernels.jl:176-244)
     dEc = 0.831 * 0.15 / E0_EV
@@ -543,14 +554,18 @@ def full_physics_problem(seed: int = 11, NE: int = 2048, Nk: int = 64, periods: 
     qt = transfer_momenta(kappa, Nphi)
     radial = (math.pi * Delta ** 2 * Lam ** 2 * np.exp(-qt ** 2 * Lam ** 2 / 4).mean(axis=2)).astype(np.complex128)
     qifr = float(np.max(np.abs(radial))) * float(np.max(np.abs(left @ right)))
-    mechs.append(Mechanism("IFR", "ifr", qifr, left=np.asfortranarray(left), right=right,
-                           radial=np.asfortranarray(radial / qifr)))
+    if kernels is None and "IFR" in want:
+        mechs.append(Mechanism("IFR", "ifr", qifr, left=np.asfortranarray(left), right=right,
+                               radial=np.asfortranarray(radial / qifr)))
     # alloy: Omega dV^2 x(1 - x) in the barriers (kernels.jl:285-319), Omega = a^3 / 4, dV = 0.6 eV
     xal = np.where(np.isin(np.floor((x % Lp) / (Lp / 4)).astype(int), [1, 3]), 0.15, 0.0)
     pre_al = (0.565e-9) ** 3 / 4 * (0.6 * E_CHARGE) ** 2 / L0 / K0
-    Kal = acoustic_block(chi, wx * xal * (1 - xal), pre_al)
-    q = float(np.max(np.abs(Kal)))
-    mechs.append(Mechanism("alloy", "momentum_independent", q, block=block_matrix(Kal / q)))
+    if kernels is None and "alloy" in want:
+        Kal = acoustic_block(chi, wx * xal * (1 - xal), pre_al)
+        q = float(np.max(np.abs(Kal)))
+        mechs.append(Mechanism("alloy", "momentum_independent", q, block=block_matrix(Kal / q)))
+    if kernels is not None:
+        mechs = list(kernels)
     kBT = KB_EV * T_K / E0_EV
     target = 3e14 * L0 ** 2 * periods
     return SCBAProblem(
@@ -559,3 +574,29 @@ def full_physics_problem(seed: int = 11, NE: int = 2048, Nk: int = 64, periods: 
         N_LO=1.0 / math.expm1(hw / (KB_EV * T_K)), gs=2, target=target, kBT=kBT,
         eta_seed=0.0005 / E0_EV, alpha=alpha, mechanisms=mechs, name=f"full_physics_N{Nb}",
     )
+
+
+def bias_sweep_problems(npoints: int = 64, seed: int = 5, Nk: int = 32, classes=((2, 8), (3, 8), (4, 8), (6, 8)),
+                        NE_choices=(1024, 1536, 2048, 2560, 3072, 3584, 4096), bias_mV=(20.0, 70.0),
+                        alpha: float = 0.5, Nqz: int = 401, Nphi: int = 64) -> List[SCBAProblem]:
+    """A batched bias sweep: `npoints` operating points from bias_mV[0] to
+    bias_mV[1] mV per period, each on one of the structure classes (periods x
+    states: N_b = 16, 24, 32, 48) and an energy grid of N_E drawn from
+    NE_choices, with N_k momenta and LO + acoustic + IFR scattering
+    (full_physics_problem).  The kernels of a class are built once and shared
+    by its points, since they do not depend on the bias or the energy grid."""
+    rng = np.random.default_rng(seed)
+    cls = rng.integers(0, len(classes), npoints)
+    nes = rng.choice(np.asarray(NE_choices), npoints)
+    biases = np.linspace(bias_mV[0], bias_mV[1], npoints)
+    kernels = {}
+    out = []
+    for i in range(npoints):
+        periods, states = classes[int(cls[i])]
+        key = (periods, states)
+        kw = dict(seed=seed + 100 * int(cls[i]), NE=int(nes[i]), Nk=Nk, periods=periods, states=states, Nqz=Nqz,
+                  Nphi=Nphi, alpha=alpha, bias_mV=float(biases[i]), mechanisms=("LO", "acoustic", "IFR"))
+        pr = full_physics_problem(kernels=kernels.get(key), **kw)
+        kernels.setdefault(key, pr.mechanisms)
+        out.append(dataclasses.replace(pr, name=f"sweep_{i}_N{pr.Nb}_NE{pr.NE}_{biases[i]:.1f}mV"))
+    return out

@@ -30,7 +30,7 @@ def test_tc_gemm_wait_timeout_is_reported_and_recoverable(gpu_ops, orc):
     try:
         with pytest.raises(_lib.QCLError) as ex:
             gpu_ops.production_static_contraction(mech, G, pr.wk, precision="c64")
-        assert ex.value.args[0] == _lib.QCL_TIMEOUT
+        assert ex.value.code == _lib.QCL_TIMEOUT
     finally:
         _lib.check(lib.qcl_debug_set_wait_limit(-1))
     got = gpu_ops.production_static_contraction(mech, G, pr.wk, precision="c64")

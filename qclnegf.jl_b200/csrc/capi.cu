@@ -488,22 +488,18 @@ int qcl_static_contraction(int precision, const qcl_mechanism* op, int NE, int N
     k.tc_bop = bop;
     k.status = (int*)st.p;
   }
-  std::vector<void*> chunk_ops;  // separable sum, complex64: one tensor-core operand per term chunk
+  std::vector<void*> chunk_ops, stage1_ops;  // separable sum, complex64: tensor-core operands per term chunk
   struct ChunkFree {
     std::vector<void*>* v;
     ~ChunkFree() {
       for (void* q : *v) cudaFree(q);
     }
-  } chunk_free{&chunk_ops};
+  } chunk_free{&chunk_ops}, stage1_free{&stage1_ops};
   if (op->kind == QCL_KERNEL_SEPARABLE_SUM && sp == QCL_C64) {
-    for (int i0 = 0; i0 < op->J; i0 += kSepChunk) {
-      const int jc = std::min(kSepChunk, op->J - i0);
-      void* b = nullptr;
-      s = tc_build_operator2((int)N2, jc * (int)N2, 1, (const Cx<float>*)blk.p + N2 * N2 * i0, nullptr, &b, 0);
-      if (b) chunk_ops.push_back(b);
-      if (s) return s;
-    }
+    if ((s = sep_build_tc_operands(Nk, Nb, op->J, ra.p, blk.p, (const double*)dwk.p, chunk_ops, stage1_ops, 0)))
+      return s;
     k.tc_chunks = chunk_ops.data();
+    k.tc_stage1 = stage1_ops.data();
     k.status = (int*)st.p;
   }
   if ((s = dG.upload(G, nb))) return s;

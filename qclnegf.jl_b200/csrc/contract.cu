@@ -547,9 +547,20 @@ static int contraction_t(const KernelOpDev& op, int NE, int Nk, int N, const dou
     Cx<R>* Z = (Cx<R>*)work;
     const int jmax = J < kSepChunk ? J : kSepChunk;  // terms per chunk
     float* awork = (float*)((char*)work + (size_t)jmax * zfield * sizeof(Cx<R>));
+    // complex64 with tensor-core stage-1 operands: G split once for all chunks,
+    // rows (e, (c,d)), K = m', behind the stage-2 work area
+    float* gwork = awork + tc_a_work_floats2((int)Mr, jmax * N2);
     int s;
+    if (sizeof(R) == 4 && op.tc_stage1 && (s = tc_split_rows(NE * N2, Nk, Gv, NEl, NEl * Nk, gwork, st))) return s;
     for (int c = 0, i0 = 0; i0 < J; ++c, i0 += kSepChunk) {
       const int jc = min(kSepChunk, J - i0);
+      if (sizeof(R) == 4 && op.tc_stage1) {
+        // stage 1 on the tensor cores: rows (e, (c,d)), columns (m, i), K = m';
+        // the output index (e, m, (c,d), i) is the chunk's intermediate layout
+        if ((s = launch_tc_presplit(NE * N2, Nk * jc, Nk, op.tc_stage1[c], gwork, Z, NEl, Nk, N2, 1.0, 0.0,
+                                    op.status, st)))
+          return s;
+      } else
       for (int i = i0; i < i0 + jc; ++i) {
         GemmArgs<R> g{};
         g.M = NE; g.Nout = Nk; g.K = Nk; g.batch = N2;
@@ -585,6 +596,49 @@ static int contraction_t(const KernelOpDev& op, int NE, int Nk, int N, const dou
   return QCL_ARG;
 }
 
+// Stage-1 operand of a chunk of separable-sum terms [i0, i0 + jc):
+// Mop[(m + Nk i') + Nk jc m'] = radial[m + Nk m' + Nk^2 (i0 + i')] (complex64).
+__global__ void sep_radial_gather_kernel(int Nk, int i0, int jc, const Cx<float>* __restrict__ radial,
+                                         Cx<float>* __restrict__ out) {
+  const long long n = (long long)Nk * jc * Nk;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+    const int m = (int)(t % Nk), ip = (int)((t / Nk) % jc), mp = (int)(t / ((long long)Nk * jc));
+    out[t] = radial[(size_t)m + (size_t)Nk * mp + (size_t)Nk * Nk * (i0 + ip)];
+  }
+}
+
+// Tensor-core operands of a complex64 separable sum: per chunk of kSepChunk
+// terms the stage-2 operand (the stacked blocks, N^2 x jc N^2) and the
+// stage-1 operand (the radial factors with the momentum weights, Nk jc x Nk).
+int sep_build_tc_operands(int Nk, int N, int J, const void* radial_c64, const void* block_c64, const double* wk,
+                          std::vector<void*>& stage2, std::vector<void*>& stage1, cudaStream_t st) {
+  const int N2 = N * N;
+  void* tmp = nullptr;
+  QCL_CUDA_CHECK(cudaMalloc(&tmp, (size_t)Nk * Nk * kSepChunk * sizeof(Cx<float>)));
+  int s = QCL_OK;
+  for (int i0 = 0; i0 < J && !s; i0 += kSepChunk) {
+    const int jc = J - i0 < kSepChunk ? J - i0 : kSepChunk;
+    void* b = nullptr;
+    s = tc_build_operator2(N2, jc * N2, 1, (const Cx<float>*)block_c64 + (size_t)N2 * N2 * i0, nullptr, &b, st);
+    if (b) stage2.push_back(b);
+    if (s) break;
+    sep_radial_gather_kernel<<<grid_cap((long long)Nk * jc * Nk, 256), 256, 0, st>>>(
+        Nk, i0, jc, (const Cx<float>*)radial_c64, (Cx<float>*)tmp);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) {
+      s = cuda_status(e, "sep_radial_gather_kernel");
+      break;
+    }
+    b = nullptr;
+    s = tc_build_operator2(Nk * jc, Nk, Nk, tmp, wk, &b, st);
+    if (b) stage1.push_back(b);
+    cudaStreamSynchronize(st);  // tmp is reused by the next chunk
+  }
+  cudaStreamSynchronize(st);
+  cudaFree(tmp);
+  return s;
+}
+
 size_t contraction_work_elems(const KernelOpDev& op, int NE, int Nk, int N) {
   if (op.kind == QCL_KERNEL_MOMENTUM_INDEPENDENT) return (size_t)NE * N * N;
   if (op.kind == QCL_KERNEL_DENSE && op.tc_bop) return (tc_a_work_floats(NE, Nk * N * N) + 1) / 2;  // complex64 units
@@ -595,7 +649,9 @@ size_t contraction_work_elems(const KernelOpDev& op, int NE, int Nk, int N) {
     // tensor-core chunks the stage-2 A operand (floats) in complex64 units
     const int jmax = op.J < kSepChunk ? op.J : kSepChunk;
     const size_t zf = (size_t)jmax * NE * Nk * N * N;
-    if (op.tc_chunks) return zf + (tc_a_work_floats2(NE * Nk, jmax * N * N) + 1) / 2;
+    if (op.tc_chunks)
+      return zf + (tc_a_work_floats2(NE * Nk, jmax * N * N) + (op.tc_stage1 ? tc_a_work_floats2(NE * N * N, Nk) : 0) +
+                   1) / 2;
     return zf;
   }
   return 0;

@@ -1,5 +1,7 @@
 // Internal launch interfaces shared by the translation units.
 #pragma once
+#include <vector>
+
 #include "common.cuh"
 
 namespace qcl {
@@ -121,6 +123,7 @@ struct KernelOpDev {
   // separable sums, complex64 fields: one prepared operand per chunk of
   // kSepChunk terms (host array of device pointers)
   const void* const* tc_chunks = nullptr;
+  const void* const* tc_stage1 = nullptr;  // separable sum: stage-1 operand per chunk (radial factors)
   int* status = nullptr;  // device status word for bounded-wait timeouts
 };
 // Terms of a separable-sum operator contracted per stage-2 GEMM: the
@@ -128,6 +131,8 @@ struct KernelOpDev {
 constexpr int kSepChunk = 8;
 inline int sep_chunks(int J) { return (J + kSepChunk - 1) / kSepChunk; }
 size_t contraction_work_elems(const KernelOpDev& op, int NE, int Nk, int N);
+int sep_build_tc_operands(int Nk, int N, int J, const void* radial_c64, const void* block_c64, const double* wk,
+                          std::vector<void*>& stage2, std::vector<void*>& stage1, cudaStream_t st);
 // tensor-core dense contraction (tc_gemm.cu)
 int tc_build_operator(int Nc, int Nk, const void* Mop_c64, const double* wk, void** Bop, cudaStream_t st);
 int tc_build_operator2(int Nout, int Kc, int Nk, const void* Mop_c64, const double* wk, void** Bop, cudaStream_t st);
@@ -137,6 +142,9 @@ size_t tc_operator_bytes(int Nout, int Kc);
 int tc_set_wait_limit(long long rounds);
 int launch_tc_contraction2(int M, int Nout, int Kc, const void* Bop, const void* A, void* S, double alpha,
                            double beta, float* awork, int* status, cudaStream_t st);
+int tc_split_rows(int M, int Kc, const void* A, long long P, long long Bs, float* awork, cudaStream_t st);
+int launch_tc_presplit(int M, int Nout, int Kc, const void* Bop, const float* awork, void* S, long long oP,
+                       long long oQ, long long oR, double alpha, double beta, int* status, cudaStream_t st);
 int launch_tc_dense_contraction(int NE, int Nc, const void* Bop, const void* G, void* S, double alpha, double beta,
                                 float* awork, int* status, cudaStream_t st);
 int launch_contraction(int precision, const KernelOpDev& op, int NE, int Nk, int N, const double* wk, const void* G,

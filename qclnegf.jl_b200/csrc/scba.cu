@@ -48,11 +48,13 @@ struct Mech {
   // complex128 copies of the operator arrays (refinement contexts): swapped in by promote
   void *block64 = nullptr, *matrix64 = nullptr, *left64 = nullptr, *right64 = nullptr, *radial64 = nullptr;
   std::vector<void*> tc_chunks;  // separable sum: tensor-core operand per term chunk (complex64 fields)
+  std::vector<void*> tc_stage1;  // separable sum: stage-1 operand per term chunk
   int* status = nullptr;
   KernelOpDev view() const {
     KernelOpDev k;
     k.tc_bop = tc_bop;
     k.tc_chunks = tc_chunks.empty() ? nullptr : tc_chunks.data();
+    k.tc_stage1 = tc_stage1.size() == tc_chunks.size() && !tc_stage1.empty() ? tc_stage1.data() : nullptr;
     k.status = status;
     k.kind = kind;
     k.J = J;
@@ -246,6 +248,7 @@ void scba_destroy(ScbaCtx* c) {
     cudaFree(m.radial);
     cudaFree(m.tc_bop);
     for (void* q : m.tc_chunks) cudaFree(q);
+    for (void* q : m.tc_stage1) cudaFree(q);
     for (void* q : {m.block64, m.matrix64, m.left64, m.right64, m.radial64}) cudaFree(q);
   }
   for (void* p : c->state) cudaFree(p);
@@ -313,7 +316,10 @@ static size_t op_work_elems(const qcl_mechanism& q, int precision, int NE, int N
   static const void* dummy[1] = {nullptr};
   if (precision != QCL_C128) {  // the tensor-core operands exist
     if (q.kind == QCL_KERNEL_DENSE) k.tc_bop = dummy;
-    if (q.kind == QCL_KERNEL_SEPARABLE_SUM) k.tc_chunks = dummy;
+    if (q.kind == QCL_KERNEL_SEPARABLE_SUM) {
+      k.tc_chunks = dummy;
+      k.tc_stage1 = dummy;
+    }
   }
   return contraction_work_elems(k, NE, Nk, N);
 }
@@ -340,7 +346,9 @@ static int plan_memory(const qcl_scba_problem* p, const qcl_mechanism* mechs, Me
     const int N2 = N * N;
     if (!c128 && q.kind == QCL_KERNEL_DENSE) mp->operators += tc_operator_bytes(Nk * N2, Nk * N2);
     if (!c128 && q.kind == QCL_KERNEL_SEPARABLE_SUM)
-      for (int i0 = 0; i0 < q.J; i0 += kSepChunk) mp->operators += tc_operator_bytes(N2, std::min(kSepChunk, q.J - i0) * N2);
+      for (int i0 = 0; i0 < q.J; i0 += kSepChunk)
+        mp->operators += tc_operator_bytes(N2, std::min(kSepChunk, q.J - i0) * N2) +
+                         tc_operator_bytes(Nk * std::min(kSepChunk, q.J - i0), Nk);
     cwork = std::max(cwork, op_work_elems(q, p->precision, NE, Nk, N) * esz);
     if (p->refinement && !c128) cwork = std::max(cwork, op_work_elems(q, QCL_C128, NE, Nk, N) * 16);
   }
@@ -533,13 +541,7 @@ int scba_create(const qcl_scba_problem* p, const qcl_mechanism* mechs, ScbaCtx**
       TRY(upload_op(c, &d.radial, q.radial, (size_t)c->Nk * c->Nk * q.J, &d.radial64));
       TRY(upload_op(c, &d.block, q.block, (size_t)N2 * N2 * q.J, &d.block64));
       if (c->precision != QCL_C128)
-        for (int i0 = 0; i0 < q.J; i0 += kSepChunk) {
-          const int jc = std::min(kSepChunk, q.J - i0);
-          void* b = nullptr;
-          s = tc_build_operator2(N2, jc * N2, 1, (const Cx<float>*)d.block + (size_t)N2 * N2 * i0, nullptr, &b, c->st);
-          if (b) d.tc_chunks.push_back(b);
-          TRY(s);
-        }
+        TRY(sep_build_tc_operands(c->Nk, c->N, q.J, d.radial, d.block, c->wk, d.tc_chunks, d.tc_stage1, c->st));
     } else {
       TRY((set_last_error("unknown kernel kind %d", q.kind), QCL_ARG));
     }
@@ -1326,6 +1328,8 @@ int scba_promote(ScbaCtx* c) {
     m.tc_bop = nullptr;
     for (void* q : m.tc_chunks) cudaFree(q);
     m.tc_chunks.clear();
+    for (void* q : m.tc_stage1) cudaFree(q);
+    m.tc_stage1.clear();
   }
   c->precision = QCL_C128;
   c->fbytes = c->nfield * 16;

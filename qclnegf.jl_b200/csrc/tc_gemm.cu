@@ -154,13 +154,20 @@ struct TcArgs {
   int M;        // rows of C actually stored (N_E)
   int Ncols;    // real columns of C actually stored (2 Nc)
   int Kpad;     // padded real K (multiple of TC_BK)
-  Cx<float>* S; // S[e + NE j], j < Ncols / 2
+  Cx<float>* S; // element (row e, complex column j) at S[tc_out_index(e, j)]
   int NE;
   double alpha, beta;
   const float* ainv;  // 1 / s_e per row of A
   const float* binv;  // 1 / s_B (device scalar)
   int* status;
+  // output index (e mod oP) + oP (j mod oQ) + oP oQ (e / oP) + oP oQ oR (j / oQ);
+  // oP = M and oQ larger than every j give the plain column-major e + M j
+  long long oP, oQ, oR;
 };
+
+__device__ __forceinline__ size_t tc_out_index(const TcArgs& p, long long e, long long j) {
+  return (size_t)((e % p.oP) + p.oP * (j % p.oQ) + p.oP * p.oQ * (e / p.oP) + p.oP * p.oQ * p.oR * (j / p.oQ));
+}
 
 // Warp roles: warps 0-7 read accumulators out (warp w: tensor-memory lanes
 // 32 (w % 4) .. + 31, columns 128 (w / 4) .. + 127) into FP32 running sums and
@@ -320,7 +327,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) tc_gemm_kernel(const __grid_con
       for (int q = 0; q < CH / 2; ++q) {
         const int nn = n0 + cbase + 2 * q;
         if (nn >= p.Ncols) continue;
-        Cx<float>* dst = p.S + (size_t)e + (size_t)p.NE * (size_t)(nn >> 1);
+        Cx<float>* dst = p.S + tc_out_index(p, e, nn >> 1);
         const float re = (float)(al * (double)sum[2 * q]), im = (float)(al * (double)sum[2 * q + 1]);
         if (p.beta == 0.0) {
           *dst = cx<float>(re, im);
@@ -369,7 +376,11 @@ __device__ __forceinline__ void split_f16(float x, __half& hi, __half& lo) {
 // values order as unsigned integers; a non-finite entry gives +inf), which
 // the caller zeroes first.  A CTA covers 32 rows x 256 values of k (coalesced
 // along e); the atomic maximum is independent of the order.
-__global__ void tc_row_max_kernel(int NE, int Nc, const Cx<float>* __restrict__ G, unsigned* __restrict__ rowmax) {
+// Rows of A address G at (e mod P) + P k + Bs (e / P): P = NE, Bs = 0 is the
+// plain column-major matrix; P = N_E, Bs = N_E N_k reads a field with rows
+// (e, (c,d)) and columns m' (the first stage of a separable-sum contraction).
+__global__ void tc_row_max_kernel(int NE, int Nc, long long P, long long Bs, const Cx<float>* __restrict__ G,
+                                  unsigned* __restrict__ rowmax) {
   __shared__ float red[8][32];
   const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;  // 32 x 8 threads
   const int e = blockIdx.x * 32 + tx;
@@ -377,7 +388,7 @@ __global__ void tc_row_max_kernel(int NE, int Nc, const Cx<float>* __restrict__ 
   float mx = 0.0f;
   if (e < NE)
     for (int k = k0 + ty; k < k1; k += 8) {
-      const Cx<float> g = G[(size_t)e + (size_t)NE * k];
+      const Cx<float> g = G[(size_t)(e % P) + (size_t)P * k + (size_t)Bs * (size_t)(e / P)];
       const float a = fmaxf(fabsf(g.x), fabsf(g.y));
       mx = (isfinite(g.x) && isfinite(g.y)) ? fmaxf(mx, a) : INFINITY;
     }
@@ -394,7 +405,8 @@ __global__ void tc_row_max_kernel(int NE, int Nc, const Cx<float>* __restrict__ 
 // first column of CTAs also writes ainv[e] = 1 / s_e.  A 32 x 32 (e, kk)
 // tile is transposed through shared memory so that both the E-fastest reads
 // and the K-contiguous writes are coalesced.
-__global__ void tc_split_a_kernel(int NE, int Nc, int Mpad, int Kpad, const Cx<float>* __restrict__ G,
+__global__ void tc_split_a_kernel(int NE, int Nc, int Mpad, int Kpad, long long P, long long Bs,
+                                  const Cx<float>* __restrict__ G,
                                   const unsigned* __restrict__ rowmax, __half* __restrict__ Ahi,
                                   __half* __restrict__ Alo, float* __restrict__ ainv) {
   __shared__ float tile[32][33];
@@ -409,7 +421,7 @@ __global__ void tc_split_a_kernel(int NE, int Nc, int Mpad, int Kpad, const Cx<f
     float v = 0.0f;
     const int k = kk >> 1;
     if (er < NE && k < Nc) {
-      const Cx<float> g = G[(size_t)er + (size_t)NE * k];
+      const Cx<float> g = G[(size_t)(er % P) + (size_t)P * k + (size_t)Bs * (size_t)(er / P)];
       v = ((kk & 1) ? g.y : g.x) * sc;
     }
     tile[r][tx] = v;
@@ -601,18 +613,39 @@ template <int BN> static int launch_tc_t(const TcMaps& maps, const TcArgs& a, in
 // e < M, j < Nout, k < Kc; Bop prepared by tc_build_operator2(Nout, Kc, ...).
 int launch_tc_contraction2(int M, int Nout, int Kc, const void* Bop, const void* A, void* S, double alpha,
                            double beta, float* awork, int* status, cudaStream_t st) {
+  int s = tc_split_rows(M, Kc, A, M, 0, awork, st);
+  if (s) return s;
+  return launch_tc_presplit(M, Nout, Kc, Bop, awork, S, M, 1ll << 40, 0, alpha, beta, status, st);
+}
+
+// The FP16 hi / lo split of A (rows addressed as in tc_row_max_kernel) into
+// awork: hi, lo (Mpad x Kpad each), row maxima, inverse row scales.
+int tc_split_rows(int M, int Kc, const void* A, long long P, long long Bs, float* awork, cudaStream_t st) {
   int Mpad, Npad, Kpad;
-  tc_dims2(M, Nout, Kc, &Mpad, &Npad, &Kpad);
+  tc_dims2(M, 1, Kc, &Mpad, &Npad, &Kpad);
   __half* Ahi = (__half*)awork;
   __half* Alo = Ahi + (size_t)Mpad * Kpad;
   unsigned* rowmax = (unsigned*)(Alo + (size_t)Mpad * Kpad);
   float* ainv = (float*)(rowmax + Mpad);
   QCL_CUDA_CHECK(cudaMemsetAsync(rowmax, 0, (size_t)Mpad * sizeof(unsigned), st));
-  tc_row_max_kernel<<<dim3(Mpad / 32, (Kc + 255) / 256), 256, 0, st>>>(M, Kc, (const Cx<float>*)A, rowmax);
+  tc_row_max_kernel<<<dim3(Mpad / 32, (Kc + 255) / 256), 256, 0, st>>>(M, Kc, P, Bs, (const Cx<float>*)A, rowmax);
   QCL_LAUNCH_CHECK("tc_row_max_kernel");
   dim3 sg((Mpad + 31) / 32, (Kpad + 31) / 32);
-  tc_split_a_kernel<<<sg, 256, 0, st>>>(M, Kc, Mpad, Kpad, (const Cx<float>*)A, rowmax, Ahi, Alo, ainv);
+  tc_split_a_kernel<<<sg, 256, 0, st>>>(M, Kc, Mpad, Kpad, P, Bs, (const Cx<float>*)A, rowmax, Ahi, Alo, ainv);
   QCL_LAUNCH_CHECK("tc_split_a_kernel");
+  return QCL_OK;
+}
+
+// The product of an A already split into awork (tc_split_rows with the same
+// M, Kc) and a prepared operand; the output index is (e mod oP) + oP (j mod oQ)
+// + oP oQ (e / oP) + oP oQ oR (j / oQ) (see TcArgs).
+int launch_tc_presplit(int M, int Nout, int Kc, const void* Bop, const float* awork, void* S, long long oP,
+                       long long oQ, long long oR, double alpha, double beta, int* status, cudaStream_t st) {
+  int Mpad, Npad, Kpad;
+  tc_dims2(M, Nout, Kc, &Mpad, &Npad, &Kpad);
+  const __half* Ahi = (const __half*)awork;
+  const __half* Alo = Ahi + (size_t)Mpad * Kpad;
+  const float* ainv = (const float*)((const unsigned*)(Alo + (size_t)Mpad * Kpad) + Mpad);
   const char* b = (const char*)Bop;
   const __half* Bhi = (const __half*)(b + 256);
   const __half* Blo = Bhi + (size_t)Npad * Kpad;
@@ -625,18 +658,9 @@ int launch_tc_contraction2(int M, int Nout, int Kc, const void* Bop, const void*
   // B rows past Npad (the last tile of a narrower width) read the zero fill
   if ((s = make_operand_map(&maps.bhi, Bhi, Npad, Kpad, bn))) return s;
   if ((s = make_operand_map(&maps.blo, Blo, Npad, Kpad, bn))) return s;
-  TcArgs a{M, 2 * Nout, Kpad, (Cx<float>*)S, M, alpha, beta, ainv, (const float*)b, status};
+  TcArgs a{M, 2 * Nout, Kpad, (Cx<float>*)S, M, alpha, beta, ainv, (const float*)b, status, oP, oQ, oR};
   if (bn == 224) return launch_tc_t<224>(maps, a, mtiles, st);
   return launch_tc_t<256>(maps, a, mtiles, st);
-}
-
-// Sets the main-loop wait limit of the tensor-core kernels on the current
-// device (rounds of mbarrier.try_wait; 0 makes every main-loop wait give up at
-// once; a negative value restores the default).
-int tc_set_wait_limit(long long rounds) {
-  const long long v = rounds >= 0 ? rounds : TC_WAIT_LIMIT;
-  QCL_CUDA_CHECK(cudaMemcpyToSymbol(g_tc_main_wait_limit, &v, sizeof(v)));
-  return QCL_OK;
 }
 
 int launch_tc_dense_contraction(int NE, int Nc, const void* Bop, const void* G, void* S, double alpha, double beta,

@@ -663,6 +663,15 @@ int launch_tc_presplit(int M, int Nout, int Kc, const void* Bop, const float* aw
   return launch_tc_t<256>(maps, a, mtiles, st);
 }
 
+// Sets the main-loop wait limit of the tensor-core kernels on the current
+// device (rounds of mbarrier.try_wait; 0 makes every main-loop wait give up at
+// once; a negative value restores the default).
+int tc_set_wait_limit(long long rounds) {
+  const long long v = rounds >= 0 ? rounds : TC_WAIT_LIMIT;
+  QCL_CUDA_CHECK(cudaMemcpyToSymbol(g_tc_main_wait_limit, &v, sizeof(v)));
+  return QCL_OK;
+}
+
 int launch_tc_dense_contraction(int NE, int Nc, const void* Bop, const void* G, void* S, double alpha, double beta,
                                 float* awork, int* status, cudaStream_t st) {
   return launch_tc_contraction2(NE, Nc, Nc, Bop, G, S, alpha, beta, awork, status, st);

@@ -53,8 +53,12 @@ def parse():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-extras", action="store_true", help="skip the variant and SCBA side measurements")
-    ap.add_argument("--capture", choices=["dyson", "hilbert", "scba", "tcgemm", "scba_all_mixed", "scba_all_c128"],
+    ap.add_argument("--capture", choices=["dyson", "hilbert", "scba", "tcgemm", "scba_all_mixed", "scba_all_c128",
+                                          "separable"],
                     help="run one small case of a kernel for an ncu capture (2 launches) and exit")
+    ap.add_argument("--study", choices=["full_physics_converged", "bias_sweep_64"],
+                    help="run one long study (seconds to minutes of GPU time), print its JSON and exit: the "
+                         "full-physics SCBA converged in both precisions, or the 64-point batched bias sweep")
     return ap.parse_args()
 
 
@@ -632,13 +636,109 @@ def extras(torch, dev, L, _lib):
             res[precision].update(j_error(Jref, J))
         solver.close()
     out["scba_tutorial_N12_30iter"] = res
-    try:
-        out["scba_all_mechanisms"] = scba_all_mechanisms(torch)
-    except Exception as ex:  # noqa: BLE001
-        import traceback
+    import traceback
 
-        out["scba_all_mechanisms"] = {"error": repr(ex), "where": traceback.format_exc(limit=4)[-600:]}
+    for key, fn in (("scba_all_mechanisms", lambda: scba_all_mechanisms(torch)),
+                    ("scba_full_physics_N32", lambda: scba_full_physics(torch)),
+                    ("bias_sweep_16", lambda: bias_sweep(torch, npoints=16, iters=4,
+                                                         classes=((2, 8), (3, 8), (4, 8)),
+                                                         NE_choices=(1024, 1536, 2048)))):
+        try:
+            out[key] = fn()
+        except Exception as ex:  # noqa: BLE001
+            out[key] = {"error": repr(ex), "where": traceback.format_exc(limit=4)[-600:]}
     return out
+
+
+def scba_full_physics(torch, timed=(2, 4)):
+    """The full-physics mixed-precision configuration at its stated size:
+    N_b = 32 (4 periods x 8 states), N_E x N_k = 2048 x 64, LO (separable
+    sum of the exact Froehlich kernel on 401 q_z nodes), acoustic, impurity
+    (separable sum of the tabulated covariance), IFR and alloy, T = 100 K.
+    FP64 and mixed precision from the same seed: seconds per iteration (CUDA
+    graphs on; one untimed iteration first), the per-phase device times of
+    the last iteration, the relative J difference over the same iterations,
+    and the memory estimate of each context."""
+    import numpy as np
+    from qclb200.problem import full_physics_problem
+    from qclb200.scba import ProductionSCBA, estimate_memory
+
+    t = time.perf_counter()
+    pr = full_physics_problem()
+    res = {"build_s": time.perf_counter() - t,
+           "terms": {m.name: int(m.radial.shape[2]) for m in pr.mechanisms if m.kind == "separable_sum"}}
+    J = {}
+    for precision, n in zip(("c128", "mixed"), timed):
+        est = estimate_memory(pr, precision=precision)
+        s = ProductionSCBA(pr, precision=precision, use_graph=True, telemetry=True)
+        s.seed()
+        rows = [s.step()]
+        times = []
+        for _ in range(n):
+            t = time.perf_counter()
+            rows.append(s.step())
+            times.append(time.perf_counter() - t)
+        s.close()
+        torch.cuda.synchronize()
+        sec = float(np.median(times))
+        J[precision] = [r["J"] for r in rows]
+        res[precision] = {"s_per_iter": sec, "iter_per_s": 1.0 / sec, "phase_ms": rows[-1]["phase_ms"],
+                          "r_Sigma": [r["r_Sigma"] for r in rows], "J": J[precision],
+                          "peak_memory_GB": est["peak"] / 1e9}
+    res["mixed_speedup_vs_fp64"] = res["mixed"]["iter_per_s"] / res["c128"]["iter_per_s"]
+    n = min(len(J["c128"]), len(J["mixed"]))
+    res["J_rel_err_mixed_vs_fp64"] = max(abs(a - b) / abs(a) for a, b in zip(J["c128"][:n], J["mixed"][:n]))
+    res["config"] = ("N_b = 32, N_E x N_k = 2048 x 64, LO + acoustic + impurity + IFR + alloy, T = 100 K, linear "
+                     "mixing 0.5, roundoff check on; iterations after the seed, CUDA graphs on")
+    return res
+
+
+def bias_sweep(torch, npoints=64, iters=5, classes=((2, 8), (3, 8), (4, 8), (6, 8)),
+               NE_choices=(1024, 1536, 2048, 2560, 3072, 3584, 4096)):
+    """The batched bias sweep: `npoints` bias points 20-70 mV per period over
+    structure classes N_b = 16 ... 48 and energy grids N_E from NE_choices,
+    N_k = 32, LO + acoustic + IFR, mixed precision, the Dyson CTA shape of
+    every class from the autotuner; `iters` iterations per point.  The
+    batched run (qcl_sweep_run: resident points in one graph launch per
+    iteration) against the same points one after another (qcl_scba_step),
+    in SCBA iterations per second, and the largest J difference between the
+    two (the same kernels run, so it is zero)."""
+    import numpy as np
+    from qclb200 import operators
+    from qclb200.problem import bias_sweep_problems
+    from qclb200.scba import BatchedSweep, ProductionSCBA
+
+    t = time.perf_counter()
+    pts = bias_sweep_problems(npoints=npoints, classes=classes, NE_choices=NE_choices)
+    res = {"build_s": time.perf_counter() - t, "points": npoints,
+           "Nb": sorted({p.Nb for p in pts}), "NE": sorted({p.NE for p in pts})}
+    tune = {}
+    for nb in sorted({p.Nb for p in pts}):
+        tune[str(nb)] = operators.autotune(nb, precision="mixed", NE=1024, Nk=32)
+    res["autotune_mixed"] = tune
+    torch.cuda.synchronize()
+    t = time.perf_counter()
+    Jseq = []
+    for p in pts:
+        s = ProductionSCBA(p, precision="mixed", use_graph=True)
+        s.seed()
+        rows = s.run(iters)
+        Jseq.append(rows[-1]["J"])
+        s.close()
+    torch.cuda.synchronize()
+    seq_s = time.perf_counter() - t
+    sw = BatchedSweep(pts, precision="mixed")
+    rows, n_it, stats = sw.run(iters)
+    sw.close()
+    res["sequential"] = {"wall_s": seq_s, "iter_per_s": npoints * iters / seq_s}
+    res["batched"] = dict(stats, iter_per_s=stats["iterations"] / stats["wall_s"])
+    res["batched_speedup"] = res["batched"]["iter_per_s"] / res["sequential"]["iter_per_s"]
+    res["J_max_rel_diff_batched_vs_sequential"] = max(abs(r["J"] - j) / abs(j) for r, j in zip(rows, Jseq))
+    operators.autotune_reset()
+    res["config"] = (f"{npoints} points, bias 20-70 mV/period, N_b in {res['Nb']}, N_E in {res['NE']}, N_k = 32, "
+                     f"LO + acoustic + IFR, mixed precision, {iters} iterations per point (seed and context "
+                     "creation included in both wall times)")
+    return res
 
 
 def j_error(Jref, J):
@@ -745,6 +845,21 @@ def run_capture(kind):
         mech = Mechanism("impurity", "dense", 1.0, matrix=M)
         for _ in range(2):
             operators.production_static_contraction(mech, G, np.ones(nk), precision="c64")
+    elif kind == "separable":
+        # one separable-sum contraction at a quarter of the full-physics energies:
+        # N_E x N_k = 512 x 64, N_b = 32, one chunk of 8 terms, complex64 then complex128
+        import numpy as np
+        from qclb200 import operators
+        from qclb200.problem import Mechanism
+
+        rng = np.random.default_rng(0)
+        ne, nk, nb, J = 512, 64, 32, 8
+        radial = np.asfortranarray(rng.standard_normal((nk, nk, J)) + 1j * rng.standard_normal((nk, nk, J)))
+        block = np.asfortranarray(rng.standard_normal((nb * nb, nb * nb, J)) + 1j * rng.standard_normal((nb * nb, nb * nb, J)))
+        mech = Mechanism("impurity", "separable_sum", 1.0, radial=radial, block=block)
+        G = np.asfortranarray(rng.standard_normal((ne, nk, nb, nb)) + 1j * rng.standard_normal((ne, nk, nb, nb)))
+        for prec in ("c64", "c128"):
+            operators.production_static_contraction(mech, G, np.ones(nk), precision=prec)
     elif kind.startswith("scba_all"):
         # the all-mechanism SCBA workload of the extras (N_E x N_k = 1024 x 32,
         # N_b = 16, LO + acoustic + impurity + IFR + alloy): seed + 3 eager
@@ -771,10 +886,80 @@ def run_capture(kind):
     print("ok", kind)
 
 
+def run_study(kind):
+    import torch
+
+    if kind == "bias_sweep_64":
+        out = bias_sweep(torch)
+    else:
+        out = full_physics_converged(torch)
+    print(json.dumps(out), flush=True)
+
+
+def full_physics_converged(torch, tol=1e-8, max_mixed=400, max_fp64=600):
+    """The full-physics configuration converged: (1) plain FP64 from the seed
+    until r_Sigma <= tol; (2) mixed precision with Anderson mixing (history in
+    complex64) to its floor, then the state promoted exactly to FP64 (on the
+    host: a refinement context cannot hold a complex128 history) and refined
+    in FP64 until r_Sigma <= tol.  Iterations, seconds, and the relative
+    difference of the converged J."""
+    import dataclasses
+
+    import numpy as np
+    from qclb200.problem import full_physics_problem
+    from qclb200.scba import ProductionSCBA
+
+    pr = full_physics_problem()
+    out = {}
+    t = time.perf_counter()
+    f = ProductionSCBA(pr, precision="c128", use_graph=True)
+    f.seed()
+    rf = f.run(max_fp64, tol)
+    f.close()
+    out["fp64"] = {"iterations": len(rf), "wall_s": time.perf_counter() - t, "r_Sigma": rf[-1]["r_Sigma"],
+                   "J": rf[-1]["J"], "r_Sigma_trace": [r["r_Sigma"] for r in rf[::10]]}
+    t = time.perf_counter()
+    pa = dataclasses.replace(pr, mixing="anderson", anderson_history_depth=2)
+    m = ProductionSCBA(pa, precision="mixed", use_graph=True)
+    m.seed()
+    rm = []
+    best = np.inf
+    for _ in range(max_mixed):
+        r = m.step()
+        rm.append(r)
+        best = min(best, r["r_Sigma"])
+        if r["r_Sigma"] <= 1e-6 or (len(rm) > 20 and min(x["r_Sigma"] for x in rm[-10:]) > 0.8 * best):
+            break
+    fams = [m.family(f_) for f_ in range(len(pr.mechanisms) + 2)]
+    m.close()
+    tm = time.perf_counter() - t
+    r = ProductionSCBA(pr, precision="c128", use_graph=True)
+    for f_, comps in enumerate(fams):
+        for c, a in enumerate(comps):
+            a = a.astype(np.complex128)
+            if c:  # Sigma< and Sigma> keep their anti-Hermitian part, as qcl_scba_promote does
+                a = np.asfortranarray(0.5 * (a - np.conj(np.swapaxes(a, 2, 3))))
+            r.upload(3 + 3 * f_ + c, a)
+    rr = r.run(max_fp64, tol)
+    r.close()
+    out["mixed_then_fp64"] = {"mixed_iterations": len(rm), "mixed_wall_s": tm, "mixed_r_Sigma": rm[-1]["r_Sigma"],
+                              "mixed_J": rm[-1]["J"], "fp64_iterations": len(rr),
+                              "wall_s": time.perf_counter() - t, "r_Sigma": rr[-1]["r_Sigma"], "J": rr[-1]["J"],
+                              "mixed_r_Sigma_trace": [x["r_Sigma"] for x in rm[::5]]}
+    Jf = out["fp64"]["J"]
+    out["J_rel_err_mixed_floor_vs_fp64"] = abs(rm[-1]["J"] - Jf) / abs(Jf)
+    out["J_rel_err_refined_vs_fp64"] = abs(rr[-1]["J"] - Jf) / abs(Jf)
+    out["time_to_solution_speedup"] = out["fp64"]["wall_s"] / out["mixed_then_fp64"]["wall_s"]
+    return out
+
+
 def main():
     args = parse()
     if args.capture:
         run_capture(args.capture)
+        return
+    if args.study:
+        run_study(args.study)
         return
     if args.impl == "reference":
         run_reference(args)

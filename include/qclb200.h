@@ -489,6 +489,26 @@ int qcl_scba_green_state(qcl_scba* ctx, void* A, double* kappa, double* scale);
  * step or seed. */
 int qcl_scba_witness(qcl_scba* ctx, qcl_psd_witness* witness);
 
+/* Implicit differentiation of the converged SCBA (tangent mode; the
+ * reference has no derivatives).  At the state of the last step -- a fixed
+ * point Sigma_fp = Phi(Sigma_fp, p) once converged -- the derivative
+ * v of Sigma_fp with respect to p solves v = Phi_Sigma v + Phi_p (the implicit-function
+ * theorem), and dJ/dp = J_Sigma v + J_p.  qcl_scba_tangent_init allocates the
+ * tangent fields (complex128 context, linear mixing, paired normalisation);
+ * qcl_scba_tangent_set uploads a component of the source Phi_p (which as in
+ * qcl_scba_download; host NULL zeroes it; which = -1 zeroes v);
+ * qcl_scba_tangent_step does one damped step v <- (1 - alpha) v +
+ * alpha (Phi_Sigma v + Phi_p) with Phi_Sigma v from the linearised Dyson,
+ * Keldysh and normalisation steps and the (linear) candidate maps, and writes
+ * out[0] = J_Sigma v (solver units, J = Jbar J0) and out[1] = the largest
+ * relative change of a tangent field.  qcl_scba_download_candidate returns a
+ * family field of the last step's mixed candidate (1 - alpha) Sigma +
+ * alpha Phi(Sigma), from which a caller forms Phi_p by differences. */
+int qcl_scba_tangent_init(qcl_scba* ctx);
+int qcl_scba_tangent_set(qcl_scba* ctx, int which, const void* host);
+int qcl_scba_tangent_step(qcl_scba* ctx, double* out);
+int qcl_scba_download_candidate(qcl_scba* ctx, int which, void* host);
+
 /* Batched sweep of independent operating points: a bias sweep, or points of
  * different structures (basis sizes, energy grids).  The reference solves
  * operating points one after another, re-using basis and kernels across

@@ -147,6 +147,10 @@ int scba_witness(ScbaCtx* c, double* out12);
 int scba_retarget(ScbaCtx* c, double Ep, double N_LO, double kBT, const void* h, const double* q);
 int scba_estimate_memory(const qcl_scba_problem* p, const qcl_mechanism* mechs, size_t out[6]);
 int scba_promote(ScbaCtx* c);
+int scba_tangent_init(ScbaCtx* c);
+int scba_tangent_set(ScbaCtx* c, int which, const void* host);
+int scba_tangent_step(ScbaCtx* c, double* out);
+int scba_download_candidate(ScbaCtx* c, int which, void* host);
 struct Sweep;
 int sweep_create(int n, const qcl_scba_problem* problems, const qcl_mechanism* const* mechanisms, size_t budget,
                  Sweep** out);
@@ -785,6 +789,38 @@ int qcl_sweep_run(qcl_sweep* sweep, int max_iter, double tol_sigma, qcl_scba_row
 }
 
 void qcl_sweep_destroy(qcl_sweep* sweep) { sweep_destroy((Sweep*)sweep); }
+
+int qcl_scba_tangent_init(qcl_scba* ctx) {
+  if (!ctx) {
+    set_last_error("ctx is required");
+    return QCL_ARG;
+  }
+  return scba_tangent_init((ScbaCtx*)ctx);
+}
+
+int qcl_scba_tangent_set(qcl_scba* ctx, int which, const void* host) {
+  if (!ctx) {
+    set_last_error("ctx is required");
+    return QCL_ARG;
+  }
+  return scba_tangent_set((ScbaCtx*)ctx, which, host);
+}
+
+int qcl_scba_tangent_step(qcl_scba* ctx, double* out) {
+  if (!ctx || !out) {
+    set_last_error("ctx and out are required");
+    return QCL_ARG;
+  }
+  return scba_tangent_step((ScbaCtx*)ctx, out);
+}
+
+int qcl_scba_download_candidate(qcl_scba* ctx, int which, void* host) {
+  if (!ctx || !host) {
+    set_last_error("ctx and host are required");
+    return QCL_ARG;
+  }
+  return scba_download_candidate((ScbaCtx*)ctx, which, host);
+}
 
 int qcl_debug_set_wait_limit(long long rounds) { return tc_set_wait_limit(rounds); }
 

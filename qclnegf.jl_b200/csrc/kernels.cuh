@@ -202,6 +202,12 @@ int launch_seed_green(int precision, int NE, int Nk, int N, const void* GR, cons
 int launch_residual_pair(int precision, size_t n, const void* o1, const void* o2, const void* n1, const void* n2,
                          double* partial, double* out2, cudaStream_t st);
 int launch_convert(int precision, size_t n, const void* in_c128, void* out, cudaStream_t st);
+// tangent of the SCBA map (tangent.cu)
+int launch_block_triple(int NE, int Nk, int N, const void* A, const void* B, const void* C, int adjC, double alpha,
+                        double beta, void* out, void* trace, cudaStream_t st);
+int launch_norm_tangent(size_t n, const void* Ln, const void* Gn, const double* coeffs, const double* dtrL,
+                        const double* dtrG, int gs, double target, double* dcoef, void* dL, void* dG,
+                        cudaStream_t st);
 int launch_promote(size_t n, const void* in_c64, void* out_c128, cudaStream_t st);
 int launch_antihermitian_part(int NE, int Nk, int N, void* X, cudaStream_t st);
 

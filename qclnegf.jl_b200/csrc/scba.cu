@@ -139,6 +139,13 @@ struct ScbaCtx {
   cudaEvent_t pev[kPhases + 1] = {};
   double phase_ms[kPhases] = {};
   double init_ms = 0;
+  // tangent of the fixed point (qcl_scba_tangent_*): v and its update (families),
+  // the source Phi_p (families), dG^{R,<,>}, the tangent totals, traces, scalars
+  std::vector<void*> tv, tw, tsrc;
+  void *tG[3] = {nullptr, nullptr, nullptr}, *ttot[3] = {nullptr, nullptr, nullptr};
+  Cx<double>*ttrL = nullptr, *ttrG = nullptr;
+  double* tscal = nullptr;  // dtrL (2), dtrG (2), dcoef (2), residual partial sums, J (2 x (2 + N))
+  double* tscal_h = nullptr;
   int parity = 0;
   bool pending_commit = false;
   int nu = 0;
@@ -253,6 +260,16 @@ void scba_destroy(ScbaCtx* c) {
   }
   for (void* p : c->state) cudaFree(p);
   for (void* p : c->cand) cudaFree(p);
+  for (auto* v : {&c->tv, &c->tw, &c->tsrc})
+    for (void* p : *v) cudaFree(p);
+  for (int k = 0; k < 3; ++k) {
+    cudaFree(c->tG[k]);
+    cudaFree(c->ttot[k]);
+  }
+  cudaFree(c->ttrL);
+  cudaFree(c->ttrG);
+  cudaFree(c->tscal);
+  if (c->tscal_h) cudaFreeHost(c->tscal_h);
   cudaFree(c->GR);
   cudaFree(c->GL);
   cudaFree(c->GG);
@@ -656,13 +673,14 @@ static int scattering_candidates(ScbaCtx* c, const void* GR, const void* GL, con
   return QCL_OK;
 }
 
-static int embedding_candidates(ScbaCtx* c, std::vector<void*>& dst) {
+static int embedding_candidates(ScbaCtx* c, std::vector<void*>& dst, const void* GR = nullptr,
+                                const void* GL = nullptr, const void* GG = nullptr) {
   const int cp = c->precision == QCL_MIXED ? QCL_C64 : c->precision;
   SandwichJob jobs[2];
   for (int sgn = 0; sgn < 2; ++sgn) {
-    jobs[sgn].X[0] = c->GR;
-    jobs[sgn].X[1] = c->GL;
-    jobs[sgn].X[2] = c->GG;
+    jobs[sgn].X[0] = GR ? GR : c->GR;
+    jobs[sgn].X[1] = GL ? GL : c->GL;
+    jobs[sgn].X[2] = GG ? GG : c->GG;
     for (int k = 0; k < 3; ++k) jobs[sgn].S[k] = field_of(dst, c->M + sgn, k);
     jobs[sgn].T = sgn == 0 ? c->Tp : c->Tm;
     jobs[sgn].plan = c->shift[sgn].view();
@@ -1541,6 +1559,150 @@ int sweep_run(Sweep* sw, int max_iter, double tol, qcl_scba_row* last, int* iter
     stats[3] = max_resident;
     stats[4] = builds;
   }
+  return QCL_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Tangent of the fixed point (implicit differentiation, forward mode).  At
+// the state of the last step, v solves v = Phi_Sigma v + s for a source s
+// (the explicit parameter derivative Phi_p, uploaded by the caller), by the
+// damped iteration v <- (1 - alpha) v + alpha (Phi_Sigma v + s), the
+// linearisation of the linear-mixing SCBA iteration itself.  Each tangent step
+// also returns the tangent of the current density, J_Sigma v.  Requires a
+// complex128 context with linear mixing and the paired normalisation.
+// ---------------------------------------------------------------------------
+enum { TS_DTRL = 0, TS_DTRG = 2, TS_DCOEF = 4, TS_FAM = 6 };
+static size_t tangent_scal_doubles(const ScbaCtx* c) { return TS_FAM + 2 * 3 * (c->M + 2) + 2 * (2 + 48) + 8; }
+
+int scba_tangent_init(ScbaCtx* c) {
+  if (c->precision != QCL_C128 || c->mixing || c->scalar_lesser) {
+    set_last_error("tangent: requires a complex128 context with linear mixing and the paired normalisation");
+    return QCL_UNSUPPORTED;
+  }
+  if (!c->tv.empty()) return QCL_OK;
+  const int nf = 3 * (c->M + 2);
+  int s;
+  for (auto* v : {&c->tv, &c->tw, &c->tsrc}) {
+    v->assign(nf, nullptr);
+    for (int i = 0; i < nf; ++i) {
+      if ((s = dalloc(&(*v)[i], c->fbytes))) return s;
+      QCL_CUDA_CHECK(cudaMemsetAsync((*v)[i], 0, c->fbytes, c->st));
+    }
+  }
+  for (int k = 0; k < 3; ++k) {
+    if ((s = dalloc(&c->tG[k], c->fbytes))) return s;
+    if ((s = dalloc(&c->ttot[k], c->fbytes))) return s;
+  }
+  if ((s = dalloc((void**)&c->ttrL, (size_t)c->NE * c->Nk * 16))) return s;
+  if ((s = dalloc((void**)&c->ttrG, (size_t)c->NE * c->Nk * 16))) return s;
+  if ((s = dalloc((void**)&c->tscal, tangent_scal_doubles(c) * sizeof(double)))) return s;
+  QCL_CUDA_CHECK(cudaMallocHost((void**)&c->tscal_h, tangent_scal_doubles(c) * sizeof(double)));
+  QCL_CUDA_CHECK(cudaStreamSynchronize(c->st));
+  return QCL_OK;
+}
+
+// which = 3 + 3 f + k (as qcl_scba_download): the source's family f component
+// k; host == NULL zeroes it.  which = -1 zeroes the tangent v itself.
+int scba_tangent_set(ScbaCtx* c, int which, const void* host) {
+  if (c->tv.empty()) {
+    set_last_error("tangent: call qcl_scba_tangent_init first");
+    return QCL_ARG;
+  }
+  if (which == -1) {
+    for (void* p : c->tv) QCL_CUDA_CHECK(cudaMemsetAsync(p, 0, c->fbytes, c->st));
+    QCL_CUDA_CHECK(cudaStreamSynchronize(c->st));
+    return QCL_OK;
+  }
+  const int idx = which - 3;
+  if (idx < 0 || idx >= (int)c->tsrc.size()) {
+    set_last_error("tangent: field index %d out of range", which);
+    return QCL_ARG;
+  }
+  if (host) QCL_CUDA_CHECK(cudaMemcpyAsync(c->tsrc[idx], host, c->fbytes, cudaMemcpyHostToDevice, c->st));
+  else QCL_CUDA_CHECK(cudaMemsetAsync(c->tsrc[idx], 0, c->fbytes, c->st));
+  QCL_CUDA_CHECK(cudaStreamSynchronize(c->st));
+  return QCL_OK;
+}
+
+// One tangent step at the state of the last SCBA step.  out[0] = J_Sigma v
+// (solver units, before the step's update: the tangent of the step's J),
+// out[1] = max over fields ||v_new - v|| / (||v_new|| + 1e-300).
+int scba_tangent_step(ScbaCtx* c, double* out) {
+  if (c->tv.empty() || !c->have_green) {
+    set_last_error("tangent: needs qcl_scba_tangent_init and a completed SCBA step");
+    return QCL_ARG;
+  }
+  int s;
+  const int F = c->M + 2, nf = 3 * F, NE = c->NE, Nk = c->Nk, N = c->N;
+  std::vector<void*>& st = c->parity == 0 ? c->state : c->cand;  // the linearisation point
+  // tangent totals
+  if ((s = totals(c, c->tv, c->ttot, 7))) return s;
+  // Dyson + Keldysh tangent
+  void *X = c->tG[0], *dL = c->tG[1], *dG = c->tG[2];
+  if ((s = launch_block_triple(NE, Nk, N, c->GR, c->ttot[0], c->GR, 0, 1.0, 0.0, X, nullptr, c->st))) return s;
+  const void* Sig[2] = {c->tot[1], c->tot[2]};
+  void* dOut[2] = {dL, dG};
+  Cx<double>* tr[2] = {c->ttrL, c->ttrG};
+  for (int k = 0; k < 2; ++k) {
+    if ((s = launch_block_triple(NE, Nk, N, X, Sig[k], c->GR, 1, 1.0, 0.0, dOut[k], nullptr, c->st))) return s;
+    if ((s = launch_block_triple(NE, Nk, N, c->GR, c->ttot[1 + k], c->GR, 1, 1.0, 1.0, dOut[k], nullptr, c->st)))
+      return s;
+    if ((s = launch_block_triple(NE, Nk, N, c->GR, Sig[k], X, 1, 1.0, 1.0, dOut[k], tr[k], c->st))) return s;
+  }
+  if ((s = launch_weighted_trace(NE, Nk, c->ttrL, c->wE, c->wk, c->rpartial, c->tscal + TS_DTRL, c->st))) return s;
+  if ((s = launch_weighted_trace(NE, Nk, c->ttrG, c->wE, c->wk, c->rpartial, c->tscal + TS_DTRG, c->st))) return s;
+  if ((s = launch_norm_tangent(c->nfield, c->GL, c->GG, c->scal + SC_COEF, c->tscal + TS_DTRL, c->tscal + TS_DTRG,
+                               c->gs, c->target, c->tscal + TS_DCOEF, dL, dG, c->st)))
+    return s;
+  // J tangent: J(v_plus, G) + J(Sigma_plus, dG)
+  double* jout = c->tscal + TS_FAM + 2 * nf;
+  if ((s = launch_observables(QCL_C128, NE, Nk, N, c->wE, c->wk, field_of(c->tv, c->M, 2), field_of(c->tv, c->M, 1),
+                              c->GL, c->GG, c->gs, c->target, c->obspartial, jout, c->st)))
+    return s;
+  if ((s = launch_observables(QCL_C128, NE, Nk, N, c->wE, c->wk, field_of(st, c->M, 2), field_of(st, c->M, 1), dL, dG,
+                              c->gs, c->target, c->obspartial, jout + 2 + N, c->st)))
+    return s;
+  // Phi_Sigma v: the linear candidate maps of the tangent Green's functions
+  if ((s = scattering_candidates(c, X, dL, dG, c->tw, false))) return s;
+  if ((s = embedding_candidates(c, c->tw, X, dL, dG))) return s;
+  // w <- Phi_Sigma v + s, then the damped update into w with the residual norms
+  const void* olds[kMaxMixFields];
+  void* cands[kMaxMixFields];
+  for (int i = 0; i < nf; ++i) {
+    if ((s = launch_axpby(QCL_C128, c->nfield, 1.0, c->tw[i], 1.0, c->tsrc[i], c->tw[i], c->st))) return s;
+    olds[i] = c->tv[i];
+    cands[i] = c->tw[i];
+  }
+  if ((s = launch_residual_mix_multi(QCL_C128, c->nfield, olds, cands, nf, c->alpha, c->mpartial, c->tscal + TS_FAM,
+                                     c->st)))
+    return s;
+  std::swap(c->tv, c->tw);
+  QCL_CUDA_CHECK(cudaMemcpyAsync(c->tscal_h, c->tscal, tangent_scal_doubles(c) * sizeof(double),
+                                 cudaMemcpyDeviceToHost, c->st));
+  QCL_CUDA_CHECK(cudaStreamSynchronize(c->st));
+  const double* h = c->tscal_h;
+  double r = 0;
+  for (int i = 0; i < nf; ++i) {
+    const double num = h[TS_FAM + 2 * i], den = h[TS_FAM + 2 * i + 1];
+    r = fmax(r, sqrt(num) / (sqrt(den) + 1e-300));
+  }
+  out[0] = h[TS_FAM + 2 * nf] + h[TS_FAM + 2 * nf + 2 + N];
+  out[1] = r;
+  return QCL_OK;
+}
+
+// The last step's mixed candidate family field (the speculative linear mix
+// (1 - alpha) Sigma + alpha Phi(Sigma) the next step would commit), for the
+// caller's difference quotient Phi_p; which as qcl_scba_download.
+int scba_download_candidate(ScbaCtx* c, int which, void* host) {
+  const int idx = which - 3;
+  if (!c->pending_commit || idx < 0 || idx >= 3 * (c->M + 2)) {
+    set_last_error("download_candidate: no pending step or field index %d out of range", which);
+    return QCL_ARG;
+  }
+  std::vector<void*>& cd = c->parity == 0 ? c->cand : c->state;
+  QCL_CUDA_CHECK(cudaStreamSynchronize(c->st));
+  QCL_CUDA_CHECK(cudaMemcpy(host, cd[idx], c->fbytes, cudaMemcpyDeviceToHost));
   return QCL_OK;
 }
 

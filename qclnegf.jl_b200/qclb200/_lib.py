@@ -163,6 +163,10 @@ def _declare(l):
         "qcl_debug_set_wait_limit": (I, [ctypes.c_longlong]),
         "qcl_autotune": (I, [I, I, I, I, P]),
         "qcl_sweep_create": (I, [I, P, P, Z, P]),
+        "qcl_scba_tangent_init": (I, [P]),
+        "qcl_scba_tangent_set": (I, [P, I, P]),
+        "qcl_scba_tangent_step": (I, [P, P]),
+        "qcl_scba_download_candidate": (I, [P, I, P]),
         "qcl_sweep_run": (I, [P, I, D, P, P, P]),
         "qcl_sweep_destroy": (None, [P]),
         "qcl_autotune_reset": (I, []),

@@ -463,7 +463,7 @@ def full_physics_problem(seed: int = 11, NE: int = 2048, Nk: int = 64, periods: 
                          Nqz: int = 401, Nphi: int = 64, lookup_nodes: int = 129, rtol: float = 1e-15,
                          alpha: float = 0.5, bias_mV: float = 50.0,
                          mechanisms=("LO", "acoustic", "impurity", "IFR", "alloy"),
-                         kernels=None) -> SCBAProblem:
+                         kernels=None, layers=(4.0, 8.5, 2.0, 16.0)) -> SCBAProblem:
     """Full-physics-shaped SCBA structure: a supercell of `periods` periods x
     `states` localised states (N_b = 32 by default) of the GaAs /
     Al0.15Ga0.85As stack 4.0 / 8.5 / 2.0 / 16.0 nm, N_E = 2048 energies over
@@ -495,7 +495,7 @@ def full_physics_problem(seed: int = 11, NE: int = 2048, Nk: int = 64, periods: 
 
     rng = np.random.default_rng(seed)
     Nb = periods * states
-    layers = [4.0, 8.5, 2.0, 16.0]
+    layers = [float(d) for d in layers]
     Ep = bias_mV * 1e-3 / E0_EV
     eps, wE = energy_grid(-0.25 / E0_EV, 0.40 / E0_EV, NE)
     Cbar = _kinetic_coefficient()
@@ -558,7 +558,10 @@ def full_physics_problem(seed: int = 11, NE: int = 2048, Nk: int = 64, periods: 
         mechs.append(Mechanism("IFR", "ifr", qifr, left=np.asfortranarray(left), right=right,
                                radial=np.asfortranarray(radial / qifr)))
     # alloy: Omega dV^2 x(1 - x) in the barriers (kernels.jl:285-319), Omega = a^3 / 4, dV = 0.6 eV
-    xal = np.where(np.isin(np.floor((x % Lp) / (Lp / 4)).astype(int), [1, 3]), 0.15, 0.0)
+    # barriers: the even layers of the stack (Al0.15Ga0.85As), wells the odd ones
+    edges = np.concatenate(([0.0], np.cumsum(layers) / L0_NM))
+    layer_of = np.clip(np.searchsorted(edges, x % Lp, side="right") - 1, 0, len(layers) - 1)
+    xal = np.where(layer_of % 2 == 0, 0.15, 0.0)
     pre_al = (0.565e-9) ** 3 / 4 * (0.6 * E_CHARGE) ** 2 / L0 / K0
     if kernels is None and "alloy" in want:
         Kal = acoustic_block(chi, wx * xal * (1 - xal), pre_al)

@@ -196,6 +196,13 @@ class ProductionSCBA:
         check(lib().qcl_scba_download(self._h, int(which), ctypes.c_void_p(out.ctypes.data)))
         return out
 
+    def download_candidate(self, which):
+        """A family field of the last step's mixed candidate
+        (1 - alpha) Sigma + alpha Phi(Sigma)."""
+        out = np.zeros(self.problem.shape, dtype=_CDT[self.precision], order="F")
+        check(lib().qcl_scba_download_candidate(self._h, int(which), ctypes.c_void_p(out.ctypes.data)))
+        return out
+
     def upload(self, which, array):
         a = _c(array, _CDT[self.precision])
         check(lib().qcl_scba_upload(self._h, int(which), ctypes.c_void_p(a.ctypes.data)))

@@ -93,10 +93,10 @@ function production_static_contraction(kind::Symbol, arrays::NamedTuple, G::Arra
                                        Σ::Array{ComplexF64,4} = zeros(ComplexF64, size(G)))
     NE, Nk, Nb, _ = size(G)
     k = kind === :momentum_independent ? 0 : kind === :dense ? 1 : kind === :ifr ? 2 :
-        kind === :low_rank ? 3 : throw(ArgumentError("unknown kernel kind $kind"))
+        kind === :low_rank ? 3 : kind === :separable_sum ? 4 : throw(ArgumentError("unknown kernel kind $kind"))
     GC.@preserve arrays begin
         p(name) = haskey(arrays, name) ? pointer(getfield(arrays, name)) : Ptr{ComplexF64}(C_NULL)
-        J = haskey(arrays, :left) ? size(arrays.left, 2) : 0
+        J = k == 4 ? size(arrays.radial, 3) : haskey(arrays, :left) ? size(arrays.left, 2) : 0
         op = Ref(Mechanism(k, 0, J, Float64(qᴷ), p(:block), p(:matrix), p(:left), p(:right), p(:radial)))
         check(ccall((:qcl_static_contraction, libqcl), Cint,
                     (Cint, Ref{Mechanism}, Cint, Cint, Cint, Ptr{Float64}, Float64, Float64,
@@ -180,6 +180,52 @@ end
 mutable struct Solver
     handle::Ptr{Cvoid}
     keep::Vector{Any}
+end
+
+"""The `Problem` struct and the mechanism operators of one fixed-point
+solve, from the reference's grids (ModelGrids ε, wᴱ, wᵏ), projected
+Hamiltonians h (N_k, N_b, N_b), neighbour couplings (BasisData.T₊, T₋) and
+scaled physics (Eᵖ, ħωᴸᴼ, N_LO, g_s, Nᴰ²ᴰ, η_seed, k_B T, α_Σ, J₀);
+`ops` = [(name, cached AbstractProductionKernel, qᴷ)] in the reference's
+mechanism order.  Every array is pushed to `keep` (rooted for the life of the
+solver).  Kernel types map to QCL_KERNEL_*: MomentumIndependent -> 0 (block),
+Dense -> 1 (matrix), _SeparableIFR -> 2 (left, right, radial), LowRank -> 3
+(left, right_adjoint); a wrapper with fields `radial`, `block` -> 4."""
+function problem_and_mechanisms(ε, wᴱ, wᵏ, h, T₊, T₋, Eᵖ, ħω, NLO, gs, target, ηseed, kBT, α, J₀, ops,
+                                keep::Vector{Any}; precision::Symbol = :c128)
+    prec = precision === :c128 ? QCL_C128 : precision === :c64 ? Cint(1) : Cint(2)
+    arrays = Any[Vector{Float64}(ε), Vector{Float64}(wᴱ), Vector{Float64}(wᵏ), Array{ComplexF64,3}(h),
+                 Matrix{ComplexF64}(T₊), Matrix{ComplexF64}(T₋)]
+    append!(keep, arrays)
+    mechs = Mechanism[]
+    nullp = Ptr{ComplexF64}(C_NULL)
+    for (name, op, q) in ops
+        isLO = Cint(name === :LO)
+        if hasfield(typeof(op), :radial) && hasfield(typeof(op), :block)       # separable sum
+            push!(keep, op.radial, op.block)
+            push!(mechs, Mechanism(4, isLO, size(op.radial, 3), q, pointer(op.block), nullp, nullp, nullp,
+                                   pointer(op.radial)))
+        elseif hasfield(typeof(op), :right_adjoint)                          # LowRankProductionKernel
+            push!(keep, op.left, op.right_adjoint)
+            push!(mechs, Mechanism(3, isLO, size(op.left, 2), q, nullp, nullp, pointer(op.left),
+                                   pointer(op.right_adjoint), nullp))
+        elseif hasfield(typeof(op), :radial)                                 # _SeparableIFRProductionKernel
+            push!(keep, op.left, op.right, op.radial)
+            push!(mechs, Mechanism(2, isLO, size(op.left, 2), q, nullp, nullp, pointer(op.left),
+                                   pointer(op.right), pointer(op.radial)))
+        elseif hasfield(typeof(op), :block)                                  # MomentumIndependent
+            push!(keep, op.block)
+            push!(mechs, Mechanism(0, isLO, 0, q, pointer(op.block), nullp, nullp, nullp, nullp))
+        else                                                                 # DenseProductionKernel
+            push!(keep, op.matrix)
+            push!(mechs, Mechanism(1, isLO, 0, q, nullp, pointer(op.matrix), nullp, nullp, nullp))
+        end
+    end
+    p = Problem(length(ε), size(h, 1), size(h, 2), pointer(arrays[1]), pointer(arrays[2]), pointer(arrays[3]),
+                pointer(arrays[4]), pointer(arrays[5]), pointer(arrays[6]), Eᵖ, ħω, NLO, Cint(gs), target,
+                ηseed, kBT, α, J₀, prec, Cint(1), Cint(length(mechs)), 0, 0, 0, 0, 0, 0, 5, 1.0, 1e-12,
+                Csize_t(0), Cint(0))
+    return p, mechs
 end
 
 function create(problem::Problem, mechanisms::Vector{Mechanism}, keep::Vector{Any})

@@ -154,7 +154,7 @@ struct TcArgs {
   int M;        // rows of C actually stored (N_E)
   int Ncols;    // real columns of C actually stored (2 Nc)
   int Kpad;     // padded real K (multiple of TC_BK)
-  Cx<float>* S; // element (row e, complex column j) at S[tc_out_index(e, j)]
+  Cx<float>* S; // element (row e, complex column j) at the output index below
   int NE;
   double alpha, beta;
   const float* ainv;  // 1 / s_e per row of A
@@ -165,9 +165,20 @@ struct TcArgs {
   long long oP, oQ, oR;
 };
 
-__device__ __forceinline__ size_t tc_out_index(const TcArgs& p, long long e, long long j) {
-  return (size_t)((e % p.oP) + p.oP * (j % p.oQ) + p.oP * p.oQ * (e / p.oP) + p.oP * p.oQ * p.oR * (j / p.oQ));
-}
+// The column part of the output index, walked j, j + 1, ... with j mod oQ and
+// j / oQ carried instead of divided per element (the row part is one per thread).
+struct TcColWalk {
+  long long r, q, step_r, step_q, oQ;
+  __device__ __forceinline__ TcColWalk(const TcArgs& p, long long j0)
+      : r(j0 % p.oQ), q(j0 / p.oQ), step_r(p.oP), step_q(p.oP * p.oQ * p.oR), oQ(p.oQ) {}
+  __device__ __forceinline__ long long offset() const { return step_r * r + step_q * q; }
+  __device__ __forceinline__ void next() {
+    if (++r == oQ) {
+      r = 0;
+      ++q;
+    }
+  }
+};
 
 // Warp roles: warps 0-7 read accumulators out (warp w: tensor-memory lanes
 // 32 (w % 4) .. + 31, columns 128 (w / 4) .. + 127) into FP32 running sums and
@@ -323,11 +334,13 @@ __global__ void __launch_bounds__(TC_THREADS, 1) tc_gemm_kernel(const __grid_con
       // no intermediate under- or overflows: one rounding to FP32, as before
       const double al = p.alpha * (double)p.ainv[e] * (double)__ldg(p.binv);
       const float be = (float)p.beta;
+      Cx<float>* row = p.S + ((e % p.oP) + p.oP * p.oQ * (e / p.oP));
+      TcColWalk col(p, (n0 + cbase) >> 1);  // n0 and cbase are even
 #pragma unroll
-      for (int q = 0; q < CH / 2; ++q) {
+      for (int q = 0; q < CH / 2; ++q, col.next()) {
         const int nn = n0 + cbase + 2 * q;
         if (nn >= p.Ncols) continue;
-        Cx<float>* dst = p.S + tc_out_index(p, e, nn >> 1);
+        Cx<float>* dst = row + col.offset();
         const float re = (float)(al * (double)sum[2 * q]), im = (float)(al * (double)sum[2 * q + 1]);
         if (p.beta == 0.0) {
           *dst = cx<float>(re, im);

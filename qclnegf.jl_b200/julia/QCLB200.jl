@@ -262,4 +262,94 @@ function download(s::Solver, which::Integer, shape::NTuple{4,Int})
     return out
 end
 
+upload!(s::Solver, which::Integer, X::Array{ComplexF64,4}) =
+    check(ccall((:qcl_scba_upload, libqcl), Cint, (Ptr{Cvoid}, Cint, Ptr{ComplexF64}), s.handle, which, X))
+
+function download_candidate(s::Solver, which::Integer, shape::NTuple{4,Int})
+    out = Array{ComplexF64,4}(undef, shape)
+    check(ccall((:qcl_scba_download_candidate, libqcl), Cint, (Ptr{Cvoid}, Cint, Ptr{ComplexF64}), s.handle,
+                which, out))
+    return out
+end
+
+# ---------------------------------------------------------------------------
+# Implicit differentiation of the converged fixed point (qcl_scba_tangent_*)
+# ---------------------------------------------------------------------------
+tangent_init!(s::Solver) = check(ccall((:qcl_scba_tangent_init, libqcl), Cint, (Ptr{Cvoid},), s.handle))
+tangent_set!(s::Solver, which::Integer, X::Array{ComplexF64,4}) =
+    check(ccall((:qcl_scba_tangent_set, libqcl), Cint, (Ptr{Cvoid}, Cint, Ptr{ComplexF64}), s.handle, which, X))
+tangent_reset!(s::Solver) =
+    check(ccall((:qcl_scba_tangent_set, libqcl), Cint, (Ptr{Cvoid}, Cint, Ptr{ComplexF64}), s.handle, -1, C_NULL))
+function tangent_step!(s::Solver)
+    out = zeros(2)
+    check(ccall((:qcl_scba_tangent_step, libqcl), Cint, (Ptr{Cvoid}, Ptr{Float64}), s.handle, out))
+    return out[1], out[2]  # J_Sigma v (solver units), largest relative change of v
+end
+
+"""A problem family for differentiation: `build(p)` returns
+`(problem, mechanisms, keep, shape)` for the parameter vector p (the bias, layer
+thicknesses, ...), `shape` = (N_E, N_k, N_b, N_b)."""
+const ProblemFamily = Function
+
+_families(nmech) = 3 .+ 3 .* (0:nmech+1)  # first component index of each self-energy family
+
+function _converged(build, p, tol, max_iter)
+    problem, mechs, keep, shape = build(p)
+    s = create(problem, mechs, keep)
+    seed!(s)
+    row = step!(s)
+    while row.r_Sigma > tol && row.nu < max_iter
+        row = step!(s)
+    end
+    row.r_Sigma <= tol || error("SCBA did not reach r_Sigma <= $tol in $max_iter iterations")
+    return s, row, problem, mechs, shape
+end
+
+# One application of the map Phi at the fixed-point state `fams` for the
+# problem at p: Phi per family component and J (the explicit dependence).
+function _map_at(build, p, fams, α)
+    problem, mechs, keep, shape = build(p)
+    s = create(problem, mechs, keep)
+    for (which, X) in fams
+        upload!(s, which, X)
+    end
+    row = step!(s)
+    phi = Dict(which => X .+ (download_candidate(s, which, shape) .- X) ./ α for (which, X) in fams)
+    return phi, row.J
+end
+
+"""dJ/dp at p0 by implicit differentiation of the FP64 fixed point
+(qcl_scba_tangent_*), with the explicit part Phi_p, J_p by central
+differences of ONE map application at the fixed point (steps[k] for p_k).
+Returns (J, dJ/dp)."""
+function implicit_gradient(build::ProblemFamily, p0::AbstractVector{<:Real}, steps::AbstractVector{<:Real};
+                           tol = 1e-11, max_iter = 20000, tangent_tol = 1e-11, max_tangent = 20000)
+    s, row, problem, mechs, shape = _converged(build, p0, tol, max_iter)
+    fams = [(which + c, download(s, which + c, shape)) for which in _families(length(mechs)) for c in 0:2]
+    tangent_init!(s)
+    grad = zeros(length(p0))
+    for k in eachindex(p0)
+        e = zeros(length(p0)); e[k] = steps[k]
+        φp, Jp = _map_at(build, p0 .+ e, fams, problem.alpha)
+        φm, Jm = _map_at(build, p0 .- e, fams, problem.alpha)
+        for (which, _) in fams
+            tangent_set!(s, which, (φp[which] .- φm[which]) ./ (2steps[k]))
+        end
+        tangent_reset!(s)
+        n, change = 0, Inf
+        while change > tangent_tol && n < max_tangent
+            _, change = tangent_step!(s)
+            n += 1
+        end
+        jv, _ = tangent_step!(s)
+        grad[k] = jv * problem.J0 + (Jp - Jm) / (2steps[k])
+    end
+    return row.J, grad
+end
+
+"""The converged current density J(p) of a problem family (the primal of
+the ChainRulesCore rrule in QCLB200ChainRulesExt)."""
+converged_current(build::ProblemFamily, p::AbstractVector{<:Real}; tol = 1e-11, max_iter = 20000) =
+    _converged(build, p, tol, max_iter)[2].J
+
 end # module

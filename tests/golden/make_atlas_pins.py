@@ -8,7 +8,15 @@ tests/golden/atlas_pins.npz:
   basis_envelopes.csv), against kernel_build.lo_form_factors;
 * one bordered periodic Poisson solve (hartree.csv, written by
   examples/10_physics_atlas.jl:256-282 with solve_periodic_poisson,
-  numerics/reference/poisson.jl:41-65), against outer.solve_periodic_poisson.
+  numerics/reference/poisson.jl:41-65), against outer.solve_periodic_poisson;
+* the non-interacting resolvent of the projected PzP-tail Hamiltonian
+  (basis_operators.csv, method pzp_tails: the 25 x 25 H of
+  examples/10_physics_atlas.jl:128-131), its eigen-energies (method energy,
+  the diagonal of C' H C), the central-period weight of each eigenstate
+  (basis_metrics.csv, method energy: 1 - outside_central_weight) and the
+  local density of states on the central rows (spectral_population.csv,
+  atlas lines 224-247: eta = 2 meV, 181 energies), summed over z, against
+  the Dyson solve G^R = ((E + i eta) I - H)^-1.
 
 The CSVs are output of the reference's Julia code (12 significant digits);
 they are read from the reference checkout, which only this script needs:
@@ -44,6 +52,22 @@ def main(ref):
     ff = rows(os.path.join(data, "form_factors.csv"))
     par = {r["name"]: float(r["value"]) for r in rows(os.path.join(data, "parameters.csv"))}
     har = rows(os.path.join(data, "hartree.csv"))
+    ops = rows(os.path.join(data, "basis_operators.csv"))
+    nb = max(int(r["a"]) for r in ops if r["method"] == "pzp_tails")
+    H = np.zeros((nb, nb), dtype=complex)
+    for r in ops:
+        if r["method"] == "pzp_tails":
+            H[int(r["a"]) - 1, int(r["b"]) - 1] = float(r["H_real_meV"]) + 1j * float(r["H_imag_meV"])
+    levels = np.array(sorted(float(r["H_real_meV"]) for r in ops if r["method"] == "energy" and r["a"] == r["b"]))
+    met = sorted((r for r in rows(os.path.join(data, "basis_metrics.csv")) if r["method"] == "energy"),
+                 key=lambda r: int(r["state"]))
+    central_weight = np.array([1.0 - float(r["outside_central_weight"]) for r in met])
+    spec = rows(os.path.join(data, "spectral_population.csv"))
+    E = sorted({float(r["energy_meV"]) for r in spec})
+    dz = float(par["period"]) / float(par["spatial_points_per_period"])
+    ldos = {e: 0.0 for e in E}
+    for r in spec:
+        ldos[float(r["energy_meV"])] += float(r["ldos_per_meV_nm"]) * dz
     np.savez_compressed(
         os.path.join(HERE, "atlas_pins.npz"),
         z_nm=z, psi_a=pa, psi_b=pb,
@@ -55,6 +79,8 @@ def main(ref):
         donors_m3=np.array([float(r["donors_m3"]) for r in har]),
         electrons_m3=np.array([float(r["electrons_m3"]) for r in har]),
         hartree_meV=np.array([float(r["hartree_meV"]) for r in har]),
+        H_pzp_meV=H, levels_meV=levels, central_weight=central_weight, eta_meV=2.0,
+        spectral_E_meV=np.array(E), central_dos_per_meV=np.array([ldos[e] for e in E]),
     )
 
 

@@ -12,14 +12,25 @@ tests/golden/atlas_pins.npz by tests/golden/make_atlas_pins.py:
 * hartree.csv: the Hartree energy of one bordered periodic Poisson solve for
   a trial electron profile (atlas lines 256-282, solve_periodic_poisson,
   numerics/reference/poisson.jl:41-65) -- the host Poisson step of the outer
-  loop (outer.solve_periodic_poisson).
+  loop (outer.solve_periodic_poisson);
+* basis_operators.csv / basis_metrics.csv / spectral_population.csv: the
+  projected 25 x 25 PzP-tail Hamiltonian, its eigen-energies, the
+  central-period weight of each eigenstate and the local density of states
+  on the central rows at eta = 2 meV (atlas lines 128-131, 224-247) -- the
+  retarded Dyson solve G^R = ((E + i eta) I - H)^-1 (_retarded_green_production,
+  numerics/optimized/production_operators.jl:1337-1385, with Sigma^R = 0):
+  tr G^R against sum_n 1 / (E + i eta - e_n), and the central density of
+  states sum_n w_n (-Im G_nn / pi) in the eigenbasis against the LDOS summed
+  over z.  CPU: the oracle's retarded_green; GPU: the Dyson kernel.
 
-The CSVs carry 12 significant digits; both agree to about 1e-12.
+The CSVs carry 12 significant digits; the form factors and the Hartree
+energy agree to about 1e-12, the spectral pins to about 1e-10.
 """
 import math
 import os
 
 import numpy as np
+import pytest
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 
@@ -59,3 +70,44 @@ def test_periodic_poisson_reproduces_reference_hartree_energy():
     assert np.max(np.abs(U * 100.0 - ref)) <= 1e-10 * np.max(np.abs(ref))
     assert rP < 1e-10 and neutrality < 1e-12  # the atlas's own checks (checks.csv)
     assert abs(np.sum(U)) / N < 1e-10
+
+
+def _spectral_checks(GR):
+    """Relative errors of tr G^R and of the central density of states against
+    the reference's spectral data; GR is (N_E, 1, 25, 25)."""
+    d = _pins()
+    E, eta = d["spectral_E_meV"], float(d["eta_meV"])
+    H = d["H_pzp_meV"]
+    _, V = np.linalg.eigh(0.5 * (H + H.conj().T))
+    tr = np.trace(GR[:, 0], axis1=1, axis2=2)
+    want_tr = np.array([np.sum(1.0 / (e + 1j * eta - d["levels_meV"])) for e in E])
+    Gn = np.einsum("an,eab,bn->en", V.conj(), GR[:, 0], V)
+    dos = -(Gn.imag / math.pi) @ d["central_weight"]
+    ref = d["central_dos_per_meV"]
+    return (float(np.max(np.abs(tr - want_tr)) / np.max(np.abs(want_tr))),
+            float(np.max(np.abs(dos - ref)) / np.max(ref)))
+
+
+def _spectral_inputs():
+    d = _pins()
+    E = np.asarray(d["spectral_E_meV"], dtype=np.float64)
+    h = np.asfortranarray(d["H_pzp_meV"][None, :, :])
+    sig = np.zeros((len(E), 1) + h.shape[1:], dtype=np.complex128, order="F")
+    return E, h, sig, float(d["eta_meV"])
+
+
+def test_oracle_dyson_reproduces_reference_spectrum(orc):
+    E, h, sig, eta = _spectral_inputs()
+    GR = orc.retarded_green(E, h, sig, eta=eta)[0]
+    err_tr, err_dos = _spectral_checks(GR)
+    assert err_tr < 1e-10 and err_dos < 1e-9, (err_tr, err_dos)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision,tol", [("c128", 1e-9), ("c64", 2e-5)])
+def test_gpu_dyson_reproduces_reference_spectrum(gpu_ops, precision, tol):
+    E, h, sig, eta = _spectral_inputs()
+    GR = gpu_ops.retarded_green(E, h, sig.astype(np.complex64) if precision == "c64" else sig, eta=eta,
+                                precision=precision)
+    err_tr, err_dos = _spectral_checks(np.asarray(GR, dtype=np.complex128))
+    assert err_tr < tol and err_dos < tol, (err_tr, err_dos)

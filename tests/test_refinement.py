@@ -144,6 +144,33 @@ def test_refined_mixed_run_reaches_the_fp64_fixed_point(gpu_ops):
 
 
 @pytest.mark.gpu
+def test_mixed_fixed_point_current_within_target_without_refinement(gpu_ops):
+    """The mixed-precision fixed point itself (no FP64 phase): run to the
+    r_Sigma floor of complex64 storage, its J is within 1e-6 relative of the
+    converged FP64 J (the north-star error target at convergence)."""
+    from qclb200.problem import small_problem
+    from qclb200.scba import ProductionSCBA
+
+    pr = dataclasses.replace(small_problem(NE=41, Nk=3, Nb=4, mechanisms=("LO", "acoustic", "IFR")), alpha=0.7)
+    f = ProductionSCBA(pr, precision="c128", use_graph=True)
+    f.seed()
+    rf = f.run(3000, 1e-10)
+    f.close()
+    assert rf[-1]["r_Sigma"] <= 1e-10
+    m = ProductionSCBA(pr, precision="mixed", use_graph=True)
+    m.seed()
+    rm = m.run(3000, 1e-6)
+    best = rm[-1]
+    for _ in range(100):  # on to the floor: the smallest r_Sigma of 100 more iterations
+        r = m.step()
+        if r["r_Sigma"] < best["r_Sigma"]:
+            best = r
+    m.close()
+    assert best["r_Sigma"] <= 1e-6
+    assert abs(best["J"] - rf[-1]["J"]) <= 1e-6 * abs(rf[-1]["J"])
+
+
+@pytest.mark.gpu
 @pytest.mark.parametrize("use_graph", [False, True])
 def test_phase_telemetry_times_every_phase(gpu_ops, use_graph):
     """Per-phase device times under the reference's phase names

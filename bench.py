@@ -635,10 +635,13 @@ def extras(torch, dev, L, _lib):
         else:
             res[precision].update(j_error(Jref, J))
         solver.close()
+    res["structure"] = ("tutorial-sized synthetic supercell (N_E x N_k = 400 x 16, N_b = 12, seeded levels and "
+                        "couplings; the reference's Schroedinger/PzP basis builder is not part of the path)")
     out["scba_tutorial_N12_30iter"] = res
     import traceback
 
-    for key, fn in (("scba_all_mechanisms", lambda: scba_all_mechanisms(torch)),
+    for key, fn in (("scba_fixed_point_small", lambda: scba_fixed_point_small(torch)),
+                    ("scba_all_mechanisms", lambda: scba_all_mechanisms(torch)),
                     ("scba_full_physics_N32", lambda: scba_full_physics(torch)),
                     ("bias_sweep_16", lambda: bias_sweep(torch, npoints=16, iters=4,
                                                          classes=((2, 8), (3, 8), (4, 8)),
@@ -739,6 +742,42 @@ def bias_sweep(torch, npoints=64, iters=5, classes=((2, 8), (3, 8), (4, 8), (6, 
                      f"LO + acoustic + IFR, mixed precision, {iters} iterations per point (seed and context "
                      "creation included in both wall times)")
     return res
+
+
+def scba_fixed_point_small(torch, tol=1e-10):
+    """J at the fixed point in each precision (N_E x N_k = 41 x 3, N_b = 4,
+    LO + acoustic + IFR, linear mixing 0.7): FP64 converged to r_Sigma <=
+    tol; mixed run to the floor of complex64 storage (the smallest r_Sigma of
+    100 iterations past 1e-6); mixed then promoted to FP64 and refined to
+    tol.  Relative J errors against the FP64 fixed point."""
+    import dataclasses
+
+    from qclb200.problem import small_problem
+    from qclb200.scba import ProductionSCBA
+
+    pr = dataclasses.replace(small_problem(NE=41, Nk=3, Nb=4, mechanisms=("LO", "acoustic", "IFR")), alpha=0.7)
+    f = ProductionSCBA(pr, precision="c128", use_graph=True)
+    f.seed()
+    rf = f.run(3000, tol)
+    f.close()
+    m = ProductionSCBA(pr, precision="mixed", use_graph=True, refinement=True)
+    m.seed()
+    rm = m.run(3000, 1e-6)
+    best = rm[-1]
+    for _ in range(100):
+        r = m.step()
+        rm.append(r)
+        if r["r_Sigma"] < best["r_Sigma"]:
+            best = r
+    m.promote()
+    rr = m.run(3000, tol)
+    m.close()
+    Jf = rf[-1]["J"]
+    return {"fp64_iterations": len(rf), "fp64_r_Sigma": rf[-1]["r_Sigma"], "J_fp64": Jf,
+            "mixed_iterations": len(rm), "mixed_floor_r_Sigma": best["r_Sigma"],
+            "J_rel_err_mixed_floor": abs(best["J"] - Jf) / abs(Jf),
+            "refined_fp64_iterations": len(rr), "refined_r_Sigma": rr[-1]["r_Sigma"],
+            "J_rel_err_refined": abs(rr[-1]["J"] - Jf) / abs(Jf)}
 
 
 def j_error(Jref, J):

@@ -39,6 +39,7 @@
 #include <cuda.h>  // CUtensorMap (the encoder is reached through cudaGetDriverEntryPoint)
 #include <cuda_fp16.h>
 
+#include <algorithm>
 #include <mutex>
 
 #include "kernels.cuh"
@@ -415,36 +416,51 @@ __global__ void tc_row_max_kernel(int NE, int Nc, long long P, long long Bs, con
 
 // A[e][2k + c] = s_e * part c of G[e + NE k] for k < Nc (zero in the padding),
 // split into fp16 hi / lo, s_e from the row maximum (rows past N_E: 1); the
-// first column of CTAs also writes ainv[e] = 1 / s_e.  A 32 x 32 (e, kk)
-// tile is transposed through shared memory so that both the E-fastest reads
-// and the K-contiguous writes are coalesced.
+// CTAs of the first K slice also write ainv[e] = 1 / s_e.  A CTA owns 32 rows
+// and walks K in tiles of 64 complex columns (128 real), gridDim.y tiles
+// apart: each complex value is read once (coalesced along e), the tile is
+// transposed through shared memory, and each row's 128 values are written as
+// half2 pairs (coalesced along K).
+constexpr int TC_SPLIT_KK = 128;
 __global__ void tc_split_a_kernel(int NE, int Nc, int Mpad, int Kpad, long long P, long long Bs,
                                   const Cx<float>* __restrict__ G,
                                   const unsigned* __restrict__ rowmax, __half* __restrict__ Ahi,
                                   __half* __restrict__ Alo, float* __restrict__ ainv) {
-  __shared__ float tile[32][33];
-  const int e0 = blockIdx.x * 32, kk0 = blockIdx.y * 32;
+  __shared__ float tile[TC_SPLIT_KK][33];
+  const int e0 = blockIdx.x * 32;
   const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;  // 32 x 8 threads
   const int er = e0 + tx;  // this thread's row in the read phase
-  const float sc = er < NE ? tc_scale_for(__uint_as_float(rowmax[er])) : 1.0f;
+  const bool rin = er < NE;
+  const float sc = rin ? tc_scale_for(__uint_as_float(rowmax[er])) : 1.0f;
   if (blockIdx.y == 0 && ty == 0 && er < Mpad) ainv[er] = 1.0f / sc;
-  for (int r = ty; r < 32; r += 8) {
-    // read: row kk = kk0 + r (fixed k, component), column e = e0 + tx (coalesced along e)
-    const int kk = kk0 + r;
-    float v = 0.0f;
-    const int k = kk >> 1;
-    if (er < NE && k < Nc) {
-      const Cx<float> g = G[(size_t)(er % P) + (size_t)P * k + (size_t)Bs * (size_t)(er / P)];
-      v = ((kk & 1) ? g.y : g.x) * sc;
+  const size_t rowbase = rin ? (size_t)(er % P) + (size_t)Bs * (size_t)(er / P) : 0;
+  for (int kk0 = blockIdx.y * TC_SPLIT_KK; kk0 < Kpad; kk0 += gridDim.y * TC_SPLIT_KK) {
+#pragma unroll
+    for (int q = 0; q < TC_SPLIT_KK / 16; ++q) {
+      const int kl = ty + 8 * q;  // complex column within the tile
+      const int k = (kk0 >> 1) + kl;
+      Cx<float> g = cx<float>(0.0f, 0.0f);
+      if (rin && k < Nc) g = G[rowbase + (size_t)P * k];
+      tile[2 * kl][tx] = g.x * sc;
+      tile[2 * kl + 1][tx] = g.y * sc;
     }
-    tile[r][tx] = v;
-  }
-  __syncthreads();
-  for (int r = ty; r < 32; r += 8) {
-    const int e = e0 + r, kk = kk0 + tx;
-    if (e >= Mpad || kk >= Kpad) continue;
-    const size_t idx = (size_t)e * Kpad + kk;
-    split_f16(tile[tx][r], Ahi[idx], Alo[idx]);
+    __syncthreads();
+    for (int r = ty; r < 32; r += 8) {
+      const int e = e0 + r;
+      if (e >= Mpad) continue;  // warp-uniform
+#pragma unroll
+      for (int h = tx; h < TC_SPLIT_KK / 2; h += 32) {
+        const int kk = kk0 + 2 * h;  // even, and Kpad is even
+        if (kk >= Kpad) continue;
+        __half h0, l0, h1, l1;
+        split_f16(tile[2 * h][r], h0, l0);
+        split_f16(tile[2 * h + 1][r], h1, l1);
+        const size_t idx = (size_t)e * Kpad + kk;
+        *reinterpret_cast<__half2*>(Ahi + idx) = __halves2half2(h0, h1);
+        *reinterpret_cast<__half2*>(Alo + idx) = __halves2half2(l0, l1);
+      }
+    }
+    __syncthreads();
   }
 }
 
@@ -643,7 +659,7 @@ int tc_split_rows(int M, int Kc, const void* A, long long P, long long Bs, float
   QCL_CUDA_CHECK(cudaMemsetAsync(rowmax, 0, (size_t)Mpad * sizeof(unsigned), st));
   tc_row_max_kernel<<<dim3(Mpad / 32, (Kc + 255) / 256), 256, 0, st>>>(M, Kc, P, Bs, (const Cx<float>*)A, rowmax);
   QCL_LAUNCH_CHECK("tc_row_max_kernel");
-  dim3 sg((Mpad + 31) / 32, (Kpad + 31) / 32);
+  dim3 sg((Mpad + 31) / 32, std::min((Kpad + TC_SPLIT_KK - 1) / TC_SPLIT_KK, 32));
   tc_split_a_kernel<<<sg, 256, 0, st>>>(M, Kc, Mpad, Kpad, P, Bs, (const Cx<float>*)A, rowmax, Ahi, Alo, ainv);
   QCL_LAUNCH_CHECK("tc_split_a_kernel");
   return QCL_OK;

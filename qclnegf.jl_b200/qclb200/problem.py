@@ -463,7 +463,8 @@ def full_physics_problem(seed: int = 11, NE: int = 2048, Nk: int = 64, periods: 
                          Nqz: int = 401, Nphi: int = 64, lookup_nodes: int = 129, rtol: float = 1e-15,
                          alpha: float = 0.5, bias_mV: float = 50.0,
                          mechanisms=("LO", "acoustic", "impurity", "IFR", "alloy"),
-                         kernels=None, layers=(4.0, 8.5, 2.0, 16.0)) -> SCBAProblem:
+                         kernels=None, layers=(4.0, 8.5, 2.0, 16.0), coupling_ev: float = 0.004,
+                         temperature_K: float = 100.0) -> SCBAProblem:
     """Full-physics-shaped SCBA structure: a supercell of `periods` periods x
     `states` localised states (N_b = 32 by default) of the GaAs /
     Al0.15Ga0.85As stack 4.0 / 8.5 / 2.0 / 16.0 nm, N_E = 2048 energies over
@@ -489,7 +490,10 @@ def full_physics_problem(seed: int = 11, NE: int = 2048, Nk: int = 64, periods: 
     mechanism list of an earlier call with the same seed, structure and N_k)
     is reused as is -- the kernels do not depend on the bias or the energy
     grid, as retarget_problem keeps them (composition/operating_point.jl:
-    25-150)."""
+    25-150).  `coupling_ev` is the scale of the random inter-period and
+    (x 0.2) intra-period couplings of the supercell Hamiltonian;
+    `temperature_K` the lattice temperature (phonon occupation, acoustic
+    kernel, k_B T of the seed)."""
     from .kernel_build import (impurity_pair_factors, lo_form_factors, lo_weights, lookup_weights,
                                separable_sum_operator, transfer_momenta)
 
@@ -502,14 +506,14 @@ def full_physics_problem(seed: int = 11, NE: int = 2048, Nk: int = 64, periods: 
     kmax = math.sqrt(0.080 / E0_EV / Cbar)
     kappa, wk = momentum_grid(kmax, Nk)
     levels = list(np.linspace(0.0, 0.24, states) + 0.004 * rng.standard_normal(states))
-    h0, Tplus, mix = _supercell(rng, periods, states, levels, Ep, 0.004)
+    h0, Tplus, mix = _supercell(rng, periods, states, levels, Ep, coupling_ev)
     h = np.zeros((Nk, Nb, Nb), dtype=np.complex128, order="F")
     for m in range(Nk):
         h[m] = h0 + Cbar * kappa[m] ** 2 * (np.eye(Nb) + mix)
     x, wx, chi, interfaces = _period_basis(rng, periods, states, layers)
     L0 = L0_NM * 1e-9
     K0 = (E0_EV * E_CHARGE) ** 2 * L0 ** 2
-    T_K = 100.0
+    T_K = float(temperature_K)
     hw = 0.0367
     mechs = []
     want = set(mechanisms)

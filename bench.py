@@ -56,7 +56,7 @@ def parse():
     ap.add_argument("--capture", choices=["dyson", "hilbert", "scba", "tcgemm", "scba_all_mixed", "scba_all_c128",
                                           "separable"],
                     help="run one small case of a kernel for an ncu capture (2 launches) and exit")
-    ap.add_argument("--study", choices=["full_physics_converged", "bias_sweep_64"],
+    ap.add_argument("--study", choices=["full_physics_converged", "all_mechanisms_converged", "bias_sweep_64"],
                     help="run one long study (seconds to minutes of GPU time), print its JSON and exit: the "
                          "full-physics SCBA converged in both precisions, or the 64-point batched bias sweep")
     return ap.parse_args()
@@ -936,31 +936,25 @@ def run_study(kind):
 
     if kind == "bias_sweep_64":
         out = bias_sweep(torch)
+    elif kind == "all_mechanisms_converged":
+        out = all_mechanisms_converged(torch)
     else:
         out = full_physics_converged(torch)
     print(json.dumps(out), flush=True)
 
 
-def full_physics_converged(torch, tol=1e-8, max_mixed=1500, max_fp64=1500, max_wall_s=2400.0,
-                           coupling_ev=0.02, temperature_K=300.0):
-    """The full-physics configuration converged to r_Sigma <= tol, at its
-    stated size and mechanisms.  The default structure's SCBA stalls near
-    r_Sigma ~ 7e-3 under linear mixing (4 meV couplings at 100 K: weakly
-    coupled populations), so the study uses the same builder with 20 meV
-    couplings at 300 K, which converges at about 0.97 per iteration.
-    (1) mixed precision from the seed until r_Sigma stops falling (its
-    complex64 floor), then promoted on the device to complex128
-    (qcl_scba_promote) and refined in FP64 to tol: the FP64 fixed point
-    J_fp;  (2) plain FP64 from the seed, bounded by max_wall_s.  Iterations,
-    device-synchronised wall seconds, traces, and the relative differences
-    against J_fp: the mixed floor's J, and (if it converged) plain FP64's."""
-    from qclb200.problem import full_physics_problem
+def converged_comparison(torch, pr, tol=1e-8, max_mixed=3000, max_fp64=3000, max_wall_s=2400.0):
+    """One problem converged to r_Sigma <= tol both ways.  (1) mixed
+    precision from the seed until r_Sigma stops falling (its complex64
+    floor: no 10 % progress over 20 iterations), then promoted on the device
+    to complex128 (qcl_scba_promote) and refined in FP64 to tol: the FP64
+    fixed point J_fp.  (2) plain FP64 from the seed to tol, bounded by
+    max_wall_s.  Iterations, device-synchronised wall seconds, r_Sigma
+    traces, and the relative J differences against J_fp of the mixed floor
+    and of plain FP64."""
     from qclb200.scba import ProductionSCBA
 
-    pr = full_physics_problem(coupling_ev=coupling_ev, temperature_K=temperature_K)
-    out = {"config": "N_b = 32, N_E x N_k = 2048 x 64, LO + acoustic + impurity + IFR + alloy, "
-                     f"couplings {coupling_ev * 1e3:g} meV, T = {temperature_K:g} K, linear mixing alpha = "
-                     f"{pr.alpha}, tolerance r_Sigma <= {tol}"}
+    out = {}
     t = time.perf_counter()
     m = ProductionSCBA(pr, precision="mixed", use_graph=True, refinement=True)
     m.seed()
@@ -972,7 +966,7 @@ def full_physics_converged(torch, tol=1e-8, max_mixed=1500, max_fp64=1500, max_w
         if best is None or r["r_Sigma"] < best["r_Sigma"]:
             best = r
         if len(rm) > 30 and min(x["r_Sigma"] for x in rm[-20:]) > 0.9 * best["r_Sigma"]:
-            break  # the complex64 floor: no progress over 20 iterations
+            break
     torch.cuda.synchronize()
     tm = time.perf_counter() - t
     m.promote()
@@ -1001,13 +995,46 @@ def full_physics_converged(torch, tol=1e-8, max_mixed=1500, max_fp64=1500, max_w
             break
     f.close()
     torch.cuda.synchronize()
-    out["fp64"] = {"iterations": len(rf), "wall_s": time.perf_counter() - t, "r_Sigma": rf[-1]["r_Sigma"],
-                   "J": rf[-1]["J"], "converged": rf[-1]["r_Sigma"] <= tol,
-                   "s_per_iter": (time.perf_counter() - t) / len(rf),
+    wall = time.perf_counter() - t
+    out["fp64"] = {"iterations": len(rf), "wall_s": wall, "r_Sigma": rf[-1]["r_Sigma"], "J": rf[-1]["J"],
+                   "converged": rf[-1]["r_Sigma"] <= tol, "s_per_iter": wall / len(rf),
                    "r_Sigma_trace": [r["r_Sigma"] for r in rf[::10]]}
     out["J_rel_diff_fp64_vs_fp64_fixed_point"] = abs(rf[-1]["J"] - Jfp) / abs(Jfp)
+    out["mixed_s_per_iter"] = tm / len(rm)
     if out["fp64"]["converged"]:
-        out["time_to_solution_speedup"] = out["fp64"]["wall_s"] / out["mixed_then_fp64"]["wall_s"]
+        out["time_to_solution_speedup"] = wall / out["mixed_then_fp64"]["wall_s"]
+    return out
+
+
+def full_physics_converged(torch, tol=1e-8, coupling_ev=0.02, temperature_K=300.0, **kw):
+    """The full-physics configuration at its stated size and mechanisms,
+    converged both ways (converged_comparison).  The default structure's
+    SCBA stalls near r_Sigma ~ 7e-3 under linear mixing (4 meV couplings at
+    100 K), so the study uses the same builder with 20 meV couplings at
+    300 K."""
+    from qclb200.problem import full_physics_problem
+
+    pr = full_physics_problem(coupling_ev=coupling_ev, temperature_K=temperature_K)
+    out = converged_comparison(torch, pr, tol=tol, **kw)
+    out["config"] = ("N_b = 32, N_E x N_k = 2048 x 64, LO + acoustic + impurity + IFR + alloy, "
+                     f"couplings {coupling_ev * 1e3:g} meV, T = {temperature_K:g} K, linear mixing alpha = "
+                     f"{pr.alpha}, tolerance r_Sigma <= {tol}")
+    return out
+
+
+def all_mechanisms_converged(torch, tol=1e-8, alpha=0.6, **kw):
+    """The all-mechanism case of the extras (N_E x N_k = 1024 x 32, N_b = 16,
+    LO + acoustic + impurity + IFR + alloy, dense LO and impurity maps)
+    converged both ways (converged_comparison)."""
+    import dataclasses
+
+    from qclb200.problem import small_problem
+
+    pr = dataclasses.replace(small_problem(NE=1024, Nk=32, Nb=16,
+                                           mechanisms=("LO", "acoustic", "impurity", "IFR", "alloy")), alpha=alpha)
+    out = converged_comparison(torch, pr, tol=tol, **kw)
+    out["config"] = ("N_E x N_k = 1024 x 32, N_b = 16, LO + acoustic + impurity + IFR + alloy (dense LO and "
+                     f"impurity maps), linear mixing alpha = {alpha}, tolerance r_Sigma <= {tol}")
     return out
 
 

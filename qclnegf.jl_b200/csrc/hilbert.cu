@@ -76,6 +76,35 @@ template <typename R, int t> __device__ __forceinline__ Cx<R> w16mul(Cx<R> z) {
   return cx<R>(z.x * c + z.y * s, z.y * c - z.x * s);
 }
 
+// z * W_32^k = z * exp(-2 pi i k / 32), k in [0, 16) (a compile-time value
+// once the caller's loop is unrolled): cos and sin of k pi / 16.
+template <typename R> __device__ __forceinline__ Cx<R> w32mul(Cx<R> z, int k) {
+  const R c1 = (R)0.98078528040323044913, s1 = (R)0.19509032201612826785;
+  const R c2 = (R)0.92387953251128675613, s2 = (R)0.38268343236508977173;
+  const R c3 = (R)0.83146961230254523708, s3 = (R)0.55557023301960222474;
+  const R c4 = (R)0.70710678118654752440;
+  R c, s;  // W = c - i s
+  switch (k & 15) {
+    case 0: return z;
+    case 1: c = c1; s = s1; break;
+    case 2: c = c2; s = s2; break;
+    case 3: c = c3; s = s3; break;
+    case 4: c = c4; s = c4; break;
+    case 5: c = s3; s = c3; break;
+    case 6: c = s2; s = c2; break;
+    case 7: c = s1; s = c1; break;
+    case 8: return cx<R>(z.y, -z.x);
+    case 9: c = -s1; s = c1; break;
+    case 10: c = -s2; s = c2; break;
+    case 11: c = -s3; s = c3; break;
+    case 12: c = -c4; s = c4; break;
+    case 13: c = -c3; s = s3; break;
+    case 14: c = -c2; s = s2; break;
+    default: c = -c1; s = s1; break;  // 15
+  }
+  return cx<R>(z.x * c + z.y * s, z.y * c - z.x * s);
+}
+
 template <int P> __host__ __device__ constexpr int bitrev(int i) {
   int r = 0;
   for (int b = 1; b < P; b <<= 1) {
@@ -126,10 +155,12 @@ template <int L> struct FftPlan {
 // result straight to global memory, without extra shared-memory sweeps.
 template <typename R> struct SmemIn {
   static constexpr bool kShared = true;
+  static constexpr bool kBatch = false;
   const Cx<R>* buf;
   __device__ __forceinline__ Cx<R> operator()(int i) const { return buf[fpad(i)]; }
 };
 template <typename R> struct SmemOut {
+  static constexpr bool kBatch = false;
   Cx<R>* buf;
   __device__ __forceinline__ void operator()(int t, Cx<R> v) const { buf[fpad(t)] = v; }
 };
@@ -216,8 +247,12 @@ __device__ __forceinline__ void stockham_pass(const In& in, const Out& out, cons
   for (int q = 0; q < Q; ++q) {
     const int j = tid + q * T;
     if (j < NB) {
+      if constexpr (In::kBatch) {
+        in.template batch<NB, RIN, RADIX>(j, v[q]);
+      } else {
 #pragma unroll
-      for (int r = 0; r < RIN; ++r) v[q][r] = in(j + r * NB);
+        for (int r = 0; r < RIN; ++r) v[q][r] = in(j + r * NB);
+      }
     }
   }
   if (In::kShared) __syncthreads();  // in place: every read before any write
@@ -234,8 +269,12 @@ __device__ __forceinline__ void stockham_pass(const In& in, const Out& out, cons
         DifStage<R, RADIX, RADIX / 2>::run(v[q]);
       }
       const int idxD = (j / NS) * NS * RADIX + k;
+      if constexpr (Out::kBatch) {
+        out.template batch<NS, RADIX>(idxD, v[q]);
+      } else {
 #pragma unroll
-      for (int r = 0; r < RADIX; ++r) out(idxD + r * NS, v[q][bitrev<RADIX>(r)]);
+        for (int r = 0; r < RADIX; ++r) out(idxD + r * NS, v[q][bitrev<RADIX>(r)]);
+      }
     }
   }
   __syncthreads();
@@ -400,9 +439,10 @@ __device__ __forceinline__ Cx<R> gamma_at(const HilbertArgs<R>& p, size_t idx) {
 // for e >= N_E; optionally copies Gam out.
 template <typename R> struct FieldIn {
   static constexpr bool kShared = false;
+  static constexpr bool kBatch = true;
   const HilbertArgs<R>* p;
   size_t base;
-  const Cx<R>* twist;  // per-sample phase, or null
+  const Cx<R>* twist;  // per-sample phase W_2L^e, or null
   __device__ __forceinline__ Cx<R> operator()(int e) const {
     if (e >= p->NE) return cx<R>(0, 0);
     Cx<R> g = gamma_at(*p, base + e);
@@ -413,10 +453,33 @@ template <typename R> struct FieldIn {
     }
     return (R)__ldg(p->wE + e) * g;
   }
+  // The first pass's inputs e = j + r NB, r < RIN (NB = L / RADIX).  In
+  // complex128 the twist W_2L^(j + r NB) = W_2L^j W_(2 RADIX)^r is one table
+  // load and a constant per r instead of RIN table loads.
+  template <int NB, int RIN, int RADIX> __device__ __forceinline__ void batch(int j, Cx<R>* v) const {
+    if (sizeof(R) == 4 || !twist) {
+#pragma unroll
+      for (int r = 0; r < RIN; ++r) v[r] = (*this)(j + r * NB);
+      return;
+    }
+    static_assert(RADIX <= 16 && 16 % RADIX == 0, "twist constants cover W_32");
+    const Cx<R> w0 = ldg_cx(twist + j);
+#pragma unroll
+    for (int r = 0; r < RIN; ++r) {
+      const int e = j + r * NB;
+      if (e >= p->NE) {
+        v[r] = cx<R>(0, 0);
+        continue;
+      }
+      const Cx<R> g = w32mul(gamma_at(*p, base + e) * w0, r * (16 / RADIX));
+      v[r] = (R)__ldg(p->wE + e) * g;
+    }
+  }
 };
 // Lam_e = conj(y[e + NE - 1]) / L straight to global memory (or the fused
 // SR_e = Lam_e - i Gam_e / 2); outputs outside [NE - 1, 2 NE - 2] are dropped.
 template <typename R> struct ResultOut {
+  static constexpr bool kBatch = false;
   const HilbertArgs<R>* p;
   size_t base;
   __device__ __forceinline__ void operator()(int t, Cx<R> v) const {
@@ -544,6 +607,7 @@ template <int LH> __device__ __forceinline__ int half_slot(int t, int NE) {
   return e < NE ? e : -1;
 }
 template <typename R, int LH> struct ParkOut {
+  static constexpr bool kBatch = false;
   const HilbertArgs<R>* p;
   size_t base;
   __device__ __forceinline__ void operator()(int t, Cx<R> v) const {
@@ -553,15 +617,16 @@ template <typename R, int LH> struct ParkOut {
   }
 };
 template <typename R, int LH> struct CompleteOut {
+  static constexpr bool kBatch = true;
   const HilbertArgs<R>* p;
   size_t base;
-  __device__ __forceinline__ void operator()(int t, Cx<R> v) const {
+  // d = v W_L^t (L = 2 LH) completes the parked even-half value
+  __device__ __forceinline__ void complete(int t, Cx<R> d) const {
     const int NE = p->NE;
     const int e = half_slot<LH>(t, NE);
     if (e < 0) return;
     Cx<R>* dst = p->SR ? p->SR : p->Lam;
     const Cx<R> a = dst[base + e];  // parked by this thread in the even half
-    const Cx<R> d = v * ldg_cx(p->tw + t);
     const Cx<R> y = t < NE - 1 ? a - d : a + d;
     const R sc = (R)p->scale_out;
     const Cx<R> lam = cx<R>(sc * y.x, -sc * y.y);
@@ -570,6 +635,20 @@ template <typename R, int LH> struct CompleteOut {
       p->SR[base + e] = cx<R>(lam.x + (R)0.5 * g.y, lam.y - (R)0.5 * g.x);
     } else {
       p->Lam[base + e] = lam;
+    }
+  }
+  __device__ __forceinline__ void operator()(int t, Cx<R> v) const { complete(t, v * ldg_cx(p->tw + t)); }
+  // The final pass's outputs t = t0 + r NS (t0 < NS = LH / RADIX): in
+  // complex128 W_L^t = W_L^t0 W_(2 RADIX)^r, one table load per thread.
+  template <int NS, int RADIX> __device__ __forceinline__ void batch(int t0, const Cx<R>* v) const {
+    if constexpr (sizeof(R) == 4 || NS * RADIX != LH) {
+#pragma unroll
+      for (int r = 0; r < RADIX; ++r) (*this)(t0 + r * NS, v[bitrev<RADIX>(r)]);
+    } else {
+      static_assert(RADIX <= 16 && 16 % RADIX == 0, "phase constants cover W_32");
+      const Cx<R> w0 = ldg_cx(p->tw + t0);
+#pragma unroll
+      for (int r = 0; r < RADIX; ++r) complete(t0 + r * NS, w32mul(v[bitrev<RADIX>(r)] * w0, r * (16 / RADIX)));
     }
   }
 };

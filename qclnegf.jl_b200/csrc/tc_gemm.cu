@@ -164,6 +164,10 @@ struct TcArgs {
   // output index (e mod oP) + oP (j mod oQ) + oP oQ (e / oP) + oP oQ oR (j / oQ);
   // oP = M and oQ larger than every j give the plain column-major e + M j
   long long oP, oQ, oR;
+  // tile order: 0 = row tiles fastest (blockIdx.x = row tile: the CTAs in
+  // flight share B tiles), 1 = column tiles fastest (blockIdx.x = column
+  // tile: they share A tiles, so an A larger than L2 is read once)
+  int cols_fastest;
 };
 
 // The column part of the output index, walked j, j + 1, ... with j mod oQ and
@@ -201,7 +205,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1) tc_gemm_kernel(const __grid_con
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(gbase + TC_STAGES * TC_STAGE_BYTES + 16 * TC_STAGES + 32);
   __shared__ volatile int s_fail;
 
-  const int m0 = blockIdx.x * TC_BM, n0 = blockIdx.y * BN;
+  const int m0 = (p.cols_fastest ? blockIdx.y : blockIdx.x) * TC_BM;
+  const int n0 = (p.cols_fastest ? blockIdx.x : blockIdx.y) * BN;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int nkb = p.Kpad / TC_BK;
   const int nch = (nkb + TC_ACC_KB - 1) / TC_ACC_KB;
@@ -631,7 +636,8 @@ template <int BN> static int launch_tc_t(const TcMaps& maps, const TcArgs& a, in
                                         TcShape<BN>::SMEM_BYTES));
     configured = true;
   }
-  dim3 grid(mtiles, (a.Ncols + BN - 1) / BN);
+  const int ntiles = (a.Ncols + BN - 1) / BN;
+  const dim3 grid = a.cols_fastest ? dim3(ntiles, mtiles) : dim3(mtiles, ntiles);
   tc_gemm_kernel<BN><<<grid, TC_THREADS, TcShape<BN>::SMEM_BYTES, st>>>(maps, a);
   QCL_LAUNCH_CHECK("tc_gemm_kernel");
   return QCL_OK;
@@ -687,7 +693,11 @@ int launch_tc_presplit(int M, int Nout, int Kc, const void* Bop, const float* aw
   // B rows past Npad (the last tile of a narrower width) read the zero fill
   if ((s = make_operand_map(&maps.bhi, Bhi, Npad, Kpad, bn))) return s;
   if ((s = make_operand_map(&maps.blo, Blo, Npad, Kpad, bn))) return s;
-  TcArgs a{M, 2 * Nout, Kpad, (Cx<float>*)S, M, alpha, beta, ainv, (const float*)b, status, oP, oQ, oR};
+  // the larger operand is read once: A larger than B (and than L2) streams
+  // with the column tiles fastest, else B does with the row tiles fastest
+  const int cols_fastest = (size_t)Mpad > (size_t)Npad && (size_t)Mpad * Kpad * 4 > (size_t)(96u << 20) &&
+                           mtiles <= 65535;
+  TcArgs a{M, 2 * Nout, Kpad, (Cx<float>*)S, M, alpha, beta, ainv, (const float*)b, status, oP, oQ, oR, cols_fastest};
   if (bn == 224) return launch_tc_t<224>(maps, a, mtiles, st);
   return launch_tc_t<256>(maps, a, mtiles, st);
 }

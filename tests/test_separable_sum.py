@@ -200,3 +200,20 @@ def test_scba_with_separable_operators_matches_dense_oracle(gpu_ops, orc, precis
     for ro, rg in zip(hist_o, hist_g):
         assert abs(rg["J"] - ro["J"]) <= tol * abs(ro["J"])
         assert abs(rg["r_Sigma"] - ro["rSigma"]) <= max(tol, 1e-6) * abs(ro["rSigma"]) + 1e-12
+
+
+@pytest.mark.gpu
+def test_separable_contraction_large_operands_c64_matches_c128(gpu_ops):
+    """Operands larger than L2 (stage 1: 524 288 rows x 64, 134 MB of FP16
+    pairs; stage 2: 65 536 rows x 4096, 1.07 GB), where the tensor-core
+    kernel runs its tiles column-fastest so that the large A is read once:
+    complex64 against the complex128 (DMMA) contraction of the same inputs,
+    which the literal-oracle tests above pin at small sizes."""
+    rng = np.random.default_rng(21)
+    NE, Nk, Nb = 2048, 32, 16
+    mech = _random_separable(rng, Nk, Nb, 8)
+    G = np.asfortranarray(rng.standard_normal((NE, Nk, Nb, Nb)) + 1j * rng.standard_normal((NE, Nk, Nb, Nb)))
+    wk = rng.uniform(0.2, 1.0, Nk)
+    ref = gpu_ops.production_static_contraction(mech, G, wk, alpha=0.9)
+    got = gpu_ops.production_static_contraction(mech, G, wk, alpha=0.9, precision="c64")
+    assert approx_err(got, ref) < 2e-6

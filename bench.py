@@ -946,7 +946,8 @@ def run_study(kind):
 def converged_comparison(torch, pr, tol=1e-8, max_mixed=3000, max_fp64=3000, max_wall_s=2400.0):
     """One problem converged to r_Sigma <= tol both ways.  (1) mixed
     precision from the seed until r_Sigma stops falling (its complex64
-    floor: no 10 % progress over 20 iterations), then promoted on the device
+    floor: the last 100 iterations did not get 10 % below the best before
+    them), then promoted on the device
     to complex128 (qcl_scba_promote) and refined in FP64 to tol: the FP64
     fixed point J_fp.  (2) plain FP64 from the seed to tol, bounded by
     max_wall_s.  Iterations, device-synchronised wall seconds, r_Sigma
@@ -965,7 +966,7 @@ def converged_comparison(torch, pr, tol=1e-8, max_mixed=3000, max_fp64=3000, max
         rm.append(r)
         if best is None or r["r_Sigma"] < best["r_Sigma"]:
             best = r
-        if len(rm) > 30 and min(x["r_Sigma"] for x in rm[-20:]) > 0.9 * best["r_Sigma"]:
+        if len(rm) > 100 and min(x["r_Sigma"] for x in rm[-100:]) > 0.9 * min(x["r_Sigma"] for x in rm[:-100]):
             break
     torch.cuda.synchronize()
     tm = time.perf_counter() - t

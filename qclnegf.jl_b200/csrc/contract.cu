@@ -300,6 +300,10 @@ struct DmArgs {
   Cx<double>* C;
   long long ldc;
   double alpha, beta;
+  // tile order: 0 = row tiles fastest (the CTAs in flight share B tiles),
+  // 1 = column tiles fastest (they share A tiles: an A larger than L2 is
+  // read once); set by launch_dmma_dense
+  int cols_fastest;
 };
 
 __device__ __forceinline__ void dm_cp16(Cx<double>* dst, const Cx<double>* src, bool valid) {
@@ -317,7 +321,8 @@ __global__ void __launch_bounds__(DM_THREADS, 2) dmma_dense_kernel(DmArgs p) {
   Cx<double>* As = reinterpret_cast<Cx<double>*>(dm_raw);   // [2][DM_BK][DM_APAD]
   Cx<double>* Bs = As + 2 * DM_BK * DM_APAD;                 // [2][DM_BK][DM_BPAD]
   double* ws = reinterpret_cast<double*>(Bs + 2 * DM_BK * DM_BPAD);  // [2][DM_BK]
-  const int m0 = blockIdx.x * DM_BM, n0 = blockIdx.y * DM_BN;
+  const int m0 = (p.cols_fastest ? blockIdx.y : blockIdx.x) * DM_BM;
+  const int n0 = (p.cols_fastest ? blockIdx.x : blockIdx.y) * DM_BN;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int wm = warp & 3, wn = warp >> 2;
   const int lr = lane >> 2, lc = lane & 3;
@@ -417,13 +422,18 @@ __global__ void __launch_bounds__(DM_THREADS, 2) dmma_dense_kernel(DmArgs p) {
   }
 }
 
-static int launch_dmma_dense(const DmArgs& a, cudaStream_t st) {
+static int launch_dmma_dense(const DmArgs& args, cudaStream_t st) {
   static bool configured = false;
   if (!configured) {
     QCL_CUDA_CHECK(cudaFuncSetAttribute(dmma_dense_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)DM_SMEM));
     configured = true;
   }
-  dim3 grid((a.M + DM_BM - 1) / DM_BM, (a.N + DM_BN - 1) / DM_BN);
+  DmArgs a = args;
+  const int mt = (a.M + DM_BM - 1) / DM_BM, nt = (a.N + DM_BN - 1) / DM_BN;
+  // the larger operand is read once: an A larger than B and than L2 streams
+  // with the column tiles fastest
+  a.cols_fastest = a.M > a.N && (size_t)a.M * a.K * sizeof(Cx<double>) > ((size_t)96 << 20) && mt <= 65535;
+  const dim3 grid = a.cols_fastest ? dim3(nt, mt) : dim3(mt, nt);
   dmma_dense_kernel<<<grid, DM_THREADS, DM_SMEM, st>>>(a);
   QCL_LAUNCH_CHECK("dmma_dense_kernel");
   return QCL_OK;

@@ -203,17 +203,26 @@ def test_scba_with_separable_operators_matches_dense_oracle(gpu_ops, orc, precis
 
 
 @pytest.mark.gpu
-def test_separable_contraction_large_operands_c64_matches_c128(gpu_ops):
+def test_separable_contraction_large_operands(gpu_ops):
     """Operands larger than L2 (stage 1: 524 288 rows x 64, 134 MB of FP16
-    pairs; stage 2: 65 536 rows x 4096, 1.07 GB), where the tensor-core
-    kernel runs its tiles column-fastest so that the large A is read once:
-    complex64 against the complex128 (DMMA) contraction of the same inputs,
-    which the literal-oracle tests above pin at small sizes."""
+    pairs; stage 2: 65 536 rows x 4096, 1.07 GB as FP16 pairs and 2.1 GB as
+    complex128), where the tensor-core and DMMA kernels run their tiles
+    column-fastest so that the large A is read once: both precisions against
+    the two stages of the Kronecker sum evaluated in numpy (complex128 1e-12,
+    complex64 2e-6)."""
     rng = np.random.default_rng(21)
-    NE, Nk, Nb = 2048, 32, 16
-    mech = _random_separable(rng, Nk, Nb, 8)
+    NE, Nk, Nb, J = 2048, 32, 16, 8
+    mech = _random_separable(rng, Nk, Nb, J)
     G = np.asfortranarray(rng.standard_normal((NE, Nk, Nb, Nb)) + 1j * rng.standard_normal((NE, Nk, Nb, Nb)))
     wk = rng.uniform(0.2, 1.0, Nk)
-    ref = gpu_ops.production_static_contraction(mech, G, wk, alpha=0.9)
-    got = gpu_ops.production_static_contraction(mech, G, wk, alpha=0.9, precision="c64")
-    assert approx_err(got, ref) < 2e-6
+    alpha = 0.9
+    Gf = G.reshape((NE, Nk, Nb * Nb), order="F") * wk[None, :, None]
+    want = np.zeros((NE, Nk, Nb * Nb), dtype=np.complex128)
+    for i in range(J):
+        Z = np.einsum("mn,enc->emc", mech.radial[:, :, i], Gf)  # stage 1
+        want += Z @ mech.block[:, :, i].T  # stage 2: S[e, m, ab] += sum_cd block[ab, cd] Z[e, m, cd]
+    want = (alpha * mech.q * want).reshape(G.shape, order="F")
+    got = gpu_ops.production_static_contraction(mech, G, wk, alpha=alpha)
+    assert approx_err(got, want) < 1e-12
+    got32 = gpu_ops.production_static_contraction(mech, G, wk, alpha=alpha, precision="c64")
+    assert approx_err(got32, want) < 2e-6

@@ -6,7 +6,7 @@ maps; the explicit dependence by one map application at p +- h) against
 central finite differences of the SCBA converged at p +- h, for the bias
 drop per period and the scattering strength of a small structure with LO
 (dense, with its energy shifts), acoustic and IFR scattering, within 1e-4
-relative (the north-star tolerance of the adjoint gradients); and the bias
+relative (the tolerance asked of the gradients); and the bias
 and four layer thicknesses of a full-physics-shaped stack with 20 meV
 couplings at 300 K.  (With the builder's default 4 meV couplings at 100 K
 these small stacks have a slow SCBA mode -- r_Sigma falls by 0.9995 per

@@ -18,7 +18,7 @@ import numpy as np
 import pytest
 
 
-def _config3_shapes(kind):
+def _full_physics_shapes(kind):
     """Problem shells at the full-physics size with the LO and impurity
     kernels dense or separable (arrays are not touched by the estimate)."""
     from qclb200.problem import Mechanism, SCBAProblem, energy_grid
@@ -47,21 +47,21 @@ def test_memory_estimate_full_physics_size():
 
     GB = 1e9
     field128 = 2048 * 64 * 32 * 32 * 16
-    dense = estimate_memory(_config3_shapes("dense"), precision="c128")
-    sep = estimate_memory(_config3_shapes("separable"), precision="c128")
+    dense = estimate_memory(_full_physics_shapes("dense"), precision="c128")
+    sep = estimate_memory(_full_physics_shapes("separable"), precision="c128")
     # state + candidate families (5 mechanisms + 2 embedding, 3 components), G, totals, two scratch fields
     assert sep["fields"] == (6 * 7 + 8) * field128
     # two dense (N_k N_b^2)^2 complex128 operators: 2 x 68.7 GB; separable: 24 x (N_k^2 + N_b^4) entries each
     assert dense["operators"] >= 2 * (64 * 1024) ** 2 * 16
     assert sep["operators"] < 2 * 24 * (64 * 64 + 1024 ** 2) * 16 + 8 * 1024 ** 2 * 16
     assert dense["peak"] > 180 * GB > sep["peak"]
-    mixed = estimate_memory(_config3_shapes("separable"), precision="mixed")
-    refine = estimate_memory(_config3_shapes("separable"), precision="mixed", refinement=True)
+    mixed = estimate_memory(_full_physics_shapes("separable"), precision="mixed")
+    refine = estimate_memory(_full_physics_shapes("separable"), precision="mixed", refinement=True)
     assert mixed["fields"] == sep["fields"] // 2
     assert refine["fields"] == sep["fields"]  # FP64-sized state for the promote
     assert refine["operators"] > mixed["operators"]  # complex128 operator copies
     assert refine["peak"] < 180 * GB
-    anderson = estimate_memory(dataclasses.replace(_config3_shapes("separable"), mixing="anderson"),
+    anderson = estimate_memory(dataclasses.replace(_full_physics_shapes("separable"), mixing="anderson"),
                                precision="c128")
     assert anderson["anderson"] == 2 * 5 * 21 * field128 + anderson["anderson"] % field128
 
@@ -147,7 +147,7 @@ def test_refined_mixed_run_reaches_the_fp64_fixed_point(gpu_ops):
 def test_mixed_fixed_point_current_within_target_without_refinement(gpu_ops):
     """The mixed-precision fixed point itself (no FP64 phase): run to the
     r_Sigma floor of complex64 storage, its J is within 1e-6 relative of the
-    converged FP64 J (the north-star error target at convergence)."""
+    converged FP64 J (the error target for J at convergence)."""
     from qclb200.problem import small_problem
     from qclb200.scba import ProductionSCBA
 

@@ -164,10 +164,11 @@ struct TcArgs {
   // output index (e mod oP) + oP (j mod oQ) + oP oQ (e / oP) + oP oQ oR (j / oQ);
   // oP = M and oQ larger than every j give the plain column-major e + M j
   long long oP, oQ, oR;
-  // tile order: 0 = row tiles fastest (blockIdx.x = row tile: the CTAs in
-  // flight share B tiles), 1 = column tiles fastest (blockIdx.x = column
-  // tile: they share A tiles, so an A larger than L2 is read once)
+  // linear tile order: 0 = row tiles fastest (the CTAs in flight share B
+  // tiles), 1 = column tiles fastest (they share A tiles, so an A larger than
+  // L2 is read once)
   int cols_fastest;
+  int mtiles;  // row tiles (M padded to TC_BM)
 };
 
 // The column part of the output index, walked j, j + 1, ... with j mod oQ and
@@ -205,11 +206,23 @@ __global__ void __launch_bounds__(TC_THREADS, 1) tc_gemm_kernel(const __grid_con
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(gbase + TC_STAGES * TC_STAGE_BYTES + 16 * TC_STAGES + 32);
   __shared__ volatile int s_fail;
 
-  const int m0 = (p.cols_fastest ? blockIdx.y : blockIdx.x) * TC_BM;
-  const int n0 = (p.cols_fastest ? blockIdx.x : blockIdx.y) * BN;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int nkb = p.Kpad / TC_BK;
-  const int nch = (nkb + TC_ACC_KB - 1) / TC_ACC_KB;
+  // persistent: this CTA's tiles are blockIdx.x + i gridDim.x (i < ntile) in
+  // the linear tile order; its K blocks and accumulation groups are counted
+  // across its tiles, so the ring stages, the two accumulators and their
+  // barrier phases run on from one tile to the next, and the epilogue of a
+  // tile overlaps the loads and MMAs of the next
+  const int nkb = p.Kpad / TC_BK;  // K blocks per tile
+  const int nch = (nkb + TC_ACC_KB - 1) / TC_ACC_KB;  // accumulation groups per tile
+  const int ntiles_n = (p.Ncols + BN - 1) / BN;
+  const long long tiles = (long long)p.mtiles * ntiles_n;
+  const int ntile = blockIdx.x < tiles ? (int)((tiles - 1 - blockIdx.x) / gridDim.x + 1) : 0;
+  const int mtiles = p.mtiles, cols_fastest = p.cols_fastest;
+  const auto tile_origin = [mtiles, ntiles_n, cols_fastest](int i, int& m0, int& n0) {
+    const int t = (int)blockIdx.x + i * (int)gridDim.x;  // tiles < 2^31
+    m0 = (cols_fastest ? t / ntiles_n : t % mtiles) * TC_BM;
+    n0 = (cols_fastest ? t % ntiles_n : t / mtiles) * BN;
+  };
   const long long lim = g_tc_main_wait_limit;
   if (threadIdx.x == 0) {
     for (int i = 0; i < TC_STAGES; ++i) {
@@ -239,8 +252,10 @@ __global__ void __launch_bounds__(TC_THREADS, 1) tc_gemm_kernel(const __grid_con
   if (warp == TC_DRAIN_WARPS) {
     // ---- producer ---------------------------------------------------------
     if (lane == 0) {
-      for (int kb = 0; kb < nkb && !s_fail; ++kb) {
-        const int s = kb % TC_STAGES;
+      for (int kb = 0; kb < ntile * nkb && !s_fail; ++kb) {  // kb: this CTA's K blocks over its tiles
+        const int s = kb % TC_STAGES, kt = kb % nkb;
+        int m0, n0;
+        tile_origin(kb / nkb, m0, n0);
         if (kb >= TC_STAGES && !mbar_wait(empty + 8 * s, (uint32_t)((kb / TC_STAGES - 1) & 1), lim)) {
           s_fail = 1;
           break;
@@ -248,18 +263,19 @@ __global__ void __launch_bounds__(TC_THREADS, 1) tc_gemm_kernel(const __grid_con
         loaded = kb + 1;
         const uint32_t st = base + s * TC_STAGE_BYTES;
         mbar_expect_tx(full + 8 * s, TC_STAGE_BYTES);
-        tma_load(st, &maps.ahi, kb * TC_BK, m0, full + 8 * s);
-        tma_load(st + TC_A_BYTES, &maps.alo, kb * TC_BK, m0, full + 8 * s);
-        tma_load(st + 2 * TC_A_BYTES, &maps.bhi, kb * TC_BK, n0, full + 8 * s);
-        tma_load(st + 2 * TC_A_BYTES + TC_B_BYTES, &maps.blo, kb * TC_BK, n0, full + 8 * s);
+        tma_load(st, &maps.ahi, kt * TC_BK, m0, full + 8 * s);
+        tma_load(st + TC_A_BYTES, &maps.alo, kt * TC_BK, m0, full + 8 * s);
+        tma_load(st + 2 * TC_A_BYTES, &maps.bhi, kt * TC_BK, n0, full + 8 * s);
+        tma_load(st + 2 * TC_A_BYTES + TC_B_BYTES, &maps.blo, kt * TC_BK, n0, full + 8 * s);
       }
     }
   } else if (warp == TC_DRAIN_WARPS + 1) {
     // ---- MMA issue --------------------------------------------------------
     if (lane == 0) {
-      for (int kb = 0; kb < nkb && !s_fail; ++kb) {
-        const int s = kb % TC_STAGES, ch = kb / TC_ACC_KB, b = ch & 1;
-        const bool first = kb % TC_ACC_KB == 0, last = (kb % TC_ACC_KB == TC_ACC_KB - 1) || kb == nkb - 1;
+      for (int kb = 0; kb < ntile * nkb && !s_fail; ++kb) {
+        // group ch counts this CTA's accumulation groups over its tiles
+        const int kt = kb % nkb, s = kb % TC_STAGES, ch = (kb / nkb) * nch + kt / TC_ACC_KB, b = ch & 1;
+        const bool first = kt % TC_ACC_KB == 0, last = (kt % TC_ACC_KB == TC_ACC_KB - 1) || kt == nkb - 1;
         if (!mbar_wait(full + 8 * s, (uint32_t)((kb / TC_STAGES) & 1), lim) ||
             (first && ch >= 2 && !mbar_wait(acc_empty + 8 * b, (uint32_t)(((ch - 2) >> 1) & 1), lim))) {
           s_fail = 1;
@@ -294,12 +310,15 @@ __global__ void __launch_bounds__(TC_THREADS, 1) tc_gemm_kernel(const __grid_con
     constexpr int CH = S::CH, LDW = S::LDW;
     const uint32_t tlane = (uint32_t)((warp & 3) * 32) << 16;
     const int cbase = (warp >> 2) * CH;
+    bool ok = true;
+    for (int it = 0; it < ntile && ok; ++it) {
+    int m0, n0;
+    tile_origin(it, m0, n0);
     float sum[CH];
 #pragma unroll
     for (int i = 0; i < CH; ++i) sum[i] = 0.0f;
-    bool ok = true;
-    for (int ch = 0; ch < nch; ++ch) {
-      const int b = ch & 1;
+    for (int cl = 0; cl < nch; ++cl) {
+      const int ch = it * nch + cl, b = ch & 1;
       // warp-uniform decision: the tensor-memory loads below are .sync.aligned
       const bool stop = __any_sync(0xffffffffu, s_fail != 0);
       const bool got = __all_sync(0xffffffffu, !stop && mbar_wait(acc_full + 8 * b, (uint32_t)((ch >> 1) & 1), lim));
@@ -356,10 +375,11 @@ __global__ void __launch_bounds__(TC_THREADS, 1) tc_gemm_kernel(const __grid_con
         }
       }
     }
+    }  // tiles
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
-  if (threadIdx.x == 0 && s_fail) record_status(p.status, QCL_TIMEOUT, (long long)blockIdx.x + 65536ll * blockIdx.y);
+  if (threadIdx.x == 0 && s_fail) record_status(p.status, QCL_TIMEOUT, (long long)blockIdx.x);
   if (warp == TC_DRAIN_WARPS + 1)
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TC_TMEM_COLS) : "memory");
   // After a failure (s_fail is final past the barrier above) copies may still be
@@ -636,9 +656,14 @@ template <int BN> static int launch_tc_t(const TcMaps& maps, const TcArgs& a, in
                                         TcShape<BN>::SMEM_BYTES));
     configured = true;
   }
-  const int ntiles = (a.Ncols + BN - 1) / BN;
-  const dim3 grid = a.cols_fastest ? dim3(ntiles, mtiles) : dim3(mtiles, ntiles);
-  tc_gemm_kernel<BN><<<grid, TC_THREADS, TcShape<BN>::SMEM_BYTES, st>>>(maps, a);
+  TcArgs b = a;
+  b.mtiles = mtiles;
+  const long long tiles = (long long)mtiles * ((a.Ncols + BN - 1) / BN);
+  int sms = 148;
+  int dev = 0;
+  if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const int grid = (int)std::min<long long>(tiles, sms);  // one persistent CTA per SM
+  tc_gemm_kernel<BN><<<grid, TC_THREADS, TcShape<BN>::SMEM_BYTES, st>>>(maps, b);
   QCL_LAUNCH_CHECK("tc_gemm_kernel");
   return QCL_OK;
 }
@@ -695,8 +720,7 @@ int launch_tc_presplit(int M, int Nout, int Kc, const void* Bop, const float* aw
   if ((s = make_operand_map(&maps.blo, Blo, Npad, Kpad, bn))) return s;
   // the larger operand is read once: A larger than B (and than L2) streams
   // with the column tiles fastest, else B does with the row tiles fastest
-  const int cols_fastest = (size_t)Mpad > (size_t)Npad && (size_t)Mpad * Kpad * 4 > (size_t)(96u << 20) &&
-                           mtiles <= 65535;
+  const int cols_fastest = (size_t)Mpad > (size_t)Npad && (size_t)Mpad * Kpad * 4 > (size_t)(96u << 20);
   TcArgs a{M, 2 * Nout, Kpad, (Cx<float>*)S, M, alpha, beta, ainv, (const float*)b, status, oP, oQ, oR, cols_fastest};
   if (bn == 224) return launch_tc_t<224>(maps, a, mtiles, st);
   return launch_tc_t<256>(maps, a, mtiles, st);

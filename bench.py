@@ -56,7 +56,8 @@ def parse():
     ap.add_argument("--capture", choices=["dyson", "hilbert", "scba", "tcgemm", "scba_all_mixed", "scba_all_c128",
                                           "separable"],
                     help="run one small case of a kernel for an ncu capture (2 launches) and exit")
-    ap.add_argument("--study", choices=["full_physics_converged", "all_mechanisms_converged", "bias_sweep_64"],
+    ap.add_argument("--study", choices=["full_physics_converged", "full_physics_converged_mixed",
+                                        "all_mechanisms_converged", "bias_sweep_64"],
                     help="run one long study (seconds to minutes of GPU time), print its JSON and exit: the "
                          "full-physics SCBA converged in both precisions, or the 64-point batched bias sweep")
     return ap.parse_args()
@@ -938,13 +939,15 @@ def run_study(kind):
         out = bias_sweep(torch)
     elif kind == "all_mechanisms_converged":
         out = all_mechanisms_converged(torch)
+    elif kind == "full_physics_converged_mixed":
+        out = full_physics_converged(torch, plain_fp64=False)
     else:
         out = full_physics_converged(torch)
     print(json.dumps(out), flush=True)
 
 
 def converged_comparison(torch, pr, tol=1e-8, max_mixed=3000, max_fp64=3000, max_wall_s=2400.0,
-                         max_refine_s=1200.0):
+                         max_refine_s=1200.0, plain_fp64=True):
     """One problem converged to r_Sigma <= tol both ways.  (1) mixed
     precision from the seed until r_Sigma stops falling (its complex64
     floor: the last 100 iterations did not get 10 % below the best before
@@ -957,6 +960,12 @@ def converged_comparison(torch, pr, tol=1e-8, max_mixed=3000, max_fp64=3000, max
     from qclb200.scba import ProductionSCBA
 
     out = {}
+
+    def progress(leg, n, r):
+        if n % 25 == 0:
+            print(json.dumps({"leg": leg, "iteration": n, "r_Sigma": r["r_Sigma"], "J": r["J"]}), file=sys.stderr,
+                  flush=True)
+
     t = time.perf_counter()
     m = ProductionSCBA(pr, precision="mixed", use_graph=True, refinement=True)
     m.seed()
@@ -965,6 +974,7 @@ def converged_comparison(torch, pr, tol=1e-8, max_mixed=3000, max_fp64=3000, max
     while len(rm) < max_mixed:
         r = m.step()
         rm.append(r)
+        progress("mixed", len(rm), r)
         if best is None or r["r_Sigma"] < best["r_Sigma"]:
             best = r
         if len(rm) > 100 and min(x["r_Sigma"] for x in rm[-100:]) > 0.9 * min(x["r_Sigma"] for x in rm[:-100]):
@@ -976,6 +986,7 @@ def converged_comparison(torch, pr, tol=1e-8, max_mixed=3000, max_fp64=3000, max
     t1 = time.perf_counter()
     while len(rr) < max_fp64 and time.perf_counter() - t1 < max_refine_s:
         rr.append(m.step())
+        progress("refine", len(rr), rr[-1])
         if rr[-1]["r_Sigma"] <= tol:
             break
     m.close()
@@ -988,12 +999,17 @@ def converged_comparison(torch, pr, tol=1e-8, max_mixed=3000, max_fp64=3000, max
                               "mixed_r_Sigma_trace": [x["r_Sigma"] for x in rm[::10]],
                               "fp64_r_Sigma_trace": [x["r_Sigma"] for x in rr[::5]]}
     out["J_rel_err_mixed_floor_vs_fp64_fixed_point"] = abs(best["J"] - Jfp) / abs(Jfp)
+    out["mixed_s_per_iter"] = tm / len(rm)
+    print(json.dumps(out), flush=True)  # the first leg, in case the second is cut short
+    if not plain_fp64:
+        return out
     t = time.perf_counter()
     f = ProductionSCBA(pr, precision="c128", use_graph=True)
     f.seed()
     rf = []
     while len(rf) < max_fp64 and time.perf_counter() - t < max_wall_s:
         rf.append(f.step())
+        progress("fp64", len(rf), rf[-1])
         if rf[-1]["r_Sigma"] <= tol:
             break
     f.close()
@@ -1003,7 +1019,6 @@ def converged_comparison(torch, pr, tol=1e-8, max_mixed=3000, max_fp64=3000, max
                    "converged": rf[-1]["r_Sigma"] <= tol, "s_per_iter": wall / len(rf),
                    "r_Sigma_trace": [r["r_Sigma"] for r in rf[::10]]}
     out["J_rel_diff_fp64_vs_fp64_fixed_point"] = abs(rf[-1]["J"] - Jfp) / abs(Jfp)
-    out["mixed_s_per_iter"] = tm / len(rm)
     if out["fp64"]["converged"]:
         out["time_to_solution_speedup"] = wall / out["mixed_then_fp64"]["wall_s"]
     return out

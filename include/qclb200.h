@@ -508,6 +508,17 @@ int qcl_scba_tangent_init(qcl_scba* ctx);
 int qcl_scba_tangent_set(qcl_scba* ctx, int which, const void* host);
 int qcl_scba_tangent_step(qcl_scba* ctx, double* out);
 int qcl_scba_download_candidate(qcl_scba* ctx, int which, void* host);
+/* The form of the paired number normalisation (_paired_number_coefficients,
+ * numerics/reference/greens.jl:155-199): the reference scales G< when the
+ * raw number is at or above the target (form 1) and otherwise moves G>
+ * weight into G< (form 2).  A particle-conserving fixed point sits on that
+ * switch, so the explicit part Phi_p of a derivative must keep the fixed
+ * point's form on both sides of p: qcl_scba_normalization_branch returns
+ * the form the last step used (1 or 2) and
+ * qcl_scba_set_normalization_branch forces one (0 restores the reference's
+ * choice). */
+int qcl_scba_set_normalization_branch(qcl_scba* ctx, int branch);
+int qcl_scba_normalization_branch(qcl_scba* ctx, int* branch);
 
 /* Batched sweep of independent operating points: a bias sweep, or points of
  * different structures (basis sizes, energy grids).  The reference solves

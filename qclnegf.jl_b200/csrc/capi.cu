@@ -151,6 +151,8 @@ int scba_tangent_init(ScbaCtx* c);
 int scba_tangent_set(ScbaCtx* c, int which, const void* host);
 int scba_tangent_step(ScbaCtx* c, double* out);
 int scba_download_candidate(ScbaCtx* c, int which, void* host);
+int scba_set_norm_branch(ScbaCtx* c, int branch);
+int scba_norm_branch(ScbaCtx* c, int* out);
 struct Sweep;
 int sweep_create(int n, const qcl_scba_problem* problems, const qcl_mechanism* const* mechanisms, size_t budget,
                  Sweep** out);
@@ -820,6 +822,22 @@ int qcl_scba_download_candidate(qcl_scba* ctx, int which, void* host) {
     return QCL_ARG;
   }
   return scba_download_candidate((ScbaCtx*)ctx, which, host);
+}
+
+int qcl_scba_set_normalization_branch(qcl_scba* ctx, int branch) {
+  if (!ctx) {
+    set_last_error("ctx is required");
+    return QCL_ARG;
+  }
+  return scba_set_norm_branch((ScbaCtx*)ctx, branch);
+}
+
+int qcl_scba_normalization_branch(qcl_scba* ctx, int* branch) {
+  if (!ctx || !branch) {
+    set_last_error("ctx and branch are required");
+    return QCL_ARG;
+  }
+  return scba_norm_branch((ScbaCtx*)ctx, branch);
 }
 
 int qcl_debug_set_wait_limit(long long rounds) { return tc_set_wait_limit(rounds); }

@@ -27,7 +27,8 @@ void dyson_set_bpc(int precision, int NP, int bpc);
 int launch_weighted_trace(int NE, int Nk, const void* tr, const double* wE, const double* wk, double* partial,
                           double* out, cudaStream_t st);
 int launch_paired_coefficients(const double* trL, const double* trG, int gs, double target, double* coeffs,
-                               int* status, cudaStream_t st, double realness_limit = 1e-10, int scalar = 0);
+                               int* status, cudaStream_t st, double realness_limit = 1e-10, int scalar = 0,
+                               int branch = 0);
 int launch_density_matrix(int precision, int NE, int Nk, int N, const void* GL, const double* wE, const double* wk,
                           double* out, cudaStream_t st);
 int launch_scalar_lesser(int precision, int NE, int Nk, int N, const void* GR, void* GL, void* GG,
@@ -206,7 +207,7 @@ int launch_convert(int precision, size_t n, const void* in_c128, void* out, cuda
 int launch_block_triple(int NE, int Nk, int N, const void* A, const void* B, const void* C, int adjC, double alpha,
                         double beta, void* out, void* trace, cudaStream_t st);
 int launch_norm_tangent(size_t n, const void* Ln, const void* Gn, const double* coeffs, const double* dtrL,
-                        const double* dtrG, int gs, double target, double* dcoef, void* dL, void* dG,
+                        const double* dtrG, int gs, double target, int branch, double* dcoef, void* dL, void* dG,
                         cudaStream_t st);
 int launch_promote(size_t n, const void* in_c64, void* out_c128, cudaStream_t st);
 int launch_antihermitian_part(int NE, int Nk, int N, void* X, cudaStream_t st);

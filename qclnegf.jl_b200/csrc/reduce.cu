@@ -99,8 +99,12 @@ int launch_weighted_trace(int NE, int Nk, const void* tr, const double* wE, cons
 // :scalar_lesser comparator (production_state.jl:54-61): only N and lambda
 // are checked (the reference never forms H there), a = 1, c = 0.
 // ---------------------------------------------------------------------------
+// branch: 0 = the reference's choice (scale G< when number >= target, else
+// move G> weight into it); 1 or 2 forces the first or the second form (its
+// formula continued across the switch), for a derivative whose explicit part
+// must stay on the branch of the fixed point.
 __global__ void paired_coefficients_kernel(const double* trL, const double* trG, int gs, double target,
-                                           double limit, double* coeffs, int* status, int scalar) {
+                                           double limit, double* coeffs, int* status, int scalar, int branch) {
   if (threadIdx.x != 0 || blockIdx.x != 0) return;
   const double pre = gs / (2.0 * M_PI);
   // -i * pre * (x + i y) = pre * (y - i x)
@@ -130,7 +134,7 @@ __global__ void paired_coefficients_kernel(const double* trL, const double* trG,
     else if (!(target <= number + holes)) code = QCL_DOMAIN;
   }
   if (!code) {
-    if (number >= target) {
+    if (branch == 1 || (branch == 0 && number >= target)) {
       a = target / number;
       c = 0.0;
     } else {
@@ -151,8 +155,9 @@ __global__ void paired_coefficients_kernel(const double* trL, const double* trG,
 // numerical_invariants.jl:5) for complex128 fields; complex64 fields carry
 // ~1e-7 relative rounding in every diagonal element, so their limit is 1e-5.
 int launch_paired_coefficients(const double* trL, const double* trG, int gs, double target, double* coeffs,
-                               int* status, cudaStream_t st, double realness_limit, int scalar) {
-  paired_coefficients_kernel<<<1, 32, 0, st>>>(trL, trG, gs, target, realness_limit, coeffs, status, scalar);
+                               int* status, cudaStream_t st, double realness_limit, int scalar, int branch) {
+  paired_coefficients_kernel<<<1, 32, 0, st>>>(trL, trG, gs, target, realness_limit, coeffs, status, scalar,
+                                               branch);
   QCL_LAUNCH_CHECK("paired_coefficients");
   return QCL_OK;
 }

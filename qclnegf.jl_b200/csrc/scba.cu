@@ -90,6 +90,7 @@ struct ScbaCtx {
   int refinement = 0;  // FP64-sized state and complex128 operator copies for qcl_scba_promote
   int diagonal = 0, averaged = 0, drop_real = 0, direct_green = 0;  // scattering-model switches
   int scalar_lesser = 0;                                             // occupation_normalization
+  int norm_branch = 0;  // paired normalisation form: 0 the reference's choice, 1 / 2 forced
   // Anderson mixing (mixing = :anderson): device history and mixer state
   int mixing = 0, and_depth = 5;
   double and_damping = 1.0, and_reg = 1e-12;
@@ -710,7 +711,8 @@ static int current_green(ScbaCtx* c, const std::vector<void*>& fam) {
   if ((s = launch_weighted_trace(c->NE, c->Nk, c->trL, c->wE, c->wk, c->rpartial, c->scal + SC_TRL, c->st))) return s;
   if ((s = launch_weighted_trace(c->NE, c->Nk, c->trG, c->wE, c->wk, c->rpartial, c->scal + SC_TRG, c->st))) return s;
   if ((s = launch_paired_coefficients(c->scal + SC_TRL, c->scal + SC_TRG, c->gs, c->target, c->scal + SC_COEF,
-                                      c->status, c->st, c->precision == QCL_C128 ? 1e-10 : 1e-5, c->scalar_lesser)))
+                                      c->status, c->st, c->precision == QCL_C128 ? 1e-10 : 1e-5, c->scalar_lesser,
+                                      c->norm_branch)))
     return s;
   const int sp = c->precision == QCL_MIXED ? QCL_C64 : c->precision;
   if (c->scalar_lesser) return launch_scalar_lesser(sp, c->NE, c->Nk, c->N, c->GR, c->GL, c->GG, c->scal + SC_COEF, c->st);
@@ -1652,7 +1654,7 @@ int scba_tangent_step(ScbaCtx* c, double* out) {
   if ((s = launch_weighted_trace(NE, Nk, c->ttrL, c->wE, c->wk, c->rpartial, c->tscal + TS_DTRL, c->st))) return s;
   if ((s = launch_weighted_trace(NE, Nk, c->ttrG, c->wE, c->wk, c->rpartial, c->tscal + TS_DTRG, c->st))) return s;
   if ((s = launch_norm_tangent(c->nfield, c->GL, c->GG, c->scal + SC_COEF, c->tscal + TS_DTRL, c->tscal + TS_DTRG,
-                               c->gs, c->target, c->tscal + TS_DCOEF, dL, dG, c->st)))
+                               c->gs, c->target, c->norm_branch, c->tscal + TS_DCOEF, dL, dG, c->st)))
     return s;
   // J tangent: J(v_plus, G) + J(Sigma_plus, dG)
   double* jout = c->tscal + TS_FAM + 2 * nf;
@@ -1688,6 +1690,33 @@ int scba_tangent_step(ScbaCtx* c, double* out) {
   }
   out[0] = h[TS_FAM + 2 * nf] + h[TS_FAM + 2 * nf + 2 + N];
   out[1] = r;
+  return QCL_OK;
+}
+
+// The form of the paired normalisation (0: the reference's choice by the sign
+// of number - target; 1 / 2: the first / second form forced, its formula
+// continued across the switch).  Graphs capture the form, so they are rebuilt.
+int scba_set_norm_branch(ScbaCtx* c, int branch) {
+  if (branch < 0 || branch > 2) {
+    set_last_error("normalisation branch %d: expected 0, 1 or 2", branch);
+    return QCL_ARG;
+  }
+  if (c->norm_branch != branch) {
+    QCL_CUDA_CHECK(cudaStreamSynchronize(c->st));
+    c->norm_branch = branch;
+    drop_graphs(c);
+  }
+  return QCL_OK;
+}
+
+// The form the last step used: 1 (scale G<) or 2 (move G> weight into G<).
+int scba_norm_branch(ScbaCtx* c, int* out) {
+  if (!c->have_green) {
+    set_last_error("normalisation branch: no completed step");
+    return QCL_ARG;
+  }
+  QCL_CUDA_CHECK(cudaStreamSynchronize(c->st));
+  *out = c->norm_branch ? c->norm_branch : (c->scal_h[SC_COEF + 3] >= c->target ? 1 : 2);
   return QCL_OK;
 }
 

@@ -115,13 +115,13 @@ int launch_block_triple(int NE, int Nk, int N, const void* A, const void* B, con
 // dH = -pre Im dtrG; branch N >= target: a = target / N, c = 0; else a = 1,
 // c = (target - N) / H.
 __global__ void norm_tangent_coeffs_kernel(const double* coeffs, const double* dtrL, const double* dtrG, int gs,
-                                           double target, double* out) {
+                                           double target, int branch, double* out) {
   if (threadIdx.x != 0 || blockIdx.x != 0) return;
   const double pre = gs / (2.0 * M_PI);
   const double N = coeffs[3], H = coeffs[4];
   const double dN = pre * dtrL[1], dH = -pre * dtrG[1];
   double da = 0, dc = 0;
-  if (N >= target) {
+  if (branch == 1 || (branch == 0 && N >= target)) {  // the form of the forward step
     da = -target / (N * N) * dN;
   } else {
     dc = -dN / H - (target - N) / (H * H) * dH;
@@ -150,9 +150,9 @@ __global__ void norm_tangent_apply_kernel(size_t n, const Cx<double>* __restrict
 }
 
 int launch_norm_tangent(size_t n, const void* Ln, const void* Gn, const double* coeffs, const double* dtrL,
-                        const double* dtrG, int gs, double target, double* dcoef, void* dL, void* dG,
+                        const double* dtrG, int gs, double target, int branch, double* dcoef, void* dL, void* dG,
                         cudaStream_t st) {
-  norm_tangent_coeffs_kernel<<<1, 32, 0, st>>>(coeffs, dtrL, dtrG, gs, target, dcoef);
+  norm_tangent_coeffs_kernel<<<1, 32, 0, st>>>(coeffs, dtrL, dtrG, gs, target, branch, dcoef);
   QCL_LAUNCH_CHECK("norm_tangent_coeffs_kernel");
   const long long g = std::min<long long>(((long long)n + 255) / 256, 148 * 16);
   norm_tangent_apply_kernel<<<(unsigned)g, 256, 0, st>>>(n, (const Cx<double>*)Ln, (const Cx<double>*)Gn, coeffs,

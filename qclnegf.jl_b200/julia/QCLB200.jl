@@ -305,11 +305,18 @@ function _converged(build, p, tol, max_iter)
     return s, row, problem, mechs, shape
 end
 
+normalization_branch(s::Solver) = (b = Ref{Cint}(0); check(ccall((:qcl_scba_normalization_branch, libqcl), Cint,
+                                   (Ptr{Cvoid}, Ref{Cint}), s.handle, b)); Int(b[]))
+set_normalization_branch!(s::Solver, b::Integer) =
+    check(ccall((:qcl_scba_set_normalization_branch, libqcl), Cint, (Ptr{Cvoid}, Cint), s.handle, b))
+
 # One application of the map Phi at the fixed-point state `fams` for the
-# problem at p: Phi per family component and J (the explicit dependence).
-function _map_at(build, p, fams, α)
+# problem at p: Phi per family component and J (the explicit dependence), with
+# the paired normalisation held in the fixed point's form `branch`.
+function _map_at(build, p, fams, α, branch)
     problem, mechs, keep, shape = build(p)
     s = create(problem, mechs, keep)
+    set_normalization_branch!(s, branch)
     for (which, X) in fams
         upload!(s, which, X)
     end
@@ -326,12 +333,13 @@ function implicit_gradient(build::ProblemFamily, p0::AbstractVector{<:Real}, ste
                            tol = 1e-11, max_iter = 20000, tangent_tol = 1e-11, max_tangent = 20000)
     s, row, problem, mechs, shape = _converged(build, p0, tol, max_iter)
     fams = [(which + c, download(s, which + c, shape)) for which in _families(length(mechs)) for c in 0:2]
+    branch = normalization_branch(s)
     tangent_init!(s)
     grad = zeros(length(p0))
     for k in eachindex(p0)
         e = zeros(length(p0)); e[k] = steps[k]
-        φp, Jp = _map_at(build, p0 .+ e, fams, problem.alpha)
-        φm, Jm = _map_at(build, p0 .- e, fams, problem.alpha)
+        φp, Jp = _map_at(build, p0 .+ e, fams, problem.alpha, branch)
+        φm, Jm = _map_at(build, p0 .- e, fams, problem.alpha, branch)
         for (which, _) in fams
             tangent_set!(s, which, (φp[which] .- φm[which]) ./ (2steps[k]))
         end

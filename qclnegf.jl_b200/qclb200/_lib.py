@@ -167,6 +167,8 @@ def _declare(l):
         "qcl_scba_tangent_set": (I, [P, I, P]),
         "qcl_scba_tangent_step": (I, [P, P]),
         "qcl_scba_download_candidate": (I, [P, I, P]),
+        "qcl_scba_set_normalization_branch": (I, [P, I]),
+        "qcl_scba_normalization_branch": (I, [P, ctypes.POINTER(ctypes.c_int)]),
         "qcl_sweep_run": (I, [P, I, D, P, P, P]),
         "qcl_sweep_destroy": (None, [P]),
         "qcl_autotune_reset": (I, []),

@@ -15,7 +15,10 @@ parameter changes in the problem's inputs (the Hamiltonian, the bias drop,
 the kernels, ...) -- is the central difference of ONE application of the map
 at the fixed point (not of a converged solve), so it carries no convergence
 error: the problem is rebuilt at p +- h, the fixed-point state is uploaded and
-one step is taken.
+one step is taken.  The paired number normalisation is held in the form the
+fixed point used (qcl_scba_set_normalization_branch): a particle-conserving
+fixed point sits on the switch between its two forms, and a difference
+across the switch would mix the two one-sided derivatives.
 
 `central_difference` converges the SCBA at p +- h instead: the check.
 """
@@ -45,10 +48,19 @@ def _converge(problem, tol, max_iter):
     return s, rows
 
 
-def _map_at(problem, fams):
+def _branch(solver):
+    b = ctypes.c_int(0)
+    check(lib().qcl_scba_normalization_branch(solver._h, ctypes.byref(b)))
+    return b.value
+
+
+def _map_at(problem, fams, branch):
     """One application of the map at the uploaded state: (Phi(Sigma) per
-    family component, J(Sigma))."""
+    family component, J(Sigma)), with the paired normalisation held in the
+    form `branch` of the fixed point (a particle-conserving fixed point sits
+    on the switch between its two forms, and p +- h must not straddle it)."""
     s = ProductionSCBA(problem, precision="c128", use_graph=False)
+    check(lib().qcl_scba_set_normalization_branch(s._h, int(branch)))
     for f, comps in enumerate(fams):
         for c, a in enumerate(comps):
             s.upload(3 + 3 * f + c, a)
@@ -77,6 +89,7 @@ def implicit_derivatives(build: Callable[[np.ndarray], object], p0: Sequence[flo
     nfam = len(pr0.mechanisms) + 2
     s, rows = _converge(pr0, tol, max_iter)
     fams = _families(s, nfam)
+    branch = _branch(s)
     J0 = pr0.J0
     lib_s = s
     check(lib().qcl_scba_tangent_init(lib_s._h))
@@ -84,8 +97,8 @@ def implicit_derivatives(build: Callable[[np.ndarray], object], p0: Sequence[flo
     for k, h in enumerate(steps):
         e = np.zeros_like(p0)
         e[k] = h
-        phi_p, Jp = _map_at(build(p0 + e), fams)
-        phi_m, Jm = _map_at(build(p0 - e), fams)
+        phi_p, Jp = _map_at(build(p0 + e), fams, branch)
+        phi_m, Jm = _map_at(build(p0 - e), fams, branch)
         for f in range(nfam):
             for c in range(3):
                 src = np.asfortranarray((phi_p[f][c] - phi_m[f][c]) / (2 * h))

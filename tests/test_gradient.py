@@ -69,3 +69,28 @@ def test_thickness_derivatives_match_central_differences(gpu_ops):
     fd = central_difference(_build_stack, p0, steps, tol=1e-12)
     for g, f in zip(got["dJ_dp"], fd):
         assert abs(g - f) <= 1e-4 * max(abs(f), 1e-6 * abs(got["J"])), (g, f)
+
+
+def _build_stack_bias(p):
+    from qclb200.problem import full_physics_problem
+
+    (bias,) = p
+    return full_physics_problem(seed=2, NE=96, Nk=6, periods=2, states=3, Nqz=41, Nphi=16, lookup_nodes=9,
+                                alpha=0.8, bias_mV=bias, mechanisms=("LO", "acoustic", "IFR"),
+                                layers=(4.0, 8.5, 2.0, 16.0), coupling_ev=0.02, temperature_K=300.0)
+
+
+def test_stack_bias_derivative_holds_the_normalisation_form(gpu_ops):
+    """dJ/dbias of the same stack: the bias moves the raw carrier number of
+    the map across the switch of the paired normalisation (number above or
+    below the target), which a particle-conserving fixed point sits on
+    (lambda -> 1).  The explicit part is evaluated with the normalisation
+    held in the fixed point's form on both sides
+    (qcl_scba_set_normalization_branch); with the reference's choice on each
+    side the central difference mixed the two one-sided branches and came
+    out 9x off."""
+    from qclb200.gradient import central_difference, implicit_derivatives
+
+    got = implicit_derivatives(_build_stack_bias, [50.0], [0.1], tol=1e-12, tangent_tol=1e-9, max_tangent=5000)
+    fd = central_difference(_build_stack_bias, [50.0], [0.1], tol=1e-12)
+    assert abs(got["dJ_dp"][0] - fd[0]) <= 1e-4 * abs(fd[0]), (got["dJ_dp"][0], fd[0])

@@ -389,7 +389,7 @@ def run_gpu(args):
     # class once per process (untimed, like a library's start-up tuning)
     from qclb200 import operators as _ops
 
-    tune = _ops.autotune(NB, precision="c128", NE=NE, Nk=8)
+    tune = _ops.autotune(NB, precision="c128", NE=NE, Nk=NK)  # tuned on the workload's own batch
 
     def dyson():
         st = L.qcl_dev_dyson_keldysh(sp, prec, NE, NK, NB, P(eps_d.data_ptr()), 0.0, P(hf.data_ptr()),

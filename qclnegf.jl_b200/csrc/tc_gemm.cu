@@ -195,7 +195,9 @@ struct TcColWalk {
 // Hand-offs are mbarriers only: full[s] (TMA bytes), empty[s] (MMAs done
 // reading stage s), acc_full[b] (accumulation in buffer b done), acc_empty[b]
 // (256 readers done with buffer b).
-template <int BN>
+// PERSIST: the CTA walks several tiles (short K); otherwise exactly one
+// (blockIdx.x), and the tile loops fold away at compile time.
+template <int BN, bool PERSIST>
 __global__ void __launch_bounds__(TC_THREADS, 1) tc_gemm_kernel(const __grid_constant__ TcMaps maps, TcArgs p) {
   using S = TcShape<BN>;
   constexpr int TC_STAGE_BYTES = S::STAGE_BYTES, TC_B_BYTES = S::B_BYTES;
@@ -219,7 +221,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) tc_gemm_kernel(const __grid_con
   const int nch = (nkb + TC_ACC_KB - 1) / TC_ACC_KB;  // accumulation groups per tile
   const int ntiles_n = (p.Ncols + BN - 1) / BN;
   const long long tiles = (long long)p.mtiles * ntiles_n;
-  const int ntile = blockIdx.x < tiles ? (int)((tiles - 1 - blockIdx.x) / gridDim.x + 1) : 0;
+  const int ntile = !PERSIST ? 1 : blockIdx.x < tiles ? (int)((tiles - 1 - blockIdx.x) / gridDim.x + 1) : 0;
   const int mtiles = p.mtiles, cols_fastest = p.cols_fastest;
   const auto tile_origin = [mtiles, ntiles_n, cols_fastest](int i, int& m0, int& n0) {
     const int t = (int)blockIdx.x + i * (int)gridDim.x;  // tiles < 2^31
@@ -256,9 +258,9 @@ __global__ void __launch_bounds__(TC_THREADS, 1) tc_gemm_kernel(const __grid_con
     // ---- producer ---------------------------------------------------------
     if (lane == 0) {
       for (int kb = 0; kb < ntile * nkb && !s_fail; ++kb) {  // kb: this CTA's K blocks over its tiles
-        const int s = kb % TC_STAGES, kt = kb % nkb;
+        const int s = kb % TC_STAGES, kt = PERSIST ? kb % nkb : kb;
         int m0, n0;
-        tile_origin(kb / nkb, m0, n0);
+        tile_origin(PERSIST ? kb / nkb : 0, m0, n0);
         if (kb >= TC_STAGES && !mbar_wait(empty + 8 * s, (uint32_t)((kb / TC_STAGES - 1) & 1), lim)) {
           s_fail = 1;
           break;
@@ -277,7 +279,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1) tc_gemm_kernel(const __grid_con
     if (lane == 0) {
       for (int kb = 0; kb < ntile * nkb && !s_fail; ++kb) {
         // group ch counts this CTA's accumulation groups over its tiles
-        const int kt = kb % nkb, s = kb % TC_STAGES, ch = (kb / nkb) * nch + kt / TC_ACC_KB, b = ch & 1;
+        const int kt = PERSIST ? kb % nkb : kb, s = kb % TC_STAGES;
+        const int ch = (PERSIST ? (kb / nkb) * nch : 0) + kt / TC_ACC_KB, b = ch & 1;
         const bool first = kt % TC_ACC_KB == 0, last = (kt % TC_ACC_KB == TC_ACC_KB - 1) || kt == nkb - 1;
         if (!mbar_wait(full + 8 * s, (uint32_t)((kb / TC_STAGES) & 1), lim) ||
             (first && ch >= 2 && !mbar_wait(acc_empty + 8 * b, (uint32_t)(((ch - 2) >> 1) & 1), lim))) {
@@ -655,7 +658,9 @@ static int tc_pick_bn(int mtiles, int Ncols) {
 template <int BN> static int launch_tc_t(const TcMaps& maps, const TcArgs& a, int mtiles, cudaStream_t st) {
   static bool configured = false;
   if (!configured) {
-    QCL_CUDA_CHECK(cudaFuncSetAttribute(tc_gemm_kernel<BN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    QCL_CUDA_CHECK(cudaFuncSetAttribute(tc_gemm_kernel<BN, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        TcShape<BN>::SMEM_BYTES));
+    QCL_CUDA_CHECK(cudaFuncSetAttribute(tc_gemm_kernel<BN, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                         TcShape<BN>::SMEM_BYTES));
     configured = true;
   }
@@ -669,11 +674,14 @@ template <int BN> static int launch_tc_t(const TcMaps& maps, const TcArgs& a, in
   // sum): one persistent CTA per SM, so that a tile's epilogue overlaps the
   // next tile's loads and MMAs (1.41 -> 1.21 ms on the 524 288 x 1024 x 128
   // case).  Long K: one CTA per tile, which the hardware schedules as SMs
-  // free up (persistent CTAs measured 10 % slower there: 5.23 -> 5.78 ms on
-  // the 32 768 x 2048 x 16 384 case).
+  // free up (the persistent form measured 10 % slower there: 5.23 -> 5.78 ms
+  // on the 32 768 x 2048 x 16 384 case).
   const bool persistent = b.Kpad / TC_BK <= 8;
   const long long grid = persistent ? std::min<long long>(tiles, sms) : tiles;
-  tc_gemm_kernel<BN><<<(unsigned)grid, TC_THREADS, TcShape<BN>::SMEM_BYTES, st>>>(maps, b);
+  if (persistent)
+    tc_gemm_kernel<BN, true><<<(unsigned)grid, TC_THREADS, TcShape<BN>::SMEM_BYTES, st>>>(maps, b);
+  else
+    tc_gemm_kernel<BN, false><<<(unsigned)grid, TC_THREADS, TcShape<BN>::SMEM_BYTES, st>>>(maps, b);
   QCL_LAUNCH_CHECK("tc_gemm_kernel");
   return QCL_OK;
 }

@@ -650,7 +650,7 @@ def extras(torch, dev, L, _lib):
     for key, fn in (("scba_fixed_point_small", lambda: scba_fixed_point_small(torch)),
                     ("scba_all_mechanisms", lambda: scba_all_mechanisms(torch)),
                     ("scba_full_physics_N32", lambda: scba_full_physics(torch)),
-                    ("bias_sweep_16", lambda: bias_sweep(torch, npoints=16, iters=4,
+                    ("bias_sweep_16", lambda: bias_sweep(torch, npoints=16, iters=12,
                                                          classes=((2, 8), (3, 8), (4, 8)),
                                                          NE_choices=(1024, 1536, 2048)))):
         try:

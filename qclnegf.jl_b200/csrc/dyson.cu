@@ -391,7 +391,7 @@ int dyson_default_bpc(int precision, int NP) {
   switch (NP) {
     case 8: return 16;
     case 16: return wide ? 4 : 8;
-    case 24: return wide ? 2 : 4;
+    case 24: return 4;  // complex128: 3.80 ms against 4.09 ms with 2 on the 4096 x 32 batch
     case 32: return wide ? 1 : 2;
     case 48: return 1;
     default: return 0;

@@ -54,7 +54,7 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-extras", action="store_true", help="skip the variant and SCBA side measurements")
     ap.add_argument("--capture", choices=["dyson", "hilbert", "scba", "tcgemm", "scba_all_mixed", "scba_all_c128",
-                                          "separable"],
+                                          "separable", "full_physics_mixed"],
                     help="run one small case of a kernel for an ncu capture (2 launches) and exit")
     ap.add_argument("--study", choices=["full_physics_converged", "full_physics_converged_mixed",
                                         "all_mechanisms_converged", "bias_sweep_64"],
@@ -906,6 +906,18 @@ def run_capture(kind):
         G = np.asfortranarray(rng.standard_normal((ne, nk, nb, nb)) + 1j * rng.standard_normal((ne, nk, nb, nb)))
         for prec in ("c64", "c128"):
             operators.production_static_contraction(mech, G, np.ones(nk), precision=prec)
+    elif kind == "full_physics_mixed":
+        # the full-physics configuration (N_b = 32, N_E x N_k = 2048 x 64, five
+        # mechanisms) in mixed precision: seed + 1 eager iteration, for a
+        # per-kernel launch list of an iteration at the stated size (73 GB on
+        # the device; for a one-pass metric list only)
+        from qclb200.problem import full_physics_problem
+        from qclb200.scba import ProductionSCBA
+
+        s = ProductionSCBA(full_physics_problem(), precision="mixed", use_graph=False)
+        s.seed()
+        s.step()
+        s.close()
     elif kind.startswith("scba_all"):
         # the all-mechanism SCBA workload of the extras (N_E x N_k = 1024 x 32,
         # N_b = 16, LO + acoustic + impurity + IFR + alloy): seed + 3 eager

@@ -186,6 +186,66 @@ __device__ __forceinline__ void team_matmul_dmma(const Cx<double>* A, const Cx<d
   }
 }
 
+// The same product with three real DMMAs per complex tile product (the 3M
+// form): T1 = Ar Br, T2 = Ai Bi, T3 = (Ar + Ai)(Br + Bi), then Re C = T1 - T2
+// and Im C = T3 - T1 - T2.  A quarter fewer tensor-core issues; the error
+// stays within the norm-wise bound of the four-product form (a few eps times
+// (|Ar| + |Ai|)(|Br| + |Bi|) per term).  Used by the Keldysh products of the
+// Dyson kernel.
+template <int NP, int TT>
+__device__ __forceinline__ void team_matmul_dmma3(const Cx<double>* A, const Cx<double>* B, DmmaTile<NP, TT>& acc,
+                                                  int N, int tt, bool adjB) {
+  constexpr int NT = DmmaTile<NP, TT>::NT, NW = DmmaTile<NP, TT>::NW, RPW = DmmaTile<NP, TT>::RPW;
+  const int warp = tt >> 5, lane = tt & 31, lr = lane >> 2, lc = lane & 3;
+  double t3[RPW][NT][2];
+#pragma unroll
+  for (int r = 0; r < RPW; ++r)
+#pragma unroll
+    for (int j = 0; j < NT; ++j)
+#pragma unroll
+      for (int i = 0; i < 2; ++i) acc.re[r][j][i] = acc.im[r][j][i] = t3[r][j][i] = 0.0;  // re: T1, im: T2
+  for (int k0 = 0; k0 < N; k0 += 4) {
+    const int k = k0 + lc;
+    const bool kin = k < N;
+    double ar[RPW], ai[RPW], as[RPW], br[NT], bi[NT], bs[NT];
+#pragma unroll
+    for (int r = 0; r < RPW; ++r) {
+      const bool rin = warp + r * NW < NT;  // warp-uniform
+      const Cx<double> a = kin && rin ? A[sw<NP>((warp + r * NW) * 8 + lr, k)] : cx<double>(0, 0);
+      ar[r] = a.x;
+      ai[r] = a.y;
+      as[r] = a.x + a.y;
+    }
+#pragma unroll
+    for (int j = 0; j < NT; ++j) {
+      Cx<double> b = cx<double>(0, 0);
+      if (kin) b = adjB ? conj(B[sw<NP>(j * 8 + lr, k)]) : B[sw<NP>(k, j * 8 + lr)];
+      br[j] = b.x;
+      bi[j] = b.y;
+      bs[j] = b.x + b.y;
+    }
+#pragma unroll
+    for (int r = 0; r < RPW; ++r)
+#pragma unroll
+      for (int j = 0; j < NT; ++j) {
+        if (RPW * NW != NT && warp + r * NW >= NT) continue;  // warp-uniform: no tile row here
+        dmma_f64(acc.re[r][j], ar[r], br[j]);
+        dmma_f64(acc.im[r][j], ai[r], bi[j]);
+        dmma_f64(t3[r][j], as[r], bs[j]);
+      }
+  }
+#pragma unroll
+  for (int r = 0; r < RPW; ++r)
+#pragma unroll
+    for (int j = 0; j < NT; ++j)
+#pragma unroll
+      for (int i = 0; i < 2; ++i) {
+        const double t1 = acc.re[r][j][i], t2 = acc.im[r][j][i];
+        acc.re[r][j][i] = t1 - t2;
+        acc.im[r][j][i] = (t3[r][j][i] - t1) - t2;
+      }
+}
+
 template <int NP, int TT>
 __device__ __forceinline__ void team_store_dmma(Cx<double>* C, const DmmaTile<NP, TT>& acc, int tt) {
   constexpr int NT = DmmaTile<NP, TT>::NT, NW = DmmaTile<NP, TT>::NW, RPW = DmmaTile<NP, TT>::RPW;

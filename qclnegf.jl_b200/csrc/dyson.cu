@@ -297,12 +297,22 @@ __global__ void __launch_bounds__(BPC* Tile<NP>::TT, (dyson_min_ctas<RS, RL, NP,
     // issued instructions for the products; measured 4.07 -> 4.00 ms at
     // N_b = 24 and 32.6 -> 29.3 ms at N_b = 48 on the operator batch.
     if constexpr (sizeof(RS) == 8 && sizeof(RM) == 8) {
+      // three real DMMAs per complex tile product up to N_b = 32; at 48 the
+      // third accumulator set spills
       DmmaTile<NP, TT> acc;
-      team_matmul_dmma<NP, TT>(G, X, acc, N, tt, false);  // T = G Sigma
+      if constexpr (NP <= 32) {
+        team_matmul_dmma3<NP, TT>(G, X, acc, N, tt, false);  // T = G Sigma
+      } else {
+        team_matmul_dmma<NP, TT>(G, X, acc, N, tt, false);
+      }
       team_sync<TT>(team);
       team_store_dmma<NP, TT>(X, acc, tt);
       team_sync<TT>(team);
-      team_matmul_dmma<NP, TT>(X, G, acc, N, tt, true);  // T G^H
+      if constexpr (NP <= 32) {
+        team_matmul_dmma3<NP, TT>(X, G, acc, N, tt, true);  // T G^H
+      } else {
+        team_matmul_dmma<NP, TT>(X, G, acc, N, tt, true);
+      }
       team_sync<TT>(team);
       team_store_dmma<NP, TT>(X, acc, tt);
       team_sync<TT>(team);

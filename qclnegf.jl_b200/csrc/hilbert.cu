@@ -14,7 +14,9 @@
 // shared memory, the two FFTs are Stockham passes (radix 16 after a first
 // pass of radix L / 16^P) with the butterflies in registers, the last forward
 // pass, the spectrum product and the first inverse pass run as one register
-// pass, the kernel spectrum is read from L2, and the inputs are read once and
+// pass, the kernel spectrum is read from L2 (from shared memory in the
+// half-length form, whose centred kernel has a real, odd spectrum: a quarter
+// of the table), and the inputs are read once and
 // the outputs written once (E is the contiguous axis, so every load/store is
 // coalesced).  The complex128 L = 8192 transform runs as two half-length
 // transforms (even / odd frequencies) in a 68 KiB buffer, so that two columns
@@ -325,11 +327,58 @@ template <typename R, int L, int NS> struct Radix16Passes<R, L, NS, 0> {
   __device__ __forceinline__ static void run(Cx<R>*, const Cx<R>*, const Cx<R>*) {}
 };
 
+// Spectrum product of the spectrum pass, conj(v K[f]) at f = j + r L/16 (r a
+// constant after unrolling).  SpecTable reads a full complex spectrum from
+// global memory (L2).
+template <typename R, int L> struct SpecTable {
+  const Cx<R>* K;
+  __device__ __forceinline__ void prepare() const {}
+  __device__ __forceinline__ Cx<R> operator()(Cx<R> v, int j, int r) const {
+    return conj(v * ldg_cx(K + j + r * (L / 16)));
+  }
+};
+
+// Spectrum of the circularly centred kernel, k[lag mod L] (lag in (-N_E,
+// N_E)).  The kernel is real and odd, so its spectrum is purely imaginary,
+// K[f] = i S[f] with S real and S[L - f] = -S[f].  In the even / odd
+// frequency halves of length LH = L/2, E[f] = S[2f] and O[f] = S[2f+1] obey
+// E[LH - f] = -E[f] and O[LH - 1 - f] = -O[f], so the table holds E[0..LH/2]
+// and O[0..LH/2): LH + 1 doubles (32 KB at L = 8192) instead of the L complex
+// values (128 KB) of the offset kernel's spectrum.  It is staged in shared
+// memory once per column (cp.async, waited for before the first spectrum
+// product).  Centring moves the wanted outputs from [N_E - 1, 2 N_E - 2] to
+// [0, N_E): the same linear convolution, since L >= 2 N_E - 1.
+__device__ __forceinline__ void hil_cp_async16(void* smem, const void* gmem) {
+  const unsigned a = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(a), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void hil_cp_async_wait() {
+  asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
+}
+__host__ __device__ constexpr int sym_table_odd_offset(int LH) { return LH / 2 + 2; }  // E padded to a 16-byte multiple
+__host__ __device__ constexpr int sym_table_doubles(int LH) { return sym_table_odd_offset(LH) + LH / 2; }
+template <int LH, bool ODD> struct SpecSym {
+  const double* S;  // shared memory, sym_table_doubles(LH) entries
+  __device__ __forceinline__ void prepare() const { hil_cp_async_wait(); }
+  __device__ __forceinline__ Cx<double> operator()(Cx<double> v, int j, int r) const {
+    constexpr int NB = LH / 16;
+    const int f = j + r * NB;
+    double s;
+    if (!ODD) {
+      s = r < 8 ? S[f] : -S[LH - f];  // r >= 8: f >= LH/2
+    } else {
+      constexpr int o = sym_table_odd_offset(LH);
+      s = r < 8 ? S[o + f] : -S[o + LH - 1 - f];
+    }
+    return cx<double>(-v.y * s, -v.x * s);  // conj(v i s)
+  }
+};
+
 // Last radix-16 pass of the forward transform, times K and conjugated (so
 // that the next forward transform computes the inverse one: IFFT(X) =
 // conj(FFT(conj X)) / L), and the first radix-16 pass of that transform.
-template <typename R, int L>
-__device__ __forceinline__ void spectrum_pass(Cx<R>* buf, const Cx<R>* __restrict__ K, const Cx<R>* __restrict__ tw,
+template <typename R, int L, typename Spec>
+__device__ __forceinline__ void spectrum_pass(Cx<R>* buf, const Spec& spec, const Cx<R>* __restrict__ tw,
                                               const Cx<R>* __restrict__ seg) {
   constexpr int T = FftPlan<L>::T;
   constexpr int NB = L / 16;
@@ -350,6 +399,7 @@ __device__ __forceinline__ void spectrum_pass(Cx<R>* buf, const Cx<R>* __restric
       for (int r = 0; r < 16; ++r) v[q][r] = buf[fpad(j + r * NB)];
     }
   }
+  spec.prepare();
   __syncthreads();
 #pragma unroll
   for (int q = 0; q < Q; ++q) {
@@ -360,7 +410,7 @@ __device__ __forceinline__ void spectrum_pass(Cx<R>* buf, const Cx<R>* __restric
       // forward output j + r NB is v[bitrev(r)]; it is input r of the next pass
       Cx<R> u[16];
 #pragma unroll
-      for (int r = 0; r < 16; ++r) u[r] = conj(v[q][bitrev<16>(r)] * ldg_cx(K + j + r * NB));
+      for (int r = 0; r < 16; ++r) u[r] = spec(v[q][bitrev<16>(r)], j, r);
       DifStage<R, 16, 8>::run(u);
 #pragma unroll
       for (int r = 0; r < 16; ++r) buf[fpad(16 * j + r)] = u[bitrev<16>(r)];
@@ -388,8 +438,8 @@ template <typename R, int L> __device__ __forceinline__ void prefetch_spectrum(c
 // conj(L * IFFT(FFT(x) .* K)) for a field read through `in` (ZHI: zero on
 // [L/2, L)), written through `out`; `buf` holds the padded column, `twt` the
 // complex64 pass tables (null for complex128).
-template <typename R, int L, bool ZHI, typename In, typename Out>
-__device__ __forceinline__ void convolve_run(const In& in, const Cx<R>* K, const Out& out, Cx<R>* buf,
+template <typename R, int L, bool ZHI, typename In, typename Spec, typename Out>
+__device__ __forceinline__ void convolve_run(const In& in, const Spec& spec, const Out& out, Cx<R>* buf,
                                              const Cx<R>* tw, const Cx<R>* twt) {
   static_assert(L >= 64 && L <= 16384, "unsupported FFT length");
   constexpr int P = conv_passes(L);
@@ -398,9 +448,9 @@ __device__ __forceinline__ void convolve_run(const In& in, const Cx<R>* K, const
   static_assert(conv_table_entries(L) == 2 * L - S - 16, "pass-table layout");
   const bool t = twt != nullptr;
   stockham_pass<R, L, S, 1, ZHI>(in, SmemOut<R>{buf}, tw, nullptr);
-  if constexpr (sizeof(R) == 4) prefetch_spectrum<R, L>(K);
+  if constexpr (sizeof(R) == 4) prefetch_spectrum<R, L>(spec.K);
   Radix16Passes<R, L, S, P - 1>::run(buf, tw, t ? twt + conv_fwd_seg(L, 0) : nullptr);
-  spectrum_pass<R, L>(buf, K, tw, t ? twt + conv_fwd_seg(L, P - 1) : nullptr);
+  spectrum_pass<R, L>(buf, spec, tw, t ? twt + conv_fwd_seg(L, P - 1) : nullptr);
   Radix16Passes<R, L, 16, P - 1>::run(buf, tw, t ? twt + conv_inv_seg(L, 1) : nullptr);
   stockham_pass<R, L, S, L / S, false>(SmemIn<R>{buf}, out, tw, t ? twt + conv_inv_seg(L, P) : nullptr);
 }
@@ -424,6 +474,7 @@ template <typename R> struct HilbertArgs {
   const Cx<R>* ksplit;  // [FFT_L(kernel)[2j], j < L/2 | FFT_L(kernel)[2j+1], j < L/2]
   const Cx<R>* twh;     // W_{L/2}^t, t < L/2
   const Cx<R>* twt;     // complex64 pass twiddle tables (null for complex128)
+  const double* ksym;   // centred kernel's spectrum / i, symmetric halves (complex128, L = 8192)
 };
 
 template <typename R>
@@ -524,10 +575,10 @@ __global__ void __launch_bounds__(FftPlan<L>::T, (hilbert_min_blocks<R, FftPlan<
 
   if constexpr (!VERIFY) {
     // results written from registers by the last pass
-    convolve_run<R, L, true>(FieldIn<R>{&p, base, nullptr}, p.khat, ResultOut<R>{&p, base}, buf, p.tw, p.twt);
+    convolve_run<R, L, true>(FieldIn<R>{&p, base, nullptr}, SpecTable<R, L>{p.khat}, ResultOut<R>{&p, base}, buf, p.tw, p.twt);
     return;
   }
-  convolve_run<R, L, true>(FieldIn<R>{&p, base, nullptr}, p.khat, so, buf, p.tw, p.twt);
+  convolve_run<R, L, true>(FieldIn<R>{&p, base, nullptr}, SpecTable<R, L>{p.khat}, so, buf, p.tw, p.twt);
   // y_L of this thread's outputs, kept in shared memory (read back by the
   // same thread) instead of registers across the second transform
   Cx<R>* lam = buf + (L + L / 16);
@@ -539,7 +590,7 @@ __global__ void __launch_bounds__(FftPlan<L>::T, (hilbert_min_blocks<R, FftPlan<
   }
   __syncthreads();
   // ---- odd-frequency half of the length-2L transform -------------------------
-  convolve_run<R, L, true>(FieldIn<R>{&p, base, p.twist}, p.kodd, so, buf, p.tw, p.twt);
+  convolve_run<R, L, true>(FieldIn<R>{&p, base, p.twist}, SpecTable<R, L>{p.kodd}, so, buf, p.tw, p.twt);
   double dsum = 0, lsum = 0;
 #pragma unroll
   for (int q = 0; q < PER; ++q) {
@@ -587,9 +638,12 @@ __global__ void __launch_bounds__(FftPlan<L>::T, (hilbert_min_blocks<R, FftPlan<
 // Even/odd frequency halves in sequence (no verification).
 //
 // The padded field is zero on [L/2, L), so its length-L spectrum splits into
-//   X[2j]   = FFT_{L/2}(x)[j],   X[2j+1] = FFT_{L/2}(x W_L^n)[j],
-// and with Y = X K_hat the length-L inverse transform is
-//   y[n] = (ye[n'] + (-1)^s W_L^{-n'} yo[n']) / L,   n = n' + s L/2,
+//   X[2j]   = FFT_{L/2}(x)[j],   X[2j+1] = FFT_{L/2}(x W_L^n)[j].
+// The kernel is the circularly centred one (SpecSym: K = i S, a real table of
+// L/2 + 1 entries in shared memory), whose wanted outputs are y[0, N_E), all
+// in the first half (N_E <= L/2).  With Y = X K the length-L inverse
+// transform there is
+//   y[n] = (ye[n] + W_L^{-n} yo[n]) / L,   0 <= n < L/2,
 // ye, yo the unnormalised length-L/2 inverse transforms of Y[2j], Y[2j+1].
 // One CTA transforms the even half, parks conj(ye) of the wanted outputs in
 // the output array, then transforms the odd half and completes each output
@@ -599,13 +653,8 @@ __global__ void __launch_bounds__(FftPlan<L>::T, (hilbert_min_blocks<R, FftPlan<
 // inverse transform.  The output must not alias the input (the field is read
 // again for the odd half).
 // ---------------------------------------------------------------------------
-// Output slot of padded index t in [0, L/2): n = t or t + L/2, whichever lies
-// in [NE - 1, 2 NE - 2] (at most one does, since NE <= L/2); -1 if neither.
-template <int LH> __device__ __forceinline__ int half_slot(int t, int NE) {
-  const int n = t >= NE - 1 ? t : t + LH;
-  const int e = n - (NE - 1);
-  return e < NE ? e : -1;
-}
+// Output slot of padded index t in [0, L/2): e = t for t < N_E, else -1.
+template <int LH> __device__ __forceinline__ int half_slot(int t, int NE) { return t < NE ? t : -1; }
 template <typename R, int LH> struct ParkOut {
   static constexpr bool kBatch = false;
   const HilbertArgs<R>* p;
@@ -627,7 +676,7 @@ template <typename R, int LH> struct CompleteOut {
     if (e < 0) return;
     Cx<R>* dst = p->SR ? p->SR : p->Lam;
     const Cx<R> a = dst[base + e];  // parked by this thread in the even half
-    const Cx<R> y = t < NE - 1 ? a - d : a + d;
+    const Cx<R> y = a + d;
     const R sc = (R)p->scale_out;
     const Cx<R> lam = cx<R>(sc * y.x, -sc * y.y);
     if (p->SR) {
@@ -658,12 +707,18 @@ __global__ void __launch_bounds__(FftPlan<LH>::T, (hilbert_min_blocks<R, FftPlan
     hilbert_halves_kernel(HilbertArgs<R> p) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   Cx<R>* buf = reinterpret_cast<Cx<R>*>(smem_raw);
+  static_assert(sizeof(R) == 8, "the centred half-length form is complex128 only");
+  double* ksh = reinterpret_cast<double*>(buf + (LH + LH / 16));  // sym_table_doubles(LH) entries
   const long long col = blockIdx.x + (long long)blockIdx.y * gridDim.x;
   if (col >= p.ncols) return;
+  // stage the spectrum table (waited for in the first spectrum pass)
+  constexpr int CHUNKS = sym_table_doubles(LH) / 2;  // 16-byte copies
+  static_assert(sym_table_doubles(LH) % 2 == 0, "16-byte table copies");
+  for (int i = threadIdx.x; i < CHUNKS; i += FftPlan<LH>::T) hil_cp_async16(ksh + 2 * i, p.ksym + 2 * i);
   const size_t base = (size_t)col * p.NE;
-  convolve_run<R, LH, false>(FieldIn<R>{&p, base, nullptr}, p.ksplit, ParkOut<R, LH>{&p, base}, buf, p.twh,
-                             nullptr);
-  convolve_run<R, LH, false>(FieldIn<R>{&p, base, p.tw}, p.ksplit + LH, CompleteOut<R, LH>{&p, base}, buf,
+  convolve_run<R, LH, false>(FieldIn<R>{&p, base, nullptr}, SpecSym<LH, false>{ksh}, ParkOut<R, LH>{&p, base}, buf,
+                             p.twh, nullptr);
+  convolve_run<R, LH, false>(FieldIn<R>{&p, base, p.tw}, SpecSym<LH, true>{ksh}, CompleteOut<R, LH>{&p, base}, buf,
                              p.twh, nullptr);
 }
 
@@ -711,6 +766,7 @@ void free_hilbert_tables(HilbertTables& t) {
   cudaFree(t.ksplit);
   cudaFree(t.twh);
   cudaFree(t.twt);
+  cudaFree(t.ksym);
   cudaFree(t.partial);
   t = HilbertTables();
 }
@@ -787,6 +843,26 @@ int prepare_hilbert_tables(HilbertTables& t, int NE, double de, int precision) {
   }
   int st;
   if (storage == QCL_C128) {
+    // centred kernel k[lag mod L]: its spectrum is i S, S real and odd
+    // (S[L - f] = -S[f]); the table keeps S[2f], f <= L/4, padded to an even
+    // count, then S[2f + 1], f < L/4 (the layout SpecSym reads)
+    std::vector<double> cr(L, 0.0), ci(L, 0.0);
+    for (int lag = 1; lag <= NE - 1; ++lag) {
+      const double v = 1.0 / (2.0 * M_PI * lag * de);
+      cr[lag] = v;
+      cr[L - lag] = -v;
+    }
+    host_fft(cr, ci);
+    const int odd0 = LH / 2 + 2;
+    std::vector<double> sym(odd0 + LH / 2, 0.0);
+    for (int f = 1; f <= LH / 2; ++f) {
+      const int g = 2 * f;  // S[0] = S[L/2] = 0 exactly
+      sym[f] = g == LH ? 0.0 : 0.5 * (ci[g] - ci[L - g]);
+    }
+    for (int f = 0; f < LH / 2; ++f) sym[odd0 + f] = 0.5 * (ci[2 * f + 1] - ci[L - 2 * f - 1]);
+    QCL_CUDA_CHECK(cudaMalloc(&t.ksym, sym.size() * sizeof(double)));
+    QCL_CUDA_CHECK(cudaMemcpy(t.ksym, sym.data(), sym.size() * sizeof(double), cudaMemcpyHostToDevice));
+    QCL_CUDA_CHECK(cudaDeviceSynchronize());
     if ((st = upload_cx<double>(&t.khat, kr, ki))) return st;
     if ((st = upload_cx<double>(&t.kodd, kor, koi))) return st;
     if ((st = upload_cx<double>(&t.tw, twr, twi))) return st;
@@ -855,7 +931,8 @@ template <typename R, int L, bool VERIFY> static int launch_hilbert_LV(const Hil
 }
 template <typename R, int LH> static int launch_hilbert_halves(const HilbertArgs<R>& a, cudaStream_t st) {
   constexpr int T = FftPlan<LH>::T;
-  constexpr size_t smem = (size_t)(LH + LH / 16) * sizeof(Cx<R>);
+  constexpr size_t smem = (size_t)(LH + LH / 16) * sizeof(Cx<R>) + sym_table_doubles(LH) * sizeof(double);
+  static_assert(2 * (smem + 1024) <= 228 * 1024, "two columns per SM");
   static bool configured = false;
   if (!configured) {
     QCL_CUDA_CHECK(cudaFuncSetAttribute(hilbert_halves_kernel<R, LH>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -943,7 +1020,8 @@ int launch_hilbert(HilbertTables& t, int precision, long long ncols, const doubl
                           1.0 / t.L,
                           (const Cx<double>*)t.ksplit,
                           (const Cx<double>*)t.twh,
-                          nullptr};
+                          nullptr,
+                          (const double*)t.ksym};
     return launch_hilbert_t<double>(a, t.L, halves, st);
   }
   HilbertArgs<float> a{t.NE,
@@ -963,7 +1041,8 @@ int launch_hilbert(HilbertTables& t, int precision, long long ncols, const doubl
                        1.0 / t.L,
                        (const Cx<float>*)t.ksplit,
                        (const Cx<float>*)t.twh,
-                       (const Cx<float>*)t.twt};
+                       (const Cx<float>*)t.twt,
+                       nullptr};
   return launch_hilbert_t<float>(a, t.L, halves, st);
 }
 

@@ -171,6 +171,7 @@ struct HilbertTables {
   void* ksplit = nullptr;
   void* twh = nullptr;
   void* twt = nullptr;
+  void* ksym = nullptr;  // complex128: the centred kernel's real spectrum halves
   double* partial = nullptr;
   long long partial_cols = 0;
 };

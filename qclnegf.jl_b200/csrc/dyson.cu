@@ -107,6 +107,163 @@ template <typename RS, typename RL, int NP, int BPC> constexpr int dyson_min_cta
   return n < 1 ? 1 : n;
 }
 
+// D build, equilibration and Gauss-Jordan of one N_b <= 24 block on a 32-lane
+// team with two-dimensional ownership: lane (rg, cg) = (lane / 4, lane % 4)
+// holds rows rg, rg + 8, rg + 16 and columns 6 cg .. 6 cg + 5 (18 entries), so
+// all 32 lanes update where one row per lane leaves 8 idle.  The arithmetic
+// per entry is that of the row-per-lane form (same pivot keys, deferred
+// scaling, speculative reciprocal); only the row sums of the equilibration
+// are added in a different order.  Step k: the 8 lanes holding column k
+// offer their best unused row, one warp max picks the pivot row p; those
+// lanes publish column k (the multipliers) and turn it into e_p; the 4 lanes
+// holding row p publish it; every lane then updates its 18 entries.  Writes
+// G (inverse columns in pivot order) into the team's G tile and the scale.
+template <typename RS, typename RL, int BPC>
+__device__ __forceinline__ void dyson_gj_2d24(const DysonArgs<RS>& p, Cx<RS>* X, Cx<RS>* G, DysonScratch<32>& S,
+                                              Cx<RS>* bufX, int team, int tt, int e, int e0, int m, bool live,
+                                              const Cx<RS>* first_sig, bool first_is_L) {
+  constexpr int NP = 24, RW = 3, CW = 6;
+  const int N = p.N, NE = p.NE, Nk = p.Nk;
+  const int rg = tt >> 2, cg = tt & 3;
+  Cx<RL> w[RW][CW];
+  const double eps_e = live ? p.eps[e] : 0.0;
+  double rmax = 0.0;
+#pragma unroll
+  for (int i = 0; i < RW; ++i) {
+    const int row = rg + 8 * i;
+    double rsum = 0.0;
+#pragma unroll
+    for (int c = 0; c < CW; ++c) {
+      const int col = CW * cg + c;
+      Cx<RL> d = cx<RL>(0, 0);
+      if (row < N && col < N) {
+        const Cx<double> hv = p.h[(size_t)m + (size_t)Nk * ((size_t)row + (size_t)N * col)];
+        const Cx<RS> sv = X[sw<NP>(row, col)];
+        double re = -hv.x - (double)sv.x, im = -hv.y - (double)sv.y;
+        if (row == col) {
+          re += eps_e;
+          im += p.eta;
+        }
+        d = cx<RL>((RL)re, (RL)im);
+        rsum += sqrt(re * re + im * im);
+      }
+      w[i][c] = d;
+    }
+    rsum += __shfl_xor_sync(0xffffffffu, rsum, 1);  // the row's four column groups
+    rsum += __shfl_xor_sync(0xffffffffu, rsum, 2);
+    rmax = fmax(rmax, rsum);
+  }
+  __syncthreads();  // every team has read its SigmaR tile: bufX is free
+  // prefetch the first Keldysh input while the inversion runs
+  if (first_sig && (first_is_L ? p.GL : p.GG)) load_blocks_async<RS, NP, BPC>(first_sig, bufX, NP * NP, e0, m, NE, Nk, N);
+  const double s = team_max<32>(rmax, tt, S.red, team);
+  const RL inv_s = (RL)(1.0 / s);
+  const bool scale_ok = s > 0.0 && isfinite(s);
+#pragma unroll
+  for (int i = 0; i < RW; ++i)
+#pragma unroll
+    for (int c = 0; c < CW; ++c) {
+      const int row = rg + 8 * i, col = CW * cg + c;
+      w[i][c] = inv_s * w[i][c];
+      if (row >= N && col == row) w[i][c] = cx<RL>(1, 0);  // identity padding
+    }
+
+  // rows rg + 8 i; bit i of `used` set once the row has been a pivot
+  unsigned used = 0u;
+  bool singular = !scale_ok;
+  int zstep = -1;
+  int mystep[RW];
+  Cx<RL> myrc[RW];
+#pragma unroll
+  for (int i = 0; i < RW; ++i) {
+    mystep[i] = rg + 8 * i;
+    myrc[i] = cx<RL>(1, 0);
+  }
+  Cx<RL>* rb0 = reinterpret_cast<Cx<RL>*>(G);  // 2 x (row NP | column NP | reciprocal)
+#pragma unroll 1
+  for (int kc = 0; kc < NP / CW; ++kc) {
+    const bool own = cg == kc;
+#pragma unroll
+    for (int u = 0; u < CW; ++u) {
+      const int k = kc * CW + u;
+      // this lane's best unused row in column k (keys as the row-per-lane form)
+      unsigned key = 0u;
+      Cx<RL> cv = cx<RL>(0, 0);
+#pragma unroll
+      for (int i = 0; i < RW; ++i) {
+        const unsigned ki = own && !((used >> i) & 1u) ? pivot_key(cabs1(w[i][u]), rg + 8 * i) : 0u;
+        if (ki > key) {
+          key = ki;
+          cv = w[i][u];
+        }
+      }
+      const Cx<RL> rc = crecip_pivot(cv);  // speculative, off the argmax path
+      key = __reduce_max_sync(0xffffffffu, key);
+      const int best = 63 - (int)(key & 63u);
+      const bool zero = pivot_key_zero(key);
+      singular |= zero;
+      if (zero && zstep < 0) zstep = k;
+      if (tt == 0) S.pivrow[k] = best;
+      Cx<RL>* rb = rb0 + (k & 1) * (2 * NP + 1);
+      // column k: the multipliers (zero for the pivot row), then e_best in place
+#pragma unroll
+      for (int i = 0; i < RW; ++i) {
+        const bool isp = rg + 8 * i == best;
+        st_shared_if(rb + NP + rg + 8 * i, isp ? cx<RL>(0, 0) : w[i][u], own);
+        if (own) w[i][u] = isp ? cx<RL>(1, 0) : cx<RL>(0, 0);
+      }
+      // row best: slot best / 8 of the four lanes with rg = best % 8
+      const bool prow = rg == (best & 7);
+#pragma unroll
+      for (int i = 0; i < RW; ++i)
+#pragma unroll
+        for (int c = 0; c < CW; ++c) st_shared_if(rb + CW * cg + c, w[i][c], prow && (best >> 3) == i);
+      Cx<RL> rp;
+      const int plane = ((best & 7) << 2) | kc;
+      rp.x = __shfl_sync(0xffffffffu, rc.x, plane);
+      rp.y = __shfl_sync(0xffffffffu, rc.y, plane);
+      team_sync<32>(team);
+      if (zero) rp = cx<RL>(0, 0);
+      if (rg == (best & 7)) {
+        const int i = best >> 3;
+        used |= 1u << i;
+        mystep[0] = i == 0 ? k : mystep[0];
+        mystep[1] = i == 1 ? k : mystep[1];
+        mystep[2] = i == 2 ? k : mystep[2];
+        myrc[0] = i == 0 ? rp : myrc[0];
+        myrc[1] = i == 1 ? rp : myrc[1];
+        myrc[2] = i == 2 ? rp : myrc[2];
+      }
+      Cx<RL> pv[CW];
+#pragma unroll
+      for (int c = 0; c < CW; ++c) pv[c] = rb[CW * cg + c];
+#pragma unroll
+      for (int i = 0; i < RW; ++i) {
+        const Cx<RL> fp = rb[NP + rg + 8 * i] * rp;
+#pragma unroll
+        for (int c = 0; c < CW; ++c) cfms(w[i][c], fp, pv[c]);
+      }
+    }
+  }
+  team_sync<32>(team);
+  if (singular && live && tt == 0)
+    record_status(p.status, QCL_SINGULAR,
+                  ((long long)e + (long long)NE * m) * kSingularPivotSpan + (scale_ok ? zstep + 1 : 0));
+  // inverse(D/s)[step][pivrow[k']] = w[k'] / pivot(step);  GR = that / s
+#pragma unroll
+  for (int i = 0; i < RW; ++i) {
+    const Cx<RL> rs = inv_s * myrc[i];
+#pragma unroll
+    for (int c = 0; c < CW; ++c) {
+      const int col = S.pivrow[CW * cg + c];
+      Cx<RL> g = rs * w[i][c];
+      if (mystep[i] >= N || col >= N) g = cx<RL>(0, 0);
+      G[sw<NP>(mystep[i], col)] = cvt<RS>(g);
+    }
+  }
+  if (tt == 0 && live && p.scale) p.scale[(size_t)e + (size_t)NE * m] = s;
+}
+
 // RS: storage precision, RL: inversion precision, RM: product precision.
 template <typename RS, typename RL, typename RM, int NP, int BPC>
 __global__ void __launch_bounds__(BPC* Tile<NP>::TT, (dyson_min_ctas<RS, RL, NP, BPC>()))
@@ -139,143 +296,150 @@ __global__ void __launch_bounds__(BPC* Tile<NP>::TT, (dyson_min_ctas<RS, RL, NP,
   cp_async_wait_all();
   __syncthreads();
 
-  // ---- D rows into registers, row-sum equilibration ---------------------------
-  const int row = tt / CPR, chunk = tt % CPR;
-  const bool has_row = row < NP;
-  Cx<RL> w[COLS];
-  const double eps_e = live ? p.eps[e] : 0.0;
-  double rowsum = 0.0;
-#pragma unroll
-  for (int j = 0; j < COLS; ++j) {
-    const int col = chunk * COLS + j;
-    Cx<RL> d = cx<RL>(0, 0);
-    if (has_row && row < N && col < N) {
-      const Cx<double> hv = p.h[(size_t)m + (size_t)Nk * ((size_t)row + (size_t)N * col)];
-      const Cx<RS> sv = X[sw<NP>(row, col)];
-      double re = -hv.x - (double)sv.x, im = -hv.y - (double)sv.y;
-      if (row == col) {
-        re += eps_e;
-        im += p.eta;
-      }
-      d = cx<RL>((RL)re, (RL)im);
-      rowsum += sqrt(re * re + im * im);
-    }
-    w[j] = d;
-  }
-  __syncthreads();  // every team has read its SigmaR tile: bufX is free
-  // prefetch the first Keldysh input while the inversion runs
-  if (first_sig && (first_is_L ? p.GL : p.GG)) load_blocks_async<RS, NP, BPC>(first_sig, bufX, MSZ, e0, m, NE, Nk, N);
-
-#pragma unroll
-  for (int o = 1; o < CPR; o <<= 1) rowsum += __shfl_xor_sync(0xffffffffu, rowsum, o);
-  const double s = team_max<TT>(rowsum, tt, S.red, team);
-  const RL inv_s = (RL)(1.0 / s);
-  const bool scale_ok = s > 0.0 && isfinite(s);
-#pragma unroll
-  for (int j = 0; j < COLS; ++j) {
-    const int col = chunk * COLS + j;
-    w[j] = inv_s * w[j];
-    if (has_row && row >= N && col == row) w[j] = cx<RL>(1, 0);  // identity padding
-  }
-
-  // ---- register-resident Gauss-Jordan, implicit pivoting, deferred scaling ----
-  // Step k picks the pivot row p among the unused rows (largest |Re|+|Im| in
-  // column k), every other row i does  w_i[k] = 0;  w_i -= (w_i[k] / w_p[k]) w_p
-  // with w_p[k] replaced by 1, and row p is left unscaled (its column-k entry
-  // becomes 1).  A row that was pivot at step k is then 1 / w_p[k] times the
-  // row of the standard in-place inverse, and it stays that multiple under the
-  // later (linear) updates, so the division by the pivot is applied once per
-  // row at the end instead of to the whole pivot row at every step.
-  bool used = !has_row;
-  bool singular = !scale_ok;
-  int zstep = -1;  // first step without a non-zero pivot (the k of SingularException(k) is zstep + 1)
-  int mystep = row;
-  Cx<RL> myrc = cx<RL>(1, 0);
-  const int lane = threadIdx.x & 31;
-  const int srclane = lane - chunk;  // first lane of this row's chunk group
-#pragma unroll 1
-  for (int kc = 0; kc < CPR; ++kc) {
-#pragma unroll 1
-    for (int grp = 0; grp < GROUPS; ++grp) {
-#pragma unroll
-      for (int u = 0; u < U; ++u) {
-        // Steps k >= N (padding) pick the identity rows and change nothing.
-        const int k = kc * COLS + grp * U + u;
-        const Cx<RL> wk = w[u];  // column k in the lanes of chunk kc (rotated chunk)
-        const bool cand = !used && chunk == kc;
-        const Cx<RL> rc = crecip_pivot(wk);  // speculative, off the argmax path
-        unsigned key = cand ? pivot_key(cabs1(wk), row) : 0u;
-        key = __reduce_max_sync(0xffffffffu, key);
-        if (TT > 32) {
-          if (lane == 0) S.wkey[(k & 1) * (TT / 32) + (tt >> 5)] = key;
-          team_sync<TT>(team);
-#pragma unroll
-          for (int q = 0; q < TT / 32; ++q) key = max(key, S.wkey[(k & 1) * (TT / 32) + q]);
-        }
-        const int best = 63 - (int)(key & 63u);
-        const bool zero = pivot_key_zero(key);
-        singular |= zero;
-        if (zero && zstep < 0) zstep = k;
-        if (tt == 0) S.pivrow[k] = best;
-        Cx<RL> f = wk;
-        if (CPR > 1) {
-          f.x = __shfl_sync(0xffffffffu, wk.x, srclane + kc);
-          f.y = __shfl_sync(0xffffffffu, wk.y, srclane + kc);
-        }
-        const bool is_pivot = row == best;
-        if (chunk == kc) w[u] = is_pivot ? cx<RL>(1, 0) : cx<RL>(0, 0);
-        Cx<RL>* rb = rowbuf + (k & 1) * (NP + 1);
-#pragma unroll
-        for (int j = 0; j < COLS; ++j) st_shared_if(rb + chunk * COLS + j, w[j], is_pivot);
-        Cx<RL> rp;
-        if (TT == 32) {
-          const int plane = (best * CPR + kc) & 31;
-          rp.x = __shfl_sync(0xffffffffu, rc.x, plane);
-          rp.y = __shfl_sync(0xffffffffu, rc.y, plane);
-          team_sync<TT>(team);
-        } else {
-          st_shared_if(rb + NP, rc, is_pivot && chunk == kc);
-          team_sync<TT>(team);
-          rp = rb[NP];
-        }
-        if (zero) rp = cx<RL>(0, 0);
-        used |= is_pivot;
-        mystep = is_pivot ? k : mystep;
-        myrc = is_pivot ? rp : myrc;
-        const Cx<RL> fp = is_pivot ? cx<RL>(0, 0) : f * rp;
-#pragma unroll
-        for (int j = 0; j < COLS; ++j) cfms(w[j], fp, rb[chunk * COLS + j]);
-      }
-      if (GROUPS > 1) {  // rotate the chunk so that the next group is at w[0..U)
-        Cx<RL> t[U];
-#pragma unroll
-        for (int j = 0; j < U; ++j) t[j] = w[j];
-#pragma unroll
-        for (int j = 0; j < COLS - U; ++j) w[j] = w[j + U];
-#pragma unroll
-        for (int j = 0; j < U; ++j) w[COLS - U + j] = t[j];
-      }
-    }
-  }
-  team_sync<TT>(team);
-  // where = block * 64 + k: k = 0 for a zero or non-finite row-sum scale, else the 1-based first zero
-  // pivot (LAPACK getrf's info), as SingularException(k) in production_operators.jl:39, 94, 1372
-  if (singular && live && tt == 0)
-    record_status(p.status, QCL_SINGULAR,
-                  ((long long)e + (long long)NE * m) * kSingularPivotSpan + (scale_ok ? zstep + 1 : 0));
-  // inverse(D/s)[step][pivrow[k']] = w[k'] / pivot(step);  GR = that / s
-  if (has_row) {
-    const Cx<RL> rs = inv_s * myrc;
-#pragma unroll
+  // two-dimensional ownership at N_b <= 24 in complex128 and complex64 (3.59 -> 3.51 ms and 2.64 ->
+  // 2.58 ms on the 4096 x 32 batch); mixed precision keeps one row per lane, where the FP64 rows beside
+  // FP32 tiles at 4 CTAs per SM would spill (3.46 -> 3.85 ms)
+  if constexpr (NP == 24 && sizeof(RS) == sizeof(RL)) {
+    dyson_gj_2d24<RS, RL, BPC>(p, X, G, S, bufX, team, tt, e, e0, m, live, first_sig, first_is_L);
+  } else {
+    // ---- D rows into registers, row-sum equilibration ---------------------------
+    const int row = tt / CPR, chunk = tt % CPR;
+    const bool has_row = row < NP;
+    Cx<RL> w[COLS];
+    const double eps_e = live ? p.eps[e] : 0.0;
+    double rowsum = 0.0;
+  #pragma unroll
     for (int j = 0; j < COLS; ++j) {
-      const int kp = chunk * COLS + j;
-      const int col = S.pivrow[kp];
-      Cx<RL> g = rs * w[j];
-      if (mystep >= N || col >= N) g = cx<RL>(0, 0);
-      G[sw<NP>(mystep, col)] = cvt<RS>(g);
+      const int col = chunk * COLS + j;
+      Cx<RL> d = cx<RL>(0, 0);
+      if (has_row && row < N && col < N) {
+        const Cx<double> hv = p.h[(size_t)m + (size_t)Nk * ((size_t)row + (size_t)N * col)];
+        const Cx<RS> sv = X[sw<NP>(row, col)];
+        double re = -hv.x - (double)sv.x, im = -hv.y - (double)sv.y;
+        if (row == col) {
+          re += eps_e;
+          im += p.eta;
+        }
+        d = cx<RL>((RL)re, (RL)im);
+        rowsum += sqrt(re * re + im * im);
+      }
+      w[j] = d;
     }
+    __syncthreads();  // every team has read its SigmaR tile: bufX is free
+    // prefetch the first Keldysh input while the inversion runs
+    if (first_sig && (first_is_L ? p.GL : p.GG)) load_blocks_async<RS, NP, BPC>(first_sig, bufX, MSZ, e0, m, NE, Nk, N);
+
+  #pragma unroll
+    for (int o = 1; o < CPR; o <<= 1) rowsum += __shfl_xor_sync(0xffffffffu, rowsum, o);
+    const double s = team_max<TT>(rowsum, tt, S.red, team);
+    const RL inv_s = (RL)(1.0 / s);
+    const bool scale_ok = s > 0.0 && isfinite(s);
+  #pragma unroll
+    for (int j = 0; j < COLS; ++j) {
+      const int col = chunk * COLS + j;
+      w[j] = inv_s * w[j];
+      if (has_row && row >= N && col == row) w[j] = cx<RL>(1, 0);  // identity padding
+    }
+
+    // ---- register-resident Gauss-Jordan, implicit pivoting, deferred scaling ----
+    // Step k picks the pivot row p among the unused rows (largest |Re|+|Im| in
+    // column k), every other row i does  w_i[k] = 0;  w_i -= (w_i[k] / w_p[k]) w_p
+    // with w_p[k] replaced by 1, and row p is left unscaled (its column-k entry
+    // becomes 1).  A row that was pivot at step k is then 1 / w_p[k] times the
+    // row of the standard in-place inverse, and it stays that multiple under the
+    // later (linear) updates, so the division by the pivot is applied once per
+    // row at the end instead of to the whole pivot row at every step.
+    bool used = !has_row;
+    bool singular = !scale_ok;
+    int zstep = -1;  // first step without a non-zero pivot (the k of SingularException(k) is zstep + 1)
+    int mystep = row;
+    Cx<RL> myrc = cx<RL>(1, 0);
+    const int lane = threadIdx.x & 31;
+    const int srclane = lane - chunk;  // first lane of this row's chunk group
+  #pragma unroll 1
+    for (int kc = 0; kc < CPR; ++kc) {
+  #pragma unroll 1
+      for (int grp = 0; grp < GROUPS; ++grp) {
+  #pragma unroll
+        for (int u = 0; u < U; ++u) {
+          // Steps k >= N (padding) pick the identity rows and change nothing.
+          const int k = kc * COLS + grp * U + u;
+          const Cx<RL> wk = w[u];  // column k in the lanes of chunk kc (rotated chunk)
+          const bool cand = !used && chunk == kc;
+          const Cx<RL> rc = crecip_pivot(wk);  // speculative, off the argmax path
+          unsigned key = cand ? pivot_key(cabs1(wk), row) : 0u;
+          key = __reduce_max_sync(0xffffffffu, key);
+          if (TT > 32) {
+            if (lane == 0) S.wkey[(k & 1) * (TT / 32) + (tt >> 5)] = key;
+            team_sync<TT>(team);
+  #pragma unroll
+            for (int q = 0; q < TT / 32; ++q) key = max(key, S.wkey[(k & 1) * (TT / 32) + q]);
+          }
+          const int best = 63 - (int)(key & 63u);
+          const bool zero = pivot_key_zero(key);
+          singular |= zero;
+          if (zero && zstep < 0) zstep = k;
+          if (tt == 0) S.pivrow[k] = best;
+          Cx<RL> f = wk;
+          if (CPR > 1) {
+            f.x = __shfl_sync(0xffffffffu, wk.x, srclane + kc);
+            f.y = __shfl_sync(0xffffffffu, wk.y, srclane + kc);
+          }
+          const bool is_pivot = row == best;
+          if (chunk == kc) w[u] = is_pivot ? cx<RL>(1, 0) : cx<RL>(0, 0);
+          Cx<RL>* rb = rowbuf + (k & 1) * (NP + 1);
+  #pragma unroll
+          for (int j = 0; j < COLS; ++j) st_shared_if(rb + chunk * COLS + j, w[j], is_pivot);
+          Cx<RL> rp;
+          if (TT == 32) {
+            const int plane = (best * CPR + kc) & 31;
+            rp.x = __shfl_sync(0xffffffffu, rc.x, plane);
+            rp.y = __shfl_sync(0xffffffffu, rc.y, plane);
+            team_sync<TT>(team);
+          } else {
+            st_shared_if(rb + NP, rc, is_pivot && chunk == kc);
+            team_sync<TT>(team);
+            rp = rb[NP];
+          }
+          if (zero) rp = cx<RL>(0, 0);
+          used |= is_pivot;
+          mystep = is_pivot ? k : mystep;
+          myrc = is_pivot ? rp : myrc;
+          const Cx<RL> fp = is_pivot ? cx<RL>(0, 0) : f * rp;
+  #pragma unroll
+          for (int j = 0; j < COLS; ++j) cfms(w[j], fp, rb[chunk * COLS + j]);
+        }
+        if (GROUPS > 1) {  // rotate the chunk so that the next group is at w[0..U)
+          Cx<RL> t[U];
+  #pragma unroll
+          for (int j = 0; j < U; ++j) t[j] = w[j];
+  #pragma unroll
+          for (int j = 0; j < COLS - U; ++j) w[j] = w[j + U];
+  #pragma unroll
+          for (int j = 0; j < U; ++j) w[COLS - U + j] = t[j];
+        }
+      }
+    }
+    team_sync<TT>(team);
+    // where = block * 64 + k: k = 0 for a zero or non-finite row-sum scale, else the 1-based first zero
+    // pivot (LAPACK getrf's info), as SingularException(k) in production_operators.jl:39, 94, 1372
+    if (singular && live && tt == 0)
+      record_status(p.status, QCL_SINGULAR,
+                    ((long long)e + (long long)NE * m) * kSingularPivotSpan + (scale_ok ? zstep + 1 : 0));
+    // inverse(D/s)[step][pivrow[k']] = w[k'] / pivot(step);  GR = that / s
+    if (has_row) {
+      const Cx<RL> rs = inv_s * myrc;
+  #pragma unroll
+      for (int j = 0; j < COLS; ++j) {
+        const int kp = chunk * COLS + j;
+        const int col = S.pivrow[kp];
+        Cx<RL> g = rs * w[j];
+        if (mystep >= N || col >= N) g = cx<RL>(0, 0);
+        G[sw<NP>(mystep, col)] = cvt<RS>(g);
+      }
+    }
+    if (tt == 0 && live && p.scale) p.scale[(size_t)e + (size_t)NE * m] = s;
   }
-  if (tt == 0 && live && p.scale) p.scale[(size_t)e + (size_t)NE * m] = s;
   __syncthreads();
   if (p.GR) store_blocks<RS, RS, NP, BPC>(p.GR, bufG, MSZ, e0, m, NE, Nk, N);
 

@@ -53,7 +53,7 @@ def parse():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-extras", action="store_true", help="skip the variant and SCBA side measurements")
-    ap.add_argument("--capture", choices=["dyson", "hilbert", "scba", "tcgemm", "scba_all_mixed", "scba_all_c128",
+    ap.add_argument("--capture", choices=["dyson", "step", "hilbert", "scba", "tcgemm", "scba_all_mixed", "scba_all_c128",
                                           "separable", "full_physics_mixed"],
                     help="run one small case of a kernel for an ncu capture (2 launches) and exit")
     ap.add_argument("--study", choices=["full_physics_converged", "full_physics_converged_mixed",
@@ -840,9 +840,10 @@ def scba_all_mechanisms(torch, NE_=1024, Nk_=32, Nb_=16, warm=2, timed=7):
 
 
 def run_capture(kind):
-    """Small cases for ncu: the same kernels as the timed step on a quarter of
-    the momenta (dyson: N_E x N_k = 4096 x 8, N_b = 24, c128, G^R + G^<), 4096
-    Hilbert columns at L = 8192, or 3 tutorial SCBA iterations."""
+    """Cases for ncu: the same kernels as the timed step on a quarter of the
+    momenta (dyson: N_E x N_k = 4096 x 8, N_b = 24, c128, G^R + G^<), the full
+    step three times (step: for a one-metric launch list only), 4096 Hilbert
+    columns at L = 8192, or 3 tutorial SCBA iterations."""
     import torch
 
     from qclb200 import _lib
@@ -864,6 +865,22 @@ def run_capture(kind):
                                                P(hf.data_ptr()), P(SR.data_ptr()), P(SL.data_ptr()), None,
                                                P(GR.data_ptr()), P(GL.data_ptr()), None, None, None, None,
                                                P(st.data_ptr())))
+    elif kind == "step":
+        # the bench step itself at full size (Dyson + Keldysh on 4096 x 32 blocks
+        # with the built-in CTA shape, which the autotuner also picks on this
+        # batch, then the Hilbert transform of all 18 432 columns), 3 times
+        hf, SR, SL, Gam = device_inputs(torch, dev, NB, seed=7, cdt=torch.complex128)
+        GR, GL, Lam = torch.empty_like(SR), torch.empty_like(SR), torch.empty_like(Gam)
+        st = torch.zeros(2, dtype=torch.int32, device=dev)
+        wE_d = torch.tensor(wE, dtype=torch.float64, device=dev)
+        for _ in range(3):
+            _lib.check(L.qcl_dev_dyson_keldysh(sp, _lib.QCL_C128, NE, NK, NB, P(eps_d.data_ptr()), 0.0,
+                                               P(hf.data_ptr()), P(SR.data_ptr()), P(SL.data_ptr()), None,
+                                               P(GR.data_ptr()), P(GL.data_ptr()), None, None, None, None,
+                                               P(st.data_ptr())))
+            _lib.check(L.qcl_dev_fft_hilbert_transform(sp, _lib.QCL_C128, NE, NK * NB * NB, float(eps[1] - eps[0]),
+                                                       P(wE_d.data_ptr()), P(Gam.data_ptr()), P(Lam.data_ptr()),
+                                                       None))
     elif kind == "hilbert":
         ncols = 4096
         g = torch.Generator(device=dev)

@@ -168,49 +168,46 @@ __device__ __forceinline__ void dyson_gj_2d24(const DysonArgs<RS>& p, Cx<RS>* X,
       if (row >= N && col == row) w[i][c] = cx<RL>(1, 0);  // identity padding
     }
 
-  // rows rg + 8 i; bit i of `used` set once the row has been a pivot
+  // rows rg + 8 i; bit i of `used` set once the row has been a pivot.  The G
+  // tile holds, until the elimination ends, two step buffers (pivot row,
+  // multipliers, spare slot), then each row's pivot reciprocal and step.
   unsigned used = 0u;
   bool singular = !scale_ok;
   int zstep = -1;
-  int mystep[RW];
-  Cx<RL> myrc[RW];
-#pragma unroll
-  for (int i = 0; i < RW; ++i) {
-    mystep[i] = rg + 8 * i;
-    myrc[i] = cx<RL>(1, 0);
-  }
-  Cx<RL>* rb0 = reinterpret_cast<Cx<RL>*>(G);  // 2 x (row NP | column NP | reciprocal)
+  Cx<RL>* rb0 = reinterpret_cast<Cx<RL>*>(G);
+  Cx<RL>* rcrow = rb0 + 2 * (2 * NP + 1);
+  int* stepof = reinterpret_cast<int*>(rcrow + NP);
+  static_assert((2 * (2 * NP + 1) + NP) * sizeof(Cx<RL>) + NP * sizeof(int) <= NP * NP * sizeof(Cx<RS>),
+                "elimination scratch fits the G tile");
 #pragma unroll 1
   for (int kc = 0; kc < NP / CW; ++kc) {
     const bool own = cg == kc;
 #pragma unroll
     for (int u = 0; u < CW; ++u) {
       const int k = kc * CW + u;
-      // this lane's best unused row in column k (keys as the row-per-lane form)
-      unsigned key = 0u;
-      Cx<RL> cv = cx<RL>(0, 0);
+      // this lane's best unused row in column k (keys as the row-per-lane form;
+      // non-zero keys are distinct, so the winner is found by equality)
+      unsigned kk[RW];
 #pragma unroll
-      for (int i = 0; i < RW; ++i) {
-        const unsigned ki = own && !((used >> i) & 1u) ? pivot_key(cabs1(w[i][u]), rg + 8 * i) : 0u;
-        if (ki > key) {
-          key = ki;
-          cv = w[i][u];
-        }
-      }
+      for (int i = 0; i < RW; ++i)
+        kk[i] = own && !((used >> i) & 1u) ? pivot_key(cabs1(w[i][u]), rg + 8 * i) : 0u;
+      const unsigned mykey = max(kk[0], max(kk[1], kk[2]));
+      Cx<RL> cv = mykey == kk[1] ? w[1][u] : w[0][u];
+      cv = mykey == kk[2] ? w[2][u] : cv;
       const Cx<RL> rc = crecip_pivot(cv);  // speculative, off the argmax path
-      key = __reduce_max_sync(0xffffffffu, key);
+      const unsigned key = __reduce_max_sync(0xffffffffu, mykey);
       const int best = 63 - (int)(key & 63u);
       const bool zero = pivot_key_zero(key);
+      const bool plane = own && mykey == key;  // the lane holding the pivot
       singular |= zero;
       if (zero && zstep < 0) zstep = k;
       if (tt == 0) S.pivrow[k] = best;
       Cx<RL>* rb = rb0 + (k & 1) * (2 * NP + 1);
-      // column k: the multipliers (zero for the pivot row), then e_best in place
+      // column k: the multipliers, then e_best in place
 #pragma unroll
       for (int i = 0; i < RW; ++i) {
-        const bool isp = rg + 8 * i == best;
-        st_shared_if(rb + NP + rg + 8 * i, isp ? cx<RL>(0, 0) : w[i][u], own);
-        if (own) w[i][u] = isp ? cx<RL>(1, 0) : cx<RL>(0, 0);
+        st_shared_if(rb + NP + rg + 8 * i, w[i][u], own);
+        if (own) w[i][u] = rg + 8 * i == best ? cx<RL>(1, 0) : cx<RL>(0, 0);
       }
       // row best: slot best / 8 of the four lanes with rg = best % 8
       const bool prow = rg == (best & 7);
@@ -218,22 +215,17 @@ __device__ __forceinline__ void dyson_gj_2d24(const DysonArgs<RS>& p, Cx<RS>* X,
       for (int i = 0; i < RW; ++i)
 #pragma unroll
         for (int c = 0; c < CW; ++c) st_shared_if(rb + CW * cg + c, w[i][c], prow && (best >> 3) == i);
+      // the pivot row's own multiplier is zero; its step and reciprocal are kept
+      st_shared_if(rb + NP + best, cx<RL>(0, 0), plane);
+      st_shared_if(rcrow + best, zero ? cx<RL>(0, 0) : rc, plane);
+      if (plane) stepof[best] = k;
       Cx<RL> rp;
-      const int plane = ((best & 7) << 2) | kc;
-      rp.x = __shfl_sync(0xffffffffu, rc.x, plane);
-      rp.y = __shfl_sync(0xffffffffu, rc.y, plane);
+      const int src = ((best & 7) << 2) | kc;
+      rp.x = __shfl_sync(0xffffffffu, rc.x, src);
+      rp.y = __shfl_sync(0xffffffffu, rc.y, src);
       team_sync<32>(team);
       if (zero) rp = cx<RL>(0, 0);
-      if (rg == (best & 7)) {
-        const int i = best >> 3;
-        used |= 1u << i;
-        mystep[0] = i == 0 ? k : mystep[0];
-        mystep[1] = i == 1 ? k : mystep[1];
-        mystep[2] = i == 2 ? k : mystep[2];
-        myrc[0] = i == 0 ? rp : myrc[0];
-        myrc[1] = i == 1 ? rp : myrc[1];
-        myrc[2] = i == 2 ? rp : myrc[2];
-      }
+      used |= prow ? 1u << (best >> 3) : 0u;
       Cx<RL> pv[CW];
 #pragma unroll
       for (int c = 0; c < CW; ++c) pv[c] = rb[CW * cg + c];
@@ -246,6 +238,14 @@ __device__ __forceinline__ void dyson_gj_2d24(const DysonArgs<RS>& p, Cx<RS>* X,
     }
   }
   team_sync<32>(team);
+  int mystep[RW];
+  Cx<RL> myrc[RW];
+#pragma unroll
+  for (int i = 0; i < RW; ++i) {
+    mystep[i] = stepof[rg + 8 * i];
+    myrc[i] = rcrow[rg + 8 * i];
+  }
+  team_sync<32>(team);  // the scratch is read before G overwrites it
   if (singular && live && tt == 0)
     record_status(p.status, QCL_SINGULAR,
                   ((long long)e + (long long)NE * m) * kSingularPivotSpan + (scale_ok ? zstep + 1 : 0));

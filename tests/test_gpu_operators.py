@@ -87,6 +87,33 @@ def test_dyson_singular_block_raises(gpu_ops):
     assert ex.value.k == 3
 
 
+@pytest.mark.parametrize("precision", ["c128", "c64", "mixed"])
+@pytest.mark.parametrize("N", [20, 24])
+def test_dyson_singular_block_pivot_index_at_padded_24(gpu_ops, N, precision):
+    """SingularException(k) with LAPACK getrf's k for blocks padded to 24 x 24
+    (the two-dimensional elimination in complex128 / complex64, one row per
+    lane in mixed precision): a zero scale, a rank-one block and a diagonal
+    block with one zero in the middle.  The energies are binary fractions, so
+    that D = eps I - Sigma^R is exact in complex64 storage as well."""
+    from qclb200 import SingularException
+
+    NE = 6
+    eps = 0.25 * np.arange(NE)
+    h = np.zeros((1, N, N), dtype=complex)
+    cases = [
+        (lambda e: np.zeros((N, N)), 0),  # D = 0 at eps[0] = 0
+        (lambda e: eps[e] * np.eye(N) - np.ones((N, N)), 2),  # D = ones: step 2 meets a zero column
+        (lambda e: eps[e] * np.eye(N) - np.diag([float(j + 1) if j != 9 else 0.0 for j in range(N)]), 10),
+    ]
+    for make, k in cases:
+        SR = np.zeros((NE, 1, N, N), dtype=complex, order="F")
+        for e in range(NE):
+            SR[e, 0] = make(e)
+        with pytest.raises(SingularException) as ex:
+            gpu_ops.retarded_green(eps, h, SR, precision=precision)
+        assert ex.value.k == k, (N, precision, k, ex.value.k)
+
+
 @pytest.mark.parametrize("NE", [37, 64, 400, 1000, 1025, 2048, 3001, 4096])
 def test_fft_hilbert_c128_matches_direct_pv(gpu_ops, orc, NE):
     rng = np.random.default_rng(NE)

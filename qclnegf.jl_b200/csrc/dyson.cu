@@ -98,11 +98,13 @@ template <typename RS, typename RL, int NP, int TT, int BPC> constexpr size_t dy
 
 // CTAs per SM that the shared memory allows (228 KB per SM, 1 KB reserved per
 // CTA), as the register budget's occupancy target -- but never below 128
-// registers per thread, where the elimination rows would spill.
+// registers per thread, where the elimination rows would spill (160 for the
+// two-dimensional elimination with FP64 entries at N_b <= 24).
 template <typename RS, typename RL, int NP, int BPC> constexpr int dyson_min_ctas() {
   constexpr size_t per = dyson_smem<RS, RL, NP, Tile<NP>::TT, BPC>() + 1024;
   constexpr int by_smem = (int)((228 * 1024) / per);
-  constexpr int by_regs = 65536 / (BPC * Tile<NP>::TT * 128);
+  constexpr int floor_regs = NP == 24 && sizeof(RL) == 8 ? 160 : 128;
+  constexpr int by_regs = 65536 / (BPC * Tile<NP>::TT * floor_regs);
   constexpr int n = by_smem < by_regs ? by_smem : by_regs;
   return n < 1 ? 1 : n;
 }
@@ -296,10 +298,8 @@ __global__ void __launch_bounds__(BPC* Tile<NP>::TT, (dyson_min_ctas<RS, RL, NP,
   cp_async_wait_all();
   __syncthreads();
 
-  // two-dimensional ownership at N_b <= 24 in complex128 and complex64 (3.59 -> 3.51 ms and 2.64 ->
-  // 2.58 ms on the 4096 x 32 batch); mixed precision keeps one row per lane, where the FP64 rows beside
-  // FP32 tiles at 4 CTAs per SM would spill (3.46 -> 3.85 ms)
-  if constexpr (NP == 24 && sizeof(RS) == sizeof(RL)) {
+  // two-dimensional ownership at N_b <= 24 (one row per lane leaves 8 of 32 lanes idle)
+  if constexpr (NP == 24) {
     dyson_gj_2d24<RS, RL, BPC>(p, X, G, S, bufX, team, tt, e, e0, m, live, first_sig, first_is_L);
   } else {
     // ---- D rows into registers, row-sum equilibration ---------------------------

@@ -93,8 +93,9 @@ def test_dyson_singular_block_pivot_index_at_padded_24(gpu_ops, N, precision):
     """SingularException(k) with LAPACK getrf's k for blocks padded to 24 x 24
     (the two-dimensional elimination in complex128 / complex64, one row per
     lane in mixed precision): a zero scale, a rank-one block and a diagonal
-    block with one zero in the middle.  The energies are binary fractions, so
-    that D = eps I - Sigma^R is exact in complex64 storage as well."""
+    block with one zero in the middle.  The energies are binary fractions and
+    the rank-one block's row sum is a power of two, so that D = eps I -
+    Sigma^R and its equilibration are exact in complex64 storage as well."""
     from qclb200 import SingularException
 
     NE = 6
@@ -102,7 +103,9 @@ def test_dyson_singular_block_pivot_index_at_padded_24(gpu_ops, N, precision):
     h = np.zeros((1, N, N), dtype=complex)
     cases = [
         (lambda e: np.zeros((N, N)), 0),  # D = 0 at eps[0] = 0
-        (lambda e: eps[e] * np.eye(N) - np.ones((N, N)), 2),  # D = ones: step 2 meets a zero column
+        # rank one, D = 1 v^T with row sum 16 (v = 1 ... 1, 1/2 ... 1/2): the
+        # equilibration is exact in complex64 too, so step 2 meets a zero column
+        (lambda e: eps[e] * np.eye(N) - np.outer(np.ones(N), [1.0] * (32 - N) + [0.5] * (2 * N - 32)), 2),
         (lambda e: eps[e] * np.eye(N) - np.diag([float(j + 1) if j != 9 else 0.0 for j in range(N)]), 10),
     ]
     for make, k in cases:

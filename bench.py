@@ -40,10 +40,11 @@ E0_EV = 0.1
 FLOP_PER_BLOCK = 24 * NB ** 3
 BYTES_PER_BLOCK = 4 * 16 * NB * NB
 # DRAM bytes (read + write) of one Dyson launch, from the ncu capture of
-# `bench.py --capture dyson` with the 3M DMMA Keldysh products and 4 blocks
-# per CTA (N_k = 8, a quarter of the blocks: 604.4 MB read, 560.6 MB written)
-# scaled by 4 to the bench launch; traffic grows with the block count.
-DYSON_TRAFFIC_BYTES = 4 * (604.4e6 + 560.6e6)
+# `bench.py --capture dyson` with the two-dimensional elimination, the 3M DMMA
+# Keldysh products and 4 blocks per CTA (N_k = 8, a quarter of the blocks:
+# 604.4 MB read, 561.2 MB written) scaled by 4 to the bench launch; traffic
+# grows with the block count.
+DYSON_TRAFFIC_BYTES = 4 * (604.4e6 + 561.2e6)
 
 
 def parse():

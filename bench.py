@@ -58,9 +58,11 @@ def parse():
                                           "separable", "full_physics_mixed"],
                     help="run one small case of a kernel for an ncu capture (2 launches) and exit")
     ap.add_argument("--study", choices=["full_physics_converged", "full_physics_converged_mixed",
-                                        "all_mechanisms_converged", "bias_sweep_64"],
+                                        "all_mechanisms_converged", "tutorial_converged", "bias_sweep_64",
+                                        "bias_sweep_small_64"],
                     help="run one long study (seconds to minutes of GPU time), print its JSON and exit: the "
-                         "full-physics SCBA converged in both precisions, or the 64-point batched bias sweep")
+                         "full-physics SCBA converged in both precisions, or a 64-point batched bias sweep "
+                         "(N_b 16-48, or small structures)")
     return ap.parse_args()
 
 
@@ -653,7 +655,8 @@ def extras(torch, dev, L, _lib):
                     ("scba_full_physics_N32", lambda: scba_full_physics(torch)),
                     ("bias_sweep_16", lambda: bias_sweep(torch, npoints=16, iters=12,
                                                          classes=((2, 8), (3, 8), (4, 8)),
-                                                         NE_choices=(1024, 1536, 2048)))):
+                                                         NE_choices=(1024, 1536, 2048))),
+                    ("bias_sweep_small_64", lambda: bias_sweep_small(torch))):
         try:
             out[key] = fn()
         except Exception as ex:  # noqa: BLE001
@@ -705,51 +708,93 @@ def scba_full_physics(torch, timed=(2, 4)):
 
 
 def bias_sweep(torch, npoints=64, iters=5, classes=((2, 8), (3, 8), (4, 8), (6, 8)),
-               NE_choices=(1024, 1536, 2048, 2560, 3072, 3584, 4096)):
+               NE_choices=(1024, 1536, 2048, 2560, 3072, 3584, 4096), Nk=32, Nqz=401, Nphi=64,
+               iterations_only=False):
     """The batched bias sweep: `npoints` bias points 20-70 mV per period over
-    structure classes N_b = 16 ... 48 and energy grids N_E from NE_choices,
-    N_k = 32, LO + acoustic + IFR, mixed precision, the Dyson CTA shape of
-    every class from the autotuner; `iters` iterations per point.  The
+    structure classes (periods x states; by default N_b = 16 ... 48) and
+    energy grids N_E from NE_choices, N_k momenta, LO + acoustic + IFR, mixed
+    precision, the Dyson CTA shape of every class from the autotuner; `iters`
+    iterations per point.  The
     batched run (qcl_sweep_run: resident points in one graph launch per
     iteration) against the same points one after another (qcl_scba_step),
     in SCBA iterations per second, and the largest J difference between the
-    two (the same kernels run, so it is zero)."""
+    two (the same kernels run, so it is zero).  With `iterations_only` the
+    iterations are also timed without context creation, seeds and graph
+    captures: each sequential point runs `iters` more iterations, timed on
+    their own, and the batched sweep runs again with 2 `iters` iterations per
+    point, the difference of the two batched wall times being its `iters`
+    iterations of every point."""
     import numpy as np
     from qclb200 import operators
     from qclb200.problem import bias_sweep_problems
     from qclb200.scba import BatchedSweep, ProductionSCBA
 
     t = time.perf_counter()
-    pts = bias_sweep_problems(npoints=npoints, classes=classes, NE_choices=NE_choices)
+    pts = bias_sweep_problems(npoints=npoints, classes=classes, NE_choices=NE_choices, Nk=Nk, Nqz=Nqz, Nphi=Nphi)
     res = {"build_s": time.perf_counter() - t, "points": npoints,
            "Nb": sorted({p.Nb for p in pts}), "NE": sorted({p.NE for p in pts})}
     tune = {}
     for nb in sorted({p.Nb for p in pts}):
-        tune[str(nb)] = operators.autotune(nb, precision="mixed", NE=1024, Nk=32)
+        tune[str(nb)] = operators.autotune(nb, precision="mixed", NE=max(p.NE for p in pts), Nk=Nk)
     res["autotune_mixed"] = tune
     torch.cuda.synchronize()
     t = time.perf_counter()
     Jseq = []
+    iter_s = 0.0
+    warm_s = 0.0
     for p in pts:
         s = ProductionSCBA(p, precision="mixed", use_graph=True)
         s.seed()
+        torch.cuda.synchronize()
+        ti = time.perf_counter()
         rows = s.run(iters)
+        iter_s += time.perf_counter() - ti
         Jseq.append(rows[-1]["J"])
+        if iterations_only:
+            ti = time.perf_counter()
+            s.run(iters)
+            warm_s += time.perf_counter() - ti
         s.close()
     torch.cuda.synchronize()
     seq_s = time.perf_counter() - t
     sw = BatchedSweep(pts, precision="mixed")
     rows, n_it, stats = sw.run(iters)
     sw.close()
-    res["sequential"] = {"wall_s": seq_s, "iter_per_s": npoints * iters / seq_s}
+    res["sequential"] = {"wall_s": seq_s, "iter_per_s": npoints * iters / seq_s, "iterations_only_s": iter_s}
     res["batched"] = dict(stats, iter_per_s=stats["iterations"] / stats["wall_s"])
     res["batched_speedup"] = res["batched"]["iter_per_s"] / res["sequential"]["iter_per_s"]
+    # lower bound: the batched wall time (context creation and seeds included)
+    # against the sequential iterations alone
+    res["batched_speedup_vs_sequential_iterations_only"] = iter_s / stats["wall_s"]
+    if iterations_only:
+        sw = BatchedSweep(pts, precision="mixed")
+        _, n2, stats2 = sw.run(2 * iters)
+        sw.close()
+        b_s = stats2["wall_s"] - stats["wall_s"]
+        res["iterations_only"] = {
+            "iterations_per_point": iters, "sequential_s": warm_s, "batched_s": b_s,
+            "sequential_ms_per_point_iteration": 1e3 * warm_s / (npoints * iters),
+            "batched_ms_per_point_iteration": 1e3 * b_s / (npoints * iters),
+            "speedup": warm_s / b_s,
+            "how": "sequential: iterations after the first `iters` of each point (graphs captured); batched: "
+                   "wall time of a 2 x iters sweep minus that of the iters sweep (creation, seeds and captures "
+                   "cancel)"}
     res["J_max_rel_diff_batched_vs_sequential"] = max(abs(r["J"] - j) / abs(j) for r, j in zip(rows, Jseq))
     operators.autotune_reset()
-    res["config"] = (f"{npoints} points, bias 20-70 mV/period, N_b in {res['Nb']}, N_E in {res['NE']}, N_k = 32, "
+    res["config"] = (f"{npoints} points, bias 20-70 mV/period, N_b in {res['Nb']}, N_E in {res['NE']}, N_k = {Nk}, "
                      f"LO + acoustic + IFR, mixed precision, {iters} iterations per point (seed and context "
                      "creation included in both wall times)")
     return res
+
+
+def bias_sweep_small(torch, npoints=64, iters=30):
+    """The batched sweep where one point does not fill the GPU: 64 bias points
+    of small structures (N_b = 12 and 16 as 3 x 4, 2 x 6 and 2 x 8 periods x
+    states; N_E in 256 ... 512, N_k = 8; LO + acoustic + IFR, mixed), whose
+    iterations are launch- and latency-bound alone and run side by side as
+    the child graphs of one launch."""
+    return bias_sweep(torch, npoints=npoints, iters=iters, classes=((3, 4), (2, 6), (2, 8)),
+                      NE_choices=(256, 384, 512), Nk=8, Nqz=101, Nphi=32, iterations_only=True)
 
 
 def scba_fixed_point_small(torch, tol=1e-10):
@@ -967,6 +1012,10 @@ def run_study(kind):
 
     if kind == "bias_sweep_64":
         out = bias_sweep(torch)
+    elif kind == "bias_sweep_small_64":
+        out = bias_sweep_small(torch)
+    elif kind == "tutorial_converged":
+        out = tutorial_converged(torch)
     elif kind == "all_mechanisms_converged":
         out = all_mechanisms_converged(torch)
     elif kind == "full_physics_converged_mixed":
@@ -977,7 +1026,7 @@ def run_study(kind):
 
 
 def converged_comparison(torch, pr, tol=1e-8, max_mixed=3000, max_fp64=3000, max_wall_s=2400.0,
-                         max_refine_s=1200.0, plain_fp64=True):
+                         max_refine_s=1200.0, plain_fp64=True, verbose=True):
     """One problem converged to r_Sigma <= tol both ways.  (1) mixed
     precision from the seed until r_Sigma stops falling (its complex64
     floor: the last 100 iterations did not get 10 % below the best before
@@ -986,13 +1035,14 @@ def converged_comparison(torch, pr, tol=1e-8, max_mixed=3000, max_fp64=3000, max
     fixed point J_fp.  (2) plain FP64 from the seed to tol, bounded by
     max_wall_s.  Iterations, device-synchronised wall seconds, r_Sigma
     traces, and the relative J differences against J_fp of the mixed floor
-    and of plain FP64."""
+    and of plain FP64.  `verbose`: progress lines on stderr and the first
+    leg's JSON on stdout before the second leg starts (the long studies)."""
     from qclb200.scba import ProductionSCBA
 
     out = {}
 
     def progress(leg, n, r):
-        if n % 25 == 0:
+        if verbose and n % 25 == 0:
             print(json.dumps({"leg": leg, "iteration": n, "r_Sigma": r["r_Sigma"], "J": r["J"]}), file=sys.stderr,
                   flush=True)
 
@@ -1030,7 +1080,8 @@ def converged_comparison(torch, pr, tol=1e-8, max_mixed=3000, max_fp64=3000, max
                               "fp64_r_Sigma_trace": [x["r_Sigma"] for x in rr[::5]]}
     out["J_rel_err_mixed_floor_vs_fp64_fixed_point"] = abs(best["J"] - Jfp) / abs(Jfp)
     out["mixed_s_per_iter"] = tm / len(rm)
-    print(json.dumps(out), flush=True)  # the first leg, in case the second is cut short
+    if verbose:
+        print(json.dumps(out), flush=True)  # the first leg, in case the second is cut short
     if not plain_fp64:
         return out
     t = time.perf_counter()
@@ -1071,6 +1122,29 @@ def full_physics_converged(torch, tol=1e-8, periods=2, states=16, alpha=0.8, cou
     out["config"] = (f"N_b = {pr.Nb} ({periods} periods x {states} states), N_E x N_k = {pr.NE} x {pr.Nk}, "
                      f"LO + acoustic + impurity + IFR + alloy, couplings {coupling_ev * 1e3:g} meV, "
                      f"T = {temperature_K:g} K, linear mixing alpha = {alpha}, tolerance r_Sigma <= {tol}")
+    return out
+
+
+def tutorial_converged(torch, tol=1e-8, mixing="anderson", **kw):
+    """The tutorial-scale problem (N_E x N_k = 400 x 16, N_b = 12, acoustic
+    phonons, mixing 0.3) converged both ways (converged_comparison): the
+    converged J of the mixed-precision floor, of the mixed run refined in
+    FP64, and of plain FP64.  Under linear mixing this structure still had
+    r_Sigma = 8.4e-5 after 15 000 iterations (J drifting by 1 % per 25
+    iterations), so the study mixes with Anderson (history depth 5) by
+    default."""
+    import dataclasses
+
+    from qclb200.problem import tutorial_problem
+
+    pr = dataclasses.replace(tutorial_problem(), mixing=mixing)
+    kw.setdefault("max_mixed", 4000)
+    kw.setdefault("max_fp64", 15000)
+    kw.setdefault("max_wall_s", 15.0)
+    kw.setdefault("max_refine_s", 15.0)
+    out = converged_comparison(torch, pr, tol=tol, **kw)
+    out["config"] = ("tutorial-sized synthetic supercell, N_E x N_k = 400 x 16, N_b = 12, acoustic phonons, "
+                     f"{mixing} mixing alpha = {pr.alpha}, tolerance r_Sigma <= {tol}, CUDA graphs on")
     return out
 
 

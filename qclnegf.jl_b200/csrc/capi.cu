@@ -877,7 +877,7 @@ int qcl_anderson_guard(int precision, int NE, int Nk, int Nb, int nfam, const vo
   DevBuf meta;
   if ((s = meta.alloc(sizeof(AndersonMeta)))) return s;
   if ((s = launch_anderson_reset((AndersonMeta*)meta.p, 0))) return s;
-  if ((s = launch_anderson_guard(sp, NE, Nk, Nb, ptr, nfam, (AndersonMeta*)meta.p, 0, 0))) return s;
+  if ((s = launch_anderson_guard(sp, NE, Nk, Nb, ptr, nfam, (AndersonMeta*)meta.p, 0, 0.0, 0))) return s;
   QCL_CUDA_CHECK(cudaDeviceSynchronize());
   AndersonMeta h;
   QCL_CUDA_CHECK(cudaMemcpy(&h, meta.p, sizeof(h), cudaMemcpyDeviceToHost));

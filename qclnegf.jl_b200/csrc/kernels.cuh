@@ -74,7 +74,7 @@ int launch_anderson_mix(int precision, size_t n, void* const* out, int nf, const
                         const AndersonMeta* m, double damping, int fallback, cudaStream_t st);
 int launch_anderson_after_guard(AndersonMeta* m, int pass, int* status, cudaStream_t st);
 int launch_anderson_guard(int precision, int NE, int Nk, int N, void* const* fields, int nfam, AndersonMeta* m,
-                          int pass, cudaStream_t st);
+                          int pass, double roundoff, cudaStream_t st);
 // dense kernel operators from angular node weights (kbuild.cu)
 size_t assemble_work_doubles();
 int launch_assemble_kernel(int form, int Nk, int Nb, int T, const double* W, const void* X, void* out, double* work,

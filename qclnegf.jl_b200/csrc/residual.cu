@@ -1132,6 +1132,7 @@ template <typename RS> static int launch_witness_detail_p(const WitnessArgs<RS>&
 constexpr int kGuardMaxFamilies = kMaxMixFields / 3;
 template <typename RS> struct GuardArgs {
   int NE, Nk, N, nfam, pass;
+  double eps;  // unit roundoff the budgets are scaled to (see launch_anderson_guard)
   const Cx<RS>* f[3 * kGuardMaxFamilies];
   AndersonMeta* meta;
 };
@@ -1159,10 +1160,9 @@ __global__ void __launch_bounds__(BPC* Tile<NP>::TT) anderson_guard_kernel(Guard
   if (p.pass == 1 && !p.meta->fallback) return;
   constexpr int TT = Tile<NP>::TT;
   constexpr size_t MSZ = (size_t)NP * NP;
-  // unit roundoff of the storage precision: the budgets of the reference
-  // (64 n eps ||X||, production_mixing.jl:48-118) scaled to the fields that
-  // are actually stored (complex64 fields carry FP32 rounding in every entry)
-  constexpr double eps = sizeof(RS) == 8 ? 2.220446049250313e-16 : 1.1920928955078125e-07;
+  // the budgets of the reference (64 n eps ||X||, production_mixing.jl:48-118)
+  // scaled to the rounding the checked fields actually carry
+  const double eps = p.eps;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   Cx<double>* bR = reinterpret_cast<Cx<double>*>(smem_raw);
   Cx<double>* bL = bR + BPC * MSZ;
@@ -1320,18 +1320,25 @@ template <typename RS> static int launch_guard_p(const GuardArgs<RS>& a, cudaStr
   }
 }
 
+// The budgets use the unit roundoff of the storage precision (complex64
+// fields carry FP32 rounding in every entry), or `roundoff` when that is
+// larger: a state promoted from complex64 to complex128 still carries the
+// FP32 rounding of the iterations that made it, and its near-zero
+// eigenvalues sit at that level.
 int launch_anderson_guard(int precision, int NE, int Nk, int N, void* const* fields, int nfam, AndersonMeta* m,
-                          int pass, cudaStream_t st) {
+                          int pass, double roundoff, cudaStream_t st) {
   if (nfam < 1 || nfam > kGuardMaxFamilies) {
     set_last_error("anderson guard: %d families out of range", nfam);
     return QCL_ARG;
   }
+  const double store_eps = precision == QCL_C128 ? 2.220446049250313e-16 : 1.1920928955078125e-07;
+  const double eps = roundoff > store_eps ? roundoff : store_eps;
   if (precision == QCL_C128) {
-    GuardArgs<double> a{NE, Nk, N, nfam, pass, {}, m};
+    GuardArgs<double> a{NE, Nk, N, nfam, pass, eps, {}, m};
     for (int i = 0; i < 3 * nfam; ++i) a.f[i] = (const Cx<double>*)fields[i];
     return launch_guard_p<double>(a, st);
   }
-  GuardArgs<float> a{NE, Nk, N, nfam, pass, {}, m};
+  GuardArgs<float> a{NE, Nk, N, nfam, pass, eps, {}, m};
   for (int i = 0; i < 3 * nfam; ++i) a.f[i] = (const Cx<float>*)fields[i];
   return launch_guard_p<float>(a, st);
 }

@@ -88,6 +88,9 @@ constexpr int kPhases = 7;
 struct ScbaCtx {
   int NE, Nk, N, M, precision, gs, verify;
   int refinement = 0;  // FP64-sized state and complex128 operator copies for qcl_scba_promote
+  // unit roundoff of the Anderson guard's budgets when above the storage
+  // precision's (a promoted state keeps the FP32 rounding it was made with)
+  double guard_roundoff = 0.0;
   int diagonal = 0, averaged = 0, drop_real = 0, direct_green = 0;  // scattering-model switches
   int scalar_lesser = 0;                                             // occupation_normalization
   int norm_branch = 0;  // paired normalisation form: 0 the reference's choice, 1 / 2 forced
@@ -801,7 +804,9 @@ static int iteration_body(ScbaCtx* c, std::vector<void*>& state, std::vector<voi
       if ((s = launch_anderson_mix(sp, c->nfield, cands, nf, c->Xh, c->Rh, c->and_depth, c->ameta, damping, pass,
                                    c->st)))
         return s;
-      if ((s = launch_anderson_guard(sp, c->NE, c->Nk, c->N, cands, F, c->ameta, pass, c->st))) return s;
+      if ((s = launch_anderson_guard(sp, c->NE, c->Nk, c->N, cands, F, c->ameta, pass, c->guard_roundoff,
+                                     c->st)))
+        return s;
       if ((s = launch_anderson_after_guard(c->ameta, pass, c->status, c->st))) return s;
     }
     QCL_CUDA_CHECK(cudaMemcpyAsync(c->ameta_h, c->ameta, sizeof(AndersonMeta), cudaMemcpyDeviceToHost, c->st));
@@ -1352,6 +1357,7 @@ int scba_promote(ScbaCtx* c) {
     m.tc_stage1.clear();
   }
   c->precision = QCL_C128;
+  c->guard_roundoff = 1.1920928955078125e-07;  // the promoted state's FP32 rounding
   c->fbytes = c->nfield * 16;
   if ((s = prepare_hilbert_tables(c->hil, c->NE, c->de, QCL_C128))) return s;
   if ((s = ensure_partial(c->hil, (long long)c->Nk * c->N * c->N))) return s;

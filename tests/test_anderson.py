@@ -118,6 +118,39 @@ def test_oracle_anderson_contracts_faster_than_linear(orc):
     assert [r["mixer"]["history_depth"] for r in ha] == [1, 2, 3, 4, 5, 5]
 
 
+def test_guard_budgets_of_a_state_stored_in_complex64(orc, monkeypatch):
+    """A state made in complex64 (a mixed-precision run promoted to
+    complex128 for its FP64 refinement) carries FP32 rounding in every entry.
+    The guard's budgets at FP64 roundoff (64 n eps ||X||) reject nearly every
+    block of it -- Sigma^R - Sigma^A = Sigma^> - Sigma^< and the
+    definiteness tests hold only to FP32 -- so a convex fallback towards
+    that state is refused and the refinement stops with a DomainError.  At
+    the FP32 roundoff the same blocks pass: the budgets a promoted context's
+    guard keeps (the roundoff argument of launch_anderson_guard, set by
+    qcl_scba_promote)."""
+    from qclb200.problem import small_problem
+
+    pr = small_problem(NE=41, Nk=3, Nb=4, mechanisms=("LO", "acoustic", "IFR"))
+    _, st = orc.scba(pr, 8, keep_state=True)
+    fams = [st["scattering"][m.name] for m in pr.mechanisms] + [st["plus"], st["minus"]]
+
+    def stored(a):
+        return np.asarray(a, np.complex64).astype(np.complex128)
+
+    def antiherm(a):  # the promotion keeps the anti-Hermitian part of Sigma^<, Sigma^>
+        return 0.5 * (a - np.conj(np.swapaxes(a, -1, -2)))
+
+    blocks = [(stored(R)[e, m], antiherm(stored(L))[e, m], antiherm(stored(G))[e, m])
+              for R, L, G in fams for e in range(pr.NE) for m in range(pr.Nk)]
+    # the FP64 state itself passes at FP64 budgets
+    assert all(orc.anderson_block_failure(R[e, m], L[e, m], G[e, m]) == 0
+               for R, L, G in fams for e in range(pr.NE) for m in range(pr.Nk))
+    failing = sum(orc.anderson_block_failure(*b) != 0 for b in blocks)
+    assert failing > len(blocks) // 2
+    monkeypatch.setattr(orc, "_EPS", 2.0 ** -23)
+    assert all(orc.anderson_block_failure(*b) == 0 for b in blocks)
+
+
 # ---------------------------------------------------------------------------
 # GPU
 # ---------------------------------------------------------------------------

@@ -455,7 +455,9 @@ int qcl_scba_mixer_info(qcl_scba* ctx, qcl_anderson_info* info);
  * QCL_C64 / QCL_MIXED to QCL_C128 for the steps that follow.  The current
  * state (with the last step's mixing committed) is converted exactly to
  * complex128 and the next step continues from it; operators switch to their
- * complex128 copies; the Anderson history restarts.  The scheme "FP32 bulk,
+ * complex128 copies; the Anderson history restarts, and its causality guard
+ * keeps budgets at the FP32 roundoff the converted state carries (at FP64
+ * roundoff nearly every block of it would fail).  The scheme "FP32 bulk,
  * FP64 refinement of the fixed point": iterate in mixed precision
  * until r_Sigma reaches its FP32 floor, then converge in FP64 (no reference
  * counterpart: the reference has no reduced precision,

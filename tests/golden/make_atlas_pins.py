@@ -16,7 +16,12 @@ tests/golden/atlas_pins.npz:
   (basis_metrics.csv, method energy: 1 - outside_central_weight) and the
   local density of states on the central rows (spectral_population.csv,
   atlas lines 224-247: eta = 2 meV, 181 energies), summed over z, against
-  the Dyson solve G^R = ((E + i eta) I - H)^-1.
+  the Dyson solve G^R = ((E + i eta) I - H)^-1;
+* the occupied part of that density of states (the same CSV's
+  occupied_per_meV_nm: the Fermi function at the chemical potential and
+  lattice temperature of optical_parameters.csv times the density of
+  states), against the equilibrium Keldysh function of the seed,
+  G^< = -f (G^R - G^A) (_seed_green_production, seed.jl:151-197).
 
 The CSVs are output of the reference's Julia code (12 significant digits);
 they are read from the reference checkout, which only this script needs:
@@ -66,8 +71,11 @@ def main(ref):
     E = sorted({float(r["energy_meV"]) for r in spec})
     dz = float(par["period"]) / float(par["spatial_points_per_period"])
     ldos = {e: 0.0 for e in E}
+    occ = {e: 0.0 for e in E}
     for r in spec:
         ldos[float(r["energy_meV"])] += float(r["ldos_per_meV_nm"]) * dz
+        occ[float(r["energy_meV"])] += float(r["occupied_per_meV_nm"]) * dz
+    opt = rows(os.path.join(data, "optical_parameters.csv"))[0]
     np.savez_compressed(
         os.path.join(HERE, "atlas_pins.npz"),
         z_nm=z, psi_a=pa, psi_b=pb,
@@ -81,6 +89,8 @@ def main(ref):
         hartree_meV=np.array([float(r["hartree_meV"]) for r in har]),
         H_pzp_meV=H, levels_meV=levels, central_weight=central_weight, eta_meV=2.0,
         spectral_E_meV=np.array(E), central_dos_per_meV=np.array([ldos[e] for e in E]),
+        central_occupied_per_meV=np.array([occ[e] for e in E]),
+        mu_meV=float(opt["chemical_potential_meV"]), temperature_K=float(opt["temperature_K"]),
     )
 
 

@@ -21,7 +21,12 @@ tests/golden/atlas_pins.npz by tests/golden/make_atlas_pins.py:
   numerics/optimized/production_operators.jl:1337-1385, with Sigma^R = 0):
   tr G^R against sum_n 1 / (E + i eta - e_n), and the central density of
   states sum_n w_n (-Im G_nn / pi) in the eigenbasis against the LDOS summed
-  over z.  CPU: the oracle's retarded_green; GPU: the Dyson kernel.
+  over z.  CPU: the oracle's retarded_green; GPU: the Dyson kernel;
+* spectral_population.csv's occupied column with optical_parameters.csv
+  (mu = 60 meV, T = 200 K): the Fermi function times that density of states
+  -- the equilibrium Keldysh function G^< = -f (G^R - G^A) of the SCBA seed
+  (_seed_green_production, numerics/optimized/seed.jl:151-197), with the
+  oracle's fermi() and the CODATA Boltzmann constant.
 
 The CSVs carry 12 significant digits; the form factors and the Hartree
 energy agree to about 1e-12, the spectral pins to about 1e-10.
@@ -111,3 +116,21 @@ def test_gpu_dyson_reproduces_reference_spectrum(gpu_ops, precision, tol):
                                 precision=precision)
     err_tr, err_dos = _spectral_checks(np.asarray(GR, dtype=np.complex128))
     assert err_tr < tol and err_dos < tol, (err_tr, err_dos)
+
+
+def test_seed_keldysh_function_reproduces_reference_occupation(orc):
+    """-i G^< / 2 pi of G^< = -f (G^R - G^A) on the central states against
+    the reference's occupied density of states (Fermi function at 60 meV and
+    200 K times the density of states, summed over z)."""
+    d = _pins()
+    E, h, sig, eta = _spectral_inputs()
+    GR = orc.retarded_green(E, h, sig, eta=eta)[0]
+    kBT = 8.617333262e-5 * 1e3 * float(d["temperature_K"])  # meV; CODATA 2018 k_B (domain/constants.jl)
+    f = orc.fermi(E, float(d["mu_meV"]), kBT)
+    GL = -f[:, None, None, None] * (GR - np.conj(np.transpose(GR, (0, 1, 3, 2))))
+    H = d["H_pzp_meV"]
+    _, V = np.linalg.eigh(0.5 * (H + H.conj().T))
+    Ln = np.einsum("an,eab,bn->en", V.conj(), GL[:, 0], V)
+    occ = (np.real(-1j * Ln) / (2 * math.pi)) @ d["central_weight"]
+    ref = d["central_occupied_per_meV"]
+    assert float(np.max(np.abs(occ - ref)) / np.max(ref)) < 1e-9

@@ -955,6 +955,102 @@ def scba(problem, iterations, verify=True, state=None, keep_state=False, termina
 
 
 # --------------------------------------------------------------------------
+# FP64 reference gradient of the converged current (the reference has no
+# derivatives).  At a fixed point Sigma = Phi(Sigma, p) of the map of one
+# SCBA iteration without mixing, dJ/dp = J_Sigma v + J_p with
+# (I - Phi_Sigma) v = Phi_p.  Phi_Sigma v and J_Sigma v are central
+# directional differences of the map (the map is smooth away from the switch
+# of the paired normalisation), the linear system is solved by GMRES on the
+# physical subspace (Sigma^<, Sigma^> anti-Hermitian per block), and Phi_p,
+# J_p are central differences of one map application at p +- h.
+# --------------------------------------------------------------------------
+def scba_map(problem, families, plans=None):
+    """One SCBA iteration without the mixing step (the order of scba()):
+    totals, Dyson/Keldysh with the paired normalisation, the scattering and
+    embedding candidates, and J of the state.  `families` lists the
+    mechanisms' (R, <, >) tuples in problem order, then plus and minus.
+    Returns (candidate families in the same order, J)."""
+    plans = plans or make_plans(problem)
+    M = len(problem.mechanisms)
+    scattering = {m.name: families[i] for i, m in enumerate(problem.mechanisms)}
+    plus, minus = families[M], families[M + 1]
+    total = total_family(problem, scattering, plus, minus)
+    green, _ = current_green(problem, total)
+    cand, _ = scattering_candidate(problem, green, plans, verify=False)
+    cplus, cminus = embedding_candidate(problem, green, plans)
+    J = current(problem, plus[2], plus[1], green["GL"], green["GG"]) * problem.J0
+    return [tuple(cand[m.name]) for m in problem.mechanisms] + [tuple(cplus), tuple(cminus)], J
+
+
+def _flatten(families):
+    return np.concatenate([np.ravel(c, order="F").view(np.float64) for f in families for c in f])
+
+
+def _unflatten(x, like):
+    out, i = [], 0
+    for f in like:
+        comps = []
+        for c in f:
+            n = 2 * c.size
+            comps.append(np.asfortranarray(x[i:i + n].view(np.complex128).reshape(c.shape, order="F")))
+            i += n
+        out.append(tuple(comps))
+    return out
+
+
+def _physical(families):
+    """Sigma^< and Sigma^> of every family projected on their anti-Hermitian
+    part (the subspace the map keeps)."""
+    return [tuple(c if k == 0 else 0.5 * (c - np.conj(np.swapaxes(c, -1, -2))) for k, c in enumerate(f))
+            for f in families]
+
+
+def implicit_gradient(build, p0, steps, iterations=2000, rtol=1e-9):
+    """dJ/dp_k at p0 for the problem family build(p): the SCBA converged by
+    `iterations` linear-mixing steps (its last state is the fixed point to
+    the map's roundoff), then the implicit-function derivative above.
+    Returns (gradient, J, r_Sigma of the last iteration)."""
+    import scipy.sparse.linalg as sla
+
+    p0 = np.asarray(p0, dtype=np.float64)
+    pr = build(p0)
+    hist, st = scba(pr, iterations, verify=False, keep_state=True)
+    fams = [tuple(np.array(c) for c in st["scattering"][m.name]) for m in pr.mechanisms]
+    fams += [tuple(np.array(c) for c in st["plus"]), tuple(np.array(c) for c in st["minus"])]
+    plans = make_plans(pr)
+    x0 = _flatten(fams)
+    scale = np.linalg.norm(x0)
+
+    def directional(v):
+        e = 1e-6 * scale / max(np.linalg.norm(v), 1e-300)
+        a, Ja = scba_map(pr, _unflatten(x0 + e * v, fams), plans)
+        b, Jb = scba_map(pr, _unflatten(x0 - e * v, fams), plans)
+        return (_flatten(a) - _flatten(b)) / (2 * e), (Ja - Jb) / (2 * e)
+
+    def project(x):
+        return _flatten(_physical(_unflatten(x, fams)))
+
+    def matvec(v):  # identity off the physical subspace keeps the operator regular
+        pv = project(v)
+        return v - project(directional(pv)[0])
+
+    n = x0.size
+    A = sla.LinearOperator((n, n), matvec=matvec, dtype=np.float64)
+    grad = []
+    for k, h in enumerate(steps):
+        e = np.zeros_like(p0)
+        e[k] = h
+        a, Ja = scba_map(build(p0 + e), fams)
+        b, Jb = scba_map(build(p0 - e), fams)
+        rhs = project((_flatten(a) - _flatten(b)) / (2 * h))
+        v, info = sla.gmres(A, rhs, rtol=rtol, atol=0.0, restart=100, maxiter=5)
+        if info < 0:
+            raise OracleError(5, "implicit gradient: GMRES breakdown")
+        grad.append(directional(v)[1] + (Ja - Jb) / (2 * h))
+    return np.array(grad), hist[-1]["J"], hist[-1]["rSigma"]
+
+
+# --------------------------------------------------------------------------
 # The reference's production path on the host cores with library arithmetic
 # (the CPU baseline of the benchmark): LAPACK through numpy (OpenBLAS) for
 # the per-block inverse and products, pocketfft (scipy.fft) for the Hilbert

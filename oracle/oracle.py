@@ -542,8 +542,11 @@ def total_family(problem, scattering, plus, minus):
     return tuple(tot)
 
 
-def current_green(problem, total):
-    """_current_green_production (numerics/optimized/production_state.jl)."""
+def current_green(problem, total, branch=0):
+    """_current_green_production (numerics/optimized/production_state.jl).
+    `branch` forces the form of the paired normalisation (1: scale G^<,
+    2: move G^> weight into G^<; 0: the reference's choice by number versus
+    target), as qcl_scba_set_normalization_branch does on the device."""
     GR, GL, GG, scale = dyson_keldysh(problem.eps, problem.h, total[0], total[1], total[2])
     number = number_functional(GL, problem.wE, problem.wk, problem.gs)
     lam = number / problem.target
@@ -558,6 +561,10 @@ def current_green(problem, total):
                     normalized=number_functional(GL, problem.wE, problem.wk, problem.gs)), lam
     holes = -number_functional(GG, problem.wE, problem.wk, problem.gs)
     a, c, lam = paired_coefficients(number, holes, problem.target)
+    if branch == 1:
+        a, c = problem.target / number, 0.0
+    elif branch == 2:
+        a, c = 1.0, (problem.target - number) / holes
     normalize_pair(GL, GG, a, c)
     return dict(GR=GR, GL=GL, GG=GG, scale=scale, number=number, holes=holes, a=a, c=c,
                 normalized=number_functional(GL, problem.wE, problem.wk, problem.gs)), lam
@@ -964,18 +971,19 @@ def scba(problem, iterations, verify=True, state=None, keep_state=False, termina
 # physical subspace (Sigma^<, Sigma^> anti-Hermitian per block), and Phi_p,
 # J_p are central differences of one map application at p +- h.
 # --------------------------------------------------------------------------
-def scba_map(problem, families, plans=None):
+def scba_map(problem, families, plans=None, branch=0):
     """One SCBA iteration without the mixing step (the order of scba()):
-    totals, Dyson/Keldysh with the paired normalisation, the scattering and
-    embedding candidates, and J of the state.  `families` lists the
-    mechanisms' (R, <, >) tuples in problem order, then plus and minus.
-    Returns (candidate families in the same order, J)."""
+    totals, Dyson/Keldysh with the paired normalisation (`branch` as in
+    current_green), the scattering and embedding candidates, and J of the
+    state.  `families` lists the mechanisms' (R, <, >) tuples in problem
+    order, then plus and minus.  Returns (candidate families in the same
+    order, J)."""
     plans = plans or make_plans(problem)
     M = len(problem.mechanisms)
     scattering = {m.name: families[i] for i, m in enumerate(problem.mechanisms)}
     plus, minus = families[M], families[M + 1]
     total = total_family(problem, scattering, plus, minus)
-    green, _ = current_green(problem, total)
+    green, _ = current_green(problem, total, branch)
     cand, _ = scattering_candidate(problem, green, plans, verify=False)
     cplus, cminus = embedding_candidate(problem, green, plans)
     J = current(problem, plus[2], plus[1], green["GL"], green["GG"]) * problem.J0
@@ -1005,11 +1013,14 @@ def _physical(families):
             for f in families]
 
 
-def implicit_gradient(build, p0, steps, iterations=2000, rtol=1e-9):
+def implicit_gradient(build, p0, steps, iterations=2000, rtol=1e-9, hold_branch=True):
     """dJ/dp_k at p0 for the problem family build(p): the SCBA converged by
     `iterations` linear-mixing steps (its last state is the fixed point to
-    the map's roundoff), then the implicit-function derivative above.
-    Returns (gradient, J, r_Sigma of the last iteration)."""
+    the map's roundoff), then the implicit-function derivative above.  With
+    `hold_branch` every map application uses the paired normalisation's form
+    at the fixed point (a fixed point near the switch between the two forms
+    would otherwise see the kink in its differences).  Returns (gradient, J,
+    r_Sigma of the last iteration, the form held: 1 or 2, 0 if none)."""
     import scipy.sparse.linalg as sla
 
     p0 = np.asarray(p0, dtype=np.float64)
@@ -1018,13 +1029,19 @@ def implicit_gradient(build, p0, steps, iterations=2000, rtol=1e-9):
     fams = [tuple(np.array(c) for c in st["scattering"][m.name]) for m in pr.mechanisms]
     fams += [tuple(np.array(c) for c in st["plus"]), tuple(np.array(c) for c in st["minus"])]
     plans = make_plans(pr)
+    branch = 0
+    if hold_branch:
+        M = len(pr.mechanisms)
+        total = total_family(pr, {m.name: fams[i] for i, m in enumerate(pr.mechanisms)}, fams[M], fams[M + 1])
+        green, _ = current_green(pr, total)
+        branch = 1 if green["number"] >= pr.target else 2
     x0 = _flatten(fams)
     scale = np.linalg.norm(x0)
 
     def directional(v):
         e = 1e-6 * scale / max(np.linalg.norm(v), 1e-300)
-        a, Ja = scba_map(pr, _unflatten(x0 + e * v, fams), plans)
-        b, Jb = scba_map(pr, _unflatten(x0 - e * v, fams), plans)
+        a, Ja = scba_map(pr, _unflatten(x0 + e * v, fams), plans, branch)
+        b, Jb = scba_map(pr, _unflatten(x0 - e * v, fams), plans, branch)
         return (_flatten(a) - _flatten(b)) / (2 * e), (Ja - Jb) / (2 * e)
 
     def project(x):
@@ -1040,14 +1057,14 @@ def implicit_gradient(build, p0, steps, iterations=2000, rtol=1e-9):
     for k, h in enumerate(steps):
         e = np.zeros_like(p0)
         e[k] = h
-        a, Ja = scba_map(build(p0 + e), fams)
-        b, Jb = scba_map(build(p0 - e), fams)
+        a, Ja = scba_map(build(p0 + e), fams, branch=branch)
+        b, Jb = scba_map(build(p0 - e), fams, branch=branch)
         rhs = project((_flatten(a) - _flatten(b)) / (2 * h))
         v, info = sla.gmres(A, rhs, rtol=rtol, atol=0.0, restart=100, maxiter=5)
         if info < 0:
             raise OracleError(5, "implicit gradient: GMRES breakdown")
         grad.append(directional(v)[1] + (Ja - Jb) / (2 * h))
-    return np.array(grad), hist[-1]["J"], hist[-1]["rSigma"]
+    return np.array(grad), hist[-1]["J"], hist[-1]["rSigma"], branch
 
 
 # --------------------------------------------------------------------------

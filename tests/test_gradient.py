@@ -95,10 +95,11 @@ def test_stack_bias_derivative_holds_the_normalisation_form(gpu_ops):
     1.4e-3 off the derivative, which Richardson extrapolation of those
     differences puts at -1.0712050e6 per mV.  With the explicit part's own
     step at 0.1 mV the implicit derivative was -1.0715e6 (2.8e-4 off, the
-    O(h^2) error of that step).  The test takes the explicit step at 0.01 mV
-    and checks against the Richardson combination of the converged-solve
-    differences at 0.1 and 0.05 mV; expected agreement a few 1e-6, asserted
-    at 1e-3."""
+    error of that step; the oracle's FP64 implicit gradient with the branch
+    held gives -1.0715221e6 at that step and -1.0712342e6, 2.7e-5 off, at
+    0.01 mV).  The test takes the explicit step at 0.01 mV and checks
+    against the Richardson combination of the converged-solve differences at
+    0.1 and 0.05 mV; expected agreement about 3e-5, asserted at 1e-3."""
     from qclb200.gradient import central_difference, implicit_derivatives
 
     got = implicit_derivatives(_build_stack_bias, [50.0], [0.01], tol=1e-12, tangent_tol=1e-9, max_tangent=5000)

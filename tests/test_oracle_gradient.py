@@ -26,7 +26,7 @@ def _build(p):
 def test_oracle_implicit_gradient_matches_converged_differences(orc):
     p0 = np.array([0.31, 0.05])  # E^p off the energy nodes: the shift interpolation is smooth there
     steps = [1e-4, 1e-5]
-    grad, J, rS = orc.implicit_gradient(_build, p0, steps, iterations=900)
+    grad, J, rS, _ = orc.implicit_gradient(_build, p0, steps, iterations=900)
     assert rS < 1e-14
     for k, h in enumerate(steps):
         e = np.zeros(2)

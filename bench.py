@@ -714,19 +714,18 @@ def bias_sweep(torch, npoints=64, iters=5, classes=((2, 8), (3, 8), (4, 8), (6, 
     structure classes (periods x states; by default N_b = 16 ... 48) and
     energy grids N_E from NE_choices, N_k momenta, LO + acoustic + IFR, mixed
     precision, the Dyson CTA shape of every class from the autotuner; `iters`
-    iterations per point.  The
-    batched run (qcl_sweep_run: resident points in one graph launch per
-    iteration) against the same points one after another (qcl_scba_step),
-    in SCBA iterations per second, and the largest J difference between the
-    two (the same kernels run, so it is zero).  Both wall times run from the
-    first host-side preparation of a point to the last row (qcl_sweep_run's
-    own wall time, without the preparation, is in batched.wall_s).  With
-    `iterations_only` the
-    iterations are also timed without context creation, seeds and graph
-    captures: each sequential point runs `iters` more iterations, timed on
-    their own, and the batched sweep runs again with 2 `iters` iterations per
-    point, the difference of the two batched wall times being its `iters`
-    iterations of every point."""
+    iterations per point.  The batched run (qcl_sweep_run: resident points
+    in one graph launch per iteration) against the same points one after
+    another (qcl_scba_step), in SCBA iterations per second, and the largest J
+    difference between the two (the same kernels run, so it is zero).  Both
+    wall times run from the first host-side preparation of a point to the
+    last row (qcl_sweep_run's own wall time, without the preparation, is in
+    batched.wall_s).  With `iterations_only` the iterations are also timed
+    without context creation, seeds and graph captures: each sequential
+    point runs `iters` more iterations, timed on their own, and the batched
+    sweep runs again with 2 `iters` iterations per point, the difference of
+    the two batched wall times being its `iters` iterations of every
+    point."""
     import numpy as np
     from qclb200 import operators
     from qclb200.problem import bias_sweep_problems
@@ -797,11 +796,12 @@ def bias_sweep(torch, npoints=64, iters=5, classes=((2, 8), (3, 8), (4, 8), (6, 
 
 
 def bias_sweep_small(torch, npoints=64, iters=30):
-    """The batched sweep where one point does not fill the GPU: 64 bias points
-    of small structures (N_b = 12 and 16 as 3 x 4, 2 x 6 and 2 x 8 periods x
-    states; N_E in 256 ... 512, N_k = 8; LO + acoustic + IFR, mixed), whose
-    iterations are launch- and latency-bound alone and run side by side as
-    the child graphs of one launch."""
+    """The batched sweep at the small end: 64 bias points of small
+    structures (N_b = 12 and 16 as 3 x 4, 2 x 6 and 2 x 8 periods x states;
+    N_E in 256 ... 512, N_k = 8; LO + acoustic + IFR, mixed), the sizes
+    where one point's kernels are shortest and running the points' iteration
+    graphs side by side has the most to gain; the iterations are also timed
+    apart from the set-up."""
     return bias_sweep(torch, npoints=npoints, iters=iters, classes=((3, 4), (2, 6), (2, 8)),
                       NE_choices=(256, 384, 512), Nk=8, Nqz=101, Nphi=32, iterations_only=True)
 
